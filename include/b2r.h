@@ -1,0 +1,360 @@
+/*
+ * b2r.h -- C ABI of the B200 RAPTOR engine (drop-in behind nigiri's routing
+ * seam).
+ *
+ * Everything crosses this boundary as plain pointers, sizes and PODs; every
+ * entry point returns an int status (B2R_OK == 0, negative on error) and never
+ * throws.  The last error message of the calling thread is available through
+ * b2r_last_error().
+ *
+ * Reference seam being replaced (paths relative to the nigiri source tree):
+ *  - routing::raptor_search(tt, rtt, search_state&, AlgoState&, query, dir)
+ *      src/routing/raptor_search.cc:94-159, instantiated for raptor_state and
+ *      gpu::gpu_raptor_state at src/routing/raptor_search.cc:161-177
+ *  - the Algo concept driven by routing::search<Dir, Algo>
+ *      include/nigiri/routing/search.h:148-171 (construction),
+ *      search.h:436-475 (next_start_time / add_start / execute / reconstruct)
+ *  - routing::one_to_all<Dir>  src/routing/one_to_all.cc:52-104
+ *  - routing::gpu::gpu_timetable / gpu_raptor_state (device image + state)
+ *      include/nigiri/routing/gpu/raptor.h:23-129
+ *
+ * Time conventions follow nigiri: unixtime = int32 minutes since 1970-01-01
+ * (unixtime_t, include/nigiri/types.h:360); days = int32 days since
+ * 1970-01-01 (date::sys_days); round times are int16 minutes relative to a
+ * per-query base day (delta_t, include/nigiri/common/delta_t.h:11-59).
+ */
+#ifndef B2R_H_
+#define B2R_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+enum b2r_status {
+  B2R_OK = 0,
+  B2R_ERR_INVALID_ARGUMENT = -1,
+  B2R_ERR_CUDA = -2,
+  B2R_ERR_OUT_OF_MEMORY = -3, /* HBM budget or device allocation exhausted */
+  B2R_ERR_CAPACITY = -4,      /* a per-query fixed-size buffer overflowed */
+  B2R_ERR_NOT_READY = -5,     /* b2r_poll: ticket still running */
+  B2R_ERR_DEVICE_STATUS = -6, /* a kernel wrote an error status word */
+  B2R_ERR_UNSUPPORTED = -7,
+  B2R_ERR_INTERNAL = -8
+};
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* b2r_last_error(void);
+
+/* ------------------------------------------------------- constants */
+#define B2R_MAX_TRANSFERS 14 /* routing/limits.h:9 kMaxTransfers */
+#define B2R_K 16             /* kMaxTransfers + 2 round rows */
+#define B2R_MAX_TRAVEL_TIME_MIN 7200 /* routing/limits.h:10 kMaxTravelTime */
+#define B2R_MAX_DAYS 512             /* types.h:62 kMaxDays */
+#define B2R_TIMETABLE_OFFSET_DAYS 5  /* types.h:53 kTimetableOffset */
+#define B2R_N_SPECIAL_STATIONS 9     /* special_stations.h:7-19 */
+#define B2R_SPECIAL_START 0u
+#define B2R_SPECIAL_END 1u
+#define B2R_INVALID_IDX 0xFFFFFFFFu
+#define B2R_UNREACHABLE 0xFFFFu
+
+/* Location types used by location_match_mode::kIntermodal
+ * (for_each_meta.h:29-35 reads kGeneratedTrack children). */
+#define B2R_LOC_STATION 0u
+#define B2R_LOC_TRACK 1u
+#define B2R_LOC_GENERATED_TRACK 2u
+
+/* Packed words, bit-identical to nigiri's:
+ *  stop      (stop.h:86-89):      location:28 | in:1 | out:1 | in_wc:1 | out_wc:1
+ *  footpath  (footpath.h:81-82):  target:23 | duration:9
+ *  delta     (types.h:619-620):   days:5 | mam:11 (days in the low bits) */
+#define B2R_STOP_LOC(w) ((w)&0x0FFFFFFFu)
+#define B2R_STOP_IN(w) (((w) >> 28) & 1u)
+#define B2R_STOP_OUT(w) (((w) >> 29) & 1u)
+#define B2R_STOP_IN_WC(w) (((w) >> 30) & 1u)
+#define B2R_STOP_OUT_WC(w) (((w) >> 31) & 1u)
+#define B2R_FP_TARGET(w) ((w)&0x7FFFFFu)
+#define B2R_FP_DURATION(w) ((w) >> 23)
+#define B2R_DELTA_DAYS(d) ((int)((d)&0x1Fu))
+#define B2R_DELTA_MAM(d) ((int)((d) >> 5))
+
+/* ------------------------------------------------------- timetable image */
+/*
+ * Flattened timetable: the arrays the RAPTOR hot path reads
+ * (timetable.h:341-398, locations_ 89-98).  CSR pairs are (index[n+1], data).
+ * All pointers are host memory owned by the caller; b2r_timetable_upload
+ * copies them into one device-resident image.
+ */
+typedef struct b2r_timetable_desc {
+  uint32_t n_locations; /* incl. the 9 special stations at 0..8 */
+  uint32_t n_routes;
+  uint32_t n_transports;
+  uint32_t n_bitfields;
+  int32_t date_range_from; /* days since epoch, timetable::date_range_.from_ */
+  int32_t date_range_to;   /* days since epoch, exclusive */
+
+  /* locations */
+  const uint8_t* transfer_time;   /* [n_locations] minutes (u8_minutes) */
+  const uint32_t* parent;         /* [n_locations] or NULL (no parents) */
+  const uint8_t* location_type;   /* [n_locations] or NULL (all stations) */
+  const uint32_t* children_index; /* CSR or NULL */
+  const uint32_t* children;
+  const uint32_t* importance; /* [n_locations] or NULL (assign_importance) */
+  uint32_t max_importance;
+  const uint32_t* footpaths_out_index; /* CSR, footpaths_out_[0] */
+  const uint32_t* footpaths_out;
+  const uint32_t* footpaths_in_index; /* CSR, footpaths_in_[0] */
+  const uint32_t* footpaths_in;
+
+  /* routes */
+  const uint32_t* route_stop_index; /* CSR route_location_seq_ */
+  const uint32_t* route_stops;
+  const uint32_t* route_transport_from; /* [n_routes] first transport */
+  const uint32_t* route_transport_to;   /* [n_routes] one past last */
+  const uint32_t* route_stop_time_from; /* [n_routes] route_stop_time_ranges_ */
+  const uint16_t* route_stop_times;     /* packed delta */
+  uint64_t n_route_stop_times;
+  const uint32_t* route_traffic_days;     /* [n_routes] bitfield index */
+  const uint32_t* transport_traffic_days; /* [n_transports] bitfield index */
+  const uint32_t* transport_route;        /* [n_transports] */
+  const uint64_t* bitfields;              /* [n_bitfields * 8] 512-bit sets */
+  const uint32_t* location_routes_index;  /* CSR location_routes_ */
+  const uint32_t* location_routes;
+
+  /* lower-bound graphs (build_lb_graph.h:11-99), packed footpath words */
+  const uint32_t* lb_fwd_index;
+  const uint32_t* lb_fwd;
+  const uint32_t* lb_bwd_index;
+  const uint32_t* lb_bwd;
+} b2r_timetable_desc;
+
+/* ------------------------------------------------------------- queries */
+enum b2r_direction { B2R_FORWARD = 0, B2R_BACKWARD = 1 };
+enum b2r_match_mode { /* location_match_mode.h:5-10 */
+  B2R_MATCH_EXACT = 0,
+  B2R_MATCH_ONLY_CHILDREN = 1,
+  B2R_MATCH_EQUIVALENT = 2,
+  B2R_MATCH_INTERMODAL = 3
+};
+enum b2r_query_kind {
+  B2R_ONE_TO_ONE = 0, /* search<Dir, raptor<..., kOneToOne>> */
+  B2R_ONE_TO_ALL = 1  /* one_to_all<Dir> */
+};
+
+/* routing::offset, query.h:28-48 */
+typedef struct b2r_offset {
+  uint32_t target;
+  int16_t duration; /* minutes */
+  int16_t pad_;
+  int32_t transport_mode_id;
+} b2r_offset;
+
+/* routing::query, query.h:70-100, restricted to the static (no rtt, no
+ * vias, no td offsets, no filters, profile 0) instantiation. */
+typedef struct b2r_query {
+  uint8_t kind;      /* b2r_query_kind */
+  uint8_t direction; /* b2r_direction */
+  uint8_t is_interval;
+  uint8_t start_match_mode;
+  uint8_t dest_match_mode;
+  uint8_t use_start_footpaths;
+  uint8_t extend_interval_earlier;
+  uint8_t extend_interval_later;
+  int32_t start_time;    /* ontrip start (unixtime) */
+  int32_t interval_from; /* pretrip start interval [from, to) */
+  int32_t interval_to;
+  const b2r_offset* start;
+  uint32_t n_start;
+  const b2r_offset* destination;
+  uint32_t n_destination;
+  int16_t max_start_offset; /* default 7200 */
+  uint8_t max_transfers;    /* default 14 */
+  uint8_t has_fastest_direct;
+  int16_t max_travel_time; /* default 7200 */
+  int16_t fastest_direct;
+  uint32_t min_connection_count;
+  double fastest_direct_factor; /* default 1.0 */
+  /* transfer_time_settings, transfer_time_settings.h:8-18 */
+  uint8_t tts_default; /* 1 = identity */
+  uint8_t pad_[3];
+  int16_t tts_min_transfer_time;
+  int16_t tts_additional_time;
+  float tts_factor;
+} b2r_query;
+
+/* Fill a query with nigiri's defaults (query.h:84-99). */
+void b2r_query_init(b2r_query* q);
+
+/* ------------------------------------------------------------- results */
+enum b2r_leg_kind {
+  B2R_LEG_TRANSPORT = 0, /* journey::run_enter_exit */
+  B2R_LEG_FOOTPATH = 1,  /* footpath */
+  B2R_LEG_OFFSET = 2     /* routing::offset (first / last mile) */
+};
+
+/* journey::leg, journey.h:42-82 */
+typedef struct b2r_leg {
+  uint32_t from;
+  uint32_t to;
+  int32_t dep_time; /* unixtime */
+  int32_t arr_time;
+  uint8_t kind;
+  uint8_t pad_;
+  uint16_t day;        /* transport: traffic day index */
+  uint32_t transport;  /* transport idx | footpath/offset target */
+  uint16_t stop_from;  /* transport: stop_range_ [from, to) */
+  uint16_t stop_to;
+  int16_t duration;    /* footpath / offset duration */
+  int16_t pad2_;
+  int32_t transport_mode_id; /* offset */
+} b2r_leg;
+
+/* journey, journey.h:84-118 */
+typedef struct b2r_journey {
+  int32_t start_time;
+  int32_t dest_time;
+  uint32_t dest;
+  uint8_t transfers;
+  uint8_t error;
+  uint16_t n_legs;
+  uint32_t first_leg; /* index into the result's leg array */
+} b2r_journey;
+
+/* Per-query result.  journeys/legs point into engine-owned memory valid
+ * until the next call on the same engine (or b2r_result_release). */
+typedef struct b2r_result {
+  int32_t status; /* B2R_OK or an error for this query alone */
+  uint32_t n_journeys;
+  const b2r_journey* journeys;
+  const b2r_leg* legs;
+  int32_t interval_from; /* routing_result::interval_ */
+  int32_t interval_to;
+  /* one_to_all: round_times rows k = 0..n_rows-1, each n_locations int16
+   * deltas relative to base_day (raptor_state::round_times_). */
+  uint32_t n_rows;
+  int32_t base_day; /* days since epoch */
+  const int16_t* round_times;
+  /* counters (raptor_stats) */
+  uint64_t n_rounds;
+  uint64_t n_start_times;
+} b2r_result;
+
+/* ---------------------------------------------------------------- engine */
+typedef struct b2r_timetable b2r_timetable; /* device image handle */
+typedef struct b2r_engine b2r_engine;       /* state pool + streams */
+
+/* Upload the flattened timetable once; the handle owns the device copy. */
+int b2r_timetable_upload(const b2r_timetable_desc* desc, int device,
+                         b2r_timetable** out);
+int b2r_timetable_destroy(b2r_timetable* tt);
+/* Device bytes held by the image. */
+uint64_t b2r_timetable_device_bytes(const b2r_timetable* tt);
+
+typedef struct b2r_engine_config {
+  uint32_t max_slots;       /* queries resident at once (multiple of 32) */
+  uint64_t hbm_budget;      /* bytes of raptor state the pool may hold */
+  uint32_t max_journeys;    /* per-query pareto set capacity (default 128) */
+  uint32_t host_threads;    /* host prep threads (0 = hardware) */
+  uint32_t use_lower_bounds;/* 1 = dijkstra lower bounds (reference default) */
+  uint32_t use_graphs;      /* 1 = capture the super-step in a CUDA graph */
+  uint32_t route_block;     /* launch shape: warps per CTA in the route scan */
+  uint32_t reserved[7];
+} b2r_engine_config;
+
+void b2r_engine_config_init(b2r_engine_config* c);
+
+/* Create an engine bound to one timetable image.  Admission is bounded by
+ * cfg->hbm_budget: the slot count is min(max_slots, budget / bytes_per_slot). */
+int b2r_engine_create(b2r_timetable* tt, const b2r_engine_config* cfg,
+                      b2r_engine** out);
+int b2r_engine_destroy(b2r_engine* e);
+/* Bytes of device state one resident query needs. */
+uint64_t b2r_engine_bytes_per_slot(const b2r_engine* e);
+uint32_t b2r_engine_slots(const b2r_engine* e);
+
+/* Batched search: runs n queries (any mix of kinds and directions) through
+ * the resident slot pool with continuous admission and blocks until all are
+ * done.  out[i] receives query i's result. */
+int b2r_search_batch(b2r_engine* e, const b2r_query* qs, uint32_t n,
+                     b2r_result* out);
+
+/* Plain engine: one query, per-round kernel launches from the host and a
+ * synchronisation per query (the launch pattern of nigiri's
+ * src/routing/gpu/raptor.cu:894-990).  Same results as b2r_search_batch. */
+int b2r_search_plain(b2r_engine* e, const b2r_query* q, b2r_result* out);
+
+/* Serving: asynchronous submission.  Queries are admitted into free slots at
+ * super-step boundaries by a driver thread; results are fetched by ticket. */
+int b2r_serve_start(b2r_engine* e);
+int b2r_serve_stop(b2r_engine* e);
+int b2r_submit(b2r_engine* e, const b2r_query* q, uint64_t* ticket);
+/* B2R_OK when done (result copied into *out, valid until b2r_release),
+ * B2R_ERR_NOT_READY otherwise. */
+int b2r_poll(b2r_engine* e, uint64_t ticket, b2r_result* out);
+int b2r_wait(b2r_engine* e, uint64_t ticket, b2r_result* out);
+int b2r_release(b2r_engine* e, uint64_t ticket);
+
+/* Timing of the last b2r_search_batch: device milliseconds of the kernels
+ * and the number of kernel launches issued (graph nodes included). */
+typedef struct b2r_batch_stats {
+  double device_ms;
+  double host_prep_ms;
+  uint64_t kernel_launches;
+  uint64_t super_steps;
+  uint64_t route_scan_launches;
+  double route_scan_ms;
+} b2r_batch_stats;
+int b2r_last_batch_stats(const b2r_engine* e, b2r_batch_stats* s);
+
+/* ------------------------------------------- host timetable construction */
+/* Host-side timetable builder (not on the hot path): the synthetic
+ * generator and nigiri's finalize() derivations (footpaths_in,
+ * location_routes, route traffic days, lower-bound graphs, importance),
+ * src/loader/init_finish.cc:64-198, build_lb_graph.h:11-99. */
+typedef struct b2r_host_timetable b2r_host_timetable;
+
+/* Synthetic timetable for workload `config` (1..5) with the given seed. */
+int b2r_tt_generate(uint32_t config, uint64_t seed, b2r_host_timetable** out);
+/* Build from base arrays (locations + routes); derived arrays are
+ * computed here.  route_stop_times must already be in nigiri's layout. */
+typedef struct b2r_tt_base {
+  uint32_t n_locations;
+  int32_t date_range_from;
+  int32_t date_range_to;
+  const uint8_t* transfer_time;
+  const uint32_t* parent; /* or NULL */
+  const uint8_t* location_type;
+  const uint32_t* footpaths_out_index;
+  const uint32_t* footpaths_out;
+  uint32_t n_routes;
+  const uint32_t* route_stop_index;
+  const uint32_t* route_stops;
+  const uint8_t* route_clasz; /* [n_routes] or NULL (all bus) */
+  const uint32_t* route_n_transports;
+  const uint16_t* route_stop_times; /* concatenated per route */
+  const uint32_t* transport_bitfield; /* [n_transports] */
+  uint32_t n_bitfields;
+  const uint64_t* bitfields;
+} b2r_tt_base;
+int b2r_tt_build(const b2r_tt_base* base, b2r_host_timetable** out);
+int b2r_tt_save(const b2r_host_timetable* t, const char* path);
+int b2r_tt_load(const char* path, b2r_host_timetable** out);
+int b2r_tt_desc(const b2r_host_timetable* t, b2r_timetable_desc* out);
+int b2r_tt_destroy(b2r_host_timetable* t);
+
+/* Seeded synthetic query stream of a workload (configs 1..5). */
+typedef struct b2r_query_set b2r_query_set;
+int b2r_queries_generate(const b2r_host_timetable* t, uint32_t config,
+                         uint64_t seed, uint32_t n, b2r_query_set** out);
+uint32_t b2r_queries_count(const b2r_query_set* s);
+const b2r_query* b2r_queries_get(const b2r_query_set* s, uint32_t i);
+int b2r_queries_destroy(b2r_query_set* s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* B2R_H_ */

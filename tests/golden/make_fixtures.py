@@ -1,0 +1,335 @@
+"""Builds tests/golden/cases.json from nigiri's own routing tests.
+
+Run in a checkout that has the nigiri sources (pass their root as argv[1]);
+the output is committed so the test suite never reads the reference at run
+time.
+
+Two kinds of content end up in cases.json:
+  * timetables: the reference tests' tiny GTFS / HRD fixtures, restated by
+    hand as UTC event times (the conversion is written next to each one);
+  * expected results: the golden journey printouts (`R"(...)"` strings) of
+    the reference tests, parsed mechanically from the test sources into
+    (departure, arrival, transfers, legs) records.
+"""
+from __future__ import annotations
+
+import datetime as dt
+import json
+import os
+import re
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def day(s: str) -> int:
+    return (dt.date.fromisoformat(s) - dt.date(1970, 1, 1)).days
+
+
+def hm(s: str) -> int:
+    h, m = s.split(":")[:2]
+    return int(h) * 60 + int(m)
+
+
+# ----------------------------------------------------------------------------
+# Timetables (stop ids / names as printed by the reference tests).
+# Route entries: {"stops": [id,...], "transports": [{"name", "day", "times"}]}
+# where times = [dep(0), arr(1), dep(1), ..., arr(n-1)] in UTC minutes after
+# midnight of `day` (may exceed 1440), i.e. nigiri's per-transport delta times
+# relative to the UTC traffic day.
+# ----------------------------------------------------------------------------
+
+def get_index(route, svc):
+    """Position at which `svc` may join `route` (a list of services sorted
+    by minutes after midnight), or None -- nigiri's FIFO rule on times
+    modulo 1440 at every stop (include/nigiri/loader/get_index.h:8-29)."""
+    key = svc["times"][0] % 1440
+    index = 0
+    while index < len(route) and route[index]["times"][0] % 1440 < key:
+        index += 1
+    for i, x in enumerate(svc["times"]):
+        earlier = index > 0 and x % 1440 < route[index - 1]["times"][i] % 1440
+        later = index < len(route) and x % 1440 > route[index]["times"][i] % 1440
+        if earlier or later:
+            return None
+    return index
+
+
+def group_routes(services):
+    """Services (in load order) -> routes: one route key per stop sequence,
+    split into sub-routes by get_index (gtfs/load_timetable.cc:288-309)."""
+    keys = {}
+    order = []
+    for svc in services:
+        k = tuple(svc["stops"])
+        if k not in keys:
+            keys[k] = [[svc]]
+            order.append(k)
+            continue
+        for sub in keys[k]:
+            idx = get_index(sub, svc)
+            if idx is not None:
+                sub.insert(idx, svc)
+                break
+        else:
+            keys[k].append([svc])
+    routes = []
+    for k in order:
+        for sub in keys[k]:
+            routes.append({"stops": list(k), "transports": [
+                {kk: v for kk, v in x.items() if kk != "stops"} for x in sub]})
+    return routes
+
+
+def utc_service(name, stops, first_day, times):
+    """Normalise a service whose UTC times are given relative to
+    `first_day`: the first departure is moved below 24:00 and the traffic
+    day shifted accordingly (README.md: first departures < 24:00)."""
+    shift = times[0] // 1440
+    d = dt.date.fromisoformat(first_day) + dt.timedelta(days=shift)
+    return {"name": name, "stops": stops, "day": d.isoformat(),
+            "times": [x - 1440 * shift for x in times]}
+
+
+def hrd_abc():
+    """test/loader/hrd/hrd_timetable.h files_abc(): two HRD services on
+    30.03.2020 (bitfield 000005), local time UTC+2 (DST since 29.03 02:00):
+      RE 1337 A 02:30 -> B 03:30, repeated 48 times every 30 min
+      RE 7331 B 02:30 -> C 03:30, repeated 92 times every 15 min
+    -> UTC: departures 00:30 + j*30 min (j = 0..48) and 00:30 + j*15 min
+    (j = 0..92) after 2020-03-30 00:00, each run 60 min."""
+    locs = [("0000001", "A"), ("0000002", "B"), ("0000003", "C"),
+            ("0000004", "D"), ("0000005", "E"), ("0000006", "F"),
+            ("0000007", "G"), ("0000008", "H"), ("0000009", "I"),
+            ("0000010", "F_META")]
+    services = []
+    for j in range(49):
+        dep = 30 + 30 * j
+        services.append(utc_service("RE 1337", ["0000001", "0000002"], "2020-03-30",
+                                    [dep, dep + 60]))
+    for j in range(93):
+        dep = 30 + 15 * j
+        services.append(utc_service("RE 7331", ["0000002", "0000003"], "2020-03-30",
+                                    [dep, dep + 60]))
+    return {
+        "date_range": ["2020-03-28", "2020-03-31"],
+        "locations": [{"id": i, "name": n, "transfer_time": 2} for i, n in locs],
+        "footpaths": [],
+        "routes": group_routes(services),
+    }
+
+
+def gtfs_transfer_time():
+    """test/routing/transfer_time_settings_test.cc test_files: agency
+    Europe/Berlin (UTC+2 on 2019-05-01), service S1 on 2019-05-01 only.
+      T1 (route 1) A 10:00 -> B 10:10      UTC 08:00 -> 08:10
+      T2 (route 2) B 10:13 -> C 10:22      UTC 08:13 -> 08:22
+      T3 (route 2) B 10:20 -> C 10:30      UTC 08:20 -> 08:30
+      T4 (route 3) A 09:55 -> C 10:35      UTC 07:55 -> 08:35
+    Stops are ~300 km apart: no footpaths; transfer time 2 min (GTFS
+    loader default).  Printed trip names are the route short names."""
+    d = "2019-05-01"
+    services = [
+        dict(utc_service("1", ["A", "B"], d, [hm("08:00"), hm("08:10")]), id="T1"),
+        dict(utc_service("2", ["B", "C"], d, [hm("08:13"), hm("08:22")]), id="T2"),
+        dict(utc_service("2", ["B", "C"], d, [hm("08:20"), hm("08:30")]), id="T3"),
+        dict(utc_service("3", ["A", "C"], d, [hm("07:55"), hm("08:35")]), id="T4"),
+    ]
+    return {
+        "date_range": ["2019-05-01", "2019-05-02"],
+        "locations": [{"id": x, "name": x, "transfer_time": 2} for x in "ABC"],
+        "footpaths": [],
+        "routes": group_routes(services),
+    }
+
+
+TIMETABLES = {"hrd_abc": hrd_abc(), "gtfs_transfer_time": gtfs_transfer_time()}
+
+# ----------------------------------------------------------------------------
+# Golden printout parser (journey::print, src/routing/journey.cc)
+# ----------------------------------------------------------------------------
+_TIME = r"(\d{4}-\d{2}-\d{2} \d{2}:\d{2})"
+_LOC = r"\(([^,]*), ([^)]*)\)"
+HEADER = re.compile(r"^\[" + _TIME + r", " + _TIME + r"\]$")
+LEG = re.compile(r"^leg (\d+): " + _LOC + r" \[" + _TIME + r"\] -> " + _LOC +
+                 r" \[" + _TIME + r"\]$")
+FOOTPATH = re.compile(r"^\s+FOOTPATH \(duration=(\d+)\)$")
+MUMO = re.compile(r"^\s+MUMO \(id=(\d+), duration=(\d+)\)$")
+TRIP = re.compile(r"\{name=([^,]*), day=([^,]*), id=([^,]*), src=")
+STOPLINE = re.compile(r"^\s+\d+: ")
+
+
+def unix_min(s: str) -> int:
+    t = dt.datetime.strptime(s, "%Y-%m-%d %H:%M")
+    return int((t - dt.datetime(1970, 1, 1)).total_seconds() // 60)
+
+
+def parse_journeys(text: str):
+    out = []
+    cur = None
+    leg = None
+    for line in text.split("\n"):
+        m = HEADER.match(line)
+        if m:
+            cur = {"dep": unix_min(m.group(1)), "arr": unix_min(m.group(2)),
+                   "transfers": None, "legs": []}
+            out.append(cur)
+            continue
+        if cur is None:
+            continue
+        if line.startswith("TRANSFERS: "):
+            cur["transfers"] = int(line.split(": ")[1])
+            continue
+        m = LEG.match(line)
+        if m:
+            leg = {"from": m.group(3), "to": m.group(6),
+                   "dep": unix_min(m.group(4)), "arr": unix_min(m.group(7)),
+                   "kind": None}
+            cur["legs"].append(leg)
+            continue
+        if leg is None:
+            continue
+        m = FOOTPATH.match(line)
+        if m:
+            leg["kind"] = "footpath"
+            leg["duration"] = int(m.group(1))
+            continue
+        m = MUMO.match(line)
+        if m:
+            leg["kind"] = "offset"
+            leg["mode_id"] = int(m.group(1))
+            leg["duration"] = int(m.group(2))
+            continue
+        if STOPLINE.match(line):
+            leg["kind"] = "transport"
+            leg["n_stops"] = leg.get("n_stops", 0) + 1
+            m = TRIP.search(line)
+            if m and "trip" not in leg:
+                leg["trip"] = m.group(3) if m.group(3) else m.group(1)
+                leg["trip_name"] = m.group(1)
+    return out
+
+
+def raw_string(src: str, name: str) -> str:
+    """Contents of `constexpr auto const <name> = R"(...)"` in src."""
+    m = re.search(r"\b" + re.escape(name) + r"\s*=\s*(?:\n\s*)?R\"(\w*)\(", src)
+    if not m:
+        raise KeyError(name)
+    delim = m.group(1)
+    start = m.end()
+    end = src.index(")" + delim + '"', start)
+    return src[start:end]
+
+
+# ----------------------------------------------------------------------------
+# Cases: query + where its golden printout lives
+# ----------------------------------------------------------------------------
+
+def t(s):  # "2020-03-30 05:00" (UTC) -> unix minutes
+    return unix_min(s)
+
+
+def cases():
+    c = []
+    # test/routing/raptor_test.cc
+    iv = [t("2020-03-30 05:00"), t("2020-03-30 06:00")]
+    c.append(dict(name="raptor_forward", timetable="hrd_abc",
+                  ref="test/routing/raptor_test.cc", golden="fwd_journeys",
+                  query=dict(start=[["0000001", 0, 0]], dest=[["0000003", 0, 0]],
+                             interval=iv, direction="fwd")))
+    c.append(dict(name="raptor_backward", timetable="hrd_abc",
+                  ref="test/routing/raptor_test.cc", golden="bwd_journeys",
+                  query=dict(start=[["0000003", 0, 0]], dest=[["0000001", 0, 0]],
+                             interval=iv, direction="bwd")))
+    # test/routing/raptor_intermodal_test.cc
+    c.append(dict(name="raptor_intermodal_forward", timetable="hrd_abc",
+                  ref="test/routing/raptor_intermodal_test.cc", golden="fwd_journeys",
+                  query=dict(start=[["0000001", 10, 99]], dest=[["0000003", 15, 77]],
+                             interval=iv, direction="fwd", start_mode="intermodal",
+                             dest_mode="intermodal")))
+    c.append(dict(name="raptor_intermodal_backward", timetable="hrd_abc",
+                  ref="test/routing/raptor_intermodal_test.cc", golden="bwd_journeys",
+                  query=dict(start=[["0000003", 15, 99]], dest=[["0000001", 10, 77]],
+                             interval=iv, direction="bwd", start_mode="intermodal",
+                             dest_mode="intermodal", min_connection_count=3,
+                             extend_earlier=True, extend_later=True)))
+    # test/routing/transfer_time_settings_test.cc
+    day_iv = [t("2019-05-01 00:00"), t("2019-05-02 00:00")]
+    tts_variants = [
+        ("default", {}, "expected_A_C_default"),
+        ("min10", dict(min_transfer_time=10), "expected_A_C_dur10"),
+        ("f1.5", dict(factor=1.5), "expected_A_C_dur3"),
+        ("f2", dict(factor=2.0), "expected_A_C_dur4"),
+        ("min10_f2", dict(min_transfer_time=10, factor=2.0), "expected_A_C_dur10"),
+        ("min3_f2", dict(min_transfer_time=3, factor=2.0), "expected_A_C_dur4"),
+        ("add2", dict(additional_time=2), "expected_A_C_dur4"),
+        ("add1_f1.5", dict(additional_time=1, factor=1.5), "expected_A_C_dur4"),
+        ("min3_add1", dict(min_transfer_time=3, additional_time=1), "expected_A_C_dur4"),
+        ("min3_add5_f2.5", dict(min_transfer_time=3, additional_time=5, factor=2.5),
+         "expected_A_C_dur10"),
+    ]
+    for d in ("fwd", "bwd"):
+        s, e = ("A", "C") if d == "fwd" else ("C", "A")
+        for vname, tts, golden in tts_variants:
+            q = dict(start=[[s, 0, 0]], dest=[[e, 0, 0]], interval=day_iv, direction=d,
+                     max_travel_time=30)
+            if vname != "default":
+                q["tts"] = dict(default=False, **tts)
+            c.append(dict(name=f"transfer_time_{vname}_{d}", timetable="gtfs_transfer_time",
+                          ref="test/routing/transfer_time_settings_test.cc",
+                          golden=golden, query=q))
+        # default max_travel_time: the direct T4 journey joins the results
+        c.append(dict(name=f"transfer_time_direct_{d}", timetable="gtfs_transfer_time",
+                      ref="test/routing/transfer_time_settings_test.cc",
+                      golden=("expected_A_C_direct", "expected_A_C_default")
+                      if d == "fwd" else ("expected_A_C_default", "expected_A_C_direct"),
+                      query=dict(start=[[s, 0, 0]], dest=[[e, 0, 0]], interval=day_iv,
+                                 direction=d)))
+    c.append(dict(name="transfer_time_max_travel_29", timetable="gtfs_transfer_time",
+                  ref="test/routing/transfer_time_settings_test.cc", golden=None,
+                  query=dict(start=[["A", 0, 0]], dest=[["C", 0, 0]], interval=day_iv,
+                             direction="fwd", max_travel_time=29,
+                             tts=dict(default=False, factor=2.0))))
+    c.append(dict(name="transfer_time_invalid_max_travel", timetable="gtfs_transfer_time",
+                  ref="test/routing/transfer_time_settings_test.cc",
+                  golden=("expected_A_C_direct", "expected_A_C_default"),
+                  query=dict(start=[["A", 0, 0]], dest=[["C", 0, 0]], interval=day_iv,
+                             direction="fwd", max_travel_time=-1440)))
+    c.append(dict(name="transfer_time_max_transfers_0", timetable="gtfs_transfer_time",
+                  ref="test/routing/transfer_time_settings_test.cc",
+                  golden="expected_A_C_direct",
+                  query=dict(start=[["A", 0, 0]], dest=[["C", 0, 0]], interval=day_iv,
+                             direction="fwd", max_transfers=0)))
+    c.append(dict(name="transfer_time_max_transfers_0_tt35", timetable="gtfs_transfer_time",
+                  ref="test/routing/transfer_time_settings_test.cc", golden=None,
+                  query=dict(start=[["A", 0, 0]], dest=[["C", 0, 0]], interval=day_iv,
+                             direction="fwd", max_transfers=0, max_travel_time=35)))
+    return c
+
+
+def main(ref_root: str):
+    out_cases = []
+    for case in cases():
+        src = open(os.path.join(ref_root, case["ref"])).read()
+        g = case["golden"]
+        if g is None:
+            expected = []
+        elif isinstance(g, tuple):
+            expected = []
+            for name in g:
+                expected += parse_journeys(raw_string(src, name))
+        else:
+            expected = parse_journeys(raw_string(src, g))
+        case = dict(case)
+        case["golden"] = list(g) if isinstance(g, tuple) else g
+        case["expected"] = expected
+        out_cases.append(case)
+    doc = {"timetables": TIMETABLES, "cases": out_cases,
+           "generated_by": "tests/golden/make_fixtures.py"}
+    with open(os.path.join(HERE, "cases.json"), "w") as f:
+        json.dump(doc, f, indent=1, sort_keys=True)
+    print(f"wrote {len(out_cases)} cases")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
