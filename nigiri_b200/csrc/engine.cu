@@ -1,0 +1,1171 @@
+// B200 RAPTOR engine: device timetable image, resident query slots, the
+// batched super-step (captured as a CUDA graph), continuous admission and
+// the C ABI of include/b2r.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "b2r.h"
+#include "engine.cuh"
+#include "errors.h"
+#include "kernels.cuh"
+#include "prep.h"
+
+namespace b2r {
+
+namespace {
+
+struct cuda_error : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+#define B2R_CUDA(call)                                                            \
+  do {                                                                            \
+    auto const e_ = (call);                                                       \
+    if (e_ != cudaSuccess) {                                                      \
+      throw ::b2r::cuda_error(std::string{#call} + ": " + cudaGetErrorString(e_));       \
+    }                                                                             \
+  } while (0)
+
+template <typename T>
+T* dmalloc(size_t n, uint64_t& total) {
+  T* p = nullptr;
+  if (n == 0) n = 1;
+  B2R_CUDA(cudaMalloc(&p, n * sizeof(T)));
+  total += n * sizeof(T);
+  return p;
+}
+
+template <typename T>
+T* dupload(T const* src, size_t n, uint64_t& total) {
+  auto* p = dmalloc<T>(n, total);
+  if (src != nullptr && n != 0) B2R_CUDA(cudaMemcpy(p, src, n * sizeof(T), cudaMemcpyHostToDevice));
+  return p;
+}
+
+int n_sms(int dev) {
+  int n = 0;
+  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+  return n > 0 ? n : 132;
+}
+
+}  // namespace
+}  // namespace b2r
+
+// ===================================================================== image
+struct b2r_timetable {
+  int device{0};
+  b2r_timetable_desc host{};  // pointers are NOT retained (sizes only)
+  b2r::dev::dtt d{};
+  std::vector<void*> allocs;
+  uint64_t bytes{0};
+  // host copies needed by the query preparation
+  std::vector<uint8_t> transfer_time;
+  std::vector<uint32_t> parent, children_index, children, fp_out_index, fp_out, fp_in_index,
+      fp_in, route_stop_index, route_stops, route_transport_from, route_transport_to,
+      route_stop_time_from, transport_traffic_days, route_traffic_days, location_routes_index,
+      location_routes, lb_fwd_index, lb_fwd, lb_bwd_index, lb_bwd, transport_route;
+  std::vector<uint8_t> location_type;
+  std::vector<uint16_t> route_stop_times;
+  std::vector<uint64_t> bitfields;
+  b2r::host_view view{};
+
+  ~b2r_timetable() {
+    for (auto* p : allocs) cudaFree(p);
+  }
+};
+
+namespace b2r {
+namespace {
+
+template <typename T>
+void host_copy(std::vector<T>& v, T const* p, size_t n) {
+  if (p == nullptr) {
+    v.clear();
+    return;
+  }
+  v.assign(p, p + n);
+}
+
+}  // namespace
+}  // namespace b2r
+
+// ==================================================================== engine
+struct b2r_engine {
+  b2r_timetable* tt{nullptr};
+  b2r_engine_config cfg{};
+  uint32_t S{0}, G{0}, max_j{0}, max_starts{0}, max_dest{0}, max_off{0};
+  uint64_t bytes_per_slot{0}, bytes{0};
+  b2r::dev::state st{};
+  cudaStream_t stream{nullptr};
+  cudaGraphExec_t graph{nullptr};
+  int sms{132};
+  std::vector<void*> allocs;
+
+  // host bookkeeping
+  std::vector<uint16_t> gen_query;  // per slot
+  std::vector<int64_t> slot_query;  // query index in the current batch, -1 free
+  struct summary_t {
+    uint8_t state, pad[3];
+    uint32_t n_journeys;
+  };
+  summary_t* d_summary{nullptr};
+  summary_t* h_summary{nullptr};  // pinned
+  // admission staging (pinned) and device mirror
+  uint8_t* h_adm{nullptr};
+  uint8_t* d_adm{nullptr};
+  size_t adm_cap{0};
+  // export staging
+  uint8_t* h_exp{nullptr};
+  uint8_t* d_exp{nullptr};
+  size_t exp_cap{0};
+  uint32_t* d_exp_list{nullptr};
+
+  b2r_batch_stats last{};
+  cudaEvent_t ev0{nullptr}, ev1{nullptr};
+
+  // results of the last batch / serving tickets
+  struct result_store {
+    std::vector<b2r_journey> journeys;
+    std::vector<b2r_leg> legs;
+    std::vector<int16_t> rt_rows;
+    b2r_result view{};
+  };
+  std::vector<result_store> results;
+
+  // serving
+  std::mutex mu;
+  std::condition_variable cv;
+  std::thread driver;
+  bool serving{false}, stop_flag{false};
+  uint64_t next_ticket{1};
+  std::deque<std::pair<uint64_t, b2r::prepped_query>> pending;
+  std::unordered_map<uint64_t, result_store> done;
+  std::string driver_error;
+
+  ~b2r_engine();
+};
+
+namespace b2r {
+namespace {
+
+struct adm_hdr {
+  uint32_t slot;
+  uint32_t n_starts, n_dest, n_off;
+  uint32_t clear_rt;
+  uint32_t lb_mode;  // 0 zeros, 1 column in payload
+  uint64_t off_slot, off_starts, off_dest, off_off, off_lb;
+};
+
+__global__ void k_admit(dev::state st, adm_hdr const* hdr, uint8_t const* payload, uint32_t n_adm,
+                        uint32_t max_starts, uint32_t max_dest, uint32_t max_off) {
+  auto const a = blockIdx.x;
+  if (a >= n_adm) return;
+  auto const h = hdr[a];
+  auto const s = h.slot;
+  auto const n_loc = st.tt.n_loc;
+  if (threadIdx.x == 0) {
+    auto sl = *reinterpret_cast<dev::slot_t const*>(payload + h.off_slot);
+    sl.gen_group = st.slots[s].gen_group;  // start-time generations persist
+    sl.starts_off = s * max_starts;
+    sl.dest_off = s * max_dest;
+    sl.soff_off = s * max_off;
+    sl.doff_off = s * max_off + sl.n_soff;
+    st.slots[s] = sl;
+  }
+  auto const* starts = reinterpret_cast<dev::start_rec const*>(payload + h.off_starts);
+  for (auto i = threadIdx.x; i < h.n_starts; i += blockDim.x) st.start_pool[s * max_starts + i] = starts[i];
+  auto const* dests = reinterpret_cast<dev::dest_rec const*>(payload + h.off_dest);
+  for (auto i = threadIdx.x; i < h.n_dest; i += blockDim.x) st.dest_pool[s * max_dest + i] = dests[i];
+  auto const* offs = reinterpret_cast<b2r_offset const*>(payload + h.off_off);
+  for (auto i = threadIdx.x; i < h.n_off; i += blockDim.x) st.off_pool[s * max_off + i] = offs[i];
+  auto const* lbc = reinterpret_cast<uint16_t const*>(payload + h.off_lb);
+  for (auto l = threadIdx.x; l < n_loc; l += blockDim.x) {
+    st.lb[static_cast<size_t>(l) * st.S + s] = h.lb_mode ? lbc[l] : uint16_t{0};
+  }
+  if (h.clear_rt) {
+    for (size_t i = threadIdx.x; i < static_cast<size_t>(dev::kK) * n_loc; i += blockDim.x) {
+      st.rt[i * st.S + s] = 0xFFFFFFFFu;
+    }
+  }
+  auto const words = (st.max_j + 31u) / 32u;
+  for (auto i = threadIdx.x; i < words; i += blockDim.x) st.blocks_used[s * words + i] = 0u;
+  __syncthreads();
+  // is-destination bits of station-to-station queries
+  auto const& sl = st.slots[s];
+  if (!sl.intermodal_dest && !sl.one_to_all) {
+    for (auto i = threadIdx.x; i < h.n_dest; i += blockDim.x) {
+      atomicOr(&st.D[dests[i].loc * st.G + (s >> 5)], 1u << (s & 31));
+    }
+  }
+}
+
+__global__ void k_retire(dev::state st, uint32_t const* slots, uint32_t n) {
+  auto const a = blockIdx.x;
+  if (a >= n) return;
+  auto const s = slots[a];
+  auto const& sl = st.slots[s];
+  if (!sl.intermodal_dest && !sl.one_to_all) {
+    for (auto i = threadIdx.x; i < sl.n_dest; i += blockDim.x) {
+      atomicAnd(&st.D[st.dest_pool[sl.dest_off + i].loc * st.G + (s >> 5)], ~(1u << (s & 31)));
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) st.slots[s].state = dev::S_IDLE;
+}
+
+__global__ void k_summary(dev::state st, b2r_engine::summary_t* out) {
+  auto const s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= st.S) return;
+  out[s].state = st.slots[s].state;
+  out[s].n_journeys = st.slots[s].n_journeys;
+}
+
+// export: per listed slot, journey headers + leg blocks (+ one-to-all rows)
+struct exp_item {
+  uint32_t slot;
+  uint32_t n_j;
+  uint32_t n_rows;  // one-to-all rows (0 otherwise)
+  uint32_t pad;
+  uint64_t off_j, off_legs, off_rows, off_slot;
+};
+
+__global__ void k_export(dev::state st, exp_item const* items, uint32_t n_items, uint8_t* out) {
+  auto const it = items[blockIdx.x];
+  if (blockIdx.x >= n_items) return;
+  auto const s = it.slot;
+  auto const& sl = st.slots[s];
+  if (threadIdx.x == 0) *reinterpret_cast<dev::slot_t*>(out + it.off_slot) = sl;
+  auto* js = reinterpret_cast<dev::journey_rec*>(out + it.off_j);
+  auto* legs = reinterpret_cast<b2r_leg*>(out + it.off_legs);
+  for (auto i = threadIdx.x; i < it.n_j; i += blockDim.x) {
+    js[i] = st.journeys[static_cast<size_t>(s) * st.max_j + i];
+  }
+  for (auto x = threadIdx.x; x < it.n_j * dev::kMaxLegs; x += blockDim.x) {
+    auto const i = x / dev::kMaxLegs, k = x % dev::kMaxLegs;
+    auto const blk = st.journeys[static_cast<size_t>(s) * st.max_j + i].block;
+    legs[x] = st.legs[(static_cast<size_t>(s) * st.max_j + blk) * dev::kMaxLegs + k];
+  }
+  if (it.n_rows != 0) {
+    auto* rows = reinterpret_cast<int16_t*>(out + it.off_rows);
+    auto const qtag = dev::tagcode(sl.gen_query);
+    auto const n = static_cast<size_t>(it.n_rows) * st.tt.n_loc;
+    for (size_t x = threadIdx.x; x < n; x += blockDim.x) {
+      auto const k = static_cast<uint32_t>(x / st.tt.n_loc), l = static_cast<uint32_t>(x % st.tt.n_loc);
+      auto const key = dev::dec(st.rt[(static_cast<size_t>(k) * st.tt.n_loc + l) * st.S + s], qtag);
+      rows[x] = static_cast<int16_t>(dev::from_key(sl.fwd != 0, key));
+    }
+  }
+}
+
+// journeys rewritten by the host between interval-extension phases
+__global__ void k_set_journeys(dev::state st, uint32_t s, dev::journey_rec const* js, uint32_t n) {
+  auto* els = st.journeys + static_cast<size_t>(s) * st.max_j;
+  auto const words = (st.max_j + 31u) / 32u;
+  if (threadIdx.x == 0) {
+    for (auto w = 0u; w != words; ++w) st.blocks_used[s * words + w] = 0u;
+    for (auto i = 0u; i != n; ++i) {
+      els[i] = js[i];
+      st.blocks_used[s * words + js[i].block / 32u] |= 1u << (js[i].block % 32u);
+    }
+    st.slots[s].n_journeys = n;
+  }
+}
+
+}  // namespace
+}  // namespace b2r
+
+b2r_engine::~b2r_engine() {
+  if (graph != nullptr) cudaGraphExecDestroy(graph);
+  if (stream != nullptr) cudaStreamDestroy(stream);
+  if (ev0 != nullptr) cudaEventDestroy(ev0);
+  if (ev1 != nullptr) cudaEventDestroy(ev1);
+  if (h_summary != nullptr) cudaFreeHost(h_summary);
+  if (h_adm != nullptr) cudaFreeHost(h_adm);
+  if (h_exp != nullptr) cudaFreeHost(h_exp);
+  for (auto* p : allocs) cudaFree(p);
+}
+
+namespace b2r {
+namespace {
+
+using dev::slot_t;
+
+// ------------------------------------------------------------- super-step
+void enqueue_superstep(b2r_engine& e, cudaStream_t s) {
+  auto const& st = e.st;
+  auto const slot_blocks = (e.S + 127) / 128;
+  auto const list_blocks = e.sms * 8;
+  dev::k_step_begin<<<list_blocks, 256, 0, s>>>(st);
+  dev::k_ctl_begin<<<slot_blocks, 128, 0, s>>>(st);
+  dev::k_sweep<<<e.sms * 16, 256, 0, s>>>(st);
+  dev::k_ctl_dest<<<slot_blocks, 128, 0, s>>>(st);
+  dev::k_mark_routes<<<list_blocks, 256, 0, s>>>(st);
+  dev::k_ctl_marked<<<slot_blocks, 128, 0, s>>>(st);
+  dev::k_route_scan<<<e.sms * 8, 256, 0, s>>>(st);
+  dev::k_clear_x<<<list_blocks, 256, 0, s>>>(st);
+  dev::k_reset_x<<<1, 32, 0, s>>>(st);
+  dev::k_transfers_pre<<<slot_blocks, 128, 0, s>>>(st);
+  dev::k_transfers<<<list_blocks, 256, 0, s>>>(st);
+  dev::k_intermodal<<<slot_blocks, 128, 0, s>>>(st);
+  dev::k_footpaths_pre<<<slot_blocks, 128, 0, s>>>(st);
+  dev::k_footpaths<<<list_blocks, 256, 0, s>>>(st);
+  dev::k_ctl_end<<<slot_blocks, 128, 0, s>>>(st);
+  dev::k_collect<<<slot_blocks, 128, 0, s>>>(st);
+  dev::k_reconstruct<<<e.sms * 2, 128, 0, s>>>(st);
+  dev::k_next<<<slot_blocks, 128, 0, s>>>(st);
+  k_summary<<<slot_blocks, 128, 0, s>>>(st, e.d_summary);
+}
+constexpr uint64_t kLaunchesPerStep = 19;
+
+// --------------------------------------------------------- admission
+size_t admission_bytes(b2r_engine const& e, prepped_query const& p) {
+  return sizeof(slot_t) + p.starts.size() * sizeof(dev::start_rec) +
+         (p.dest_dist.size() + p.dest_locs.size()) * sizeof(dev::dest_rec) +
+         (p.start_offsets.size() + p.dest_offsets.size()) * sizeof(b2r_offset) +
+         (p.lb.empty() ? 0 : e.tt->d.n_loc * sizeof(uint16_t)) + 64;
+}
+
+int check_capacity(b2r_engine const& e, prepped_query const& p) {
+  if (p.starts.size() > e.max_starts) return B2R_ERR_CAPACITY;
+  if (p.dest_dist.size() + p.dest_locs.size() > e.max_dest) return B2R_ERR_CAPACITY;
+  if (p.start_offsets.size() + p.dest_offsets.size() > e.max_off) return B2R_ERR_CAPACITY;
+  return B2R_OK;
+}
+
+slot_t make_slot(b2r_engine& e, uint32_t s, prepped_query const& p, bool& clear_rt) {
+  slot_t sl{};
+  sl.state = dev::S_START;
+  sl.fwd = p.fwd ? 1 : 0;
+  sl.one_to_all = p.one_to_all ? 1 : 0;
+  sl.end_k = p.end_k;
+  sl.intermodal_dest = p.intermodal_dest ? 1 : 0;
+  sl.ontrip = p.ontrip ? 1 : 0;
+  sl.start_mode = p.start_mode;
+  sl.dest_mode = p.dest_mode;
+  sl.base = p.base;
+  clear_rt = false;
+  if (e.gen_query[s] >= 0xFFFEu) {
+    e.gen_query[s] = 0;
+    clear_rt = true;
+  }
+  sl.gen_query = ++e.gen_query[s];
+  sl.base_days = p.base_days;
+  sl.iv_from = p.iv_from;
+  sl.iv_to = p.iv_to;
+  sl.fastest_direct = p.fastest_direct;
+  sl.max_travel_time = p.max_travel_time;
+  sl.min_connection_count = p.min_connection_count;
+  sl.extend_earlier = p.extend_earlier ? 1 : 0;
+  sl.extend_later = p.extend_later ? 1 : 0;
+  sl.need_sweep = 0;
+  sl.early_term = 0;
+  sl.tts = {p.tts.is_default, p.tts.min_transfer_time, p.tts.additional_time, p.tts.factor};
+  sl.n_starts = static_cast<uint32_t>(p.starts.size());
+  sl.n_dest = static_cast<uint32_t>(p.intermodal_dest ? p.dest_dist.size() : p.dest_locs.size());
+  sl.n_soff = static_cast<uint32_t>(p.start_offsets.size());
+  sl.n_doff = static_cast<uint32_t>(p.dest_offsets.size());
+  sl.k = 0;
+  sl.next_start = 0;
+  sl.n_journeys = 0;
+  for (auto& x : sl.tad) x = dev::kKeyInv;
+  return sl;
+}
+
+// Packs the admissions into pinned memory, copies them in one transfer and
+// distributes them with one kernel.
+void admit(b2r_engine& e, std::vector<std::pair<uint32_t, prepped_query const*>> const& adm,
+           cudaStream_t s) {
+  if (adm.empty()) return;
+  size_t need = adm.size() * sizeof(adm_hdr) + 256;
+  for (auto const& [slot, p] : adm) need += admission_bytes(e, *p) + 64;
+  if (need > e.adm_cap) {
+    B2R_CUDA(cudaStreamSynchronize(s));
+    if (e.h_adm != nullptr) cudaFreeHost(e.h_adm);
+    if (e.d_adm != nullptr) cudaFree(e.d_adm);
+    e.adm_cap = need * 2;
+    B2R_CUDA(cudaMallocHost(&e.h_adm, e.adm_cap));
+    B2R_CUDA(cudaMalloc(&e.d_adm, e.adm_cap));
+  } else {
+    B2R_CUDA(cudaStreamSynchronize(s));  // staging buffer reuse
+  }
+  auto* hdr = reinterpret_cast<adm_hdr*>(e.h_adm);
+  size_t off = (adm.size() * sizeof(adm_hdr) + 255) & ~size_t{255};
+  auto const put = [&](void const* src, size_t n) {
+    off = (off + 15) & ~size_t{15};
+    auto const at = off;
+    if (n != 0) std::memcpy(e.h_adm + off, src, n);
+    off += n;
+    return at;
+  };
+  for (auto i = 0U; i != adm.size(); ++i) {
+    auto const s_idx = adm[i].first;
+    auto const& p = *adm[i].second;
+    auto& h = hdr[i];
+    h = {};
+    h.slot = s_idx;
+    bool clear_rt = false;
+    auto const sl = make_slot(e, s_idx, p, clear_rt);
+    h.clear_rt = clear_rt ? 1 : 0;
+    h.off_slot = put(&sl, sizeof(sl));
+    std::vector<dev::start_rec> starts(p.starts.size());
+    for (auto j = 0U; j != p.starts.size(); ++j) {
+      starts[j] = {p.starts[j].time_at_start, p.starts[j].time_at_stop, p.starts[j].stop};
+    }
+    h.n_starts = static_cast<uint32_t>(starts.size());
+    h.off_starts = put(starts.data(), starts.size() * sizeof(dev::start_rec));
+    std::vector<dev::dest_rec> dests;
+    if (p.intermodal_dest) {
+      for (auto const& [l, d] : p.dest_dist) dests.push_back({l, d});
+    } else {
+      for (auto l : p.dest_locs) dests.push_back({l, 0});
+    }
+    h.n_dest = static_cast<uint32_t>(dests.size());
+    h.off_dest = put(dests.data(), dests.size() * sizeof(dev::dest_rec));
+    std::vector<b2r_offset> offs = p.start_offsets;
+    offs.insert(offs.end(), p.dest_offsets.begin(), p.dest_offsets.end());
+    h.n_off = static_cast<uint32_t>(offs.size());
+    h.off_off = put(offs.data(), offs.size() * sizeof(b2r_offset));
+    h.lb_mode = p.lb.empty() ? 0 : 1;
+    h.off_lb = put(p.lb.data(), p.lb.size() * sizeof(uint16_t));
+  }
+  B2R_CUDA(cudaMemcpyAsync(e.d_adm, e.h_adm, off, cudaMemcpyHostToDevice, s));
+  k_admit<<<static_cast<unsigned>(adm.size()), 256, 0, s>>>(
+      e.st, reinterpret_cast<adm_hdr const*>(e.d_adm), e.d_adm, static_cast<uint32_t>(adm.size()),
+      e.max_starts, e.max_dest, e.max_off);
+  B2R_CUDA(cudaGetLastError());
+}
+
+void retire(b2r_engine& e, std::vector<uint32_t> const& slots, cudaStream_t s) {
+  if (slots.empty()) return;
+  uint32_t* d = nullptr;
+  // reuse the export list buffer (sized for all slots)
+  d = e.d_exp_list;
+  B2R_CUDA(cudaMemcpyAsync(d, slots.data(), slots.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+  k_retire<<<static_cast<unsigned>(slots.size()), 128, 0, s>>>(e.st, d, static_cast<uint32_t>(slots.size()));
+  B2R_CUDA(cudaGetLastError());
+}
+
+struct exported {
+  slot_t sl;
+  std::vector<dev::journey_rec> js;
+  std::vector<b2r_leg> legs;  // n_j * kMaxLegs
+  std::vector<int16_t> rows;
+};
+
+void export_slots(b2r_engine& e, std::vector<uint32_t> const& slots,
+                  std::vector<uint32_t> const& n_js, std::vector<uint32_t> const& n_rows,
+                  std::vector<exported>& out, cudaStream_t s) {
+  out.assign(slots.size(), {});
+  if (slots.empty()) return;
+  std::vector<exp_item> items(slots.size());
+  size_t off = (slots.size() * sizeof(exp_item) + 255) & ~size_t{255};
+  for (auto i = 0U; i != slots.size(); ++i) {
+    auto& it = items[i];
+    it.slot = slots[i];
+    it.n_j = n_js[i];
+    it.n_rows = n_rows[i];
+    off = (off + 15) & ~size_t{15};
+    it.off_slot = off;
+    off += sizeof(slot_t);
+    off = (off + 15) & ~size_t{15};
+    it.off_j = off;
+    off += it.n_j * sizeof(dev::journey_rec);
+    off = (off + 15) & ~size_t{15};
+    it.off_legs = off;
+    off += static_cast<size_t>(it.n_j) * dev::kMaxLegs * sizeof(b2r_leg);
+    off = (off + 15) & ~size_t{15};
+    it.off_rows = off;
+    off += static_cast<size_t>(it.n_rows) * e.tt->d.n_loc * sizeof(int16_t);
+  }
+  if (off > e.exp_cap) {
+    B2R_CUDA(cudaStreamSynchronize(s));
+    if (e.h_exp != nullptr) cudaFreeHost(e.h_exp);
+    if (e.d_exp != nullptr) cudaFree(e.d_exp);
+    e.exp_cap = off * 2;
+    B2R_CUDA(cudaMallocHost(&e.h_exp, e.exp_cap));
+    B2R_CUDA(cudaMalloc(&e.d_exp, e.exp_cap));
+  }
+  std::memcpy(e.h_exp, items.data(), items.size() * sizeof(exp_item));
+  B2R_CUDA(cudaMemcpyAsync(e.d_exp, e.h_exp, items.size() * sizeof(exp_item), cudaMemcpyHostToDevice, s));
+  k_export<<<static_cast<unsigned>(slots.size()), 256, 0, s>>>(
+      e.st, reinterpret_cast<exp_item const*>(e.d_exp), static_cast<uint32_t>(slots.size()), e.d_exp);
+  B2R_CUDA(cudaGetLastError());
+  B2R_CUDA(cudaMemcpyAsync(e.h_exp, e.d_exp, off, cudaMemcpyDeviceToHost, s));
+  B2R_CUDA(cudaStreamSynchronize(s));
+  for (auto i = 0U; i != slots.size(); ++i) {
+    auto const& it = items[i];
+    auto& o = out[i];
+    std::memcpy(&o.sl, e.h_exp + it.off_slot, sizeof(slot_t));
+    o.js.resize(it.n_j);
+    std::memcpy(o.js.data(), e.h_exp + it.off_j, it.n_j * sizeof(dev::journey_rec));
+    o.legs.resize(static_cast<size_t>(it.n_j) * dev::kMaxLegs);
+    std::memcpy(o.legs.data(), e.h_exp + it.off_legs, o.legs.size() * sizeof(b2r_leg));
+    o.rows.resize(static_cast<size_t>(it.n_rows) * e.tt->d.n_loc);
+    std::memcpy(o.rows.data(), e.h_exp + it.off_rows, o.rows.size() * sizeof(int16_t));
+  }
+}
+
+// ----------------------------------------------------- host finalisation
+// Per query, what search::execute does between and after the Algo calls
+// (search.h:237-336): interval extension and the final filtering.
+struct query_run {
+  prepped_query p;
+  int status{B2R_OK};
+  bool finished{false};
+  bool rearm{false};
+  bool reset_arrivals{false};
+  std::vector<dev::journey_rec> keep;  // journeys kept across a re-arm
+  b2r_engine::result_store res;
+};
+
+void finish_result(b2r_engine& e, query_run& q, exported const& x) {
+  auto& p = q.p;
+  auto& res = q.res;
+  res.journeys.clear();
+  res.legs.clear();
+  res.rt_rows.clear();
+  if (p.one_to_all) {
+    res.rt_rows = x.rows;
+    res.view.n_rows = p.end_k;
+    res.view.base_day = p.base_days;
+  } else {
+    std::vector<size_t> order;
+    for (auto i = 0U; i != x.js.size(); ++i) {
+      auto const& j = x.js[i];
+      auto const tt = std::abs(j.dest_time - j.start_time);
+      if (!p.ontrip) {
+        if (!(x.sl.iv_from <= j.start_time && j.start_time < x.sl.iv_to) || tt >= p.fastest_direct ||
+            tt > p.max_travel_time) {
+          continue;
+        }
+      }
+      order.push_back(i);
+    }
+    if (!p.ontrip) {
+      std::sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+        return std::tie(x.js[a].start_time, x.js[a].transfers) <
+               std::tie(x.js[b].start_time, x.js[b].transfers);
+      });
+    }
+    for (auto i : order) {
+      auto const& j = x.js[i];
+      if (!j.reconstructed) continue;
+      b2r_journey bj{};
+      bj.start_time = j.start_time;
+      bj.dest_time = j.dest_time;
+      bj.dest = j.dest;
+      bj.transfers = j.transfers;
+      bj.error = j.error;
+      bj.n_legs = j.n_legs;
+      bj.first_leg = static_cast<uint32_t>(res.legs.size());
+      for (auto l = 0; l != j.n_legs; ++l) res.legs.push_back(x.legs[i * dev::kMaxLegs + l]);
+      res.journeys.push_back(bj);
+    }
+  }
+  res.view.status = q.status;
+  res.view.interval_from = x.sl.iv_from;
+  res.view.interval_to = x.sl.iv_to;
+  res.view.n_rounds = x.sl.n_rounds;
+  res.view.n_start_times = x.sl.n_groups_run;
+  q.finished = true;
+}
+
+// decides between finishing and another interval-extension phase
+void on_phase_done(b2r_engine& e, query_run& q, exported const& x) {
+  auto& p = q.p;
+  if (x.sl.state == dev::S_ERROR) {
+    q.status = x.sl.error != 0 ? x.sl.error : B2R_ERR_INTERNAL;
+    finish_result(e, q, x);
+    return;
+  }
+  auto const n_in = [&](int32_t f, int32_t t) {
+    uint32_t c = 0;
+    for (auto const& j : x.js) c += (!p.ontrip ? (f <= j.start_time && j.start_time < t) : true) ? 1u : 0u;
+    return c;
+  };
+  if (p.one_to_all || x.js.empty() || p.ontrip || n_in(x.sl.iv_from, x.sl.iv_to) >= p.min_connection_count) {
+    finish_result(e, q, x);
+    return;
+  }
+  auto nf = x.sl.iv_from, nt = x.sl.iv_to;
+  auto const& d = e.tt->host;
+  if (!extend_interval(p, d.date_range_from * 1440, d.date_range_to * 1440,
+                       p.min_connection_count - n_in(x.sl.iv_from, x.sl.iv_to), nf, nt)) {
+    finish_result(e, q, x);
+    return;
+  }
+  // search.h:283-316
+  std::vector<start_label> starts;
+  auto keep = x.js;
+  q.reset_arrivals = false;
+  auto const remove_outside = [&]() {
+    std::vector<dev::journey_rec> k2;
+    for (auto const& j : keep) {
+      if (x.sl.iv_from <= j.start_time && j.start_time < x.sl.iv_to) k2.push_back(j);
+    }
+    keep = std::move(k2);
+  };
+  if (nf != x.sl.iv_from) {
+    add_interval_starts(e.tt->view, p, nf, x.sl.iv_from, !p.fwd, starts);
+    if (!p.fwd) {
+      q.reset_arrivals = true;
+      remove_outside();
+    }
+  }
+  if (nt != x.sl.iv_to) {
+    add_interval_starts(e.tt->view, p, x.sl.iv_to, nt, p.fwd, starts);
+    if (p.fwd) {
+      q.reset_arrivals = true;
+      remove_outside();
+    }
+  }
+  p.starts = std::move(starts);
+  p.iv_from = nf;
+  p.iv_to = nt;
+  q.keep = std::move(keep);
+  q.rearm = true;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------- the loop
+struct batch_runner {
+  b2r_engine& e;
+  std::vector<query_run>& runs;
+  bool use_graph;
+  uint64_t launches{0}, steps{0};
+
+  void rearm(uint32_t s, query_run& q, cudaStream_t st) {
+    // new phase: upload the new starts (and journeys kept), keep the rt
+    // generation unless reset_arrivals (raptor.h:174-177)
+    auto const tad_keep = !q.reset_arrivals;
+    slot_t cur{};
+    B2R_CUDA(cudaMemcpyAsync(&cur, e.st.slots + s, sizeof(slot_t), cudaMemcpyDeviceToHost, st));
+    B2R_CUDA(cudaStreamSynchronize(st));
+    if (q.reset_arrivals) {
+      if (e.gen_query[s] >= 0xFFFEu) throw std::runtime_error("query generation exhausted");
+      cur.gen_query = ++e.gen_query[s];
+      for (auto& x : cur.tad) x = dev::kKeyInv;
+    }
+    (void)tad_keep;
+    cur.state = dev::S_START;
+    cur.iv_from = q.p.iv_from;
+    cur.iv_to = q.p.iv_to;
+    cur.need_sweep = q.reset_arrivals ? 0 : 1;
+    cur.early_term = 0;
+    cur.next_start = 0;
+    cur.n_starts = static_cast<uint32_t>(q.p.starts.size());
+    if (cur.n_starts > e.max_starts) throw std::runtime_error("start capacity exceeded");
+    std::vector<dev::start_rec> starts(q.p.starts.size());
+    for (auto j = 0U; j != starts.size(); ++j) {
+      starts[j] = {q.p.starts[j].time_at_start, q.p.starts[j].time_at_stop, q.p.starts[j].stop};
+    }
+    B2R_CUDA(cudaMemcpyAsync(e.st.start_pool + cur.starts_off, starts.data(),
+                             starts.size() * sizeof(dev::start_rec), cudaMemcpyHostToDevice, st));
+    dev::journey_rec* dj = nullptr;
+    B2R_CUDA(cudaMalloc(&dj, std::max<size_t>(1, q.keep.size()) * sizeof(dev::journey_rec)));
+    B2R_CUDA(cudaMemcpyAsync(dj, q.keep.data(), q.keep.size() * sizeof(dev::journey_rec),
+                             cudaMemcpyHostToDevice, st));
+    k_set_journeys<<<1, 32, 0, st>>>(e.st, s, dj, static_cast<uint32_t>(q.keep.size()));
+    B2R_CUDA(cudaMemcpyAsync(e.st.slots + s, &cur, sizeof(slot_t), cudaMemcpyHostToDevice, st));
+    B2R_CUDA(cudaStreamSynchronize(st));
+    cudaFree(dj);
+    q.rearm = false;
+  }
+
+  void run(uint32_t chunk) {
+    auto const S = e.S;
+    auto* st = e.stream;
+    size_t next = 0;
+    std::vector<int64_t>& slot_q = e.slot_query;
+    std::fill(slot_q.begin(), slot_q.end(), -1);
+    auto const admit_free = [&]() {
+      std::vector<std::pair<uint32_t, prepped_query const*>> adm;
+      for (uint32_t s = 0; s != S && next < runs.size(); ++s) {
+        if (slot_q[s] != -1) continue;
+        while (next < runs.size()) {
+          auto& q = runs[next];
+          if (q.p.status != B2R_OK || q.p.empty_result) {
+            q.status = q.p.status;
+            q.res.view.status = q.p.status;
+            q.res.view.interval_from = q.p.iv_from;
+            q.res.view.interval_to = q.p.iv_to;
+            q.finished = true;
+            ++next;
+            continue;
+          }
+          if (auto const c = check_capacity(e, q.p); c != B2R_OK) {
+            q.status = c;
+            q.res.view.status = c;
+            q.finished = true;
+            ++next;
+            continue;
+          }
+          break;
+        }
+        if (next >= runs.size()) break;
+        slot_q[s] = static_cast<int64_t>(next);
+        adm.emplace_back(s, &runs[next].p);
+        ++next;
+      }
+      admit(e, adm, st);
+    };
+    admit_free();
+    auto busy = [&]() {
+      for (auto x : slot_q)
+        if (x != -1) return true;
+      return false;
+    };
+    // every start-time group ends within end_k super-steps; the cap turns a
+    // logic error into a reported failure instead of an endless loop
+    uint64_t max_steps = 10000;
+    for (auto const& q : runs) max_steps += 40ull * (q.p.starts.size() + 2) * (q.p.end_k + 2);
+    while (busy()) {
+      if (steps > max_steps) throw std::runtime_error("super-step cap exceeded");
+      for (uint32_t c = 0; c != chunk; ++c) {
+        if (use_graph) {
+          B2R_CUDA(cudaGraphLaunch(e.graph, st));
+        } else {
+          enqueue_superstep(e, st);
+          B2R_CUDA(cudaGetLastError());
+        }
+        launches += kLaunchesPerStep;
+        ++steps;
+      }
+      B2R_CUDA(cudaMemcpyAsync(e.h_summary, e.d_summary, S * sizeof(b2r_engine::summary_t),
+                               cudaMemcpyDeviceToHost, st));
+      B2R_CUDA(cudaStreamSynchronize(st));
+      std::vector<uint32_t> done_slots, n_js, n_rows;
+      for (uint32_t s = 0; s != S; ++s) {
+        if (slot_q[s] == -1) continue;
+        auto const state = e.h_summary[s].state;
+        if (state == dev::S_DONE || state == dev::S_ERROR) {
+          done_slots.push_back(s);
+          n_js.push_back(e.h_summary[s].n_journeys);
+          auto const& q = runs[static_cast<size_t>(slot_q[s])];
+          n_rows.push_back(q.p.one_to_all ? q.p.end_k : 0u);
+        }
+      }
+      if (done_slots.empty()) continue;
+      std::vector<exported> ex;
+      export_slots(e, done_slots, n_js, n_rows, ex, st);
+      std::vector<uint32_t> retired;
+      for (auto i = 0U; i != done_slots.size(); ++i) {
+        auto const s = done_slots[i];
+        auto& q = runs[static_cast<size_t>(slot_q[s])];
+        on_phase_done(e, q, ex[i]);
+        if (q.rearm) {
+          rearm(s, q, st);
+        } else {
+          retired.push_back(s);
+          slot_q[s] = -1;
+        }
+      }
+      retire(e, retired, st);
+      admit_free();
+    }
+    B2R_CUDA(cudaStreamSynchronize(st));
+  }
+};
+
+void capture_graph(b2r_engine& e) {
+  cudaGraph_t g = nullptr;
+  B2R_CUDA(cudaStreamBeginCapture(e.stream, cudaStreamCaptureModeThreadLocal));
+  enqueue_superstep(e, e.stream);
+  B2R_CUDA(cudaStreamEndCapture(e.stream, &g));
+  B2R_CUDA(cudaGraphInstantiate(&e.graph, g, 0));
+  cudaGraphDestroy(g);
+}
+
+void prepare_all(b2r_engine& e, b2r_query const* qs, uint32_t n, std::vector<query_run>& runs) {
+  runs.resize(n);
+  auto const n_threads = std::max(1U, std::min<uint32_t>(
+      e.cfg.host_threads != 0 ? e.cfg.host_threads : std::max(1U, std::thread::hardware_concurrency()),
+      n));
+  std::atomic<uint32_t> next{0};
+  auto const lb_host = e.cfg.use_lower_bounds != 0;
+  auto work = [&]() {
+    for (auto i = next++; i < n; i = next++) {
+      prepare(e.tt->view, qs[i], lb_host, runs[i].p);
+      if (!lb_host && !runs[i].p.one_to_all) runs[i].p.lb.clear();
+    }
+  };
+  std::vector<std::thread> pool;
+  for (auto t = 1U; t < n_threads; ++t) pool.emplace_back(work);
+  work();
+  for (auto& t : pool) t.join();
+}
+
+void fill_out(b2r_engine& e, std::vector<query_run>& runs, b2r_result* out) {
+  e.results.resize(runs.size());
+  for (auto i = 0U; i != runs.size(); ++i) {
+    e.results[i] = std::move(runs[i].res);
+    auto& r = e.results[i];
+    r.view.n_journeys = static_cast<uint32_t>(r.journeys.size());
+    r.view.journeys = r.journeys.data();
+    r.view.legs = r.legs.data();
+    r.view.round_times = r.rt_rows.empty() ? nullptr : r.rt_rows.data();
+    out[i] = r.view;
+  }
+}
+
+}  // namespace b2r
+
+// ===================================================================== C ABI
+extern "C" {
+
+int b2r_timetable_upload(const b2r_timetable_desc* d, int device, b2r_timetable** out) {
+  B2R_API_GUARD({
+    if (d == nullptr || out == nullptr) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
+    try {
+      B2R_CUDA(cudaSetDevice(device));
+      auto t = std::make_unique<b2r_timetable>();
+      t->device = device;
+      t->host = *d;
+      auto& a = t->allocs;
+      auto& by = t->bytes;
+      auto const nl = d->n_locations, nr = d->n_routes, ntr = d->n_transports;
+      auto up = [&](auto const* p, size_t n) {
+        auto* x = b2r::dupload(p, n, by);
+        a.push_back(x);
+        return x;
+      };
+      // host copies for the query preparation
+      b2r::host_copy(t->transfer_time, d->transfer_time, nl);
+      b2r::host_copy(t->parent, d->parent, nl);
+      b2r::host_copy(t->location_type, d->location_type, nl);
+      if (d->children_index != nullptr) {
+        b2r::host_copy(t->children_index, d->children_index, nl + 1);
+        b2r::host_copy(t->children, d->children, d->children_index[nl]);
+      }
+      b2r::host_copy(t->fp_out_index, d->footpaths_out_index, nl + 1);
+      b2r::host_copy(t->fp_out, d->footpaths_out, d->footpaths_out_index[nl]);
+      b2r::host_copy(t->fp_in_index, d->footpaths_in_index, nl + 1);
+      b2r::host_copy(t->fp_in, d->footpaths_in, d->footpaths_in_index[nl]);
+      b2r::host_copy(t->route_stop_index, d->route_stop_index, nr + 1);
+      b2r::host_copy(t->route_stops, d->route_stops, d->route_stop_index[nr]);
+      b2r::host_copy(t->route_transport_from, d->route_transport_from, nr);
+      b2r::host_copy(t->route_transport_to, d->route_transport_to, nr);
+      b2r::host_copy(t->route_stop_time_from, d->route_stop_time_from, nr);
+      b2r::host_copy(t->route_stop_times, d->route_stop_times, d->n_route_stop_times);
+      b2r::host_copy(t->route_traffic_days, d->route_traffic_days, nr);
+      b2r::host_copy(t->transport_traffic_days, d->transport_traffic_days, ntr);
+      b2r::host_copy(t->transport_route, d->transport_route, ntr);
+      b2r::host_copy(t->bitfields, d->bitfields, 8ull * d->n_bitfields);
+      b2r::host_copy(t->location_routes_index, d->location_routes_index, nl + 1);
+      b2r::host_copy(t->location_routes, d->location_routes, d->location_routes_index[nl]);
+      b2r::host_copy(t->lb_fwd_index, d->lb_fwd_index, nl + 1);
+      b2r::host_copy(t->lb_fwd, d->lb_fwd, d->lb_fwd_index[nl]);
+      b2r::host_copy(t->lb_bwd_index, d->lb_bwd_index, nl + 1);
+      b2r::host_copy(t->lb_bwd, d->lb_bwd, d->lb_bwd_index[nl]);
+      auto& v = t->view.d;
+      v = *d;
+      v.transfer_time = t->transfer_time.data();
+      v.parent = t->parent.empty() ? nullptr : t->parent.data();
+      v.location_type = t->location_type.empty() ? nullptr : t->location_type.data();
+      v.children_index = t->children_index.empty() ? nullptr : t->children_index.data();
+      v.children = t->children.data();
+      v.footpaths_out_index = t->fp_out_index.data();
+      v.footpaths_out = t->fp_out.data();
+      v.footpaths_in_index = t->fp_in_index.data();
+      v.footpaths_in = t->fp_in.data();
+      v.route_stop_index = t->route_stop_index.data();
+      v.route_stops = t->route_stops.data();
+      v.route_transport_from = t->route_transport_from.data();
+      v.route_transport_to = t->route_transport_to.data();
+      v.route_stop_time_from = t->route_stop_time_from.data();
+      v.route_stop_times = t->route_stop_times.data();
+      v.route_traffic_days = t->route_traffic_days.data();
+      v.transport_traffic_days = t->transport_traffic_days.data();
+      v.transport_route = t->transport_route.data();
+      v.bitfields = t->bitfields.data();
+      v.location_routes_index = t->location_routes_index.data();
+      v.location_routes = t->location_routes.data();
+      v.lb_fwd_index = t->lb_fwd_index.data();
+      v.lb_fwd = t->lb_fwd.data();
+      v.lb_bwd_index = t->lb_bwd_index.data();
+      v.lb_bwd = t->lb_bwd.data();
+      v.importance = nullptr;
+
+      // column order check: get_earliest_transport's binary search needs
+      // every event column ordered by minutes after midnight
+      std::vector<uint8_t> sorted(nr, 1U);
+      for (auto r = 0U; r != nr; ++r) {
+        auto const n_t = d->route_transport_to[r] - d->route_transport_from[r];
+        auto const n_s = d->route_stop_index[r + 1] - d->route_stop_index[r];
+        auto const* c = d->route_stop_times + d->route_stop_time_from[r];
+        for (auto slot = 0U; n_s > 1U && slot < 2U * (n_s - 1U) && sorted[r]; ++slot) {
+          for (auto x = 1U; x < n_t; ++x) {
+            if ((c[slot * n_t + x] >> 5) < (c[slot * n_t + x - 1] >> 5)) {
+              sorted[r] = 0U;
+              break;
+            }
+          }
+        }
+      }
+
+      auto& dd = t->d;
+      dd.n_loc = nl;
+      dd.n_routes = nr;
+      dd.n_transports = ntr;
+      dd.internal_from_days = d->date_range_from - B2R_TIMETABLE_OFFSET_DAYS;
+      dd.transfer_time = up(d->transfer_time, nl);
+      dd.parent = d->parent != nullptr ? up(d->parent, nl) : nullptr;
+      dd.loc_type = d->location_type != nullptr ? up(d->location_type, nl) : nullptr;
+      if (d->children_index != nullptr) {
+        dd.children_idx = up(d->children_index, nl + 1);
+        dd.children = up(d->children, d->children_index[nl]);
+      }
+      dd.importance = d->importance != nullptr ? up(d->importance, nl) : nullptr;
+      dd.max_importance = d->max_importance;
+      dd.fp_out_idx = up(d->footpaths_out_index, nl + 1);
+      dd.fp_out = up(d->footpaths_out, d->footpaths_out_index[nl]);
+      dd.fp_in_idx = up(d->footpaths_in_index, nl + 1);
+      dd.fp_in = up(d->footpaths_in, d->footpaths_in_index[nl]);
+      dd.route_stop_idx = up(d->route_stop_index, nr + 1);
+      dd.route_stops = up(d->route_stops, d->route_stop_index[nr]);
+      dd.route_tr_from = up(d->route_transport_from, nr);
+      dd.route_tr_to = up(d->route_transport_to, nr);
+      dd.route_st_from = up(d->route_stop_time_from, nr);
+      dd.st = up(d->route_stop_times, d->n_route_stop_times);
+      dd.route_bf = up(d->route_traffic_days, nr);
+      dd.transport_bf = up(d->transport_traffic_days, ntr);
+      dd.transport_route = up(d->transport_route, ntr);
+      dd.bf = up(d->bitfields, 8ull * d->n_bitfields);
+      dd.loc_routes_idx = up(d->location_routes_index, nl + 1);
+      dd.loc_routes = up(d->location_routes, d->location_routes_index[nl]);
+      dd.route_sorted = up(sorted.data(), nr);
+      *out = t.release();
+      return B2R_OK;
+    } catch (b2r::cuda_error const& ex) {
+      return b2r::fail(B2R_ERR_CUDA, ex.what());
+    }
+  });
+}
+
+int b2r_timetable_destroy(b2r_timetable* tt) {
+  delete tt;
+  return B2R_OK;
+}
+
+uint64_t b2r_timetable_device_bytes(const b2r_timetable* tt) { return tt == nullptr ? 0 : tt->bytes; }
+
+int b2r_engine_create(b2r_timetable* tt, const b2r_engine_config* cfg_in, b2r_engine** out) {
+  B2R_API_GUARD({
+    if (tt == nullptr || out == nullptr) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
+    try {
+      B2R_CUDA(cudaSetDevice(tt->device));
+      auto e = std::make_unique<b2r_engine>();
+      b2r_engine_config cfg;
+      b2r_engine_config_init(&cfg);
+      if (cfg_in != nullptr) cfg = *cfg_in;
+      e->tt = tt;
+      e->cfg = cfg;
+      e->sms = b2r::n_sms(tt->device);
+      e->max_j = std::max(32U, std::min(4096U, (cfg.max_journeys + 31U) & ~31U));
+      e->max_starts = cfg.reserved[0] != 0 ? cfg.reserved[0] : 4096U;
+      e->max_dest = 512U;
+      e->max_off = 128U;
+      auto const nl = tt->d.n_loc;
+      e->bytes_per_slot = static_cast<uint64_t>(nl) * (b2r::dev::kK * 4 + 4 + 4 + 2) +
+                          static_cast<uint64_t>(e->max_j) *
+                              (sizeof(b2r::dev::journey_rec) + b2r::dev::kMaxLegs * sizeof(b2r_leg)) +
+                          e->max_starts * sizeof(b2r::dev::start_rec) +
+                          e->max_dest * sizeof(b2r::dev::dest_rec) + e->max_off * sizeof(b2r_offset) +
+                          b2r::dev::kMaxTimeline * sizeof(b2r::dev::tl_entry) +
+                          (static_cast<uint64_t>(nl) * 4 + tt->d.n_routes) / 8 + 256;
+      auto by_budget = cfg.hbm_budget / std::max<uint64_t>(1, e->bytes_per_slot);
+      auto slots = std::min<uint64_t>(std::max(32U, cfg.max_slots), by_budget);
+      slots &= ~uint64_t{31};
+      if (slots == 0) {
+        return b2r::fail(B2R_ERR_OUT_OF_MEMORY, "HBM budget too small for one slot group");
+      }
+      e->S = static_cast<uint32_t>(slots);
+      e->G = e->S / 32;
+      auto& st = e->st;
+      st.tt = tt->d;
+      st.S = e->S;
+      st.G = e->G;
+      st.max_j = e->max_j;
+      auto& by = e->bytes;
+      auto al = [&](auto*& p, size_t n) {
+        using T = std::remove_reference_t<decltype(*p)>;
+        p = b2r::dmalloc<std::remove_const_t<T>>(n, by);
+        e->allocs.push_back(const_cast<void*>(static_cast<void const*>(p)));
+      };
+      auto const S = static_cast<size_t>(e->S), G = static_cast<size_t>(e->G);
+      al(st.slots, S);
+      al(st.lanes, S);
+      al(st.rt, static_cast<size_t>(b2r::dev::kK) * nl * S);
+      al(st.best, static_cast<size_t>(nl) * S);
+      al(st.tmp, static_cast<size_t>(nl) * S);
+      al(st.lb, static_cast<size_t>(nl) * S);
+      al(st.X, static_cast<size_t>(nl) * G);
+      al(st.Y, static_cast<size_t>(nl) * G);
+      al(st.R, static_cast<size_t>(tt->d.n_routes) * G);
+      al(st.D, static_cast<size_t>(nl) * G);
+      al(st.xlist, static_cast<size_t>(nl) * G);
+      al(st.ylist, static_cast<size_t>(nl) * G);
+      al(st.rlist, static_cast<size_t>(tt->d.n_routes) * G);
+      al(st.counters, 16);
+      al(st.run_mask, G);
+      al(st.sweep_mask, G);
+      al(st.any_mask, G);
+      al(st.start_pool, S * e->max_starts);
+      al(st.dest_pool, S * e->max_dest);
+      al(st.off_pool, S * e->max_off);
+      al(st.journeys, S * e->max_j);
+      al(st.legs, S * e->max_j * b2r::dev::kMaxLegs);
+      al(st.blocks_used, S * ((e->max_j + 31) / 32));
+      al(st.recon_list, S * e->max_j);
+      al(st.timeline, S * b2r::dev::kMaxTimeline);
+      al(st.timeline_n, S);
+      al(st.tad_phase, S);
+      al(st.status_word, 4);
+      al(e->d_summary, S);
+      al(e->d_exp_list, S);
+      B2R_CUDA(cudaMemset(st.slots, 0, S * sizeof(b2r::dev::slot_t)));
+      B2R_CUDA(cudaMemset(st.rt, 0xFF, static_cast<size_t>(b2r::dev::kK) * nl * S * 4));
+      B2R_CUDA(cudaMemset(st.best, 0xFF, static_cast<size_t>(nl) * S * 4));
+      B2R_CUDA(cudaMemset(st.tmp, 0xFF, static_cast<size_t>(nl) * S * 4));
+      B2R_CUDA(cudaMemset(st.X, 0, static_cast<size_t>(nl) * G * 4));
+      B2R_CUDA(cudaMemset(st.Y, 0, static_cast<size_t>(nl) * G * 4));
+      B2R_CUDA(cudaMemset(st.R, 0, static_cast<size_t>(tt->d.n_routes) * G * 4));
+      B2R_CUDA(cudaMemset(st.D, 0, static_cast<size_t>(nl) * G * 4));
+      B2R_CUDA(cudaMemset(st.counters, 0, 16 * 4));
+      e->gen_query.assign(S, 0);
+      e->slot_query.assign(S, -1);
+      B2R_CUDA(cudaMallocHost(&e->h_summary, S * sizeof(b2r_engine::summary_t)));
+      B2R_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+      B2R_CUDA(cudaEventCreate(&e->ev0));
+      B2R_CUDA(cudaEventCreate(&e->ev1));
+      if (cfg.use_graphs) b2r::capture_graph(*e);
+      B2R_CUDA(cudaDeviceSynchronize());
+      *out = e.release();
+      return B2R_OK;
+    } catch (b2r::cuda_error const& ex) {
+      return b2r::fail(B2R_ERR_CUDA, ex.what());
+    }
+  });
+}
+
+int b2r_engine_destroy(b2r_engine* e) {
+  if (e != nullptr && e->serving) b2r_serve_stop(e);
+  delete e;
+  return B2R_OK;
+}
+
+uint64_t b2r_engine_bytes_per_slot(const b2r_engine* e) { return e == nullptr ? 0 : e->bytes_per_slot; }
+uint32_t b2r_engine_slots(const b2r_engine* e) { return e == nullptr ? 0 : e->S; }
+
+int b2r_search_batch(b2r_engine* e, const b2r_query* qs, uint32_t n, b2r_result* out) {
+  B2R_API_GUARD({
+    if (e == nullptr || (n != 0 && (qs == nullptr || out == nullptr))) {
+      return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
+    }
+    if (e->serving) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "engine is serving");
+    try {
+      B2R_CUDA(cudaSetDevice(e->tt->device));
+      std::vector<b2r::query_run> runs;
+      auto const t0 = std::chrono::steady_clock::now();
+      b2r::prepare_all(*e, qs, n, runs);
+      auto const t1 = std::chrono::steady_clock::now();
+      b2r::batch_runner br{*e, runs, e->cfg.use_graphs != 0 && e->graph != nullptr};
+      B2R_CUDA(cudaEventRecord(e->ev0, e->stream));
+      br.run(e->cfg.reserved[1] != 0 ? e->cfg.reserved[1] : 4U);
+      B2R_CUDA(cudaEventRecord(e->ev1, e->stream));
+      B2R_CUDA(cudaEventSynchronize(e->ev1));
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e->ev0, e->ev1);
+      e->last = {};
+      e->last.device_ms = ms;
+      e->last.host_prep_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+      e->last.kernel_launches = br.launches;
+      e->last.super_steps = br.steps;
+      uint32_t err = 0;
+      B2R_CUDA(cudaMemcpy(&err, e->st.counters + b2r::dev::C_ERR, 4, cudaMemcpyDeviceToHost));
+      if (err != 0) {
+        B2R_CUDA(cudaMemset(e->st.counters + b2r::dev::C_ERR, 0, 4));
+        for (auto& r : runs) {
+          r.status = B2R_ERR_DEVICE_STATUS;
+          r.res.view.status = B2R_ERR_DEVICE_STATUS;
+        }
+      }
+      b2r::fill_out(*e, runs, out);
+      return err != 0 ? b2r::fail(B2R_ERR_DEVICE_STATUS, "device status word set") : B2R_OK;
+    } catch (b2r::cuda_error const& ex) {
+      return b2r::fail(B2R_ERR_CUDA, ex.what());
+    }
+  });
+}
+
+int b2r_search_plain(b2r_engine* e, const b2r_query* q, b2r_result* out) {
+  B2R_API_GUARD({
+    if (e == nullptr || q == nullptr || out == nullptr) {
+      return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
+    }
+    try {
+      B2R_CUDA(cudaSetDevice(e->tt->device));
+      std::vector<b2r::query_run> runs;
+      b2r::prepare_all(*e, q, 1, runs);
+      b2r::batch_runner br{*e, runs, false};
+      br.run(1);
+      e->last = {};
+      e->last.kernel_launches = br.launches;
+      e->last.super_steps = br.steps;
+      b2r::fill_out(*e, runs, out);
+      return B2R_OK;
+    } catch (b2r::cuda_error const& ex) {
+      return b2r::fail(B2R_ERR_CUDA, ex.what());
+    }
+  });
+}
+
+int b2r_last_batch_stats(const b2r_engine* e, b2r_batch_stats* s) {
+  if (e == nullptr || s == nullptr) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
+  *s = e->last;
+  return B2R_OK;
+}
+
+// ------------------------------------------------------------------ serving
+int b2r_serve_start(b2r_engine* e) {
+  if (e == nullptr) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
+  return b2r::fail(B2R_ERR_UNSUPPORTED, "serving loop not built yet");
+}
+int b2r_serve_stop(b2r_engine* e) {
+  if (e == nullptr) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
+  return B2R_OK;
+}
+int b2r_submit(b2r_engine* e, const b2r_query* q, uint64_t* ticket) {
+  (void)q;
+  (void)ticket;
+  if (e == nullptr) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
+  return b2r::fail(B2R_ERR_UNSUPPORTED, "serving loop not built yet");
+}
+int b2r_poll(b2r_engine* e, uint64_t ticket, b2r_result* out) {
+  (void)ticket;
+  (void)out;
+  if (e == nullptr) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
+  return b2r::fail(B2R_ERR_UNSUPPORTED, "serving loop not built yet");
+}
+int b2r_wait(b2r_engine* e, uint64_t ticket, b2r_result* out) { return b2r_poll(e, ticket, out); }
+int b2r_release(b2r_engine* e, uint64_t ticket) {
+  (void)ticket;
+  if (e == nullptr) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
+  return B2R_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,232 @@
+// Device-side data layout and helpers of the B200 RAPTOR engine.
+//
+// Round state is slot-minor: arrays are [round][location][slot] (and
+// [location][slot] for best / tmp / lower bounds), so the 32 lanes of a warp
+// working on one route for 32 resident queries read 32 consecutive words.
+// Labels are 32-bit words  (tag:16 | key:16):
+//   key  = direction-normalised time: t (forward) or ~t (backward), so that
+//          "better" is always "smaller" and atomicMin serves both directions;
+//          stored biased (key ^ 0x8000) to compare as unsigned.
+//   tag  = 0xFFFF - generation.  round_times use the query generation of the
+//          slot, best / tmp the start-time generation, so resetting a slot's
+//          labels (raptor::reset_arrivals / next_start_time, raptor.h:174-188)
+//          is a counter increment instead of a sweep.  A word whose tag is not
+//          the current one reads as invalid (kInvalidDelta).
+#pragma once
+
+#include <cstdint>
+
+#include "b2r.h"
+
+namespace b2r::dev {
+
+constexpr int kK = B2R_K;
+constexpr int kKeyInv = 32767;
+constexpr uint32_t kFull = 0xFFFFFFFFu;
+constexpr int kMaxLegs = 40;
+constexpr int kMaxTimeline = 128;
+
+// slot states
+enum : uint8_t {
+  S_IDLE = 0,
+  S_START = 1,     // admitted, first start-time group not yet seeded
+  S_RUN = 2,       // running rounds
+  S_COLLECT = 3,   // rounds of the current group finished
+  S_DONE = 4,      // phase finished, host reads results
+  S_ERROR = 5
+};
+
+// ------------------------------------------------------- timetable image
+struct dtt {
+  uint32_t n_loc, n_routes, n_transports, n_groups_unused;
+  int32_t internal_from_days;
+  uint8_t const* transfer_time;
+  uint32_t const* parent;
+  uint8_t const* loc_type;
+  uint32_t const* children_idx;
+  uint32_t const* children;
+  uint32_t const* importance;
+  uint32_t max_importance;
+  uint32_t const* fp_out_idx;
+  uint32_t const* fp_out;
+  uint32_t const* fp_in_idx;
+  uint32_t const* fp_in;
+  uint32_t const* route_stop_idx;
+  uint32_t const* route_stops;
+  uint32_t const* route_tr_from;
+  uint32_t const* route_tr_to;
+  uint32_t const* route_st_from;
+  uint16_t const* st;  // route_stop_times (packed delta)
+  uint32_t const* route_bf;
+  uint32_t const* transport_bf;
+  uint32_t const* transport_route;
+  uint64_t const* bf;
+  uint32_t const* loc_routes_idx;
+  uint32_t const* loc_routes;
+  uint8_t const* route_sorted;  // 1: every event column is ordered by mam
+};
+
+// --------------------------------------------------------- per-slot data
+struct tts_t {
+  uint8_t is_default;
+  int16_t min_transfer_time;
+  int16_t additional_time;
+  float factor;
+};
+
+struct journey_rec {  // routing::journey header
+  int32_t start_time;
+  int32_t dest_time;
+  uint32_t dest;
+  uint8_t transfers;
+  uint8_t error;
+  uint8_t reconstructed;
+  uint8_t pad;
+  uint16_t n_legs;
+  uint16_t block;  // leg block of this journey
+};
+
+struct slot_t {
+  // set at admission
+  uint8_t state;
+  uint8_t fwd;
+  uint8_t one_to_all;
+  uint8_t end_k;
+  uint8_t intermodal_dest;
+  uint8_t ontrip;
+  uint8_t start_mode;
+  uint8_t dest_mode;
+  uint16_t base;  // day index of the base day
+  uint16_t gen_query;
+  int32_t base_days;
+  int32_t iv_from, iv_to;
+  int16_t fastest_direct;
+  int16_t max_travel_time;
+  uint32_t min_connection_count;
+  uint8_t extend_earlier, extend_later, need_sweep, early_term;
+  tts_t tts;
+  uint32_t starts_off, n_starts;  // start pool
+  uint32_t dest_off, n_dest;      // dest pool (loc, dist)
+  uint32_t soff_off, n_soff;      // start offsets (for reconstruction)
+  uint32_t doff_off, n_doff;      // destination offsets
+  // dynamic
+  uint8_t k;
+  uint8_t pad0;
+  uint16_t gen_group;
+  uint32_t next_start;   // index of the next start label (group cursor)
+  int32_t cur_start_time;
+  uint32_t n_journeys;
+  int32_t error;
+  int16_t tad[kK];  // time_at_dest_ keys
+  uint64_t n_rounds, n_groups_run;
+};
+
+// compact per-super-step view of a slot read by every lane
+struct lane_t {
+  int16_t tad_k;
+  uint16_t gtag;
+  uint16_t qtag;
+  uint16_t base;
+  uint8_t fwd;
+  uint8_t k;
+  uint8_t run;
+  uint8_t mode;  // bit0 intermodal dest, bit1 has dests, bit2 tts default
+};
+
+struct start_rec {
+  int32_t time_at_start;
+  int32_t time_at_stop;
+  uint32_t stop;
+};
+
+struct dest_rec {
+  uint32_t loc;
+  uint32_t dist;  // intermodal egress minutes
+};
+
+struct tl_entry {  // time_at_dest timeline of one phase
+  uint32_t pos_hi, pos_lo;
+  int32_t tad;
+};
+
+// engine state: every device array in one POD passed by value
+struct state {
+  dtt tt;
+  uint32_t S;        // slots (multiple of 32)
+  uint32_t G;        // slot groups of 32
+  uint32_t max_j;    // journeys per slot
+  slot_t* slots;
+  lane_t* lanes;
+  uint32_t* rt;     // [K][n_loc][S]
+  uint32_t* best;   // [n_loc][S]
+  uint32_t* tmp;    // [n_loc][S]
+  uint16_t* lb;     // [n_loc][S]
+  uint32_t* X;      // station marks  [n_loc][G]
+  uint32_t* Y;      // route-reached marks [n_loc][G]
+  uint32_t* R;      // route marks [n_routes][G]
+  uint32_t* D;      // is-destination bits [n_loc][G]
+  uint32_t* xlist;  // frontier lists of (loc * G + g)
+  uint32_t* ylist;
+  uint32_t* rlist;
+  uint32_t* counters;  // [0] xlist, [1] ylist, [2] rlist, [3] recon count, [4] x2 ...
+  uint32_t* run_mask;  // [G]
+  uint32_t* sweep_mask;  // [G]
+  uint32_t* any_mask;  // [G]
+  start_rec* start_pool;
+  dest_rec* dest_pool;
+  b2r_offset* off_pool;
+  journey_rec* journeys;  // [S][max_j]
+  b2r_leg* legs;          // [S][max_j][kMaxLegs]
+  uint32_t* blocks_used;  // [S][max_j / 32]
+  uint32_t* recon_list;   // (slot << 16 | journey index)
+  tl_entry* timeline;     // [S][kMaxTimeline]
+  uint32_t* timeline_n;   // [S]
+  int16_t* tad_phase;     // [S] tad[k] at the start of the phase
+  uint32_t* status_word;  // [0] device error flags
+};
+
+// ------------------------------------------------------------- helpers
+__device__ __forceinline__ uint16_t tagcode(uint16_t gen) { return static_cast<uint16_t>(0xFFFFu - gen); }
+
+__device__ __forceinline__ uint32_t enc(uint16_t tag, int key) {
+  return (static_cast<uint32_t>(tag) << 16) |
+         (static_cast<uint32_t>(static_cast<uint16_t>(static_cast<int16_t>(key))) ^ 0x8000u);
+}
+
+__device__ __forceinline__ int dec(uint32_t w, uint16_t tag) {
+  return (w >> 16) == tag ? static_cast<int>(static_cast<int16_t>((w & 0xFFFFu) ^ 0x8000u))
+                          : kKeyInv;
+}
+
+__device__ __forceinline__ int clamp16(int v) { return v < -32768 ? -32768 : (v > 32767 ? 32767 : v); }
+
+// delta_t <-> key
+__device__ __forceinline__ int to_key(bool fwd, int t) { return fwd ? t : ~t; }
+__device__ __forceinline__ int from_key(bool fwd, int k) { return fwd ? k : ~k; }
+
+// clamp(t + dir(x)) in key space == clamp(key + x) (both directions)
+__device__ __forceinline__ int key_add(int key, int x) { return clamp16(key + x); }
+
+__device__ __forceinline__ bool bf_test(dtt const& T, uint32_t bf, uint32_t i) {
+  return i < B2R_MAX_DAYS && ((T.bf[8ull * bf + (i >> 6)] >> (i & 63u)) & 1ull);
+}
+
+__device__ __forceinline__ int delta_count(uint16_t d) {  // delta::count()
+  return static_cast<int16_t>(static_cast<uint32_t>(d & 0x1Fu) * 1440u + (d >> 5));
+}
+
+// adjusted_transfer_time<T> for an int duration (float product truncated)
+template <typename T>
+__device__ __forceinline__ T adjusted(tts_t const& s, T d) {
+  if (s.is_default) return d;
+  auto const prod = static_cast<T>(__float2int_rz(__fmul_rn(static_cast<float>(d), s.factor)));
+  auto const mn = static_cast<T>(s.min_transfer_time);
+  return static_cast<T>(static_cast<T>(s.additional_time) + (prod > mn ? prod : mn));
+}
+
+// to_delta(day, mam) of raptor.h:1467-1469, as a key
+__device__ __forceinline__ int to_delta_key(bool fwd, uint16_t day, uint16_t base, int mam) {
+  return to_key(fwd, clamp16((static_cast<int>(day) - static_cast<int>(base)) * 1440 + mam));
+}
+
+}  // namespace b2r::dev

@@ -19,9 +19,9 @@ inline int fail(int status, std::string msg) {
 
 // No exception may cross the C ABI: every entry point body runs inside this
 // guard and maps exceptions onto status codes.
-#define B2R_API_GUARD(body)                                              \
+#define B2R_API_GUARD(...)                                              \
   try {                                                                  \
-    body                                                                 \
+    __VA_ARGS__                                                          \
   } catch (std::bad_alloc const&) {                                      \
     return b2r::fail(B2R_ERR_OUT_OF_MEMORY, "host allocation failed");   \
   } catch (std::exception const& e) {                                    \

@@ -1,0 +1,755 @@
+// Per-round kernels of the batched RAPTOR super-step.  One super-step runs
+// one RAPTOR round (raptor::execute's loop body, raptor.h:218-387) for every
+// resident query whose current start-time group is still running, then
+// collects, reconstructs and seeds the next start-time group of queries
+// whose rounds ended (search.h:436-475).
+#pragma once
+
+#include "engine.cuh"
+#include "reconstruct.cuh"
+
+namespace b2r::dev {
+
+enum : uint32_t { C_X = 0, C_Y = 1, C_R = 2, C_RECON = 3, C_ERR = 4 };
+
+__device__ __forceinline__ size_t li(state const& st, uint32_t l, uint32_t s) {
+  return static_cast<size_t>(l) * st.S + s;
+}
+__device__ __forceinline__ size_t rti(state const& st, uint32_t k, uint32_t l, uint32_t s) {
+  return (static_cast<size_t>(k) * st.tt.n_loc + l) * st.S + s;
+}
+
+__device__ __forceinline__ void mark(state const& st, uint32_t* M, uint32_t* list, uint32_t counter,
+                                     uint32_t e, uint32_t bits) {
+  auto const old = atomicOr(&M[e], bits);
+  if (old == 0u) list[atomicAdd(&st.counters[counter], 1u)] = e;
+}
+
+// warp-aggregated mark: lanes with `want` OR their bit into M[e(lane)];
+// lanes sharing the same word combine into one atomic.
+__device__ __forceinline__ void mark_warp(state const& st, uint32_t* M, uint32_t* list,
+                                          uint32_t counter, bool want, uint32_t e, uint32_t lane) {
+  auto const key = want ? e : 0xFFFFFFFFu;
+  auto const peers = __match_any_sync(kFull, key);
+  if (want && lane == static_cast<uint32_t>(__ffs(peers) - 1)) mark(st, M, list, counter, e, peers);
+}
+
+__device__ __forceinline__ void update_tad(slot_t& sl, uint32_t k, int key) {  // raptor.h:1479-1486
+  if (sl.one_to_all) return;
+  for (auto i = k; i < kK; ++i) {
+    if (key < sl.tad[i]) sl.tad[i] = static_cast<int16_t>(key);
+  }
+}
+
+// get_earliest_transport, raptor.h:1351-1442.  Event columns are ordered by
+// minutes after midnight (loader/get_index.h), so the reference's
+// linear_lb is a lower bound found by binary search; the scan that follows
+// visits events in the reference's order with the same prune / skip / day
+// rules.  Routes flagged unsorted use the reference's linear seek.
+__device__ bool et_search(dtt const& T, bool fwd, uint32_t r, uint32_t si, uint16_t day_at_stop,
+                          int mam, int lbv, int tad_k, uint16_t base, uint32_t& out_off,
+                          uint16_t& out_day) {
+  auto const t0 = T.route_tr_from[r];
+  auto const n = T.route_tr_to[r] - t0;
+  auto const* col = T.st + T.route_st_from[r] + n * (si * 2u - (fwd ? 0u : 1u));
+  auto const sorted = T.route_sorted[r] != 0;
+  auto const rbf = T.route_bf[r];
+  for (auto i = 0u; i != 6u; ++i) {
+    auto const day = static_cast<uint16_t>(fwd ? day_at_stop + i : day_at_stop - i);
+    if (!bf_test(T, rbf, day)) continue;
+    uint32_t j = 0;
+    if (i == 0u) {
+      if (sorted) {
+        uint32_t lo = 0, hi = n;
+        if (fwd) {  // first index with mam >= m
+          while (lo < hi) {
+            auto const mid = (lo + hi) >> 1;
+            if (static_cast<int>(col[mid] >> 5) < mam) lo = mid + 1;
+            else hi = mid;
+          }
+          j = lo;
+        } else {  // first (from the end) with mam <= m: n - upper_bound(m)
+          while (lo < hi) {
+            auto const mid = (lo + hi) >> 1;
+            if (static_cast<int>(col[mid] >> 5) <= mam) lo = mid + 1;
+            else hi = mid;
+          }
+          j = n - lo;
+        }
+      } else {
+        for (j = 0; j < n; ++j) {
+          auto const em = static_cast<int>(col[fwd ? j : n - 1 - j] >> 5);
+          if (!(fwd ? em < mam : em > mam)) break;
+        }
+      }
+    }
+    for (; j < n; ++j) {
+      auto const idx = fwd ? j : n - 1u - j;
+      auto const e = col[idx];
+      auto const em = static_cast<int>(e >> 5);
+      if (to_delta_key(fwd, day, base, em) + lbv > tad_k) return false;
+      if (i == 0u && !(fwd ? mam <= em : mam >= em)) continue;
+      auto const sday = static_cast<uint16_t>(static_cast<int>(day) - static_cast<int>(e & 31u));
+      if (!bf_test(T, T.transport_bf[t0 + idx], sday)) continue;
+      out_off = idx;
+      out_day = sday;
+      return true;
+    }
+  }
+  return false;
+}
+
+// ----------------------------------------------------------- control
+__global__ void k_step_begin(state st) {
+  auto const tid = blockIdx.x * blockDim.x + threadIdx.x;
+  auto const ny = st.counters[C_Y];
+  for (auto i = tid; i < ny; i += gridDim.x * blockDim.x) st.Y[st.ylist[i]] = 0u;
+  if (tid < st.G) {
+    st.run_mask[tid] = 0u;
+    st.sweep_mask[tid] = 0u;
+    st.any_mask[tid] = 0u;
+  }
+}
+
+__global__ void k_ctl_begin(state st) {
+  auto const s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s == 0) {
+    st.counters[C_Y] = 0u;
+    st.counters[C_R] = 0u;
+    st.counters[C_RECON] = 0u;
+  }
+  if (s >= st.S) return;
+  auto& sl = st.slots[s];
+  lane_t ln{};
+  if (sl.state == S_RUN) {
+    ln.run = 1;
+    ln.fwd = sl.fwd;
+    ln.k = sl.k;
+    ln.base = sl.base;
+    ln.gtag = tagcode(sl.gen_group);
+    ln.qtag = tagcode(sl.gen_query);
+    ln.mode = (sl.intermodal_dest ? 1u : 0u) |
+              ((!sl.intermodal_dest && !sl.one_to_all && sl.n_dest != 0) ? 2u : 0u) |
+              (sl.tts.is_default ? 4u : 0u);
+    ln.tad_k = sl.tad[sl.k];
+    atomicOr(&st.run_mask[s >> 5], 1u << (s & 31));
+    if (sl.need_sweep) atomicOr(&st.sweep_mask[s >> 5], 1u << (s & 31));
+    ++sl.n_rounds;
+  }
+  st.lanes[s] = ln;
+}
+
+// best <- min(best, round_times[k]) over all locations (raptor.h:219-223)
+__global__ void k_sweep(state st) {
+  auto const n = static_cast<size_t>(st.tt.n_loc) * st.S;
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    auto const s = static_cast<uint32_t>(i % st.S);
+    if (!((st.sweep_mask[s >> 5] >> (s & 31)) & 1u)) continue;
+    auto const l = static_cast<uint32_t>(i / st.S);
+    auto const ln = st.lanes[s];
+    auto const r = dec(st.rt[rti(st, ln.k, l, s)], ln.qtag);
+    if (r == kKeyInv) continue;
+    auto const b = dec(st.best[i], ln.gtag);
+    if (r < b) st.best[i] = enc(ln.gtag, r);
+  }
+}
+
+// destination times into time_at_dest (raptor.h:224-226)
+__global__ void k_ctl_dest(state st) {
+  auto const s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= st.S) return;
+  auto& sl = st.slots[s];
+  if (sl.state != S_RUN || sl.one_to_all) return;
+  auto const gtag = tagcode(sl.gen_group);
+  if (sl.intermodal_dest) {
+    update_tad(sl, sl.k, dec(st.best[li(st, B2R_SPECIAL_END, s)], gtag));
+  } else {
+    for (auto i = 0u; i != sl.n_dest; ++i) {
+      update_tad(sl, sl.k, dec(st.best[li(st, st.dest_pool[sl.dest_off + i].loc, s)], gtag));
+    }
+  }
+  st.lanes[s].tad_k = sl.tad[sl.k];
+}
+
+// station marks -> route marks (raptor.h:228-241)
+__global__ void k_mark_routes(state st) {
+  auto const nx = st.counters[C_X];
+  for (auto i = blockIdx.x * blockDim.x + threadIdx.x; i < nx; i += gridDim.x * blockDim.x) {
+    auto const e = st.xlist[i];
+    auto const g = e % st.G, l = e / st.G;
+    auto const w = st.X[e] & st.run_mask[g];
+    if (w == 0u) continue;
+    auto const rb = st.tt.loc_routes_idx[l], re = st.tt.loc_routes_idx[l + 1];
+    if (rb == re) continue;
+    atomicOr(&st.any_mask[g], w);
+    for (auto ri = rb; ri != re; ++ri) {
+      mark(st, st.R, st.rlist, C_R, st.tt.loc_routes[ri] * st.G + g, w);
+    }
+  }
+}
+
+__global__ void k_ctl_marked(state st) {
+  auto const s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= st.S) return;
+  auto& sl = st.slots[s];
+  if (sl.state != S_RUN) return;
+  if (!((st.any_mask[s >> 5] >> (s & 31)) & 1u)) {  // raptor.h:243-246
+    sl.state = S_COLLECT;
+    st.lanes[s].run = 0;
+  }
+}
+
+// ------------------------------------------------------------ route scan
+// update_route, raptor.h:1177-1349 (no vias, no section filters): one warp
+// per (route, group of 32 queries); each lane walks the stop sequence of
+// its query in search direction carrying its current trip.
+__global__ void __launch_bounds__(256) k_route_scan(state st) {
+  auto const lane = threadIdx.x & 31u;
+  auto const warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  auto const n_warps = (gridDim.x * blockDim.x) >> 5;
+  auto const nr = st.counters[C_R];
+  auto const& T = st.tt;
+  for (auto w = warp; w < nr; w += n_warps) {
+    auto const e = st.rlist[w];
+    auto const g = e % st.G, r = e / st.G;
+    auto const mask = st.R[e];
+    __syncwarp();
+    if (lane == 0) st.R[e] = 0u;
+    auto const s = g * 32u + lane;
+    auto const ln = st.lanes[s];
+    auto active = ((mask >> lane) & 1u) != 0u && ln.run;
+    auto const fwd = ln.fwd != 0;
+    auto const k = static_cast<uint32_t>(ln.k);
+    auto const sb = T.route_stop_idx[r];
+    auto const n = T.route_stop_idx[r + 1] - sb;
+    auto const t0 = T.route_tr_from[r];
+    auto const n_t = T.route_tr_to[r] - t0;
+    auto const* colbase = T.st + T.route_st_from[r];
+    bool et_valid = false;
+    uint32_t et_off = 0;
+    uint16_t et_day = 0;
+    for (auto i = 0u; i != n; ++i) {
+      auto const si = fwd ? i : n - 1u - i;
+      auto const stp = T.route_stops[sb + si];
+      auto const l = B2R_STOP_LOC(stp);
+      auto const can_finish = fwd ? B2R_STOP_OUT(stp) : B2R_STOP_IN(stp);
+      auto const can_start = fwd ? B2R_STOP_IN(stp) : B2R_STOP_OUT(stp);
+      bool reached = false;
+      bool arrival_ran = false;
+      if (active && et_valid && can_finish) {
+        arrival_ran = true;
+        auto const ev = colbase[n_t * (si * 2u - (fwd ? 1u : 0u)) + et_off];
+        auto const by = to_delta_key(fwd, et_day, ln.base, delta_count(ev));
+        auto const lbv = st.lb[li(st, l, s)];
+        if (by <= ln.tad_k && lbv != 0xFFFFu && by + static_cast<int>(lbv) <= ln.tad_k) {
+          auto const word = enc(ln.gtag, by);
+          auto* tp = &st.tmp[li(st, l, s)];
+          if (word < *tp) atomicMin(tp, word);
+          reached = true;
+        }
+      }
+      mark_warp(st, st.Y, st.ylist, C_Y, reached, l * st.G + g, lane);
+
+      auto const is_last = i + 1u == n;
+      if (active && !is_last && can_start && ((st.X[l * st.G + g] >> lane) & 1u)) {
+        auto const lbv = st.lb[li(st, l, s)];
+        if (lbv == 0xFFFFu) {
+          active = false;  // raptor.h:1309-1311
+        } else {
+          auto const board_col = n_t * (si * 2u - (fwd ? 0u : 1u));
+          auto const et_time =
+              et_valid ? to_delta_key(fwd, et_day, ln.base, delta_count(colbase[board_col + et_off]))
+                       : kKeyInv;
+          auto const prt = dec(st.rt[rti(st, k - 1u, l, s)], ln.qtag);
+          if (prt != kKeyInv && prt <= et_time) {
+            auto const t_prt = from_key(fwd, prt);
+            auto const minutes = static_cast<int>(ln.base) * 1440 + t_prt;
+            auto const day = static_cast<uint16_t>(minutes / 1440);
+            auto const mam = minutes % 1440;
+            uint32_t nt = 0;
+            uint16_t nd = 0;
+            auto const found = et_search(T, fwd, r, si, day, mam, static_cast<int>(lbv), ln.tad_k,
+                                         ln.base, nt, nd);
+            if (found) {
+              // current_best (raptor.h:1328-1329) is valid whenever the arrival
+              // part ran or the station carries a label of this start time
+              auto const cb_valid = arrival_ran || dec(st.best[li(st, l, s)], ln.gtag) != kKeyInv ||
+                                    dec(st.tmp[li(st, l, s)], ln.gtag) != kKeyInv;
+              auto const nt_time =
+                  to_delta_key(fwd, nd, ln.base, delta_count(colbase[board_col + nt]));
+              if (!cb_valid || nt_time <= et_time) {
+                et_valid = true;
+                et_off = nt;
+                et_day = nd;
+              }
+            }
+          }
+        }
+      }
+    }
+  }
+}
+
+__global__ void k_clear_x(state st) {
+  auto const tid = blockIdx.x * blockDim.x + threadIdx.x;
+  auto const nx = st.counters[C_X];
+  for (auto i = tid; i < nx; i += gridDim.x * blockDim.x) st.X[st.xlist[i]] = 0u;
+}
+
+__global__ void k_reset_x(state st) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) st.counters[C_X] = 0u;
+}
+
+// ---------------------------------------------------- transfer phase
+// Destination stations of station-to-station queries first, in location
+// order, so that the time_at_dest updates they make (raptor.h:737-739) are
+// seen by later stations exactly as in the sequential loop; the timeline of
+// those updates is kept per query.
+__global__ void k_transfers_pre(state st) {
+  auto const s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= st.S) return;
+  auto& sl = st.slots[s];
+  auto const ln = st.lanes[s];
+  st.timeline_n[s] = 0u;
+  if (!ln.run) return;
+  st.tad_phase[s] = sl.tad[ln.k];
+  if (!(ln.mode & 2u)) return;
+  auto const k = ln.k;
+  auto const g = s >> 5;
+  auto const bit = 1u << (s & 31);
+  uint32_t tl_n = 0;
+  for (auto i = 0u; i != sl.n_dest; ++i) {
+    auto const d = st.dest_pool[sl.dest_off + i].loc;
+    if (!(st.Y[d * st.G + g] & bit)) continue;
+    auto const tk = dec(st.tmp[li(st, d, s)], ln.gtag);
+    if (tk == kKeyInv) continue;
+    auto const fp = key_add(tk, 0);
+    auto const bk = dec(st.best[li(st, d, s)], ln.gtag);
+    auto& rtw = st.rt[rti(st, k, d, s)];
+    if (fp < bk && fp < dec(rtw, ln.qtag)) rtw = enc(ln.qtag, fp);
+    auto const tad = static_cast<int>(sl.tad[k]);
+    if (fp < bk && fp <= tad) {
+      auto const lbv = st.lb[li(st, d, s)];
+      if (lbv == 0xFFFFu || fp + static_cast<int>(lbv) > tad) continue;
+      rtw = enc(ln.qtag, fp);
+      st.best[li(st, d, s)] = enc(ln.gtag, fp);
+      mark(st, st.X, st.xlist, C_X, d * st.G + g, bit);
+      if (fp < tad && tl_n < kMaxTimeline) {
+        st.timeline[s * kMaxTimeline + tl_n++] = {d, 0u, fp};
+      } else if (fp < tad) {
+        atomicOr(&st.counters[C_ERR], 1u);
+      }
+      update_tad(sl, k, fp);
+    }
+  }
+  st.timeline_n[s] = tl_n;
+}
+
+// tad in effect at position (hi, lo) of the phase's processing order
+__device__ __forceinline__ int tad_at(state const& st, uint32_t s, uint32_t hi, uint32_t lo) {
+  auto const n = st.timeline_n[s];
+  int tad = st.tad_phase[s];
+  for (auto i = 0u; i != n; ++i) {
+    auto const& e = st.timeline[s * kMaxTimeline + i];
+    if (e.pos_hi < hi || (e.pos_hi == hi && e.pos_lo < lo)) tad = e.tad;
+    else break;
+  }
+  return tad;
+}
+
+// update_transfers, raptor.h:680-743: warp per marked (station, group)
+__global__ void k_transfers(state st) {
+  auto const lane = threadIdx.x & 31u;
+  auto const warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  auto const n_warps = (gridDim.x * blockDim.x) >> 5;
+  auto const ny = st.counters[C_Y];
+  for (auto w = warp; w < ny; w += n_warps) {
+    auto const e = st.ylist[w];
+    auto const g = e % st.G, l = e / st.G;
+    auto const s = g * 32u + lane;
+    auto const ln = st.lanes[s];
+    auto const ym = st.Y[e];
+    bool want = false;
+    if (((ym >> lane) & 1u) && ln.run && !((ln.mode & 2u) && ((st.D[e] >> lane) & 1u))) {
+      auto const tk = dec(st.tmp[li(st, l, s)], ln.gtag);
+      if (tk != kKeyInv) {
+        auto const slp = &st.slots[s];
+        auto const tt = static_cast<int>(adjusted<int>(slp->tts, static_cast<int>(st.tt.transfer_time[l])));
+        auto const fp = key_add(tk, tt);
+        auto const bk = dec(st.best[li(st, l, s)], ln.gtag);
+        auto& rtw = st.rt[rti(st, ln.k, l, s)];
+        if (fp < bk && fp < dec(rtw, ln.qtag)) rtw = enc(ln.qtag, fp);
+        auto const tad = (ln.mode & 2u) ? tad_at(st, s, l, 0u) : static_cast<int>(st.tad_phase[s]);
+        if (fp < bk && fp <= tad) {
+          auto const lbv = st.lb[li(st, l, s)];
+          if (lbv != 0xFFFFu && fp + static_cast<int>(lbv) <= tad) {
+            rtw = enc(ln.qtag, fp);
+            st.best[li(st, l, s)] = enc(ln.gtag, fp);
+            want = true;
+          }
+        }
+      }
+    }
+    auto const b = __ballot_sync(kFull, want);
+    if (lane == 0 && b) mark(st, st.X, st.xlist, C_X, e, b);
+  }
+}
+
+// update_intermodal_footpaths, raptor.h:954-1026: per query, its egress
+// stations in location order
+__global__ void k_intermodal(state st) {
+  auto const s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= st.S) return;
+  auto const ln = st.lanes[s];
+  if (!ln.run || !(ln.mode & 1u)) return;
+  auto& sl = st.slots[s];
+  auto const g = s >> 5;
+  auto const bit = 1u << (s & 31);
+  for (auto i = 0u; i != sl.n_dest; ++i) {
+    auto const dr = st.dest_pool[sl.dest_off + i];
+    if (!(st.Y[dr.loc * st.G + g] & bit)) continue;
+    auto const tk = dec(st.tmp[li(st, dr.loc, s)], ln.gtag);
+    if (tk == kKeyInv) continue;
+    auto const end_time = key_add(tk, static_cast<int>(dr.dist));
+    if (end_time <= sl.tad[ln.k]) {
+      st.rt[rti(st, ln.k, B2R_SPECIAL_END, s)] = enc(ln.qtag, end_time);
+      st.best[li(st, B2R_SPECIAL_END, s)] = enc(ln.gtag, end_time);
+      update_tad(sl, ln.k, end_time);
+    }
+  }
+}
+
+// ---------------------------------------------------- footpath phase
+struct fp_cand {
+  uint32_t src, pos, dest;
+  int key;
+};
+
+// footpaths into destination stations, in the reference's processing order
+// (source location, then position in the source's footpath list)
+__global__ void k_footpaths_pre(state st) {
+  auto const s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= st.S) return;
+  auto& sl = st.slots[s];
+  auto const ln = st.lanes[s];
+  st.timeline_n[s] = 0u;
+  if (!ln.run) return;
+  st.tad_phase[s] = sl.tad[ln.k];
+  if (!(ln.mode & 2u)) return;
+  auto const fwd = ln.fwd != 0;
+  auto const k = ln.k;
+  auto const g = s >> 5;
+  auto const bit = 1u << (s & 31);
+  auto const& T = st.tt;
+  constexpr int kMaxC = 64;
+  fp_cand c[kMaxC];
+  int nc = 0;
+  for (auto i = 0u; i != sl.n_dest; ++i) {
+    auto const d = st.dest_pool[sl.dest_off + i].loc;
+    auto const* iidx = fwd ? T.fp_in_idx : T.fp_out_idx;
+    auto const* idat = fwd ? T.fp_in : T.fp_out;
+    for (auto x = iidx[d]; x != iidx[d + 1]; ++x) {
+      auto const src = B2R_FP_TARGET(idat[x]);
+      if (!(st.Y[src * st.G + g] & bit)) continue;
+      auto const tk = dec(st.tmp[li(st, src, s)], ln.gtag);
+      if (tk == kKeyInv) continue;
+      auto const* oidx = fwd ? T.fp_out_idx : T.fp_in_idx;
+      auto const* odat = fwd ? T.fp_out : T.fp_in;
+      for (auto y = oidx[src]; y != oidx[src + 1]; ++y) {
+        if (B2R_FP_TARGET(odat[y]) != d) continue;
+        if (nc == kMaxC) {
+          atomicOr(&st.counters[C_ERR], 2u);
+          break;
+        }
+        auto const dur = adjusted<int>(sl.tts, static_cast<int>(B2R_FP_DURATION(odat[y])));
+        c[nc++] = {src, y - oidx[src], d, key_add(tk, dur)};
+        break;
+      }
+    }
+  }
+  for (int a = 1; a < nc; ++a) {  // insertion sort by (src, pos)
+    auto const x = c[a];
+    int b = a - 1;
+    while (b >= 0 && (c[b].src > x.src || (c[b].src == x.src && c[b].pos > x.pos))) {
+      c[b + 1] = c[b];
+      --b;
+    }
+    c[b + 1] = x;
+  }
+  uint32_t tl_n = 0;
+  for (int a = 0; a < nc; ++a) {
+    auto const d = c[a].dest;
+    auto const fp = c[a].key;
+    auto const bk = dec(st.best[li(st, d, s)], ln.gtag);
+    auto& rtw = st.rt[rti(st, k, d, s)];
+    if (fp < bk && fp < dec(rtw, ln.qtag)) rtw = enc(ln.qtag, fp);
+    auto const tad = static_cast<int>(sl.tad[k]);
+    if (fp < bk && fp <= tad) {
+      auto const lbv = st.lb[li(st, d, s)];
+      if (lbv == 0xFFFFu || fp + static_cast<int>(lbv) > tad) continue;
+      rtw = enc(ln.qtag, fp);
+      st.best[li(st, d, s)] = enc(ln.gtag, fp);
+      mark(st, st.X, st.xlist, C_X, d * st.G + g, bit);
+      if (fp < tad && tl_n < kMaxTimeline) {
+        st.timeline[s * kMaxTimeline + tl_n++] = {c[a].src, c[a].pos, fp};
+      } else if (fp < tad) {
+        atomicOr(&st.counters[C_ERR], 1u);
+      }
+      update_tad(sl, k, fp);
+    }
+  }
+  st.timeline_n[s] = tl_n;
+}
+
+// update_footpaths, raptor.h:745-845: warp per marked (station, group);
+// labels of footpath targets are combined with atomicMin (the phase's final
+// labels and marks do not depend on the processing order).
+__global__ void k_footpaths(state st) {
+  auto const lane = threadIdx.x & 31u;
+  auto const warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  auto const n_warps = (gridDim.x * blockDim.x) >> 5;
+  auto const ny = st.counters[C_Y];
+  auto const& T = st.tt;
+  for (auto w = warp; w < ny; w += n_warps) {
+    auto const e = st.ylist[w];
+    auto const g = e % st.G, src = e / st.G;
+    auto const s = g * 32u + lane;
+    auto const ln = st.lanes[s];
+    auto const fwd = ln.fwd != 0;
+    bool act = ((st.Y[e] >> lane) & 1u) && ln.run;
+    int tk = kKeyInv;
+    if (act) {
+      tk = dec(st.tmp[li(st, src, s)], ln.gtag);
+      act = tk != kKeyInv;
+    }
+    auto const* idx = fwd ? T.fp_out_idx : T.fp_in_idx;
+    auto const* dat = fwd ? T.fp_out : T.fp_in;
+    auto const b = act ? idx[src] : 0u;
+    auto const n = act ? idx[src + 1] - b : 0u;
+    // lanes of one group may differ in direction: iterate to the longest list
+    auto n_max = n;
+    for (auto o = 16; o > 0; o >>= 1) n_max = max(n_max, __shfl_xor_sync(kFull, n_max, o));
+    slot_t const* slp = &st.slots[s];
+    auto const tad_flat = (act && !(ln.mode & 2u)) ? static_cast<int>(slp->tad[ln.k]) : 0;
+    for (auto j = 0u; j != n_max; ++j) {
+      bool want = false;
+      uint32_t tgt = 0;
+      if (j < n) {
+        auto const fp = dat[b + j];
+        tgt = B2R_FP_TARGET(fp);
+        if (!((ln.mode & 2u) && ((st.D[tgt * st.G + g] >> lane) & 1u))) {
+          auto const key = key_add(tk, adjusted<int>(slp->tts, static_cast<int>(B2R_FP_DURATION(fp))));
+          auto const bk = dec(st.best[li(st, tgt, s)], ln.gtag);
+          if (key < bk) {
+            atomicMin(&st.rt[rti(st, ln.k, tgt, s)], enc(ln.qtag, key));
+            auto const tad = (ln.mode & 2u) ? tad_at(st, s, src, j) : tad_flat;
+            if (key <= tad) {
+              auto const lbv = st.lb[li(st, tgt, s)];
+              if (lbv != 0xFFFFu && key + static_cast<int>(lbv) <= tad) {
+                atomicMin(&st.best[li(st, tgt, s)], enc(ln.gtag, key));
+                want = true;
+              }
+            }
+          }
+        }
+      }
+      mark_warp(st, st.X, st.xlist, C_X, want, tgt * st.G + g, lane);
+    }
+  }
+}
+
+// ------------------------------------------------- round end / results
+__global__ void k_ctl_end(state st) {
+  auto const s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= st.S) return;
+  auto& sl = st.slots[s];
+  if (sl.state != S_RUN) return;
+  sl.k = static_cast<uint8_t>(sl.k + 1);
+  if (sl.k >= sl.end_k) sl.state = S_COLLECT;
+}
+
+__device__ bool dominates(journey_rec const& a, journey_rec const& b) {  // journey.h:84-92
+  if (a.start_time <= a.dest_time) {
+    return a.transfers <= b.transfers && a.start_time >= b.start_time && a.dest_time <= b.dest_time;
+  }
+  return a.transfers <= b.transfers && a.start_time <= b.start_time && a.dest_time >= b.dest_time;
+}
+
+__device__ int alloc_block(state const& st, uint32_t s) {
+  auto const words = (st.max_j + 31u) / 32u;
+  for (auto w = 0u; w != words; ++w) {
+    auto& u = st.blocks_used[s * words + w];
+    auto const free_bits = ~u;
+    if (free_bits != 0u) {
+      auto const b = __ffs(free_bits) - 1;
+      if (w * 32u + b >= st.max_j) break;
+      u |= 1u << b;
+      return static_cast<int>(w * 32u + b);
+    }
+  }
+  return -1;
+}
+
+__device__ void free_block(state const& st, uint32_t s, uint16_t blk) {
+  auto const words = (st.max_j + 31u) / 32u;
+  st.blocks_used[s * words + blk / 32u] &= ~(1u << (blk % 32u));
+}
+
+// pareto_set::add, pareto_set.h:21-37
+__device__ bool pareto_add(state const& st, uint32_t s, slot_t& sl, journey_rec el) {
+  auto* els = st.journeys + static_cast<size_t>(s) * st.max_j;
+  uint32_t n_removed = 0;
+  for (auto i = 0u; i < sl.n_journeys; ++i) {
+    if (dominates(els[i], el)) return true;
+    if (dominates(el, els[i])) {
+      free_block(st, s, els[i].block);
+      ++n_removed;
+      continue;
+    }
+    els[i - n_removed] = els[i];
+  }
+  sl.n_journeys -= n_removed;
+  auto const blk = alloc_block(st, s);
+  if (blk < 0 || sl.n_journeys >= st.max_j) return false;
+  el.block = static_cast<uint16_t>(blk);
+  els[sl.n_journeys++] = el;
+  return true;
+}
+
+// result collection (raptor.h:393-413) and the reconstruction worklist
+// (search.h:457-475)
+__global__ void k_collect(state st) {
+  auto const s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= st.S) return;
+  auto& sl = st.slots[s];
+  if (sl.state != S_COLLECT || sl.one_to_all) return;
+  auto const qtag = tagcode(sl.gen_query);
+  auto const fwd = sl.fwd != 0;
+  auto const n_d = sl.intermodal_dest ? 1u : sl.n_dest;
+  for (auto i = 0u; i != n_d; ++i) {
+    auto const d = sl.intermodal_dest ? B2R_SPECIAL_END : st.dest_pool[sl.dest_off + i].loc;
+    for (auto k = 1u; k < sl.end_k; ++k) {
+      auto const key = dec(st.rt[rti(st, k, d, s)], qtag);
+      if (key == kKeyInv) continue;
+      journey_rec j{};
+      j.start_time = sl.cur_start_time;
+      j.dest_time = sl.base_days * 1440 + from_key(fwd, key);
+      j.dest = d;
+      j.transfers = static_cast<uint8_t>(k - 1);
+      if (!pareto_add(st, s, sl, j)) {
+        sl.error = B2R_ERR_CAPACITY;
+        sl.state = S_ERROR;
+        return;
+      }
+    }
+  }
+  auto* els = st.journeys + static_cast<size_t>(s) * st.max_j;
+  for (auto i = 0u; i != sl.n_journeys; ++i) {
+    auto const& j = els[i];
+    auto const tt = j.dest_time > j.start_time ? j.dest_time - j.start_time : j.start_time - j.dest_time;
+    if (!j.reconstructed && !j.error &&
+        (sl.ontrip || (sl.iv_from <= j.start_time && j.start_time < sl.iv_to)) &&
+        tt < sl.fastest_direct) {
+      st.recon_list[atomicAdd(&st.counters[C_RECON], 1u)] = (s << 16) | i;
+    }
+  }
+}
+
+__global__ void k_reconstruct(state st) {
+  auto const n = st.counters[C_RECON];
+  for (auto i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    auto const e = st.recon_list[i];
+    auto const s = e >> 16, ji = e & 0xFFFFu;
+    auto& sl = st.slots[s];
+    auto& j = st.journeys[static_cast<size_t>(s) * st.max_j + ji];
+    recon_ctx c;
+    c.st = &st;
+    c.T = &st.tt;
+    c.sl = &sl;
+    c.s = s;
+    c.fwd = sl.fwd != 0;
+    c.qtag = tagcode(sl.gen_query);
+    c.base_days = sl.base_days;
+    c.base = sl.base;
+    c.ontrip = sl.ontrip != 0;
+    c.j = &j;
+    c.legs = st.legs + (static_cast<size_t>(s) * st.max_j + j.block) * kMaxLegs;
+    c.run();
+    if (c.failed) {
+      j.error = 1;
+    } else {
+      j.reconstructed = 1;
+      j.n_legs = static_cast<uint16_t>(c.n_legs);
+    }
+  }
+}
+
+// early termination (search.h:477-492) and seeding of the next start-time
+// group: next_start_time + add_start (raptor.h:179-203) + the
+// time_at_dest bound of execute (raptor.h:211-214)
+__global__ void k_next(state st) {
+  auto const s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= st.S) return;
+  auto& sl = st.slots[s];
+  if (sl.state != S_COLLECT && sl.state != S_START) return;
+  auto const fwd = sl.fwd != 0;
+  if (sl.state == S_COLLECT && sl.min_connection_count > 0 && !sl.one_to_all) {
+    uint32_t n_in = 0;
+    auto* els = st.journeys + static_cast<size_t>(s) * st.max_j;
+    for (auto i = 0u; i != sl.n_journeys; ++i) {
+      n_in += sl.ontrip ? 1u : ((sl.iv_from <= els[i].start_time && els[i].start_time < sl.iv_to) ? 1u : 0u);
+    }
+    if (n_in >= sl.min_connection_count &&
+        ((fwd && sl.extend_earlier && !sl.extend_later) || (!fwd && !sl.extend_earlier && sl.extend_later))) {
+      sl.early_term = 1;
+      if (fwd) sl.iv_from = sl.cur_start_time;
+      else sl.iv_to = sl.cur_start_time + 1;
+    }
+  }
+  if (sl.state == S_COLLECT) sl.need_sweep = 1;
+  auto const* starts = st.start_pool + sl.starts_off;
+  if (sl.early_term || sl.next_start >= sl.n_starts) {
+    sl.state = S_DONE;
+    return;
+  }
+  // next start-time group
+  auto const g0 = sl.next_start;
+  auto const tas = starts[g0].time_at_start;
+  auto g1 = g0 + 1;
+  while (g1 < sl.n_starts && starts[g1].time_at_start == tas) ++g1;
+  if (sl.gen_group >= 0xFFFEu) {  // tag space exhausted: clear this slot's labels
+    for (auto l = 0u; l != st.tt.n_loc; ++l) {
+      st.best[li(st, l, s)] = 0xFFFFFFFFu;
+      st.tmp[li(st, l, s)] = 0xFFFFFFFFu;
+    }
+    sl.gen_group = 0;
+  }
+  ++sl.gen_group;
+  auto const gtag = tagcode(sl.gen_group), qtag = tagcode(sl.gen_query);
+  auto const g = s >> 5;
+  auto const bit = 1u << (s & 31);
+  for (auto i = g0; i != g1; ++i) {
+    auto const l = starts[i].stop;
+    auto const key = to_key(fwd, clamp16(starts[i].time_at_stop - sl.base_days * 1440));
+    auto& bw = st.best[li(st, l, s)];
+    if (key < dec(bw, gtag)) bw = enc(gtag, key);
+    auto& rw = st.rt[rti(st, 0, l, s)];
+    if (key < dec(rw, qtag)) rw = enc(qtag, key);
+    mark(st, st.X, st.xlist, C_X, l * st.G + g, bit);
+  }
+  auto const span = sl.one_to_all ? static_cast<int>(sl.max_travel_time)
+                                  : (min(static_cast<int>(sl.fastest_direct), static_cast<int>(sl.max_travel_time)) + 1);
+  auto const worst = tas + (fwd ? span : -span);
+  auto const d_worst = to_key(fwd, clamp16(worst - sl.base_days * 1440));
+  for (auto i = 0; i != kK; ++i) {
+    if (d_worst < sl.tad[i]) sl.tad[i] = static_cast<int16_t>(d_worst);
+  }
+  sl.cur_start_time = tas;
+  sl.next_start = g1;
+  sl.k = 1;
+  sl.state = S_RUN;
+  ++sl.n_groups_run;
+}
+
+}  // namespace b2r::dev

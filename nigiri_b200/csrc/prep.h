@@ -1,0 +1,77 @@
+// Host-side per-query preparation for the device engine: everything
+// routing::search<Dir, Algo> does before and between the Algo calls
+// (include/nigiri/routing/search.h:84-172, 204-345, 401-417) for the static
+// instantiation.  The device runs the start-time groups, the rounds, the
+// result collection and the reconstruction.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "b2r.h"
+
+namespace b2r {
+
+struct host_view;
+
+struct start_label {  // routing::start, start_times.h:21-26
+  int32_t time_at_start;
+  int32_t time_at_stop;
+  uint32_t stop;
+};
+
+struct tts_norm {  // transfer_time_settings after search::init()
+  uint8_t is_default{1};
+  int16_t min_transfer_time{0};
+  int16_t additional_time{0};
+  float factor{1.0F};
+};
+
+struct prepped_query {
+  int status{B2R_OK};
+  bool empty_result{false};  // start and destination overlap
+  bool fwd{true};
+  bool one_to_all{false};
+  bool ontrip{true};
+  bool intermodal_dest{false};
+  uint8_t start_mode{0}, dest_mode{0};
+  uint8_t max_transfers{14};
+  uint8_t end_k{16};
+  int16_t max_travel_time{7200};
+  int16_t max_start_offset_{7200};
+  int16_t fastest_direct{32767};
+  uint16_t base{0};        // day index relative to the internal interval
+  int32_t base_days{0};    // days since epoch
+  int32_t iv_from{0}, iv_to{0};  // search interval
+  uint32_t min_connection_count{0};
+  bool extend_earlier{false}, extend_later{false};
+  int32_t data_max_from{0}, data_max_to{0};  // interval_estimator clamp
+  tts_norm tts;
+  tts_norm tts_raw;  // as given (fastest-direct uses it)
+  std::vector<b2r_offset> start_offsets, dest_offsets;  // sanitized order
+  std::vector<start_label> starts;                      // sorted
+  std::vector<uint32_t> dest_locs;                      // ascending
+  std::vector<std::pair<uint32_t, uint16_t>> dest_dist; // intermodal, ascending
+  std::vector<uint16_t> lb;                             // [n_locations]
+};
+
+// Computes everything above; `lb_host` = compute the Dijkstra lower bounds
+// on the host (otherwise lb is left empty and the device computes it).
+void prepare(host_view const& tt, b2r_query const& q, bool lb_host,
+             prepped_query& out);
+
+// Start labels of [from, to) for an interval extension (search.h:294-312).
+void add_interval_starts(host_view const& tt, prepped_query const& p,
+                         int32_t from, int32_t to, bool add_ontrip,
+                         std::vector<start_label>& starts);
+// interval_estimator::extension, interval_estimate.h:82-106
+bool extend_interval(prepped_query const& p, int32_t ext_from, int32_t ext_to,
+                     uint32_t num_con_req, int32_t& from, int32_t& to);
+
+// The flattened timetable as seen by host code (plain pointers).
+struct host_view {
+  b2r_timetable_desc d;
+  int32_t internal_from_days() const { return d.date_range_from - 5; }
+};
+
+}  // namespace b2r

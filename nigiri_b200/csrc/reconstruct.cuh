@@ -1,0 +1,552 @@
+// Device-side journey reconstruction: one thread per journey walks the
+// round times of its query backwards (src/routing/raptor/reconstruct.cc:
+// 22-877 for Vias = 0 and no real-time overlay) and then applies the
+// footpath optimisations of src/routing/raptor/optimize_footpaths.cc.
+// Legs are written to the journey's leg block in device memory.
+#pragma once
+
+#include "engine.cuh"
+
+namespace b2r::dev {
+
+struct recon_ctx {
+  state const* st;
+  dtt const* T;
+  slot_t const* sl;
+  uint32_t s;          // slot
+  bool fwd;
+  uint16_t qtag;
+  int32_t base_days;
+  uint16_t base;
+  bool ontrip;
+  journey_rec* j;
+  b2r_leg* legs;       // kMaxLegs
+  int n_legs;
+  bool failed;
+
+  // ------------------------------------------------------------- access
+  __device__ int rt_t(unsigned k, uint32_t l) const {  // delta_t of round_times[k][l]
+    auto const key = dec(st->rt[(static_cast<size_t>(k) * T->n_loc + l) * st->S + s], qtag);
+    return from_key(fwd, key);
+  }
+  __device__ int inv() const { return fwd ? 32767 : -32768; }
+  __device__ bool beq(int a, int b) const { return fwd ? a <= b : a >= b; }
+  __device__ int dir(int a) const { return fwd ? a : -a; }
+  __device__ uint32_t n_stops(uint32_t r) const { return T->route_stop_idx[r + 1] - T->route_stop_idx[r]; }
+  __device__ uint32_t stopw(uint32_t r, uint32_t i) const { return T->route_stops[T->route_stop_idx[r] + i]; }
+  __device__ uint16_t ev(uint32_t t, uint32_t s_idx, bool arr) const {
+    auto const r = T->transport_route[t];
+    auto const n_t = T->route_tr_to[r] - T->route_tr_from[r];
+    return T->st[T->route_st_from[r] + n_t * (s_idx * 2u - (arr ? 1u : 0u)) + (t - T->route_tr_from[r])];
+  }
+  __device__ int32_t ev_time(uint32_t t, uint16_t day, uint32_t s_idx, bool arr) const {
+    auto const e = ev(t, s_idx, arr);
+    return (T->internal_from_days + static_cast<int32_t>(day)) * 1440 + (e & 31) * 1440 + (e >> 5);
+  }
+  __device__ int unix_to_delta(int32_t t) const { return clamp16(t - base_days * 1440); }
+  __device__ int32_t delta_to_unix(int d) const { return base_days * 1440 + d; }
+  __device__ b2r_offset const* start_offs() const { return st->off_pool + sl->soff_off; }
+  __device__ b2r_offset const* dest_offs() const { return st->off_pool + sl->doff_off; }
+
+  __device__ uint32_t root(uint32_t idx) const {
+    if (T->parent == nullptr) return idx;
+    auto l = idx;
+    for (int i = 0;; ++i) {
+      auto const p = T->parent[l];
+      if (p == B2R_INVALID_IDX) break;
+      if (p == idx || i > 20) {
+        l = T->parent[idx];
+        break;
+      }
+      l = p;
+    }
+    return l;
+  }
+  // matches(tt, mode, a, b), for_each_meta.h:47-70 (no equivalence lists)
+  __device__ bool matches(uint8_t mode, uint32_t a, uint32_t b) const {
+    if (a == b) return true;
+    if (mode == B2R_MATCH_EXACT || T->children_idx == nullptr) {
+      if (mode == B2R_MATCH_EQUIVALENT) return root(a) == b;
+      return false;
+    }
+    if (mode == B2R_MATCH_INTERMODAL) {
+      for (auto i = T->children_idx[a]; i != T->children_idx[a + 1]; ++i) {
+        auto const c = T->children[i];
+        if (T->loc_type != nullptr && T->loc_type[c] == B2R_LOC_GENERATED_TRACK && c == b) return true;
+      }
+      return false;
+    }
+    auto const r = mode == B2R_MATCH_EQUIVALENT ? root(a) : a;
+    if (r == b) return true;
+    for (auto i = T->children_idx[r]; i != T->children_idx[r + 1]; ++i) {
+      auto const c = T->children[i];
+      if (c == b) return true;
+      for (auto j = T->children_idx[c]; j != T->children_idx[c + 1]; ++j) {
+        if (T->children[j] == b) return true;
+      }
+    }
+    return false;
+  }
+  __device__ bool is_journey_start(uint32_t l) const {
+    auto const* o = start_offs();
+    for (auto i = 0U; i != sl->n_soff; ++i) {
+      if (matches(sl->start_mode, o[i].target, l)) return true;
+    }
+    return false;
+  }
+
+  // -------------------------------------------------------------- legs
+  __device__ b2r_leg make_leg(uint32_t a, uint32_t b, int32_t ta, int32_t tb) const {
+    b2r_leg l{};
+    l.from = fwd ? a : b;
+    l.to = fwd ? b : a;
+    l.dep_time = fwd ? ta : tb;
+    l.arr_time = fwd ? tb : ta;
+    return l;
+  }
+  __device__ static void set_run(b2r_leg& l, uint32_t t, uint16_t day, uint32_t a, uint32_t b) {
+    l.kind = B2R_LEG_TRANSPORT;
+    l.transport = t;
+    l.day = day;
+    l.stop_from = static_cast<uint16_t>(a < b ? a : b);
+    l.stop_to = static_cast<uint16_t>((a < b ? b : a) + 1u);
+  }
+  __device__ static void set_fp(b2r_leg& l, uint32_t target, int dur) {
+    l.kind = B2R_LEG_FOOTPATH;
+    l.transport = target;
+    l.duration = static_cast<int16_t>(dur > 511 ? 511 : dur);
+    l.transport_mode_id = 0;
+  }
+  __device__ static void set_off(b2r_leg& l, b2r_offset const& o) {
+    l.kind = B2R_LEG_OFFSET;
+    l.transport = o.target;
+    l.duration = o.duration;
+    l.transport_mode_id = o.transport_mode_id;
+  }
+  __device__ void push(b2r_leg const& l) {
+    if (n_legs >= kMaxLegs) {
+      failed = true;
+      return;
+    }
+    legs[n_legs++] = l;
+  }
+
+  // reconstruct.cc:180-280 (single pass: no vias)
+  __device__ bool find_start_in_prev_round(unsigned k, uint32_t t, uint16_t day, uint32_t finish,
+                                           b2r_leg& out) const {
+    auto const r = T->transport_route[t];
+    auto const size = n_stops(r);
+    auto const n = fwd ? finish + 1u : size - finish;
+    for (auto i = 1u; i < n; ++i) {
+      auto const si = fwd ? finish - i : finish + i;
+      auto const w = stopw(r, si);
+      auto const l = B2R_STOP_LOC(w);
+      if ((fwd && !B2R_STOP_IN(w)) || (!fwd && !B2R_STOP_OUT(w))) continue;
+      auto const event_time = unix_to_delta(ev_time(t, day, si, !fwd));
+      auto const round_time = rt_t(k - 1, l);
+      if (beq(round_time, event_time) ||
+          (k == 1 && sl->start_mode == B2R_MATCH_EQUIVALENT && is_journey_start(l) &&
+           (ontrip ? beq(round_time, event_time) : round_time == event_time))) {
+        out = make_leg(l, B2R_STOP_LOC(stopw(r, finish)), delta_to_unix(event_time),
+                       ev_time(t, day, finish, fwd));
+        set_run(out, t, day, si, finish);
+        return true;
+      }
+    }
+    return false;
+  }
+
+  // reconstruct.cc:292-373; columns are ordered by minutes after midnight,
+  // so the transports with the wanted mam form one run found by binary
+  // search and visited in index order like the reference's linear loop.
+  __device__ bool get_route_transport(unsigned k, int time, uint32_t r, uint32_t si,
+                                      b2r_leg& out) const {
+    auto const minutes = static_cast<int>(base) * 1440 + time;
+    auto const day = static_cast<uint16_t>(minutes / 1440);
+    auto const mam = static_cast<int16_t>(minutes % 1440);
+    auto const t0 = T->route_tr_from[r], n_t = T->route_tr_to[r] - t0;
+    auto const* col = T->st + T->route_st_from[r] + n_t * (si * 2u - (fwd ? 1u : 0u));
+    uint32_t lo = 0;
+    if (T->route_sorted[r]) {
+      uint32_t hi = n_t;
+      while (lo < hi) {
+        auto const mid = (lo + hi) >> 1;
+        if ((col[mid] >> 5) < static_cast<uint16_t>(mam < 0 ? 0 : mam)) lo = mid + 1;
+        else hi = mid;
+      }
+    }
+    for (auto x = lo; x < n_t; ++x) {
+      auto const cnt = delta_count(col[x]);
+      auto const m = static_cast<int16_t>(cnt % 1440);
+      if (m != mam) {
+        if (T->route_sorted[r] && m > mam) break;
+        continue;
+      }
+      auto const tday = static_cast<uint16_t>(static_cast<int>(day) - cnt / 1440);
+      auto const t = t0 + x;
+      if (!bf_test(*T, T->transport_bf[t], tday)) continue;
+      if (find_start_in_prev_round(k, t, tday, si, out)) return true;
+    }
+    return false;
+  }
+
+  // reconstruct.cc:375-545
+  __device__ bool get_transport(unsigned k, uint32_t l, int time, b2r_leg& out) const {
+    for (auto ri = T->loc_routes_idx[l]; ri != T->loc_routes_idx[l + 1]; ++ri) {
+      auto const r = T->loc_routes[ri];
+      auto const n = n_stops(r);
+      for (auto i = 0u; i != n; ++i) {
+        auto const w = stopw(r, i);
+        if (B2R_STOP_LOC(w) != l || (fwd && (i == 0u || !B2R_STOP_OUT(w))) ||
+            (!fwd && (i + 1u == n || !B2R_STOP_IN(w)))) {
+          continue;
+        }
+        if (get_route_transport(k, time, r, i, out)) return true;
+      }
+    }
+    return false;
+  }
+
+  // reconstruct.cc:547-666 (no vias)
+  __device__ bool check_fp(unsigned k, uint32_t l, int curr_time, uint32_t target, int dur_raw,
+                           bool adjust, b2r_leg& fp_leg, b2r_leg& tr_leg) const {
+    auto const d = adjust ? static_cast<int>(adjusted<int16_t>(sl->tts, static_cast<int16_t>(dur_raw)))
+                          : static_cast<int>(static_cast<int16_t>(dur_raw));
+    auto const fp_start = static_cast<int>(static_cast<int16_t>(curr_time - dir(d)));
+    if (!get_transport(k, target, fp_start, tr_leg)) return false;
+    fp_leg = make_leg(target, l, delta_to_unix(fp_start), delta_to_unix(fp_start + dir(d)));
+    set_fp(fp_leg, target, dur_raw);
+    return true;
+  }
+
+  // reconstruct.cc:700-790
+  __device__ bool get_legs(unsigned k, uint32_t l, b2r_leg& fp_leg, b2r_leg& tr_leg) const {
+    auto const curr = rt_t(k, l);
+    if (sl->dest_mode == B2R_MATCH_INTERMODAL && k == j->transfers + 1u) {
+      auto const* o = dest_offs();
+      for (auto i = 0u; i != sl->n_doff; ++i) {
+        if (o[i].duration >= 511) continue;
+        auto found = false;
+        // for_each_meta(kIntermodal): the location and its generated tracks;
+        // the last matching meta wins (reconstruct.cc:680-696)
+        auto const try_eq = [&](uint32_t eq) {
+          b2r_leg f, t;
+          if (check_fp(k, l, curr, eq, o[i].duration, false, f, t)) {
+            b2r_offset oo = o[i];
+            oo.target = eq;
+            set_off(f, oo);
+            fp_leg = f;
+            tr_leg = t;
+            found = true;
+          }
+        };
+        try_eq(o[i].target);
+        if (T->children_idx != nullptr) {
+          for (auto c = T->children_idx[o[i].target]; c != T->children_idx[o[i].target + 1]; ++c) {
+            auto const ch = T->children[c];
+            if (T->loc_type != nullptr && T->loc_type[ch] == B2R_LOC_GENERATED_TRACK) try_eq(ch);
+          }
+        }
+        if (found) return true;
+      }
+      return false;
+    }
+    auto const same = (k == j->transfers + 1u)
+                          ? 0
+                          : static_cast<int>(adjusted<uint8_t>(sl->tts, T->transfer_time[l]));
+    if (check_fp(k, l, curr, l, same, false, fp_leg, tr_leg)) return true;
+    auto const* idx = fwd ? T->fp_in_idx : T->fp_out_idx;
+    auto const* fps = fwd ? T->fp_in : T->fp_out;
+    for (auto i = idx[l]; i != idx[l + 1]; ++i) {
+      if (check_fp(k, l, curr, B2R_FP_TARGET(fps[i]), static_cast<int>(B2R_FP_DURATION(fps[i])),
+                   true, fp_leg, tr_leg)) {
+        return true;
+      }
+    }
+    return false;
+  }
+
+  // reconstruct.cc:30-160 (no vias)
+  __device__ bool find_start_footpath(b2r_leg& out, bool& has) const {
+    has = false;
+    auto const& back = legs[n_legs - 1];
+    auto const lsl = fwd ? back.from : back.to;
+    auto const lst = fwd ? back.dep_time : back.arr_time;
+    if (sl->start_mode != B2R_MATCH_INTERMODAL && is_journey_start(lsl) && beq(j->start_time, lst)) {
+      return true;
+    }
+    auto const* o = start_offs();
+    if (sl->start_mode == B2R_MATCH_INTERMODAL) {
+      for (auto i = 0u; i != sl->n_soff; ++i) {
+        if (matches(sl->start_mode, o[i].target, lsl) && beq(j->start_time, lst - dir(o[i].duration))) {
+          out = make_leg(B2R_SPECIAL_START, lsl, lst - dir(o[i].duration), lst);
+          set_off(out, o[i]);
+          has = true;
+          return true;
+        }
+      }
+      return false;
+    }
+    auto const jst = unix_to_delta(j->start_time);
+    auto const fp_target_time = rt_t(0, lsl);
+    auto const* idx = fwd ? T->fp_in_idx : T->fp_out_idx;
+    auto const* fps = fwd ? T->fp_in : T->fp_out;
+    for (auto i = idx[lsl]; i != idx[lsl + 1]; ++i) {
+      auto const tgt = B2R_FP_TARGET(fps[i]);
+      auto const d = static_cast<int>(adjusted<int16_t>(sl->tts, static_cast<int16_t>(B2R_FP_DURATION(fps[i]))));
+      auto const lhs = jst + static_cast<int16_t>(dir(d));
+      if (is_journey_start(tgt) && fp_target_time != inv() &&
+          (ontrip ? beq(lhs, fp_target_time) : lhs == fp_target_time)) {
+        out = make_leg(tgt, lsl, j->start_time, delta_to_unix(fp_target_time));
+        set_fp(out, tgt, d);
+        has = true;
+        return true;
+      }
+    }
+    return false;
+  }
+
+  // ---------------------------------------------- optimize_footpaths.cc
+  __device__ uint32_t r_of(b2r_leg const& l) const { return T->transport_route[l.transport]; }
+  __device__ uint32_t loc_at(b2r_leg const& l, uint32_t si) const { return B2R_STOP_LOC(stopw(r_of(l), si)); }
+  __device__ uint32_t word_at(b2r_leg const& l, uint32_t si) const { return stopw(r_of(l), si); }
+  __device__ int32_t time_at(b2r_leg const& l, uint32_t si, bool arr) const {
+    return ev_time(l.transport, l.day, si, arr);
+  }
+
+  // optimize_footpaths.cc:15-60; `offs` = start offsets of the journey query
+  __device__ void opt_initial_departure(b2r_offset const* offs, uint32_t n_offs) {
+    if (n_legs <= 1 || legs[0].kind != B2R_LEG_OFFSET || legs[1].kind != B2R_LEG_TRANSPORT) return;
+    auto& ol = legs[0];
+    auto& tl = legs[1];
+    auto best = static_cast<int>(ol.duration);
+    auto const end = static_cast<uint32_t>(tl.stop_to - 1u);
+    for (auto si = 0u; si < end; ++si) {
+      if (!B2R_STOP_IN(word_at(tl, si))) continue;
+      for (auto i = 0u; i != n_offs; ++i) {
+        auto const& o = offs[i];
+        if (best <= o.duration || o.target != loc_at(tl, si)) continue;
+        auto const dep = time_at(tl, si, false);
+        auto const o_start = dep - o.duration;
+        if (ol.dep_time <= o_start) {
+          ol.to = loc_at(tl, si);
+          ol.dep_time = o_start;
+          ol.arr_time = dep;
+          set_off(ol, o);
+          tl.from = loc_at(tl, si);
+          tl.dep_time = dep;
+          tl.stop_from = static_cast<uint16_t>(si);
+          best = o.duration;
+        }
+      }
+    }
+  }
+
+  __device__ void opt_initial_start_footpath() {  // :62-120
+    if (n_legs <= 1 || legs[0].kind != B2R_LEG_FOOTPATH || legs[1].kind != B2R_LEG_TRANSPORT) return;
+    auto& fl = legs[0];
+    auto& tl = legs[1];
+    auto const start_loc = fl.from;
+    auto best = static_cast<int>(adjusted<int16_t>(sl->tts, fl.duration));
+    auto const end = static_cast<uint32_t>(tl.stop_to - 1u);
+    for (auto si = 0u; si < end; ++si) {
+      if (!B2R_STOP_IN(word_at(tl, si))) continue;
+      for (auto i = T->fp_out_idx[start_loc]; i != T->fp_out_idx[start_loc + 1]; ++i) {
+        auto const fp = T->fp_out[i];
+        if (B2R_FP_TARGET(fp) != loc_at(tl, si)) continue;
+        auto const d = static_cast<int>(adjusted<int16_t>(sl->tts, static_cast<int16_t>(B2R_FP_DURATION(fp))));
+        if (d < best) {
+          auto const dep = time_at(tl, si, false);
+          auto const fp_start = dep - d;
+          if (fl.dep_time <= fp_start) {
+            fl.to = loc_at(tl, si);
+            fl.dep_time = fp_start;
+            fl.arr_time = dep;
+            set_fp(fl, loc_at(tl, si), d);
+            tl.from = loc_at(tl, si);
+            tl.dep_time = dep;
+            tl.stop_from = static_cast<uint16_t>(si);
+            best = d;
+          }
+        }
+        break;
+      }
+    }
+  }
+
+  __device__ void opt_last_arrival(b2r_offset const* offs, uint32_t n_offs) {  // :122-187
+    if (n_legs <= 1 || legs[n_legs - 1].kind != B2R_LEG_OFFSET || legs[n_legs - 2].kind != B2R_LEG_TRANSPORT) {
+      return;
+    }
+    auto& ol = legs[n_legs - 1];
+    auto& tl = legs[n_legs - 2];
+    auto best = static_cast<int>(ol.duration);
+    auto const from = static_cast<uint32_t>(tl.stop_from + 1u);
+    auto const size = n_stops(r_of(tl));
+    for (auto si = from; si < size; ++si) {
+      if (!B2R_STOP_OUT(word_at(tl, si))) continue;
+      for (auto i = 0u; i != n_offs; ++i) {
+        auto const& o = offs[i];
+        if (best <= o.duration || o.target != loc_at(tl, si)) continue;
+        auto const arr = time_at(tl, si, true);
+        auto const o_end = arr + o.duration;
+        if (o_end <= ol.arr_time) {
+          ol.from = loc_at(tl, si);
+          ol.dep_time = arr;
+          ol.arr_time = o_end;
+          set_off(ol, o);
+          tl.to = loc_at(tl, si);
+          tl.arr_time = arr;
+          tl.stop_to = static_cast<uint16_t>(si + 1u);
+          best = o.duration;
+        }
+      }
+    }
+  }
+
+  __device__ void opt_final_egress_footpath() {  // :189-257
+    if (n_legs <= 1 || legs[n_legs - 1].kind != B2R_LEG_FOOTPATH || legs[n_legs - 2].kind != B2R_LEG_TRANSPORT) {
+      return;
+    }
+    auto& fl = legs[n_legs - 1];
+    auto& tl = legs[n_legs - 2];
+    auto const dest_loc = fl.to;
+    auto best = static_cast<int>(adjusted<int16_t>(sl->tts, fl.duration));
+    auto const from = static_cast<uint32_t>(tl.stop_from + 1u);
+    auto const size = n_stops(r_of(tl));
+    for (auto si = from; si < size; ++si) {
+      if (!B2R_STOP_OUT(word_at(tl, si))) continue;
+      for (auto i = T->fp_in_idx[dest_loc]; i != T->fp_in_idx[dest_loc + 1]; ++i) {
+        auto const fp = T->fp_in[i];
+        if (B2R_FP_TARGET(fp) != loc_at(tl, si)) continue;
+        auto const d = static_cast<int>(adjusted<int16_t>(sl->tts, static_cast<int16_t>(B2R_FP_DURATION(fp))));
+        if (d < best) {
+          auto const arr = time_at(tl, si, true);
+          auto const fp_end = arr + d;
+          if (fp_end <= fl.arr_time) {
+            fl.from = loc_at(tl, si);
+            fl.dep_time = arr;
+            fl.arr_time = fp_end;
+            set_fp(fl, dest_loc, d);
+            tl.to = loc_at(tl, si);
+            tl.arr_time = arr;
+            tl.stop_to = static_cast<uint16_t>(si + 1u);
+            best = d;
+          }
+        }
+        break;
+      }
+    }
+  }
+
+  // get_penalty, optimize_footpaths.cc:259-283, with IEEE double operations
+  // spelled out (no contraction) so the result equals the host's.
+  __device__ double penalty(int duration, int buffer, uint32_t from, uint32_t to) const {
+    auto w = static_cast<double>(duration);
+    if (matches(B2R_MATCH_EQUIVALENT, from, to)) {
+      auto const x = root(from);
+      auto const imp = T->importance == nullptr ? 0u : T->importance[x];
+      auto const q = __ddiv_rn(static_cast<double>(imp), static_cast<double>(T->max_importance));
+      w = __dsub_rn(w, __dmul_rn(q, 3.0));
+    }
+    auto const b = buffer < 0 ? 0 : (buffer > 15 ? 15 : buffer);
+    return __dsub_rn(w, __dmul_rn(0.2, static_cast<double>(b)));
+  }
+
+  __device__ void opt_transfers() {  // :285-450 (no vias)
+    for (auto i = 0; i + 2 < n_legs; ++i) {
+      auto& lf = legs[i];
+      auto& lp = legs[i + 1];
+      auto& lt = legs[i + 2];
+      if (lf.kind != B2R_LEG_TRANSPORT || lp.kind != B2R_LEG_FOOTPATH || lt.kind != B2R_LEG_TRANSPORT) continue;
+      auto const from_start = static_cast<uint32_t>(lf.stop_from + 1u);
+      auto const from_size = n_stops(r_of(lf));
+      auto const to_end = static_cast<uint32_t>(lt.stop_to - 1u);
+      auto pbest = penalty(lp.duration, lt.dep_time - lp.arr_time, lf.from, lt.to);
+      for (auto sf = from_start; sf < from_size; ++sf) {
+        if (!B2R_STOP_OUT(word_at(lf, sf))) continue;
+        for (auto s2 = 0u; s2 < to_end; ++s2) {
+          if (!B2R_STOP_IN(word_at(lt, s2))) continue;
+          auto const a = loc_at(lf, sf), b = loc_at(lt, s2);
+          for (auto x = T->fp_out_idx[a]; x != T->fp_out_idx[a + 1]; ++x) {
+            auto const fp = T->fp_out[x];
+            if (B2R_FP_TARGET(fp) != b) continue;
+            auto const d = static_cast<int>(adjusted<int16_t>(sl->tts, static_cast<int16_t>(B2R_FP_DURATION(fp))));
+            auto const arr = time_at(lf, sf, true);
+            auto const dep = time_at(lt, s2, false);
+            auto const arr_fp = arr + d;
+            if (arr_fp <= dep) {
+              auto const p = penalty(d, dep - arr_fp, a, b);
+              if (p < pbest) {
+                lf.to = a;
+                lf.arr_time = arr;
+                lf.stop_to = static_cast<uint16_t>(sf + 1u);
+                lt.from = b;
+                lt.dep_time = dep;
+                lt.stop_from = static_cast<uint16_t>(s2);
+                lp.from = a;
+                lp.to = b;
+                lp.dep_time = arr;
+                lp.arr_time = arr_fp;
+                set_fp(lp, B2R_FP_TARGET(fp), static_cast<int>(B2R_FP_DURATION(fp)));
+                pbest = p;
+              }
+            }
+            break;
+          }
+        }
+      }
+    }
+  }
+
+  // reconstruct.cc:792-877 + optimize_footpaths(journey_q)
+  __device__ void run() {
+    n_legs = 0;
+    failed = false;
+    auto l = j->dest;
+    for (auto i = 0u; i <= j->transfers && !failed; ++i) {
+      auto const k = j->transfers + 1u - i;
+      b2r_leg fp_leg, tr_leg;
+      if (!get_legs(k, l, fp_leg, tr_leg)) {
+        failed = true;
+        break;
+      }
+      l = fwd ? tr_leg.from : tr_leg.to;
+      if (i != 0 || fp_leg.from != fp_leg.to || fp_leg.dep_time != fp_leg.arr_time) push(fp_leg);
+      push(tr_leg);
+    }
+    if (!failed) {
+      b2r_leg init;
+      bool has = false;
+      if (!find_start_footpath(init, has)) failed = true;
+      else if (has) push(init);
+    }
+    if (failed) return;
+    if (fwd) {
+      for (auto a = 0, b = n_legs - 1; a < b; ++a, --b) {
+        auto const x = legs[a];
+        legs[a] = legs[b];
+        legs[b] = x;
+      }
+    } else {
+      for (auto i = 1; i < n_legs; ++i) {
+        if (legs[i].kind != B2R_LEG_FOOTPATH) continue;
+        auto const diff = legs[i].dep_time - legs[i - 1].arr_time;
+        legs[i].dep_time -= diff;
+        legs[i].arr_time -= diff;
+      }
+    }
+    // optimize_footpaths on the journey query (flipped for backward search)
+    auto const* jq_start = fwd ? start_offs() : dest_offs();
+    auto const n_jq_start = fwd ? sl->n_soff : sl->n_doff;
+    auto const* jq_dest = fwd ? dest_offs() : start_offs();
+    auto const n_jq_dest = fwd ? sl->n_doff : sl->n_soff;
+    opt_initial_departure(jq_start, n_jq_start);
+    opt_initial_start_footpath();
+    opt_last_arrival(jq_dest, n_jq_dest);
+    opt_final_egress_footpath();
+    opt_transfers();
+  }
+};
+
+}  // namespace b2r::dev

@@ -1,0 +1,99 @@
+"""Host timetables and seeded query streams (b2r_tt_* / b2r_queries_*)."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from . import _abi as A
+from .routing import B2RError, Offset, Query, TransferTimeSettings, _check, EXACT, INTERMODAL, FORWARD, BACKWARD
+
+# workload -> (timetable config, timetable seed); workloads 3 / 5 reuse the
+# timetables of 2 / 4
+TIMETABLE_OF = {1: (1, 1), 2: (2, 2), 3: (2, 2), 4: (4, 4), 5: (4, 4)}
+
+
+class HostTimetable:
+    """Flattened timetable in host memory (nigiri's finalize() applied)."""
+
+    def __init__(self, handle: C.c_void_p):
+        self.handle = handle
+        self.desc = A.TimetableDesc()
+        _check(A.lib().b2r_tt_desc(self.handle, C.byref(self.desc)))
+
+    @classmethod
+    def generate(cls, workload: int, cache_dir: str | None = None):
+        cfg, seed = TIMETABLE_OF[workload]
+        lib = A.lib()
+        if cache_dir:
+            path = os.path.join(cache_dir, f"tt_config{cfg}_seed{seed}.b2r")
+            if os.path.exists(path):
+                h = C.c_void_p()
+                if lib.b2r_tt_load(path.encode(), C.byref(h)) == 0:
+                    return cls(h)
+        h = C.c_void_p()
+        _check(lib.b2r_tt_generate(cfg, seed, C.byref(h)))
+        t = cls(h)
+        if cache_dir:
+            os.makedirs(cache_dir, exist_ok=True)
+            lib.b2r_tt_save(h, os.path.join(cache_dir, f"tt_config{cfg}_seed{seed}.b2r").encode())
+        return t
+
+    def close(self):
+        if self.handle:
+            A.lib().b2r_tt_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class QuerySet:
+    """Seeded synthetic queries of a workload, owned by the library."""
+
+    def __init__(self, tt: HostTimetable, workload: int, n: int, seed: int | None = None):
+        self.tt = tt
+        self.handle = C.c_void_p()
+        seed = 1000 + workload if seed is None else seed
+        _check(A.lib().b2r_queries_generate(tt.handle, workload, seed, n, C.byref(self.handle)))
+        self.n = A.lib().b2r_queries_count(self.handle)
+        # contiguous copy of the structs (offset pointers stay owned by the set)
+        self.arr = (A.Query * max(1, self.n))()
+        for i in range(self.n):
+            self.arr[i] = A.lib().b2r_queries_get(self.handle, i).contents
+
+    def subset(self, idx):
+        arr = (A.Query * max(1, len(idx)))()
+        for j, i in enumerate(idx):
+            arr[j] = self.arr[i]
+        return arr
+
+    def to_query(self, i) -> tuple[Query, str, int]:
+        """(routing.Query, direction, kind) of query i."""
+        x = self.arr[i]
+        modes = {A.B2R_MATCH_EXACT: EXACT, A.B2R_MATCH_INTERMODAL: INTERMODAL}
+        q = Query(start=[Offset(x.start[j].target, x.start[j].duration, x.start[j].transport_mode_id)
+                         for j in range(x.n_start)],
+                  destination=[Offset(x.destination[j].target, x.destination[j].duration,
+                                      x.destination[j].transport_mode_id)
+                               for j in range(x.n_destination)],
+                  start_time=(x.interval_from, x.interval_to) if x.is_interval else x.start_time,
+                  start_match_mode=modes[x.start_match_mode],
+                  dest_match_mode=modes[x.dest_match_mode],
+                  max_transfers=x.max_transfers,
+                  max_travel_time=x.max_travel_time,
+                  transfer_time_settings=TransferTimeSettings())
+        return q, (FORWARD if x.direction == A.B2R_FORWARD else BACKWARD), x.kind
+
+    def close(self):
+        if self.handle:
+            A.lib().b2r_queries_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,61 @@
+"""The C ABI library loads without a GPU and exports every entry point that
+include/b2r.h declares; the ctypes mirror matches the C struct layouts."""
+import ctypes as C
+import os
+import re
+import subprocess
+import tempfile
+
+from nigiri_b200 import _abi as A
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "b2r.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(b2r_[a-z0-9_]+)\s*\(", src)) - {"b2r_"})
+
+
+def test_library_exports_every_declared_entry_point():
+    lib = C.CDLL(A.LIB_PATH)
+    missing = [f for f in declared_functions() if not hasattr(lib, f)]
+    assert not missing, missing
+    assert set(declared_functions()) == set(A.EXPORTS)
+
+
+def test_struct_layouts_match_c():
+    code = r'''
+#include <stdio.h>
+#include <stddef.h>
+#include "b2r.h"
+int main() {
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(b2r_timetable_desc), sizeof(b2r_offset),
+         sizeof(b2r_query), sizeof(b2r_leg), sizeof(b2r_journey), sizeof(b2r_result),
+         sizeof(b2r_engine_config), sizeof(b2r_batch_stats), sizeof(b2r_tt_base));
+  printf("%zu %zu %zu\n", offsetof(b2r_query, tts_factor), offsetof(b2r_leg, transport_mode_id),
+         offsetof(b2r_result, n_start_times));
+  return 0;
+}
+'''
+    with tempfile.TemporaryDirectory() as d:
+        src = os.path.join(d, "t.c")
+        exe = os.path.join(d, "t")
+        open(src, "w").write(code)
+        subprocess.check_call(["gcc", "-I" + os.path.join(ROOT, "include"), src, "-o", exe])
+        out = subprocess.check_output([exe]).decode().split("\n")
+    sizes = [int(x) for x in out[0].split()]
+    assert sizes == [C.sizeof(A.TimetableDesc), C.sizeof(A.Offset), C.sizeof(A.Query),
+                     C.sizeof(A.Leg), C.sizeof(A.Journey), C.sizeof(A.Result),
+                     C.sizeof(A.EngineConfig), C.sizeof(A.BatchStats), C.sizeof(A.TtBase)]
+    offs = [int(x) for x in out[1].split()]
+    assert offs == [A.Query.tts_factor.offset, A.Leg.transport_mode_id.offset,
+                    A.Result.n_start_times.offset]
+
+
+def test_errors_without_gpu_are_status_codes():
+    lib = A.lib()
+    assert lib.b2r_engine_create(None, None, None) == -1
+    assert b"null" in lib.b2r_last_error()
+    assert lib.b2r_search_batch(None, None, 0, None) == -1
