@@ -1,0 +1,353 @@
+#!/usr/bin/env python
+"""Batched RAPTOR throughput of the B200 engine on the 40k-stop regional
+timetable (workload 2: 10,000-query class, intermodal one-to-one, batches of
+1024 resident queries per device pass).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B]
+    python bench.py --impl reference ...   # the CPU raptor (oracle) arm
+
+A step is one batch of B seeded queries through b2r_search_batch.  `value`
+is queries / device time of the batch (timetable resident, queries
+prepared); `e2e` is queries / wall time of the C-ABI call from host query
+structs to host results (host preparation, admission copies, result copies
+included).  Under torchrun every rank runs its own engine on its own query
+shard (replicas; no collective on the data path) and the max over ranks is
+reported.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = 2
+METRIC = "queries/sec & p99 latency, batched/served vs 1-query GPU RAPTOR, bit-exact"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--batch", type=int, default=1024)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--cpu-sample", type=int, default=0, help="queries in the CPU baseline sample")
+    p.add_argument("--no-extras", action="store_true", help="skip plain / roofline / CPU legs")
+    return p.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def percentile(xs, q):
+    if not xs:
+        return None
+    xs = sorted(xs)
+    k = (len(xs) - 1) * q
+    f = int(k)
+    c = min(f + 1, len(xs) - 1)
+    return xs[f] + (xs[c] - xs[f]) * (k - f)
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ncu_traffic_per_unit():
+    """DRAM bytes per scanned (route, query) stop step of the route scan
+    from the committed ncu capture (profiles/route_scan_traffic.json)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "route_scan_traffic.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return None
+
+
+# --------------------------------------------------------------- CPU arms
+def cpu_run(desc, qarr, n, threads):
+    import oracle_lib  # tests/ is on the path only for the CPU arms
+    lat = (C.c_double * max(1, n))()
+    nj = C.c_uint64()
+    wall = C.c_double()
+    oracle_lib.lib().or_run_many(C.byref(desc), qarr, n, threads, lat, C.byref(nj), C.byref(wall))
+    return wall.value, [lat[i] / 1e3 for i in range(n)], nj.value
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def reference_arm(args, rank, world):
+    """The reference's CPU raptor (oracle restatement) on all host threads."""
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from nigiri_b200.timetable import HostTimetable, QuerySet
+    h = HostTimetable.generate(WORKLOAD)
+    sample = args.cpu_sample or 512
+    threads = host_threads()
+    qs = QuerySet(h, WORKLOAD, sample * (args.steps + args.warmup), seed=1000 + WORKLOAD)
+    for w in range(args.warmup):
+        cpu_run(h.desc, qs.subset(range(w * sample, (w + 1) * sample)), sample, threads)
+    total, lats = 0.0, []
+    for k in range(args.steps):
+        off = (args.warmup + k) * sample
+        wall, lat, _ = cpu_run(h.desc, qs.subset(range(off, off + sample)), sample, threads)
+        total += wall
+        lats += lat
+    qps = sample * args.steps / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": qps, "unit": "queries/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int16", "data": "synthetic (seeded generator)",
+        "config": config_block(args, sample),
+        "p50_ms": percentile(lats, 0.5), "p99_ms": percentile(lats, 0.99),
+        "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": threads, "kind": "port",
+                         "sample": f"{sample} workload-2 queries per step, one query per thread"},
+        "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def config_block(args, batch):
+    return {"workload": "regional-40k-stops batched one-to-one (intermodal offset sets)",
+            "timetable": "40,009 locations, 4,000 base routes, ~436k transports, 365 days",
+            "global_batch": batch, "queries_per_step": batch, "max_transfers": 14,
+            "parallelism": f"replicas x{args.gpus}", "lower_bounds": "host dijkstra",
+            "l2": "round state of a step (>2.5 GB) exceeds L2; 512 MB written between steps"}
+
+
+# --------------------------------------------------------------- GPU arm
+def gpu_arm(args, rank, world, local):
+    import torch
+    from nigiri_b200 import _abi as A
+    from nigiri_b200 import routing as R
+    from nigiri_b200.timetable import HostTimetable, QuerySet
+
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+        pg = dist
+    h = HostTimetable.generate(WORKLOAD)
+    dtt = R.Timetable(h.desc, device=local, owner=h)
+    B = args.batch
+    eng = R.Engine(dtt, max_slots=B)
+    n_total = B * (args.warmup + args.steps)
+    qs = QuerySet(h, WORKLOAD, n_total, seed=1000 + WORKLOAD + 7919 * rank)
+    lib = A.lib()
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+
+    def one_batch(off, engine=eng):
+        arr = qs.subset(range(off, off + B))
+        out = (A.Result * B)()
+        t0 = time.perf_counter()
+        rc = lib.b2r_search_batch(engine.handle, arr, B, out)
+        t1 = time.perf_counter()
+        if rc != 0:
+            raise RuntimeError(lib.b2r_last_error().decode())
+        st = engine.stats()
+        return t1 - t0, st, out
+
+    for w in range(args.warmup):
+        one_batch(w * B)
+    clocks = ClockSampler(local)
+    clocks.start()
+    walls, devs, lats, launches, h2d, d2h = [], [], [], 0, 0, 0
+    for k in range(args.steps):
+        flush.fill_(k & 0xFF)
+        torch.cuda.synchronize()
+        if pg is not None:
+            pg.barrier()
+        wall, st, out = one_batch((args.warmup + k) * B)
+        torch.cuda.synchronize()
+        walls.append(wall)
+        devs.append(st.device_ms / 1e3)
+        launches += st.kernel_launches
+        for i in range(B):
+            lats.append(out[i].latency_ms)
+            d2h += out[i].n_journeys * C.sizeof(A.Journey)
+    ck = clocks.stop()
+    tot_wall, tot_dev = sum(walls), sum(devs)
+    if pg is not None:
+        t = torch.tensor([tot_wall, tot_dev], dtype=torch.float64, device=f"cuda:{local}")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        tot_wall, tot_dev = t.tolist()
+    n_q = B * args.steps * world
+    value = n_q / tot_dev
+    e2e = n_q / tot_wall
+    # host->device bytes: query structs + offsets + lower-bound columns
+    h2d_step = B * (C.sizeof(A.Query) + 2 * h.desc.n_locations)
+
+    extras = {}
+    if rank == 0 and not args.no_extras:
+        extras = extras_legs(args, h, dtt, qs, B, local)
+    if rank == 0:
+        peak, peak_kind = measured_peak()
+        rl = extras.get("roofline")
+        line = {
+            "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot_dev / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int16",
+            "data": "synthetic (seeded generator: timetable seed 2, query seed 1002+rank)",
+            "config": config_block(args, B),
+            "p50_ms": percentile(lats, 0.5), "p99_ms": percentile(lats, 0.99),
+            "e2e": {"value": e2e, "unit": "queries/s", "h2d_bytes_per_step": h2d_step,
+                    "d2h_bytes_per_step": d2h // max(1, args.steps)},
+            "gpu_launches": launches,
+            "clocks": ck,
+        }
+        line.update({k: v for k, v in extras.items()})
+        if rl is not None:
+            rl["peak"] = peak
+            rl["peak_kind"] = peak_kind
+            rl["frac"] = rl["achieved"] / peak
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def extras_legs(args, h, dtt, qs, B, local):
+    """Plain one-query-per-launch baseline, route-scan roofline and the CPU
+    baseline (rank 0, outside the timed region)."""
+    import torch
+    from nigiri_b200 import _abi as A
+    from nigiri_b200 import routing as R
+    lib = A.lib()
+    out = {}
+    # plain engine: one query per pass, per-round launches, sync per round
+    plain = R.Engine(dtt, max_slots=32, use_graphs=False)
+    n_plain = 64
+    arr = qs.subset(range(n_plain))
+    res = A.Result()
+    lat = []
+    t0 = time.perf_counter()
+    for i in range(n_plain):
+        a = time.perf_counter()
+        if lib.b2r_search_plain(plain.handle, C.byref(arr[i]), C.byref(res)) != 0:
+            raise RuntimeError(lib.b2r_last_error().decode())
+        lat.append((time.perf_counter() - a) * 1e3)
+    t1 = time.perf_counter()
+    out["plain_gpu"] = {"value": n_plain / (t1 - t0), "unit": "queries/s",
+                        "p50_ms": percentile(lat, 0.5), "p99_ms": percentile(lat, 0.99),
+                        "queries": n_plain}
+    del plain
+    # roofline of the route scan: CUDA events around every launch
+    prof = R.Engine(dtt, max_slots=B, profile=True)
+    arr = qs.subset(range(B))
+    o = (A.Result * B)()
+    if lib.b2r_search_batch(prof.handle, arr, B, o) != 0:
+        raise RuntimeError(lib.b2r_last_error().decode())
+    st = prof.stats()
+    per_launch_bytes = st.route_scan_bytes / max(1, st.route_scan_launches)
+    per_launch_s = st.route_scan_ms / 1e3 / max(1, st.route_scan_launches)
+    traffic = None
+    t = ncu_traffic_per_unit()
+    if t is not None and st.route_stop_visits:
+        traffic = t["dram_bytes_per_stop_visit"] * st.route_stop_visits / max(1, st.route_scan_launches)
+    out["roofline"] = {
+        "bound": "hbm", "achieved": per_launch_bytes / per_launch_s / 1e9, "peak": None,
+        "unit": "GB/s", "frac": None, "traffic": traffic,
+        "kernel": "k_route_scan", "launches": st.route_scan_launches,
+        "avg_launch_ms": per_launch_s * 1e3, "algorithmic_bytes_per_launch": per_launch_bytes,
+        "route_stop_visits": st.route_stop_visits, "route_scan_share_of_device_time":
+            st.route_scan_ms / max(1e-9, st.device_ms),
+    }
+    del prof
+    # CPU baseline: the oracle on a bounded sample, all host threads
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    threads = host_threads()
+    sample = args.cpu_sample or min(B, 512)
+    wall, lat, _ = cpu_run(h.desc, qs.subset(range(sample)), sample, threads)
+    out["cpu_baseline"] = {"value": sample / wall, "unit": "queries/s", "cores": threads,
+                           "kind": "port", "sample": f"{sample} queries of the step-0 batch",
+                           "p99_ms": percentile(lat, 0.99)}
+    return out
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+    else:
+        gpu_arm(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -240,6 +240,8 @@ typedef struct b2r_result {
   /* counters (raptor_stats) */
   uint64_t n_rounds;
   uint64_t n_start_times;
+  /* time from the batch call to this query's completion (host clock) */
+  double latency_ms;
 } b2r_result;
 
 /* ---------------------------------------------------------------- engine */
@@ -261,7 +263,11 @@ typedef struct b2r_engine_config {
   uint32_t use_lower_bounds;/* 1 = dijkstra lower bounds (reference default) */
   uint32_t use_graphs;      /* 1 = capture the super-step in a CUDA graph */
   uint32_t route_block;     /* launch shape: warps per CTA in the route scan */
-  uint32_t reserved[7];
+  uint32_t max_starts;      /* start labels per query (default 4096) */
+  uint32_t steps_per_sync;  /* super-steps between host checks (default 4) */
+  uint32_t profile;         /* 1 = time route scans with CUDA events and
+                               count their work (disables graphs) */
+  uint32_t reserved[4];
 } b2r_engine_config;
 
 void b2r_engine_config_init(b2r_engine_config* c);
@@ -305,7 +311,13 @@ typedef struct b2r_batch_stats {
   uint64_t kernel_launches;
   uint64_t super_steps;
   uint64_t route_scan_launches;
-  double route_scan_ms;
+  double route_scan_ms;     /* summed CUDA-event time of the route scans
+                               (profiling engines only) */
+  uint64_t route_stop_visits; /* (route, query) stop steps scanned */
+  uint64_t et_events;         /* event times examined by trip searches */
+  uint64_t et_days;           /* service days examined by trip searches */
+  uint64_t label_writes;      /* tmp label improvements */
+  uint64_t route_scan_bytes;  /* algorithmic bytes of the route scans */
 } b2r_batch_stats;
 int b2r_last_batch_stats(const b2r_engine* e, b2r_batch_stats* s);
 

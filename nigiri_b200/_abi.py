@@ -93,6 +93,7 @@ class Result(C.Structure):
         ("n_rows", C.c_uint32), ("base_day", C.c_int32),
         ("round_times", C.POINTER(C.c_int16)),
         ("n_rounds", C.c_uint64), ("n_start_times", C.c_uint64),
+        ("latency_ms", C.c_double),
     ]
 
 
@@ -101,14 +102,18 @@ class EngineConfig(C.Structure):
         ("max_slots", C.c_uint32), ("hbm_budget", C.c_uint64),
         ("max_journeys", C.c_uint32), ("host_threads", C.c_uint32),
         ("use_lower_bounds", C.c_uint32), ("use_graphs", C.c_uint32),
-        ("route_block", C.c_uint32), ("reserved", C.c_uint32 * 7),
+        ("route_block", C.c_uint32), ("max_starts", C.c_uint32),
+        ("steps_per_sync", C.c_uint32), ("profile", C.c_uint32), ("reserved", C.c_uint32 * 4),
     ]
 
 
 class BatchStats(C.Structure):
     _fields_ = [("device_ms", C.c_double), ("host_prep_ms", C.c_double),
                 ("kernel_launches", C.c_uint64), ("super_steps", C.c_uint64),
-                ("route_scan_launches", C.c_uint64), ("route_scan_ms", C.c_double)]
+                ("route_scan_launches", C.c_uint64), ("route_scan_ms", C.c_double),
+                ("route_stop_visits", C.c_uint64), ("et_events", C.c_uint64),
+                ("et_days", C.c_uint64), ("label_writes", C.c_uint64),
+                ("route_scan_bytes", C.c_uint64)]
 
 
 class TtBase(C.Structure):

@@ -135,6 +135,10 @@ struct b2r_engine {
 
   b2r_batch_stats last{};
   cudaEvent_t ev0{nullptr}, ev1{nullptr};
+  // profiling: event pairs bracketing each route-scan launch
+  std::vector<cudaEvent_t> prof_ev;
+  size_t prof_used{0};
+  std::chrono::steady_clock::time_point batch_t0;
 
   // results of the last batch / serving tickets
   struct result_store {
@@ -288,6 +292,7 @@ __global__ void k_set_journeys(dev::state st, uint32_t s, dev::journey_rec const
 }  // namespace b2r
 
 b2r_engine::~b2r_engine() {
+  for (auto ev : prof_ev) cudaEventDestroy(ev);
   if (graph != nullptr) cudaGraphExecDestroy(graph);
   if (stream != nullptr) cudaStreamDestroy(stream);
   if (ev0 != nullptr) cudaEventDestroy(ev0);
@@ -314,7 +319,19 @@ void enqueue_superstep(b2r_engine& e, cudaStream_t s) {
   dev::k_ctl_dest<<<slot_blocks, 128, 0, s>>>(st);
   dev::k_mark_routes<<<list_blocks, 256, 0, s>>>(st);
   dev::k_ctl_marked<<<slot_blocks, 128, 0, s>>>(st);
+  cudaEvent_t ev_a = nullptr, ev_b = nullptr;
+  if (e.cfg.profile) {  // CUDA events on the launching stream around the scan
+    while (e.prof_used + 2 > e.prof_ev.size()) {
+      cudaEvent_t x;
+      B2R_CUDA(cudaEventCreate(&x));
+      e.prof_ev.push_back(x);
+    }
+    ev_a = e.prof_ev[e.prof_used++];
+    ev_b = e.prof_ev[e.prof_used++];
+    B2R_CUDA(cudaEventRecord(ev_a, s));
+  }
   dev::k_route_scan<<<e.sms * 8, 256, 0, s>>>(st);
+  if (e.cfg.profile) B2R_CUDA(cudaEventRecord(ev_b, s));
   dev::k_clear_x<<<list_blocks, 256, 0, s>>>(st);
   dev::k_reset_x<<<1, 32, 0, s>>>(st);
   dev::k_transfers_pre<<<slot_blocks, 128, 0, s>>>(st);
@@ -763,10 +780,14 @@ struct batch_runner {
       std::vector<exported> ex;
       export_slots(e, done_slots, n_js, n_rows, ex, st);
       std::vector<uint32_t> retired;
+      auto const now_ms = std::chrono::duration<double, std::milli>(
+                              std::chrono::steady_clock::now() - e.batch_t0)
+                              .count();
       for (auto i = 0U; i != done_slots.size(); ++i) {
         auto const s = done_slots[i];
         auto& q = runs[static_cast<size_t>(slot_q[s])];
         on_phase_done(e, q, ex[i]);
+        q.res.view.latency_ms = now_ms;
         if (q.rearm) {
           rearm(s, q, st);
         } else {
@@ -976,7 +997,8 @@ int b2r_engine_create(b2r_timetable* tt, const b2r_engine_config* cfg_in, b2r_en
       e->cfg = cfg;
       e->sms = b2r::n_sms(tt->device);
       e->max_j = std::max(32U, std::min(4096U, (cfg.max_journeys + 31U) & ~31U));
-      e->max_starts = cfg.reserved[0] != 0 ? cfg.reserved[0] : 4096U;
+      e->max_starts = cfg.max_starts != 0 ? cfg.max_starts : 4096U;
+      if (cfg.profile) e->cfg.use_graphs = 0;
       e->max_dest = 512U;
       e->max_off = 128U;
       auto const nl = tt->d.n_loc;
@@ -1036,6 +1058,9 @@ int b2r_engine_create(b2r_timetable* tt, const b2r_engine_config* cfg_in, b2r_en
       al(st.tad_phase, S);
       al(st.status_word, 4);
       al(e->d_summary, S);
+      al(st.prof, 8);
+      st.profile = cfg.profile ? 1u : 0u;
+      B2R_CUDA(cudaMemset(st.prof, 0, 8 * sizeof(unsigned long long)));
       al(e->d_exp_list, S);
       B2R_CUDA(cudaMemset(st.slots, 0, S * sizeof(b2r::dev::slot_t)));
       B2R_CUDA(cudaMemset(st.rt, 0xFF, static_cast<size_t>(b2r::dev::kK) * nl * S * 4));
@@ -1052,7 +1077,7 @@ int b2r_engine_create(b2r_timetable* tt, const b2r_engine_config* cfg_in, b2r_en
       B2R_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
       B2R_CUDA(cudaEventCreate(&e->ev0));
       B2R_CUDA(cudaEventCreate(&e->ev1));
-      if (cfg.use_graphs) b2r::capture_graph(*e);
+      if (e->cfg.use_graphs) b2r::capture_graph(*e);
       B2R_CUDA(cudaDeviceSynchronize());
       *out = e.release();
       return B2R_OK;
@@ -1081,11 +1106,14 @@ int b2r_search_batch(b2r_engine* e, const b2r_query* qs, uint32_t n, b2r_result*
       B2R_CUDA(cudaSetDevice(e->tt->device));
       std::vector<b2r::query_run> runs;
       auto const t0 = std::chrono::steady_clock::now();
+      e->batch_t0 = t0;
       b2r::prepare_all(*e, qs, n, runs);
       auto const t1 = std::chrono::steady_clock::now();
       b2r::batch_runner br{*e, runs, e->cfg.use_graphs != 0 && e->graph != nullptr};
+      e->prof_used = 0;
+      if (e->cfg.profile) B2R_CUDA(cudaMemsetAsync(e->st.prof, 0, 8 * sizeof(unsigned long long), e->stream));
       B2R_CUDA(cudaEventRecord(e->ev0, e->stream));
-      br.run(e->cfg.reserved[1] != 0 ? e->cfg.reserved[1] : 4U);
+      br.run(e->cfg.steps_per_sync != 0 ? e->cfg.steps_per_sync : 4U);
       B2R_CUDA(cudaEventRecord(e->ev1, e->stream));
       B2R_CUDA(cudaEventSynchronize(e->ev1));
       float ms = 0;
@@ -1095,6 +1123,27 @@ int b2r_search_batch(b2r_engine* e, const b2r_query* qs, uint32_t n, b2r_result*
       e->last.host_prep_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
       e->last.kernel_launches = br.launches;
       e->last.super_steps = br.steps;
+      if (e->cfg.profile) {
+        double scan_ms = 0;
+        for (size_t i = 0; i + 1 < e->prof_used; i += 2) {
+          float x = 0;
+          cudaEventElapsedTime(&x, e->prof_ev[i], e->prof_ev[i + 1]);
+          scan_ms += x;
+        }
+        unsigned long long c[8] = {};
+        B2R_CUDA(cudaMemcpy(c, e->st.prof, sizeof(c), cudaMemcpyDeviceToHost));
+        e->last.route_scan_launches = e->prof_used / 2;
+        e->last.route_scan_ms = scan_ms;
+        e->last.route_stop_visits = c[0];
+        e->last.et_events = c[1];
+        e->last.et_days = c[2];
+        e->last.label_writes = c[3];
+        // byte model of the route phase: per scanned stop of a query the
+        // stop word (4 B), its previous-round label (2 B) and one event time
+        // (2 B); per trip search 2 B per examined event and 8 B per examined
+        // service day; 2 B per label write
+        e->last.route_scan_bytes = c[0] * 8ull + c[1] * 2ull + c[2] * 8ull + c[3] * 2ull;
+      }
       uint32_t err = 0;
       B2R_CUDA(cudaMemcpy(&err, e->st.counters + b2r::dev::C_ERR, 4, cudaMemcpyDeviceToHost));
       if (err != 0) {

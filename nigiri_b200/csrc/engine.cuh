@@ -183,6 +183,8 @@ struct state {
   uint32_t* timeline_n;   // [S]
   int16_t* tad_phase;     // [S] tad[k] at the start of the phase
   uint32_t* status_word;  // [0] device error flags
+  unsigned long long* prof;  // route-scan work counters (profiling engines)
+  uint32_t profile;
 };
 
 // ------------------------------------------------------------- helpers

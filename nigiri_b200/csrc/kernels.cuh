@@ -48,7 +48,7 @@ __device__ __forceinline__ void update_tad(slot_t& sl, uint32_t k, int key) {  /
 // rules.  Routes flagged unsorted use the reference's linear seek.
 __device__ bool et_search(dtt const& T, bool fwd, uint32_t r, uint32_t si, uint16_t day_at_stop,
                           int mam, int lbv, int tad_k, uint16_t base, uint32_t& out_off,
-                          uint16_t& out_day) {
+                          uint16_t& out_day, uint32_t& n_ev, uint32_t& n_days) {
   auto const t0 = T.route_tr_from[r];
   auto const n = T.route_tr_to[r] - t0;
   auto const* col = T.st + T.route_st_from[r] + n * (si * 2u - (fwd ? 0u : 1u));
@@ -56,6 +56,7 @@ __device__ bool et_search(dtt const& T, bool fwd, uint32_t r, uint32_t si, uint1
   auto const rbf = T.route_bf[r];
   for (auto i = 0u; i != 6u; ++i) {
     auto const day = static_cast<uint16_t>(fwd ? day_at_stop + i : day_at_stop - i);
+    ++n_days;
     if (!bf_test(T, rbf, day)) continue;
     uint32_t j = 0;
     if (i == 0u) {
@@ -64,6 +65,7 @@ __device__ bool et_search(dtt const& T, bool fwd, uint32_t r, uint32_t si, uint1
         if (fwd) {  // first index with mam >= m
           while (lo < hi) {
             auto const mid = (lo + hi) >> 1;
+            ++n_ev;
             if (static_cast<int>(col[mid] >> 5) < mam) lo = mid + 1;
             else hi = mid;
           }
@@ -71,6 +73,7 @@ __device__ bool et_search(dtt const& T, bool fwd, uint32_t r, uint32_t si, uint1
         } else {  // first (from the end) with mam <= m: n - upper_bound(m)
           while (lo < hi) {
             auto const mid = (lo + hi) >> 1;
+            ++n_ev;
             if (static_cast<int>(col[mid] >> 5) <= mam) lo = mid + 1;
             else hi = mid;
           }
@@ -86,6 +89,7 @@ __device__ bool et_search(dtt const& T, bool fwd, uint32_t r, uint32_t si, uint1
     for (; j < n; ++j) {
       auto const idx = fwd ? j : n - 1u - j;
       auto const e = col[idx];
+      ++n_ev;
       auto const em = static_cast<int>(e >> 5);
       if (to_delta_key(fwd, day, base, em) + lbv > tad_k) return false;
       if (i == 0u && !(fwd ? mam <= em : mam >= em)) continue;
@@ -229,7 +233,9 @@ __global__ void __launch_bounds__(256) k_route_scan(state st) {
     bool et_valid = false;
     uint32_t et_off = 0;
     uint16_t et_day = 0;
+    uint32_t p_ev = 0, p_days = 0, p_writes = 0, p_stops = 0;
     for (auto i = 0u; i != n; ++i) {
+      p_stops += active ? 1u : 0u;
       auto const si = fwd ? i : n - 1u - i;
       auto const stp = T.route_stops[sb + si];
       auto const l = B2R_STOP_LOC(stp);
@@ -245,7 +251,10 @@ __global__ void __launch_bounds__(256) k_route_scan(state st) {
         if (by <= ln.tad_k && lbv != 0xFFFFu && by + static_cast<int>(lbv) <= ln.tad_k) {
           auto const word = enc(ln.gtag, by);
           auto* tp = &st.tmp[li(st, l, s)];
-          if (word < *tp) atomicMin(tp, word);
+          if (word < *tp) {
+            atomicMin(tp, word);
+            ++p_writes;
+          }
           reached = true;
         }
       }
@@ -270,7 +279,7 @@ __global__ void __launch_bounds__(256) k_route_scan(state st) {
             uint32_t nt = 0;
             uint16_t nd = 0;
             auto const found = et_search(T, fwd, r, si, day, mam, static_cast<int>(lbv), ln.tad_k,
-                                         ln.base, nt, nd);
+                                         ln.base, nt, nd, p_ev, p_days);
             if (found) {
               // current_best (raptor.h:1328-1329) is valid whenever the arrival
               // part ran or the station carries a label of this start time
@@ -286,6 +295,20 @@ __global__ void __launch_bounds__(256) k_route_scan(state st) {
             }
           }
         }
+      }
+    }
+    if (st.profile) {  // work counters for the roofline (warp-reduced)
+      for (auto o = 16; o > 0; o >>= 1) {
+        p_stops += __shfl_xor_sync(kFull, p_stops, o);
+        p_ev += __shfl_xor_sync(kFull, p_ev, o);
+        p_days += __shfl_xor_sync(kFull, p_days, o);
+        p_writes += __shfl_xor_sync(kFull, p_writes, o);
+      }
+      if (lane == 0) {
+        atomicAdd(&st.prof[0], static_cast<unsigned long long>(p_stops));
+        atomicAdd(&st.prof[1], static_cast<unsigned long long>(p_ev));
+        atomicAdd(&st.prof[2], static_cast<unsigned long long>(p_days));
+        atomicAdd(&st.prof[3], static_cast<unsigned long long>(p_writes));
       }
     }
   }

@@ -196,7 +196,7 @@ class Engine:
 
     def __init__(self, tt: Timetable, max_slots=1024, hbm_budget=64 << 30, max_journeys=128,
                  use_lower_bounds=True, use_graphs=True, host_threads=0, steps_per_sync=4,
-                 max_starts=4096):
+                 max_starts=4096, profile=False):
         cfg = A.EngineConfig()
         A.lib().b2r_engine_config_init(C.byref(cfg))
         cfg.max_slots = max_slots
@@ -205,8 +205,9 @@ class Engine:
         cfg.use_lower_bounds = int(use_lower_bounds)
         cfg.use_graphs = int(use_graphs)
         cfg.host_threads = host_threads
-        cfg.reserved[0] = max_starts
-        cfg.reserved[1] = steps_per_sync
+        cfg.max_starts = max_starts
+        cfg.steps_per_sync = steps_per_sync
+        cfg.profile = int(profile)
         self.tt = tt
         self.handle = C.c_void_p()
         _check(A.lib().b2r_engine_create(tt.handle, C.byref(cfg), C.byref(self.handle)))
