@@ -42,6 +42,8 @@ def parse():
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--cpu-sample", type=int, default=0, help="queries in the CPU baseline sample")
     p.add_argument("--no-extras", action="store_true", help="skip plain / roofline / CPU legs")
+    p.add_argument("--ncu-case", action="store_true",
+                   help="one batch without CUDA graphs (the case profiled with ncu)")
     return p.parse_args()
 
 
@@ -340,9 +342,31 @@ def extras_legs(args, h, dtt, qs, B, local):
     return out
 
 
+def ncu_case(args, local):
+    """One batch of `--batch` workload-2 queries, kernels launched one by one
+    (no graph) so that a profiler sees every launch."""
+    from nigiri_b200 import _abi as A
+    from nigiri_b200 import routing as R
+    from nigiri_b200.timetable import HostTimetable, QuerySet
+    h = HostTimetable.generate(WORKLOAD)
+    dtt = R.Timetable(h.desc, device=local, owner=h)
+    eng = R.Engine(dtt, max_slots=args.batch, use_graphs=False)
+    qs = QuerySet(h, WORKLOAD, args.batch, seed=1000 + WORKLOAD)
+    out = (A.Result * args.batch)()
+    rc = A.lib().b2r_search_batch(eng.handle, qs.arr, args.batch, out)
+    if rc != 0:
+        raise RuntimeError(A.lib().b2r_last_error().decode())
+    st = eng.stats()
+    print(json.dumps({"ncu_case": True, "batch": args.batch, "super_steps": st.super_steps,
+                      "kernel_launches": st.kernel_launches, "device_ms": st.device_ms}))
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
+    if args.ncu_case:
+        ncu_case(args, local)
+        return
     if args.impl == "reference":
         reference_arm(args, rank, world)
     else:
