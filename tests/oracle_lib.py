@@ -59,6 +59,12 @@ class OracleResult:
         lib().or_result_view(self.h, C.byref(self.view), C.byref(self.stats))
         self.n_loc = desc.n_locations
 
+    def records(self):
+        """Journey records, read while this result (which owns the journey
+        arrays the view points into) is alive."""
+        from journeys import records
+        return records(self.view)
+
     def state(self):
         import numpy as np
         rt = C.POINTER(C.c_int16)()
