@@ -341,7 +341,7 @@ void enqueue_superstep(b2r_engine& e, cudaStream_t s) {
   dev::k_footpaths<<<list_blocks, 256, 0, s>>>(st);
   dev::k_ctl_end<<<slot_blocks, 128, 0, s>>>(st);
   dev::k_collect<<<slot_blocks, 128, 0, s>>>(st);
-  dev::k_reconstruct<<<e.sms * 2, 128, 0, s>>>(st);
+  dev::k_reconstruct<<<e.sms * 4, 128, 0, s>>>(st);
   dev::k_next<<<slot_blocks, 128, 0, s>>>(st);
   k_summary<<<slot_blocks, 128, 0, s>>>(st, e.d_summary);
 }
@@ -539,6 +539,7 @@ void export_slots(b2r_engine& e, std::vector<uint32_t> const& slots,
 // Per query, what search::execute does between and after the Algo calls
 // (search.h:237-336): interval extension and the final filtering.
 struct query_run {
+  std::atomic<bool> ready{false};  // host preparation finished
   prepped_query p;
   int status{B2R_OK};
   bool finished{false};
@@ -664,6 +665,7 @@ struct batch_runner {
   std::vector<query_run>& runs;
   bool use_graph;
   uint64_t launches{0}, steps{0};
+  double busy_ms{0};  // device time of the super-step chunks
 
   void rearm(uint32_t s, query_run& q, cudaStream_t st) {
     // new phase: upload the new starts (and journeys kept), keep the rt
@@ -715,6 +717,7 @@ struct batch_runner {
         if (slot_q[s] != -1) continue;
         while (next < runs.size()) {
           auto& q = runs[next];
+          if (!q.ready.load(std::memory_order_acquire)) break;
           if (q.p.status != B2R_OK || q.p.empty_result) {
             q.status = q.p.status;
             q.res.view.status = q.p.status;
@@ -733,7 +736,7 @@ struct batch_runner {
           }
           break;
         }
-        if (next >= runs.size()) break;
+        if (next >= runs.size() || !runs[next].ready.load(std::memory_order_acquire)) break;
         slot_q[s] = static_cast<int64_t>(next);
         adm.emplace_back(s, &runs[next].p);
         ++next;
@@ -741,7 +744,13 @@ struct batch_runner {
       admit(e, adm, st);
     };
     admit_free();
+    auto busy_slots = [&]() {
+      for (auto x : slot_q)
+        if (x != -1) return true;
+      return false;
+    };
     auto busy = [&]() {
+      if (next < runs.size()) return true;  // queries still being prepared
       for (auto x : slot_q)
         if (x != -1) return true;
       return false;
@@ -752,6 +761,12 @@ struct batch_runner {
     for (auto const& q : runs) max_steps += 40ull * (q.p.starts.size() + 2) * (q.p.end_k + 2);
     while (busy()) {
       if (steps > max_steps) throw std::runtime_error("super-step cap exceeded");
+      if (!busy_slots()) {  // every resident query finished: wait for preparation
+        std::this_thread::yield();
+        admit_free();
+        continue;
+      }
+      B2R_CUDA(cudaEventRecord(e.ev0, st));
       for (uint32_t c = 0; c != chunk; ++c) {
         if (use_graph) {
           B2R_CUDA(cudaGraphLaunch(e.graph, st));
@@ -762,9 +777,16 @@ struct batch_runner {
         launches += kLaunchesPerStep;
         ++steps;
       }
+      B2R_CUDA(cudaEventRecord(e.ev1, st));
       B2R_CUDA(cudaMemcpyAsync(e.h_summary, e.d_summary, S * sizeof(b2r_engine::summary_t),
                                cudaMemcpyDeviceToHost, st));
       B2R_CUDA(cudaStreamSynchronize(st));
+      {
+        float ms = 0;
+        B2R_CUDA(cudaEventElapsedTime(&ms, e.ev0, e.ev1));
+        busy_ms += ms;
+      }
+      admit_free();  // queries whose preparation finished meanwhile
       std::vector<uint32_t> done_slots, n_js, n_rows;
       for (uint32_t s = 0; s != S; ++s) {
         if (slot_q[s] == -1) continue;
@@ -811,24 +833,36 @@ void capture_graph(b2r_engine& e) {
   cudaGraphDestroy(g);
 }
 
-void prepare_all(b2r_engine& e, b2r_query const* qs, uint32_t n, std::vector<query_run>& runs) {
-  runs.resize(n);
-  auto const n_threads = std::max(1U, std::min<uint32_t>(
-      e.cfg.host_threads != 0 ? e.cfg.host_threads : std::max(1U, std::thread::hardware_concurrency()),
-      n));
-  std::atomic<uint32_t> next{0};
-  auto const lb_host = e.cfg.use_lower_bounds != 0;
-  auto work = [&]() {
-    for (auto i = next++; i < n; i = next++) {
-      prepare(e.tt->view, qs[i], lb_host, runs[i].p);
-      if (!lb_host && !runs[i].p.one_to_all) runs[i].p.lb.clear();
-    }
-  };
+// Host preparation on worker threads, in query order, overlapping the
+// device work of the queries already admitted.
+struct preparer {
   std::vector<std::thread> pool;
-  for (auto t = 1U; t < n_threads; ++t) pool.emplace_back(work);
-  work();
-  for (auto& t : pool) t.join();
-}
+  std::atomic<uint32_t> next{0};
+  void start(b2r_engine& e, b2r_query const* qs, uint32_t n, std::vector<query_run>& runs,
+             bool inline_all) {
+    auto const hw = std::max(1U, std::thread::hardware_concurrency());
+    auto const n_threads = std::max(1U, std::min<uint32_t>(
+        e.cfg.host_threads != 0 ? e.cfg.host_threads : (hw > 1 ? hw - 1 : 1), n));
+    auto const lb_host = e.cfg.use_lower_bounds != 0;
+    auto work = [&e, qs, n, &runs, lb_host, this]() {
+      for (auto i = next++; i < n; i = next++) {
+        prepare(e.tt->view, qs[i], lb_host, runs[i].p);
+        if (!lb_host && !runs[i].p.one_to_all) runs[i].p.lb.clear();
+        runs[i].ready.store(true, std::memory_order_release);
+      }
+    };
+    if (inline_all) {
+      work();
+      return;
+    }
+    for (auto t = 0U; t < n_threads; ++t) pool.emplace_back(work);
+  }
+  void join() {
+    for (auto& t : pool) t.join();
+    pool.clear();
+  }
+  ~preparer() { join(); }
+};
 
 void fill_out(b2r_engine& e, std::vector<query_run>& runs, b2r_result* out) {
   e.results.resize(runs.size());
@@ -969,6 +1003,25 @@ int b2r_timetable_upload(const b2r_timetable_desc* d, int device, b2r_timetable*
       dd.loc_routes_idx = up(d->location_routes_index, nl + 1);
       dd.loc_routes = up(d->location_routes, d->location_routes_index[nl]);
       dd.route_sorted = up(sorted.data(), nr);
+      {  // location -> (route, stop position) pairs (reconstruct.cc:496-515 order)
+        std::vector<uint32_t> idx(nl + 1, 0U), rr;
+        std::vector<uint16_t> ss;
+        for (auto l = 0U; l != nl; ++l) {
+          for (auto ri = d->location_routes_index[l]; ri != d->location_routes_index[l + 1]; ++ri) {
+            auto const r = d->location_routes[ri];
+            for (auto i = d->route_stop_index[r]; i != d->route_stop_index[r + 1]; ++i) {
+              if (B2R_STOP_LOC(d->route_stops[i]) == l) {
+                rr.push_back(r);
+                ss.push_back(static_cast<uint16_t>(i - d->route_stop_index[r]));
+              }
+            }
+          }
+          idx[l + 1] = static_cast<uint32_t>(rr.size());
+        }
+        dd.lrs_idx = up(idx.data(), idx.size());
+        dd.lrs_route = up(rr.data(), rr.size());
+        dd.lrs_stop = up(ss.data(), ss.size());
+      }
       *out = t.release();
       return B2R_OK;
     } catch (b2r::cuda_error const& ex) {
@@ -1104,23 +1157,21 @@ int b2r_search_batch(b2r_engine* e, const b2r_query* qs, uint32_t n, b2r_result*
     if (e->serving) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "engine is serving");
     try {
       B2R_CUDA(cudaSetDevice(e->tt->device));
-      std::vector<b2r::query_run> runs;
+      std::vector<b2r::query_run> runs(n);
       auto const t0 = std::chrono::steady_clock::now();
       e->batch_t0 = t0;
-      b2r::prepare_all(*e, qs, n, runs);
-      auto const t1 = std::chrono::steady_clock::now();
+      b2r::preparer prep;
+      prep.start(*e, qs, n, runs, false);
       b2r::batch_runner br{*e, runs, e->cfg.use_graphs != 0 && e->graph != nullptr};
       e->prof_used = 0;
       if (e->cfg.profile) B2R_CUDA(cudaMemsetAsync(e->st.prof, 0, 8 * sizeof(unsigned long long), e->stream));
-      B2R_CUDA(cudaEventRecord(e->ev0, e->stream));
       br.run(e->cfg.steps_per_sync != 0 ? e->cfg.steps_per_sync : 4U);
-      B2R_CUDA(cudaEventRecord(e->ev1, e->stream));
-      B2R_CUDA(cudaEventSynchronize(e->ev1));
-      float ms = 0;
-      cudaEventElapsedTime(&ms, e->ev0, e->ev1);
+      prep.join();
+      auto const t1 = std::chrono::steady_clock::now();
+      B2R_CUDA(cudaStreamSynchronize(e->stream));
       e->last = {};
-      e->last.device_ms = ms;
-      e->last.host_prep_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+      e->last.device_ms = br.busy_ms;
+      e->last.host_prep_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();  // wall of the call
       e->last.kernel_launches = br.launches;
       e->last.super_steps = br.steps;
       if (e->cfg.profile) {
@@ -1168,8 +1219,9 @@ int b2r_search_plain(b2r_engine* e, const b2r_query* q, b2r_result* out) {
     }
     try {
       B2R_CUDA(cudaSetDevice(e->tt->device));
-      std::vector<b2r::query_run> runs;
-      b2r::prepare_all(*e, q, 1, runs);
+      std::vector<b2r::query_run> runs(1);
+      b2r::preparer prep;
+      prep.start(*e, q, 1, runs, true);
       b2r::batch_runner br{*e, runs, false};
       br.run(1);
       e->last = {};

@@ -64,6 +64,11 @@ struct dtt {
   uint32_t const* loc_routes_idx;
   uint32_t const* loc_routes;
   uint8_t const* route_sorted;  // 1: every event column is ordered by mam
+  // location -> (route, stop position) pairs in the order reconstruction
+  // visits them: routes of location_routes_, then stop positions ascending
+  uint32_t const* lrs_idx;
+  uint32_t const* lrs_route;
+  uint16_t const* lrs_stop;
 };
 
 // --------------------------------------------------------- per-slot data

@@ -680,8 +680,11 @@ __global__ void k_collect(state st) {
 }
 
 __global__ void k_reconstruct(state st) {
+  auto const lane = threadIdx.x & 31u;
+  auto const warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  auto const n_warps = (gridDim.x * blockDim.x) >> 5;
   auto const n = st.counters[C_RECON];
-  for (auto i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  for (auto i = warp; i < n; i += n_warps) {
     auto const e = st.recon_list[i];
     auto const s = e >> 16, ji = e & 0xFFFFu;
     auto& sl = st.slots[s];
@@ -697,13 +700,17 @@ __global__ void k_reconstruct(state st) {
     c.base = sl.base;
     c.ontrip = sl.ontrip != 0;
     c.j = &j;
+    c.lane = lane;
     c.legs = st.legs + (static_cast<size_t>(s) * st.max_j + j.block) * kMaxLegs;
     c.run();
-    if (c.failed) {
-      j.error = 1;
-    } else {
-      j.reconstructed = 1;
-      j.n_legs = static_cast<uint16_t>(c.n_legs);
+    __syncwarp();
+    if (lane == 0) {
+      if (c.failed) {
+        j.error = 1;
+      } else {
+        j.reconstructed = 1;
+        j.n_legs = static_cast<uint16_t>(c.n_legs);
+      }
     }
   }
 }

@@ -145,8 +145,10 @@ int16_t fastest_direct(view const& v, b2r_query const& q, std::vector<b2r_offset
   return static_cast<int16_t>(std::ceil(end_dist * q.fastest_direct_factor));
 }
 
-// dijkstra.cc:18-67 over the precomputed lower-bound graph, dial buckets
-// bounded by kMaxTravelTime.
+// dijkstra.cc:18-67 over the precomputed lower-bound graph: a bucket queue
+// over distances 0..kMaxTravelTime (dial.h) whose buckets are reused across
+// queries of the same thread.  Shortest distances do not depend on the pop
+// order inside a bucket.
 void lower_bounds(view const& v, prepped_query const& p, std::vector<uint16_t>& dist) {
   auto const n = v.d.n_locations;
   dist.assign(n, kUnreach);
@@ -159,13 +161,18 @@ void lower_bounds(view const& v, prepped_query const& p, std::vector<uint16_t>& 
       it->second = std::min(static_cast<uint16_t>(o.duration), it->second);
     });
   }
-  std::vector<std::vector<uint32_t>> bucket(B2R_MAX_TRAVEL_TIME_MIN + 1);
-  size_t cur = 0, size = 0;
+  constexpr uint32_t kBuckets = B2R_MAX_TRAVEL_TIME_MIN + 1;
+  thread_local std::vector<std::vector<uint32_t>> bucket(kBuckets);
+  size_t cur = kBuckets, size = 0, hi = 0;
+  auto const push = [&](uint32_t l, uint32_t d) {
+    bucket[d].push_back(l);
+    cur = std::min<size_t>(cur, d);
+    hi = std::max<size_t>(hi, d);
+    ++size;
+  };
   for (auto const& [l, dd] : seed) {
     v.metas(p.dest_mode, l, [&](uint32_t m) {
-      bucket[dd].push_back(m);
-      cur = std::min<size_t>(cur, dd);
-      ++size;
+      push(m, dd);
       dist[m] = std::min(dd, dist[m]);
     });
   }
@@ -179,11 +186,10 @@ void lower_bounds(view const& v, prepped_query const& p, std::vector<uint16_t>& 
     if (dist[l] < cur) continue;
     for (auto e = gi[l]; e != gi[l + 1]; ++e) {
       auto const tgt = B2R_FP_TARGET(gd[e]);
-      auto const nd = cur + B2R_FP_DURATION(gd[e]);
-      if (nd < dist[tgt] && nd < bucket.size()) {
+      auto const nd = static_cast<uint32_t>(cur) + B2R_FP_DURATION(gd[e]);
+      if (nd < dist[tgt] && nd < kBuckets) {
         dist[tgt] = static_cast<uint16_t>(nd);
-        bucket[nd].push_back(tgt);
-        ++size;
+        push(tgt, nd);
       }
     }
   }

@@ -1,8 +1,11 @@
-// Device-side journey reconstruction: one thread per journey walks the
-// round times of its query backwards (src/routing/raptor/reconstruct.cc:
-// 22-877 for Vias = 0 and no real-time overlay) and then applies the
-// footpath optimisations of src/routing/raptor/optimize_footpaths.cc.
-// Legs are written to the journey's leg block in device memory.
+// Device-side journey reconstruction: one warp per journey walks the round
+// times of its query backwards (src/routing/raptor/reconstruct.cc:22-877 for
+// Vias = 0 and no real-time overlay) and then applies the footpath
+// optimisations of src/routing/raptor/optimize_footpaths.cc.  The search for
+// the transport that produced a label is split across the lanes (one
+// (route, stop position) candidate per lane); a ballot keeps the first
+// success in the reference's iteration order.  The sequential parts run
+// redundantly on all lanes; lane 0 owns the journey's leg block.
 #pragma once
 
 #include "engine.cuh"
@@ -20,9 +23,11 @@ struct recon_ctx {
   uint16_t base;
   bool ontrip;
   journey_rec* j;
-  b2r_leg* legs;       // kMaxLegs
+  b2r_leg* legs;       // kMaxLegs, written by lane 0
   int n_legs;
   bool failed;
+  uint32_t lane;
+  b2r_leg last;        // last pushed leg (all lanes)
 
   // ------------------------------------------------------------- access
   __device__ int rt_t(unsigned k, uint32_t l) const {  // delta_t of round_times[k][l]
@@ -128,7 +133,21 @@ struct recon_ctx {
       failed = true;
       return;
     }
-    legs[n_legs++] = l;
+    if (lane == 0) legs[n_legs] = l;
+    ++n_legs;
+    last = l;
+  }
+
+  __device__ static b2r_leg shfl_leg(b2r_leg const& l, int src) {
+    static_assert(sizeof(b2r_leg) % 4 == 0, "leg size");
+    constexpr int kW = sizeof(b2r_leg) / 4;
+    uint32_t w[kW];
+    memcpy(w, &l, sizeof(b2r_leg));
+#pragma unroll
+    for (int i = 0; i < kW; ++i) w[i] = __shfl_sync(kFull, w[i], src);
+    b2r_leg out;
+    memcpy(&out, w, sizeof(b2r_leg));
+    return out;
   }
 
   // reconstruct.cc:180-280 (single pass: no vias)
@@ -190,18 +209,27 @@ struct recon_ctx {
     return false;
   }
 
-  // reconstruct.cc:375-545
+  // reconstruct.cc:375-545: the (route, stop position) pairs of location l
+  // in the reference's order, 32 per step, first success wins
   __device__ bool get_transport(unsigned k, uint32_t l, int time, b2r_leg& out) const {
-    for (auto ri = T->loc_routes_idx[l]; ri != T->loc_routes_idx[l + 1]; ++ri) {
-      auto const r = T->loc_routes[ri];
-      auto const n = n_stops(r);
-      for (auto i = 0u; i != n; ++i) {
+    auto const b = T->lrs_idx[l], e = T->lrs_idx[l + 1];
+    for (auto base = b; base < e; base += 32u) {
+      auto const x = base + lane;
+      bool ok = false;
+      b2r_leg leg{};
+      if (x < e) {
+        auto const r = T->lrs_route[x];
+        auto const i = static_cast<uint32_t>(T->lrs_stop[x]);
         auto const w = stopw(r, i);
-        if (B2R_STOP_LOC(w) != l || (fwd && (i == 0u || !B2R_STOP_OUT(w))) ||
-            (!fwd && (i + 1u == n || !B2R_STOP_IN(w)))) {
-          continue;
+        auto const n = n_stops(r);
+        if (!((fwd && (i == 0u || !B2R_STOP_OUT(w))) || (!fwd && (i + 1u == n || !B2R_STOP_IN(w))))) {
+          ok = get_route_transport(k, time, r, i, leg);
         }
-        if (get_route_transport(k, time, r, i, out)) return true;
+      }
+      auto const m = __ballot_sync(kFull, ok);
+      if (m != 0u) {
+        out = shfl_leg(leg, __ffs(m) - 1);
+        return true;
       }
     }
     return false;
@@ -269,7 +297,7 @@ struct recon_ctx {
   // reconstruct.cc:30-160 (no vias)
   __device__ bool find_start_footpath(b2r_leg& out, bool& has) const {
     has = false;
-    auto const& back = legs[n_legs - 1];
+    auto const& back = last;
     auto const lsl = fwd ? back.from : back.to;
     auto const lst = fwd ? back.dep_time : back.arr_time;
     if (sl->start_mode != B2R_MATCH_INTERMODAL && is_journey_start(lsl) && beq(j->start_time, lst)) {
@@ -521,7 +549,7 @@ struct recon_ctx {
       if (!find_start_footpath(init, has)) failed = true;
       else if (has) push(init);
     }
-    if (failed) return;
+    if (failed || lane != 0) return;
     if (fwd) {
       for (auto a = 0, b = n_legs - 1; a < b; ++a, --b) {
         auto const x = legs[a];
