@@ -260,7 +260,10 @@ typedef struct b2r_engine_config {
   uint64_t hbm_budget;      /* bytes of raptor state the pool may hold */
   uint32_t max_journeys;    /* per-query pareto set capacity (default 128) */
   uint32_t host_threads;    /* host prep threads (0 = hardware) */
-  uint32_t use_lower_bounds;/* 1 = dijkstra lower bounds (reference default) */
+  uint32_t use_lower_bounds;/* Dijkstra lower bounds for target pruning
+                               (raptor.h:33 kUseLowerBounds): 0 = off (lb = 0,
+                               like nigiri's GPU raptor), 1 = on the host
+                               (default), 2 = on the device */
   uint32_t use_graphs;      /* 1 = capture the super-step in a CUDA graph */
   uint32_t route_block;     /* launch shape: warps per CTA in the route scan */
   uint32_t max_starts;      /* start labels per query (default 4096) */
@@ -320,6 +323,9 @@ typedef struct b2r_batch_stats {
   uint64_t et_days;           /* service days examined by trip searches */
   uint64_t label_writes;      /* tmp label improvements */
   uint64_t route_scan_bytes;  /* algorithmic bytes of the route scans */
+  double lb_ms;               /* wall time of device lower-bound solves */
+  uint64_t lb_iterations;     /* solver iterations (8 per chunk) */
+  uint64_t lb_relaxations;    /* improving edge relaxations */
 } b2r_batch_stats;
 int b2r_last_batch_stats(const b2r_engine* e, b2r_batch_stats* s);
 

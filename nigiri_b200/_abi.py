@@ -113,7 +113,8 @@ class BatchStats(C.Structure):
                 ("route_scan_launches", C.c_uint64), ("route_scan_ms", C.c_double),
                 ("route_stop_visits", C.c_uint64), ("et_events", C.c_uint64),
                 ("et_days", C.c_uint64), ("label_writes", C.c_uint64),
-                ("route_scan_bytes", C.c_uint64)]
+                ("route_scan_bytes", C.c_uint64), ("lb_ms", C.c_double),
+                ("lb_iterations", C.c_uint64), ("lb_relaxations", C.c_uint64)]
 
 
 class TtBase(C.Structure):

@@ -111,6 +111,7 @@ struct b2r_engine {
   b2r::dev::state st{};
   cudaStream_t stream{nullptr};
   cudaGraphExec_t graph{nullptr};
+  cudaGraphExec_t lb_graph{nullptr};  // 4 x 2 Bellman-Ford iterations
   int sms{132};
   std::vector<void*> allocs;
 
@@ -123,6 +124,9 @@ struct b2r_engine {
   };
   summary_t* d_summary{nullptr};
   summary_t* h_summary{nullptr};  // pinned
+  uint32_t* h_lbcount{nullptr};   // pinned
+  uint64_t lb_chunks{0};
+  double lb_ms{0};
   // admission staging (pinned) and device mirror
   uint8_t* h_adm{nullptr};
   uint8_t* d_adm{nullptr};
@@ -169,8 +173,10 @@ struct adm_hdr {
   uint32_t slot;
   uint32_t n_starts, n_dest, n_off;
   uint32_t clear_rt;
-  uint32_t lb_mode;  // 0 zeros, 1 column in payload
-  uint64_t off_slot, off_starts, off_dest, off_off, off_lb;
+  uint32_t lb_mode;  // 0 zeros, 1 column in payload, 2 computed on the device
+  uint32_t n_seeds;
+  uint32_t pad;
+  uint64_t off_slot, off_starts, off_dest, off_off, off_lb, off_seeds;
 };
 
 __global__ void k_admit(dev::state st, adm_hdr const* hdr, uint8_t const* payload, uint32_t n_adm,
@@ -196,17 +202,30 @@ __global__ void k_admit(dev::state st, adm_hdr const* hdr, uint8_t const* payloa
   auto const* offs = reinterpret_cast<b2r_offset const*>(payload + h.off_off);
   for (auto i = threadIdx.x; i < h.n_off; i += blockDim.x) st.off_pool[s * max_off + i] = offs[i];
   auto const* lbc = reinterpret_cast<uint16_t const*>(payload + h.off_lb);
-  for (auto l = threadIdx.x; l < n_loc; l += blockDim.x) {
-    st.lb[static_cast<size_t>(l) * st.S + s] = h.lb_mode ? lbc[l] : uint16_t{0};
+  if (h.lb_mode != 2) {
+    for (auto l = threadIdx.x; l < n_loc; l += blockDim.x) {
+      st.lb[static_cast<size_t>(l) * st.S + s] = h.lb_mode ? lbc[l] : uint16_t{0};
+    }
   }
-  if (h.clear_rt) {
+  if (h.clear_rt) {  // query generations wrapped: no stale tag may survive
     for (size_t i = threadIdx.x; i < static_cast<size_t>(dev::kK) * n_loc; i += blockDim.x) {
       st.rt[i * st.S + s] = 0xFFFFFFFFu;
     }
+    for (size_t i = threadIdx.x; i < n_loc; i += blockDim.x) st.dist[i * st.S + s] = 0xFFFFFFFFu;
   }
   auto const words = (st.max_j + 31u) / 32u;
   for (auto i = threadIdx.x; i < words; i += blockDim.x) st.blocks_used[s * words + i] = 0u;
   __syncthreads();
+  if (h.lb_mode == 2) {  // Dijkstra seeds into the device frontier
+    auto const qtag = dev::tagcode(st.slots[s].gen_query);
+    auto const* seeds = reinterpret_cast<uint32_t const*>(payload + h.off_seeds);
+    for (auto i = threadIdx.x; i < h.n_seeds; i += blockDim.x) {
+      auto const l = seeds[2 * i];
+      atomicMin(&st.dist[static_cast<size_t>(l) * st.S + s], dev::enc(qtag, static_cast<int>(seeds[2 * i + 1])));
+      dev::mark(st, st.F[0], st.flist[0], dev::C_F0, l * st.G + (s >> 5), 1u << (s & 31));
+    }
+    if (threadIdx.x == 0) atomicOr(&st.lb_mask[s >> 5], 1u << (s & 31));
+  }
   // is-destination bits of station-to-station queries
   auto const& sl = st.slots[s];
   if (!sl.intermodal_dest && !sl.one_to_all) {
@@ -294,10 +313,12 @@ __global__ void k_set_journeys(dev::state st, uint32_t s, dev::journey_rec const
 b2r_engine::~b2r_engine() {
   for (auto ev : prof_ev) cudaEventDestroy(ev);
   if (graph != nullptr) cudaGraphExecDestroy(graph);
+  if (lb_graph != nullptr) cudaGraphExecDestroy(lb_graph);
   if (stream != nullptr) cudaStreamDestroy(stream);
   if (ev0 != nullptr) cudaEventDestroy(ev0);
   if (ev1 != nullptr) cudaEventDestroy(ev1);
   if (h_summary != nullptr) cudaFreeHost(h_summary);
+  if (h_lbcount != nullptr) cudaFreeHost(h_lbcount);
   if (h_adm != nullptr) cudaFreeHost(h_adm);
   if (h_exp != nullptr) cudaFreeHost(h_exp);
   for (auto* p : allocs) cudaFree(p);
@@ -403,9 +424,50 @@ slot_t make_slot(b2r_engine& e, uint32_t s, prepped_query const& p, bool& clear_
 
 // Packs the admissions into pinned memory, copies them in one transfer and
 // distributes them with one kernel.
+void enqueue_lb_chunk(b2r_engine& e, cudaStream_t s) {
+  for (auto it = 0; it != 4; ++it) {
+    for (uint32_t p = 0; p != 2; ++p) {
+      dev::k_lb_relax<<<e.sms * 8, 256, 0, s>>>(e.st, p);
+      dev::k_lb_clear<<<e.sms * 4, 256, 0, s>>>(e.st, p);
+      dev::k_lb_reset<<<1, 32, 0, s>>>(e.st, p);
+    }
+  }
+}
+
+// Runs the device Dijkstra of every query admitted in this wave to
+// completion, then writes their lower-bound columns.
+void solve_lower_bounds(b2r_engine& e, cudaStream_t s) {
+  auto const t0 = std::chrono::steady_clock::now();
+  uint32_t pending = 1;
+  uint64_t chunks = 0;
+  while (pending != 0) {
+    if (e.lb_graph != nullptr) {
+      B2R_CUDA(cudaGraphLaunch(e.lb_graph, s));
+    } else {
+      enqueue_lb_chunk(e, s);
+    }
+    ++chunks;
+    B2R_CUDA(cudaMemcpyAsync(e.h_lbcount, e.st.counters + dev::C_F0, sizeof(uint32_t),
+                             cudaMemcpyDeviceToHost, s));
+    B2R_CUDA(cudaStreamSynchronize(s));
+    pending = *e.h_lbcount;
+    if (chunks > 100000) throw std::runtime_error("lower-bound solver did not converge");
+  }
+  e.lb_chunks += chunks;
+  if (e.tt->d.n_with_children != 0) {
+    dev::k_lb_children<<<(e.S + 127) / 128, 128, 0, s>>>(e.st);
+  }
+  dev::k_lb_finish<<<e.sms * 16, 256, 0, s>>>(e.st);
+  B2R_CUDA(cudaMemsetAsync(e.st.lb_mask, 0, e.G * sizeof(uint32_t), s));
+  B2R_CUDA(cudaGetLastError());
+  B2R_CUDA(cudaStreamSynchronize(s));
+  e.lb_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
 void admit(b2r_engine& e, std::vector<std::pair<uint32_t, prepped_query const*>> const& adm,
            cudaStream_t s) {
   if (adm.empty()) return;
+  bool any_device_lb = false;
   size_t need = adm.size() * sizeof(adm_hdr) + 256;
   for (auto const& [slot, p] : adm) need += admission_bytes(e, *p) + 64;
   if (need > e.adm_cap) {
@@ -455,14 +517,23 @@ void admit(b2r_engine& e, std::vector<std::pair<uint32_t, prepped_query const*>>
     offs.insert(offs.end(), p.dest_offsets.begin(), p.dest_offsets.end());
     h.n_off = static_cast<uint32_t>(offs.size());
     h.off_off = put(offs.data(), offs.size() * sizeof(b2r_offset));
-    h.lb_mode = p.lb.empty() ? 0 : 1;
+    h.lb_mode = !p.lb.empty() ? 1 : (e.cfg.use_lower_bounds == 2 && !p.one_to_all ? 2 : 0);
     h.off_lb = put(p.lb.data(), p.lb.size() * sizeof(uint16_t));
+    std::vector<uint32_t> seeds;
+    for (auto const& [l, d] : p.lb_seeds) {
+      seeds.push_back(l);
+      seeds.push_back(d);
+    }
+    h.n_seeds = static_cast<uint32_t>(p.lb_seeds.size());
+    h.off_seeds = put(seeds.data(), seeds.size() * sizeof(uint32_t));
+    any_device_lb = any_device_lb || h.lb_mode == 2;
   }
   B2R_CUDA(cudaMemcpyAsync(e.d_adm, e.h_adm, off, cudaMemcpyHostToDevice, s));
   k_admit<<<static_cast<unsigned>(adm.size()), 256, 0, s>>>(
       e.st, reinterpret_cast<adm_hdr const*>(e.d_adm), e.d_adm, static_cast<uint32_t>(adm.size()),
       e.max_starts, e.max_dest, e.max_off);
   B2R_CUDA(cudaGetLastError());
+  if (any_device_lb) solve_lower_bounds(e, s);
 }
 
 void retire(b2r_engine& e, std::vector<uint32_t> const& slots, cudaStream_t s) {
@@ -843,11 +914,10 @@ struct preparer {
     auto const hw = std::max(1U, std::thread::hardware_concurrency());
     auto const n_threads = std::max(1U, std::min<uint32_t>(
         e.cfg.host_threads != 0 ? e.cfg.host_threads : (hw > 1 ? hw - 1 : 1), n));
-    auto const lb_host = e.cfg.use_lower_bounds != 0;
-    auto work = [&e, qs, n, &runs, lb_host, this]() {
+    auto const lb_mode = static_cast<int>(e.cfg.use_lower_bounds);
+    auto work = [&e, qs, n, &runs, lb_mode, this]() {
       for (auto i = next++; i < n; i = next++) {
-        prepare(e.tt->view, qs[i], lb_host, runs[i].p);
-        if (!lb_host && !runs[i].p.one_to_all) runs[i].p.lb.clear();
+        prepare(e.tt->view, qs[i], lb_mode, runs[i].p);
         runs[i].ready.store(true, std::memory_order_release);
       }
     };
@@ -1003,6 +1073,20 @@ int b2r_timetable_upload(const b2r_timetable_desc* d, int device, b2r_timetable*
       dd.loc_routes_idx = up(d->location_routes_index, nl + 1);
       dd.loc_routes = up(d->location_routes, d->location_routes_index[nl]);
       dd.route_sorted = up(sorted.data(), nr);
+      dd.lbg_fwd_idx = up(d->lb_fwd_index, nl + 1);
+      dd.lbg_fwd = up(d->lb_fwd, d->lb_fwd_index[nl]);
+      dd.lbg_bwd_idx = up(d->lb_bwd_index, nl + 1);
+      dd.lbg_bwd = up(d->lb_bwd, d->lb_bwd_index[nl]);
+      {
+        std::vector<uint32_t> wc;
+        if (d->children_index != nullptr) {
+          for (auto l = 0U; l != nl; ++l) {
+            if (d->children_index[l + 1] != d->children_index[l]) wc.push_back(l);
+          }
+        }
+        dd.with_children = up(wc.data(), wc.size());
+        dd.n_with_children = static_cast<uint32_t>(wc.size());
+      }
       {  // location -> (route, stop position) pairs (reconstruct.cc:496-515 order)
         std::vector<uint32_t> idx(nl + 1, 0U), rr;
         std::vector<uint16_t> ss;
@@ -1055,7 +1139,7 @@ int b2r_engine_create(b2r_timetable* tt, const b2r_engine_config* cfg_in, b2r_en
       e->max_dest = 512U;
       e->max_off = 128U;
       auto const nl = tt->d.n_loc;
-      e->bytes_per_slot = static_cast<uint64_t>(nl) * (b2r::dev::kK * 4 + 4 + 4 + 2) +
+      e->bytes_per_slot = static_cast<uint64_t>(nl) * (b2r::dev::kK * 4 + 4 + 4 + 2 + 4) +
                           static_cast<uint64_t>(e->max_j) *
                               (sizeof(b2r::dev::journey_rec) + b2r::dev::kMaxLegs * sizeof(b2r_leg)) +
                           e->max_starts * sizeof(b2r::dev::start_rec) +
@@ -1112,6 +1196,16 @@ int b2r_engine_create(b2r_timetable* tt, const b2r_engine_config* cfg_in, b2r_en
       al(st.status_word, 4);
       al(e->d_summary, S);
       al(st.prof, 8);
+      al(st.dist, static_cast<size_t>(nl) * S);
+      al(st.F[0], static_cast<size_t>(nl) * G);
+      al(st.F[1], static_cast<size_t>(nl) * G);
+      al(st.flist[0], static_cast<size_t>(nl) * G);
+      al(st.flist[1], static_cast<size_t>(nl) * G);
+      al(st.lb_mask, G);
+      B2R_CUDA(cudaMemset(st.dist, 0xFF, static_cast<size_t>(nl) * S * 4));
+      B2R_CUDA(cudaMemset(st.F[0], 0, static_cast<size_t>(nl) * G * 4));
+      B2R_CUDA(cudaMemset(st.F[1], 0, static_cast<size_t>(nl) * G * 4));
+      B2R_CUDA(cudaMemset(st.lb_mask, 0, G * 4));
       st.profile = cfg.profile ? 1u : 0u;
       B2R_CUDA(cudaMemset(st.prof, 0, 8 * sizeof(unsigned long long)));
       al(e->d_exp_list, S);
@@ -1127,10 +1221,19 @@ int b2r_engine_create(b2r_timetable* tt, const b2r_engine_config* cfg_in, b2r_en
       e->gen_query.assign(S, 0);
       e->slot_query.assign(S, -1);
       B2R_CUDA(cudaMallocHost(&e->h_summary, S * sizeof(b2r_engine::summary_t)));
+      B2R_CUDA(cudaMallocHost(&e->h_lbcount, sizeof(uint32_t)));
       B2R_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
       B2R_CUDA(cudaEventCreate(&e->ev0));
       B2R_CUDA(cudaEventCreate(&e->ev1));
-      if (e->cfg.use_graphs) b2r::capture_graph(*e);
+      if (e->cfg.use_graphs) {
+        b2r::capture_graph(*e);
+        cudaGraph_t g = nullptr;
+        B2R_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+        b2r::enqueue_lb_chunk(*e, e->stream);
+        B2R_CUDA(cudaStreamEndCapture(e->stream, &g));
+        B2R_CUDA(cudaGraphInstantiate(&e->lb_graph, g, 0));
+        cudaGraphDestroy(g);
+      }
       B2R_CUDA(cudaDeviceSynchronize());
       *out = e.release();
       return B2R_OK;
@@ -1164,6 +1267,8 @@ int b2r_search_batch(b2r_engine* e, const b2r_query* qs, uint32_t n, b2r_result*
       prep.start(*e, qs, n, runs, false);
       b2r::batch_runner br{*e, runs, e->cfg.use_graphs != 0 && e->graph != nullptr};
       e->prof_used = 0;
+      e->lb_ms = 0;
+      e->lb_chunks = 0;
       if (e->cfg.profile) B2R_CUDA(cudaMemsetAsync(e->st.prof, 0, 8 * sizeof(unsigned long long), e->stream));
       br.run(e->cfg.steps_per_sync != 0 ? e->cfg.steps_per_sync : 4U);
       prep.join();
@@ -1174,6 +1279,8 @@ int b2r_search_batch(b2r_engine* e, const b2r_query* qs, uint32_t n, b2r_result*
       e->last.host_prep_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();  // wall of the call
       e->last.kernel_launches = br.launches;
       e->last.super_steps = br.steps;
+      e->last.lb_ms = e->lb_ms;
+      e->last.lb_iterations = e->lb_chunks * 8;
       if (e->cfg.profile) {
         double scan_ms = 0;
         for (size_t i = 0; i + 1 < e->prof_used; i += 2) {
@@ -1194,6 +1301,7 @@ int b2r_search_batch(b2r_engine* e, const b2r_query* qs, uint32_t n, b2r_result*
         // (2 B); per trip search 2 B per examined event and 8 B per examined
         // service day; 2 B per label write
         e->last.route_scan_bytes = c[0] * 8ull + c[1] * 2ull + c[2] * 8ull + c[3] * 2ull;
+        e->last.lb_relaxations = c[4];
       }
       uint32_t err = 0;
       B2R_CUDA(cudaMemcpy(&err, e->st.counters + b2r::dev::C_ERR, 4, cudaMemcpyDeviceToHost));

@@ -64,6 +64,13 @@ struct dtt {
   uint32_t const* loc_routes_idx;
   uint32_t const* loc_routes;
   uint8_t const* route_sorted;  // 1: every event column is ordered by mam
+  // lower-bound graphs (build_lb_graph.h), packed footpath words
+  uint32_t const* lbg_fwd_idx;
+  uint32_t const* lbg_fwd;
+  uint32_t const* lbg_bwd_idx;
+  uint32_t const* lbg_bwd;
+  uint32_t const* with_children;  // locations that have children, ascending
+  uint32_t n_with_children;
   // location -> (route, stop position) pairs in the order reconstruction
   // visits them: routes of location_routes_, then stop positions ascending
   uint32_t const* lrs_idx;
@@ -190,6 +197,12 @@ struct state {
   uint32_t* status_word;  // [0] device error flags
   unsigned long long* prof;  // route-scan work counters (profiling engines)
   uint32_t profile;
+  // lower bounds computed on the device: tagged distances, frontier bits
+  // and lists (double-buffered), slots waiting for their bounds
+  uint32_t* dist;        // [n_loc][S]
+  uint32_t* F[2];        // [n_loc][G]
+  uint32_t* flist[2];
+  uint32_t* lb_mask;     // [G]
 };
 
 // ------------------------------------------------------------- helpers

@@ -10,7 +10,7 @@
 
 namespace b2r::dev {
 
-enum : uint32_t { C_X = 0, C_Y = 1, C_R = 2, C_RECON = 3, C_ERR = 4 };
+enum : uint32_t { C_X = 0, C_Y = 1, C_R = 2, C_RECON = 3, C_ERR = 4, C_F0 = 5, C_F1 = 6 };
 
 __device__ __forceinline__ size_t li(state const& st, uint32_t l, uint32_t s) {
   return static_cast<size_t>(l) * st.S + s;
@@ -780,6 +780,99 @@ __global__ void k_next(state st) {
   sl.k = 1;
   sl.state = S_RUN;
   ++sl.n_groups_run;
+}
+
+// ------------------------------------------------------- lower bounds
+// Dijkstra from the destinations over the lower-bound graph (dijkstra.cc:
+// 18-67, dial.h), computed for all newly admitted queries at once as a
+// frontier-driven Bellman-Ford: distances are shortest-path lengths capped
+// below kMaxTravelTime + 1 = 7201 (the dial's bucket count), which no
+// processing order changes (all weights are non-negative).
+constexpr uint32_t kLbBuckets = B2R_MAX_TRAVEL_TIME_MIN + 1;
+
+__global__ void k_lb_relax(state st, uint32_t p) {
+  auto const lane = threadIdx.x & 31u;
+  auto const warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  auto const n_warps = (gridDim.x * blockDim.x) >> 5;
+  auto const n = st.counters[C_F0 + p];
+  auto const& T = st.tt;
+  for (auto w = warp; w < n; w += n_warps) {
+    auto const e = st.flist[p][w];
+    auto const g = e % st.G, l = e / st.G;
+    auto const m = st.F[p][e];
+    auto const s = g * 32u + lane;
+    auto const& sl = st.slots[s];
+    bool act = (m >> lane) & 1u;
+    auto const qtag = tagcode(sl.gen_query);
+    int d = kKeyInv;
+    if (act) {
+      d = dec(st.dist[li(st, l, s)], qtag);
+      act = d != kKeyInv;
+    }
+    auto const fwd = sl.fwd != 0;
+    auto const* gi = fwd ? T.lbg_fwd_idx : T.lbg_bwd_idx;
+    auto const* gd = fwd ? T.lbg_fwd : T.lbg_bwd;
+    auto const b = act ? gi[l] : 0u;
+    auto const cnt = act ? gi[l + 1] - b : 0u;
+    auto n_max = cnt;
+    for (auto o = 16; o > 0; o >>= 1) n_max = max(n_max, __shfl_xor_sync(kFull, n_max, o));
+    for (auto j = 0u; j != n_max; ++j) {
+      bool improved = false;
+      uint32_t tgt = 0;
+      if (j < cnt) {
+        auto const edge = gd[b + j];
+        tgt = B2R_FP_TARGET(edge);
+        auto const nd = static_cast<uint32_t>(d) + B2R_FP_DURATION(edge);
+        if (nd < kLbBuckets) {
+          auto const word = enc(qtag, static_cast<int>(nd));
+          auto* dp = &st.dist[li(st, tgt, s)];
+          if (word < *dp) improved = word < atomicMin(dp, word);
+          if (improved && st.profile) atomicAdd(&st.prof[4], 1ull);
+        }
+      }
+      mark_warp(st, st.F[1 - p], st.flist[1 - p], C_F0 + (1 - p), improved, tgt * st.G + g, lane);
+    }
+  }
+}
+
+__global__ void k_lb_clear(state st, uint32_t p) {
+  auto const n = st.counters[C_F0 + p];
+  for (auto i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    st.F[p][st.flist[p][i]] = 0u;
+  }
+}
+
+__global__ void k_lb_reset(state st, uint32_t p) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) st.counters[C_F0 + p] = 0u;
+}
+
+// children inherit their parent's bound (dijkstra.cc:60-65), in location
+// order per query
+__global__ void k_lb_children(state st) {
+  auto const s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= st.S || !((st.lb_mask[s >> 5] >> (s & 31)) & 1u)) return;
+  auto const qtag = tagcode(st.slots[s].gen_query);
+  auto const& T = st.tt;
+  for (auto x = 0u; x != T.n_with_children; ++x) {
+    auto const i = T.with_children[x];
+    auto const lbw = st.dist[li(st, i, s)];
+    for (auto c = T.children_idx[i]; c != T.children_idx[i + 1]; ++c) {
+      auto* cw = &st.dist[li(st, T.children[c], s)];
+      if (dec(lbw, qtag) < dec(*cw, qtag)) *cw = lbw;
+    }
+  }
+}
+
+// tagged distances -> the u16 lower-bound column (unreachable = 0xFFFF)
+__global__ void k_lb_finish(state st) {
+  auto const n = static_cast<size_t>(st.tt.n_loc) * st.S;
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    auto const s = static_cast<uint32_t>(i % st.S);
+    if (!((st.lb_mask[s >> 5] >> (s & 31)) & 1u)) continue;
+    auto const d = dec(st.dist[i], tagcode(st.slots[s].gen_query));
+    st.lb[i] = d == kKeyInv ? uint16_t{0xFFFFu} : static_cast<uint16_t>(d);
+  }
 }
 
 }  // namespace b2r::dev

@@ -149,6 +149,25 @@ int16_t fastest_direct(view const& v, b2r_query const& q, std::vector<b2r_offset
 // over distances 0..kMaxTravelTime (dial.h) whose buckets are reused across
 // queries of the same thread.  Shortest distances do not depend on the pop
 // order inside a bucket.
+// Dijkstra seeds: per root location the minimum offset, then every meta of
+// the root with that distance (dijkstra.cc:26-48).
+void lb_seeds(view const& v, prepped_query const& p,
+              std::vector<std::pair<uint32_t, uint16_t>>& out) {
+  std::map<uint32_t, uint16_t> seed;
+  for (auto const& o : p.dest_offsets) {
+    v.metas(p.dest_mode, o.target, [&](uint32_t x) {
+      auto const r = v.root(x);
+      auto it = seed.find(r);
+      if (it == seed.end()) it = seed.emplace(r, kUnreach).first;
+      it->second = std::min(static_cast<uint16_t>(o.duration), it->second);
+    });
+  }
+  out.clear();
+  for (auto const& [l, dd] : seed) {
+    v.metas(p.dest_mode, l, [&](uint32_t m) { out.emplace_back(m, dd); });
+  }
+}
+
 void lower_bounds(view const& v, prepped_query const& p, std::vector<uint16_t>& dist) {
   auto const n = v.d.n_locations;
   dist.assign(n, kUnreach);
@@ -311,7 +330,7 @@ void sort_starts(bool fwd, std::vector<start_label>& s) {  // search.h:408-410
 
 }  // namespace
 
-void prepare(host_view const& hv, b2r_query const& q, bool lb_host, prepped_query& p) {
+void prepare(host_view const& hv, b2r_query const& q, int lb_mode, prepped_query& p) {
   view const v{hv.d};
   p = prepped_query{};
   p.fwd = q.direction == B2R_FORWARD;
@@ -396,7 +415,8 @@ void prepare(host_view const& hv, b2r_query const& q, bool lb_host, prepped_quer
     std::sort(p.dest_locs.begin(), p.dest_locs.end());
     p.dest_locs.erase(std::unique(p.dest_locs.begin(), p.dest_locs.end()), p.dest_locs.end());
   }
-  if (lb_host) lower_bounds(v, p, p.lb);
+  if (lb_mode == 1) lower_bounds(v, p, p.lb);
+  if (lb_mode == 2) lb_seeds(v, p, p.lb_seeds);
   auto const mid = static_cast<int64_t>(p.iv_from) + (p.iv_to - p.iv_from) / 2;
   p.base = static_cast<uint16_t>(round_to_days(mid) - hv.internal_from_days());
   p.base_days = hv.internal_from_days() + p.base;

@@ -53,11 +53,14 @@ struct prepped_query {
   std::vector<uint32_t> dest_locs;                      // ascending
   std::vector<std::pair<uint32_t, uint16_t>> dest_dist; // intermodal, ascending
   std::vector<uint16_t> lb;                             // [n_locations]
+  // Dijkstra seeds (location, distance) for lower bounds computed on the
+  // device (dijkstra.cc:26-48)
+  std::vector<std::pair<uint32_t, uint16_t>> lb_seeds;
 };
 
-// Computes everything above; `lb_host` = compute the Dijkstra lower bounds
-// on the host (otherwise lb is left empty and the device computes it).
-void prepare(host_view const& tt, b2r_query const& q, bool lb_host,
+// Computes everything above.  lb_mode: 0 = no lower bounds (lb = 0),
+// 1 = Dijkstra on the host (lb filled), 2 = on the device (lb_seeds filled).
+void prepare(host_view const& tt, b2r_query const& q, int lb_mode,
              prepped_query& out);
 
 // Start labels of [from, to) for an interval extension (search.h:294-312).

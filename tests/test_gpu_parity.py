@@ -148,3 +148,16 @@ def test_one_to_all_rows_match_oracle(workload, c1, c2):
         orows, _, base_day = o.state()
         assert r.base_day == base_day
         assert np.array_equal(rows, orows[: r.n_rows]), i
+
+
+@pytest.mark.parametrize("lb_mode", ["device", False])
+def test_lower_bound_modes_give_identical_journeys(c2, lb_mode):
+    """Lower bounds only prune: journeys are the same with bounds computed
+    on the device, on the host, or without bounds (nigiri's GPU raptor runs
+    without them, gpu/raptor.h:60)."""
+    h, dtt, eng = c2
+    other = R.Engine(dtt, max_slots=128, use_lower_bounds=lb_mode)
+    qs = QuerySet(h, 2, 64, seed=31)
+    a, _ = run_batch(eng, qs.arr, qs.n)
+    b, _ = run_batch(other, qs.arr, qs.n)
+    assert a == b
