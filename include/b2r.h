@@ -295,6 +295,47 @@ int b2r_search_batch(b2r_engine* e, const b2r_query* qs, uint32_t n,
  * src/routing/gpu/raptor.cu:894-990).  Same results as b2r_search_batch. */
 int b2r_search_plain(b2r_engine* e, const b2r_query* q, b2r_result* out);
 
+/* One-to-all search of ONE query that allocates nothing.  It has no
+ * counterpart in the reference: nigiri's one_to_all (one_to_all.cc:52-92)
+ * allocates its raptor_state per call.
+ *
+ * For callers that cannot allocate device memory on the query path:
+ * request handlers of a serving process whose device memory is owned by
+ * another allocator (a framework's caching allocator, or a fixed pool that
+ * reserves the HBM), and latency-critical paths that must not call
+ * cudaMalloc / cudaFree because cudaFree synchronises the whole device and
+ * stalls every other stream of the process (the batched engine included).
+ * The call uses no engine, calls no cudaMalloc, cudaFree or other allocating
+ * routine, and keeps its working state in one fixed device array of
+ * B2R_NOALLOC_SCRATCH_BYTES that lives in the library.
+ *
+ * - q->kind must be B2R_ONE_TO_ALL.  The timetable may have at most
+ *   B2R_NOALLOC_MAX_LOCATIONS locations and B2R_NOALLOC_MAX_ROUTES routes,
+ *   the query at most B2R_NOALLOC_MAX_OFFSETS start offsets; larger inputs
+ *   are rejected with B2R_ERR_CAPACITY and a message (b2r_last_error).
+ * - round_times (host memory, capacity elements) receives n_rows rows of
+ *   n_locations int16 deltas relative to *base_day, exactly the rows
+ *   b2r_search_batch returns for the same query (raptor_state::
+ *   round_times_).  n_rows = min(max_transfers, B2R_MAX_TRANSFERS) + 2.
+ * - stream: a cudaStream_t on tt's device, or NULL for the default stream.
+ *   The call returns when the rows are in round_times.
+ * - Set-up: the first call on a device, with that device current, loads the
+ *   library's device module (the driver reserves the scratch array then)
+ *   and looks up the array's address; later calls reuse it.  Make the first
+ *   call on each device before any stream capture.
+ * - Every call on a device shares the one scratch array: calls that overlap
+ *   on the GPU (from two streams or two host threads) race and corrupt each
+ *   other's results.  Issue them one at a time per device.
+ * - A rejected call records its error message for b2r_last_error on the
+ *   host heap; a call that succeeds touches no allocator. */
+#define B2R_NOALLOC_MAX_LOCATIONS 65536u
+#define B2R_NOALLOC_MAX_ROUTES 65536u
+#define B2R_NOALLOC_MAX_OFFSETS 64u
+#define B2R_NOALLOC_SCRATCH_BYTES (8388608u + 256u) /* 8 MiB + counters */
+int b2r_one_to_all_noalloc(const b2r_timetable* tt, const b2r_query* q,
+                           int16_t* round_times, uint64_t capacity,
+                           uint32_t* n_rows, int32_t* base_day, void* stream);
+
 /* Serving: asynchronous submission.  Queries are admitted into free slots at
  * super-step boundaries by a driver thread; results are fetched by ticket. */
 int b2r_serve_start(b2r_engine* e);

@@ -12,8 +12,16 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libb2r.so")
 
 B2R_OK = 0
+B2R_ERR_INVALID_ARGUMENT = -1
+B2R_ERR_CAPACITY = -4
 B2R_ERR_NOT_READY = -5
 B2R_K = 16
+B2R_MAX_TRANSFERS = 14
+# limits of b2r_one_to_all_noalloc's fixed scratch array
+B2R_NOALLOC_MAX_LOCATIONS = 65536
+B2R_NOALLOC_MAX_ROUTES = 65536
+B2R_NOALLOC_MAX_OFFSETS = 64
+B2R_NOALLOC_SCRATCH_BYTES = 8388608 + 256
 B2R_FORWARD, B2R_BACKWARD = 0, 1
 B2R_MATCH_EXACT, B2R_MATCH_ONLY_CHILDREN, B2R_MATCH_EQUIVALENT, B2R_MATCH_INTERMODAL = 0, 1, 2, 3
 B2R_ONE_TO_ONE, B2R_ONE_TO_ALL = 0, 1
@@ -141,6 +149,7 @@ EXPORTS = [
     "b2r_tt_generate", "b2r_tt_build", "b2r_tt_save", "b2r_tt_load",
     "b2r_tt_desc", "b2r_tt_destroy", "b2r_queries_generate",
     "b2r_queries_count", "b2r_queries_get", "b2r_queries_destroy",
+    "b2r_one_to_all_noalloc",
 ]
 
 
@@ -176,6 +185,8 @@ def _declare(lib):
         "b2r_queries_count": (C.c_uint32, [vp]),
         "b2r_queries_get": (C.POINTER(Query), [vp, C.c_uint32]),
         "b2r_queries_destroy": (C.c_int, [vp]),
+        "b2r_one_to_all_noalloc": (C.c_int, [vp, C.POINTER(Query), C.POINTER(C.c_int16), C.c_uint64,
+                                             C.POINTER(C.c_uint32), C.POINTER(C.c_int32), vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -22,6 +22,7 @@
 #include "errors.h"
 #include "kernels.cuh"
 #include "prep.h"
+#include "timetable_image.h"
 
 namespace b2r {
 
@@ -63,29 +64,6 @@ int n_sms(int dev) {
 
 }  // namespace
 }  // namespace b2r
-
-// ===================================================================== image
-struct b2r_timetable {
-  int device{0};
-  b2r_timetable_desc host{};  // pointers are NOT retained (sizes only)
-  b2r::dev::dtt d{};
-  std::vector<void*> allocs;
-  uint64_t bytes{0};
-  // host copies needed by the query preparation
-  std::vector<uint8_t> transfer_time;
-  std::vector<uint32_t> parent, children_index, children, fp_out_index, fp_out, fp_in_index,
-      fp_in, route_stop_index, route_stops, route_transport_from, route_transport_to,
-      route_stop_time_from, transport_traffic_days, route_traffic_days, location_routes_index,
-      location_routes, lb_fwd_index, lb_fwd, lb_bwd_index, lb_bwd, transport_route;
-  std::vector<uint8_t> location_type;
-  std::vector<uint16_t> route_stop_times;
-  std::vector<uint64_t> bitfields;
-  b2r::host_view view{};
-
-  ~b2r_timetable() {
-    for (auto* p : allocs) cudaFree(p);
-  }
-};
 
 namespace b2r {
 namespace {

@@ -9,11 +9,6 @@
 
 namespace b2r {
 
-namespace {
-
-constexpr uint16_t kUnreach = 0xFFFFu;
-constexpr int kMaxDur = 511;  // footpath::kMaxDuration
-
 // std::chrono::round<days> of a minute time point (ties to even)
 int32_t round_to_days(int64_t m) {
   int64_t const d0 = m >= 0 ? m / 1440 : -((-m + 1439) / 1440);
@@ -21,6 +16,11 @@ int32_t round_to_days(int64_t m) {
   if (r0 == r1) return static_cast<int32_t>((d0 & 1) ? d0 + 1 : d0);
   return static_cast<int32_t>(r0 < r1 ? d0 : d0 + 1);
 }
+
+namespace {
+
+constexpr uint16_t kUnreach = 0xFFFFu;
+constexpr int kMaxDur = 511;  // footpath::kMaxDuration
 
 template <typename T>
 T adjust(tts_norm const& s, T d) {  // transfer_time_settings.h:20-31

@@ -58,6 +58,9 @@ struct prepped_query {
   std::vector<std::pair<uint32_t, uint16_t>> lb_seeds;
 };
 
+// std::chrono::round<days> of a minute time point (ties to even).
+int32_t round_to_days(int64_t minutes);
+
 // Computes everything above.  lb_mode: 0 = no lower bounds (lb = 0),
 // 1 = Dijkstra on the host (lb filled), 2 = on the device (lb_seeds filled).
 void prepare(host_view const& tt, b2r_query const& q, int lb_mode,

@@ -59,3 +59,28 @@ def test_errors_without_gpu_are_status_codes():
     assert lib.b2r_engine_create(None, None, None) == -1
     assert b"null" in lib.b2r_last_error()
     assert lib.b2r_search_batch(None, None, 0, None) == -1
+
+
+def test_noalloc_limits_match_header_and_null_arguments_are_rejected():
+    code = r'''
+#include <stdio.h>
+#include "b2r.h"
+int main() {
+  printf("%u %u %u %u\n", B2R_NOALLOC_MAX_LOCATIONS, B2R_NOALLOC_MAX_ROUTES,
+         B2R_NOALLOC_MAX_OFFSETS, B2R_NOALLOC_SCRATCH_BYTES);
+  return 0;
+}
+'''
+    with tempfile.TemporaryDirectory() as d:
+        src = os.path.join(d, "t.c")
+        exe = os.path.join(d, "t")
+        open(src, "w").write(code)
+        subprocess.check_call(["gcc", "-I" + os.path.join(ROOT, "include"), src, "-o", exe])
+        got = [int(x) for x in subprocess.check_output([exe]).split()]
+    assert got == [A.B2R_NOALLOC_MAX_LOCATIONS, A.B2R_NOALLOC_MAX_ROUTES,
+                   A.B2R_NOALLOC_MAX_OFFSETS, A.B2R_NOALLOC_SCRATCH_BYTES]
+    lib = A.lib()
+    n_rows = C.c_uint32()
+    assert lib.b2r_one_to_all_noalloc(None, None, None, 0, C.byref(n_rows), None, None) == \
+        A.B2R_ERR_INVALID_ARGUMENT
+    assert b"null" in lib.b2r_last_error()
