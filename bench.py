@@ -44,6 +44,8 @@ def parse():
     p.add_argument("--no-extras", action="store_true", help="skip plain / roofline / CPU legs")
     p.add_argument("--ncu-case", action="store_true",
                    help="one batch without CUDA graphs (the case profiled with ncu)")
+    p.add_argument("--ncu-counters", action="store_true",
+                   help="with --ncu-case: count route-scan work (stop visits, events)")
     return p.parse_args()
 
 
@@ -188,7 +190,7 @@ def config_block(args, batch):
     return {"workload": "regional-40k-stops batched one-to-one (intermodal offset sets)",
             "timetable": "40,009 locations, 4,000 base routes, ~436k transports, 365 days",
             "global_batch": batch, "queries_per_step": batch, "max_transfers": 14,
-            "parallelism": f"replicas x{args.gpus}", "lower_bounds": "host dijkstra",
+            "parallelism": f"replicas x{args.gpus}", "lower_bounds": "all-pairs tables on the device (built once per timetable, before timing)",
             "l2": "round state of a step (>2.5 GB) exceeds L2; 512 MB written between steps"}
 
 
@@ -240,9 +242,10 @@ def gpu_arm(args, rank, world, local):
         walls.append(wall)
         devs.append(st.device_ms / 1e3)
         launches += st.kernel_launches
+        h2d += st.h2d_bytes
+        d2h += st.d2h_bytes
         for i in range(B):
             lats.append(out[i].latency_ms)
-            d2h += out[i].n_journeys * C.sizeof(A.Journey)
     ck = clocks.stop()
     tot_wall, tot_dev = sum(walls), sum(devs)
     if pg is not None:
@@ -252,8 +255,8 @@ def gpu_arm(args, rank, world, local):
     n_q = B * args.steps * world
     value = n_q / tot_dev
     e2e = n_q / tot_wall
-    # host->device bytes: query structs + offsets + lower-bound columns
-    h2d_step = B * (C.sizeof(A.Query) + 2 * h.desc.n_locations)
+    # bytes the engine copied between host and device (its own count)
+    h2d_step = h2d // max(1, args.steps)
 
     extras = {}
     if rank == 0 and not args.no_extras:
@@ -327,7 +330,9 @@ def extras_legs(args, h, dtt, qs, B, local):
         "unit": "GB/s", "frac": None, "traffic": traffic,
         "kernel": "k_route_scan", "launches": st.route_scan_launches,
         "avg_launch_ms": per_launch_s * 1e3, "algorithmic_bytes_per_launch": per_launch_bytes,
-        "route_stop_visits": st.route_stop_visits, "route_scan_share_of_device_time":
+        "route_stop_visits": st.route_stop_visits,
+        "lane_utilisation": st.route_stop_visits / max(1, 32 * st.route_warp_steps),
+        "route_scan_share_of_device_time":
             st.route_scan_ms / max(1e-9, st.device_ms),
     }
     del prof
@@ -350,7 +355,7 @@ def ncu_case(args, local):
     from nigiri_b200.timetable import HostTimetable, QuerySet
     h = HostTimetable.generate(WORKLOAD)
     dtt = R.Timetable(h.desc, device=local, owner=h)
-    eng = R.Engine(dtt, max_slots=args.batch, use_graphs=False)
+    eng = R.Engine(dtt, max_slots=args.batch, use_graphs=False, profile=args.ncu_counters)
     qs = QuerySet(h, WORKLOAD, args.batch, seed=1000 + WORKLOAD)
     out = (A.Result * args.batch)()
     rc = A.lib().b2r_search_batch(eng.handle, qs.arr, args.batch, out)
@@ -358,7 +363,11 @@ def ncu_case(args, local):
         raise RuntimeError(A.lib().b2r_last_error().decode())
     st = eng.stats()
     print(json.dumps({"ncu_case": True, "batch": args.batch, "super_steps": st.super_steps,
-                      "kernel_launches": st.kernel_launches, "device_ms": st.device_ms}))
+                      "kernel_launches": st.kernel_launches, "device_ms": st.device_ms,
+                      "route_scan_launches": st.route_scan_launches,
+                      "route_stop_visits": st.route_stop_visits,
+                      "route_warp_steps": st.route_warp_steps,
+                      "route_scan_bytes": st.route_scan_bytes}))
 
 
 def main():

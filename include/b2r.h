@@ -255,6 +255,10 @@ int b2r_timetable_destroy(b2r_timetable* tt);
 /* Device bytes held by the image. */
 uint64_t b2r_timetable_device_bytes(const b2r_timetable* tt);
 
+/* Largest all-pairs lower-bound tables an engine builds (both directions):
+ * 16 GiB, i.e. up to 65,536 locations. */
+#define B2R_LB_TABLE_MAX_BYTES (16ull << 30)
+
 typedef struct b2r_engine_config {
   uint32_t max_slots;       /* queries resident at once (multiple of 32) */
   uint64_t hbm_budget;      /* bytes of raptor state the pool may hold */
@@ -262,8 +266,13 @@ typedef struct b2r_engine_config {
   uint32_t host_threads;    /* host prep threads (0 = hardware) */
   uint32_t use_lower_bounds;/* Dijkstra lower bounds for target pruning
                                (raptor.h:33 kUseLowerBounds): 0 = off (lb = 0,
-                               like nigiri's GPU raptor), 1 = on the host
-                               (default), 2 = on the device */
+                               like nigiri's GPU raptor), 1 = on the host,
+                               2 = solved on the device, 3 = from all-pairs
+                               tables on the device (default; built once per
+                               timetable on the host threads, 2 * n_locations^2
+                               * 2 bytes; falls back to 1 above
+                               B2R_LB_TABLE_MAX_BYTES).  Journeys are the same
+                               in every mode. */
   uint32_t use_graphs;      /* 1 = capture the super-step in a CUDA graph */
   uint32_t route_block;     /* launch shape: warps per CTA in the route scan */
   uint32_t max_starts;      /* start labels per query (default 4096) */
@@ -367,6 +376,10 @@ typedef struct b2r_batch_stats {
   double lb_ms;               /* wall time of device lower-bound solves */
   uint64_t lb_iterations;     /* solver iterations (8 per chunk) */
   uint64_t lb_relaxations;    /* improving edge relaxations */
+  uint64_t h2d_bytes;         /* host->device bytes the call copied */
+  uint64_t d2h_bytes;         /* device->host bytes the call copied */
+  uint64_t route_warp_steps;  /* stop steps of route-scan warps (32 lanes
+                                 each; profiling engines only) */
 } b2r_batch_stats;
 int b2r_last_batch_stats(const b2r_engine* e, b2r_batch_stats* s);
 

@@ -122,7 +122,9 @@ class BatchStats(C.Structure):
                 ("route_stop_visits", C.c_uint64), ("et_events", C.c_uint64),
                 ("et_days", C.c_uint64), ("label_writes", C.c_uint64),
                 ("route_scan_bytes", C.c_uint64), ("lb_ms", C.c_double),
-                ("lb_iterations", C.c_uint64), ("lb_relaxations", C.c_uint64)]
+                ("lb_iterations", C.c_uint64), ("lb_relaxations", C.c_uint64),
+                ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64),
+                ("route_warp_steps", C.c_uint64)]
 
 
 class TtBase(C.Structure):

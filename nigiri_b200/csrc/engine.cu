@@ -105,6 +105,9 @@ struct b2r_engine {
   uint32_t* h_lbcount{nullptr};   // pinned
   uint64_t lb_chunks{0};
   double lb_ms{0};
+  b2r::dev::journey_rec* d_keep{};  // journeys kept across interval-extension phases
+  // host<->device bytes copied by the current batch call
+  uint64_t h2d_bytes{0}, d2h_bytes{0};
   // admission staging (pinned) and device mirror
   uint8_t* h_adm{nullptr};
   uint8_t* d_adm{nullptr};
@@ -151,7 +154,7 @@ struct adm_hdr {
   uint32_t slot;
   uint32_t n_starts, n_dest, n_off;
   uint32_t clear_rt;
-  uint32_t lb_mode;  // 0 zeros, 1 column in payload, 2 computed on the device
+  uint32_t lb_mode;  // 0 zeros, 1 column in payload, 2 solved on the device, 3 from the table
   uint32_t n_seeds;
   uint32_t pad;
   uint64_t off_slot, off_starts, off_dest, off_off, off_lb, off_seeds;
@@ -180,7 +183,7 @@ __global__ void k_admit(dev::state st, adm_hdr const* hdr, uint8_t const* payloa
   auto const* offs = reinterpret_cast<b2r_offset const*>(payload + h.off_off);
   for (auto i = threadIdx.x; i < h.n_off; i += blockDim.x) st.off_pool[s * max_off + i] = offs[i];
   auto const* lbc = reinterpret_cast<uint16_t const*>(payload + h.off_lb);
-  if (h.lb_mode != 2) {
+  if (h.lb_mode < 2) {
     for (auto l = threadIdx.x; l < n_loc; l += blockDim.x) {
       st.lb[static_cast<size_t>(l) * st.S + s] = h.lb_mode ? lbc[l] : uint16_t{0};
     }
@@ -203,6 +206,37 @@ __global__ void k_admit(dev::state st, adm_hdr const* hdr, uint8_t const* payloa
       dev::mark(st, st.F[0], st.flist[0], dev::C_F0, l * st.G + (s >> 5), 1u << (s & 31));
     }
     if (threadIdx.x == 0) atomicOr(&st.lb_mask[s >> 5], 1u << (s & 31));
+  }
+  if (h.lb_mode == 3) {
+    // Dijkstra from the seeds (dijkstra.cc:18-67) as a minimum over table
+    // rows: every path of length <= kMaxTravelTime only passes locations
+    // closer than that, so min(seed distance + row) is the capped multi-
+    // source distance.
+    auto const* seeds = reinterpret_cast<uint32_t const*>(payload + h.off_seeds);
+    auto const* tab = st.slots[s].fwd ? st.lb_table_fwd : st.lb_table_bwd;
+    for (auto x = threadIdx.x; x < n_loc; x += blockDim.x) {
+      uint32_t best = 0xFFFFu;
+      for (auto i = 0u; i != h.n_seeds; ++i) {
+        auto const m = seeds[2 * i];
+        auto const d = tab[static_cast<size_t>(m) * n_loc + x];
+        if (d == 0xFFFFu) continue;
+        auto const c = seeds[2 * i + 1] + d;
+        if ((c <= B2R_MAX_TRAVEL_TIME_MIN || x == m) && c < best) best = c;
+      }
+      st.lb[static_cast<size_t>(x) * st.S + s] = static_cast<uint16_t>(best);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {  // children inherit the parent's bound, in location order
+      auto const& T = st.tt;
+      for (auto w = 0u; w != T.n_with_children; ++w) {
+        auto const i = T.with_children[w];
+        auto const lbv = st.lb[static_cast<size_t>(i) * st.S + s];
+        for (auto c = T.children_idx[i]; c != T.children_idx[i + 1]; ++c) {
+          auto& cv = st.lb[static_cast<size_t>(T.children[c]) * st.S + s];
+          if (lbv < cv) cv = lbv;
+        }
+      }
+    }
   }
   // is-destination bits of station-to-station queries
   auto const& sl = st.slots[s];
@@ -425,6 +459,7 @@ void solve_lower_bounds(b2r_engine& e, cudaStream_t s) {
       enqueue_lb_chunk(e, s);
     }
     ++chunks;
+    e.d2h_bytes += sizeof(uint32_t);
     B2R_CUDA(cudaMemcpyAsync(e.h_lbcount, e.st.counters + dev::C_F0, sizeof(uint32_t),
                              cudaMemcpyDeviceToHost, s));
     B2R_CUDA(cudaStreamSynchronize(s));
@@ -440,6 +475,37 @@ void solve_lower_bounds(b2r_engine& e, cudaStream_t s) {
   B2R_CUDA(cudaGetLastError());
   B2R_CUDA(cudaStreamSynchronize(s));
   e.lb_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// The all-pairs lower-bound tables of a timetable: row s holds the
+// Dijkstra distances from location s over the forward- / backward-search
+// lower-bound graph.  Built on the host threads in row blocks and uploaded
+// block by block; kept with the timetable for every later engine.
+void ensure_lb_table(b2r_timetable& t, unsigned threads) {
+  std::lock_guard<std::mutex> lock{t.lb_table_mutex};
+  if (t.lb_table[0] != nullptr) return;
+  auto const n = static_cast<size_t>(t.d.n_loc);
+  constexpr size_t kBlock = 1024;
+  std::vector<uint16_t> buf(kBlock * n);
+  for (auto dir = 0; dir != 2; ++dir) {
+    auto* dst = dmalloc<uint16_t>(n * n, t.bytes);
+    t.allocs.push_back(dst);
+    for (size_t b = 0; b < n; b += kBlock) {
+      auto const rows = std::min(kBlock, n - b);
+      std::atomic<size_t> next{0};
+      auto work = [&]() {
+        for (auto r = next++; r < rows; r = next++) {
+          lb_table_row(t.view, dir == 0, static_cast<uint32_t>(b + r), buf.data() + r * n);
+        }
+      };
+      std::vector<std::thread> pool;
+      for (auto i = 1U; i < threads; ++i) pool.emplace_back(work);
+      work();
+      for (auto& th : pool) th.join();
+      B2R_CUDA(cudaMemcpy(dst + b * n, buf.data(), rows * n * sizeof(uint16_t), cudaMemcpyHostToDevice));
+    }
+    t.lb_table[dir] = dst;
+  }
 }
 
 void admit(b2r_engine& e, std::vector<std::pair<uint32_t, prepped_query const*>> const& adm,
@@ -495,7 +561,11 @@ void admit(b2r_engine& e, std::vector<std::pair<uint32_t, prepped_query const*>>
     offs.insert(offs.end(), p.dest_offsets.begin(), p.dest_offsets.end());
     h.n_off = static_cast<uint32_t>(offs.size());
     h.off_off = put(offs.data(), offs.size() * sizeof(b2r_offset));
-    h.lb_mode = !p.lb.empty() ? 1 : (e.cfg.use_lower_bounds == 2 && !p.one_to_all ? 2 : 0);
+    h.lb_mode = !p.lb.empty() ? 1
+                : p.one_to_all       ? 0
+                : e.cfg.use_lower_bounds == 2 ? 2
+                : e.cfg.use_lower_bounds == 3 ? 3
+                                              : 0;
     h.off_lb = put(p.lb.data(), p.lb.size() * sizeof(uint16_t));
     std::vector<uint32_t> seeds;
     for (auto const& [l, d] : p.lb_seeds) {
@@ -506,6 +576,7 @@ void admit(b2r_engine& e, std::vector<std::pair<uint32_t, prepped_query const*>>
     h.off_seeds = put(seeds.data(), seeds.size() * sizeof(uint32_t));
     any_device_lb = any_device_lb || h.lb_mode == 2;
   }
+  e.h2d_bytes += off;
   B2R_CUDA(cudaMemcpyAsync(e.d_adm, e.h_adm, off, cudaMemcpyHostToDevice, s));
   k_admit<<<static_cast<unsigned>(adm.size()), 256, 0, s>>>(
       e.st, reinterpret_cast<adm_hdr const*>(e.d_adm), e.d_adm, static_cast<uint32_t>(adm.size()),
@@ -519,6 +590,7 @@ void retire(b2r_engine& e, std::vector<uint32_t> const& slots, cudaStream_t s) {
   uint32_t* d = nullptr;
   // reuse the export list buffer (sized for all slots)
   d = e.d_exp_list;
+  e.h2d_bytes += slots.size() * sizeof(uint32_t);
   B2R_CUDA(cudaMemcpyAsync(d, slots.data(), slots.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
   k_retire<<<static_cast<unsigned>(slots.size()), 128, 0, s>>>(e.st, d, static_cast<uint32_t>(slots.size()));
   B2R_CUDA(cudaGetLastError());
@@ -565,10 +637,12 @@ void export_slots(b2r_engine& e, std::vector<uint32_t> const& slots,
     B2R_CUDA(cudaMalloc(&e.d_exp, e.exp_cap));
   }
   std::memcpy(e.h_exp, items.data(), items.size() * sizeof(exp_item));
+  e.h2d_bytes += items.size() * sizeof(exp_item);
   B2R_CUDA(cudaMemcpyAsync(e.d_exp, e.h_exp, items.size() * sizeof(exp_item), cudaMemcpyHostToDevice, s));
   k_export<<<static_cast<unsigned>(slots.size()), 256, 0, s>>>(
       e.st, reinterpret_cast<exp_item const*>(e.d_exp), static_cast<uint32_t>(slots.size()), e.d_exp);
   B2R_CUDA(cudaGetLastError());
+  e.d2h_bytes += off;
   B2R_CUDA(cudaMemcpyAsync(e.h_exp, e.d_exp, off, cudaMemcpyDeviceToHost, s));
   B2R_CUDA(cudaStreamSynchronize(s));
   for (auto i = 0U; i != slots.size(); ++i) {
@@ -721,6 +795,7 @@ struct batch_runner {
     // generation unless reset_arrivals (raptor.h:174-177)
     auto const tad_keep = !q.reset_arrivals;
     slot_t cur{};
+    e.d2h_bytes += sizeof(slot_t);
     B2R_CUDA(cudaMemcpyAsync(&cur, e.st.slots + s, sizeof(slot_t), cudaMemcpyDeviceToHost, st));
     B2R_CUDA(cudaStreamSynchronize(st));
     if (q.reset_arrivals) {
@@ -743,14 +818,15 @@ struct batch_runner {
     }
     B2R_CUDA(cudaMemcpyAsync(e.st.start_pool + cur.starts_off, starts.data(),
                              starts.size() * sizeof(dev::start_rec), cudaMemcpyHostToDevice, st));
-    dev::journey_rec* dj = nullptr;
-    B2R_CUDA(cudaMalloc(&dj, std::max<size_t>(1, q.keep.size()) * sizeof(dev::journey_rec)));
+    if (q.keep.size() > e.max_j) throw std::runtime_error("journey capacity exceeded");
+    auto* dj = e.d_keep;  // engine-owned, reused (this function synchronises)
     B2R_CUDA(cudaMemcpyAsync(dj, q.keep.data(), q.keep.size() * sizeof(dev::journey_rec),
                              cudaMemcpyHostToDevice, st));
     k_set_journeys<<<1, 32, 0, st>>>(e.st, s, dj, static_cast<uint32_t>(q.keep.size()));
     B2R_CUDA(cudaMemcpyAsync(e.st.slots + s, &cur, sizeof(slot_t), cudaMemcpyHostToDevice, st));
     B2R_CUDA(cudaStreamSynchronize(st));
-    cudaFree(dj);
+    e.h2d_bytes += starts.size() * sizeof(dev::start_rec) + q.keep.size() * sizeof(dev::journey_rec) +
+                   sizeof(slot_t);
     q.rearm = false;
   }
 
@@ -827,6 +903,7 @@ struct batch_runner {
         ++steps;
       }
       B2R_CUDA(cudaEventRecord(e.ev1, st));
+      e.d2h_bytes += S * sizeof(b2r_engine::summary_t);
       B2R_CUDA(cudaMemcpyAsync(e.h_summary, e.d_summary, S * sizeof(b2r_engine::summary_t),
                                cudaMemcpyDeviceToHost, st));
       B2R_CUDA(cudaStreamSynchronize(st));
@@ -1116,6 +1193,15 @@ int b2r_engine_create(b2r_timetable* tt, const b2r_engine_config* cfg_in, b2r_en
       if (cfg.profile) e->cfg.use_graphs = 0;
       e->max_dest = 512U;
       e->max_off = 128U;
+      if (cfg.use_lower_bounds == 3) {  // the table when it fits, else the host Dijkstra
+        auto const n = static_cast<uint64_t>(tt->d.n_loc);
+        if (2 * n * n * sizeof(uint16_t) <= B2R_LB_TABLE_MAX_BYTES) {
+          auto const hw = std::max(1U, std::thread::hardware_concurrency());
+          b2r::ensure_lb_table(*tt, cfg.host_threads != 0 ? cfg.host_threads : hw);
+        } else {
+          e->cfg.use_lower_bounds = 1;
+        }
+      }
       auto const nl = tt->d.n_loc;
       e->bytes_per_slot = static_cast<uint64_t>(nl) * (b2r::dev::kK * 4 + 4 + 4 + 2 + 4) +
                           static_cast<uint64_t>(e->max_j) *
@@ -1180,6 +1266,8 @@ int b2r_engine_create(b2r_timetable* tt, const b2r_engine_config* cfg_in, b2r_en
       al(st.flist[0], static_cast<size_t>(nl) * G);
       al(st.flist[1], static_cast<size_t>(nl) * G);
       al(st.lb_mask, G);
+      st.lb_table_fwd = tt->lb_table[0];
+      st.lb_table_bwd = tt->lb_table[1];
       B2R_CUDA(cudaMemset(st.dist, 0xFF, static_cast<size_t>(nl) * S * 4));
       B2R_CUDA(cudaMemset(st.F[0], 0, static_cast<size_t>(nl) * G * 4));
       B2R_CUDA(cudaMemset(st.F[1], 0, static_cast<size_t>(nl) * G * 4));
@@ -1187,6 +1275,7 @@ int b2r_engine_create(b2r_timetable* tt, const b2r_engine_config* cfg_in, b2r_en
       st.profile = cfg.profile ? 1u : 0u;
       B2R_CUDA(cudaMemset(st.prof, 0, 8 * sizeof(unsigned long long)));
       al(e->d_exp_list, S);
+      al(e->d_keep, e->max_j);
       B2R_CUDA(cudaMemset(st.slots, 0, S * sizeof(b2r::dev::slot_t)));
       B2R_CUDA(cudaMemset(st.rt, 0xFF, static_cast<size_t>(b2r::dev::kK) * nl * S * 4));
       B2R_CUDA(cudaMemset(st.best, 0xFF, static_cast<size_t>(nl) * S * 4));
@@ -1247,6 +1336,8 @@ int b2r_search_batch(b2r_engine* e, const b2r_query* qs, uint32_t n, b2r_result*
       e->prof_used = 0;
       e->lb_ms = 0;
       e->lb_chunks = 0;
+      e->h2d_bytes = 0;
+      e->d2h_bytes = 0;
       if (e->cfg.profile) B2R_CUDA(cudaMemsetAsync(e->st.prof, 0, 8 * sizeof(unsigned long long), e->stream));
       br.run(e->cfg.steps_per_sync != 0 ? e->cfg.steps_per_sync : 4U);
       prep.join();
@@ -1259,6 +1350,8 @@ int b2r_search_batch(b2r_engine* e, const b2r_query* qs, uint32_t n, b2r_result*
       e->last.super_steps = br.steps;
       e->last.lb_ms = e->lb_ms;
       e->last.lb_iterations = e->lb_chunks * 8;
+      e->last.h2d_bytes = e->h2d_bytes;
+      e->last.d2h_bytes = e->d2h_bytes;
       if (e->cfg.profile) {
         double scan_ms = 0;
         for (size_t i = 0; i + 1 < e->prof_used; i += 2) {
@@ -1280,6 +1373,7 @@ int b2r_search_batch(b2r_engine* e, const b2r_query* qs, uint32_t n, b2r_result*
         // service day; 2 B per label write
         e->last.route_scan_bytes = c[0] * 8ull + c[1] * 2ull + c[2] * 8ull + c[3] * 2ull;
         e->last.lb_relaxations = c[4];
+        e->last.route_warp_steps = c[5];
       }
       uint32_t err = 0;
       B2R_CUDA(cudaMemcpy(&err, e->st.counters + b2r::dev::C_ERR, 4, cudaMemcpyDeviceToHost));

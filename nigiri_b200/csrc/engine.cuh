@@ -203,6 +203,9 @@ struct state {
   uint32_t* F[2];        // [n_loc][G]
   uint32_t* flist[2];
   uint32_t* lb_mask;     // [G]
+  // all-pairs lower-bound tables (forward / backward search), or null
+  uint16_t const* lb_table_fwd;
+  uint16_t const* lb_table_bwd;
 };
 
 // ------------------------------------------------------------- helpers

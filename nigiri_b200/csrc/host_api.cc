@@ -46,7 +46,7 @@ void b2r_engine_config_init(b2r_engine_config* c) {
   c->hbm_budget = 64ull << 30;
   c->max_journeys = 128;
   c->host_threads = 0;
-  c->use_lower_bounds = 1;
+  c->use_lower_bounds = 3;
   c->use_graphs = 1;
   c->route_block = 4;
 }

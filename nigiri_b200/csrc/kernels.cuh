@@ -144,67 +144,67 @@ __global__ void k_ctl_marked(state st) {
 }
 
 // ------------------------------------------------------------ route scan
-// update_route, raptor.h:1177-1349 (no vias, no section filters): one warp
-// per (route, group of 32 queries); each lane walks the stop sequence of
-// its query in search direction carrying its current trip.
+// update_route, raptor.h:1177-1349 (no vias, no section filters) for every
+// (route, query) pair marked this round.  One thread per marked (route,
+// group of 32 queries) entry walks the route once for each query of the
+// entry's mask, carrying that query's current trip: resident queries are
+// unrelated, so an entry holds few queries and a warp-per-entry scan would
+// leave most lanes idle.  Labels are combined with atomicMin and marks with
+// atomicOr, so the order of the pairs does not matter.
 __global__ void __launch_bounds__(256) k_route_scan(state st) {
-  auto const lane = threadIdx.x & 31u;
-  auto const warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  auto const n_warps = (gridDim.x * blockDim.x) >> 5;
+  auto const tid = blockIdx.x * blockDim.x + threadIdx.x;
+  auto const n_threads = gridDim.x * blockDim.x;
   auto const nr = st.counters[C_R];
   auto const& T = st.tt;
-  for (auto w = warp; w < nr; w += n_warps) {
+  uint32_t p_ev = 0, p_days = 0, p_writes = 0, p_stops = 0;
+  for (auto w = tid; w < nr; w += n_threads) {
     auto const e = st.rlist[w];
     auto const g = e % st.G, r = e / st.G;
-    auto const mask = st.R[e];
-    __syncwarp();
-    if (lane == 0) st.R[e] = 0u;
-    auto const s = g * 32u + lane;
-    auto const ln = st.lanes[s];
-    auto active = ((mask >> lane) & 1u) != 0u && ln.run;
-    auto const fwd = ln.fwd != 0;
-    auto const k = static_cast<uint32_t>(ln.k);
+    auto mask = st.R[e];
+    st.R[e] = 0u;
     auto const sb = T.route_stop_idx[r];
     auto const n = T.route_stop_idx[r + 1] - sb;
     auto const t0 = T.route_tr_from[r];
     auto const n_t = T.route_tr_to[r] - t0;
     auto const* colbase = T.st + T.route_st_from[r];
-    bool et_valid = false;
-    uint32_t et_off = 0;
-    uint16_t et_day = 0;
-    uint32_t p_ev = 0, p_days = 0, p_writes = 0, p_stops = 0;
-    for (auto i = 0u; i != n; ++i) {
-      p_stops += active ? 1u : 0u;
-      auto const si = fwd ? i : n - 1u - i;
-      auto const stp = T.route_stops[sb + si];
-      auto const l = B2R_STOP_LOC(stp);
-      auto const can_finish = fwd ? B2R_STOP_OUT(stp) : B2R_STOP_IN(stp);
-      auto const can_start = fwd ? B2R_STOP_IN(stp) : B2R_STOP_OUT(stp);
-      bool reached = false;
-      bool arrival_ran = false;
-      if (active && et_valid && can_finish) {
-        arrival_ran = true;
-        auto const ev = colbase[n_t * (si * 2u - (fwd ? 1u : 0u)) + et_off];
-        auto const by = to_delta_key(fwd, et_day, ln.base, delta_count(ev));
-        auto const lbv = st.lb[li(st, l, s)];
-        if (by <= ln.tad_k && lbv != 0xFFFFu && by + static_cast<int>(lbv) <= ln.tad_k) {
-          auto const word = enc(ln.gtag, by);
-          auto* tp = &st.tmp[li(st, l, s)];
-          if (word < *tp) {
-            atomicMin(tp, word);
-            ++p_writes;
+    while (mask != 0u) {
+      auto const b = static_cast<uint32_t>(__ffs(mask) - 1);
+      mask &= mask - 1u;
+      auto const s = g * 32u + b;
+      auto const ln = st.lanes[s];
+      if (!ln.run) continue;
+      auto const bit = 1u << b;
+      auto const fwd = ln.fwd != 0;
+      auto const k = static_cast<uint32_t>(ln.k);
+      bool et_valid = false;
+      uint32_t et_off = 0;
+      uint16_t et_day = 0;
+      for (auto i = 0u; i != n; ++i) {
+        ++p_stops;
+        auto const si = fwd ? i : n - 1u - i;
+        auto const stp = T.route_stops[sb + si];
+        auto const l = B2R_STOP_LOC(stp);
+        auto const can_finish = fwd ? B2R_STOP_OUT(stp) : B2R_STOP_IN(stp);
+        auto const can_start = fwd ? B2R_STOP_IN(stp) : B2R_STOP_OUT(stp);
+        bool arrival_ran = false;
+        if (et_valid && can_finish) {
+          arrival_ran = true;
+          auto const ev = colbase[n_t * (si * 2u - (fwd ? 1u : 0u)) + et_off];
+          auto const by = to_delta_key(fwd, et_day, ln.base, delta_count(ev));
+          auto const lbv = st.lb[li(st, l, s)];
+          if (by <= ln.tad_k && lbv != 0xFFFFu && by + static_cast<int>(lbv) <= ln.tad_k) {
+            auto const word = enc(ln.gtag, by);
+            auto* tp = &st.tmp[li(st, l, s)];
+            if (word < *tp) {
+              atomicMin(tp, word);
+              ++p_writes;
+            }
+            mark(st, st.Y, st.ylist, C_Y, l * st.G + g, bit);
           }
-          reached = true;
         }
-      }
-      mark_warp(st, st.Y, st.ylist, C_Y, reached, l * st.G + g, lane);
-
-      auto const is_last = i + 1u == n;
-      if (active && !is_last && can_start && ((st.X[l * st.G + g] >> lane) & 1u)) {
-        auto const lbv = st.lb[li(st, l, s)];
-        if (lbv == 0xFFFFu) {
-          active = false;  // raptor.h:1309-1311
-        } else {
+        if (i + 1u != n && can_start && (st.X[l * st.G + g] & bit)) {
+          auto const lbv = st.lb[li(st, l, s)];
+          if (lbv == 0xFFFFu) break;  // raptor.h:1309-1311: no later stop of this query
           auto const board_col = n_t * (si * 2u - (fwd ? 0u : 1u));
           auto const et_time =
               et_valid ? to_delta_key(fwd, et_day, ln.base, delta_count(colbase[board_col + et_off]))
@@ -236,19 +236,23 @@ __global__ void __launch_bounds__(256) k_route_scan(state st) {
         }
       }
     }
-    if (st.profile) {  // work counters for the roofline (warp-reduced)
-      for (auto o = 16; o > 0; o >>= 1) {
-        p_stops += __shfl_xor_sync(kFull, p_stops, o);
-        p_ev += __shfl_xor_sync(kFull, p_ev, o);
-        p_days += __shfl_xor_sync(kFull, p_days, o);
-        p_writes += __shfl_xor_sync(kFull, p_writes, o);
-      }
-      if (lane == 0) {
-        atomicAdd(&st.prof[0], static_cast<unsigned long long>(p_stops));
-        atomicAdd(&st.prof[1], static_cast<unsigned long long>(p_ev));
-        atomicAdd(&st.prof[2], static_cast<unsigned long long>(p_days));
-        atomicAdd(&st.prof[3], static_cast<unsigned long long>(p_writes));
-      }
+  }
+  if (st.profile) {  // work counters for the roofline (warp-reduced)
+    __syncwarp();
+    auto steps_max = p_stops;
+    for (auto o = 16; o > 0; o >>= 1) {
+      p_stops += __shfl_xor_sync(kFull, p_stops, o);
+      p_ev += __shfl_xor_sync(kFull, p_ev, o);
+      p_days += __shfl_xor_sync(kFull, p_days, o);
+      p_writes += __shfl_xor_sync(kFull, p_writes, o);
+      steps_max = max(steps_max, __shfl_xor_sync(kFull, steps_max, o));
+    }
+    if ((threadIdx.x & 31u) == 0) {
+      atomicAdd(&st.prof[0], static_cast<unsigned long long>(p_stops));
+      atomicAdd(&st.prof[1], static_cast<unsigned long long>(p_ev));
+      atomicAdd(&st.prof[2], static_cast<unsigned long long>(p_days));
+      atomicAdd(&st.prof[3], static_cast<unsigned long long>(p_writes));
+      atomicAdd(&st.prof[5], static_cast<unsigned long long>(steps_max));  // warp stop steps
     }
   }
 }

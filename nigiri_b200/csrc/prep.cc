@@ -218,6 +218,41 @@ void lower_bounds(view const& v, prepped_query const& p, std::vector<uint16_t>& 
   }
 }
 
+}  // namespace
+
+// One row of the all-pairs lower-bound table: the Dijkstra of
+// lower_bounds() from the single seed `src` at distance 0, without the
+// children step (applied per query after the rows are combined).
+void lb_table_row(host_view const& hv, bool fwd, uint32_t src, uint16_t* row) {
+  auto const n = hv.d.n_locations;
+  std::fill(row, row + n, kUnreach);
+  constexpr uint32_t kBuckets = B2R_MAX_TRAVEL_TIME_MIN + 1;
+  thread_local std::vector<std::vector<uint32_t>> bucket(kBuckets);
+  size_t cur = 0, size = 1;
+  bucket[0].push_back(src);
+  row[src] = 0;
+  auto const* gi = fwd ? hv.d.lb_fwd_index : hv.d.lb_bwd_index;
+  auto const* gd = fwd ? hv.d.lb_fwd : hv.d.lb_bwd;
+  while (size != 0) {
+    while (bucket[cur].empty()) ++cur;
+    auto const l = bucket[cur].back();
+    bucket[cur].pop_back();
+    --size;
+    if (row[l] < cur) continue;
+    for (auto e = gi[l]; e != gi[l + 1]; ++e) {
+      auto const tgt = B2R_FP_TARGET(gd[e]);
+      auto const nd = static_cast<uint32_t>(cur) + B2R_FP_DURATION(gd[e]);
+      if (nd < row[tgt] && nd < kBuckets) {
+        row[tgt] = static_cast<uint16_t>(nd);
+        bucket[nd].push_back(tgt);
+        ++size;
+      }
+    }
+  }
+}
+
+namespace {
+
 uint16_t event(b2r_timetable_desc const& d, uint32_t r, uint32_t t, uint32_t s, bool arr) {
   auto const n_t = d.route_transport_to[r] - d.route_transport_from[r];
   return d.route_stop_times[d.route_stop_time_from[r] + n_t * (s * 2 - (arr ? 1U : 0U)) +
@@ -416,7 +451,7 @@ void prepare(host_view const& hv, b2r_query const& q, int lb_mode, prepped_query
     p.dest_locs.erase(std::unique(p.dest_locs.begin(), p.dest_locs.end()), p.dest_locs.end());
   }
   if (lb_mode == 1) lower_bounds(v, p, p.lb);
-  if (lb_mode == 2) lb_seeds(v, p, p.lb_seeds);
+  if (lb_mode == 2 || lb_mode == 3) lb_seeds(v, p, p.lb_seeds);
   auto const mid = static_cast<int64_t>(p.iv_from) + (p.iv_to - p.iv_from) / 2;
   p.base = static_cast<uint16_t>(round_to_days(mid) - hv.internal_from_days());
   p.base_days = hv.internal_from_days() + p.base;

@@ -58,11 +58,17 @@ struct prepped_query {
   std::vector<std::pair<uint32_t, uint16_t>> lb_seeds;
 };
 
+// Row `src` of the all-pairs lower-bound table: shortest distances from
+// src over the forward- or backward-search lower-bound graph, 0xFFFF beyond
+// kMaxTravelTime (row must hold n_locations values).
+void lb_table_row(host_view const& tt, bool fwd, uint32_t src, uint16_t* row);
+
 // std::chrono::round<days> of a minute time point (ties to even).
 int32_t round_to_days(int64_t minutes);
 
 // Computes everything above.  lb_mode: 0 = no lower bounds (lb = 0),
-// 1 = Dijkstra on the host (lb filled), 2 = on the device (lb_seeds filled).
+// 1 = Dijkstra on the host (lb filled), 2 = on the device and 3 = from the
+// all-pairs table on the device (lb_seeds filled).
 void prepare(host_view const& tt, b2r_query const& q, int lb_mode,
              prepped_query& out);
 

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 #include <vector>
 
 #include "b2r.h"
@@ -27,6 +28,11 @@ struct b2r_timetable {
   std::vector<uint16_t> route_stop_times;
   std::vector<uint64_t> bitfields;
   b2r::host_view view{};
+  // all-pairs lower-bound tables [source][location] (u16 minutes, 0xFFFF
+  // unreachable) for forward and backward searches, built by the first
+  // engine that uses them
+  uint16_t* lb_table[2]{nullptr, nullptr};
+  std::mutex lb_table_mutex;
 
   ~b2r_timetable() {
     for (auto* p : allocs) cudaFree(p);

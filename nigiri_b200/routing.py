@@ -202,9 +202,11 @@ class Engine:
         cfg.max_slots = max_slots
         cfg.hbm_budget = hbm_budget
         cfg.max_journeys = max_journeys
-        # True / "host" -> host Dijkstra (1); "device" -> device solver (2);
+        # True / "table" -> all-pairs tables on the device when they fit, else
+        # host Dijkstra (3); "host" -> 1; "device" -> device solver (2);
         # False -> none (0)
-        cfg.use_lower_bounds = {True: 1, "host": 1, "device": 2, False: 0}[use_lower_bounds]
+        cfg.use_lower_bounds = {True: 3, "table": 3, "host": 1, "device": 2,
+                                False: 0}[use_lower_bounds]
         cfg.use_graphs = int(use_graphs)
         cfg.host_threads = host_threads
         cfg.max_starts = max_starts

@@ -150,7 +150,7 @@ def test_one_to_all_rows_match_oracle(workload, c1, c2):
         assert np.array_equal(rows, orows[: r.n_rows]), i
 
 
-@pytest.mark.parametrize("lb_mode", ["device", False])
+@pytest.mark.parametrize("lb_mode", ["host", "device", False])
 def test_lower_bound_modes_give_identical_journeys(c2, lb_mode):
     """Lower bounds only prune: journeys are the same with bounds computed
     on the device, on the host, or without bounds (nigiri's GPU raptor runs
