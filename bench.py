@@ -367,6 +367,9 @@ def ncu_case(args, local):
                       "route_scan_launches": st.route_scan_launches,
                       "route_stop_visits": st.route_stop_visits,
                       "route_warp_steps": st.route_warp_steps,
+                      "route_scan_ms": st.route_scan_ms, "recon_ms": st.recon_ms,
+                      "recon_max_journey_us": st.recon_max_journey_us,
+                      "recon_journeys": st.recon_journeys,
                       "route_scan_bytes": st.route_scan_bytes}))
 
 

@@ -380,6 +380,10 @@ typedef struct b2r_batch_stats {
   uint64_t d2h_bytes;         /* device->host bytes the call copied */
   uint64_t route_warp_steps;  /* stop steps of route-scan warps (32 lanes
                                  each; profiling engines only) */
+  double recon_ms;            /* summed CUDA-event time of the reconstruction
+                                 launches (profiling engines only) */
+  double recon_max_journey_us; /* longest single journey reconstruction */
+  uint64_t recon_journeys;    /* journeys reconstructed */
 } b2r_batch_stats;
 int b2r_last_batch_stats(const b2r_engine* e, b2r_batch_stats* s);
 

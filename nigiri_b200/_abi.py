@@ -124,7 +124,8 @@ class BatchStats(C.Structure):
                 ("route_scan_bytes", C.c_uint64), ("lb_ms", C.c_double),
                 ("lb_iterations", C.c_uint64), ("lb_relaxations", C.c_uint64),
                 ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64),
-                ("route_warp_steps", C.c_uint64)]
+                ("route_warp_steps", C.c_uint64), ("recon_ms", C.c_double),
+                ("recon_max_journey_us", C.c_double), ("recon_journeys", C.c_uint64)]
 
 
 class TtBase(C.Structure):

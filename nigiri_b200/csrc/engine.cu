@@ -123,6 +123,8 @@ struct b2r_engine {
   // profiling: event pairs bracketing each route-scan launch
   std::vector<cudaEvent_t> prof_ev;
   size_t prof_used{0};
+  std::vector<cudaEvent_t> prof_rc_ev;  // around the reconstruction launches
+  size_t prof_rc_used{0};
   std::chrono::steady_clock::time_point batch_t0;
 
   // results of the last batch / serving tickets
@@ -324,6 +326,7 @@ __global__ void k_set_journeys(dev::state st, uint32_t s, dev::journey_rec const
 
 b2r_engine::~b2r_engine() {
   for (auto ev : prof_ev) cudaEventDestroy(ev);
+  for (auto ev : prof_rc_ev) cudaEventDestroy(ev);
   if (graph != nullptr) cudaGraphExecDestroy(graph);
   if (lb_graph != nullptr) cudaGraphExecDestroy(lb_graph);
   if (stream != nullptr) cudaStreamDestroy(stream);
@@ -374,7 +377,19 @@ void enqueue_superstep(b2r_engine& e, cudaStream_t s) {
   dev::k_footpaths<<<list_blocks, 256, 0, s>>>(st);
   dev::k_ctl_end<<<slot_blocks, 128, 0, s>>>(st);
   dev::k_collect<<<slot_blocks, 128, 0, s>>>(st);
+  cudaEvent_t rc_a = nullptr, rc_b = nullptr;
+  if (e.cfg.profile) {
+    while (e.prof_rc_used + 2 > e.prof_rc_ev.size()) {
+      cudaEvent_t x;
+      B2R_CUDA(cudaEventCreate(&x));
+      e.prof_rc_ev.push_back(x);
+    }
+    rc_a = e.prof_rc_ev[e.prof_rc_used++];
+    rc_b = e.prof_rc_ev[e.prof_rc_used++];
+    B2R_CUDA(cudaEventRecord(rc_a, s));
+  }
   dev::k_reconstruct<<<e.sms * 4, 128, 0, s>>>(st);
+  if (e.cfg.profile) B2R_CUDA(cudaEventRecord(rc_b, s));
   dev::k_next<<<slot_blocks, 128, 0, s>>>(st);
   k_summary<<<slot_blocks, 128, 0, s>>>(st, e.d_summary);
 }
@@ -1334,6 +1349,7 @@ int b2r_search_batch(b2r_engine* e, const b2r_query* qs, uint32_t n, b2r_result*
       prep.start(*e, qs, n, runs, false);
       b2r::batch_runner br{*e, runs, e->cfg.use_graphs != 0 && e->graph != nullptr};
       e->prof_used = 0;
+      e->prof_rc_used = 0;
       e->lb_ms = 0;
       e->lb_chunks = 0;
       e->h2d_bytes = 0;
@@ -1374,6 +1390,15 @@ int b2r_search_batch(b2r_engine* e, const b2r_query* qs, uint32_t n, b2r_result*
         e->last.route_scan_bytes = c[0] * 8ull + c[1] * 2ull + c[2] * 8ull + c[3] * 2ull;
         e->last.lb_relaxations = c[4];
         e->last.route_warp_steps = c[5];
+        double rc_ms = 0;
+        for (size_t i = 0; i + 1 < e->prof_rc_used; i += 2) {
+          float x = 0;
+          cudaEventElapsedTime(&x, e->prof_rc_ev[i], e->prof_rc_ev[i + 1]);
+          rc_ms += x;
+        }
+        e->last.recon_ms = rc_ms;
+        e->last.recon_max_journey_us = static_cast<double>(c[6]) / 1e3;
+        e->last.recon_journeys = c[7];
       }
       uint32_t err = 0;
       B2R_CUDA(cudaMemcpy(&err, e->st.counters + b2r::dev::C_ERR, 4, cudaMemcpyDeviceToHost));

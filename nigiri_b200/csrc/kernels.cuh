@@ -628,6 +628,8 @@ __global__ void k_reconstruct(state st) {
   auto const n_warps = (gridDim.x * blockDim.x) >> 5;
   auto const n = st.counters[C_RECON];
   for (auto i = warp; i < n; i += n_warps) {
+    uint64_t t_begin = 0;
+    if (st.profile) asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t_begin));
     auto const e = st.recon_list[i];
     auto const s = e >> 16, ji = e & 0xFFFFu;
     auto& sl = st.slots[s];
@@ -653,6 +655,12 @@ __global__ void k_reconstruct(state st) {
       } else {
         j.reconstructed = 1;
         j.n_legs = static_cast<uint16_t>(c.n_legs);
+      }
+      if (st.profile) {  // longest single reconstruction (ns), journeys
+        uint64_t t_end = 0;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t_end));
+        atomicMax(&st.prof[6], static_cast<unsigned long long>(t_end - t_begin));
+        atomicAdd(&st.prof[7], 1ull);
       }
     }
   }

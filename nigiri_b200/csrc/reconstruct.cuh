@@ -150,22 +150,37 @@ struct recon_ctx {
     return out;
   }
 
-  // reconstruct.cc:180-280 (single pass: no vias)
+  // reconstruct.cc:180-280 (single pass: no vias).  The stops before the
+  // exit stop are split across the lanes; the ballot keeps the first one in
+  // the reference's order.  Called by the whole warp with equal arguments.
   __device__ bool find_start_in_prev_round(unsigned k, uint32_t t, uint16_t day, uint32_t finish,
                                            b2r_leg& out) const {
     auto const r = T->transport_route[t];
     auto const size = n_stops(r);
     auto const n = fwd ? finish + 1u : size - finish;
-    for (auto i = 1u; i < n; ++i) {
-      auto const si = fwd ? finish - i : finish + i;
-      auto const w = stopw(r, si);
-      auto const l = B2R_STOP_LOC(w);
-      if ((fwd && !B2R_STOP_IN(w)) || (!fwd && !B2R_STOP_OUT(w))) continue;
-      auto const event_time = unix_to_delta(ev_time(t, day, si, !fwd));
-      auto const round_time = rt_t(k - 1, l);
-      if (beq(round_time, event_time) ||
-          (k == 1 && sl->start_mode == B2R_MATCH_EQUIVALENT && is_journey_start(l) &&
-           (ontrip ? beq(round_time, event_time) : round_time == event_time))) {
+    for (auto i0 = 1u; i0 < n; i0 += 32u) {
+      auto const i = i0 + lane;
+      bool ok = false;
+      uint32_t si = 0, l = 0;
+      int event_time = 0;
+      if (i < n) {
+        si = fwd ? finish - i : finish + i;
+        auto const w = stopw(r, si);
+        l = B2R_STOP_LOC(w);
+        if (!((fwd && !B2R_STOP_IN(w)) || (!fwd && !B2R_STOP_OUT(w)))) {
+          event_time = unix_to_delta(ev_time(t, day, si, !fwd));
+          auto const round_time = rt_t(k - 1, l);
+          ok = beq(round_time, event_time) ||
+               (k == 1 && sl->start_mode == B2R_MATCH_EQUIVALENT && is_journey_start(l) &&
+                (ontrip ? beq(round_time, event_time) : round_time == event_time));
+        }
+      }
+      auto const m = __ballot_sync(kFull, ok);
+      if (m != 0u) {
+        auto const src = __ffs(m) - 1;
+        si = __shfl_sync(kFull, si, src);
+        l = __shfl_sync(kFull, l, src);
+        event_time = __shfl_sync(kFull, event_time, src);
         out = make_leg(l, B2R_STOP_LOC(stopw(r, finish)), delta_to_unix(event_time),
                        ev_time(t, day, finish, fwd));
         set_run(out, t, day, si, finish);
@@ -175,73 +190,126 @@ struct recon_ctx {
     return false;
   }
 
-  // reconstruct.cc:292-373; columns are ordered by minutes after midnight,
-  // so the transports with the wanted mam form one run found by binary
-  // search and visited in index order like the reference's linear loop.
-  __device__ bool get_route_transport(unsigned k, int time, uint32_t r, uint32_t si,
-                                      b2r_leg& out) const {
+  // The transports of route r whose event at stop si has the minutes after
+  // midnight of `time` (reconstruct.cc:292-373), one at a time from
+  // `cursor`: columns are ordered by minutes after midnight, so they form
+  // one run found by binary search and visited in index order.
+  __device__ uint32_t first_cursor(int time, uint32_t r, uint32_t si) const {
+    if (!T->route_sorted[r]) return 0u;
+    auto const mam = static_cast<int16_t>((static_cast<int>(base) * 1440 + time) % 1440);
+    auto const n_t = T->route_tr_to[r] - T->route_tr_from[r];
+    auto const* col = T->st + T->route_st_from[r] + n_t * (si * 2u - (fwd ? 1u : 0u));
+    uint32_t lo = 0, hi = n_t;
+    while (lo < hi) {
+      auto const mid = (lo + hi) >> 1;
+      if ((col[mid] >> 5) < static_cast<uint16_t>(mam < 0 ? 0 : mam)) lo = mid + 1;
+      else hi = mid;
+    }
+    return lo;
+  }
+  __device__ bool next_transport(int time, uint32_t r, uint32_t si, uint32_t& cursor, uint32_t& t,
+                                 uint16_t& tday) const {
     auto const minutes = static_cast<int>(base) * 1440 + time;
     auto const day = static_cast<uint16_t>(minutes / 1440);
     auto const mam = static_cast<int16_t>(minutes % 1440);
     auto const t0 = T->route_tr_from[r], n_t = T->route_tr_to[r] - t0;
     auto const* col = T->st + T->route_st_from[r] + n_t * (si * 2u - (fwd ? 1u : 0u));
-    uint32_t lo = 0;
-    if (T->route_sorted[r]) {
-      uint32_t hi = n_t;
-      while (lo < hi) {
-        auto const mid = (lo + hi) >> 1;
-        if ((col[mid] >> 5) < static_cast<uint16_t>(mam < 0 ? 0 : mam)) lo = mid + 1;
-        else hi = mid;
-      }
-    }
-    for (auto x = lo; x < n_t; ++x) {
+    for (auto x = cursor; x < n_t; ++x) {
       auto const cnt = delta_count(col[x]);
       auto const m = static_cast<int16_t>(cnt % 1440);
       if (m != mam) {
         if (T->route_sorted[r] && m > mam) break;
         continue;
       }
-      auto const tday = static_cast<uint16_t>(static_cast<int>(day) - cnt / 1440);
-      auto const t = t0 + x;
-      if (!bf_test(*T, T->transport_bf[t], tday)) continue;
-      if (find_start_in_prev_round(k, t, tday, si, out)) return true;
+      auto const td = static_cast<uint16_t>(static_cast<int>(day) - cnt / 1440);
+      if (!bf_test(*T, T->transport_bf[t0 + x], td)) continue;
+      cursor = x + 1u;
+      t = t0 + x;
+      tday = td;
+      return true;
     }
+    cursor = n_t;
     return false;
   }
 
-  // reconstruct.cc:375-545: the (route, stop position) pairs of location l
-  // in the reference's order, 32 per step, first success wins
-  __device__ bool get_transport(unsigned k, uint32_t l, int time, b2r_leg& out) const {
-    auto const b = T->lrs_idx[l], e = T->lrs_idx[l + 1];
-    for (auto base = b; base < e; base += 32u) {
-      auto const x = base + lane;
-      bool ok = false;
-      b2r_leg leg{};
-      if (x < e) {
-        auto const r = T->lrs_route[x];
-        auto const i = static_cast<uint32_t>(T->lrs_stop[x]);
-        auto const w = stopw(r, i);
-        auto const n = n_stops(r);
-        if (!((fwd && (i == 0u || !B2R_STOP_OUT(w))) || (!fwd && (i + 1u == n || !B2R_STOP_IN(w))))) {
-          ok = get_route_transport(k, time, r, i, leg);
+  // get_transport (reconstruct.cc:375-545) for a list of footpath
+  // candidates, tried in order: candidate f reaches location `target(f)` at
+  // `time(f)`; its (route, stop position) pairs are visited in the
+  // reference's order.  All pairs of all candidates form one sequence that
+  // the lanes take 32 at a time; the first success in sequence order wins.
+  // get(f, target, time) describes candidate f (lane-local); returns the
+  // winning candidate or -1.
+  template <typename Get>
+  __device__ int get_transport(unsigned k, uint32_t n_cand, Get&& get, b2r_leg& out) const {
+    for (auto f0 = 0u; f0 < n_cand; f0 += 32u) {
+      // lane f: candidate f0 + f, its pair range and the inclusive prefix sum
+      auto const f = f0 + lane;
+      uint32_t tg = 0, pb = 0, cnt = 0;
+      int tm = 0;
+      if (f < n_cand) {
+        get(f, tg, tm);
+        pb = T->lrs_idx[tg];
+        cnt = T->lrs_idx[tg + 1] - pb;
+      }
+      auto end = cnt;
+      for (auto o = 1u; o < 32u; o <<= 1) {
+        auto const v = __shfl_up_sync(kFull, end, o);
+        if (lane >= o) end += v;
+      }
+      auto const total = __shfl_sync(kFull, end, 31);
+      for (auto p0 = 0u; p0 < total; p0 += 32u) {
+        auto const p = p0 + lane;
+        // owner candidate of pair p: the first lane whose prefix end > p
+        uint32_t owner = 0;
+        for (auto b = 16u; b > 0u; b >>= 1) {
+          auto const probe = owner + b - 1u;
+          auto const e = __shfl_sync(kFull, end, static_cast<int>(probe));
+          if (e <= p) owner += b;
+        }
+        auto const o_tm = __shfl_sync(kFull, tm, static_cast<int>(owner));
+        auto const o_pb = __shfl_sync(kFull, pb, static_cast<int>(owner));
+        auto const o_end = __shfl_sync(kFull, end, static_cast<int>(owner));
+        auto const o_cnt = __shfl_sync(kFull, cnt, static_cast<int>(owner));
+        bool has = false;
+        uint32_t r = 0, i = 0, cursor = 0, t = 0;
+        uint16_t tday = 0;
+        if (p < total) {
+          auto const x = o_pb + (p - (o_end - o_cnt));
+          r = T->lrs_route[x];
+          i = static_cast<uint32_t>(T->lrs_stop[x]);
+          auto const w = stopw(r, i);
+          auto const n = n_stops(r);
+          if (!((fwd && (i == 0u || !B2R_STOP_OUT(w))) || (!fwd && (i + 1u == n || !B2R_STOP_IN(w))))) {
+            cursor = first_cursor(o_tm, r, i);
+            has = next_transport(o_tm, r, i, cursor, t, tday);
+          }
+        }
+        for (auto m = __ballot_sync(kFull, has); m != 0u; m = __ballot_sync(kFull, has)) {
+          auto const src = static_cast<int>(__ffs(m) - 1);
+          auto const bt = __shfl_sync(kFull, t, src);
+          auto const bday = static_cast<uint16_t>(__shfl_sync(kFull, static_cast<uint32_t>(tday), src));
+          auto const bi = __shfl_sync(kFull, i, src);
+          if (find_start_in_prev_round(k, bt, bday, bi, out)) {
+            return static_cast<int>(f0 + __shfl_sync(kFull, owner, src));
+          }
+          if (static_cast<int>(lane) == src) has = next_transport(o_tm, r, i, cursor, t, tday);
         }
       }
-      auto const m = __ballot_sync(kFull, ok);
-      if (m != 0u) {
-        out = shfl_leg(leg, __ffs(m) - 1);
-        return true;
-      }
     }
-    return false;
+    return -1;
   }
 
-  // reconstruct.cc:547-666 (no vias)
+  // check_fp (reconstruct.cc:547-666, no vias) for one footpath
   __device__ bool check_fp(unsigned k, uint32_t l, int curr_time, uint32_t target, int dur_raw,
                            bool adjust, b2r_leg& fp_leg, b2r_leg& tr_leg) const {
     auto const d = adjust ? static_cast<int>(adjusted<int16_t>(sl->tts, static_cast<int16_t>(dur_raw)))
                           : static_cast<int>(static_cast<int16_t>(dur_raw));
     auto const fp_start = static_cast<int>(static_cast<int16_t>(curr_time - dir(d)));
-    if (!get_transport(k, target, fp_start, tr_leg)) return false;
+    auto const one = [&](uint32_t, uint32_t& tg, int& tm) {
+      tg = target;
+      tm = fp_start;
+    };
+    if (get_transport(k, 1u, one, tr_leg) < 0) return false;
     fp_leg = make_leg(target, l, delta_to_unix(fp_start), delta_to_unix(fp_start + dir(d)));
     set_fp(fp_leg, target, dur_raw);
     return true;
@@ -279,19 +347,43 @@ struct recon_ctx {
       }
       return false;
     }
+    // candidate 0: staying at l (transfer time, or none at the destination);
+    // candidates 1..: the footpaths into l, in order
     auto const same = (k == j->transfers + 1u)
                           ? 0
                           : static_cast<int>(adjusted<uint8_t>(sl->tts, T->transfer_time[l]));
-    if (check_fp(k, l, curr, l, same, false, fp_leg, tr_leg)) return true;
     auto const* idx = fwd ? T->fp_in_idx : T->fp_out_idx;
     auto const* fps = fwd ? T->fp_in : T->fp_out;
-    for (auto i = idx[l]; i != idx[l + 1]; ++i) {
-      if (check_fp(k, l, curr, B2R_FP_TARGET(fps[i]), static_cast<int>(B2R_FP_DURATION(fps[i])),
-                   true, fp_leg, tr_leg)) {
-        return true;
+    auto const fb = idx[l];
+    auto const raw = [&](uint32_t f, uint32_t& tg, int& dur) {
+      if (f == 0u) {
+        tg = l;
+        dur = same;
+      } else {
+        auto const w = fps[fb + f - 1u];
+        tg = B2R_FP_TARGET(w);
+        dur = static_cast<int>(B2R_FP_DURATION(w));
       }
-    }
-    return false;
+    };
+    auto const eff = [&](uint32_t f, int dur) {
+      return f == 0u ? static_cast<int>(static_cast<int16_t>(dur))
+                     : static_cast<int>(adjusted<int16_t>(sl->tts, static_cast<int16_t>(dur)));
+    };
+    auto const get = [&](uint32_t f, uint32_t& tg, int& tm) {
+      int dur = 0;
+      raw(f, tg, dur);
+      tm = static_cast<int>(static_cast<int16_t>(curr - dir(eff(f, dur))));
+    };
+    auto const f = get_transport(k, 1u + (idx[l + 1] - fb), get, tr_leg);
+    if (f < 0) return false;
+    uint32_t tg = 0;
+    int dur = 0;
+    raw(static_cast<uint32_t>(f), tg, dur);
+    auto const d = eff(static_cast<uint32_t>(f), dur);
+    auto const fp_start = static_cast<int>(static_cast<int16_t>(curr - dir(d)));
+    fp_leg = make_leg(tg, l, delta_to_unix(fp_start), delta_to_unix(fp_start + dir(d)));
+    set_fp(fp_leg, tg, dur);
+    return true;
   }
 
   // reconstruct.cc:30-160 (no vias)
@@ -481,50 +573,91 @@ struct recon_ctx {
     return __dsub_rn(w, __dmul_rn(0.2, static_cast<double>(b)));
   }
 
-  __device__ void opt_transfers() {  // :285-450 (no vias)
+  // optimize_footpaths.cc:285-450 (no vias).  For each transport-footpath-
+  // transport triple the (exit stop, entry stop) pairs are split across the
+  // lanes; pairs do not depend on each other except through the running best
+  // penalty, so the sequential loop keeps the first pair (in its order) with
+  // the smallest penalty below the initial one, which is what the warp
+  // reduction over (penalty, pair index) selects.  Called by the whole warp;
+  // lane 0 writes the legs.
+  __device__ void opt_transfers() {
     for (auto i = 0; i + 2 < n_legs; ++i) {
-      auto& lf = legs[i];
-      auto& lp = legs[i + 1];
-      auto& lt = legs[i + 2];
+      __syncwarp();
+      auto const lf = legs[i];
+      auto const lp = legs[i + 1];
+      auto const lt = legs[i + 2];
       if (lf.kind != B2R_LEG_TRANSPORT || lp.kind != B2R_LEG_FOOTPATH || lt.kind != B2R_LEG_TRANSPORT) continue;
       auto const from_start = static_cast<uint32_t>(lf.stop_from + 1u);
       auto const from_size = n_stops(r_of(lf));
       auto const to_end = static_cast<uint32_t>(lt.stop_to - 1u);
-      auto pbest = penalty(lp.duration, lt.dep_time - lp.arr_time, lf.from, lt.to);
-      for (auto sf = from_start; sf < from_size; ++sf) {
-        if (!B2R_STOP_OUT(word_at(lf, sf))) continue;
-        for (auto s2 = 0u; s2 < to_end; ++s2) {
-          if (!B2R_STOP_IN(word_at(lt, s2))) continue;
-          auto const a = loc_at(lf, sf), b = loc_at(lt, s2);
-          for (auto x = T->fp_out_idx[a]; x != T->fp_out_idx[a + 1]; ++x) {
-            auto const fp = T->fp_out[x];
-            if (B2R_FP_TARGET(fp) != b) continue;
-            auto const d = static_cast<int>(adjusted<int16_t>(sl->tts, static_cast<int16_t>(B2R_FP_DURATION(fp))));
-            auto const arr = time_at(lf, sf, true);
-            auto const dep = time_at(lt, s2, false);
-            auto const arr_fp = arr + d;
-            if (arr_fp <= dep) {
-              auto const p = penalty(d, dep - arr_fp, a, b);
-              if (p < pbest) {
-                lf.to = a;
-                lf.arr_time = arr;
-                lf.stop_to = static_cast<uint16_t>(sf + 1u);
-                lt.from = b;
-                lt.dep_time = dep;
-                lt.stop_from = static_cast<uint16_t>(s2);
-                lp.from = a;
-                lp.to = b;
-                lp.dep_time = arr;
-                lp.arr_time = arr_fp;
-                set_fp(lp, B2R_FP_TARGET(fp), static_cast<int>(B2R_FP_DURATION(fp)));
-                pbest = p;
-              }
+      auto const pbest0 = penalty(lp.duration, lt.dep_time - lp.arr_time, lf.from, lt.to);
+      auto const n_sf = from_size > from_start ? from_size - from_start : 0u;
+      auto const n_pairs = n_sf * to_end;
+      double best = pbest0;
+      uint32_t best_idx = 0xFFFFFFFFu, best_fp = 0;
+      int32_t best_arr = 0, best_dep = 0, best_d = 0;
+      for (auto x = lane; x < n_pairs; x += 32u) {
+        auto const sf = from_start + x / to_end, s2 = x % to_end;
+        if (!B2R_STOP_OUT(word_at(lf, sf)) || !B2R_STOP_IN(word_at(lt, s2))) continue;
+        auto const a = loc_at(lf, sf), b = loc_at(lt, s2);
+        for (auto y = T->fp_out_idx[a]; y != T->fp_out_idx[a + 1]; ++y) {
+          auto const fp = T->fp_out[y];
+          if (B2R_FP_TARGET(fp) != b) continue;
+          auto const d = static_cast<int>(adjusted<int16_t>(sl->tts, static_cast<int16_t>(B2R_FP_DURATION(fp))));
+          auto const arr = time_at(lf, sf, true);
+          auto const dep = time_at(lt, s2, false);
+          auto const arr_fp = arr + d;
+          if (arr_fp <= dep) {
+            auto const pen = penalty(d, dep - arr_fp, a, b);
+            if (pen < best) {  // lanes visit their pairs in increasing order
+              best = pen;
+              best_idx = x;
+              best_fp = fp;
+              best_arr = arr;
+              best_dep = dep;
+              best_d = d;
             }
-            break;
           }
+          break;
         }
       }
+      // (penalty, pair index) minimum over the warp
+      auto win_pen = best;
+      auto win_idx = best_idx;
+      for (auto o = 16; o > 0; o >>= 1) {
+        auto const op = __shfl_xor_sync(kFull, win_pen, o);
+        auto const oi = __shfl_xor_sync(kFull, win_idx, o);
+        if (op < win_pen || (op == win_pen && oi < win_idx)) {
+          win_pen = op;
+          win_idx = oi;
+        }
+      }
+      if (win_idx == 0xFFFFFFFFu) continue;  // no pair below the initial penalty
+      auto const owner = static_cast<int>(win_idx % 32u);
+      auto const w_fp = __shfl_sync(kFull, best_fp, owner);
+      auto const w_arr = __shfl_sync(kFull, best_arr, owner);
+      auto const w_dep = __shfl_sync(kFull, best_dep, owner);
+      auto const w_d = __shfl_sync(kFull, best_d, owner);
+      if (lane == 0) {
+        auto const sf = from_start + win_idx / to_end, s2 = win_idx % to_end;
+        auto const a = loc_at(lf, sf), b = loc_at(lt, s2);
+        auto& wf = legs[i];
+        auto& wp = legs[i + 1];
+        auto& wt = legs[i + 2];
+        wf.to = a;
+        wf.arr_time = w_arr;
+        wf.stop_to = static_cast<uint16_t>(sf + 1u);
+        wt.from = b;
+        wt.dep_time = w_dep;
+        wt.stop_from = static_cast<uint16_t>(s2);
+        wp.from = a;
+        wp.to = b;
+        wp.dep_time = w_arr;
+        wp.arr_time = w_arr + w_d;
+        set_fp(wp, B2R_FP_TARGET(w_fp), static_cast<int>(B2R_FP_DURATION(w_fp)));
+      }
     }
+    __syncwarp();
   }
 
   // reconstruct.cc:792-877 + optimize_footpaths(journey_q)
@@ -549,30 +682,32 @@ struct recon_ctx {
       if (!find_start_footpath(init, has)) failed = true;
       else if (has) push(init);
     }
-    if (failed || lane != 0) return;
-    if (fwd) {
-      for (auto a = 0, b = n_legs - 1; a < b; ++a, --b) {
-        auto const x = legs[a];
-        legs[a] = legs[b];
-        legs[b] = x;
+    if (failed) return;
+    if (lane == 0) {
+      if (fwd) {
+        for (auto a = 0, b = n_legs - 1; a < b; ++a, --b) {
+          auto const x = legs[a];
+          legs[a] = legs[b];
+          legs[b] = x;
+        }
+      } else {
+        for (auto i = 1; i < n_legs; ++i) {
+          if (legs[i].kind != B2R_LEG_FOOTPATH) continue;
+          auto const diff = legs[i].dep_time - legs[i - 1].arr_time;
+          legs[i].dep_time -= diff;
+          legs[i].arr_time -= diff;
+        }
       }
-    } else {
-      for (auto i = 1; i < n_legs; ++i) {
-        if (legs[i].kind != B2R_LEG_FOOTPATH) continue;
-        auto const diff = legs[i].dep_time - legs[i - 1].arr_time;
-        legs[i].dep_time -= diff;
-        legs[i].arr_time -= diff;
-      }
+      // optimize_footpaths on the journey query (flipped for backward search)
+      auto const* jq_start = fwd ? start_offs() : dest_offs();
+      auto const n_jq_start = fwd ? sl->n_soff : sl->n_doff;
+      auto const* jq_dest = fwd ? dest_offs() : start_offs();
+      auto const n_jq_dest = fwd ? sl->n_doff : sl->n_soff;
+      opt_initial_departure(jq_start, n_jq_start);
+      opt_initial_start_footpath();
+      opt_last_arrival(jq_dest, n_jq_dest);
+      opt_final_egress_footpath();
     }
-    // optimize_footpaths on the journey query (flipped for backward search)
-    auto const* jq_start = fwd ? start_offs() : dest_offs();
-    auto const n_jq_start = fwd ? sl->n_soff : sl->n_doff;
-    auto const* jq_dest = fwd ? dest_offs() : start_offs();
-    auto const n_jq_dest = fwd ? sl->n_doff : sl->n_soff;
-    opt_initial_departure(jq_start, n_jq_start);
-    opt_initial_start_footpath();
-    opt_last_arrival(jq_dest, n_jq_dest);
-    opt_final_egress_footpath();
     opt_transfers();
   }
 };
