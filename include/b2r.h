@@ -387,6 +387,13 @@ typedef struct b2r_batch_stats {
 } b2r_batch_stats;
 int b2r_last_batch_stats(const b2r_engine* e, b2r_batch_stats* s);
 
+/* Profiling engines (b2r_engine_config::profile = 1): per route-scan launch of
+ * the last b2r_search_batch, its CUDA-event time, the marked (route, query
+ * group) entries it scanned and the (route, query) stop steps it made.  *n
+ * receives the number of launches; at most cap are written. */
+int b2r_last_batch_scan_profile(const b2r_engine* e, double* scan_ms, uint64_t* entries,
+                                uint64_t* stop_visits, uint32_t cap, uint32_t* n);
+
 /* ------------------------------------------- host timetable construction */
 /* Host-side timetable builder (not on the hot path): the synthetic
  * generator and nigiri's finalize() derivations (footpaths_in,

@@ -152,7 +152,7 @@ EXPORTS = [
     "b2r_tt_generate", "b2r_tt_build", "b2r_tt_save", "b2r_tt_load",
     "b2r_tt_desc", "b2r_tt_destroy", "b2r_queries_generate",
     "b2r_queries_count", "b2r_queries_get", "b2r_queries_destroy",
-    "b2r_one_to_all_noalloc",
+    "b2r_one_to_all_noalloc", "b2r_last_batch_scan_profile",
 ]
 
 
@@ -188,6 +188,9 @@ def _declare(lib):
         "b2r_queries_count": (C.c_uint32, [vp]),
         "b2r_queries_get": (C.POINTER(Query), [vp, C.c_uint32]),
         "b2r_queries_destroy": (C.c_int, [vp]),
+        "b2r_last_batch_scan_profile": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_uint64),
+                                                  C.POINTER(C.c_uint64), C.c_uint32,
+                                                  C.POINTER(C.c_uint32)]),
         "b2r_one_to_all_noalloc": (C.c_int, [vp, C.POINTER(Query), C.POINTER(C.c_int16), C.c_uint64,
                                              C.POINTER(C.c_uint32), C.POINTER(C.c_int32), vp]),
     }

@@ -125,6 +125,9 @@ struct b2r_engine {
   size_t prof_used{0};
   std::vector<cudaEvent_t> prof_rc_ev;  // around the reconstruction launches
   size_t prof_rc_used{0};
+  // per route-scan launch: marked entries, cumulative stop visits
+  static constexpr uint32_t kProfRows = 4096;
+  unsigned long long* d_prof_rows{};
   std::chrono::steady_clock::time_point batch_t0;
 
   // results of the last batch / serving tickets
@@ -270,6 +273,13 @@ __global__ void k_summary(dev::state st, b2r_engine::summary_t* out) {
   out[s].n_journeys = st.slots[s].n_journeys;
 }
 
+// profiling engines: the marked-entry count and cumulative stop visits after
+// route-scan launch `idx`
+__global__ void k_prof_row(dev::state st, unsigned long long* rows, uint32_t idx) {
+  rows[2 * idx] = st.counters[dev::C_R];
+  rows[2 * idx + 1] = st.prof[0];
+}
+
 // export: per listed slot, journey headers + leg blocks (+ one-to-all rows)
 struct exp_item {
   uint32_t slot;
@@ -367,7 +377,12 @@ void enqueue_superstep(b2r_engine& e, cudaStream_t s) {
     B2R_CUDA(cudaEventRecord(ev_a, s));
   }
   dev::k_route_scan<<<e.sms * 8, 256, 0, s>>>(st);
-  if (e.cfg.profile) B2R_CUDA(cudaEventRecord(ev_b, s));
+  if (e.cfg.profile) {
+    B2R_CUDA(cudaEventRecord(ev_b, s));
+    auto const idx = static_cast<uint32_t>(e.prof_used / 2 - 1);
+    if (idx < b2r_engine::kProfRows) k_prof_row<<<1, 1, 0, s>>>(st, e.d_prof_rows, idx);
+  }
+  dev::k_list_reached<<<e.sms * 8, 256, 0, s>>>(st);
   dev::k_clear_x<<<list_blocks, 256, 0, s>>>(st);
   dev::k_reset_x<<<1, 32, 0, s>>>(st);
   dev::k_transfers_pre<<<slot_blocks, 128, 0, s>>>(st);
@@ -393,7 +408,7 @@ void enqueue_superstep(b2r_engine& e, cudaStream_t s) {
   dev::k_next<<<slot_blocks, 128, 0, s>>>(st);
   k_summary<<<slot_blocks, 128, 0, s>>>(st, e.d_summary);
 }
-constexpr uint64_t kLaunchesPerStep = 19;
+constexpr uint64_t kLaunchesPerStep = 20;
 
 // --------------------------------------------------------- admission
 size_t admission_bytes(b2r_engine const& e, prepped_query const& p) {
@@ -1291,6 +1306,7 @@ int b2r_engine_create(b2r_timetable* tt, const b2r_engine_config* cfg_in, b2r_en
       B2R_CUDA(cudaMemset(st.prof, 0, 8 * sizeof(unsigned long long)));
       al(e->d_exp_list, S);
       al(e->d_keep, e->max_j);
+      if (cfg.profile) al(e->d_prof_rows, 2 * b2r_engine::kProfRows);
       B2R_CUDA(cudaMemset(st.slots, 0, S * sizeof(b2r::dev::slot_t)));
       B2R_CUDA(cudaMemset(st.rt, 0xFF, static_cast<size_t>(b2r::dev::kK) * nl * S * 4));
       B2R_CUDA(cudaMemset(st.best, 0xFF, static_cast<size_t>(nl) * S * 4));
@@ -1437,6 +1453,36 @@ int b2r_search_plain(b2r_engine* e, const b2r_query* q, b2r_result* out) {
     } catch (b2r::cuda_error const& ex) {
       return b2r::fail(B2R_ERR_CUDA, ex.what());
     }
+  });
+}
+
+int b2r_last_batch_scan_profile(const b2r_engine* e, double* scan_ms, uint64_t* entries,
+                                uint64_t* stop_visits, uint32_t cap, uint32_t* n) {
+  B2R_API_GUARD({
+    if (e == nullptr || n == nullptr) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
+    if (!e->cfg.profile) return b2r::fail(B2R_ERR_UNSUPPORTED, "engine was not created with profile = 1");
+    auto const launches = static_cast<uint32_t>(std::min<size_t>(e->prof_used / 2, b2r_engine::kProfRows));
+    *n = launches;
+    auto const m = std::min(cap, launches);
+    if (m == 0) return B2R_OK;
+    if (scan_ms == nullptr || entries == nullptr || stop_visits == nullptr) {
+      return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null output array");
+    }
+    std::vector<unsigned long long> rows(2 * m);
+    if (cudaMemcpy(rows.data(), e->d_prof_rows, rows.size() * sizeof(unsigned long long),
+                   cudaMemcpyDeviceToHost) != cudaSuccess) {
+      return b2r::fail(B2R_ERR_CUDA, "reading the profile rows failed");
+    }
+    unsigned long long prev = 0;
+    for (auto i = 0U; i != m; ++i) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e->prof_ev[2 * i], e->prof_ev[2 * i + 1]);
+      scan_ms[i] = ms;
+      entries[i] = rows[2 * i];
+      stop_visits[i] = rows[2 * i + 1] - prev;
+      prev = rows[2 * i + 1];
+    }
+    return B2R_OK;
   });
 }
 

@@ -145,65 +145,102 @@ __global__ void k_ctl_marked(state st) {
 
 // ------------------------------------------------------------ route scan
 // update_route, raptor.h:1177-1349 (no vias, no section filters) for every
-// (route, query) pair marked this round.  One thread per marked (route,
-// group of 32 queries) entry walks the route once for each query of the
-// entry's mask, carrying that query's current trip: resident queries are
-// unrelated, so an entry holds few queries and a warp-per-entry scan would
-// leave most lanes idle.  Labels are combined with atomicMin and marks with
-// atomicOr, so the order of the pairs does not matter.
-__global__ void __launch_bounds__(256) k_route_scan(state st) {
-  auto const tid = blockIdx.x * blockDim.x + threadIdx.x;
-  auto const n_threads = gridDim.x * blockDim.x;
+// (route, query) pair marked this round.  A warp takes 32 marked (route,
+// group of 32 queries) entries, lists their (route, query) pairs and gives
+// one pair to each lane per pass: resident queries are unrelated, so an
+// entry holds few queries, and a lane per query of one entry would leave
+// most lanes idle.  Each lane walks its route in search direction carrying
+// its query's current trip, with the next stops' words, station marks and
+// lower bounds loaded ahead.  Labels are combined with atomicMin and marks
+// with atomicOr, so the order of the pairs does not matter.
+__global__ void __launch_bounds__(256, 3) k_route_scan(state st) {
+  auto const lane = threadIdx.x & 31u;
+  auto const warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  auto const n_warps = (gridDim.x * blockDim.x) >> 5;
   auto const nr = st.counters[C_R];
   auto const& T = st.tt;
   uint32_t p_ev = 0, p_days = 0, p_writes = 0, p_stops = 0;
-  for (auto w = tid; w < nr; w += n_threads) {
-    auto const e = st.rlist[w];
-    auto const g = e % st.G, r = e / st.G;
-    auto mask = st.R[e];
-    st.R[e] = 0u;
-    auto const sb = T.route_stop_idx[r];
-    auto const n = T.route_stop_idx[r + 1] - sb;
-    auto const t0 = T.route_tr_from[r];
-    auto const n_t = T.route_tr_to[r] - t0;
-    auto const* colbase = T.st + T.route_st_from[r];
-    while (mask != 0u) {
-      auto const b = static_cast<uint32_t>(__ffs(mask) - 1);
-      mask &= mask - 1u;
+  for (auto w0 = warp * 32u; w0 < nr; w0 += n_warps * 32u) {
+    // lane: entry w0 + lane, its query mask and the inclusive prefix sum
+    auto const w = w0 + lane;
+    uint32_t e = 0, mask = 0;
+    if (w < nr) {
+      e = st.rlist[w];
+      mask = st.R[e];
+      st.R[e] = 0u;
+    }
+    auto const cnt = static_cast<uint32_t>(__popc(mask));
+    auto end = cnt;
+    for (auto o = 1u; o < 32u; o <<= 1) {
+      auto const v = __shfl_up_sync(kFull, end, o);
+      if (lane >= o) end += v;
+    }
+    auto const total = __shfl_sync(kFull, end, 31);
+    for (auto p0 = 0u; p0 < total; p0 += 32u) {
+      auto const p = p0 + lane;
+      uint32_t owner = 0;  // first lane whose prefix end exceeds p
+      for (auto b = 16u; b > 0u; b >>= 1) {
+        if (__shfl_sync(kFull, end, static_cast<int>(owner + b - 1u)) <= p) owner += b;
+      }
+      auto const o_e = __shfl_sync(kFull, e, static_cast<int>(owner));
+      auto o_mask = __shfl_sync(kFull, mask, static_cast<int>(owner));
+      auto const o_first = __shfl_sync(kFull, end, static_cast<int>(owner)) -
+                           __shfl_sync(kFull, cnt, static_cast<int>(owner));
+      if (p >= total) continue;
+      for (auto x = p - o_first; x != 0u; --x) o_mask &= o_mask - 1u;
+      auto const b = static_cast<uint32_t>(__ffs(o_mask) - 1);
+      auto const g = o_e % st.G, r = o_e / st.G;
       auto const s = g * 32u + b;
       auto const ln = st.lanes[s];
       if (!ln.run) continue;
       auto const bit = 1u << b;
       auto const fwd = ln.fwd != 0;
       auto const k = static_cast<uint32_t>(ln.k);
+      auto const sb = T.route_stop_idx[r];
+      auto const n = T.route_stop_idx[r + 1] - sb;
+      auto const n_t = T.route_tr_to[r] - T.route_tr_from[r];
+      auto const* colbase = T.st + T.route_st_from[r];
+      auto const stop_word = [&](uint32_t i) { return T.route_stops[sb + (fwd ? i : n - 1u - i)]; };
       bool et_valid = false;
       uint32_t et_off = 0;
       uint16_t et_day = 0;
+      uint16_t ev = 0;  // arrival event of the current trip at this stop
+      // loads ahead: stop word two stops ahead, mark, bound and the current
+      // trip's arrival event one ahead
+      auto stp = stop_word(0);
+      auto xw = st.X[B2R_STOP_LOC(stp) * st.G + g];
+      auto lbv = st.lb[li(st, B2R_STOP_LOC(stp), s)];
+      auto stp_next = n > 1u ? stop_word(1) : 0u;
       for (auto i = 0u; i != n; ++i) {
         ++p_stops;
+        auto const stp_after = i + 2u < n ? stop_word(i + 2u) : 0u;
+        uint32_t xw_next = 0;
+        uint16_t lb_next = 0;
+        if (i + 1u < n) {
+          auto const ln_next = B2R_STOP_LOC(stp_next);
+          xw_next = st.X[ln_next * st.G + g];
+          lb_next = st.lb[li(st, ln_next, s)];
+        }
         auto const si = fwd ? i : n - 1u - i;
-        auto const stp = T.route_stops[sb + si];
         auto const l = B2R_STOP_LOC(stp);
         auto const can_finish = fwd ? B2R_STOP_OUT(stp) : B2R_STOP_IN(stp);
         auto const can_start = fwd ? B2R_STOP_IN(stp) : B2R_STOP_OUT(stp);
         bool arrival_ran = false;
         if (et_valid && can_finish) {
           arrival_ran = true;
-          auto const ev = colbase[n_t * (si * 2u - (fwd ? 1u : 0u)) + et_off];
           auto const by = to_delta_key(fwd, et_day, ln.base, delta_count(ev));
-          auto const lbv = st.lb[li(st, l, s)];
           if (by <= ln.tad_k && lbv != 0xFFFFu && by + static_cast<int>(lbv) <= ln.tad_k) {
             auto const word = enc(ln.gtag, by);
             auto* tp = &st.tmp[li(st, l, s)];
-            if (word < *tp) {
-              atomicMin(tp, word);
-              ++p_writes;
+            if (st.profile) {
+              if (word < atomicMin(tp, word)) ++p_writes;
+            } else {
+              atomicMin(tp, word);  // result unused: no round trip
             }
-            mark(st, st.Y, st.ylist, C_Y, l * st.G + g, bit);
+            atomicOr(&st.Y[l * st.G + g], bit);  // listed by k_list_reached
           }
         }
-        if (i + 1u != n && can_start && (st.X[l * st.G + g] & bit)) {
-          auto const lbv = st.lb[li(st, l, s)];
+        if (i + 1u != n && can_start && (xw & bit)) {
           if (lbv == 0xFFFFu) break;  // raptor.h:1309-1311: no later stop of this query
           auto const board_col = n_t * (si * 2u - (fwd ? 0u : 1u));
           auto const et_time =
@@ -234,6 +271,14 @@ __global__ void __launch_bounds__(256) k_route_scan(state st) {
             }
           }
         }
+        if (et_valid && i + 1u < n) {  // the next stop's arrival event of the (new) current trip
+          auto const si_next = fwd ? i + 1u : n - 2u - i;
+          ev = colbase[n_t * (si_next * 2u - (fwd ? 1u : 0u)) + et_off];
+        }
+        stp = stp_next;
+        stp_next = stp_after;
+        xw = xw_next;
+        lbv = lb_next;
       }
     }
   }
@@ -247,13 +292,31 @@ __global__ void __launch_bounds__(256) k_route_scan(state st) {
       p_writes += __shfl_xor_sync(kFull, p_writes, o);
       steps_max = max(steps_max, __shfl_xor_sync(kFull, steps_max, o));
     }
-    if ((threadIdx.x & 31u) == 0) {
+    if (lane == 0) {
       atomicAdd(&st.prof[0], static_cast<unsigned long long>(p_stops));
       atomicAdd(&st.prof[1], static_cast<unsigned long long>(p_ev));
       atomicAdd(&st.prof[2], static_cast<unsigned long long>(p_days));
       atomicAdd(&st.prof[3], static_cast<unsigned long long>(p_writes));
       atomicAdd(&st.prof[5], static_cast<unsigned long long>(steps_max));  // warp stop steps
     }
+  }
+}
+
+// frontier list of the stations reached by the route scan: every nonzero
+// route-reached word (location, group), one counter add per warp
+__global__ void k_list_reached(state st) {
+  auto const lane = threadIdx.x & 31u;
+  auto const n = st.tt.n_loc * st.G;
+  auto const stride = gridDim.x * blockDim.x;
+  for (auto i0 = blockIdx.x * blockDim.x; i0 < n; i0 += stride) {
+    auto const i = i0 + threadIdx.x;
+    auto const on = i < n && st.Y[i] != 0u;
+    auto const m = __ballot_sync(kFull, on);
+    if (m == 0u) continue;
+    uint32_t at = 0;
+    if (lane == 0) at = atomicAdd(&st.counters[C_Y], static_cast<uint32_t>(__popc(m)));
+    at = __shfl_sync(kFull, at, 0);
+    if (on) st.ylist[at + static_cast<uint32_t>(__popc(m & ((1u << lane) - 1u)))] = i;
   }
 }
 

@@ -254,6 +254,16 @@ class Engine:
         _check(A.lib().b2r_last_batch_stats(self.handle, C.byref(s)))
         return s
 
+    def scan_profile(self, cap: int = 4096):
+        """Per route-scan launch of the last batch (profiling engines):
+        [(milliseconds, marked entries, stop visits)]."""
+        ms = (C.c_double * cap)()
+        ent = (C.c_uint64 * cap)()
+        vis = (C.c_uint64 * cap)()
+        n = C.c_uint32()
+        _check(A.lib().b2r_last_batch_scan_profile(self.handle, ms, ent, vis, cap, C.byref(n)))
+        return [(ms[i], ent[i], vis[i]) for i in range(min(cap, n.value))]
+
 
 def _journeys(res: A.Result) -> List[Journey]:
     out = []
