@@ -139,15 +139,10 @@ struct b2r_engine {
   };
   std::vector<result_store> results;
 
-  // serving
-  std::mutex mu;
-  std::condition_variable cv;
-  std::thread driver;
-  bool serving{false}, stop_flag{false};
-  uint64_t next_ticket{1};
-  std::deque<std::pair<uint64_t, b2r::prepped_query>> pending;
-  std::unordered_map<uint64_t, result_store> done;
-  std::string driver_error;
+  // serving (b2r_serve_start .. b2r_serve_stop): driver thread, preparation
+  // pool and tickets; type-erased because the state is defined further down
+  bool serving{false};
+  std::shared_ptr<void> serve;
 
   ~b2r_engine();
 };
@@ -813,52 +808,53 @@ void on_phase_done(b2r_engine& e, query_run& q, exported const& x) {
 }  // namespace
 
 // ------------------------------------------------------------- the loop
+// a new interval-extension phase for the query in slot s (search.h:283-316)
+void rearm(b2r_engine& e, uint32_t s, query_run& q, cudaStream_t st) {
+  // new phase: upload the new starts (and journeys kept), keep the rt
+  // generation unless reset_arrivals (raptor.h:174-177)
+  auto const tad_keep = !q.reset_arrivals;
+  slot_t cur{};
+  e.d2h_bytes += sizeof(slot_t);
+  B2R_CUDA(cudaMemcpyAsync(&cur, e.st.slots + s, sizeof(slot_t), cudaMemcpyDeviceToHost, st));
+  B2R_CUDA(cudaStreamSynchronize(st));
+  if (q.reset_arrivals) {
+    if (e.gen_query[s] >= 0xFFFEu) throw std::runtime_error("query generation exhausted");
+    cur.gen_query = ++e.gen_query[s];
+    for (auto& x : cur.tad) x = dev::kKeyInv;
+  }
+  (void)tad_keep;
+  cur.state = dev::S_START;
+  cur.iv_from = q.p.iv_from;
+  cur.iv_to = q.p.iv_to;
+  cur.need_sweep = q.reset_arrivals ? 0 : 1;
+  cur.early_term = 0;
+  cur.next_start = 0;
+  cur.n_starts = static_cast<uint32_t>(q.p.starts.size());
+  if (cur.n_starts > e.max_starts) throw std::runtime_error("start capacity exceeded");
+  std::vector<dev::start_rec> starts(q.p.starts.size());
+  for (auto j = 0U; j != starts.size(); ++j) {
+    starts[j] = {q.p.starts[j].time_at_start, q.p.starts[j].time_at_stop, q.p.starts[j].stop};
+  }
+  B2R_CUDA(cudaMemcpyAsync(e.st.start_pool + cur.starts_off, starts.data(),
+                           starts.size() * sizeof(dev::start_rec), cudaMemcpyHostToDevice, st));
+  if (q.keep.size() > e.max_j) throw std::runtime_error("journey capacity exceeded");
+  auto* dj = e.d_keep;  // engine-owned, reused (this function synchronises)
+  B2R_CUDA(cudaMemcpyAsync(dj, q.keep.data(), q.keep.size() * sizeof(dev::journey_rec),
+                           cudaMemcpyHostToDevice, st));
+  k_set_journeys<<<1, 32, 0, st>>>(e.st, s, dj, static_cast<uint32_t>(q.keep.size()));
+  B2R_CUDA(cudaMemcpyAsync(e.st.slots + s, &cur, sizeof(slot_t), cudaMemcpyHostToDevice, st));
+  B2R_CUDA(cudaStreamSynchronize(st));
+  e.h2d_bytes += starts.size() * sizeof(dev::start_rec) + q.keep.size() * sizeof(dev::journey_rec) +
+                 sizeof(slot_t);
+  q.rearm = false;
+}
+
 struct batch_runner {
   b2r_engine& e;
   std::vector<query_run>& runs;
   bool use_graph;
   uint64_t launches{0}, steps{0};
   double busy_ms{0};  // device time of the super-step chunks
-
-  void rearm(uint32_t s, query_run& q, cudaStream_t st) {
-    // new phase: upload the new starts (and journeys kept), keep the rt
-    // generation unless reset_arrivals (raptor.h:174-177)
-    auto const tad_keep = !q.reset_arrivals;
-    slot_t cur{};
-    e.d2h_bytes += sizeof(slot_t);
-    B2R_CUDA(cudaMemcpyAsync(&cur, e.st.slots + s, sizeof(slot_t), cudaMemcpyDeviceToHost, st));
-    B2R_CUDA(cudaStreamSynchronize(st));
-    if (q.reset_arrivals) {
-      if (e.gen_query[s] >= 0xFFFEu) throw std::runtime_error("query generation exhausted");
-      cur.gen_query = ++e.gen_query[s];
-      for (auto& x : cur.tad) x = dev::kKeyInv;
-    }
-    (void)tad_keep;
-    cur.state = dev::S_START;
-    cur.iv_from = q.p.iv_from;
-    cur.iv_to = q.p.iv_to;
-    cur.need_sweep = q.reset_arrivals ? 0 : 1;
-    cur.early_term = 0;
-    cur.next_start = 0;
-    cur.n_starts = static_cast<uint32_t>(q.p.starts.size());
-    if (cur.n_starts > e.max_starts) throw std::runtime_error("start capacity exceeded");
-    std::vector<dev::start_rec> starts(q.p.starts.size());
-    for (auto j = 0U; j != starts.size(); ++j) {
-      starts[j] = {q.p.starts[j].time_at_start, q.p.starts[j].time_at_stop, q.p.starts[j].stop};
-    }
-    B2R_CUDA(cudaMemcpyAsync(e.st.start_pool + cur.starts_off, starts.data(),
-                             starts.size() * sizeof(dev::start_rec), cudaMemcpyHostToDevice, st));
-    if (q.keep.size() > e.max_j) throw std::runtime_error("journey capacity exceeded");
-    auto* dj = e.d_keep;  // engine-owned, reused (this function synchronises)
-    B2R_CUDA(cudaMemcpyAsync(dj, q.keep.data(), q.keep.size() * sizeof(dev::journey_rec),
-                             cudaMemcpyHostToDevice, st));
-    k_set_journeys<<<1, 32, 0, st>>>(e.st, s, dj, static_cast<uint32_t>(q.keep.size()));
-    B2R_CUDA(cudaMemcpyAsync(e.st.slots + s, &cur, sizeof(slot_t), cudaMemcpyHostToDevice, st));
-    B2R_CUDA(cudaStreamSynchronize(st));
-    e.h2d_bytes += starts.size() * sizeof(dev::start_rec) + q.keep.size() * sizeof(dev::journey_rec) +
-                   sizeof(slot_t);
-    q.rearm = false;
-  }
 
   void run(uint32_t chunk) {
     auto const S = e.S;
@@ -967,7 +963,7 @@ struct batch_runner {
         on_phase_done(e, q, ex[i]);
         q.res.view.latency_ms = now_ms;
         if (q.rearm) {
-          rearm(s, q, st);
+          rearm(e, s, q, st);
         } else {
           retired.push_back(s);
           slot_q[s] = -1;
@@ -1031,6 +1027,188 @@ void fill_out(b2r_engine& e, std::vector<query_run>& runs, b2r_result* out) {
     out[i] = r.view;
   }
 }
+
+// ------------------------------------------------------------- serving
+// Continuous batching: submitted queries are prepared on a host pool and
+// admitted into free slots at super-step boundaries while the queries
+// already resident keep running; finished slots are exported and retired
+// after every chunk of super-steps.  One driver thread owns the device.
+struct serve_item {
+  uint64_t ticket{0};
+  b2r_query q{};
+  std::vector<b2r_offset> start, dest;  // the query's offsets (copied)
+  std::chrono::steady_clock::time_point t_submit;
+  query_run run;
+  bool finished{false};
+};
+
+struct serve_state {
+  explicit serve_state(b2r_engine& eng) : e{eng}, slot_item(eng.S, nullptr) {}
+  b2r_engine& e;
+  std::mutex mu;
+  std::condition_variable cv_prep, cv_driver, cv_done;
+  std::deque<serve_item*> to_prepare, ready;
+  std::unordered_map<uint64_t, std::unique_ptr<serve_item>> items;
+  std::vector<serve_item*> slot_item;
+  uint64_t next_ticket{1};
+  uint64_t unfinished{0};  // submitted, not finished
+  bool stop{false};
+  int failed_status{B2R_OK};
+  std::string failed_msg;
+  std::vector<std::thread> prep_pool;
+  std::thread driver;
+
+  void finish(serve_item& it) {  // with mu held
+    auto& r = it.run.res;
+    r.view.n_journeys = static_cast<uint32_t>(r.journeys.size());
+    r.view.journeys = r.journeys.data();
+    r.view.legs = r.legs.data();
+    r.view.round_times = r.rt_rows.empty() ? nullptr : r.rt_rows.data();
+    r.view.latency_ms =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - it.t_submit).count();
+    it.finished = true;
+    --unfinished;
+  }
+
+  void fail_item(serve_item& it, int status) {  // with mu held
+    it.run.status = status;
+    it.run.res.view.status = status;
+    finish(it);
+  }
+
+  void prep_loop() {
+    auto const lb_mode = static_cast<int>(e.cfg.use_lower_bounds);
+    std::unique_lock<std::mutex> lock{mu};
+    while (true) {
+      cv_prep.wait(lock, [&] { return stop || !to_prepare.empty(); });
+      if (to_prepare.empty()) return;  // stopping and nothing left
+      auto* it = to_prepare.front();
+      to_prepare.pop_front();
+      lock.unlock();
+      auto status = B2R_OK;
+      try {
+        prepare(e.tt->view, it->q, lb_mode, it->run.p);
+      } catch (...) {
+        status = B2R_ERR_INTERNAL;
+      }
+      lock.lock();
+      if (status != B2R_OK) {
+        fail_item(*it, status);
+        cv_done.notify_all();
+        cv_driver.notify_one();  // it may be waiting for the last query to end
+        continue;
+      }
+      ready.push_back(it);
+      cv_driver.notify_one();
+    }
+  }
+
+  void driver_loop() {
+    auto* st = e.stream;
+    auto const chunk = e.cfg.steps_per_sync != 0 ? e.cfg.steps_per_sync : 2U;
+    auto const use_graph = e.cfg.use_graphs != 0 && e.graph != nullptr;
+    try {
+      B2R_CUDA(cudaSetDevice(e.tt->device));
+      while (true) {
+        std::vector<std::pair<uint32_t, prepped_query const*>> adm;
+        bool any_busy = false;
+        {
+          std::unique_lock<std::mutex> lock{mu};
+          auto const has_busy = [&] {
+            for (auto* x : slot_item)
+              if (x != nullptr) return true;
+            return false;
+          };
+          if (!has_busy()) {
+            cv_driver.wait(lock, [&] { return !ready.empty() || (stop && unfinished == 0); });
+            if (ready.empty() && stop && unfinished == 0) return;
+          }
+          for (uint32_t s = 0; s != e.S && !ready.empty(); ++s) {
+            if (slot_item[s] != nullptr) continue;
+            while (!ready.empty()) {
+              auto* it = ready.front();
+              auto const& p = it->run.p;
+              if (p.status != B2R_OK || p.empty_result) {
+                ready.pop_front();
+                it->run.res.view.interval_from = p.iv_from;
+                it->run.res.view.interval_to = p.iv_to;
+                fail_item(*it, p.status);
+                cv_done.notify_all();
+                continue;
+              }
+              if (auto const c = check_capacity(e, p); c != B2R_OK) {
+                ready.pop_front();
+                fail_item(*it, c);
+                cv_done.notify_all();
+                continue;
+              }
+              ready.pop_front();
+              slot_item[s] = it;
+              adm.emplace_back(s, &it->run.p);
+              break;
+            }
+          }
+          any_busy = has_busy();
+        }
+        admit(e, adm, st);
+        if (!any_busy) continue;
+        for (uint32_t c = 0; c != chunk; ++c) {
+          if (use_graph) {
+            B2R_CUDA(cudaGraphLaunch(e.graph, st));
+          } else {
+            enqueue_superstep(e, st);
+            B2R_CUDA(cudaGetLastError());
+          }
+        }
+        B2R_CUDA(cudaMemcpyAsync(e.h_summary, e.d_summary, e.S * sizeof(b2r_engine::summary_t),
+                                 cudaMemcpyDeviceToHost, st));
+        B2R_CUDA(cudaStreamSynchronize(st));
+        std::vector<uint32_t> done_slots, n_js, n_rows;
+        for (uint32_t s = 0; s != e.S; ++s) {
+          if (slot_item[s] == nullptr) continue;
+          auto const state = e.h_summary[s].state;
+          if (state == dev::S_DONE || state == dev::S_ERROR) {
+            done_slots.push_back(s);
+            n_js.push_back(e.h_summary[s].n_journeys);
+            n_rows.push_back(slot_item[s]->run.p.one_to_all ? slot_item[s]->run.p.end_k : 0u);
+          }
+        }
+        if (done_slots.empty()) continue;
+        std::vector<exported> ex;
+        export_slots(e, done_slots, n_js, n_rows, ex, st);
+        std::vector<uint32_t> retired;
+        for (auto i = 0U; i != done_slots.size(); ++i) {
+          auto const s = done_slots[i];
+          auto& it = *slot_item[s];
+          on_phase_done(e, it.run, ex[i]);
+          if (it.run.rearm) {
+            rearm(e, s, it.run, st);
+            continue;
+          }
+          retired.push_back(s);
+          std::lock_guard<std::mutex> lock{mu};
+          slot_item[s] = nullptr;
+          finish(it);
+        }
+        retire(e, retired, st);
+        cv_done.notify_all();
+      }
+    } catch (std::exception const& ex) {
+      std::lock_guard<std::mutex> lock{mu};
+      failed_status = B2R_ERR_CUDA;
+      failed_msg = ex.what();
+      for (auto& [t, it] : items) {
+        if (!it->finished) fail_item(*it, B2R_ERR_CUDA);
+      }
+      for (auto& x : slot_item) x = nullptr;
+      ready.clear();
+      to_prepare.clear();
+      cv_done.notify_all();
+    }
+  }
+};
+
+serve_state* serving_of(b2r_engine* e) { return static_cast<serve_state*>(e->serve.get()); }
 
 }  // namespace b2r
 
@@ -1494,30 +1672,106 @@ int b2r_last_batch_stats(const b2r_engine* e, b2r_batch_stats* s) {
 
 // ------------------------------------------------------------------ serving
 int b2r_serve_start(b2r_engine* e) {
-  if (e == nullptr) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
-  return b2r::fail(B2R_ERR_UNSUPPORTED, "serving loop not built yet");
+  B2R_API_GUARD({
+    if (e == nullptr) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
+    if (e->serving) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "engine is already serving");
+    auto ss = std::make_shared<b2r::serve_state>(*e);
+    auto const hw = std::max(1U, std::thread::hardware_concurrency());
+    auto const n_prep = e->cfg.host_threads != 0 ? e->cfg.host_threads : std::max(1U, std::min(8U, hw / 2));
+    for (auto i = 0U; i != n_prep; ++i) ss->prep_pool.emplace_back([p = ss.get()] { p->prep_loop(); });
+    ss->driver = std::thread([p = ss.get()] { p->driver_loop(); });
+    e->serve = ss;
+    e->serving = true;
+    return B2R_OK;
+  });
 }
+
 int b2r_serve_stop(b2r_engine* e) {
-  if (e == nullptr) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
-  return B2R_OK;
+  B2R_API_GUARD({
+    if (e == nullptr) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
+    if (!e->serving) return B2R_OK;
+    auto* ss = b2r::serving_of(e);
+    {
+      std::lock_guard<std::mutex> lock{ss->mu};
+      ss->stop = true;
+    }
+    ss->cv_prep.notify_all();
+    ss->cv_driver.notify_all();
+    for (auto& t : ss->prep_pool) t.join();
+    ss->prep_pool.clear();
+    {
+      std::lock_guard<std::mutex> lock{ss->mu};  // nothing is prepared any more
+      ss->cv_driver.notify_all();
+    }
+    if (ss->driver.joinable()) ss->driver.join();
+    e->serving = false;  // finished results stay readable until released
+    return ss->failed_status == B2R_OK ? B2R_OK : b2r::fail(ss->failed_status, ss->failed_msg);
+  });
 }
+
 int b2r_submit(b2r_engine* e, const b2r_query* q, uint64_t* ticket) {
-  (void)q;
-  (void)ticket;
-  if (e == nullptr) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
-  return b2r::fail(B2R_ERR_UNSUPPORTED, "serving loop not built yet");
+  B2R_API_GUARD({
+    if (e == nullptr || q == nullptr || ticket == nullptr) {
+      return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
+    }
+    if (!e->serving) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "engine is not serving (b2r_serve_start)");
+    auto* ss = b2r::serving_of(e);
+    auto it = std::make_unique<b2r::serve_item>();
+    it->q = *q;
+    it->start.assign(q->start, q->start + (q->start != nullptr ? q->n_start : 0U));
+    it->dest.assign(q->destination, q->destination + (q->destination != nullptr ? q->n_destination : 0U));
+    it->q.start = it->start.data();
+    it->q.n_start = static_cast<uint32_t>(it->start.size());
+    it->q.destination = it->dest.data();
+    it->q.n_destination = static_cast<uint32_t>(it->dest.size());
+    it->t_submit = std::chrono::steady_clock::now();
+    std::lock_guard<std::mutex> lock{ss->mu};
+    if (ss->stop) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "engine is stopping");
+    if (ss->failed_status != B2R_OK) return b2r::fail(ss->failed_status, ss->failed_msg);
+    it->ticket = ss->next_ticket++;
+    *ticket = it->ticket;
+    auto* raw = it.get();
+    ss->items.emplace(it->ticket, std::move(it));
+    ss->to_prepare.push_back(raw);
+    ++ss->unfinished;
+    ss->cv_prep.notify_one();
+    return B2R_OK;
+  });
 }
-int b2r_poll(b2r_engine* e, uint64_t ticket, b2r_result* out) {
-  (void)ticket;
-  (void)out;
-  if (e == nullptr) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
-  return b2r::fail(B2R_ERR_UNSUPPORTED, "serving loop not built yet");
+
+namespace {
+int serve_result(b2r_engine* e, uint64_t ticket, b2r_result* out, bool block) {
+  B2R_API_GUARD({
+    if (e == nullptr || out == nullptr) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
+    auto* ss = b2r::serving_of(e);
+    if (ss == nullptr) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "engine never served");
+    std::unique_lock<std::mutex> lock{ss->mu};
+    auto const found = ss->items.find(ticket);
+    if (found == ss->items.end()) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "unknown ticket");
+    auto& it = *found->second;
+    if (block) ss->cv_done.wait(lock, [&] { return it.finished; });
+    if (!it.finished) return B2R_ERR_NOT_READY;
+    *out = it.run.res.view;
+    return B2R_OK;
+  });
 }
-int b2r_wait(b2r_engine* e, uint64_t ticket, b2r_result* out) { return b2r_poll(e, ticket, out); }
+}  // namespace
+
+int b2r_poll(b2r_engine* e, uint64_t ticket, b2r_result* out) { return serve_result(e, ticket, out, false); }
+int b2r_wait(b2r_engine* e, uint64_t ticket, b2r_result* out) { return serve_result(e, ticket, out, true); }
+
 int b2r_release(b2r_engine* e, uint64_t ticket) {
-  (void)ticket;
-  if (e == nullptr) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
-  return B2R_OK;
+  B2R_API_GUARD({
+    if (e == nullptr) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
+    auto* ss = b2r::serving_of(e);
+    if (ss == nullptr) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "engine never served");
+    std::lock_guard<std::mutex> lock{ss->mu};
+    auto const found = ss->items.find(ticket);
+    if (found == ss->items.end()) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "unknown ticket");
+    if (!found->second->finished) return b2r::fail(B2R_ERR_NOT_READY, "ticket still running");
+    ss->items.erase(found);
+    return B2R_OK;
+  });
 }
 
 }  // extern "C"

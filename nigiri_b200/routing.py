@@ -310,3 +310,42 @@ def one_to_all(engine: Engine, queries: Sequence[Query], direction=FORWARD,
         rows = np.ctypeslib.as_array(r.round_times, shape=(r.n_rows * n,)).reshape(r.n_rows, n).copy()
         return OneToAllResult(rows, r.base_day, dirs[i])
     return engine.run(qb, len(queries), conv, plain=plain)
+
+
+class Server:
+    """Continuous-batching request loop on an engine (b2r_serve_start):
+    queries submitted from any thread are admitted into free slots while
+    earlier ones are still running; each ticket's result stays readable
+    until it is released."""
+
+    def __init__(self, engine: Engine):
+        self.engine = engine
+        _check(A.lib().b2r_serve_start(engine.handle))
+
+    def submit_raw(self, q: A.Query) -> int:
+        """Submits a b2r_query (offsets are copied by the engine)."""
+        t = C.c_uint64()
+        _check(A.lib().b2r_submit(self.engine.handle, C.byref(q), C.byref(t)))
+        return t.value
+
+    def poll(self, ticket: int):
+        """The b2r_result of a finished ticket, or None while it runs."""
+        r = A.Result()
+        rc = A.lib().b2r_poll(self.engine.handle, ticket, C.byref(r))
+        if rc == A.B2R_ERR_NOT_READY:
+            return None
+        _check(rc)
+        return r
+
+    def wait(self, ticket: int) -> A.Result:
+        r = A.Result()
+        _check(A.lib().b2r_wait(self.engine.handle, ticket, C.byref(r)))
+        return r
+
+    def release(self, ticket: int):
+        _check(A.lib().b2r_release(self.engine.handle, ticket))
+
+    def stop(self):
+        """Finishes every submitted query, then stops the loop."""
+        if self.engine.handle:
+            _check(A.lib().b2r_serve_stop(self.engine.handle))

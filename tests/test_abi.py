@@ -84,3 +84,15 @@ int main() {
     assert lib.b2r_one_to_all_noalloc(None, None, None, 0, C.byref(n_rows), None, None) == \
         A.B2R_ERR_INVALID_ARGUMENT
     assert b"null" in lib.b2r_last_error()
+
+
+def test_serving_entry_points_reject_null_engine():
+    lib = A.lib()
+    t = C.c_uint64()
+    r = A.Result()
+    assert lib.b2r_serve_start(None) == A.B2R_ERR_INVALID_ARGUMENT
+    assert lib.b2r_serve_stop(None) == A.B2R_ERR_INVALID_ARGUMENT
+    assert lib.b2r_submit(None, None, C.byref(t)) == A.B2R_ERR_INVALID_ARGUMENT
+    assert lib.b2r_poll(None, 1, C.byref(r)) == A.B2R_ERR_INVALID_ARGUMENT
+    assert lib.b2r_wait(None, 1, C.byref(r)) == A.B2R_ERR_INVALID_ARGUMENT
+    assert lib.b2r_release(None, 1) == A.B2R_ERR_INVALID_ARGUMENT
