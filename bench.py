@@ -261,6 +261,7 @@ def gpu_arm(args, rank, world, local):
     extras = {}
     if rank == 0 and not args.no_extras:
         extras = extras_legs(args, h, dtt, qs, B, local)
+        extras["served"] = served_leg(eng, qs, [5000.0, 15000.0, 25000.0, None], 4096)
     if rank == 0:
         peak, peak_kind = measured_peak()
         rl = extras.get("roofline")
@@ -285,6 +286,48 @@ def gpu_arm(args, rank, world, local):
     if pg is not None:
         pg.barrier()
         pg.destroy_process_group()
+
+
+def served_leg(eng, qs, rates, n_per_rate, seed=17):
+    """Continuous batching: queries arrive as a Poisson stream at each
+    offered rate (and all at once for the saturation point) and are
+    submitted to the request loop as they arrive; latency is submit ->
+    result, measured by the engine."""
+    import random
+    from nigiri_b200 import routing as R
+    srv = R.Server(eng)
+    out = []
+    try:
+        for rate in rates:
+            rnd = random.Random(seed)
+            n = min(n_per_rate, qs.n)
+            gaps = [0.0] * n if rate is None else [rnd.expovariate(rate) for _ in range(n)]
+            tickets, t_sub = [], []
+            t0 = time.perf_counter()
+            due = t0
+            for i in range(n):
+                due += gaps[i]
+                while True:
+                    now = time.perf_counter()
+                    if now >= due:
+                        break
+                    if due - now > 2e-4:
+                        time.sleep(due - now - 1e-4)
+                t_sub.append(time.perf_counter())
+                tickets.append(srv.submit_raw(qs.arr[i]))
+            lat, t_end = [], t0
+            for i, tk in enumerate(tickets):
+                r = srv.wait(tk)
+                lat.append(r.latency_ms)
+                t_end = max(t_end, t_sub[i] + r.latency_ms / 1e3)
+                srv.release(tk)
+            out.append({"offered_qps": rate if rate is not None else "all at once",
+                        "achieved_qps": n / (t_end - t0), "queries": n,
+                        "p50_ms": percentile(lat, 0.5), "p95_ms": percentile(lat, 0.95),
+                        "p99_ms": percentile(lat, 0.99)})
+    finally:
+        srv.stop()
+    return out
 
 
 def extras_legs(args, h, dtt, qs, B, local):
