@@ -190,14 +190,19 @@ def config_block(args, batch):
     return {"workload": "regional-40k-stops batched one-to-one (intermodal offset sets)",
             "timetable": "40,009 locations, 4,000 base routes, ~436k transports, 365 days",
             "global_batch": batch, "queries_per_step": batch, "max_transfers": 14,
-            "parallelism": f"replicas x{args.gpus}", "lower_bounds": "all-pairs tables on the device (built once per timetable, before timing)",
-            "l2": "round state of a step (>2.5 GB) exceeds L2; 512 MB written between steps"}
+            "parallelism": f"replicas x{args.gpus}"}
+
+
+METHOD = {"lower_bounds": "all-pairs tables on the device (built once per timetable, before timing)",
+          "l2": "round state of a step (>2.5 GB) exceeds L2; 512 MB written between steps",
+          "admission": "continuous: queries enter free slots between super-steps"}
 
 
 # --------------------------------------------------------------- GPU arm
 def gpu_arm(args, rank, world, local):
     import torch
     from nigiri_b200 import _abi as A
+    from nigiri_b200 import replicas
     from nigiri_b200 import routing as R
     from nigiri_b200.timetable import HostTimetable, QuerySet
 
@@ -212,7 +217,7 @@ def gpu_arm(args, rank, world, local):
     B = args.batch
     eng = R.Engine(dtt, max_slots=B)
     n_total = B * (args.warmup + args.steps)
-    qs = QuerySet(h, WORKLOAD, n_total, seed=1000 + WORKLOAD + 7919 * rank)
+    qs = QuerySet(h, WORKLOAD, n_total, seed=replicas.query_seed(1000 + WORKLOAD, rank))
     lib = A.lib()
     flush = torch.empty(512 << 20, dtype=torch.uint8, device=f"cuda:{local}")
 
@@ -248,13 +253,10 @@ def gpu_arm(args, rank, world, local):
             lats.append(out[i].latency_ms)
     ck = clocks.stop()
     tot_wall, tot_dev = sum(walls), sum(devs)
-    if pg is not None:
-        t = torch.tensor([tot_wall, tot_dev], dtype=torch.float64, device=f"cuda:{local}")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        tot_wall, tot_dev = t.tolist()
+    tot_wall, tot_dev = replicas.max_over_ranks([tot_wall, tot_dev], pg, f"cuda:{local}")
     n_q = B * args.steps * world
-    value = n_q / tot_dev
-    e2e = n_q / tot_wall
+    value = replicas.whole_job_throughput(B * args.steps, world, tot_dev)
+    e2e = replicas.whole_job_throughput(B * args.steps, world, tot_wall)
     # bytes the engine copied between host and device (its own count)
     h2d_step = h2d // max(1, args.steps)
 
@@ -270,7 +272,7 @@ def gpu_arm(args, rank, world, local):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot_dev / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int16",
             "data": "synthetic (seeded generator: timetable seed 2, query seed 1002+rank)",
-            "config": config_block(args, B),
+            "config": config_block(args, B), "method": METHOD,
             "p50_ms": percentile(lats, 0.5), "p99_ms": percentile(lats, 0.99),
             "e2e": {"value": e2e, "unit": "queries/s", "h2d_bytes_per_step": h2d_step,
                     "d2h_bytes_per_step": d2h // max(1, args.steps)},
@@ -387,6 +389,10 @@ def extras_legs(args, h, dtt, qs, B, local):
     out["cpu_baseline"] = {"value": sample / wall, "unit": "queries/s", "cores": threads,
                            "kind": "port", "sample": f"{sample} queries of the step-0 batch",
                            "p99_ms": percentile(lat, 0.99)}
+    wall1, lat1, _ = cpu_run(h.desc, qs.subset(range(64)), 64, 1)
+    out["cpu_baseline_1thread"] = {"value": 64 / wall1, "unit": "queries/s", "cores": 1,
+                                   "kind": "port", "sample": "64 queries of the step-0 batch",
+                                   "p50_ms": percentile(lat1, 0.5), "p99_ms": percentile(lat1, 0.99)}
     return out
 
 
