@@ -46,6 +46,8 @@ def parse():
                    help="one batch without CUDA graphs (the case profiled with ncu)")
     p.add_argument("--ncu-counters", action="store_true",
                    help="with --ncu-case: count route-scan work (stop visits, events)")
+    p.add_argument("--ncu-workload", type=int, default=2, choices=[1, 2, 3, 4, 5],
+                   help="with --ncu-case: the workload's timetable and queries")
     return p.parse_args()
 
 
@@ -402,10 +404,10 @@ def ncu_case(args, local):
     from nigiri_b200 import _abi as A
     from nigiri_b200 import routing as R
     from nigiri_b200.timetable import HostTimetable, QuerySet
-    h = HostTimetable.generate(WORKLOAD)
+    h = HostTimetable.generate(args.ncu_workload)
     dtt = R.Timetable(h.desc, device=local, owner=h)
     eng = R.Engine(dtt, max_slots=args.batch, use_graphs=False, profile=args.ncu_counters)
-    qs = QuerySet(h, WORKLOAD, args.batch, seed=1000 + WORKLOAD)
+    qs = QuerySet(h, args.ncu_workload, args.batch, seed=1000 + args.ncu_workload)
     out = (A.Result * args.batch)()
     rc = A.lib().b2r_search_batch(eng.handle, qs.arr, args.batch, out)
     if rc != 0:

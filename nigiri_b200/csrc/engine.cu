@@ -284,27 +284,32 @@ struct exp_item {
   uint64_t off_j, off_legs, off_rows, off_slot;
 };
 
+// blockIdx.x = item, blockIdx.y = share of the item's one-to-all rows
+// (rows are n_rows x n_locations values: many blocks per item)
 __global__ void k_export(dev::state st, exp_item const* items, uint32_t n_items, uint8_t* out) {
-  auto const it = items[blockIdx.x];
   if (blockIdx.x >= n_items) return;
+  auto const it = items[blockIdx.x];
   auto const s = it.slot;
   auto const& sl = st.slots[s];
-  if (threadIdx.x == 0) *reinterpret_cast<dev::slot_t*>(out + it.off_slot) = sl;
-  auto* js = reinterpret_cast<dev::journey_rec*>(out + it.off_j);
-  auto* legs = reinterpret_cast<b2r_leg*>(out + it.off_legs);
-  for (auto i = threadIdx.x; i < it.n_j; i += blockDim.x) {
-    js[i] = st.journeys[static_cast<size_t>(s) * st.max_j + i];
-  }
-  for (auto x = threadIdx.x; x < it.n_j * dev::kMaxLegs; x += blockDim.x) {
-    auto const i = x / dev::kMaxLegs, k = x % dev::kMaxLegs;
-    auto const blk = st.journeys[static_cast<size_t>(s) * st.max_j + i].block;
-    legs[x] = st.legs[(static_cast<size_t>(s) * st.max_j + blk) * dev::kMaxLegs + k];
+  if (blockIdx.y == 0) {
+    if (threadIdx.x == 0) *reinterpret_cast<dev::slot_t*>(out + it.off_slot) = sl;
+    auto* js = reinterpret_cast<dev::journey_rec*>(out + it.off_j);
+    auto* legs = reinterpret_cast<b2r_leg*>(out + it.off_legs);
+    for (auto i = threadIdx.x; i < it.n_j; i += blockDim.x) {
+      js[i] = st.journeys[static_cast<size_t>(s) * st.max_j + i];
+    }
+    for (auto x = threadIdx.x; x < it.n_j * dev::kMaxLegs; x += blockDim.x) {
+      auto const i = x / dev::kMaxLegs, k = x % dev::kMaxLegs;
+      auto const blk = st.journeys[static_cast<size_t>(s) * st.max_j + i].block;
+      legs[x] = st.legs[(static_cast<size_t>(s) * st.max_j + blk) * dev::kMaxLegs + k];
+    }
   }
   if (it.n_rows != 0) {
     auto* rows = reinterpret_cast<int16_t*>(out + it.off_rows);
     auto const qtag = dev::tagcode(sl.gen_query);
     auto const n = static_cast<size_t>(it.n_rows) * st.tt.n_loc;
-    for (size_t x = threadIdx.x; x < n; x += blockDim.x) {
+    for (size_t x = static_cast<size_t>(blockIdx.y) * blockDim.x + threadIdx.x; x < n;
+         x += static_cast<size_t>(gridDim.y) * blockDim.x) {
       auto const k = static_cast<uint32_t>(x / st.tt.n_loc), l = static_cast<uint32_t>(x % st.tt.n_loc);
       auto const key = dev::dec(st.rt[(static_cast<size_t>(k) * st.tt.n_loc + l) * st.S + s], qtag);
       rows[x] = static_cast<int16_t>(dev::from_key(sl.fwd != 0, key));
@@ -664,7 +669,12 @@ void export_slots(b2r_engine& e, std::vector<uint32_t> const& slots,
   std::memcpy(e.h_exp, items.data(), items.size() * sizeof(exp_item));
   e.h2d_bytes += items.size() * sizeof(exp_item);
   B2R_CUDA(cudaMemcpyAsync(e.d_exp, e.h_exp, items.size() * sizeof(exp_item), cudaMemcpyHostToDevice, s));
-  k_export<<<static_cast<unsigned>(slots.size()), 256, 0, s>>>(
+  uint32_t row_blocks = 1;  // spread one-to-all rows over the SMs
+  for (auto const r : n_rows) {
+    if (r != 0) row_blocks = std::max<uint32_t>(row_blocks, static_cast<uint32_t>(e.sms) * 4u /
+                                                                static_cast<uint32_t>(slots.size()) + 1u);
+  }
+  k_export<<<dim3(static_cast<unsigned>(slots.size()), row_blocks), 256, 0, s>>>(
       e.st, reinterpret_cast<exp_item const*>(e.d_exp), static_cast<uint32_t>(slots.size()), e.d_exp);
   B2R_CUDA(cudaGetLastError());
   e.d2h_bytes += off;
@@ -808,6 +818,28 @@ void on_phase_done(b2r_engine& e, query_run& q, exported const& x) {
 }  // namespace
 
 // ------------------------------------------------------------- the loop
+// Free slots for admission.  Range queries run several start-time groups and
+// so sweep their round times every round (k_sweep); they take slots from the
+// top of the pool, all other queries from the bottom, so that the sweeping
+// slots share slot groups.
+template <typename Free>
+struct slot_picker {
+  slot_picker(uint32_t n, Free f) : is_free{f}, n_slots{n}, hi{static_cast<int64_t>(n) - 1} {}
+  int64_t take(bool top) {
+    if (top) {
+      while (hi >= 0 && !is_free(static_cast<uint32_t>(hi))) --hi;
+      return hi < 0 ? -1 : hi--;
+    }
+    while (lo < n_slots && !is_free(static_cast<uint32_t>(lo))) ++lo;
+    return lo >= n_slots ? -1 : lo++;
+  }
+  Free is_free;
+  int64_t n_slots;
+  int64_t lo{0}, hi;
+};
+
+bool sweeps(prepped_query const& p) { return !p.ontrip && !p.one_to_all; }
+
 // a new interval-extension phase for the query in slot s (search.h:283-316)
 void rearm(b2r_engine& e, uint32_t s, query_run& q, cudaStream_t st) {
   // new phase: upload the new starts (and journeys kept), keep the rt
@@ -864,8 +896,8 @@ struct batch_runner {
     std::fill(slot_q.begin(), slot_q.end(), -1);
     auto const admit_free = [&]() {
       std::vector<std::pair<uint32_t, prepped_query const*>> adm;
-      for (uint32_t s = 0; s != S && next < runs.size(); ++s) {
-        if (slot_q[s] != -1) continue;
+      slot_picker pick{S, [&](uint32_t s) { return slot_q[s] == -1; }};
+      while (next < runs.size()) {
         while (next < runs.size()) {
           auto& q = runs[next];
           if (!q.ready.load(std::memory_order_acquire)) break;
@@ -888,8 +920,10 @@ struct batch_runner {
           break;
         }
         if (next >= runs.size() || !runs[next].ready.load(std::memory_order_acquire)) break;
+        auto const s = pick.take(sweeps(runs[next].p));
+        if (s < 0) break;
         slot_q[s] = static_cast<int64_t>(next);
-        adm.emplace_back(s, &runs[next].p);
+        adm.emplace_back(static_cast<uint32_t>(s), &runs[next].p);
         ++next;
       }
       admit(e, adm, st);
@@ -1123,8 +1157,8 @@ struct serve_state {
             cv_driver.wait(lock, [&] { return !ready.empty() || (stop && unfinished == 0); });
             if (ready.empty() && stop && unfinished == 0) return;
           }
-          for (uint32_t s = 0; s != e.S && !ready.empty(); ++s) {
-            if (slot_item[s] != nullptr) continue;
+          slot_picker pick{e.S, [&](uint32_t s) { return slot_item[s] == nullptr; }};
+          while (!ready.empty()) {
             while (!ready.empty()) {
               auto* it = ready.front();
               auto const& p = it->run.p;
@@ -1142,11 +1176,15 @@ struct serve_state {
                 cv_done.notify_all();
                 continue;
               }
-              ready.pop_front();
-              slot_item[s] = it;
-              adm.emplace_back(s, &it->run.p);
               break;
             }
+            if (ready.empty()) break;
+            auto* it = ready.front();
+            auto const s = pick.take(sweeps(it->run.p));
+            if (s < 0) break;
+            ready.pop_front();
+            slot_item[s] = it;
+            adm.emplace_back(static_cast<uint32_t>(s), &it->run.p);
           }
           any_busy = has_busy();
         }

@@ -83,18 +83,25 @@ __global__ void k_ctl_begin(state st) {
 }
 
 // best <- min(best, round_times[k]) over all locations (raptor.h:219-223)
+// for the slots whose earlier start-time groups left round times behind
+// (range queries).  Warp per (location, slot group) over the groups holding
+// such slots only, lane = slot: admission packs range queries into the same
+// groups, so the lanes read neighbouring words.
 __global__ void k_sweep(state st) {
-  auto const n = static_cast<size_t>(st.tt.n_loc) * st.S;
-  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
-       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
-    auto const s = static_cast<uint32_t>(i % st.S);
-    if (!((st.sweep_mask[s >> 5] >> (s & 31)) & 1u)) continue;
-    auto const l = static_cast<uint32_t>(i / st.S);
+  auto const lane = threadIdx.x & 31u;
+  auto const warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  auto const n_warps = (gridDim.x * blockDim.x) >> 5;
+  for (auto g = 0u; g != st.G; ++g) {
+    auto const m = st.sweep_mask[g];
+    if (m == 0u || !((m >> lane) & 1u)) continue;
+    auto const s = g * 32u + lane;
     auto const ln = st.lanes[s];
-    auto const r = dec(st.rt[rti(st, ln.k, l, s)], ln.qtag);
-    if (r == kKeyInv) continue;
-    auto const b = dec(st.best[i], ln.gtag);
-    if (r < b) st.best[i] = enc(ln.gtag, r);
+    for (auto l = warp; l < st.tt.n_loc; l += n_warps) {
+      auto const r = dec(st.rt[rti(st, ln.k, l, s)], ln.qtag);
+      if (r == kKeyInv) continue;
+      auto& bw = st.best[li(st, l, s)];
+      if (r < dec(bw, ln.gtag)) bw = enc(ln.gtag, r);
+    }
   }
 }
 
