@@ -270,9 +270,10 @@ typedef struct b2r_engine_config {
                                2 = solved on the device, 3 = from all-pairs
                                tables on the device (default; built once per
                                timetable on the host threads, 2 * n_locations^2
-                               * 2 bytes; falls back to 1 above
-                               B2R_LB_TABLE_MAX_BYTES).  Journeys are the same
-                               in every mode. */
+                               * 2 bytes; falls back to 0 above
+                               B2R_LB_TABLE_MAX_BYTES, where the host
+                               Dijkstra would cost more than the pruning
+                               saves).  Journeys are the same in every mode. */
   uint32_t use_graphs;      /* 1 = capture the super-step in a CUDA graph */
   uint32_t route_block;     /* launch shape: warps per CTA in the route scan */
   uint32_t max_starts;      /* start labels per query (default 4096) */
@@ -384,6 +385,10 @@ typedef struct b2r_batch_stats {
                                  launches (profiling engines only) */
   double recon_max_journey_us; /* longest single journey reconstruction */
   uint64_t recon_journeys;    /* journeys reconstructed */
+  double host_prep_cpu_ms;    /* query preparation, summed over the workers */
+  double host_admit_ms;       /* admission (staging + copies), driver thread */
+  double host_export_ms;      /* export, finalisation and retirement */
+  double host_idle_ms;        /* driver waiting for preparation, no slot busy */
 } b2r_batch_stats;
 int b2r_last_batch_stats(const b2r_engine* e, b2r_batch_stats* s);
 

@@ -125,7 +125,9 @@ class BatchStats(C.Structure):
                 ("lb_iterations", C.c_uint64), ("lb_relaxations", C.c_uint64),
                 ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64),
                 ("route_warp_steps", C.c_uint64), ("recon_ms", C.c_double),
-                ("recon_max_journey_us", C.c_double), ("recon_journeys", C.c_uint64)]
+                ("recon_max_journey_us", C.c_double), ("recon_journeys", C.c_uint64),
+                ("host_prep_cpu_ms", C.c_double), ("host_admit_ms", C.c_double),
+                ("host_export_ms", C.c_double), ("host_idle_ms", C.c_double)]
 
 
 class TtBase(C.Structure):

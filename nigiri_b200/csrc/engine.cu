@@ -81,6 +81,26 @@ void host_copy(std::vector<T>& v, T const* p, size_t n) {
 }  // namespace b2r
 
 // ==================================================================== engine
+// Allocator whose value-initialisation is default-initialisation: large
+// result arrays that are overwritten right away are not zero-filled first.
+template <typename T>
+struct uninit_allocator : std::allocator<T> {
+  template <typename U>
+  struct rebind {
+    using other = uninit_allocator<U>;
+  };
+  using std::allocator<T>::allocator;
+  template <typename U>
+  void construct(U* p) noexcept {
+    ::new (static_cast<void*>(p)) U;
+  }
+  template <typename U, typename... Args>
+  void construct(U* p, Args&&... args) {
+    ::new (static_cast<void*>(p)) U(std::forward<Args>(args)...);
+  }
+};
+using row_vector = std::vector<int16_t, uninit_allocator<int16_t>>;
+
 struct b2r_engine {
   b2r_timetable* tt{nullptr};
   b2r_engine_config cfg{};
@@ -108,6 +128,10 @@ struct b2r_engine {
   b2r::dev::journey_rec* d_keep{};  // journeys kept across interval-extension phases
   // host<->device bytes copied by the current batch call
   uint64_t h2d_bytes{0}, d2h_bytes{0};
+  // host time of the current batch call: preparation (summed over the
+  // workers), admission, export + finalisation, waiting for preparation
+  std::atomic<uint64_t> prep_ns{0};
+  double admit_ms{0}, export_ms{0}, idle_ms{0};
   // admission staging (pinned) and device mirror
   uint8_t* h_adm{nullptr};
   uint8_t* d_adm{nullptr};
@@ -134,7 +158,7 @@ struct b2r_engine {
   struct result_store {
     std::vector<b2r_journey> journeys;
     std::vector<b2r_leg> legs;
-    std::vector<int16_t> rt_rows;
+    row_vector rt_rows;
     b2r_result view{};
   };
   std::vector<result_store> results;
@@ -364,6 +388,7 @@ void enqueue_superstep(b2r_engine& e, cudaStream_t s) {
   dev::k_sweep<<<e.sms * 16, 256, 0, s>>>(st);
   dev::k_ctl_dest<<<slot_blocks, 128, 0, s>>>(st);
   dev::k_mark_routes<<<list_blocks, 256, 0, s>>>(st);
+  dev::k_list_routes<<<e.sms * 8, 256, 0, s>>>(st);
   dev::k_ctl_marked<<<slot_blocks, 128, 0, s>>>(st);
   cudaEvent_t ev_a = nullptr, ev_b = nullptr;
   if (e.cfg.profile) {  // CUDA events on the launching stream around the scan
@@ -408,7 +433,7 @@ void enqueue_superstep(b2r_engine& e, cudaStream_t s) {
   dev::k_next<<<slot_blocks, 128, 0, s>>>(st);
   k_summary<<<slot_blocks, 128, 0, s>>>(st, e.d_summary);
 }
-constexpr uint64_t kLaunchesPerStep = 20;
+constexpr uint64_t kLaunchesPerStep = 21;
 
 // --------------------------------------------------------- admission
 size_t admission_bytes(b2r_engine const& e, prepped_query const& p) {
@@ -630,7 +655,7 @@ struct exported {
   slot_t sl;
   std::vector<dev::journey_rec> js;
   std::vector<b2r_leg> legs;  // n_j * kMaxLegs
-  std::vector<int16_t> rows;
+  row_vector rows;
 };
 
 void export_slots(b2r_engine& e, std::vector<uint32_t> const& slots,
@@ -689,7 +714,24 @@ void export_slots(b2r_engine& e, std::vector<uint32_t> const& slots,
     o.legs.resize(static_cast<size_t>(it.n_j) * dev::kMaxLegs);
     std::memcpy(o.legs.data(), e.h_exp + it.off_legs, o.legs.size() * sizeof(b2r_leg));
     o.rows.resize(static_cast<size_t>(it.n_rows) * e.tt->d.n_loc);
-    std::memcpy(o.rows.data(), e.h_exp + it.off_rows, o.rows.size() * sizeof(int16_t));
+  }
+  // one-to-all rows (n_rows x n_locations each): large copies out of the
+  // pinned staging buffer, split over a few threads
+  size_t row_bytes = 0;
+  for (auto const& o : out) row_bytes += o.rows.size() * sizeof(int16_t);
+  auto const copy_rows = [&](size_t first, size_t step) {
+    for (auto i = first; i < slots.size(); i += step) {
+      std::memcpy(out[i].rows.data(), e.h_exp + items[i].off_rows, out[i].rows.size() * sizeof(int16_t));
+    }
+  };
+  if (row_bytes < (size_t{32} << 20)) {
+    copy_rows(0, 1);
+  } else {
+    auto const n_threads = std::min<size_t>(8, std::max(1U, std::thread::hardware_concurrency() / 2));
+    std::vector<std::thread> pool;
+    for (size_t t = 1; t < n_threads; ++t) pool.emplace_back(copy_rows, t, n_threads);
+    copy_rows(0, n_threads);
+    for (auto& th : pool) th.join();
   }
 }
 
@@ -707,14 +749,14 @@ struct query_run {
   b2r_engine::result_store res;
 };
 
-void finish_result(b2r_engine& e, query_run& q, exported const& x) {
+void finish_result(b2r_engine& e, query_run& q, exported& x) {
   auto& p = q.p;
   auto& res = q.res;
   res.journeys.clear();
   res.legs.clear();
   res.rt_rows.clear();
   if (p.one_to_all) {
-    res.rt_rows = x.rows;
+    res.rt_rows = std::move(x.rows);  // one-to-all rows can be large
     res.view.n_rows = p.end_k;
     res.view.base_day = p.base_days;
   } else {
@@ -760,7 +802,7 @@ void finish_result(b2r_engine& e, query_run& q, exported const& x) {
 }
 
 // decides between finishing and another interval-extension phase
-void on_phase_done(b2r_engine& e, query_run& q, exported const& x) {
+void on_phase_done(b2r_engine& e, query_run& q, exported& x) {
   auto& p = q.p;
   if (x.sl.state == dev::S_ERROR) {
     q.status = x.sl.error != 0 ? x.sl.error : B2R_ERR_INTERNAL;
@@ -926,7 +968,9 @@ struct batch_runner {
         adm.emplace_back(static_cast<uint32_t>(s), &runs[next].p);
         ++next;
       }
+      auto const t0 = std::chrono::steady_clock::now();
       admit(e, adm, st);
+      e.admit_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     };
     admit_free();
     auto busy_slots = [&]() {
@@ -947,7 +991,9 @@ struct batch_runner {
     while (busy()) {
       if (steps > max_steps) throw std::runtime_error("super-step cap exceeded");
       if (!busy_slots()) {  // every resident query finished: wait for preparation
+        auto const t0 = std::chrono::steady_clock::now();
         std::this_thread::yield();
+        e.idle_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         admit_free();
         continue;
       }
@@ -985,6 +1031,7 @@ struct batch_runner {
         }
       }
       if (done_slots.empty()) continue;
+      auto const t_exp = std::chrono::steady_clock::now();
       std::vector<exported> ex;
       export_slots(e, done_slots, n_js, n_rows, ex, st);
       std::vector<uint32_t> retired;
@@ -1004,6 +1051,7 @@ struct batch_runner {
         }
       }
       retire(e, retired, st);
+      e.export_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_exp).count();
       admit_free();
     }
     B2R_CUDA(cudaStreamSynchronize(st));
@@ -1032,7 +1080,10 @@ struct preparer {
     auto const lb_mode = static_cast<int>(e.cfg.use_lower_bounds);
     auto work = [&e, qs, n, &runs, lb_mode, this]() {
       for (auto i = next++; i < n; i = next++) {
+        auto const t0 = std::chrono::steady_clock::now();
         prepare(e.tt->view, qs[i], lb_mode, runs[i].p);
+        e.prep_ns += static_cast<uint64_t>(
+            std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0).count());
         runs[i].ready.store(true, std::memory_order_release);
       }
     };
@@ -1439,13 +1490,13 @@ int b2r_engine_create(b2r_timetable* tt, const b2r_engine_config* cfg_in, b2r_en
       if (cfg.profile) e->cfg.use_graphs = 0;
       e->max_dest = 512U;
       e->max_off = 128U;
-      if (cfg.use_lower_bounds == 3) {  // the table when it fits, else the host Dijkstra
+      if (cfg.use_lower_bounds == 3) {  // the table when it fits, else no bounds
         auto const n = static_cast<uint64_t>(tt->d.n_loc);
         if (2 * n * n * sizeof(uint16_t) <= B2R_LB_TABLE_MAX_BYTES) {
           auto const hw = std::max(1U, std::thread::hardware_concurrency());
           b2r::ensure_lb_table(*tt, cfg.host_threads != 0 ? cfg.host_threads : hw);
         } else {
-          e->cfg.use_lower_bounds = 1;
+          e->cfg.use_lower_bounds = 0;
         }
       }
       auto const nl = tt->d.n_loc;
@@ -1577,15 +1628,17 @@ int b2r_search_batch(b2r_engine* e, const b2r_query* qs, uint32_t n, b2r_result*
       std::vector<b2r::query_run> runs(n);
       auto const t0 = std::chrono::steady_clock::now();
       e->batch_t0 = t0;
-      b2r::preparer prep;
-      prep.start(*e, qs, n, runs, false);
-      b2r::batch_runner br{*e, runs, e->cfg.use_graphs != 0 && e->graph != nullptr};
       e->prof_used = 0;
       e->prof_rc_used = 0;
       e->lb_ms = 0;
       e->lb_chunks = 0;
       e->h2d_bytes = 0;
       e->d2h_bytes = 0;
+      e->prep_ns = 0;
+      e->admit_ms = e->export_ms = e->idle_ms = 0;
+      b2r::preparer prep;
+      prep.start(*e, qs, n, runs, false);
+      b2r::batch_runner br{*e, runs, e->cfg.use_graphs != 0 && e->graph != nullptr};
       if (e->cfg.profile) B2R_CUDA(cudaMemsetAsync(e->st.prof, 0, 8 * sizeof(unsigned long long), e->stream));
       br.run(e->cfg.steps_per_sync != 0 ? e->cfg.steps_per_sync : 4U);
       prep.join();
@@ -1600,6 +1653,10 @@ int b2r_search_batch(b2r_engine* e, const b2r_query* qs, uint32_t n, b2r_result*
       e->last.lb_iterations = e->lb_chunks * 8;
       e->last.h2d_bytes = e->h2d_bytes;
       e->last.d2h_bytes = e->d2h_bytes;
+      e->last.host_prep_cpu_ms = static_cast<double>(e->prep_ns.load()) / 1e6;
+      e->last.host_admit_ms = e->admit_ms;
+      e->last.host_export_ms = e->export_ms;
+      e->last.host_idle_ms = e->idle_ms;
       if (e->cfg.profile) {
         double scan_ms = 0;
         for (size_t i = 0; i + 1 < e->prof_used; i += 2) {

@@ -134,10 +134,30 @@ __global__ void k_mark_routes(state st) {
     if (rb == re) continue;
     atomicOr(&st.any_mask[g], w);
     for (auto ri = rb; ri != re; ++ri) {
-      mark(st, st.R, st.rlist, C_R, st.tt.loc_routes[ri] * st.G + g, w);
+      atomicOr(&st.R[st.tt.loc_routes[ri] * st.G + g], w);  // listed by k_list_routes
     }
   }
 }
+
+// list of the words of W[0, n) that are nonzero, one counter add per warp
+__device__ __forceinline__ void list_nonzero(state const& st, uint32_t const* W, uint32_t n,
+                                             uint32_t* list, uint32_t counter) {
+  auto const lane = threadIdx.x & 31u;
+  auto const stride = gridDim.x * blockDim.x;
+  for (auto i0 = blockIdx.x * blockDim.x; i0 < n; i0 += stride) {
+    auto const i = i0 + threadIdx.x;
+    auto const on = i < n && W[i] != 0u;
+    auto const m = __ballot_sync(kFull, on);
+    if (m == 0u) continue;
+    uint32_t at = 0;
+    if (lane == 0) at = atomicAdd(&st.counters[counter], static_cast<uint32_t>(__popc(m)));
+    at = __shfl_sync(kFull, at, 0);
+    if (on) list[at + static_cast<uint32_t>(__popc(m & ((1u << lane) - 1u)))] = i;
+  }
+}
+
+// marked (route, group) entries of this round
+__global__ void k_list_routes(state st) { list_nonzero(st, st.R, st.tt.n_routes * st.G, st.rlist, C_R); }
 
 __global__ void k_ctl_marked(state st) {
   auto const s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -310,22 +330,8 @@ __global__ void __launch_bounds__(256, 3) k_route_scan(state st) {
 }
 
 // frontier list of the stations reached by the route scan: every nonzero
-// route-reached word (location, group), one counter add per warp
-__global__ void k_list_reached(state st) {
-  auto const lane = threadIdx.x & 31u;
-  auto const n = st.tt.n_loc * st.G;
-  auto const stride = gridDim.x * blockDim.x;
-  for (auto i0 = blockIdx.x * blockDim.x; i0 < n; i0 += stride) {
-    auto const i = i0 + threadIdx.x;
-    auto const on = i < n && st.Y[i] != 0u;
-    auto const m = __ballot_sync(kFull, on);
-    if (m == 0u) continue;
-    uint32_t at = 0;
-    if (lane == 0) at = atomicAdd(&st.counters[C_Y], static_cast<uint32_t>(__popc(m)));
-    at = __shfl_sync(kFull, at, 0);
-    if (on) st.ylist[at + static_cast<uint32_t>(__popc(m & ((1u << lane) - 1u)))] = i;
-  }
-}
+// route-reached word (location, group)
+__global__ void k_list_reached(state st) { list_nonzero(st, st.Y, st.tt.n_loc * st.G, st.ylist, C_Y); }
 
 __global__ void k_clear_x(state st) {
   auto const tid = blockIdx.x * blockDim.x + threadIdx.x;
