@@ -42,6 +42,7 @@ def parse():
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--cpu-sample", type=int, default=0, help="queries in the CPU baseline sample")
     p.add_argument("--no-extras", action="store_true", help="skip plain / roofline / CPU legs")
+    p.add_argument("--no-national", action="store_true", help="skip the national-scale leg")
     p.add_argument("--ncu-case", action="store_true",
                    help="one batch without CUDA graphs (the case profiled with ncu)")
     p.add_argument("--ncu-counters", action="store_true",
@@ -266,6 +267,9 @@ def gpu_arm(args, rank, world, local):
     if rank == 0 and not args.no_extras:
         extras = extras_legs(args, h, dtt, qs, B, local)
         extras["served"] = served_leg(eng, qs, [5000.0, 15000.0, 25000.0, None], 4096)
+        del eng
+        if not args.no_national:
+            extras["national"] = national_leg(local)
     if rank == 0:
         peak, peak_kind = measured_peak()
         rl = extras.get("roofline")
@@ -292,11 +296,12 @@ def gpu_arm(args, rank, world, local):
         pg.destroy_process_group()
 
 
-def served_leg(eng, qs, rates, n_per_rate, seed=17):
+def served_leg(eng, qs, rates, n_per_rate, seed=17, keep_every=0, kept=None):
     """Continuous batching: queries arrive as a Poisson stream at each
     offered rate (and all at once for the saturation point) and are
     submitted to the request loop as they arrive; latency is submit ->
-    result, measured by the engine."""
+    result, measured by the engine.  With keep_every = m, every m-th
+    answer is kept in `kept` (query index -> result key) for checking."""
     import random
     from nigiri_b200 import routing as R
     srv = R.Server(eng)
@@ -304,7 +309,7 @@ def served_leg(eng, qs, rates, n_per_rate, seed=17):
     try:
         for rate in rates:
             rnd = random.Random(seed)
-            n = min(n_per_rate, qs.n)
+            n = min(n_per_rate(rate) if callable(n_per_rate) else n_per_rate, qs.n)
             gaps = [0.0] * n if rate is None else [rnd.expovariate(rate) for _ in range(n)]
             tickets, t_sub = [], []
             t0 = time.perf_counter()
@@ -322,6 +327,8 @@ def served_leg(eng, qs, rates, n_per_rate, seed=17):
             lat, t_end = [], t0
             for i, tk in enumerate(tickets):
                 r = srv.wait(tk)
+                if keep_every and i % keep_every == 0 and kept is not None:
+                    kept[i] = result_key(r, eng.tt.n_locations)
                 lat.append(r.latency_ms)
                 t_end = max(t_end, t_sub[i] + r.latency_ms / 1e3)
                 srv.release(tk)
@@ -331,6 +338,90 @@ def served_leg(eng, qs, rates, n_per_rate, seed=17):
                         "p99_ms": percentile(lat, 0.99)})
     finally:
         srv.stop()
+    return out
+
+
+def result_key(r, n_loc):
+    """A query's complete answer: journeys with every leg, or one-to-all rows."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from journeys import records
+    if r.round_times:
+        rows = np.ctypeslib.as_array(r.round_times, shape=(r.n_rows * n_loc,))
+        return ("rows", r.status, r.base_day, rows.tobytes())
+    return ("journeys", r.status, records(r))
+
+
+def national_leg(local):
+    """National-scale timetable (300k stops, 25k base routes, 2.7M transports,
+    stay-seated chain routes).  Batched: batches of 256 mixing one-to-one, 1 h
+    range and one-to-all queries.  Served: the request loop fed by Poisson
+    streams of the 70% one-to-one / 20% 2 h range / 10% one-to-all mix at
+    200 .. 20,000 q/s.  Plain: one query per launch sequence.  CPU: the
+    oracle on all host threads, on the served answers kept for checking (1%),
+    which are compared with its results."""
+    from nigiri_b200 import _abi as A
+    from nigiri_b200 import routing as R
+    from nigiri_b200.timetable import HostTimetable, QuerySet
+    lib = A.lib()
+    h = HostTimetable.generate(4)
+    dtt = R.Timetable(h.desc, device=local, owner=h)
+    n_loc = h.desc.n_locations
+    out = {"timetable": f"{n_loc:,} locations, {h.desc.n_routes:,} routes, "
+                        f"{h.desc.n_transports:,} transports, 365 days"}
+    eng = R.Engine(dtt, max_slots=1024)
+    B = 256
+    qs = QuerySet(h, 4, B * 4, seed=1004)
+    res = (A.Result * B)()
+    devs, walls = [], []
+    for k in range(4):
+        arr = qs.subset(range(k * B, (k + 1) * B))
+        t0 = time.perf_counter()
+        if lib.b2r_search_batch(eng.handle, arr, B, res) != 0:
+            raise RuntimeError(lib.b2r_last_error().decode())
+        if k > 0:  # the first batch warms up
+            walls.append(time.perf_counter() - t0)
+            devs.append(eng.stats().device_ms / 1e3)
+    out["batched"] = {"batch": B, "queries": B * 3, "value": B * 3 / sum(devs),
+                      "e2e": B * 3 / sum(walls), "unit": "queries/s",
+                      "ms_per_batch": sum(walls) / 3 * 1e3}
+    # plain: one query per launch sequence (same engine design, per-round launches)
+    plain = R.Engine(dtt, max_slots=32, use_graphs=False)
+    arr = qs.subset(range(32))
+    one = A.Result()
+    t0 = time.perf_counter()
+    for i in range(32):
+        if lib.b2r_search_plain(plain.handle, C.byref(arr[i]), C.byref(one)) != 0:
+            raise RuntimeError(lib.b2r_last_error().decode())
+    out["plain_gpu"] = {"value": 32 / (time.perf_counter() - t0), "unit": "queries/s", "queries": 32}
+    del plain
+    # served (continuous batching), 1% of the answers kept for the check
+    sq = QuerySet(h, 5, 4096, seed=1005)
+    kept = {}
+    out["served"] = served_leg(eng, sq, [200.0, 1000.0, 5000.0, 20000.0, None],
+                               lambda r: 4096 if r is None else max(256, min(4096, int(r))),
+                               keep_every=100, kept=kept)
+    del eng
+    # CPU baseline on the kept queries, which also checks their answers
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib
+    idx = sorted(kept)
+    threads = host_threads()
+    wall, lat, _ = cpu_run(h.desc, sq.subset(idx), len(idx), threads)
+    out["cpu_baseline"] = {"value": len(idx) / wall, "unit": "queries/s", "cores": threads,
+                           "kind": "port", "sample": f"{len(idx)} served queries (1%)"}
+    mismatches = 0
+    for i in idx:
+        q = sq.arr[i]
+        o = oracle_lib.OracleResult(h.desc, q)
+        if q.kind == A.B2R_ONE_TO_ALL:
+            rows, _, base_day = o.state()
+            n_rows = len(kept[i][3]) // (2 * n_loc)
+            want = ("rows", 0, base_day, rows[:n_rows].tobytes())
+        else:
+            want = ("journeys", 0, o.records())
+        mismatches += 0 if kept[i] == want else 1
+    out["checked_against_cpu"] = {"queries": len(idx), "mismatches": mismatches}
     return out
 
 
