@@ -431,9 +431,10 @@ void enqueue_superstep(b2r_engine& e, cudaStream_t s) {
   dev::k_reconstruct<<<e.sms * 4, 128, 0, s>>>(st);
   if (e.cfg.profile) B2R_CUDA(cudaEventRecord(rc_b, s));
   dev::k_next<<<slot_blocks, 128, 0, s>>>(st);
+  dev::k_list_marked<<<e.sms * 8, 256, 0, s>>>(st);
   k_summary<<<slot_blocks, 128, 0, s>>>(st, e.d_summary);
 }
-constexpr uint64_t kLaunchesPerStep = 21;
+constexpr uint64_t kLaunchesPerStep = 22;
 
 // --------------------------------------------------------- admission
 size_t admission_bytes(b2r_engine const& e, prepped_query const& p) {

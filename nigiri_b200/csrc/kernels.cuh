@@ -35,6 +35,49 @@ __device__ __forceinline__ void mark_warp(state const& st, uint32_t* M, uint32_t
   if (want && lane == static_cast<uint32_t>(__ffs(peers) - 1)) mark(st, M, list, counter, e, peers);
 }
 
+// Visits the (entry, query) pairs of a frontier list: a warp takes 32 list
+// entries (a location or route with a group of 32 queries), and its lanes
+// take their set query bits, one pair per lane per pass.  Resident queries
+// are unrelated, so an entry holds few of its 32 queries; a lane per query of
+// one entry would leave most lanes idle.  word(e) returns the entry's query
+// bits; f(e, b) runs for every set bit b.  f must not synchronise the warp.
+template <typename Word, typename F>
+__device__ __forceinline__ void for_each_pair(uint32_t const* list, uint32_t n, Word&& word, F&& f) {
+  auto const lane = threadIdx.x & 31u;
+  auto const warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  auto const n_warps = (gridDim.x * blockDim.x) >> 5;
+  for (auto w0 = warp * 32u; w0 < n; w0 += n_warps * 32u) {
+    auto const w = w0 + lane;
+    uint32_t e = 0, mask = 0;
+    if (w < n) {
+      e = list[w];
+      mask = word(e);
+    }
+    auto const cnt = static_cast<uint32_t>(__popc(mask));
+    auto end = cnt;  // inclusive prefix sum of the pair counts
+    for (auto o = 1u; o < 32u; o <<= 1) {
+      auto const v = __shfl_up_sync(kFull, end, o);
+      if (lane >= o) end += v;
+    }
+    auto const total = __shfl_sync(kFull, end, 31);
+    for (auto p0 = 0u; p0 < total; p0 += 32u) {
+      auto const p = p0 + lane;
+      uint32_t owner = 0;  // first lane whose prefix end exceeds p
+      for (auto b = 16u; b > 0u; b >>= 1) {
+        if (__shfl_sync(kFull, end, static_cast<int>(owner + b - 1u)) <= p) owner += b;
+      }
+      auto const o_e = __shfl_sync(kFull, e, static_cast<int>(owner));
+      auto o_mask = __shfl_sync(kFull, mask, static_cast<int>(owner));
+      auto const o_first = __shfl_sync(kFull, end, static_cast<int>(owner)) -
+                           __shfl_sync(kFull, cnt, static_cast<int>(owner));
+      if (p < total) {
+        for (auto x = p - o_first; x != 0u; --x) o_mask &= o_mask - 1u;
+        f(o_e, static_cast<uint32_t>(__ffs(o_mask) - 1));
+      }
+    }
+  }
+}
+
 __device__ __forceinline__ void update_tad(slot_t& sl, uint32_t k, int key) {  // raptor.h:1479-1486
   if (sl.one_to_all) return;
   for (auto i = k; i < kK; ++i) {
@@ -329,6 +372,10 @@ __global__ void __launch_bounds__(256, 3) k_route_scan(state st) {
   }
 }
 
+// frontier list of the stations marked this round (transfers, footpaths,
+// start labels): every nonzero station-mark word (location, group)
+__global__ void k_list_marked(state st) { list_nonzero(st, st.X, st.tt.n_loc * st.G, st.xlist, C_X); }
+
 // frontier list of the stations reached by the route scan: every nonzero
 // route-reached word (location, group)
 __global__ void k_list_reached(state st) { list_nonzero(st, st.Y, st.tt.n_loc * st.G, st.ylist, C_Y); }
@@ -376,7 +423,7 @@ __global__ void k_transfers_pre(state st) {
       if (lbv == 0xFFFFu || fp + static_cast<int>(lbv) > tad) continue;
       rtw = enc(ln.qtag, fp);
       st.best[li(st, d, s)] = enc(ln.gtag, fp);
-      mark(st, st.X, st.xlist, C_X, d * st.G + g, bit);
+      atomicOr(&st.X[d * st.G + g], bit);  // listed by k_list_marked
       if (fp < tad && tl_n < kMaxTimeline) {
         st.timeline[s * kMaxTimeline + tl_n++] = {d, 0u, fp};
       } else if (fp < tad) {
@@ -400,22 +447,17 @@ __device__ __forceinline__ int tad_at(state const& st, uint32_t s, uint32_t hi, 
   return tad;
 }
 
-// update_transfers, raptor.h:680-743: warp per marked (station, group)
+// update_transfers, raptor.h:680-743: lane per reached (station, query)
 __global__ void k_transfers(state st) {
-  auto const lane = threadIdx.x & 31u;
-  auto const warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  auto const n_warps = (gridDim.x * blockDim.x) >> 5;
-  auto const ny = st.counters[C_Y];
-  for (auto w = warp; w < ny; w += n_warps) {
-    auto const e = st.ylist[w];
-    auto const g = e % st.G, l = e / st.G;
-    auto const s = g * 32u + lane;
-    auto const ln = st.lanes[s];
-    auto const ym = st.Y[e];
-    bool want = false;
-    if (((ym >> lane) & 1u) && ln.run && !((ln.mode & 2u) && ((st.D[e] >> lane) & 1u))) {
-      auto const tk = dec(st.tmp[li(st, l, s)], ln.gtag);
-      if (tk != kKeyInv) {
+  for_each_pair(
+      st.ylist, st.counters[C_Y], [&](uint32_t e) { return st.Y[e]; },
+      [&](uint32_t e, uint32_t b) {
+        auto const g = e % st.G, l = e / st.G;
+        auto const s = g * 32u + b;
+        auto const ln = st.lanes[s];
+        if (!ln.run || ((ln.mode & 2u) && ((st.D[e] >> b) & 1u))) return;
+        auto const tk = dec(st.tmp[li(st, l, s)], ln.gtag);
+        if (tk == kKeyInv) return;
         auto const slp = &st.slots[s];
         auto const tt = static_cast<int>(adjusted<int>(slp->tts, static_cast<int>(st.tt.transfer_time[l])));
         auto const fp = key_add(tk, tt);
@@ -428,14 +470,10 @@ __global__ void k_transfers(state st) {
           if (lbv != 0xFFFFu && fp + static_cast<int>(lbv) <= tad) {
             rtw = enc(ln.qtag, fp);
             st.best[li(st, l, s)] = enc(ln.gtag, fp);
-            want = true;
+            atomicOr(&st.X[e], 1u << b);  // listed by k_list_marked
           }
         }
-      }
-    }
-    auto const b = __ballot_sync(kFull, want);
-    if (lane == 0 && b) mark(st, st.X, st.xlist, C_X, e, b);
-  }
+      });
 }
 
 // update_intermodal_footpaths, raptor.h:954-1026: per query, its egress
@@ -532,7 +570,7 @@ __global__ void k_footpaths_pre(state st) {
       if (lbv == 0xFFFFu || fp + static_cast<int>(lbv) > tad) continue;
       rtw = enc(ln.qtag, fp);
       st.best[li(st, d, s)] = enc(ln.gtag, fp);
-      mark(st, st.X, st.xlist, C_X, d * st.G + g, bit);
+      atomicOr(&st.X[d * st.G + g], bit);  // listed by k_list_marked
       if (fp < tad && tl_n < kMaxTimeline) {
         st.timeline[s * kMaxTimeline + tl_n++] = {c[a].src, c[a].pos, fp};
       } else if (fp < tad) {
@@ -544,61 +582,44 @@ __global__ void k_footpaths_pre(state st) {
   st.timeline_n[s] = tl_n;
 }
 
-// update_footpaths, raptor.h:745-845: warp per marked (station, group);
-// labels of footpath targets are combined with atomicMin (the phase's final
-// labels and marks do not depend on the processing order).
+// update_footpaths, raptor.h:745-845: lane per reached (station, query),
+// walking the station's footpaths; labels of footpath targets are combined
+// with atomicMin (the phase's final labels and marks do not depend on the
+// processing order).
 __global__ void k_footpaths(state st) {
-  auto const lane = threadIdx.x & 31u;
-  auto const warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  auto const n_warps = (gridDim.x * blockDim.x) >> 5;
-  auto const ny = st.counters[C_Y];
   auto const& T = st.tt;
-  for (auto w = warp; w < ny; w += n_warps) {
-    auto const e = st.ylist[w];
-    auto const g = e % st.G, src = e / st.G;
-    auto const s = g * 32u + lane;
-    auto const ln = st.lanes[s];
-    auto const fwd = ln.fwd != 0;
-    bool act = ((st.Y[e] >> lane) & 1u) && ln.run;
-    int tk = kKeyInv;
-    if (act) {
-      tk = dec(st.tmp[li(st, src, s)], ln.gtag);
-      act = tk != kKeyInv;
-    }
-    auto const* idx = fwd ? T.fp_out_idx : T.fp_in_idx;
-    auto const* dat = fwd ? T.fp_out : T.fp_in;
-    auto const b = act ? idx[src] : 0u;
-    auto const n = act ? idx[src + 1] - b : 0u;
-    // lanes of one group may differ in direction: iterate to the longest list
-    auto n_max = n;
-    for (auto o = 16; o > 0; o >>= 1) n_max = max(n_max, __shfl_xor_sync(kFull, n_max, o));
-    slot_t const* slp = &st.slots[s];
-    auto const tad_flat = (act && !(ln.mode & 2u)) ? static_cast<int>(slp->tad[ln.k]) : 0;
-    for (auto j = 0u; j != n_max; ++j) {
-      bool want = false;
-      uint32_t tgt = 0;
-      if (j < n) {
-        auto const fp = dat[b + j];
-        tgt = B2R_FP_TARGET(fp);
-        if (!((ln.mode & 2u) && ((st.D[tgt * st.G + g] >> lane) & 1u))) {
+  for_each_pair(
+      st.ylist, st.counters[C_Y], [&](uint32_t e) { return st.Y[e]; },
+      [&](uint32_t e, uint32_t b) {
+        auto const g = e % st.G, src = e / st.G;
+        auto const s = g * 32u + b;
+        auto const ln = st.lanes[s];
+        if (!ln.run) return;
+        auto const tk = dec(st.tmp[li(st, src, s)], ln.gtag);
+        if (tk == kKeyInv) return;
+        auto const fwd = ln.fwd != 0;
+        auto const* idx = fwd ? T.fp_out_idx : T.fp_in_idx;
+        auto const* dat = fwd ? T.fp_out : T.fp_in;
+        auto const fb = idx[src], n = idx[src + 1] - fb;
+        slot_t const* slp = &st.slots[s];
+        auto const tad_flat = (ln.mode & 2u) ? 0 : static_cast<int>(slp->tad[ln.k]);
+        for (auto j = 0u; j != n; ++j) {
+          auto const fp = dat[fb + j];
+          auto const tgt = B2R_FP_TARGET(fp);
+          if ((ln.mode & 2u) && ((st.D[tgt * st.G + g] >> b) & 1u)) continue;
           auto const key = key_add(tk, adjusted<int>(slp->tts, static_cast<int>(B2R_FP_DURATION(fp))));
           auto const bk = dec(st.best[li(st, tgt, s)], ln.gtag);
-          if (key < bk) {
-            atomicMin(&st.rt[rti(st, ln.k, tgt, s)], enc(ln.qtag, key));
-            auto const tad = (ln.mode & 2u) ? tad_at(st, s, src, j) : tad_flat;
-            if (key <= tad) {
-              auto const lbv = st.lb[li(st, tgt, s)];
-              if (lbv != 0xFFFFu && key + static_cast<int>(lbv) <= tad) {
-                atomicMin(&st.best[li(st, tgt, s)], enc(ln.gtag, key));
-                want = true;
-              }
-            }
+          if (key >= bk) continue;
+          atomicMin(&st.rt[rti(st, ln.k, tgt, s)], enc(ln.qtag, key));
+          auto const tad = (ln.mode & 2u) ? tad_at(st, s, src, j) : tad_flat;
+          if (key > tad) continue;
+          auto const lbv = st.lb[li(st, tgt, s)];
+          if (lbv != 0xFFFFu && key + static_cast<int>(lbv) <= tad) {
+            atomicMin(&st.best[li(st, tgt, s)], enc(ln.gtag, key));
+            atomicOr(&st.X[tgt * st.G + g], 1u << b);  // listed by k_list_marked
           }
         }
-      }
-      mark_warp(st, st.X, st.xlist, C_X, want, tgt * st.G + g, lane);
-    }
-  }
+      });
 }
 
 // ------------------------------------------------- round end / results
@@ -793,7 +814,7 @@ __global__ void k_next(state st) {
     if (key < dec(bw, gtag)) bw = enc(gtag, key);
     auto& rw = st.rt[rti(st, 0, l, s)];
     if (key < dec(rw, qtag)) rw = enc(qtag, key);
-    mark(st, st.X, st.xlist, C_X, l * st.G + g, bit);
+    atomicOr(&st.X[l * st.G + g], bit);  // listed by k_list_marked
   }
   auto const span = sl.one_to_all ? static_cast<int>(sl.max_travel_time)
                                   : (min(static_cast<int>(sl.fastest_direct), static_cast<int>(sl.max_travel_time)) + 1);
