@@ -235,6 +235,10 @@ def gpu_arm(args, rank, world, local):
         st = engine.stats()
         return t1 - t0, st, out
 
+    # launch shape picked by the autotuner on a separate sample of the workload
+    tune_qs = QuerySet(h, WORKLOAD, B, seed=9000 + WORKLOAD)
+    tune = eng.autotune(tune_qs.arr, tune_qs.n)
+    shape = {f: getattr(tune.best, f) for f, _ in A.LaunchShape._fields_}
     for w in range(args.warmup):
         one_batch(w * B)
     clocks = ClockSampler(local)
@@ -278,7 +282,10 @@ def gpu_arm(args, rank, world, local):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot_dev / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int16",
             "data": "synthetic (seeded generator: timetable seed 2, query seed 1002+rank)",
-            "config": config_block(args, B), "method": METHOD,
+            "config": config_block(args, B),
+            "method": dict(METHOD, launch_shape=shape,
+                           autotune={"tried": tune.n_tried, "start_ms": tune.start_ms,
+                                     "best_ms": tune.best_ms}),
             "p50_ms": percentile(lats, 0.5), "p99_ms": percentile(lats, 0.99),
             "e2e": {"value": e2e, "unit": "queries/s", "h2d_bytes_per_step": h2d_step,
                     "d2h_bytes_per_step": d2h // max(1, args.steps)},

@@ -392,6 +392,33 @@ typedef struct b2r_batch_stats {
 } b2r_batch_stats;
 int b2r_last_batch_stats(const b2r_engine* e, b2r_batch_stats* s);
 
+/* Launch shape of the super-step's main kernels.  Results do not depend on
+ * it; throughput does, with the timetable, the query mix and the slot
+ * count.  The counterpart of the reference's fixed GPU launch configuration
+ * (src/routing/gpu/raptor.cu:894-990). */
+typedef struct b2r_launch_shape {
+  uint32_t scan_blocks_per_sm;  /* route scan grid = SMs x this (default 8) */
+  uint32_t scan_threads;        /* route scan block: 32..256 threads, x32 (256) */
+  uint32_t pair_blocks_per_sm;  /* route marking, transfers, footpaths (8) */
+  uint32_t recon_blocks_per_sm; /* reconstruction, 128-thread blocks (4) */
+  uint32_t steps_per_sync;      /* super-steps between host checks (4) */
+} b2r_launch_shape;
+int b2r_engine_get_shape(const b2r_engine* e, b2r_launch_shape* out);
+/* Rejects values out of range; re-captures the super-step graph. */
+int b2r_engine_set_shape(b2r_engine* e, const b2r_launch_shape* shape);
+
+/* Autotuner: runs `sample` (n queries, results discarded) once per candidate
+ * launch shape, one knob at a time over a small grid of values, keeps the
+ * shape with the shortest batch wall time and reports what it tried.  The
+ * last-batch results and statistics are overwritten. */
+typedef struct b2r_tune_report {
+  uint32_t n_tried;
+  b2r_launch_shape start, best;
+  double start_ms, best_ms; /* wall time of the sample batch */
+} b2r_tune_report;
+int b2r_engine_autotune(b2r_engine* e, const b2r_query* sample, uint32_t n,
+                        b2r_tune_report* report);
+
 /* Profiling engines (b2r_engine_config::profile = 1): per route-scan launch of
  * the last b2r_search_batch, its CUDA-event time, the marked (route, query
  * group) entries it scanned and the (route, query) stop steps it made.  *n

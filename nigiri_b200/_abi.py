@@ -130,6 +130,17 @@ class BatchStats(C.Structure):
                 ("host_export_ms", C.c_double), ("host_idle_ms", C.c_double)]
 
 
+class LaunchShape(C.Structure):
+    _fields_ = [("scan_blocks_per_sm", C.c_uint32), ("scan_threads", C.c_uint32),
+                ("pair_blocks_per_sm", C.c_uint32), ("recon_blocks_per_sm", C.c_uint32),
+                ("steps_per_sync", C.c_uint32)]
+
+
+class TuneReport(C.Structure):
+    _fields_ = [("n_tried", C.c_uint32), ("start", LaunchShape), ("best", LaunchShape),
+                ("start_ms", C.c_double), ("best_ms", C.c_double)]
+
+
 class TtBase(C.Structure):
     _fields_ = [
         ("n_locations", C.c_uint32), ("date_range_from", C.c_int32),
@@ -155,6 +166,7 @@ EXPORTS = [
     "b2r_tt_desc", "b2r_tt_destroy", "b2r_queries_generate",
     "b2r_queries_count", "b2r_queries_get", "b2r_queries_destroy",
     "b2r_one_to_all_noalloc", "b2r_last_batch_scan_profile",
+    "b2r_engine_get_shape", "b2r_engine_set_shape", "b2r_engine_autotune",
 ]
 
 
@@ -190,6 +202,9 @@ def _declare(lib):
         "b2r_queries_count": (C.c_uint32, [vp]),
         "b2r_queries_get": (C.POINTER(Query), [vp, C.c_uint32]),
         "b2r_queries_destroy": (C.c_int, [vp]),
+        "b2r_engine_get_shape": (C.c_int, [vp, C.POINTER(LaunchShape)]),
+        "b2r_engine_set_shape": (C.c_int, [vp, C.POINTER(LaunchShape)]),
+        "b2r_engine_autotune": (C.c_int, [vp, C.POINTER(Query), C.c_uint32, C.POINTER(TuneReport)]),
         "b2r_last_batch_scan_profile": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_uint64),
                                                   C.POINTER(C.c_uint64), C.c_uint32,
                                                   C.POINTER(C.c_uint32)]),

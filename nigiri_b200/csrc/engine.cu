@@ -109,6 +109,7 @@ struct b2r_engine {
   b2r::dev::state st{};
   cudaStream_t stream{nullptr};
   cudaGraphExec_t graph{nullptr};
+  b2r_launch_shape shape{8, 256, 8, 4, 4};  // launch shape of the super-step
   cudaGraphExec_t lb_graph{nullptr};  // 4 x 2 Bellman-Ford iterations
   int sms{132};
   std::vector<void*> allocs;
@@ -387,7 +388,8 @@ void enqueue_superstep(b2r_engine& e, cudaStream_t s) {
   dev::k_ctl_begin<<<slot_blocks, 128, 0, s>>>(st);
   dev::k_sweep<<<e.sms * 16, 256, 0, s>>>(st);
   dev::k_ctl_dest<<<slot_blocks, 128, 0, s>>>(st);
-  dev::k_mark_routes<<<list_blocks, 256, 0, s>>>(st);
+  auto const pair_blocks = e.sms * e.shape.pair_blocks_per_sm;
+  dev::k_mark_routes<<<pair_blocks, 256, 0, s>>>(st);
   dev::k_list_routes<<<e.sms * 8, 256, 0, s>>>(st);
   dev::k_ctl_marked<<<slot_blocks, 128, 0, s>>>(st);
   cudaEvent_t ev_a = nullptr, ev_b = nullptr;
@@ -401,7 +403,7 @@ void enqueue_superstep(b2r_engine& e, cudaStream_t s) {
     ev_b = e.prof_ev[e.prof_used++];
     B2R_CUDA(cudaEventRecord(ev_a, s));
   }
-  dev::k_route_scan<<<e.sms * 8, 256, 0, s>>>(st);
+  dev::k_route_scan<<<e.sms * e.shape.scan_blocks_per_sm, e.shape.scan_threads, 0, s>>>(st);
   if (e.cfg.profile) {
     B2R_CUDA(cudaEventRecord(ev_b, s));
     auto const idx = static_cast<uint32_t>(e.prof_used / 2 - 1);
@@ -411,10 +413,10 @@ void enqueue_superstep(b2r_engine& e, cudaStream_t s) {
   dev::k_clear_x<<<list_blocks, 256, 0, s>>>(st);
   dev::k_reset_x<<<1, 32, 0, s>>>(st);
   dev::k_transfers_pre<<<slot_blocks, 128, 0, s>>>(st);
-  dev::k_transfers<<<list_blocks, 256, 0, s>>>(st);
+  dev::k_transfers<<<pair_blocks, 256, 0, s>>>(st);
   dev::k_intermodal<<<slot_blocks, 128, 0, s>>>(st);
   dev::k_footpaths_pre<<<slot_blocks, 128, 0, s>>>(st);
-  dev::k_footpaths<<<list_blocks, 256, 0, s>>>(st);
+  dev::k_footpaths<<<pair_blocks, 256, 0, s>>>(st);
   dev::k_ctl_end<<<slot_blocks, 128, 0, s>>>(st);
   dev::k_collect<<<slot_blocks, 128, 0, s>>>(st);
   cudaEvent_t rc_a = nullptr, rc_b = nullptr;
@@ -428,7 +430,7 @@ void enqueue_superstep(b2r_engine& e, cudaStream_t s) {
     rc_b = e.prof_rc_ev[e.prof_rc_used++];
     B2R_CUDA(cudaEventRecord(rc_a, s));
   }
-  dev::k_reconstruct<<<e.sms * 4, 128, 0, s>>>(st);
+  dev::k_reconstruct<<<e.sms * e.shape.recon_blocks_per_sm, 128, 0, s>>>(st);
   if (e.cfg.profile) B2R_CUDA(cudaEventRecord(rc_b, s));
   dev::k_next<<<slot_blocks, 128, 0, s>>>(st);
   dev::k_list_marked<<<e.sms * 8, 256, 0, s>>>(st);
@@ -1191,7 +1193,7 @@ struct serve_state {
 
   void driver_loop() {
     auto* st = e.stream;
-    auto const chunk = e.cfg.steps_per_sync != 0 ? e.cfg.steps_per_sync : 2U;
+    auto const chunk = e.cfg.steps_per_sync != 0 ? e.cfg.steps_per_sync : std::min(2U, e.shape.steps_per_sync);
     auto const use_graph = e.cfg.use_graphs != 0 && e.graph != nullptr;
     try {
       B2R_CUDA(cudaSetDevice(e.tt->device));
@@ -1489,6 +1491,7 @@ int b2r_engine_create(b2r_timetable* tt, const b2r_engine_config* cfg_in, b2r_en
       e->max_j = std::max(32U, std::min(4096U, (cfg.max_journeys + 31U) & ~31U));
       e->max_starts = cfg.max_starts != 0 ? cfg.max_starts : 4096U;
       if (cfg.profile) e->cfg.use_graphs = 0;
+      if (cfg.steps_per_sync != 0) e->shape.steps_per_sync = cfg.steps_per_sync;
       e->max_dest = 512U;
       e->max_off = 128U;
       if (cfg.use_lower_bounds == 3) {  // the table when it fits, else no bounds
@@ -1641,7 +1644,7 @@ int b2r_search_batch(b2r_engine* e, const b2r_query* qs, uint32_t n, b2r_result*
       prep.start(*e, qs, n, runs, false);
       b2r::batch_runner br{*e, runs, e->cfg.use_graphs != 0 && e->graph != nullptr};
       if (e->cfg.profile) B2R_CUDA(cudaMemsetAsync(e->st.prof, 0, 8 * sizeof(unsigned long long), e->stream));
-      br.run(e->cfg.steps_per_sync != 0 ? e->cfg.steps_per_sync : 4U);
+      br.run(e->shape.steps_per_sync);
       prep.join();
       auto const t1 = std::chrono::steady_clock::now();
       B2R_CUDA(cudaStreamSynchronize(e->stream));
@@ -1723,6 +1726,99 @@ int b2r_search_plain(b2r_engine* e, const b2r_query* q, b2r_result* out) {
       e->last.kernel_launches = br.launches;
       e->last.super_steps = br.steps;
       b2r::fill_out(*e, runs, out);
+      return B2R_OK;
+    } catch (b2r::cuda_error const& ex) {
+      return b2r::fail(B2R_ERR_CUDA, ex.what());
+    }
+  });
+}
+
+int b2r_engine_get_shape(const b2r_engine* e, b2r_launch_shape* out) {
+  if (e == nullptr || out == nullptr) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
+  *out = e->shape;
+  return B2R_OK;
+}
+
+int b2r_engine_set_shape(b2r_engine* e, const b2r_launch_shape* sh) {
+  B2R_API_GUARD({
+    if (e == nullptr || sh == nullptr) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
+    if (e->serving) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "engine is serving");
+    auto const ok = sh->scan_blocks_per_sm >= 1 && sh->scan_blocks_per_sm <= 64 &&
+                    sh->scan_threads >= 32 && sh->scan_threads <= 256 && sh->scan_threads % 32 == 0 &&
+                    sh->pair_blocks_per_sm >= 1 && sh->pair_blocks_per_sm <= 64 &&
+                    sh->recon_blocks_per_sm >= 1 && sh->recon_blocks_per_sm <= 64 &&
+                    sh->steps_per_sync >= 1 && sh->steps_per_sync <= 64;
+    if (!ok) {
+      return b2r::fail(B2R_ERR_INVALID_ARGUMENT,
+                       "launch shape out of range (blocks per SM 1..64, scan threads 32..256 in steps "
+                       "of 32, steps per sync 1..64)");
+    }
+    try {
+      B2R_CUDA(cudaSetDevice(e->tt->device));
+      e->shape = *sh;
+      if (e->graph != nullptr) {  // the graph holds the old launch configuration
+        B2R_CUDA(cudaStreamSynchronize(e->stream));
+        cudaGraphExecDestroy(e->graph);
+        e->graph = nullptr;
+        b2r::capture_graph(*e);
+      }
+      return B2R_OK;
+    } catch (b2r::cuda_error const& ex) {
+      return b2r::fail(B2R_ERR_CUDA, ex.what());
+    }
+  });
+}
+
+int b2r_engine_autotune(b2r_engine* e, const b2r_query* sample, uint32_t n, b2r_tune_report* report) {
+  B2R_API_GUARD({
+    if (e == nullptr || sample == nullptr || n == 0) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
+    if (e->serving) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "engine is serving");
+    std::vector<b2r_result> out(n);
+    // objective: wall time of the sample batch (best of two runs)
+    auto const measure = [&](b2r_launch_shape const& sh) -> double {
+      if (auto const rc = b2r_engine_set_shape(e, &sh); rc != B2R_OK) throw b2r::cuda_error(b2r_last_error());
+      auto best = 1e300;
+      for (auto rep = 0; rep != 2; ++rep) {
+        if (b2r_search_batch(e, sample, n, out.data()) != B2R_OK) throw b2r::cuda_error(b2r_last_error());
+        best = std::min(best, e->last.host_prep_ms);
+      }
+      return best;
+    };
+    try {
+      b2r_tune_report rep{};
+      auto cur = e->shape;
+      rep.start = cur;
+      if (b2r_search_batch(e, sample, n, out.data()) != B2R_OK) return B2R_ERR_INTERNAL;  // warm-up
+      auto cur_ms = measure(cur);
+      rep.start_ms = cur_ms;
+      rep.n_tried = 1;
+      // coordinate descent, one pass over the knobs
+      struct knob {
+        uint32_t b2r_launch_shape::*field;
+        std::vector<uint32_t> values;
+      };
+      std::vector<knob> const knobs = {{&b2r_launch_shape::scan_blocks_per_sm, {2, 4, 8, 16, 32}},
+                                       {&b2r_launch_shape::scan_threads, {128, 256}},
+                                       {&b2r_launch_shape::pair_blocks_per_sm, {2, 4, 8, 16}},
+                                       {&b2r_launch_shape::recon_blocks_per_sm, {1, 2, 4, 8}},
+                                       {&b2r_launch_shape::steps_per_sync, {1, 2, 4, 8}}};
+      for (auto const& k : knobs) {
+        for (auto const v : k.values) {
+          if (cur.*(k.field) == v) continue;
+          auto trial = cur;
+          trial.*(k.field) = v;
+          auto const ms = measure(trial);
+          ++rep.n_tried;
+          if (ms < cur_ms) {
+            cur = trial;
+            cur_ms = ms;
+          }
+        }
+      }
+      if (b2r_engine_set_shape(e, &cur) != B2R_OK) return B2R_ERR_CUDA;
+      rep.best = cur;
+      rep.best_ms = cur_ms;
+      if (report != nullptr) *report = rep;
       return B2R_OK;
     } catch (b2r::cuda_error const& ex) {
       return b2r::fail(B2R_ERR_CUDA, ex.what());

@@ -254,6 +254,23 @@ class Engine:
         _check(A.lib().b2r_last_batch_stats(self.handle, C.byref(s)))
         return s
 
+    @property
+    def shape(self) -> A.LaunchShape:
+        sh = A.LaunchShape()
+        _check(A.lib().b2r_engine_get_shape(self.handle, C.byref(sh)))
+        return sh
+
+    @shape.setter
+    def shape(self, sh: A.LaunchShape):
+        _check(A.lib().b2r_engine_set_shape(self.handle, C.byref(sh)))
+
+    def autotune(self, qarr, n: int) -> A.TuneReport:
+        """Picks the launch shape with the shortest batch time on a sample
+        (b2r_engine_autotune); results do not depend on the shape."""
+        rep = A.TuneReport()
+        _check(A.lib().b2r_engine_autotune(self.handle, qarr, n, C.byref(rep)))
+        return rep
+
     def scan_profile(self, cap: int = 4096):
         """Per route-scan launch of the last batch (profiling engines):
         [(milliseconds, marked entries, stop visits)]."""

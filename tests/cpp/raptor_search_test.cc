@@ -1,0 +1,150 @@
+// Parity harness in the style of nigiri's test/raptor_search.cc: the same
+// queries run through the C++ mirror of nigiri's routing interface
+// (b2r.hpp -> the B200 engine) and through the CPU oracle (test
+// infrastructure), and the complete journeys (every leg) must be equal.
+// One-to-all searches compare the round times of every location.
+//
+//   raptor_search_test            exit 0 when every query matches
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "b2r.hpp"
+#include "oracle.h"
+
+namespace r = b2r::routing;
+
+namespace {
+
+r::query from_c(b2r_query const& c) {  // the generator's queries in nigiri's terms
+  r::query q;
+  if (c.is_interval) q.start_time_ = r::interval{c.interval_from, c.interval_to};
+  else q.start_time_ = c.start_time;
+  q.start_match_mode_ = static_cast<r::location_match_mode>(c.start_match_mode);
+  q.dest_match_mode_ = static_cast<r::location_match_mode>(c.dest_match_mode);
+  q.use_start_footpaths_ = c.use_start_footpaths != 0;
+  for (auto i = 0U; i != c.n_start; ++i) {
+    q.start_.push_back({c.start[i].target, c.start[i].duration, c.start[i].transport_mode_id});
+  }
+  for (auto i = 0U; i != c.n_destination; ++i) {
+    q.destination_.push_back({c.destination[i].target, c.destination[i].duration,
+                              c.destination[i].transport_mode_id});
+  }
+  q.max_start_offset_ = c.max_start_offset;
+  q.max_transfers_ = c.max_transfers;
+  q.max_travel_time_ = c.max_travel_time;
+  q.min_connection_count_ = c.min_connection_count;
+  q.extend_interval_earlier_ = c.extend_interval_earlier != 0;
+  q.extend_interval_later_ = c.extend_interval_later != 0;
+  if (c.has_fastest_direct) q.fastest_direct_ = c.fastest_direct;
+  q.fastest_direct_factor_ = c.fastest_direct_factor;
+  q.transfer_time_settings_ = {c.tts_default != 0, c.tts_min_transfer_time, c.tts_additional_time,
+                               c.tts_factor};
+  return q;
+}
+
+void print(char const* who, std::vector<r::journey> const& js) {
+  std::printf("  %s: %zu journeys\n", who, js.size());
+  for (auto const& j : js) {
+    std::printf("    [%d -> %d] transfers=%u dest=%u\n", j.start_time_, j.dest_time_, j.transfers_, j.dest_);
+    for (auto const& l : j.legs_) {
+      std::printf("      %u -> %u  %d .. %d  ", l.from_, l.to_, l.dep_time_, l.arr_time_);
+      if (auto const* t = std::get_if<r::run_enter_exit>(&l.uses_)) {
+        std::printf("transport %u day %u stops [%u, %u)\n", t->transport_, t->day_, t->stop_from_, t->stop_to_);
+      } else if (auto const* f = std::get_if<r::footpath>(&l.uses_)) {
+        std::printf("footpath %u min\n", f->duration_);
+      } else {
+        auto const& o = std::get<r::offset>(l.uses_);
+        std::printf("offset %u min mode %d\n", o.duration_, o.transport_mode_id_);
+      }
+    }
+  }
+}
+
+std::vector<r::journey> oracle_journeys(b2r_timetable_desc const& d, b2r_query const& q) {
+  or_result* res = nullptr;
+  b2r::check(or_search(&d, &q, &res), "or_search");
+  b2r_result view{};
+  or_result_view(res, &view, nullptr);
+  auto out = r::journeys_of(view);
+  or_result_free(res);
+  return out;
+}
+
+int run_workload(uint32_t workload, uint32_t timetable_seed, uint32_t n, uint64_t query_seed) {
+  b2r_host_timetable* h = nullptr;
+  b2r::check(b2r_tt_generate(workload, timetable_seed, &h), "b2r_tt_generate");
+  b2r_timetable_desc d{};
+  b2r_tt_desc(h, &d);
+  b2r_query_set* qs = nullptr;
+  b2r::check(b2r_queries_generate(h, workload, query_seed, n, &qs), "b2r_queries_generate");
+  auto const n_q = b2r_queries_count(qs);
+
+  b2r::timetable tt{d};
+  b2r::engine eng{tt};
+  int bad = 0;
+  size_t n_journeys = 0;
+  for (auto dir : {r::direction::kForward, r::direction::kBackward}) {
+    std::vector<r::query> batch;
+    std::vector<b2r_query const*> cq;
+    for (auto i = 0U; i != n_q; ++i) {
+      auto const* c = b2r_queries_get(qs, i);
+      if (c->kind != B2R_ONE_TO_ONE || c->direction != static_cast<uint8_t>(dir)) continue;
+      batch.push_back(from_c(*c));
+      cq.push_back(c);
+    }
+    if (batch.empty()) continue;
+    auto const got = r::raptor_search(eng, batch, dir);
+    for (auto i = 0U; i != batch.size(); ++i) {
+      auto const want = oracle_journeys(d, *cq[i]);
+      n_journeys += want.size();
+      if (got[i].status_ != B2R_OK || got[i].journeys_ != want) {
+        ++bad;
+        std::printf("workload %u query %u (%s) differs\n", workload, i,
+                    dir == r::direction::kForward ? "forward" : "backward");
+        print("engine", got[i].journeys_);
+        print("oracle", want);
+      }
+    }
+  }
+  // one-to-all on the first queries of the set, both directions
+  for (auto i = 0U; i != 4U && i < n_q; ++i) {
+    auto c = *b2r_queries_get(qs, i);
+    c.kind = B2R_ONE_TO_ALL;
+    c.n_destination = 0;
+    c.is_interval = 0;
+    c.direction = static_cast<uint8_t>(i % 2U);
+    auto const state = r::one_to_all(eng, from_c(c), static_cast<r::direction>(c.direction));
+    or_result* res = nullptr;
+    b2r::check(or_search(&d, &c, &res), "or_search");
+    int16_t const* rows = nullptr;
+    int16_t const* best = nullptr;
+    int32_t base_day = 0;
+    or_result_state(res, &rows, &best, &base_day);
+    auto const same = base_day == state.base_day_ &&
+                      std::memcmp(rows, state.round_times_.data(), state.round_times_.size() * 2) == 0;
+    or_result_free(res);
+    if (!same) {
+      ++bad;
+      std::printf("workload %u one_to_all %u differs\n", workload, i);
+    }
+  }
+  std::printf("workload %u: %u queries, %zu journeys, %d differ\n", workload, n_q, n_journeys, bad);
+  b2r_queries_destroy(qs);
+  b2r_tt_destroy(h);
+  return bad;
+}
+
+}  // namespace
+
+int main() {
+  try {
+    auto bad = run_workload(1, 1, 200, 4711);  // city, forward one-to-one
+    bad += run_workload(3, 2, 48, 4712);        // regional, range, both directions
+    std::printf(bad == 0 ? "ok\n" : "FAILED\n");
+    return bad == 0 ? 0 : 1;
+  } catch (b2r::error const& e) {
+    std::printf("error %d: %s\n", e.status, e.what());
+    return 2;
+  }
+}

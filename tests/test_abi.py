@@ -31,9 +31,10 @@ def test_struct_layouts_match_c():
 #include <stddef.h>
 #include "b2r.h"
 int main() {
-  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(b2r_timetable_desc), sizeof(b2r_offset),
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(b2r_timetable_desc), sizeof(b2r_offset),
          sizeof(b2r_query), sizeof(b2r_leg), sizeof(b2r_journey), sizeof(b2r_result),
-         sizeof(b2r_engine_config), sizeof(b2r_batch_stats), sizeof(b2r_tt_base));
+         sizeof(b2r_engine_config), sizeof(b2r_batch_stats), sizeof(b2r_tt_base),
+         sizeof(b2r_launch_shape), sizeof(b2r_tune_report));
   printf("%zu %zu %zu\n", offsetof(b2r_query, tts_factor), offsetof(b2r_leg, transport_mode_id),
          offsetof(b2r_result, n_start_times));
   return 0;
@@ -48,7 +49,8 @@ int main() {
     sizes = [int(x) for x in out[0].split()]
     assert sizes == [C.sizeof(A.TimetableDesc), C.sizeof(A.Offset), C.sizeof(A.Query),
                      C.sizeof(A.Leg), C.sizeof(A.Journey), C.sizeof(A.Result),
-                     C.sizeof(A.EngineConfig), C.sizeof(A.BatchStats), C.sizeof(A.TtBase)]
+                     C.sizeof(A.EngineConfig), C.sizeof(A.BatchStats), C.sizeof(A.TtBase),
+                     C.sizeof(A.LaunchShape), C.sizeof(A.TuneReport)]
     offs = [int(x) for x in out[1].split()]
     assert offs == [A.Query.tts_factor.offset, A.Leg.transport_mode_id.offset,
                     A.Result.n_start_times.offset]
@@ -96,3 +98,11 @@ def test_serving_entry_points_reject_null_engine():
     assert lib.b2r_poll(None, 1, C.byref(r)) == A.B2R_ERR_INVALID_ARGUMENT
     assert lib.b2r_wait(None, 1, C.byref(r)) == A.B2R_ERR_INVALID_ARGUMENT
     assert lib.b2r_release(None, 1) == A.B2R_ERR_INVALID_ARGUMENT
+
+
+def test_launch_shape_entry_points_reject_null():
+    lib = A.lib()
+    sh = A.LaunchShape()
+    assert lib.b2r_engine_get_shape(None, C.byref(sh)) == A.B2R_ERR_INVALID_ARGUMENT
+    assert lib.b2r_engine_set_shape(None, C.byref(sh)) == A.B2R_ERR_INVALID_ARGUMENT
+    assert lib.b2r_engine_autotune(None, None, 0, None) == A.B2R_ERR_INVALID_ARGUMENT
