@@ -192,8 +192,19 @@ void finalize(host_timetable& t) {
   if (t.parent.empty()) t.parent.assign(t.n_locations, kInvalid);
   if (t.location_type.empty()) t.location_type.assign(t.n_locations, 0U);
   if (t.children_index.empty()) {
+    // children_ of each parent in location order, as the loaders append
+    // them while reading stops (gtfs/stop.cc, hrd/stamm/meta_stations)
+    std::vector<uint32_t> n_children(t.n_locations, 0U);
+    for (auto l = 0U; l != t.n_locations; ++l) {
+      if (t.parent[l] != kInvalid) ++n_children[t.parent[l]];
+    }
     t.children_index.assign(t.n_locations + 1U, 0U);
-    t.children.clear();
+    for (auto l = 0U; l != t.n_locations; ++l) t.children_index[l + 1] = t.children_index[l] + n_children[l];
+    t.children.assign(t.children_index[t.n_locations], 0U);
+    auto fill = std::vector<uint32_t>(t.children_index.begin(), t.children_index.end() - 1);
+    for (auto l = 0U; l != t.n_locations; ++l) {
+      if (t.parent[l] != kInvalid) t.children[fill[t.parent[l]]++] = l;
+    }
   }
 
   // footpaths_in from footpaths_out, then sorted by duration

@@ -51,6 +51,10 @@ class FixtureTimetable:
         tt_ = np.zeros(n_loc, np.uint8)
         for k, x in enumerate(spec["locations"]):
             tt_[N_SPECIAL + k] = x.get("transfer_time", 2)
+        parent = np.full(n_loc, 0xFFFFFFFF, np.uint32)
+        for k, x in enumerate(spec["locations"]):
+            if x.get("parent"):
+                parent[N_SPECIAL + k] = self.loc_idx[x["parent"]]
         fps = [[] for _ in range(n_loc)]
         for a, b, dur in spec.get("footpaths", []):
             fps[self.loc_idx[a]].append((self.loc_idx[b] & 0x7FFFFF) | (dur << 23))
@@ -96,7 +100,7 @@ class FixtureTimetable:
                 for tr in trs:
                     stop_times.append(_enc(tr["times"][2 * s + 1]))
         self.arrays = dict(
-            transfer_time=tt_, fp_index=fp_index, fp_data=np.array(fp_data or [0], np.uint32),
+            transfer_time=tt_, parent=parent, fp_index=fp_index, fp_data=np.array(fp_data or [0], np.uint32),
             route_stop_index=np.array(route_stop_index, np.uint32),
             route_stops=np.array(route_stops or [0], np.uint32),
             route_n_t=np.array(route_n_t or [0], np.uint32),
@@ -111,6 +115,8 @@ class FixtureTimetable:
         base.date_range_from = d_from
         base.date_range_to = d_to
         base.transfer_time = p(a["transfer_time"], C.c_uint8)
+        if any(x.get("parent") for x in spec["locations"]):
+            base.parent = p(a["parent"], C.c_uint32)
         base.footpaths_out_index = p(a["fp_index"], C.c_uint32)
         base.footpaths_out = p(a["fp_data"], C.c_uint32)
         base.n_routes = len(spec["routes"])
@@ -134,7 +140,8 @@ class FixtureTimetable:
             pass
 
 
-MODES = {"exact": A.B2R_MATCH_EXACT, "intermodal": A.B2R_MATCH_INTERMODAL}
+MODES = {"exact": A.B2R_MATCH_EXACT, "intermodal": A.B2R_MATCH_INTERMODAL,
+         "equivalent": A.B2R_MATCH_EQUIVALENT, "only_children": A.B2R_MATCH_ONLY_CHILDREN}
 
 
 class FixtureQuery:
@@ -170,6 +177,8 @@ class FixtureQuery:
             qq.max_travel_time = q["max_travel_time"]
         if "max_transfers" in q:
             qq.max_transfers = q["max_transfers"]
+        if "max_start_offset" in q:
+            qq.max_start_offset = q["max_start_offset"]
         qq.min_connection_count = q.get("min_connection_count", 0)
         qq.extend_interval_earlier = 1 if q.get("extend_earlier") else 0
         qq.extend_interval_later = 1 if q.get("extend_later") else 0

@@ -143,7 +143,62 @@ def gtfs_transfer_time():
     }
 
 
-TIMETABLES = {"hrd_abc": hrd_abc(), "gtfs_transfer_time": gtfs_transfer_time()}
+def hrd_simple():
+    """test/loader/hrd/hrd_timetable.h files_simple(): like files_abc() but
+    the second service runs back from B to A:
+      RE 1337 A 02:30 -> B 03:30, repeated 48 times every 30 min
+      RE 7331 B 02:30 -> A 03:30, repeated 92 times every 15 min
+    on 30.03.2020, local time UTC+2 -> UTC departures 00:30 + j*30 / j*15."""
+    locs = [("0000001", "A"), ("0000002", "B"), ("0000003", "C"),
+            ("0000004", "D"), ("0000005", "E"), ("0000006", "F"),
+            ("0000007", "G"), ("0000008", "H"), ("0000009", "I"),
+            ("0000010", "F_META")]
+    services = []
+    for j in range(49):
+        dep = 30 + 30 * j
+        services.append(utc_service("RE 1337", ["0000001", "0000002"], "2020-03-30",
+                                    [dep, dep + 60]))
+    for j in range(93):
+        dep = 30 + 15 * j
+        services.append(utc_service("RE 7331", ["0000002", "0000001"], "2020-03-30",
+                                    [dep, dep + 60]))
+    return {
+        "date_range": ["2020-03-28", "2020-03-31"],
+        "locations": [{"id": i, "name": n, "transfer_time": 2} for i, n in locs],
+        "footpaths": [],
+        "routes": group_routes(services),
+    }
+
+
+def gtfs_dijkstra():
+    """test/routing/dijkstra_test.cc dijkstra_files(): agency Europe/Berlin
+    (UTC+2 on 2024-06-08), service S on 2024-06-08 only.  C1, C2 are children
+    of C and D1, D2 children of station D; transfers.txt (type 2) gives
+    footpaths D1 <-> D2 of 600 s and C1 <-> C2 of 900 s (no coordinates, so
+    no other footpaths).
+      AB_TRP A 09:00 -> B 09:30     UTC 07:00 -> 07:30
+      BC_TRP B 10:00 -> C2 11:00    UTC 08:00 -> 09:00
+      DB_TRP D1 09:30 -> B 09:45    UTC 07:30 -> 07:45
+      DC_TRP D2 10:30 -> C1 11:30   UTC 08:30 -> 09:30"""
+    d = "2024-06-08"
+    services = [
+        dict(utc_service("AB", ["A", "B"], d, [hm("07:00"), hm("07:30")]), id="AB_TRP"),
+        dict(utc_service("BC", ["B", "C2"], d, [hm("08:00"), hm("09:00")]), id="BC_TRP"),
+        dict(utc_service("DB", ["D1", "B"], d, [hm("07:30"), hm("07:45")]), id="DB_TRP"),
+        dict(utc_service("DC", ["D2", "C1"], d, [hm("08:30"), hm("09:30")]), id="DC_TRP"),
+    ]
+    parents = {"C1": "C", "C2": "C", "D1": "D", "D2": "D"}
+    return {
+        "date_range": ["2024-06-07", "2024-06-09"],
+        "locations": [{"id": x, "name": x, "transfer_time": 2, "parent": parents.get(x)}
+                      for x in ["A", "B", "C", "C1", "C2", "D", "D1", "D2"]],
+        "footpaths": [["D1", "D2", 10], ["D2", "D1", 10], ["C1", "C2", 15], ["C2", "C1", 15]],
+        "routes": group_routes(services),
+    }
+
+
+TIMETABLES = {"hrd_abc": hrd_abc(), "gtfs_transfer_time": gtfs_transfer_time(),
+              "hrd_simple": hrd_simple(), "gtfs_dijkstra": gtfs_dijkstra()}
 
 # ----------------------------------------------------------------------------
 # Golden printout parser (journey::print, src/routing/journey.cc)
@@ -307,6 +362,46 @@ def cases():
     return c
 
 
+# ----------------------------------------------------------------------------
+# Known answers of intermediate steps: start labels (start_times_test.cc) and
+# lower bounds (dijkstra_test.cc), parsed from the test sources.
+# ----------------------------------------------------------------------------
+START_LINE = re.compile(r"^\|  \{time_at_start=" + _TIME + r", time_at_stop=" + _TIME +
+                        r", stop=([^}]*)\}$")
+
+
+def parse_starts(text: str):
+    out = []
+    for line in text.splitlines():
+        m = START_LINE.match(line.strip("\n"))
+        if m:
+            out.append([unix_min(m.group(1)), unix_min(m.group(2)), m.group(3)])
+    return out
+
+
+def known_answers(ref_root: str):
+    ka = []
+    src = open(os.path.join(ref_root, "test/routing/start_times_test.cc")).read()
+    ka.append(dict(name="start_times_interval", kind="starts", timetable="hrd_simple",
+                   ref="test/routing/start_times_test.cc",
+                   query=dict(start=[["0000001", 15, 0], ["0000002", 30, 0]],
+                              dest=[], interval=[t("2020-03-30 00:00"), t("2020-03-31 00:00")],
+                              direction="fwd", max_start_offset=32767),
+                   expected=parse_starts(raw_string(src, "expected"))))
+    src = open(os.path.join(ref_root, "test/routing/dijkstra_test.cc")).read()
+    got = re.findall(r"EXPECT_EQ\((\d+)U, dists\[(\w+)_l\.v_\]\)", src)
+    names = {"d1": "D1", "d": "D"}
+    start = t("2024-06-08 07:00")
+    queries = [dict(start=[["D1", 0, 0]], dest=[["C2", 0, 0]], start_time=start),
+               dict(start=[["D", 0, 0]], dest=[["C", 0, 0]], start_time=start,
+                    start_mode="equivalent", dest_mode="equivalent")]
+    for (value, var), q in zip(got, queries):
+        ka.append(dict(name=f"dijkstra_{var}", kind="lower_bounds", timetable="gtfs_dijkstra",
+                       ref="test/routing/dijkstra_test.cc", query=q,
+                       expected=[[names[var], int(value)]]))
+    return ka
+
+
 def main(ref_root: str):
     out_cases = []
     for case in cases():
@@ -325,6 +420,7 @@ def main(ref_root: str):
         case["expected"] = expected
         out_cases.append(case)
     doc = {"timetables": TIMETABLES, "cases": out_cases,
+           "known_answers": known_answers(ref_root),
            "generated_by": "tests/golden/make_fixtures.py"}
     with open(os.path.join(HERE, "cases.json"), "w") as f:
         json.dump(doc, f, indent=1, sort_keys=True)

@@ -161,3 +161,33 @@ def test_lower_bound_modes_give_identical_journeys(c2, lb_mode):
     a, _ = run_batch(eng, qs.arr, qs.n)
     b, _ = run_batch(other, qs.arr, qs.n)
     assert a == b
+
+
+FIXTURE_QUERIES = [
+    # parents and children (dijkstra_test.cc's feed): exact, equivalent,
+    # range, both directions
+    ("gtfs_dijkstra", dict(start=[["D1", 0, 0]], dest=[["C2", 0, 0]], start_time=28630500)),
+    ("gtfs_dijkstra", dict(start=[["D", 0, 0]], dest=[["C", 0, 0]], start_time=28630500,
+                           start_mode="equivalent", dest_mode="equivalent")),
+    ("gtfs_dijkstra", dict(start=[["A", 0, 0], ["D1", 5, 0]], dest=[["C", 0, 0]],
+                           interval=[28630440, 28630680], dest_mode="equivalent")),
+    ("gtfs_dijkstra", dict(start=[["C2", 0, 0]], dest=[["D", 0, 0]], interval=[28630620, 28630740],
+                           direction="bwd", dest_mode="equivalent", start_mode="equivalent")),
+    # start_times_test.cc's feed: two start offsets over a day
+    ("hrd_simple", dict(start=[["0000001", 15, 0], ["0000002", 30, 0]], dest=[["0000002", 0, 0]],
+                        interval=[26425440, 26426880])),
+    ("hrd_simple", dict(start=[["0000002", 0, 0]], dest=[["0000001", 10, 0]],
+                        interval=[26425440, 26426880], direction="bwd")),
+]
+
+
+@pytest.mark.parametrize("tt_name,q", FIXTURE_QUERIES)
+def test_fixture_queries_match_oracle(golden_engines, tt_name, q):
+    """Engine against the oracle on the fixtures of nigiri's start-time and
+    Dijkstra tests (the oracle is pinned on their known answers)."""
+    ftt, _, eng = golden_engines[tt_name]
+    fq = F.FixtureQuery(A.lib(), ftt, q)
+    res = A.Result()
+    assert A.lib().b2r_search_batch(eng.handle, C.byref(fq.q), 1, C.byref(res)) == 0
+    exp = oracle_lib.OracleResult(ftt.desc, fq.q).records()
+    assert records(res) == exp

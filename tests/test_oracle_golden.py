@@ -30,3 +30,34 @@ def test_golden_cases_cover_both_directions_and_intermodal():
     assert any("backward" in n or n.endswith("_bwd") for n in names)
     assert any("intermodal" in n for n in names)
     assert sum(len(c["expected"]) for c in CASES["cases"]) >= 40
+
+
+def _names(tt):
+    by_id = {x["id"]: x["name"] for x in tt.spec["locations"]}
+    return {idx: by_id.get(i, i) for i, idx in tt.loc_idx.items()}
+
+
+@pytest.mark.parametrize("ka", CASES["known_answers"], ids=[k["name"] for k in CASES["known_answers"]])
+def test_oracle_known_answers(ka, timetables):
+    """Intermediate results pinned by nigiri's own tests: the start labels of
+    an interval search (start_times_test.cc) and Dijkstra lower bounds over
+    a timetable with parent stations (dijkstra_test.cc)."""
+    tt = timetables[ka["timetable"]]
+    q = F.FixtureQuery(A.lib(), tt, ka["query"])
+    L = oracle_lib.lib()
+    name = _names(tt)
+    if ka["kind"] == "starts":
+        cap = 1 << 14
+        tas, tst = (C.c_int32 * cap)(), (C.c_int32 * cap)()
+        stop = (C.c_uint32 * cap)()
+        n = C.c_uint32()
+        assert L.or_get_starts(C.byref(tt.desc), C.byref(q.q), tas, tst, stop, cap, C.byref(n)) == 0
+        # the test's own order: descending by (time_at_start, time_at_stop,
+        # stop), duplicates removed
+        got = sorted({(tas[i], tst[i], stop[i]) for i in range(n.value)}, reverse=True)
+        assert [[a, b, name[s]] for a, b, s in got] == ka["expected"]
+    else:
+        dists = (C.c_uint16 * tt.desc.n_locations)()
+        assert L.or_lower_bounds(C.byref(tt.desc), C.byref(q.q), dists) == 0
+        for loc, value in ka["expected"]:
+            assert dists[tt.loc_idx[loc]] == value, loc
