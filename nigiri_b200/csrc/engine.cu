@@ -109,6 +109,7 @@ struct b2r_engine {
   b2r::dev::state st{};
   cudaStream_t stream{nullptr};
   cudaGraphExec_t graph{nullptr};
+  cudaStream_t stream2{nullptr};  // exports overlapping the super-steps
   b2r_launch_shape shape{8, 256, 8, 4, 4};  // launch shape of the super-step
   cudaGraphExec_t lb_graph{nullptr};  // 4 x 2 Bellman-Ford iterations
   int sms{132};
@@ -365,6 +366,7 @@ b2r_engine::~b2r_engine() {
   if (graph != nullptr) cudaGraphExecDestroy(graph);
   if (lb_graph != nullptr) cudaGraphExecDestroy(lb_graph);
   if (stream != nullptr) cudaStreamDestroy(stream);
+  if (stream2 != nullptr) cudaStreamDestroy(stream2);
   if (ev0 != nullptr) cudaEventDestroy(ev0);
   if (ev1 != nullptr) cudaEventDestroy(ev1);
   if (h_summary != nullptr) cudaFreeHost(h_summary);
@@ -975,31 +977,24 @@ struct batch_runner {
       admit(e, adm, st);
       e.admit_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     };
-    admit_free();
-    auto busy_slots = [&]() {
+    // Pipelined: right after the sync of chunk c the next chunk is
+    // launched, and the slots that finished in chunk c are exported on a
+    // second stream while it runs.  Finished slots are left alone by the
+    // super-step kernels, so the export reads stable data.  Their
+    // retirement is queued behind the chunk in flight, whose summary still
+    // shows them finished: they stay "retiring" (not admissible, state
+    // ignored) until that summary has been read.
+    constexpr int64_t kRetiring = -2;
+    std::vector<uint8_t> stale(S, 0);  // rearmed: the next summary predates it
+    std::vector<b2r_engine::summary_t> sum(S);
+    bool in_flight = false;
+    auto const running = [&]() {
       for (auto x : slot_q)
-        if (x != -1) return true;
+        if (x >= 0) return true;
       return false;
     };
-    auto busy = [&]() {
-      if (next < runs.size()) return true;  // queries still being prepared
-      for (auto x : slot_q)
-        if (x != -1) return true;
-      return false;
-    };
-    // every start-time group ends within end_k super-steps; the cap turns a
-    // logic error into a reported failure instead of an endless loop
-    uint64_t max_steps = 10000;
-    for (auto const& q : runs) max_steps += 40ull * (q.p.starts.size() + 2) * (q.p.end_k + 2);
-    while (busy()) {
-      if (steps > max_steps) throw std::runtime_error("super-step cap exceeded");
-      if (!busy_slots()) {  // every resident query finished: wait for preparation
-        auto const t0 = std::chrono::steady_clock::now();
-        std::this_thread::yield();
-        e.idle_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-        admit_free();
-        continue;
-      }
+    auto const busy = [&]() { return next < runs.size() || running(); };
+    auto const launch_chunk = [&]() {
       B2R_CUDA(cudaEventRecord(e.ev0, st));
       for (uint32_t c = 0; c != chunk; ++c) {
         if (use_graph) {
@@ -1015,28 +1010,62 @@ struct batch_runner {
       e.d2h_bytes += S * sizeof(b2r_engine::summary_t);
       B2R_CUDA(cudaMemcpyAsync(e.h_summary, e.d_summary, S * sizeof(b2r_engine::summary_t),
                                cudaMemcpyDeviceToHost, st));
+      in_flight = true;
+    };
+    // every start-time group ends within end_k super-steps; the cap turns a
+    // logic error into a reported failure instead of an endless loop
+    uint64_t max_steps = 10000;
+    for (auto const& q : runs) max_steps += 40ull * (q.p.starts.size() + 2) * (q.p.end_k + 2);
+    admit_free();
+    while (busy()) {
+      if (steps > max_steps) throw std::runtime_error("super-step cap exceeded");
+      if (!in_flight) {
+        if (!running()) {  // every resident query finished: wait for preparation
+          for (auto& x : slot_q)
+            if (x == kRetiring) x = -1;  // no summary in flight can predate it
+          auto const t0 = std::chrono::steady_clock::now();
+          std::this_thread::yield();
+          e.idle_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+          admit_free();
+          continue;
+        }
+        launch_chunk();
+      }
       B2R_CUDA(cudaStreamSynchronize(st));
+      in_flight = false;
       {
         float ms = 0;
         B2R_CUDA(cudaEventElapsedTime(&ms, e.ev0, e.ev1));
         busy_ms += ms;
       }
-      admit_free();  // queries whose preparation finished meanwhile
+      std::copy(e.h_summary, e.h_summary + S, sum.begin());
+      for (auto& x : slot_q)
+        if (x == kRetiring) x = -1;  // their retirement ran before this summary's chunk ended
       std::vector<uint32_t> done_slots, n_js, n_rows;
       for (uint32_t s = 0; s != S; ++s) {
-        if (slot_q[s] == -1) continue;
-        auto const state = e.h_summary[s].state;
+        if (slot_q[s] < 0) continue;
+        if (stale[s]) {
+          stale[s] = 0;
+          continue;
+        }
+        auto const state = sum[s].state;
         if (state == dev::S_DONE || state == dev::S_ERROR) {
           done_slots.push_back(s);
-          n_js.push_back(e.h_summary[s].n_journeys);
+          n_js.push_back(sum[s].n_journeys);
           auto const& q = runs[static_cast<size_t>(slot_q[s])];
           n_rows.push_back(q.p.one_to_all ? q.p.end_k : 0u);
         }
       }
+      admit_free();  // into free slots, queued before the next chunk
+      // next chunk in flight unless every resident query has just finished
+      if (running() && (done_slots.size() < static_cast<size_t>(std::count_if(
+                                                 slot_q.begin(), slot_q.end(), [](int64_t x) { return x >= 0; })))) {
+        launch_chunk();
+      }
       if (done_slots.empty()) continue;
       auto const t_exp = std::chrono::steady_clock::now();
       std::vector<exported> ex;
-      export_slots(e, done_slots, n_js, n_rows, ex, st);
+      export_slots(e, done_slots, n_js, n_rows, ex, e.stream2);
       std::vector<uint32_t> retired;
       auto const now_ms = std::chrono::duration<double, std::milli>(
                               std::chrono::steady_clock::now() - e.batch_t0)
@@ -1048,14 +1077,15 @@ struct batch_runner {
         q.res.view.latency_ms = now_ms;
         if (q.rearm) {
           rearm(e, s, q, st);
+          stale[s] = in_flight ? 1 : 0;
         } else {
           retired.push_back(s);
-          slot_q[s] = -1;
+          slot_q[s] = in_flight ? kRetiring : -1;
         }
       }
       retire(e, retired, st);
       e.export_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_exp).count();
-      admit_free();
+      if (!in_flight) admit_free();
     }
     B2R_CUDA(cudaStreamSynchronize(st));
   }
@@ -1592,6 +1622,7 @@ int b2r_engine_create(b2r_timetable* tt, const b2r_engine_config* cfg_in, b2r_en
       B2R_CUDA(cudaMallocHost(&e->h_summary, S * sizeof(b2r_engine::summary_t)));
       B2R_CUDA(cudaMallocHost(&e->h_lbcount, sizeof(uint32_t)));
       B2R_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+      B2R_CUDA(cudaStreamCreateWithFlags(&e->stream2, cudaStreamNonBlocking));
       B2R_CUDA(cudaEventCreate(&e->ev0));
       B2R_CUDA(cudaEventCreate(&e->ev1));
       if (e->cfg.use_graphs) {
