@@ -61,6 +61,14 @@ const char* b2r_last_error(void);
 #define B2R_INVALID_IDX 0xFFFFFFFFu
 #define B2R_UNREACHABLE 0xFFFFu
 
+/* Route flags (types.h:417-423 route_flag) and the all-classes mask
+ * (routing/clasz_mask.h:13-25: bit c = transport class c allowed). */
+#define B2R_FLAG_BIKES 0u
+#define B2R_FLAG_CARS 1u
+#define B2R_FLAG_WHEELCHAIR 2u
+#define B2R_FLAG_RESERVATION_NOT_REQUIRED 3u
+#define B2R_ALL_CLASZ 0xFFFFFFFFu
+
 /* Location types used by location_match_mode::kIntermodal
  * (for_each_meta.h:29-35 reads kGeneratedTrack children). */
 #define B2R_LOC_STATION 0u
@@ -129,6 +137,15 @@ typedef struct b2r_timetable_desc {
   const uint32_t* lb_fwd;
   const uint32_t* lb_bwd_index;
   const uint32_t* lb_bwd;
+
+  /* route filters (timetable.h:348-361): class per route, and per route flag
+   * f (B2R_FLAG_*) bit 2f = set on all sections, bit 2f+1 = set on some
+   * (route_flags_), plus per section s of route r the flag bits at
+   * route_section_flags[route_stop_index[r] + s] (route_flags_per_section_).
+   * NULL: class 0, no flags. */
+  const uint8_t* route_clasz;
+  const uint8_t* route_flags;
+  const uint8_t* route_section_flags;
 } b2r_timetable_desc;
 
 /* ------------------------------------------------------------- queries */
@@ -183,6 +200,13 @@ typedef struct b2r_query {
   int16_t tts_min_transfer_time;
   int16_t tts_additional_time;
   float tts_factor;
+  /* filters (query.h:91-94): allowed transport classes, and routes / sections
+   * that must carry bikes, carry cars, need no reservation */
+  uint32_t allowed_claszes; /* default B2R_ALL_CLASZ */
+  uint8_t require_bike_transport;
+  uint8_t require_car_transport;
+  uint8_t no_compulsory_reservation;
+  uint8_t pad2_;
 } b2r_query;
 
 /* Fill a query with nigiri's defaults (query.h:84-99). */
@@ -455,6 +479,8 @@ typedef struct b2r_tt_base {
   const uint32_t* transport_bitfield; /* [n_transports] */
   uint32_t n_bitfields;
   const uint64_t* bitfields;
+  const uint8_t* route_flags;         /* [n_routes] or NULL (no flags) */
+  const uint8_t* route_section_flags; /* [route_stop_index[n_routes]] or NULL */
 } b2r_tt_base;
 int b2r_tt_build(const b2r_tt_base* base, b2r_host_timetable** out);
 int b2r_tt_save(const b2r_host_timetable* t, const char* path);

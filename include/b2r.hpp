@@ -12,8 +12,8 @@
  *  - routing::one_to_all        include/nigiri/routing/one_to_all.h:22-25
  *  - routing::raptor_state      round_times_ of raptor_state.h:22-111
  * restricted to what the engine runs: the static timetable (no real-time
- * overlay), no vias, no time-dependent offsets, no clasz / bike / car /
- * wheelchair filters, profile 0.  Times are minutes since the epoch
+ * overlay), no vias, no time-dependent offsets, no wheelchair profile
+ * (profile 0); class, bike, car and reservation filters included.  Times are minutes since the epoch
  * (unixtime_t), durations minutes.
  *
  * Errors: every call that fails throws b2r::error with the C ABI's status
@@ -92,6 +92,10 @@ struct query {
   std::optional<duration_t> fastest_direct_{};
   double fastest_direct_factor_{1.0};
   transfer_time_settings transfer_time_settings_{};
+  uint16_t allowed_claszes_{0xFFFFU};  // clasz_mask_t: bit c = class c allowed
+  bool require_bike_transport_{false};
+  bool require_car_transport_{false};
+  bool no_compulsory_reservation_{false};
 };
 
 struct run_enter_exit {  // journey::run_enter_exit (transport, day, stops)
@@ -219,6 +223,10 @@ struct c_query {
     c.tts_min_transfer_time = s.min_transfer_time_;
     c.tts_additional_time = s.additional_time_;
     c.tts_factor = s.factor_;
+    c.allowed_claszes = q.allowed_claszes_;
+    c.require_bike_transport = q.require_bike_transport_ ? 1 : 0;
+    c.require_car_transport = q.require_car_transport_ ? 1 : 0;
+    c.no_compulsory_reservation = q.no_compulsory_reservation_ ? 1 : 0;
   }
   static std::vector<b2r_offset> to_c(std::vector<offset> const& v) {
     std::vector<b2r_offset> out;

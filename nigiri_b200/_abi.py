@@ -25,6 +25,8 @@ B2R_NOALLOC_SCRATCH_BYTES = 8388608 + 256
 B2R_FORWARD, B2R_BACKWARD = 0, 1
 B2R_MATCH_EXACT, B2R_MATCH_ONLY_CHILDREN, B2R_MATCH_EQUIVALENT, B2R_MATCH_INTERMODAL = 0, 1, 2, 3
 B2R_ONE_TO_ONE, B2R_ONE_TO_ALL = 0, 1
+B2R_FLAG_BIKES, B2R_FLAG_CARS, B2R_FLAG_WHEELCHAIR, B2R_FLAG_RESERVATION_NOT_REQUIRED = 0, 1, 2, 3
+B2R_ALL_CLASZ = 0xFFFFFFFF
 B2R_LEG_TRANSPORT, B2R_LEG_FOOTPATH, B2R_LEG_OFFSET = 0, 1, 2
 
 _u8p, _u16p, _u32p, _u64p = (C.POINTER(C.c_uint8), C.POINTER(C.c_uint16),
@@ -50,6 +52,7 @@ class TimetableDesc(C.Structure):
         ("location_routes_index", _u32p), ("location_routes", _u32p),
         ("lb_fwd_index", _u32p), ("lb_fwd", _u32p),
         ("lb_bwd_index", _u32p), ("lb_bwd", _u32p),
+        ("route_clasz", _u8p), ("route_flags", _u8p), ("route_section_flags", _u8p),
     ]
 
 
@@ -74,6 +77,9 @@ class Query(C.Structure):
         ("tts_default", C.c_uint8), ("pad_", C.c_uint8 * 3),
         ("tts_min_transfer_time", C.c_int16), ("tts_additional_time", C.c_int16),
         ("tts_factor", C.c_float),
+        ("allowed_claszes", C.c_uint32), ("require_bike_transport", C.c_uint8),
+        ("require_car_transport", C.c_uint8), ("no_compulsory_reservation", C.c_uint8),
+        ("pad2_", C.c_uint8),
     ]
 
 
@@ -151,6 +157,7 @@ class TtBase(C.Structure):
         ("route_clasz", _u8p), ("route_n_transports", _u32p),
         ("route_stop_times", _u16p), ("transport_bitfield", _u32p),
         ("n_bitfields", C.c_uint32), ("bitfields", _u64p),
+        ("route_flags", _u8p), ("route_section_flags", _u8p),
     ]
 
 

@@ -483,6 +483,8 @@ slot_t make_slot(b2r_engine& e, uint32_t s, prepped_query const& p, bool& clear_
   sl.need_sweep = 0;
   sl.early_term = 0;
   sl.tts = {p.tts.is_default, p.tts.min_transfer_time, p.tts.additional_time, p.tts.factor};
+  sl.allowed_claszes = p.allowed_claszes;
+  sl.req_flags = p.req_flags;
   sl.n_starts = static_cast<uint32_t>(p.starts.size());
   sl.n_dest = static_cast<uint32_t>(p.intermodal_dest ? p.dest_dist.size() : p.dest_locs.size());
   sl.n_soff = static_cast<uint32_t>(p.start_offsets.size());
@@ -1409,6 +1411,27 @@ int b2r_timetable_upload(const b2r_timetable_desc* d, int device, b2r_timetable*
       v.lb_bwd_index = t->lb_bwd_index.data();
       v.lb_bwd = t->lb_bwd.data();
       v.importance = nullptr;
+      v.route_clasz = nullptr;  // the host preparation does not filter routes
+      v.route_flags = nullptr;
+      v.route_section_flags = nullptr;
+
+      // route filter words: class | all-sections flags << 4 | some << 8
+      std::vector<uint16_t> rfilter(nr, 10U);  // no classes given: bus
+      for (auto r = 0U; r != nr; ++r) {
+        auto const c = d->route_clasz != nullptr ? d->route_clasz[r] : 10U;
+        if (c >= 16U) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "route_clasz out of range (0..15)");
+        auto const fl = d->route_flags != nullptr ? d->route_flags[r] : 0U;
+        uint32_t all = 0U, some = 0U;
+        for (auto f = 0U; f != 4U; ++f) {
+          all |= ((fl >> (2U * f)) & 1U) << f;
+          some |= ((fl >> (2U * f + 1U)) & 1U) << f;
+        }
+        rfilter[r] = static_cast<uint16_t>(c | (all << 4) | (some << 8));
+      }
+      std::vector<uint8_t> rsec(d->route_stop_index[nr], 0U);
+      if (d->route_section_flags != nullptr) {
+        std::copy(d->route_section_flags, d->route_section_flags + rsec.size(), rsec.begin());
+      }
 
       // column order check: get_earliest_transport's binary search needs
       // every event column ordered by minutes after midnight
@@ -1458,6 +1481,8 @@ int b2r_timetable_upload(const b2r_timetable_desc* d, int device, b2r_timetable*
       dd.loc_routes_idx = up(d->location_routes_index, nl + 1);
       dd.loc_routes = up(d->location_routes, d->location_routes_index[nl]);
       dd.route_sorted = up(sorted.data(), nr);
+      dd.route_filter = up(rfilter.data(), nr);
+      dd.route_sec = up(rsec.data(), rsec.size());
       dd.lbg_fwd_idx = up(d->lb_fwd_index, nl + 1);
       dd.lbg_fwd = up(d->lb_fwd, d->lb_fwd_index[nl]);
       dd.lbg_bwd_idx = up(d->lb_bwd_index, nl + 1);

@@ -76,6 +76,12 @@ struct dtt {
   uint32_t const* lrs_idx;
   uint32_t const* lrs_route;
   uint16_t const* lrs_stop;
+  // route filters: per route, bits 0-3 transport class, 4-7 the flags set on
+  // all sections, 8-11 the flags set on some sections (route_clasz_ and
+  // route_flags_, timetable.h:348-355); per route stop index s of route r
+  // the flags of the section s -> s + 1 (route_flags_per_section_)
+  uint16_t const* route_filter;
+  uint8_t const* route_sec;
 };
 
 // --------------------------------------------------------- per-slot data
@@ -116,6 +122,9 @@ struct slot_t {
   int16_t max_travel_time;
   uint32_t min_connection_count;
   uint8_t extend_earlier, extend_later, need_sweep, early_term;
+  uint16_t allowed_claszes;  // bit c: transport class c allowed
+  uint8_t req_flags;         // bit f: route flag f required
+  uint8_t pad_f;
   tts_t tts;
   uint32_t starts_off, n_starts;  // start pool
   uint32_t dest_off, n_dest;      // dest pool (loc, dist)
@@ -133,8 +142,9 @@ struct slot_t {
   uint64_t n_rounds, n_groups_run;
 };
 
-// compact per-super-step view of a slot read by every lane
-struct lane_t {
+// compact per-super-step view of a slot read by every lane (one 16-byte
+// load)
+struct __align__(16) lane_t {
   int16_t tad_k;
   uint16_t gtag;
   uint16_t qtag;
@@ -143,6 +153,9 @@ struct lane_t {
   uint8_t k;
   uint8_t run;
   uint8_t mode;  // bit0 intermodal dest, bit1 has dests, bit2 tts default
+  uint16_t claszes;  // allowed transport classes
+  uint8_t req;       // required route flags
+  uint8_t pad;
 };
 
 struct start_rec {
@@ -232,6 +245,25 @@ __device__ __forceinline__ int key_add(int key, int x) { return clamp16(key + x)
 
 __device__ __forceinline__ bool bf_test(dtt const& T, uint32_t bf, uint32_t i) {
   return i < B2R_MAX_DAYS && ((T.bf[8ull * bf + (i >> 6)] >> (i & 63u)) & 1ull);
+}
+
+// The route filters of loop_routes (raptor.h:499-545) and of get_transport
+// (reconstruct.cc:456-498): false if route r's class is not allowed or a
+// required flag is on none of its sections; `sec` receives the required
+// flags that are on some but not all sections, which the walk along the
+// route checks section by section (raptor.h:1194-1217).
+__device__ __forceinline__ bool route_allowed(dtt const& T, uint32_t r, uint32_t claszes, uint32_t req,
+                                              uint32_t& sec) {
+  auto const f = static_cast<uint32_t>(T.route_filter[r]);
+  auto const need = req & ~(f >> 4);  // required, not on all sections
+  sec = need;
+  return ((claszes >> (f & 15u)) & 1u) != 0u && (need & ~(f >> 8) & 15u) == 0u;
+}
+
+// whether section s of route r (from its stop s to s + 1) carries every
+// flag of `sec`
+__device__ __forceinline__ bool section_ok(dtt const& T, uint32_t r_stop_base, uint32_t s, uint32_t sec) {
+  return (static_cast<uint32_t>(T.route_sec[r_stop_base + s]) & sec) == sec;
 }
 
 __device__ __forceinline__ int delta_count(uint16_t d) {  // delta::count()

@@ -298,9 +298,34 @@ host_timetable generate(uint32_t config, uint64_t seed) {
     auto const mam = static_cast<uint16_t>(minutes % 1440);
     return static_cast<uint16_t>((days & 0x1Fu) | (mam << 5));
   };
+  // route classes and flags come from a stream of their own, so that the
+  // network and its trips are the same with or without them.  Classes: bus
+  // mostly, then tram, subway, suburban, regional.  Flags per section
+  // (bikes, cars, wheelchair, no reservation): a route carries a flag on
+  // all, some or none of its sections.
+  rng frnd{seed * 0xD1B54A32D192ED03ull + config + 1U};
+  struct flag_mix {
+    double all, some;
+  };
+  static constexpr flag_mix kFlagMix[4] = {
+      {0.55, 0.20}, {0.05, 0.05}, {0.50, 0.20}, {0.80, 0.10}};
   t.route_stop_index.assign(1, 0U);
   for (auto const& seq : base_seq) {
     auto const n = static_cast<uint32_t>(seq.size());
+    uint8_t clasz = 10U;
+    {
+      auto const u = frnd.unit();
+      clasz = u < 0.60 ? 10U : u < 0.75 ? 9U : u < 0.85 ? 8U : u < 0.95 ? 7U : 6U;
+    }
+    std::vector<uint8_t> sections(n, 0U);  // section s: stop s -> s + 1
+    for (auto f = 0U; f != 4U; ++f) {
+      auto const u = frnd.unit();
+      auto const some = u >= kFlagMix[f].all && u < kFlagMix[f].all + kFlagMix[f].some;
+      for (auto s = 0U; s + 1U < n; ++s) {
+        auto const on = u < kFlagMix[f].all || (some && frnd.unit() < 0.6);
+        if (on) sections[s] = static_cast<uint8_t>(sections[s] | (1U << f));
+      }
+    }
     std::vector<int> hop(n, 0), dwell(n, 0);
     for (auto s = 1U; s < n; ++s) hop[s] = static_cast<int>(rnd.uni(1, 4));
     for (auto s = 1U; s + 1U < n; ++s) dwell[s] = static_cast<int>(rnd.uni(0, 1));
@@ -345,7 +370,9 @@ host_timetable generate(uint32_t config, uint64_t seed) {
       for (auto j = 0U; j != sub.size(); ++j) t.transport_traffic_days.push_back(bf);
       t.route_transport_to.push_back(static_cast<uint32_t>(t.transport_traffic_days.size()));
       t.route_stop_time_from.push_back(static_cast<uint32_t>(t.route_stop_times.size()));
-      t.route_clasz.push_back(10U);
+      t.route_clasz.push_back(clasz);
+      t.route_section_flags.insert(t.route_section_flags.end(), sections.begin(),
+                                   sections.end());
       for (auto slot = 0U; slot != 2 * (n - 1); ++slot) {
         for (auto const* tr : sub) t.route_stop_times.push_back(enc(tr->times[slot]));
       }

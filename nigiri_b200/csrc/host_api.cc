@@ -38,6 +38,7 @@ void b2r_query_init(b2r_query* q) {
   q->fastest_direct_factor = 1.0;
   q->tts_default = 1;
   q->tts_factor = 1.0F;
+  q->allowed_claszes = B2R_ALL_CLASZ;
 }
 
 void b2r_engine_config_init(b2r_engine_config* c) {
@@ -86,7 +87,20 @@ int b2r_tt_build(const b2r_tt_base* b, b2r_host_timetable** out) {
     t.route_stop_index.assign(b->route_stop_index, b->route_stop_index + b->n_routes + 1);
     t.route_stops.assign(b->route_stops, b->route_stops + b->route_stop_index[b->n_routes]);
     if (b->route_clasz != nullptr) {
+      for (auto r = 0U; r != b->n_routes; ++r) {
+        if (b->route_clasz[r] >= 16U) {  // clasz::kNumClasses (types.h:394-412)
+          delete h;
+          return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "b2r_tt_build: route_clasz out of range (0..15)");
+        }
+      }
       t.route_clasz.assign(b->route_clasz, b->route_clasz + b->n_routes);
+    }
+    if (b->route_flags != nullptr) {
+      t.route_flags.assign(b->route_flags, b->route_flags + b->n_routes);
+    }
+    if (b->route_section_flags != nullptr) {
+      t.route_section_flags.assign(b->route_section_flags,
+                                   b->route_section_flags + b->route_stop_index[b->n_routes]);
     }
     t.route_transport_from.resize(b->n_routes);
     t.route_transport_to.resize(b->n_routes);

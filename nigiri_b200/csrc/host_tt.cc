@@ -174,6 +174,10 @@ b2r_timetable_desc host_timetable::desc() const {
   d.lb_fwd = lb_fwd.data();
   d.lb_bwd_index = lb_bwd_index.data();
   d.lb_bwd = lb_bwd.data();
+  d.route_clasz = route_clasz.empty() ? nullptr : route_clasz.data();
+  d.route_flags = route_flags.empty() ? nullptr : route_flags.data();
+  d.route_section_flags =
+      route_section_flags.empty() ? nullptr : route_section_flags.data();
   return d;
 }
 
@@ -286,16 +290,47 @@ void finalize(host_timetable& t) {
   build_lb_graph(t, true, t.lb_fwd_index, t.lb_fwd);
   build_lb_graph(t, false, t.lb_bwd_index, t.lb_bwd);
 
+  // route flags: absent means no route carries any flag.  From per-section
+  // flags, a route's flag f is "on all sections" when every section of the
+  // route has it and "on some" when at least one has it
+  // (timetable::register_route, timetable.cc:136-156).
+  if (!t.route_section_flags.empty() && t.route_flags.empty()) {
+    t.route_flags.assign(t.n_routes, 0U);
+    for (auto r = 0U; r != t.n_routes; ++r) {
+      auto const b = t.route_stop_index[r], n_sections = t.route_stop_index[r + 1] - b - 1U;
+      for (auto f = 0U; f != 4U; ++f) {
+        auto count = 0U;
+        for (auto s = 0U; s != n_sections; ++s) count += (t.route_section_flags[b + s] >> f) & 1U;
+        if (count == n_sections && n_sections != 0U) t.route_flags[r] |= static_cast<uint8_t>(1U << (2U * f));
+        if (count != 0U) t.route_flags[r] |= static_cast<uint8_t>(1U << (2U * f + 1U));
+      }
+    }
+  }
+  if (!t.route_flags.empty() && t.route_section_flags.empty()) {
+    // whole-route flags only: every section carries the "all sections" bits
+    t.route_section_flags.assign(t.route_stop_index[t.n_routes], 0U);
+    for (auto r = 0U; r != t.n_routes; ++r) {
+      uint8_t all = 0U;
+      for (auto f = 0U; f != 4U; ++f) {
+        if (t.route_flags[r] & (1U << (2U * f))) all |= static_cast<uint8_t>(1U << f);
+      }
+      for (auto i = t.route_stop_index[r]; i != t.route_stop_index[r + 1]; ++i) {
+        t.route_section_flags[i] = all;
+      }
+    }
+  }
+
   // importance, loader/init_finish.cc:64-102 (float accumulation into a
-  // uint32, class priorities of the reference table)
+  // uint32; class priorities of the reference table, zero past kOther's
+  // slot 12 as its 16-entry array leaves them)
   {
-    static constexpr float kPrio[13] = {20, 20, 20, 20, 20, 16, 15,
-                                        10, 10, 3,  2,  10, 1};
+    static constexpr float kPrio[16] = {20, 20, 20, 20, 20, 16, 15, 10,
+                                        10, 3,  2,  10, 1,  0,  0,  0};
     if (t.route_clasz.empty()) t.route_clasz.assign(t.n_routes, 10U);  // bus
     t.importance.assign(t.n_locations, 0U);
     t.max_importance = 0U;
     for (auto l = 0U; l != t.n_locations; ++l) {
-      unsigned counts[13] = {};
+      unsigned counts[16] = {};
       for (auto ri = t.location_routes_index[l];
            ri != t.location_routes_index[l + 1]; ++ri) {
         auto const r = t.location_routes[ri];
@@ -309,7 +344,7 @@ void finalize(host_timetable& t) {
       }
       auto const p = t.parent[l];
       auto& x = t.importance[p == kInvalid ? l : p];
-      for (auto c = 0; c != 13; ++c) {
+      for (auto c = 0; c != 16; ++c) {
         x += kPrio[c] * static_cast<float>(counts[c]);
       }
       t.max_importance = std::max(t.max_importance, x);
@@ -319,7 +354,7 @@ void finalize(host_timetable& t) {
 
 // ------------------------------------------------------------ persistence
 namespace {
-constexpr uint64_t kMagic = 0x3132424d49544232ull;  // "2BTIMB21"
+constexpr uint64_t kMagic = 0x3232424d49544232ull;  // "2BTIMB22"
 
 template <typename T>
 void put_vec(std::FILE* f, std::vector<T> const& v) {
@@ -343,7 +378,8 @@ bool get_vec(std::FILE* f, std::vector<T>& v) {
   X(route_transport_to) X(route_stop_time_from) X(route_stop_times)            \
   X(route_traffic_days) X(transport_traffic_days) X(transport_route)           \
   X(bitfields) X(location_routes_index) X(location_routes) X(lb_fwd_index)     \
-  X(lb_fwd) X(lb_bwd_index) X(lb_bwd) X(x) X(y)
+  X(lb_fwd) X(lb_bwd_index) X(lb_bwd) X(x) X(y) X(route_flags)                \
+  X(route_section_flags)
 
 bool save(host_timetable const& t, std::string const& path) {
   auto* f = std::fopen(path.c_str(), "wb");

@@ -29,6 +29,9 @@ struct host_timetable {
 
   std::vector<uint32_t> route_stop_index, route_stops;
   std::vector<uint8_t> route_clasz;
+  // per route: bit 2f = flag f on all sections, 2f+1 = on some sections;
+  // per route stop index (section s -> s+1): the flag bits of that section
+  std::vector<uint8_t> route_flags, route_section_flags;
   std::vector<uint32_t> route_transport_from, route_transport_to;
   std::vector<uint32_t> route_stop_time_from;
   std::vector<uint16_t> route_stop_times;

@@ -118,6 +118,8 @@ __global__ void k_ctl_begin(state st) {
               ((!sl.intermodal_dest && !sl.one_to_all && sl.n_dest != 0) ? 2u : 0u) |
               (sl.tts.is_default ? 4u : 0u);
     ln.tad_k = sl.tad[sl.k];
+    ln.claszes = sl.allowed_claszes;
+    ln.req = sl.req_flags;
     atomicOr(&st.run_mask[s >> 5], 1u << (s & 31));
     if (sl.need_sweep) atomicOr(&st.sweep_mask[s >> 5], 1u << (s & 31));
     ++sl.n_rounds;
@@ -214,7 +216,7 @@ __global__ void k_ctl_marked(state st) {
 }
 
 // ------------------------------------------------------------ route scan
-// update_route, raptor.h:1177-1349 (no vias, no section filters) for every
+// update_route, raptor.h:1177-1349 (no vias) for every
 // (route, query) pair marked this round.  A warp takes 32 marked (route,
 // group of 32 queries) entries, lists their (route, query) pairs and gives
 // one pair to each lane per pass: resident queries are unrelated, so an
@@ -263,6 +265,8 @@ __global__ void __launch_bounds__(256, 3) k_route_scan(state st) {
       auto const s = g * 32u + b;
       auto const ln = st.lanes[s];
       if (!ln.run) continue;
+      uint32_t sec = 0u;  // required flags checked per section
+      if ((ln.claszes != 0xFFFFu || ln.req != 0u) && !route_allowed(T, r, ln.claszes, ln.req, sec)) continue;
       auto const bit = 1u << b;
       auto const fwd = ln.fwd != 0;
       auto const k = static_cast<uint32_t>(ln.k);
@@ -295,6 +299,9 @@ __global__ void __launch_bounds__(256, 3) k_route_scan(state st) {
         auto const l = B2R_STOP_LOC(stp);
         auto const can_finish = fwd ? B2R_STOP_OUT(stp) : B2R_STOP_IN(stp);
         auto const can_start = fwd ? B2R_STOP_IN(stp) : B2R_STOP_OUT(stp);
+        if (sec != 0u && i != 0u && !section_ok(T, sb, fwd ? i - 1u : si, sec)) {
+          et_valid = false;  // raptor.h:1194-1217: the section ridden lacks a flag
+        }
         bool arrival_ran = false;
         if (et_valid && can_finish) {
           arrival_ran = true;

@@ -69,6 +69,8 @@ struct params {
   uint8_t end_k;
   uint32_t n_off;
   dev::tts_t tts;
+  uint16_t claszes;  // allowed transport classes
+  uint8_t req;       // required route flags
   b2r_offset off[B2R_NOALLOC_MAX_OFFSETS];
 };
 
@@ -228,6 +230,8 @@ __global__ void __cluster_dims__(kCtas, 1, 1) __launch_bounds__(kThreads, 1)
     for (auto w = tid; w < n_marked; w += kAll) {
       auto const r = ldu(&rlist[w]);
       R[r] = 0u;
+      uint32_t sec = 0u;  // required flags checked per section
+      if ((P.claszes != 0xFFFFu || P.req != 0u) && !dev::route_allowed(T, r, P.claszes, P.req, sec)) continue;
       auto const sb = T.route_stop_idx[r];
       auto const n = T.route_stop_idx[r + 1] - sb;
       auto const n_t = T.route_tr_to[r] - T.route_tr_from[r];
@@ -241,6 +245,9 @@ __global__ void __cluster_dims__(kCtas, 1, 1) __launch_bounds__(kThreads, 1)
         auto const l = B2R_STOP_LOC(stp);
         auto const can_finish = fwd ? B2R_STOP_OUT(stp) : B2R_STOP_IN(stp);
         auto const can_start = fwd ? B2R_STOP_IN(stp) : B2R_STOP_OUT(stp);
+        if (sec != 0u && i != 0u && !dev::section_ok(T, sb, fwd ? i - 1u : si, sec)) {
+          et_valid = false;  // raptor.h:1194-1217
+        }
         bool arrival_ran = false;
         if (et_valid && can_finish) {
           arrival_ran = true;
@@ -419,6 +426,10 @@ int run(b2r_timetable const* tt, b2r_query const* q, int16_t* round_times, uint6
   P.base = static_cast<uint16_t>(round_to_days(q->start_time) - tt->d.internal_from_days);
   P.base_days = tt->d.internal_from_days + P.base;
   P.tts = {q->tts_default, q->tts_min_transfer_time, q->tts_additional_time, q->tts_factor};
+  P.claszes = static_cast<uint16_t>(q->allowed_claszes & 0xFFFFu);
+  P.req = static_cast<uint8_t>((q->require_bike_transport != 0 ? 1u << B2R_FLAG_BIKES : 0u) |
+                               (q->require_car_transport != 0 ? 1u << B2R_FLAG_CARS : 0u) |
+                               (q->no_compulsory_reservation != 0 ? 1u << B2R_FLAG_RESERVATION_NOT_REQUIRED : 0u));
   auto const span = static_cast<int>(q->max_travel_time);
   auto const worst = std::clamp(q->start_time + (fwd ? span : -span) - P.base_days * 1440, -32768, 32767);
   P.tad = std::min(dev::kKeyInv, fwd ? worst : ~worst);

@@ -379,6 +379,11 @@ void prepare(host_view const& hv, b2r_query const& q, int lb_mode, prepped_query
   p.min_connection_count = q.min_connection_count;
   p.extend_earlier = q.extend_interval_earlier != 0;
   p.extend_later = q.extend_interval_later != 0;
+  p.allowed_claszes = static_cast<uint16_t>(q.allowed_claszes & 0xFFFFU);  // 16 classes
+  p.req_flags = static_cast<uint8_t>(
+      (q.require_bike_transport != 0 ? 1U << B2R_FLAG_BIKES : 0U) |
+      (q.require_car_transport != 0 ? 1U << B2R_FLAG_CARS : 0U) |
+      (q.no_compulsory_reservation != 0 ? 1U << B2R_FLAG_RESERVATION_NOT_REQUIRED : 0U));
   p.start_offsets.assign(q.start, q.start + q.n_start);
   p.dest_offsets.assign(q.destination, q.destination + q.n_destination);
   p.tts_raw = {q.tts_default, q.tts_min_transfer_time, q.tts_additional_time, q.tts_factor};

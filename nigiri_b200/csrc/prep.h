@@ -45,6 +45,8 @@ struct prepped_query {
   int32_t iv_from{0}, iv_to{0};  // search interval
   uint32_t min_connection_count{0};
   bool extend_earlier{false}, extend_later{false};
+  uint16_t allowed_claszes{0xFFFFU};  // bit c: transport class c allowed
+  uint8_t req_flags{0U};              // bit f: route flag f required
   int32_t data_max_from{0}, data_max_to{0};  // interval_estimator clamp
   tts_norm tts;
   tts_norm tts_raw;  // as given (fastest-direct uses it)

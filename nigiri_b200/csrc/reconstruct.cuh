@@ -152,22 +152,26 @@ struct recon_ctx {
 
   // reconstruct.cc:180-280 (single pass: no vias).  The stops before the
   // exit stop are split across the lanes; the ballot keeps the first one in
-  // the reference's order.  Called by the whole warp with equal arguments.
+  // the reference's order.  A section lacking one of the flags `sec` ends
+  // the ride (reconstruct.cc:239-250): stops at or past the first such
+  // section do not count.  Called by the whole warp with equal arguments.
   __device__ bool find_start_in_prev_round(unsigned k, uint32_t t, uint16_t day, uint32_t finish,
-                                           b2r_leg& out) const {
+                                           uint32_t sec, b2r_leg& out) const {
     auto const r = T->transport_route[t];
     auto const size = n_stops(r);
     auto const n = fwd ? finish + 1u : size - finish;
     for (auto i0 = 1u; i0 < n; i0 += 32u) {
       auto const i = i0 + lane;
-      bool ok = false;
+      bool ok = false, cut = false;
       uint32_t si = 0, l = 0;
       int event_time = 0;
       if (i < n) {
         si = fwd ? finish - i : finish + i;
         auto const w = stopw(r, si);
         l = B2R_STOP_LOC(w);
-        if (!((fwd && !B2R_STOP_IN(w)) || (!fwd && !B2R_STOP_OUT(w)))) {
+        // departure section forward, arrival section backward
+        cut = sec != 0u && !section_ok(*T, T->route_stop_idx[r], fwd ? si : si - 1u, sec);
+        if (!cut && !((fwd && !B2R_STOP_IN(w)) || (!fwd && !B2R_STOP_OUT(w)))) {
           event_time = unix_to_delta(ev_time(t, day, si, !fwd));
           auto const round_time = rt_t(k - 1, l);
           ok = beq(round_time, event_time) ||
@@ -175,7 +179,9 @@ struct recon_ctx {
                 (ontrip ? beq(round_time, event_time) : round_time == event_time));
         }
       }
-      auto const m = __ballot_sync(kFull, ok);
+      auto m = __ballot_sync(kFull, ok);
+      auto const cuts = __ballot_sync(kFull, cut);
+      if (cuts != 0u) m &= (1u << (__ffs(cuts) - 1)) - 1u;  // lanes before the first cut
       if (m != 0u) {
         auto const src = __ffs(m) - 1;
         si = __shfl_sync(kFull, si, src);
@@ -186,6 +192,7 @@ struct recon_ctx {
         set_run(out, t, day, si, finish);
         return true;
       }
+      if (cuts != 0u) return false;
     }
     return false;
   }
@@ -271,7 +278,7 @@ struct recon_ctx {
         auto const o_end = __shfl_sync(kFull, end, static_cast<int>(owner));
         auto const o_cnt = __shfl_sync(kFull, cnt, static_cast<int>(owner));
         bool has = false;
-        uint32_t r = 0, i = 0, cursor = 0, t = 0;
+        uint32_t r = 0, i = 0, cursor = 0, t = 0, sec = 0;
         uint16_t tday = 0;
         if (p < total) {
           auto const x = o_pb + (p - (o_end - o_cnt));
@@ -279,7 +286,10 @@ struct recon_ctx {
           i = static_cast<uint32_t>(T->lrs_stop[x]);
           auto const w = stopw(r, i);
           auto const n = n_stops(r);
-          if (!((fwd && (i == 0u || !B2R_STOP_OUT(w))) || (!fwd && (i + 1u == n || !B2R_STOP_IN(w))))) {
+          auto const allowed = (sl->allowed_claszes == 0xFFFFu && sl->req_flags == 0u) ||
+                               route_allowed(*T, r, sl->allowed_claszes, sl->req_flags, sec);
+          if (allowed &&
+              !((fwd && (i == 0u || !B2R_STOP_OUT(w))) || (!fwd && (i + 1u == n || !B2R_STOP_IN(w))))) {
             cursor = first_cursor(o_tm, r, i);
             has = next_transport(o_tm, r, i, cursor, t, tday);
           }
@@ -289,7 +299,8 @@ struct recon_ctx {
           auto const bt = __shfl_sync(kFull, t, src);
           auto const bday = static_cast<uint16_t>(__shfl_sync(kFull, static_cast<uint32_t>(tday), src));
           auto const bi = __shfl_sync(kFull, i, src);
-          if (find_start_in_prev_round(k, bt, bday, bi, out)) {
+          auto const bsec = __shfl_sync(kFull, sec, src);
+          if (find_start_in_prev_round(k, bt, bday, bi, bsec, out)) {
             return static_cast<int>(f0 + __shfl_sync(kFull, owner, src));
           }
           if (static_cast<int>(lane) == src) has = next_transport(o_tm, r, i, cursor, t, tday);

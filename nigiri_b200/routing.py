@@ -68,6 +68,10 @@ class Query:  # routing::query (static subset)
         default_factory=TransferTimeSettings)
     fastest_direct: Optional[int] = None
     fastest_direct_factor: float = 1.0
+    allowed_claszes: int = 0xFFFF  # bit c: transport class c (clasz_mask_t)
+    require_bike_transport: bool = False
+    require_car_transport: bool = False
+    no_compulsory_reservation: bool = False
 
 
 @dataclasses.dataclass
@@ -157,6 +161,10 @@ class _QueryBuffer:
             x.tts_min_transfer_time = tts.min_transfer_time
             x.tts_additional_time = tts.additional_time
             x.tts_factor = tts.factor
+            x.allowed_claszes = q.allowed_claszes
+            x.require_bike_transport = int(q.require_bike_transport)
+            x.require_car_transport = int(q.require_car_transport)
+            x.no_compulsory_reservation = int(q.no_compulsory_reservation)
             if q.fastest_direct is not None:
                 x.has_fastest_direct = 1
                 x.fastest_direct = q.fastest_direct

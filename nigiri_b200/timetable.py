@@ -84,7 +84,11 @@ class QuerySet:
                   dest_match_mode=modes[x.dest_match_mode],
                   max_transfers=x.max_transfers,
                   max_travel_time=x.max_travel_time,
-                  transfer_time_settings=TransferTimeSettings())
+                  transfer_time_settings=TransferTimeSettings(),
+                  allowed_claszes=x.allowed_claszes & 0xFFFF,
+                  require_bike_transport=bool(x.require_bike_transport),
+                  require_car_transport=bool(x.require_car_transport),
+                  no_compulsory_reservation=bool(x.no_compulsory_reservation))
         return q, (FORWARD if x.direction == A.B2R_FORWARD else BACKWARD), x.kind
 
     def close(self):

@@ -87,6 +87,19 @@ struct tt_view {
   uint32_t stop(uint32_t r, uint32_t i) const {
     return d.route_stops[d.route_stop_index[r] + i];
   }
+  // route_clasz_ / route_flags_ / route_flags_per_section_
+  // (timetable.h:348-361); absent arrays: bus, no flags
+  uint8_t clasz(uint32_t r) const {
+    return d.route_clasz == nullptr ? 10U : d.route_clasz[r];
+  }
+  uint8_t flags(uint32_t r) const {
+    return d.route_flags == nullptr ? 0U : d.route_flags[r];
+  }
+  uint8_t section_flags(uint32_t r, uint32_t section) const {
+    return d.route_section_flags == nullptr
+               ? 0U
+               : d.route_section_flags[d.route_stop_index[r] + section];
+  }
   // event_times_at_stop, timetable.h:155-164
   uint16_t const* event_times(uint32_t r, uint32_t s, bool arr) const {
     auto const idx = d.route_stop_time_from[r] + n_t(r) * (s * 2 - (arr ? 1 : 0));
@@ -214,6 +227,8 @@ struct query_t {
   bool has_fastest_direct{false};
   int16_t fastest_direct{0};
   double fastest_direct_factor{1.0};
+  uint32_t allowed_claszes{B2R_ALL_CLASZ};
+  uint8_t required_flags{0};  // bit f: route flag f required
 
   void flip_dir() {  // query.cc:52-57
     std::swap(start, dest);
@@ -259,6 +274,13 @@ query_t to_query(b2r_query const& q) {
   r.has_fastest_direct = q.has_fastest_direct != 0;
   r.fastest_direct = q.fastest_direct;
   r.fastest_direct_factor = q.fastest_direct_factor;
+  r.allowed_claszes = q.allowed_claszes;
+  r.required_flags = static_cast<uint8_t>(
+      (q.require_bike_transport != 0 ? 1U << B2R_FLAG_BIKES : 0U) |
+      (q.require_car_transport != 0 ? 1U << B2R_FLAG_CARS : 0U) |
+      (q.no_compulsory_reservation != 0
+           ? 1U << B2R_FLAG_RESERVATION_NOT_REQUIRED
+           : 0U));
   return r;
 }
 
@@ -365,6 +387,32 @@ struct bitvec {
   }
 };
 
+// The route filters of loop_routes (raptor.h:499-545) and get_transport
+// (reconstruct.cc:456-498): false if route r's class is not allowed or a
+// required flag is on none of its sections; `sections` receives the
+// required flags set on some but not all sections, which the walk along the
+// route then checks section by section.
+bool route_allowed(tt_view const& tt, uint32_t allowed_claszes, uint8_t required_flags,
+                   uint32_t r, uint8_t& sections) {
+  sections = 0U;
+  auto const c = tt.clasz(r);
+  if (c >= 32U || ((allowed_claszes >> c) & 1U) == 0U) return false;
+  auto const fl = tt.flags(r);
+  for (auto f = 0U; f != 4U; ++f) {
+    if (((required_flags >> f) & 1U) == 0U) continue;
+    if ((fl >> (2U * f)) & 1U) continue;                     // on all sections
+    if (((fl >> (2U * f + 1U)) & 1U) == 0U) return false;  // on none
+    sections = static_cast<uint8_t>(sections | (1U << f));
+  }
+  return true;
+}
+
+// whether the section from stop s to stop s + 1 of route r carries every
+// flag in `sections`
+bool section_ok(tt_view const& tt, uint32_t r, uint32_t s, uint8_t sections) {
+  return (tt.section_flags(r, s) & sections) == sections;
+}
+
 // ---------------------------------------------------------------- raptor
 // raptor<Dir, false, 0, Mode>, raptor.h:25-1535
 struct raptor_t {
@@ -382,6 +430,8 @@ struct raptor_t {
   uint16_t base_;
   tts_t tts;
   or_stats& st;
+  uint32_t allowed_claszes{B2R_ALL_CLASZ};  // query filters
+  uint8_t required_flags{0U};
 
   delta_t kInvalid() const { return fwd ? 32767 : -32768; }
   bool is_better(int a, int b) const { return fwd ? a < b : a > b; }
@@ -492,8 +542,10 @@ struct raptor_t {
       station_mark.clear();
 
       route_mark.for_each([&](uint32_t r) {
+        uint8_t sections = 0U;
+        if (!route_allowed(tt, allowed_claszes, required_flags, r, sections)) return;
         ++st.n_routes_visited;
-        any_marked |= update_route(k, r);
+        any_marked |= update_route(k, r, sections);
       });
       if (!any_marked) break;
 
@@ -604,7 +656,7 @@ struct raptor_t {
     });
   }
 
-  bool update_route(unsigned k, uint32_t r) {  // raptor.h:1177-1349
+  bool update_route(unsigned k, uint32_t r, uint8_t sections) {  // raptor.h:1177-1349
     auto const n_stops = tt.n_stops(r);
     auto any_marked = false;
     bool et_valid = false;
@@ -619,6 +671,13 @@ struct raptor_t {
       auto const is_last = i == n_stops - 1U;
       auto const can_finish = fwd ? B2R_STOP_OUT(stp) : B2R_STOP_IN(stp);
       auto const can_start = fwd ? B2R_STOP_IN(stp) : B2R_STOP_OUT(stp);
+
+      // section filters, raptor.h:1194-1217: the trip carried into this
+      // stop is dropped if the section it rode lacks a required flag
+      if (sections != 0U && i != 0U &&
+          !section_ok(tt, r, fwd ? stop_idx - 1U : stop_idx, sections)) {
+        et_valid = false;
+      }
 
       delta_t current_best = kInvalid();
       if (et_valid && can_finish) {
@@ -1023,7 +1082,7 @@ struct reconstructor {
 
   // reconstruct.cc:180-280 (Vias = 0: only the first pass runs)
   std::optional<leg_t> find_start_in_prev_round(unsigned k, uint32_t t, uint16_t day,
-                                                uint32_t finish) {
+                                                uint32_t finish, uint8_t sections) {
     auto const r = tt.d.transport_route[t];
     auto const size = tt.n_stops(r);
     auto const n_stops = fwd ? finish + 1U : size - finish;
@@ -1031,6 +1090,12 @@ struct reconstructor {
       auto const stop_idx = fwd ? finish - i : finish + i;
       auto const stp = tt.stop(r, stop_idx);
       auto const l = B2R_STOP_LOC(stp);
+      // reconstruct.cc:239-250: a section without a required flag ends the
+      // ride (departure section forward, arrival section backward)
+      if (sections != 0U &&
+          !section_ok(tt, r, fwd ? stop_idx : stop_idx - 1U, sections)) {
+        break;
+      }
       if ((fwd && !B2R_STOP_IN(stp)) || (!fwd && !B2R_STOP_OUT(stp))) continue;
       auto const event_time = unix_to_delta(base, stop_time(t, day, stop_idx, !fwd));
       auto const round_time = rt(k - 1, l);
@@ -1050,7 +1115,7 @@ struct reconstructor {
 
   // reconstruct.cc:292-373
   std::optional<leg_t> get_route_transport(unsigned k, delta_t time, uint32_t r,
-                                           uint32_t stop_idx) {
+                                           uint32_t stop_idx, uint8_t sections) {
     auto const [day, mam] = split_day_mam(base_day_idx, time);
     for (auto t = tt.d.route_transport_from[r]; t != tt.d.route_transport_to[r]; ++t) {
       auto const ev = tt.event_mam(t, stop_idx, fwd);
@@ -1059,17 +1124,19 @@ struct reconstructor {
       auto const traffic_day = static_cast<int>(day) - cnt / 1440;
       auto const tday = static_cast<uint16_t>(traffic_day);
       if (!tt.transport_active(t, tday)) continue;
-      auto leg = find_start_in_prev_round(k, t, tday, stop_idx);
+      auto leg = find_start_in_prev_round(k, t, tday, stop_idx, sections);
       if (leg.has_value()) return leg;
     }
     return std::nullopt;
   }
 
-  // reconstruct.cc:375-545 (no rtt, no filters)
+  // reconstruct.cc:375-545 (no rtt)
   std::optional<leg_t> get_transport(unsigned k, uint32_t l, delta_t time) {
     for (auto ri = tt.d.location_routes_index[l]; ri != tt.d.location_routes_index[l + 1];
          ++ri) {
       auto const r = tt.d.location_routes[ri];
+      uint8_t sections = 0U;
+      if (!route_allowed(tt, q.allowed_claszes, q.required_flags, r, sections)) continue;
       auto const n = tt.n_stops(r);
       for (auto i = 0U; i != n; ++i) {
         auto const stp = tt.stop(r, i);
@@ -1077,7 +1144,7 @@ struct reconstructor {
             (!fwd && (i == n - 1U || !B2R_STOP_IN(stp)))) {
           continue;
         }
-        auto leg = get_route_transport(k, time, r, i);
+        auto leg = get_route_transport(k, time, r, i, sections);
         if (leg.has_value()) return leg;
       }
     }
@@ -1476,6 +1543,8 @@ void run_search(tt_view const& tt, query_t q, bool fwd, search_result& res) {
   auto const base_idx =
       static_cast<uint16_t>(round_days(mid) - tt.internal_from_days());
   raptor_t algo{tt, fwd, false, is_dest, dist_to_dest, lb, base_idx, tts, st};
+  algo.allowed_claszes = q.allowed_claszes;
+  algo.required_flags = q.required_flags;
   q.sanitize();  // search ctor body
 
   pareto_t results;
@@ -1685,6 +1754,8 @@ void run_one_to_all(tt_view const& tt, query_t const& q, bool fwd, search_result
   std::vector<uint16_t> lb(tt.d.n_locations, 0U);
   auto const base = static_cast<uint16_t>(round_days(q.start_time) - tt.internal_from_days());
   raptor_t r{tt, fwd, true, is_dest, dist_to_dest, lb, base, q.tts, st};
+  r.allowed_claszes = q.allowed_claszes;
+  r.required_flags = q.required_flags;
   pareto_t results;
   r.next_start_time();
   ++st.n_start_times;

@@ -69,6 +69,8 @@ class FixtureTimetable:
         bf_of = {}
         route_stop_index = [0]
         route_stops = []
+        route_clasz = []
+        section_flags = []  # per route stop: flags of the section it starts
         route_n_t = []
         stop_times = []
         transport_bf = []
@@ -79,6 +81,8 @@ class FixtureTimetable:
                 route_stops.append(self.loc_idx[s] | (w[0] << 28) | (w[1] << 29)
                                    | (1 << 30) | (1 << 31))
             route_stop_index.append(len(route_stops))
+            route_clasz.append(r.get("clasz", 10))
+            section_flags += list(r.get("sections", [0] * (len(r["stops"]) - 1))) + [0]
             trs = r["transports"]  # already in route order (mam-sorted)
             # traffic day of the transport = its day; the times stay relative
             route_n_t.append(len(trs))
@@ -107,6 +111,8 @@ class FixtureTimetable:
             stop_times=np.array(stop_times or [0], np.uint16),
             transport_bf=np.array(transport_bf or [0], np.uint32),
             bitfields=np.concatenate(bf_list).astype(np.uint64),
+            route_clasz=np.array(route_clasz or [0], np.uint8),
+            section_flags=np.array(section_flags or [0], np.uint8),
         )
         a = self.arrays
         p = lambda arr, t: arr.ctypes.data_as(C.POINTER(t))
@@ -127,6 +133,9 @@ class FixtureTimetable:
         base.transport_bitfield = p(a["transport_bf"], C.c_uint32)
         base.n_bitfields = len(bf_list)
         base.bitfields = p(a["bitfields"], C.c_uint64)
+        base.route_clasz = p(a["route_clasz"], C.c_uint8)
+        if any(a["section_flags"]):
+            base.route_section_flags = p(a["section_flags"], C.c_uint8)
         self.handle = C.c_void_p()
         rc = lib.b2r_tt_build(C.byref(base), C.byref(self.handle))
         assert rc == 0, rc
@@ -184,6 +193,11 @@ class FixtureQuery:
         qq.extend_interval_later = 1 if q.get("extend_later") else 0
         if q.get("kind") == "one_to_all":
             qq.kind = A.B2R_ONE_TO_ALL
+        if "claszes" in q:
+            qq.allowed_claszes = q["claszes"]
+        qq.require_bike_transport = 1 if q.get("bikes") else 0
+        qq.require_car_transport = 1 if q.get("cars") else 0
+        qq.no_compulsory_reservation = 1 if q.get("no_reservation") else 0
         tts = q.get("tts")
         if tts is not None:
             qq.tts_default = 1 if tts.get("default", True) else 0

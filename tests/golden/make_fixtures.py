@@ -56,12 +56,14 @@ def get_index(route, svc):
 
 
 def group_routes(services):
-    """Services (in load order) -> routes: one route key per stop sequence,
-    split into sub-routes by get_index (gtfs/load_timetable.cc:288-309)."""
+    """Services (in load order) -> routes: one route key per (stop sequence,
+    transport class, per-section flags), split into sub-routes by get_index
+    (gtfs/load_timetable.cc:277-309)."""
     keys = {}
     order = []
     for svc in services:
-        k = tuple(svc["stops"])
+        k = (tuple(svc["stops"]), svc.get("clasz", 10),
+             tuple(svc.get("sections", [0] * (len(svc["stops"]) - 1))))
         if k not in keys:
             keys[k] = [[svc]]
             order.append(k)
@@ -76,8 +78,10 @@ def group_routes(services):
     routes = []
     for k in order:
         for sub in keys[k]:
-            routes.append({"stops": list(k), "transports": [
-                {kk: v for kk, v in x.items() if kk != "stops"} for x in sub]})
+            routes.append({"stops": list(k[0]), "clasz": k[1], "sections": list(k[2]),
+                           "transports": [
+                               {kk: v for kk, v in x.items()
+                                if kk not in ("stops", "clasz", "sections")} for x in sub]})
     return routes
 
 
@@ -197,8 +201,120 @@ def gtfs_dijkstra():
     }
 
 
+def gtfs_clasz():
+    """test/routing/clasz_filter_test.cc test_files: agency Europe/Berlin
+    (UTC+1 on 2024-03-01), service S1 on 2024-03-01 only.  GTFS route types
+    give the classes (src/loader/gtfs/route.cc:22-45, 105): 1100 -> kAir (0),
+    3 -> kBus (10), 2 -> kRegional (6).
+      AIR (route X, air)  A 10:00 -> C 11:00   UTC 09:00 -> 10:00
+      T1  (route 1, bus)  A 10:00 -> B 10:55   UTC 09:00 -> 09:55
+      T2  (route 2, rail) B 11:05 -> C 12:00   UTC 10:05 -> 11:00
+    Stops are far apart: no footpaths, transfer time 2 min."""
+    d = "2024-03-01"
+    services = [
+        dict(utc_service("X", ["A", "C"], d, [hm("09:00"), hm("10:00")]), id="AIR", clasz=0),
+        dict(utc_service("1", ["A", "B"], d, [hm("09:00"), hm("09:55")]), id="T1", clasz=10),
+        dict(utc_service("2", ["B", "C"], d, [hm("10:05"), hm("11:00")]), id="T2", clasz=6),
+    ]
+    return {
+        "date_range": ["2024-03-01", "2024-03-02"],
+        "locations": [{"id": x, "name": x, "transfer_time": 2} for x in "ABC"],
+        "footpaths": [],
+        "routes": group_routes(services),
+    }
+
+
+# Route flag bits (include/nigiri/types.h:417-423).
+FLAG_BIKES, FLAG_RESERVATION_NOT_REQUIRED = 0, 3
+
+
+def flag_service(name, stops, times, sections, flag):
+    """A service of 2019-05-01 (UTC times) whose section s carries `flag`
+    when sections[s] is true."""
+    return dict(utc_service(name, stops, "2019-05-01", [hm(x) for x in times]), clasz=10,
+                sections=[(1 << flag) if x else 0 for x in sections])
+
+
+def gtfs_flags_1(flag):
+    """Timetable 1 of test/routing/bike_transport_test.cc and of
+    test/routing/no_compulsory_reservation_test.cc (same stops and times;
+    the flag is bikes_allowed = 1, resp. pickup_type != 2, per trip --
+    src/loader/gtfs/trip.cc:296-316).  Europe/Berlin, UTC+2 on 2019-05-01:
+      T0 (route 0) A 08:00 - B 08:10 - C 08:20            no flag
+      T1 (route 1) A 08:00 - B 08:15 - C 08:30            flag
+      T2 (route 1) A 09:00 - B 09:15 - C 09:30            no flag
+    Block 1 holds T3 (route 2, C 08:35 - D 08:40, flag), T5 (route 3,
+    D 08:42 - E 08:50 - F 08:55, no flag), T4 (route 2, C 08:45 - D 08:50,
+    flag) and T6 (route 3, D 08:52 - E 09:00 - F 09:05, flag).  The block's
+    rule services (block::rule_services, src/loader/gtfs/trip.cc:31-106)
+    chain trips whose first stop is the last stop of the one before: T3>T5
+    and T4>T6, each one transport over C-D-E-F with per-section flags
+    [1, 0, 0] and [1, 1, 1].  The route key includes the flags, so T0 / T2
+    share a route, T1 has its own, and so has each chained transport.
+    Printed names are the route short names of the first trip."""
+    services = [
+        flag_service("0", list("ABC"), ["08:00", "08:10", "08:10", "08:20"], [0, 0], flag),
+        flag_service("1", list("ABC"), ["08:00", "08:15", "08:15", "08:30"], [1, 1], flag),
+        flag_service("1", list("ABC"), ["09:00", "09:15", "09:15", "09:30"], [0, 0], flag),
+        flag_service("2", list("CDEF"), ["08:35", "08:40", "08:42", "08:50", "08:50", "08:55"],
+                     [1, 0, 0], flag),
+        flag_service("2", list("CDEF"), ["08:45", "08:50", "08:52", "09:00", "09:00", "09:05"],
+                     [1, 1, 1], flag),
+    ]
+    return {
+        "date_range": ["2019-05-01", "2019-05-02"],
+        "locations": [{"id": x, "name": x, "transfer_time": 2} for x in "ABCDEF"],
+        "footpaths": [],
+        "routes": group_routes(services),
+    }
+
+
+def gtfs_flags_2(flag):
+    """Timetable 2 of the same two tests: blocks T1>T2 and T3>T4, the flag on
+    every trip but T1 (UTC):
+      T1>T2 (route 1) A 08:00 - B 08:10/08:15 - C 08:20 - D 08:25  [0, 1, 1]
+      T3>T4 (route 1) A 08:00 - B 08:20/08:25 - C 08:30 - D 08:35  [1, 1, 1]"""
+    services = [
+        flag_service("1", list("ABCD"), ["08:00", "08:10", "08:15", "08:20", "08:20", "08:25"],
+                     [0, 1, 1], flag),
+        flag_service("1", list("ABCD"), ["08:00", "08:20", "08:25", "08:30", "08:30", "08:35"],
+                     [1, 1, 1], flag),
+    ]
+    return {
+        "date_range": ["2019-05-01", "2019-05-02"],
+        "locations": [{"id": x, "name": x, "transfer_time": 2} for x in "ABCD"],
+        "footpaths": [],
+        "routes": group_routes(services),
+    }
+
+
+def gtfs_flags_3(flag):
+    """Timetable 3 of the same two tests: blocks T1>T2>T3 and T4>T5>T6, the
+    flag on every trip but T2 (UTC):
+      T1>T2>T3 (route 1) A 08:00 - B 08:10/08:15 - C 08:20/08:25 - D 08:30  [1, 0, 1]
+      T4>T5>T6 (route 1) A 08:00 - B 08:20/08:25 - C 08:30/08:35 - D 08:40  [1, 1, 1]"""
+    services = [
+        flag_service("1", list("ABCD"), ["08:00", "08:10", "08:15", "08:20", "08:25", "08:30"],
+                     [1, 0, 1], flag),
+        flag_service("1", list("ABCD"), ["08:00", "08:20", "08:25", "08:30", "08:35", "08:40"],
+                     [1, 1, 1], flag),
+    ]
+    return {
+        "date_range": ["2019-05-01", "2019-05-02"],
+        "locations": [{"id": x, "name": x, "transfer_time": 2} for x in "ABCD"],
+        "footpaths": [],
+        "routes": group_routes(services),
+    }
+
+
 TIMETABLES = {"hrd_abc": hrd_abc(), "gtfs_transfer_time": gtfs_transfer_time(),
-              "hrd_simple": hrd_simple(), "gtfs_dijkstra": gtfs_dijkstra()}
+              "hrd_simple": hrd_simple(), "gtfs_dijkstra": gtfs_dijkstra(),
+              "gtfs_clasz": gtfs_clasz(),
+              "gtfs_bikes_1": gtfs_flags_1(FLAG_BIKES), "gtfs_bikes_2": gtfs_flags_2(FLAG_BIKES),
+              "gtfs_bikes_3": gtfs_flags_3(FLAG_BIKES),
+              "gtfs_reservation_1": gtfs_flags_1(FLAG_RESERVATION_NOT_REQUIRED),
+              "gtfs_reservation_2": gtfs_flags_2(FLAG_RESERVATION_NOT_REQUIRED),
+              "gtfs_reservation_3": gtfs_flags_3(FLAG_RESERVATION_NOT_REQUIRED)}
 
 # ----------------------------------------------------------------------------
 # Golden printout parser (journey::print, src/routing/journey.cc)
@@ -359,6 +475,39 @@ def cases():
                   ref="test/routing/transfer_time_settings_test.cc", golden=None,
                   query=dict(start=[["A", 0, 0]], dest=[["C", 0, 0]], interval=day_iv,
                              direction="fwd", max_transfers=0, max_travel_time=35)))
+    # test/routing/clasz_filter_test.cc (forward only, as there)
+    clasz_iv = [t("2024-03-01 00:00"), t("2024-03-02 00:00")]
+    air, regional, bus, ship = 1 << 0, 1 << 6, 1 << 10, 1 << 11
+    for vname, mask, golden in [("all", 0xFFFF, "expected"),
+                                ("bus_regional_air", bus | regional | air, "expected"),
+                                ("bus_regional", bus | regional, "expected_1"),
+                                ("ship", ship, None)]:
+        c.append(dict(name=f"clasz_{vname}", timetable="gtfs_clasz",
+                      ref="test/routing/clasz_filter_test.cc", golden=golden,
+                      query=dict(start=[["A", 0, 0]], dest=[["C", 0, 0]], interval=clasz_iv,
+                                 direction="fwd", claszes=mask)))
+    # test/routing/bike_transport_test.cc, no_compulsory_reservation_test.cc
+    flag_iv = [t("2019-05-01 00:00"), t("2019-05-02 00:00")]
+    for kind, ref, key, off, on in [
+            ("bikes", "test/routing/bike_transport_test.cc", "bikes", "no_bike", "bike"),
+            ("reservation", "test/routing/no_compulsory_reservation_test.cc",
+             "no_reservation", "compulsory", "no_reservation")]:
+        for tt_no, a, b, g_off, g_on in [
+                (1, "A", "C", f"expected_A_C_{off}", f"expected_A_C_{on}"),
+                (1, "C", "D", "expected_C_D", "expected_C_D"),
+                (1, "A", "D", f"expected_A_D_{off}", f"expected_A_D_{on}"),
+                (1, "A", "F", f"expected_A_F_{off}", f"expected_A_F_{on}"),
+                (2, "A", "D", f"expected2_A_D_{off}", f"expected2_A_D_{on}"),
+                (3, "A", "D", f"expected3_A_D_{off}", f"expected3_A_D_{on}")]:
+            for d in ("fwd", "bwd"):
+                s, e = (a, b) if d == "fwd" else (b, a)
+                for req, golden in ((False, g_off), (True, g_on)):
+                    q = dict(start=[[s, 0, 0]], dest=[[e, 0, 0]], interval=flag_iv, direction=d)
+                    if req:
+                        q[key] = True
+                    c.append(dict(name=f"{kind}{tt_no}_{a}{b}_{'req' if req else 'any'}_{d}",
+                                  timetable=f"gtfs_{kind}_{tt_no}", ref=ref, golden=golden,
+                                  query=q))
     return c
 
 

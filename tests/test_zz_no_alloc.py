@@ -15,7 +15,12 @@ from nigiri_b200.timetable import HostTimetable, QuerySet
 pytestmark = pytest.mark.gpu
 
 
-def one_to_all_queries(h, n, seed):
+# (allowed classes, bikes, no reservation): not bus; bikes; tram or bus
+# without compulsory reservation
+FILTERS = [(0xFFFF & ~(1 << 10), 0, 0), (0xFFFF, 1, 0), ((1 << 10) | (1 << 9), 0, 1)]
+
+
+def one_to_all_queries(h, n, seed, filters=False):
     qs = QuerySet(h, 1, n, seed=seed)
     arr = (A.Query * qs.n)()
     for i in range(qs.n):
@@ -23,6 +28,11 @@ def one_to_all_queries(h, n, seed):
         arr[i].kind = A.B2R_ONE_TO_ALL
         arr[i].n_destination = 0
         arr[i].direction = i % 2
+        if filters:
+            mask, bikes, resv = FILTERS[i % len(FILTERS)]
+            arr[i].allowed_claszes = mask
+            arr[i].require_bike_transport = bikes
+            arr[i].no_compulsory_reservation = resv
     return qs, arr
 
 
@@ -38,13 +48,14 @@ def noalloc_rows(lib, tt, q, n_loc):
     return buf[: n_rows.value * n_loc].reshape(n_rows.value, n_loc), base_day.value
 
 
-@pytest.mark.parametrize("workload", [1, 2])
-def test_noalloc_rows_equal_batched_rows_on_two_calls_in_a_row(workload):
+@pytest.mark.parametrize("workload,filters", [(1, False), (2, False), (2, True)],
+                         ids=["w1", "w2", "w2_filters"])
+def test_noalloc_rows_equal_batched_rows_on_two_calls_in_a_row(workload, filters):
     lib = A.lib()
     h = HostTimetable.generate(workload)
     tt = R.Timetable(h.desc, owner=h)
     eng = R.Engine(tt, max_slots=64)
-    qs, arr = one_to_all_queries(h, 6, seed=40 + workload)
+    qs, arr = one_to_all_queries(h, 6, seed=40 + workload, filters=filters)
     out = (A.Result * qs.n)()
     assert lib.b2r_search_batch(eng.handle, arr, qs.n, out) == A.B2R_OK, lib.b2r_last_error()
     n = h.desc.n_locations
