@@ -69,6 +69,10 @@ const char* b2r_last_error(void);
 #define B2R_FLAG_RESERVATION_NOT_REQUIRED 3u
 #define B2R_ALL_CLASZ 0xFFFFFFFFu
 
+/* Search algorithms (b2r_query::algorithm). */
+#define B2R_ALGO_RAPTOR 0u
+#define B2R_ALGO_PONG 1u
+
 /* Location types used by location_match_mode::kIntermodal
  * (for_each_meta.h:29-35 reads kGeneratedTrack children). */
 #define B2R_LOC_STATION 0u
@@ -206,7 +210,9 @@ typedef struct b2r_query {
   uint8_t require_bike_transport;
   uint8_t require_car_transport;
   uint8_t no_compulsory_reservation;
-  uint8_t pad2_;
+  /* B2R_ALGO_RAPTOR: routing::raptor_search (search<raptor>, raptor_search.cc);
+   * B2R_ALGO_PONG: routing::pong_search (pong.cc:63-475), one-to-one only */
+  uint8_t algorithm;
 } b2r_query;
 
 /* Fill a query with nigiri's defaults (query.h:84-99). */
@@ -431,10 +437,11 @@ int b2r_engine_get_shape(const b2r_engine* e, b2r_launch_shape* out);
 /* Rejects values out of range; re-captures the super-step graph. */
 int b2r_engine_set_shape(b2r_engine* e, const b2r_launch_shape* shape);
 
-/* Autotuner: runs `sample` (n queries, results discarded) once per candidate
- * launch shape, one knob at a time over a small grid of values, keeps the
- * shape with the shortest batch wall time and reports what it tried.  The
- * last-batch results and statistics are overwritten. */
+/* Autotuner: runs `sample` (n queries, results discarded) three times per
+ * candidate launch shape, one knob at a time over a small grid of values
+ * (coordinate descent, repeated until a pass changes nothing, at most three
+ * passes), keeps the shape with the shortest batch wall time and reports
+ * what it tried.  The last-batch results and statistics are overwritten. */
 typedef struct b2r_tune_report {
   uint32_t n_tried;
   b2r_launch_shape start, best;

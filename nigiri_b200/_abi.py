@@ -27,6 +27,7 @@ B2R_MATCH_EXACT, B2R_MATCH_ONLY_CHILDREN, B2R_MATCH_EQUIVALENT, B2R_MATCH_INTERM
 B2R_ONE_TO_ONE, B2R_ONE_TO_ALL = 0, 1
 B2R_FLAG_BIKES, B2R_FLAG_CARS, B2R_FLAG_WHEELCHAIR, B2R_FLAG_RESERVATION_NOT_REQUIRED = 0, 1, 2, 3
 B2R_ALL_CLASZ = 0xFFFFFFFF
+B2R_ALGO_RAPTOR, B2R_ALGO_PONG = 0, 1
 B2R_LEG_TRANSPORT, B2R_LEG_FOOTPATH, B2R_LEG_OFFSET = 0, 1, 2
 
 _u8p, _u16p, _u32p, _u64p = (C.POINTER(C.c_uint8), C.POINTER(C.c_uint16),
@@ -79,7 +80,7 @@ class Query(C.Structure):
         ("tts_factor", C.c_float),
         ("allowed_claszes", C.c_uint32), ("require_bike_transport", C.c_uint8),
         ("require_car_transport", C.c_uint8), ("no_compulsory_reservation", C.c_uint8),
-        ("pad2_", C.c_uint8),
+        ("algorithm", C.c_uint8),
     ]
 
 

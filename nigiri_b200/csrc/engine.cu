@@ -1830,11 +1830,11 @@ int b2r_engine_autotune(b2r_engine* e, const b2r_query* sample, uint32_t n, b2r_
     if (e == nullptr || sample == nullptr || n == 0) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
     if (e->serving) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "engine is serving");
     std::vector<b2r_result> out(n);
-    // objective: wall time of the sample batch (best of two runs)
+    // objective: wall time of the sample batch (best of three runs)
     auto const measure = [&](b2r_launch_shape const& sh) -> double {
       if (auto const rc = b2r_engine_set_shape(e, &sh); rc != B2R_OK) throw b2r::cuda_error(b2r_last_error());
       auto best = 1e300;
-      for (auto rep = 0; rep != 2; ++rep) {
+      for (auto rep = 0; rep != 3; ++rep) {
         if (b2r_search_batch(e, sample, n, out.data()) != B2R_OK) throw b2r::cuda_error(b2r_last_error());
         best = std::min(best, e->last.host_prep_ms);
       }
@@ -1848,7 +1848,8 @@ int b2r_engine_autotune(b2r_engine* e, const b2r_query* sample, uint32_t n, b2r_
       auto cur_ms = measure(cur);
       rep.start_ms = cur_ms;
       rep.n_tried = 1;
-      // coordinate descent, one pass over the knobs
+      // coordinate descent over the knobs, repeated until a pass changes
+      // nothing (at most three passes)
       struct knob {
         uint32_t b2r_launch_shape::*field;
         std::vector<uint32_t> values;
@@ -1858,18 +1859,25 @@ int b2r_engine_autotune(b2r_engine* e, const b2r_query* sample, uint32_t n, b2r_
                                        {&b2r_launch_shape::pair_blocks_per_sm, {2, 4, 8, 16}},
                                        {&b2r_launch_shape::recon_blocks_per_sm, {1, 2, 4, 8}},
                                        {&b2r_launch_shape::steps_per_sync, {1, 2, 4, 8}}};
-      for (auto const& k : knobs) {
-        for (auto const v : k.values) {
-          if (cur.*(k.field) == v) continue;
-          auto trial = cur;
-          trial.*(k.field) = v;
-          auto const ms = measure(trial);
-          ++rep.n_tried;
-          if (ms < cur_ms) {
-            cur = trial;
-            cur_ms = ms;
+      for (auto pass = 0; pass != 3; ++pass) {
+        auto changed = false;
+        for (auto const& k : knobs) {
+          auto const at_start = cur.*(k.field);
+          for (auto const v : k.values) {
+            if (cur.*(k.field) == v) continue;
+            auto trial = cur;
+            trial.*(k.field) = v;
+            auto const ms = measure(trial);
+            ++rep.n_tried;
+            if (ms < cur_ms) {
+              cur = trial;
+              cur_ms = ms;
+            }
           }
+          changed = changed || cur.*(k.field) != at_start;
         }
+        if (!changed) break;
+        cur_ms = measure(cur);  // re-measured: the first figure may have been a lucky one
       }
       if (b2r_engine_set_shape(e, &cur) != B2R_OK) return B2R_ERR_CUDA;
       rep.best = cur;

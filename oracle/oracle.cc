@@ -13,6 +13,9 @@
 #include <limits>
 #include <map>
 #include <optional>
+#include <queue>
+#include <array>
+#include <iterator>
 #include <stdexcept>
 #include <thread>
 #include <unordered_map>
@@ -229,6 +232,7 @@ struct query_t {
   double fastest_direct_factor{1.0};
   uint32_t allowed_claszes{B2R_ALL_CLASZ};
   uint8_t required_flags{0};  // bit f: route flag f required
+  bool pong{false};           // pong_search instead of search<raptor>
 
   void flip_dir() {  // query.cc:52-57
     std::swap(start, dest);
@@ -281,6 +285,7 @@ query_t to_query(b2r_query const& q) {
       (q.no_compulsory_reservation != 0
            ? 1U << B2R_FLAG_RESERVATION_NOT_REQUIRED
            : 0U));
+  r.pong = q.algorithm == B2R_ALGO_PONG;
   return r;
 }
 
@@ -344,8 +349,14 @@ struct journey_t {
   int travel_time() const { return std::abs(dest_time - start_time); }
 };
 
-struct pareto_t {  // pareto_set.h:21-37
+struct pareto_t {  // pareto_set.h:17-37
   std::vector<journey_t> els;
+  bool is_dominated(journey_t const& el) const {
+    for (auto const& x : els) {
+      if (x.dominates(el)) return true;
+    }
+    return false;
+  }
   bool add(journey_t&& el) {
     auto n_removed = size_t{0};
     for (auto i = 0U; i < els.size(); ++i) {
@@ -432,6 +443,10 @@ struct raptor_t {
   or_stats& st;
   uint32_t allowed_claszes{B2R_ALL_CLASZ};  // query filters
   uint8_t required_flags{0U};
+  // pong's pruning bounds (raptor_state::bounds_storage_, raptor.h:117-172):
+  // rows [k][location] folded from another search's round times
+  std::vector<delta_t> bounds;
+  unsigned bounds_last_k{0U};
 
   delta_t kInvalid() const { return fwd ? 32767 : -32768; }
   bool is_better(int a, int b) const { return fwd ? a < b : a > b; }
@@ -488,6 +503,28 @@ struct raptor_t {
     best[l] = static_cast<delta_t>(get_best(unix_to_delta(base_days(), t), best[l]));
     RT(0, l) = static_cast<delta_t>(get_best(unix_to_delta(base_days(), t), RT(0, l)));
     station_mark.set(l);
+  }
+
+  // fill_bounds, raptor.h:117-170 (no vias, no td footpaths): row 0 is
+  // round 0, row k the best of rounds 0..k
+  void fill_bounds(size_t n_rows, std::vector<delta_t>& dst) const {
+    dst.resize(static_cast<size_t>(kK) * n_loc);
+    for (auto x = 0U; x != n_loc; ++x) dst[x] = rt[x];
+    for (auto k = size_t{1U}; k < n_rows; ++k) {
+      for (auto x = 0U; x != n_loc; ++x) {
+        auto const s = rt[k * n_loc + x], d = dst[(k - 1) * n_loc + x];
+        dst[k * n_loc + x] = fwd ? std::min(s, d) : std::max(s, d);
+      }
+    }
+  }
+  // within_bounds, raptor.h:458-489: the label t at l in round k may not
+  // beat the bounding search's row (last_k - k) at l by less than l's
+  // transfer time
+  bool within_bounds(unsigned k, uint32_t l, int t) const {
+    if (bounds_last_k == 0U) return true;
+    auto const row = bounds[static_cast<size_t>(bounds_last_k - k) * n_loc + l];
+    auto const transfer = dir(adjusted<int>(tts, tt.d.transfer_time[l]));
+    return is_better_or_eq(t, row + transfer);
   }
 
   uint16_t get_lb(uint32_t i) const { return lb[i]; }
@@ -586,7 +623,7 @@ struct raptor_t {
               ? 0
               : dir(adjusted<int>(tts, tt.d.transfer_time[i]));
       auto const fp_target_time = clamp16(tmp_time + transfer_time);
-      if (is_better(fp_target_time, best[i])) {
+      if (bounds_last_k == 0U && is_better(fp_target_time, best[i])) {
         RT(k, i) = static_cast<delta_t>(get_best(fp_target_time, RT(k, i)));
         ++st.n_label_writes;
       }
@@ -596,6 +633,7 @@ struct raptor_t {
             !is_better_or_eq(fp_target_time + dir(get_lb(i)), time_at_dest[k])) {
           return;
         }
+        if (!within_bounds(k, i, fp_target_time)) return;
         RT(k, i) = fp_target_time;
         best[i] = fp_target_time;
         st.n_label_writes += 2;
@@ -617,7 +655,7 @@ struct raptor_t {
         if (tmp_time == kInvalid()) continue;
         auto const fp_target_time = clamp16(
             tmp_time + dir(adjusted<int>(tts, static_cast<int>(B2R_FP_DURATION(fp)))));
-        if (is_better(fp_target_time, best[target])) {
+        if (bounds_last_k == 0U && is_better(fp_target_time, best[target])) {
           RT(k, target) = static_cast<delta_t>(get_best(fp_target_time, RT(k, target)));
           ++st.n_label_writes;
         }
@@ -628,6 +666,7 @@ struct raptor_t {
                                time_at_dest[k])) {
             continue;
           }
+          if (!within_bounds(k, target, fp_target_time)) continue;
           RT(k, target) = fp_target_time;
           best[target] = fp_target_time;
           st.n_label_writes += 2;
@@ -685,7 +724,8 @@ struct raptor_t {
         current_best = static_cast<delta_t>(
             get_best(get_best(RT(k - 1, l), tmp[l]), best[l]));
         if (is_better_or_eq(by_transport, time_at_dest[k]) && lb_reachable(l) &&
-            is_better_or_eq(by_transport + dir(get_lb(l)), time_at_dest[k])) {
+            is_better_or_eq(by_transport + dir(get_lb(l)), time_at_dest[k]) &&
+            within_bounds(k, l, by_transport)) {
           tmp[l] = static_cast<delta_t>(get_best(by_transport, tmp[l]));
           ++st.n_label_writes;
           station_mark.set(l);
@@ -1770,6 +1810,333 @@ void run_one_to_all(tt_view const& tt, query_t const& q, bool fwd, search_result
   res.base_day = r.base_days();
 }
 
+// ------------------------------------------------------------------- pong
+// lookup_footpath, direct.cc:65-160, for the exact-match offsets of an
+// alternative query (no td footpaths, profile 0): the shortest way from an
+// offset's location to `loc` (boarding) or from `loc` to it (alighting),
+// either the reflexive transfer time or a footpath.
+std::optional<leg_t> lookup_footpath(tt_view const& tt, query_t const& q, uint32_t loc,
+                                     unixtime t, bool boarding) {
+  auto const& offs = boarding ? q.start : q.dest;
+  auto const use_footpaths = boarding ? q.use_start_footpaths : true;
+  int best_dur = kFpMaxDuration;
+  uint32_t best_source = 0U;
+  for (auto const& o : offs) {
+    auto const l = o.target;  // for_each_meta of kExact
+    if (l == loc && o.duration < best_dur) {
+      best_dur = o.duration + adjusted<uint8_t>(q.tts, tt.d.transfer_time[l]);
+      best_source = o.target;
+    }
+    if (!use_footpaths) continue;
+    auto eff = kFpMaxDuration;
+    auto const& idx = boarding ? tt.d.footpaths_out_index : tt.d.footpaths_in_index;
+    auto const* fps = boarding ? tt.d.footpaths_out : tt.d.footpaths_in;
+    for (auto fi = idx[l]; fi != idx[l + 1]; ++fi) {
+      if (B2R_FP_TARGET(fps[fi]) != loc) continue;
+      auto const adj =
+          adjusted<int16_t>(q.tts, static_cast<int16_t>(B2R_FP_DURATION(fps[fi])));
+      if (adj < eff) eff = adj;
+    }
+    if (eff >= kFpMaxDuration) continue;
+    auto const total = o.duration + eff;
+    if (total < best_dur) {
+      best_dur = total;
+      best_source = o.target;
+    }
+  }
+  if (best_dur >= kFpMaxDuration) return std::nullopt;
+  leg_t l;
+  l.from = boarding ? best_source : loc;
+  l.to = boarding ? loc : best_source;
+  l.dep = boarding ? t - best_dur : t;
+  l.arr = boarding ? t : t + best_dur;
+  set_fp(l, l.to, best_dur);
+  return l;
+}
+
+// The first journey get_direct_journeys<kForward> (direct.cc:454-605)
+// yields for an exact-match one-to-one query departing at `time` or later:
+// per (route, boarding stop, alighting stop) the first departure route_gen
+// (direct.cc:281-376) accepts, merged by arrival time in a binary heap as
+// the reference's priority queue does.  Returns walk, transit, walk.
+std::optional<std::array<leg_t, 3>> first_direct_journey(tt_view const& tt, query_t const& q,
+                                                         unixtime time) {
+  auto const from = q.start.front().target, to = q.dest.front().target;
+  std::vector<uint32_t> boarding{from}, alighting{to};
+  for (auto fi = tt.d.footpaths_out_index[from]; fi != tt.d.footpaths_out_index[from + 1]; ++fi) {
+    boarding.push_back(B2R_FP_TARGET(tt.d.footpaths_out[fi]));
+  }
+  for (auto fi = tt.d.footpaths_in_index[to]; fi != tt.d.footpaths_in_index[to + 1]; ++fi) {
+    alighting.push_back(B2R_FP_TARGET(tt.d.footpaths_in[fi]));
+  }
+  auto const has = [](std::vector<uint32_t> const& v, uint32_t x) {
+    return std::find(v.begin(), v.end(), x) != v.end();
+  };
+  auto const routes_of = [&](std::vector<uint32_t> const& locs) {
+    std::vector<uint32_t> rs;
+    for (auto const l : locs) {
+      for (auto ri = tt.d.location_routes_index[l]; ri != tt.d.location_routes_index[l + 1]; ++ri) {
+        rs.push_back(tt.d.location_routes[ri]);
+      }
+    }
+    std::sort(rs.begin(), rs.end());
+    rs.erase(std::unique(rs.begin(), rs.end()), rs.end());
+    return rs;
+  };
+  auto const from_routes = routes_of(boarding), to_routes = routes_of(alighting);
+  std::vector<uint32_t> both;
+  std::set_intersection(from_routes.begin(), from_routes.end(), to_routes.begin(),
+                        to_routes.end(), std::back_inserter(both));
+
+  auto const day_hi = tt.d.date_range_to + 1 - tt.internal_from_days();
+  std::vector<std::array<leg_t, 3>> heads;
+  for (auto const r : both) {
+    // route filters of direct.cc:503-513: class, flag on some or all sections
+    if (((q.allowed_claszes >> tt.clasz(r)) & 1U) == 0U) continue;
+    auto const fl = tt.flags(r);
+    auto skip = false;
+    for (auto f = 0U; f != 4U; ++f) {
+      if (((q.required_flags >> f) & 1U) != 0U && ((fl >> (2U * f)) & 3U) == 0U) skip = true;
+    }
+    if (skip) continue;
+    // run_stop::is_flag_set(f, kDep) of section s (rt/frun.cc:453-475)
+    auto const flag_set = [&](uint32_t f, uint32_t s) {
+      if ((fl >> (2U * f)) & 1U) return true;
+      if (((fl >> (2U * f + 1U)) & 1U) == 0U) return false;
+      return ((tt.section_flags(r, s) >> f) & 1U) != 0U;
+    };
+    auto const n = tt.n_stops(r);
+    // for_each_pair, direct.cc:429-450
+    std::optional<uint32_t> board;
+    for (auto i = 0U; i != n; ++i) {
+      auto const stp = tt.stop(r, i);
+      auto const loc = B2R_STOP_LOC(stp);
+      if (board.has_value()) {
+        if (!has(alighting, loc) || !B2R_STOP_OUT(stp)) continue;
+        auto const a = *board, b = i;
+        board.reset();
+        // sections_violate_constraints, direct.cc:242-260
+        auto violates = false;
+        for (auto s = a; s != b && !violates; ++s) {
+          for (auto f = 0U; f != 4U; ++f) {
+            if (((q.required_flags >> f) & 1U) != 0U && !flag_set(f, s)) violates = true;
+          }
+        }
+        if (violates) continue;
+        // route_gen<kForward>: days from time's day on, transports in order
+        auto const boarding_loc = B2R_STOP_LOC(tt.stop(r, a));
+        auto const alighting_loc = B2R_STOP_LOC(tt.stop(r, b));
+        auto const* ev = tt.event_times(r, a, false);
+        auto const n_t = tt.n_t(r);
+        auto found = false;
+        for (auto day = (time - tt.internal_from()) / 1440; !found && day <= day_hi; ++day) {
+          if (!tt.route_active(r, static_cast<uint16_t>(day))) continue;
+          for (auto x = 0U; x != n_t; ++x) {
+            auto const day_off = day - static_cast<int>(B2R_DELTA_DAYS(ev[x]));
+            if (day_off < 0 || day_off >= B2R_MAX_DAYS) continue;
+            auto const t = tt.d.route_transport_from[r] + x;
+            auto const sd = static_cast<uint16_t>(day_off);
+            if (!tt.transport_active(t, sd)) continue;
+            auto const bt = tt.event_time(t, sd, a, false), at = tt.event_time(t, sd, b, true);
+            auto const bw = lookup_footpath(tt, q, boarding_loc, bt, true);
+            auto const aw = lookup_footpath(tt, q, alighting_loc, at, false);
+            if (!bw.has_value() || !aw.has_value() || bw->dep < time) continue;
+            leg_t transit = make_leg(true, boarding_loc, alighting_loc, bt, at);
+            set_run(transit, t, sd, static_cast<uint16_t>(a), static_cast<uint16_t>(b));
+            heads.push_back({*bw, transit, *aw});
+            found = true;
+            break;
+          }
+        }
+      } else if (has(boarding, loc) && B2R_STOP_IN(stp)) {
+        board = i;
+      }
+    }
+  }
+  if (heads.empty()) return std::nullopt;
+  auto const cmp = [&](size_t a, size_t b) { return heads[a][2].arr > heads[b][2].arr; };
+  std::priority_queue<size_t, std::vector<size_t>, decltype(cmp)> heap{cmp};
+  for (auto i = size_t{0}; i != heads.size(); ++i) heap.push(i);
+  return heads[heap.top()];
+}
+
+// get_earliest_alternative, pong.cc:35-61: the earliest direct journey from
+// `from` (reached at from_arr) to `to` that arrives by to_dep, its walk
+// moved to start at from_arr.
+std::optional<std::array<leg_t, 3>> get_earliest_alternative(tt_view const& tt,
+                                                             query_t const& q, uint32_t from,
+                                                             uint32_t to, unixtime from_arr,
+                                                             unixtime to_dep) {
+  query_t dq;  // make_alternative_query, leg_alternatives.cc:27-45
+  dq.start_mode = B2R_MATCH_EXACT;
+  dq.dest_mode = B2R_MATCH_EXACT;
+  dq.use_start_footpaths = true;
+  dq.start = {{from, 0, 0}};
+  dq.dest = {{to, 0, 0}};
+  dq.allowed_claszes = q.allowed_claszes;
+  dq.required_flags = q.required_flags;
+  dq.tts = q.tts;
+  auto legs = first_direct_journey(tt, dq, from_arr);
+  if (!legs.has_value() || (*legs)[2].arr > to_dep) return std::nullopt;
+  auto const walk = (*legs)[0].arr - (*legs)[0].dep;
+  (*legs)[0].dep = from_arr;
+  (*legs)[0].arr = from_arr + walk;
+  return legs;
+}
+
+// pong.cc:63-475 for Rt = false, Vias = 0, no td offsets: a ping search from
+// the current start time, then for each of its results (most transfers
+// first) a pong search back from its arrival, bounded by the ping's round
+// times, that finds the latest departure; the sweep continues one minute
+// after the earliest such departure.
+void run_pong(tt_view const& tt, query_t q, bool fwd, search_result& res) {
+  auto& st = res.stats;
+  q.sanitize();
+  auto const fastest_direct = get_fastest_direct(tt, q, fwd);
+  auto const search_interval = q.is_interval ? interval_t{q.iv_from, q.iv_to}
+                                             : interval_t{q.start_time, q.start_time};
+  auto const mid = static_cast<int64_t>(search_interval.from) +
+                   (search_interval.to - search_interval.from) / 2;
+  auto const base_idx = static_cast<uint16_t>(round_days(mid) - tt.internal_from_days());
+
+  bitvec ping_is_dest;
+  std::vector<uint16_t> ping_dist, ping_lb;
+  collect_destinations(tt, q, ping_is_dest, ping_dist);
+  dijkstra_lb(tt, q, fwd, ping_lb);
+  raptor_t ping{tt, fwd, false, ping_is_dest, ping_dist, ping_lb, base_idx, q.tts, st};
+  ping.allowed_claszes = q.allowed_claszes;
+  ping.required_flags = q.required_flags;
+
+  auto qf = q;
+  qf.flip_dir();
+  bitvec pong_is_dest;
+  std::vector<uint16_t> pong_dist;
+  collect_destinations(tt, qf, pong_is_dest, pong_dist);
+  std::vector<uint16_t> const pong_lb(tt.d.n_locations, 0U);  // kPruneWithPingBounds
+  raptor_t pong{tt, !fwd, false, pong_is_dest, pong_dist, pong_lb, base_idx, q.tts, st};
+  pong.allowed_claszes = q.allowed_claszes;
+  pong.required_flags = q.required_flags;
+  // the pong's start labels walk only for station starts (pong.cc:291-295)
+  qf.use_start_footpaths = qf.start_mode != B2R_MATCH_INTERMODAL;
+
+  pareto_t results;
+  std::vector<start_t> starts;
+  auto start_time = fwd ? search_interval.from : search_interval.to - 1;
+  auto const end_time = fwd ? search_interval.to : search_interval.from - 1;
+  auto const is_better = [&](int a, int b) { return fwd ? a < b : a > b; };
+  auto const is_validated = [&](journey_t const& j) { return is_better(j.dest_time, start_time); };
+  auto const result_count = [&](bool include_too_slow) {
+    auto c = 0U;
+    for (auto const& j : results.els) {
+      c += (is_validated(j) && (include_too_slow || (j.travel_time() < fastest_direct &&
+                                                     j.travel_time() <= q.max_travel_time)))
+               ? 1U
+               : 0U;
+    }
+    return c;
+  };
+  auto const ext_from = tt.external_from(), ext_to = tt.external_to();
+  while ((is_better(start_time, end_time) ||
+          result_count(true) + result_count(false) < 2U * q.min_connection_count) &&
+         ext_from <= start_time && start_time < ext_to) {
+    // ping
+    starts.clear();
+    get_starts(tt, fwd, {false, start_time, {}}, q, q.tts, starts, false);
+    ping.reset_arrivals();
+    ping.next_start_time();
+    ++st.n_start_times;
+    for (auto const& s : starts) ping.add_start(s.stop, s.time_at_stop);
+    auto const worst_time_at_dest =
+        start_time + (fwd ? 1 : -1) * std::min(q.max_travel_time + 1440, int{kMaxTravelTime});
+    pareto_t ping_results;
+    ping.execute(start_time, q.max_transfers, worst_time_at_dest, ping_results);
+    if (ping_results.els.empty()) break;
+    std::erase_if(ping_results.els,
+                  [&](journey_t const& x) { return results.is_dominated(x); });
+    if (ping_results.els.empty()) break;
+    std::sort(ping_results.els.begin(), ping_results.els.end(),
+              [](journey_t const& a, journey_t const& b) { return a.transfers > b.transfers; });
+
+    // pongs
+    ping.fill_bounds(ping_results.els.front().transfers + size_t{1U}, pong.bounds);
+    pong.reset_arrivals();
+    for (auto& ping_j : ping_results.els) {
+      pong.bounds_last_k = ping_j.transfers + 1U;
+      starts.clear();
+      get_starts(tt, !fwd, {false, ping_j.dest_time, {}}, qf, q.tts, starts, false);
+      pong.next_start_time();
+      ++st.n_start_times;
+      for (auto const& s : starts) pong.add_start(s.stop, s.time_at_stop);
+      pong.execute(ping_j.dest_time, ping_j.transfers, ping_j.start_time, results);
+      auto const match = std::find_if(results.els.begin(), results.els.end(), [&](journey_t const& p) {
+        return p.transfers == ping_j.transfers && p.start_time == ping_j.dest_time;
+      });
+      if (match == results.els.end()) throw std::runtime_error{"no pong"};
+      if (!match->reconstructed && !match->error) {
+        reconstructor rc{tt, qf, pong, *match, !fwd, pong.base_days(), base_idx, !q.is_interval};
+        rc.run();
+      }
+      ping_j.start_time = match->dest_time;
+    }
+
+    // next start time
+    auto const first_it = std::min_element(
+        ping_results.els.begin(), ping_results.els.end(),
+        [&](journey_t const& a, journey_t const& b) { return is_better(a.start_time, b.start_time); });
+    auto const next = first_it->start_time + (fwd ? 1 : -1);
+    if (!is_better(start_time, next)) throw std::runtime_error{"no pong progress"};
+    start_time = next;
+  }
+
+  std::erase_if(results.els, [&](journey_t const& j) {
+    auto const j_start = j.dest_time;
+    auto const out_of_interval =
+        fwd ? !q.extend_later && j_start >= search_interval.to
+            : !q.extend_earlier && j_start < search_interval.from;
+    return !j.reconstructed || !is_validated(j) || out_of_interval ||
+           j.travel_time() >= fastest_direct || j.travel_time() > q.max_travel_time;
+  });
+  for (auto& j : results.els) std::swap(j.start_time, j.dest_time);
+  res.interval = {fwd ? search_interval.from : start_time + 1,
+                  fwd ? start_time : search_interval.to};
+  for (auto& j : results.els) {
+    auto const swap = [](uint32_t l) { return l == kStart ? kEnd : l == kEnd ? kStart : l; };
+    j.legs.front().from = swap(j.legs.front().from);
+    j.legs.back().to = swap(j.legs.back().to);
+  }
+  std::sort(results.els.begin(), results.els.end(), [](journey_t const& a, journey_t const& b) {
+    return std::tie(a.start_time, a.transfers) < std::tie(b.start_time, b.transfers);
+  });
+  if (fwd) {  // pong.cc:433-472: earlier alternatives for inner rides
+    for (auto& j : results.els) {
+      for (auto w = size_t{0}; w + 5U <= j.legs.size(); ++w) {
+        auto& l = j.legs;
+        if (l[w].kind != B2R_LEG_TRANSPORT || l[w + 2].kind != B2R_LEG_TRANSPORT ||
+            l[w + 4].kind != B2R_LEG_TRANSPORT) {
+          continue;
+        }
+        auto const& front = l[w];
+        auto const from_stop = static_cast<uint32_t>(front.stop_to - 1U);
+        auto const from = B2R_STOP_LOC(tt.stop(tt.d.transport_route[front.transport], from_stop));
+        auto const arr_time = tt.event_time(front.transport, front.day, from_stop, true);
+        auto const& back = l[w + 4];
+        auto const to = B2R_STOP_LOC(tt.stop(tt.d.transport_route[back.transport], back.stop_from));
+        auto const dep_time = tt.event_time(back.transport, back.day, back.stop_from, false);
+        auto const earlier = get_earliest_alternative(tt, q, from, to, arr_time, dep_time);
+        if (earlier.has_value()) {
+          l[w + 1] = (*earlier)[0];
+          l[w + 2] = (*earlier)[1];
+          l[w + 3] = (*earlier)[2];
+        }
+      }
+    }
+  }
+  res.journeys = std::move(results.els);
+  res.rt = pong.rt;
+  res.best = pong.best;
+  res.base_day = pong.base_days();
+}
+
 uint64_t byte_model(or_stats const& s) {
   // algorithmic bytes of the hot path (bytes the reference loop must touch):
   //  route phase: 4 B stop word + 2 B previous-round label + 2 B event per
@@ -1807,6 +2174,8 @@ int or_search(const b2r_timetable_desc* tt, const b2r_query* q, or_result** out)
       res->r.n_rows = end_k;
       res->r.ota_rows.assign(res->r.rt.begin(),
                              res->r.rt.begin() + static_cast<size_t>(end_k) * tt->n_locations);
+    } else if (qq.pong) {
+      oracle::run_pong(v, qq, fwd, res->r);
     } else {
       oracle::run_search(v, qq, fwd, res->r);
     }
@@ -1878,6 +2247,41 @@ int or_result_state(const or_result* r, const int16_t** round_times,
 }
 
 void or_result_free(or_result* r) { delete r; }
+
+// get_earliest_alternative (pong.cc:35-61) with the filters and transfer
+// time settings of q: 1 and three legs if found, 0 if not.
+int or_earliest_alternative(const b2r_timetable_desc* tt, const b2r_query* q, uint32_t from,
+                            uint32_t to, int32_t from_arr, int32_t to_dep, b2r_leg* legs) {
+  if (tt == nullptr || q == nullptr || legs == nullptr) return B2R_ERR_INVALID_ARGUMENT;
+  try {
+    oracle::tt_view const v{*tt};
+    auto const qq = oracle::to_query(*q);
+    auto const r = oracle::get_earliest_alternative(v, qq, from, to, from_arr, to_dep);
+    if (!r.has_value()) return 0;
+    for (auto i = 0U; i != 3U; ++i) {
+      auto const& l = (*r)[i];
+      b2r_leg bl{};
+      bl.from = l.from;
+      bl.to = l.to;
+      bl.dep_time = l.dep;
+      bl.arr_time = l.arr;
+      bl.kind = l.kind;
+      if (l.kind == B2R_LEG_TRANSPORT) {
+        bl.transport = l.transport;
+        bl.day = l.day;
+        bl.stop_from = l.stop_from;
+        bl.stop_to = l.stop_to;
+      } else {
+        bl.transport = l.target;
+        bl.duration = l.duration;
+      }
+      legs[i] = bl;
+    }
+    return 1;
+  } catch (std::exception const&) {
+    return B2R_ERR_INTERNAL;
+  }
+}
 
 int or_get_starts(const b2r_timetable_desc* tt, const b2r_query* q, int32_t* tas,
                   int32_t* tst, uint32_t* stop, uint32_t capacity, uint32_t* n) {

@@ -193,6 +193,8 @@ class FixtureQuery:
         qq.extend_interval_later = 1 if q.get("extend_later") else 0
         if q.get("kind") == "one_to_all":
             qq.kind = A.B2R_ONE_TO_ALL
+        if q.get("algorithm") == "pong":
+            qq.algorithm = A.B2R_ALGO_PONG
         if "claszes" in q:
             qq.allowed_claszes = q["claszes"]
         qq.require_bike_transport = 1 if q.get("bikes") else 0
@@ -231,6 +233,16 @@ def journeys_to_records(tt: FixtureTimetable, res: A.Result):
             rec["legs"].append(leg)
         out.append(rec)
     return out
+
+
+def in_window(q, records):
+    """The records whose anchor (departure forward, arrival backward) lies
+    in the query's interval -- the window in which nigiri's test harness
+    requires pong and range RAPTOR to print the same journeys
+    (test/raptor_search.cc:198-237)."""
+    lo, hi = q["interval"]
+    key = "dep" if q.get("direction", "fwd") == "fwd" else "arr"
+    return [r for r in records if lo <= r[key] < hi]
 
 
 def strip_expected(expected, names_by_trip=None):

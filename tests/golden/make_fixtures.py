@@ -307,7 +307,74 @@ def gtfs_flags_3(flag):
     }
 
 
+def gtfs_pong_lookahead():
+    """test/routing/pong_minlookahead_test.cc kTimetable: agency
+    Europe/London (UTC+1 on 2026-06-01), service MON on Mondays of
+    2026-06-01..07 (only 2026-06-01 is a Monday), stops without coordinates
+    (no footpaths), route type 2 -> kRegional (6); each trip is alone in its
+    block:
+      R0_MON (route R0) S0 05:00 -> S1 06:00   UTC 04:00 -> 05:00
+      R1_MON (route R1) S1 08:00 -> S2 10:00   UTC 07:00 -> 09:00"""
+    d = "2026-06-01"
+    services = [
+        dict(utc_service("R0", ["S0", "S1"], d, [hm("04:00"), hm("05:00")]), id="R0_MON", clasz=6),
+        dict(utc_service("R1", ["S1", "S2"], d, [hm("07:00"), hm("09:00")]), id="R1_MON", clasz=6),
+    ]
+    return {
+        "date_range": ["2026-06-01", "2026-06-07"],
+        "locations": [{"id": x, "name": x, "transfer_time": 2} for x in ["S0", "S1", "S2"]],
+        "footpaths": [],
+        "routes": group_routes(services),
+    }
+
+
+def gtfs_pong_gap():
+    """test/routing/pong_gap_truncation_test.cc test_files(): agency Etc/UTC,
+    service S on 2024-06-19, stops ~150 km apart (no footpaths), route type 2
+    -> kRegional (6):
+      PH (route PH) A 09:59 -> B 11:00
+      EA (route EA) A 10:05 -> C 10:20
+      EB (route EB) C 10:30 -> B 11:00
+      L  (route L)  A 15:00 -> B 15:30"""
+    d = "2024-06-19"
+    services = [
+        dict(utc_service("PH", ["A", "B"], d, [hm("09:59"), hm("11:00")]), id="PH", clasz=6),
+        dict(utc_service("EA", ["A", "C"], d, [hm("10:05"), hm("10:20")]), id="EA", clasz=6),
+        dict(utc_service("EB", ["C", "B"], d, [hm("10:30"), hm("11:00")]), id="EB", clasz=6),
+        dict(utc_service("L", ["A", "B"], d, [hm("15:00"), hm("15:30")]), id="L", clasz=6),
+    ]
+    return {
+        "date_range": ["2024-06-18", "2024-06-20"],
+        "locations": [{"id": x, "name": x, "transfer_time": 2} for x in "ACB"],
+        "footpaths": [],
+        "routes": group_routes(services),
+    }
+
+
+FLAG_CARS = 1
+
+
+def gtfs_alternative_block(flag, first_has):
+    """test/routing/pong_get_earliest_alternative_test.cc: agency
+    Europe/Berlin (UTC+2 on 2024-06-19), service S on 2024-06-19, one block
+    of two trips chained into one transport A 08:00 - B 08:15 - C 08:30
+    (UTC) whose sections carry `flag` as [first_has, not first_has]:
+    bikes [0, 1] (T_NO_BIKE > T_BIKE), cars [1, 0] (T_CAR > T_NO_CAR)."""
+    s = dict(utc_service("R1", list("ABC"), "2024-06-19",
+                         [hm("08:00"), hm("08:15"), hm("08:15"), hm("08:30")]), clasz=10,
+             sections=[(1 << flag) if first_has else 0, 0 if first_has else (1 << flag)])
+    return {
+        "date_range": ["2024-06-18", "2024-06-20"],
+        "locations": [{"id": x, "name": x, "transfer_time": 2} for x in "ABC"],
+        "footpaths": [],
+        "routes": group_routes([s]),
+    }
+
+
 TIMETABLES = {"hrd_abc": hrd_abc(), "gtfs_transfer_time": gtfs_transfer_time(),
+              "gtfs_pong_lookahead": gtfs_pong_lookahead(), "gtfs_pong_gap": gtfs_pong_gap(),
+              "gtfs_alternative_bikes": gtfs_alternative_block(FLAG_BIKES, False),
+              "gtfs_alternative_cars": gtfs_alternative_block(FLAG_CARS, True),
               "hrd_simple": hrd_simple(), "gtfs_dijkstra": gtfs_dijkstra(),
               "gtfs_clasz": gtfs_clasz(),
               "gtfs_bikes_1": gtfs_flags_1(FLAG_BIKES), "gtfs_bikes_2": gtfs_flags_2(FLAG_BIKES),
@@ -486,6 +553,21 @@ def cases():
                       ref="test/routing/clasz_filter_test.cc", golden=golden,
                       query=dict(start=[["A", 0, 0]], dest=[["C", 0, 0]], interval=clasz_iv,
                                  direction="fwd", claszes=mask)))
+    # test/routing/pong_minlookahead_test.cc (pong_search called directly)
+    la = dict(start=[["S0", 0, 0]], dest=[["S2", 0, 0]], direction="fwd", algorithm="pong",
+              start_mode="equivalent", dest_mode="equivalent", max_travel_time=300,
+              min_connection_count=1, extend_later=True)
+    for name, extra, golden in [
+            ("pong_ignores_interval_4h01",
+             dict(interval=[t("2026-06-01 00:00"), t("2026-06-01 04:01")]), "kJourneys"),
+            ("pong_ignores_interval_4h",
+             dict(interval=[t("2026-06-01 00:00"), t("2026-06-01 04:00")]), "kJourneys"),
+            ("pong_min_lookahead_5h", dict(start_time=t("2026-06-01 00:00")), "kJourneys"),
+            ("pong_min_lookahead_4h59",
+             dict(start_time=t("2026-06-01 00:00"), max_travel_time=299), None)]:
+        c.append(dict(name=name, timetable="gtfs_pong_lookahead",
+                      ref="test/routing/pong_minlookahead_test.cc", golden=golden,
+                      query=dict(la, **extra)))
     # test/routing/bike_transport_test.cc, no_compulsory_reservation_test.cc
     flag_iv = [t("2019-05-01 00:00"), t("2019-05-02 00:00")]
     for kind, ref, key, off, on in [
@@ -548,6 +630,31 @@ def known_answers(ref_root: str):
         ka.append(dict(name=f"dijkstra_{var}", kind="lower_bounds", timetable="gtfs_dijkstra",
                        ref="test/routing/dijkstra_test.cc", query=q,
                        expected=[[names[var], int(value)]]))
+    # pong_gap_truncation_test.cc: the departures of range RAPTOR's result
+    # (its `expected` vector: day + 10h + 5min, day + 15h); pong must not
+    # depart before the interval either (the harness's EXPECT_GE)
+    src = open(os.path.join(ref_root, "test/routing/pong_gap_truncation_test.cc")).read()
+    assert "day + 10h + 5min, day + 15h" in src
+    gq = dict(start=[["A", 0, 0]], dest=[["B", 0, 0]], direction="fwd",
+              interval=[t("2024-06-19 10:00"), t("2024-06-19 10:03")],
+              start_mode="equivalent", dest_mode="equivalent", min_connection_count=2,
+              extend_later=True)
+    ka.append(dict(name="pong_gap_truncation_range", kind="departures", timetable="gtfs_pong_gap",
+                   ref="test/routing/pong_gap_truncation_test.cc", query=gq,
+                   expected=[t("2024-06-19 10:05"), t("2024-06-19 15:00")]))
+    ka.append(dict(name="pong_gap_truncation_pong", kind="departures", timetable="gtfs_pong_gap",
+                   ref="test/routing/pong_gap_truncation_test.cc",
+                   query=dict(gq, algorithm="pong"), not_before=t("2024-06-19 10:00")))
+    # pong_get_earliest_alternative_test.cc: A -> C between 06:00 and 12:00
+    # UTC on the block transport, found without the flag, not with it
+    for tt_name, key in (("gtfs_alternative_bikes", "bikes"), ("gtfs_alternative_cars", "cars")):
+        for req in (False, True):
+            ka.append(dict(name=f"earliest_alternative_{key}_{'req' if req else 'any'}",
+                           kind="earliest_alternative", timetable=tt_name,
+                           ref="test/routing/pong_get_earliest_alternative_test.cc",
+                           query=dict(start=[["A", 0, 0]], dest=[["C", 0, 0]],
+                                      start_time=t("2024-06-19 06:00"), **({key: True} if req else {})),
+                           to_dep=t("2024-06-19 12:00"), expected=not req))
     return ka
 
 

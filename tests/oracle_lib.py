@@ -44,6 +44,9 @@ def lib():
         L.or_run_many.argtypes = [C.POINTER(A.TimetableDesc), C.POINTER(A.Query), C.c_uint32,
                                   C.c_uint32, C.POINTER(C.c_double), C.POINTER(C.c_uint64),
                                   C.POINTER(C.c_double)]
+        L.or_earliest_alternative.argtypes = [C.POINTER(A.TimetableDesc), C.POINTER(A.Query),
+                                              C.c_uint32, C.c_uint32, C.c_int32, C.c_int32,
+                                              C.POINTER(A.Leg)]
         _lib = L
     return _lib
 

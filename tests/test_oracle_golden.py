@@ -25,6 +25,29 @@ def test_oracle_matches_golden(case, timetables):
     assert F.journeys_to_records(tt, r.view) == F.strip_expected(case["expected"])
 
 
+INTERVAL_CASES = [c for c in CASES["cases"] if "interval" in c["query"]]
+
+
+@pytest.mark.parametrize("case", INTERVAL_CASES, ids=[c["name"] for c in INTERVAL_CASES])
+def test_oracle_pong_matches_golden_in_window(case, timetables):
+    """pong_search against the same golden printouts: inside the query's
+    interval its journeys print exactly as range RAPTOR's, and outside it
+    they respect the interval-extension flags (test/raptor_search.cc:198-237
+    runs every interval query of nigiri's tests this way)."""
+    tt = timetables[case["timetable"]]
+    qd = dict(case["query"], algorithm="pong")
+    q = F.FixtureQuery(A.lib(), tt, qd)
+    r = oracle_lib.OracleResult(tt.desc, q.q)
+    got = F.journeys_to_records(tt, r.view)
+    lo, hi = qd["interval"]
+    key = "dep" if qd.get("direction", "fwd") == "fwd" else "arr"
+    if not qd.get("extend_earlier"):
+        assert all(j[key] >= lo for j in got)
+    if not qd.get("extend_later"):
+        assert all(j[key] < hi for j in got)
+    assert F.in_window(qd, got) == F.in_window(qd, F.strip_expected(case["expected"]))
+
+
 def test_golden_cases_cover_both_directions_and_intermodal():
     names = [c["name"] for c in CASES["cases"]]
     assert any("backward" in n or n.endswith("_bwd") for n in names)
@@ -56,6 +79,22 @@ def test_oracle_known_answers(ka, timetables):
         # stop), duplicates removed
         got = sorted({(tas[i], tst[i], stop[i]) for i in range(n.value)}, reverse=True)
         assert [[a, b, name[s]] for a, b, s in got] == ka["expected"]
+    elif ka["kind"] == "departures":
+        r = oracle_lib.OracleResult(tt.desc, q.q)
+        deps = sorted(j["dep"] for j in F.journeys_to_records(tt, r.view))
+        if "expected" in ka:
+            assert deps == ka["expected"]
+        if "not_before" in ka:
+            assert all(d >= ka["not_before"] for d in deps)
+    elif ka["kind"] == "earliest_alternative":
+        legs = (A.Leg * 3)()
+        qq = q.q
+        rc = L.or_earliest_alternative(C.byref(tt.desc), C.byref(qq), tt.loc_idx["A"],
+                                       tt.loc_idx["C"], qq.start_time, ka["to_dep"], legs)
+        assert rc == (1 if ka["expected"] else 0)
+        if rc == 1:
+            assert [legs[i].kind for i in range(3)] == [A.B2R_LEG_FOOTPATH, A.B2R_LEG_TRANSPORT,
+                                                       A.B2R_LEG_FOOTPATH]
     else:
         dists = (C.c_uint16 * tt.desc.n_locations)()
         assert L.or_lower_bounds(C.byref(tt.desc), C.byref(q.q), dists) == 0
