@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "b2r.h"
+#include "direct.h"
 #include "engine.cuh"
 #include "errors.h"
 #include "kernels.cuh"
@@ -176,14 +177,23 @@ struct b2r_engine {
 namespace b2r {
 namespace {
 
+// admission flags: the previous phase's rounds 0..n-1 folded into pong
+// bounds (raptor.h:117-170), round times and time_at_dest kept (a pong
+// after the first of its iteration), destination bits of the previous
+// phase cleared (the slot changes phase without retiring)
+constexpr uint32_t kAdmFillRows = 0xFFu;
+constexpr uint32_t kAdmKeepRt = 1u << 8;
+constexpr uint32_t kAdmRephase = 1u << 9;
+
 struct adm_hdr {
   uint32_t slot;
   uint32_t n_starts, n_dest, n_off;
   uint32_t clear_rt;
   uint32_t lb_mode;  // 0 zeros, 1 column in payload, 2 solved on the device, 3 from the table
   uint32_t n_seeds;
-  uint32_t pad;
-  uint64_t off_slot, off_starts, off_dest, off_off, off_lb, off_seeds;
+  uint32_t flags;
+  uint32_t n_keep, pad;
+  uint64_t off_slot, off_starts, off_dest, off_off, off_lb, off_seeds, off_keep;
 };
 
 __global__ void k_admit(dev::state st, adm_hdr const* hdr, uint8_t const* payload, uint32_t n_adm,
@@ -193,9 +203,39 @@ __global__ void k_admit(dev::state st, adm_hdr const* hdr, uint8_t const* payloa
   auto const h = hdr[a];
   auto const s = h.slot;
   auto const n_loc = st.tt.n_loc;
+  auto const fill_rows = h.flags & kAdmFillRows;
+  __shared__ int16_t old_tad[dev::kK];
+  if (h.flags != 0u) {  // the slot's previous phase, read before it is overwritten
+    auto const& old = st.slots[s];
+    if ((h.flags & kAdmKeepRt) != 0u && threadIdx.x < dev::kK) old_tad[threadIdx.x] = old.tad[threadIdx.x];
+    if ((h.flags & kAdmRephase) != 0u && !old.intermodal_dest && !old.one_to_all) {
+      for (auto i = threadIdx.x; i < old.n_dest; i += blockDim.x) {
+        atomicAnd(&st.D[st.dest_pool[old.dest_off + i].loc * st.G + (s >> 5)], ~(1u << (s & 31)));
+      }
+    }
+    if (fill_rows != 0u) {
+      // fill_bounds: row k = best of rounds 0..k of the previous (ping)
+      // search, stored as a key of the flipped (pong) search
+      auto const oq = dev::tagcode(old.gen_query);
+      auto const ofwd = old.fwd != 0;
+      for (auto l = threadIdx.x; l < n_loc; l += blockDim.x) {
+        int best = dev::kKeyInv;
+        for (auto k = 0u; k != fill_rows; ++k) {
+          auto const at = (static_cast<size_t>(k) * n_loc + l) * st.S + s;
+          auto const key = dev::dec(st.rt[at], oq);
+          if (key < best) best = key;
+          st.bounds[at] = static_cast<int16_t>(dev::to_key(!ofwd, dev::from_key(ofwd, best)));
+        }
+      }
+    }
+    __syncthreads();
+  }
   if (threadIdx.x == 0) {
     auto sl = *reinterpret_cast<dev::slot_t const*>(payload + h.off_slot);
     sl.gen_group = st.slots[s].gen_group;  // start-time generations persist
+    if ((h.flags & kAdmKeepRt) != 0u) {
+      for (auto i = 0; i != dev::kK; ++i) sl.tad[i] = old_tad[i];
+    }
     sl.starts_off = s * max_starts;
     sl.dest_off = s * max_dest;
     sl.soff_off = s * max_off;
@@ -223,6 +263,14 @@ __global__ void k_admit(dev::state st, adm_hdr const* hdr, uint8_t const* payloa
   auto const words = (st.max_j + 31u) / 32u;
   for (auto i = threadIdx.x; i < words; i += blockDim.x) st.blocks_used[s * words + i] = 0u;
   __syncthreads();
+  if (h.n_keep != 0u && threadIdx.x == 0) {  // a pong's shared result set (pong.cc:322-326)
+    auto const* keep = reinterpret_cast<dev::journey_rec const*>(payload + h.off_keep);
+    auto* els = st.journeys + static_cast<size_t>(s) * st.max_j;
+    for (auto i = 0u; i != h.n_keep; ++i) {
+      els[i] = keep[i];
+      st.blocks_used[s * words + keep[i].block / 32u] |= 1u << (keep[i].block % 32u);
+    }
+  }
   if (h.lb_mode == 2) {  // Dijkstra seeds into the device frontier
     auto const qtag = dev::tagcode(st.slots[s].gen_query);
     auto const* seeds = reinterpret_cast<uint32_t const*>(payload + h.off_seeds);
@@ -455,7 +503,9 @@ int check_capacity(b2r_engine const& e, prepped_query const& p) {
   return B2R_OK;
 }
 
-slot_t make_slot(b2r_engine& e, uint32_t s, prepped_query const& p, bool& clear_rt) {
+// new_gen: a new query generation (raptor::reset_arrivals); otherwise the
+// round times of the slot's previous phase stay in effect
+slot_t make_slot(b2r_engine& e, uint32_t s, prepped_query const& p, bool& clear_rt, bool new_gen = true) {
   slot_t sl{};
   sl.state = dev::S_START;
   sl.fwd = p.fwd ? 1 : 0;
@@ -467,11 +517,14 @@ slot_t make_slot(b2r_engine& e, uint32_t s, prepped_query const& p, bool& clear_
   sl.dest_mode = p.dest_mode;
   sl.base = p.base;
   clear_rt = false;
-  if (e.gen_query[s] >= 0xFFFEu) {
-    e.gen_query[s] = 0;
-    clear_rt = true;
+  if (new_gen) {
+    if (e.gen_query[s] >= 0xFFFEu) {
+      e.gen_query[s] = 0;
+      clear_rt = true;
+    }
+    ++e.gen_query[s];
   }
-  sl.gen_query = ++e.gen_query[s];
+  sl.gen_query = e.gen_query[s];
   sl.base_days = p.base_days;
   sl.iv_from = p.iv_from;
   sl.iv_to = p.iv_to;
@@ -480,11 +533,16 @@ slot_t make_slot(b2r_engine& e, uint32_t s, prepped_query const& p, bool& clear_
   sl.min_connection_count = p.min_connection_count;
   sl.extend_earlier = p.extend_earlier ? 1 : 0;
   sl.extend_later = p.extend_later ? 1 : 0;
-  sl.need_sweep = 0;
+  sl.need_sweep = p.need_sweep ? 1 : 0;
   sl.early_term = 0;
   sl.tts = {p.tts.is_default, p.tts.min_transfer_time, p.tts.additional_time, p.tts.factor};
   sl.allowed_claszes = p.allowed_claszes;
   sl.req_flags = p.req_flags;
+  sl.blast = p.blast;
+  sl.recon_mode = p.recon_mode;
+  sl.recon_transfers = p.recon_transfers;
+  sl.recon_start = p.recon_start;
+  sl.span = p.span;
   sl.n_starts = static_cast<uint32_t>(p.starts.size());
   sl.n_dest = static_cast<uint32_t>(p.intermodal_dest ? p.dest_dist.size() : p.dest_locs.size());
   sl.n_soff = static_cast<uint32_t>(p.start_offsets.size());
@@ -570,12 +628,21 @@ void ensure_lb_table(b2r_timetable& t, unsigned threads) {
   }
 }
 
-void admit(b2r_engine& e, std::vector<std::pair<uint32_t, prepped_query const*>> const& adm,
-           cudaStream_t s) {
+// one admission: a query (or the next phase of one) into slot `slot`
+struct adm_req {
+  uint32_t slot;
+  prepped_query const* p;
+  uint32_t flags{0};                                // kAdm*
+  std::vector<dev::journey_rec> const* keep{nullptr};  // journeys the slot starts with
+};
+
+void admit(b2r_engine& e, std::vector<adm_req> const& adm, cudaStream_t s) {
   if (adm.empty()) return;
   bool any_device_lb = false;
   size_t need = adm.size() * sizeof(adm_hdr) + 256;
-  for (auto const& [slot, p] : adm) need += admission_bytes(e, *p) + 64;
+  for (auto const& r : adm) {
+    need += admission_bytes(e, *r.p) + 64 + (r.keep ? r.keep->size() * sizeof(dev::journey_rec) + 16 : 0);
+  }
   if (need > e.adm_cap) {
     B2R_CUDA(cudaStreamSynchronize(s));
     if (e.h_adm != nullptr) cudaFreeHost(e.h_adm);
@@ -596,14 +663,21 @@ void admit(b2r_engine& e, std::vector<std::pair<uint32_t, prepped_query const*>>
     return at;
   };
   for (auto i = 0U; i != adm.size(); ++i) {
-    auto const s_idx = adm[i].first;
-    auto const& p = *adm[i].second;
+    auto const s_idx = adm[i].slot;
+    auto const& p = *adm[i].p;
     auto& h = hdr[i];
     h = {};
     h.slot = s_idx;
+    h.flags = adm[i].flags;
     bool clear_rt = false;
-    auto const sl = make_slot(e, s_idx, p, clear_rt);
+    auto sl = make_slot(e, s_idx, p, clear_rt, (adm[i].flags & kAdmKeepRt) == 0u);
     h.clear_rt = clear_rt ? 1 : 0;
+    if (adm[i].keep != nullptr) {
+      if (adm[i].keep->size() > e.max_j) throw std::runtime_error("journey capacity exceeded");
+      h.n_keep = static_cast<uint32_t>(adm[i].keep->size());
+      sl.n_journeys = h.n_keep;
+      h.off_keep = put(adm[i].keep->data(), adm[i].keep->size() * sizeof(dev::journey_rec));
+    }
     h.off_slot = put(&sl, sizeof(sl));
     std::vector<dev::start_rec> starts(p.starts.size());
     for (auto j = 0U; j != p.starts.size(); ++j) {
@@ -623,7 +697,8 @@ void admit(b2r_engine& e, std::vector<std::pair<uint32_t, prepped_query const*>>
     offs.insert(offs.end(), p.dest_offsets.begin(), p.dest_offsets.end());
     h.n_off = static_cast<uint32_t>(offs.size());
     h.off_off = put(offs.data(), offs.size() * sizeof(b2r_offset));
-    h.lb_mode = !p.lb.empty() ? 1
+    h.lb_mode = p.no_lb            ? 0
+                : !p.lb.empty()      ? 1
                 : p.one_to_all       ? 0
                 : e.cfg.use_lower_bounds == 2 ? 2
                 : e.cfg.use_lower_bounds == 3 ? 3
@@ -745,6 +820,17 @@ void export_slots(b2r_engine& e, std::vector<uint32_t> const& slots,
 // ----------------------------------------------------- host finalisation
 // Per query, what search::execute does between and after the Algo calls
 // (search.h:237-336): interval extension and the final filtering.
+// pong_search's sweep (pong.cc:236-361) between device phases
+struct pong_run {
+  int32_t start_time{0};
+  std::vector<dev::journey_rec> results;  // the shared result set, pong frame
+  std::vector<b2r_leg> legs;              // kMaxLegs per result
+  std::vector<dev::journey_rec> ping;     // this iteration's ping results
+  size_t next{0};                         // ping result of the next pong
+  bool in_ping{true};
+  uint64_t n_rounds{0}, n_phases{0};
+};
+
 struct query_run {
   std::atomic<bool> ready{false};  // host preparation finished
   prepped_query p;
@@ -754,6 +840,12 @@ struct query_run {
   bool reset_arrivals{false};
   std::vector<dev::journey_rec> keep;  // journeys kept across a re-arm
   b2r_engine::result_store res;
+  // pong: sweep state and the staged next phase of the query's slot
+  std::unique_ptr<pong_run> pong;
+  prepped_query phase;
+  uint32_t adm_flags{0};
+  std::vector<dev::journey_rec> upload;
+  bool readmit{false};
 };
 
 void finish_result(b2r_engine& e, query_run& q, exported& x) {
@@ -864,6 +956,225 @@ void on_phase_done(b2r_engine& e, query_run& q, exported& x) {
   q.rearm = true;
 }
 
+// ------------------------------------------------------------------ pong
+// pong.cc:363-472 after the sweep: unfinished, unvalidated, out-of-interval
+// and too slow journeys dropped, start and destination time swapped back,
+// the special stations of the first and last leg swapped, sorted by
+// departure and transfers, and (forward) inner rides replaced by earlier
+// direct alternatives.
+void finish_pong(b2r_engine& e, query_run& q) {
+  auto const& plan = *q.p.pong;
+  auto& r = *q.pong;
+  auto const fwd = plan.fwd;
+  auto const better = [&](int32_t a, int32_t b) { return fwd ? a < b : a > b; };
+  struct item {
+    dev::journey_rec j;
+    std::vector<b2r_leg> legs;
+  };
+  std::vector<item> out;
+  for (auto i = 0U; i != r.results.size(); ++i) {
+    auto const& j = r.results[i];
+    auto const tt = std::abs(j.dest_time - j.start_time);
+    auto const out_of_iv = fwd ? !plan.extend_later && j.dest_time >= plan.iv_to
+                               : !plan.extend_earlier && j.dest_time < plan.iv_from;
+    if (!j.reconstructed || !better(j.dest_time, r.start_time) || out_of_iv || tt >= plan.fastest_direct ||
+        tt > plan.max_travel_time) {
+      continue;
+    }
+    item it{j, {}};
+    std::swap(it.j.start_time, it.j.dest_time);
+    it.legs.assign(r.legs.begin() + static_cast<std::ptrdiff_t>(i) * dev::kMaxLegs,
+                   r.legs.begin() + static_cast<std::ptrdiff_t>(i) * dev::kMaxLegs + j.n_legs);
+    auto const swap = [](uint32_t l) {
+      return l == B2R_SPECIAL_START ? B2R_SPECIAL_END : l == B2R_SPECIAL_END ? B2R_SPECIAL_START : l;
+    };
+    if (!it.legs.empty()) {
+      it.legs.front().from = swap(it.legs.front().from);
+      it.legs.back().to = swap(it.legs.back().to);
+    }
+    out.push_back(std::move(it));
+  }
+  std::sort(out.begin(), out.end(), [](item const& a, item const& b) {
+    return std::tie(a.j.start_time, a.j.transfers) < std::tie(b.j.start_time, b.j.transfers);
+  });
+  if (fwd) {
+    auto const& v = e.tt->view;
+    auto const& d = v.d;
+    auto const loc = [&](b2r_leg const& l, uint32_t s) {
+      auto const rr = d.transport_route[l.transport];
+      return B2R_STOP_LOC(d.route_stops[d.route_stop_index[rr] + s]);
+    };
+    for (auto& it : out) {
+      auto& l = it.legs;
+      for (auto w = size_t{0}; w + 5U <= l.size(); ++w) {
+        if (l[w].kind != B2R_LEG_TRANSPORT || l[w + 2].kind != B2R_LEG_TRANSPORT ||
+            l[w + 4].kind != B2R_LEG_TRANSPORT) {
+          continue;
+        }
+        std::array<b2r_leg, 3> alt;
+        if (earliest_alternative(v, plan.ping.tts, plan.ping.allowed_claszes, plan.ping.req_flags,
+                                 loc(l[w], l[w].stop_to - 1U), loc(l[w + 4], l[w + 4].stop_from),
+                                 l[w].arr_time, l[w + 4].dep_time, alt)) {
+          l[w + 1] = alt[0];
+          l[w + 2] = alt[1];
+          l[w + 3] = alt[2];
+        }
+      }
+    }
+  }
+  auto& res = q.res;
+  res.journeys.clear();
+  res.legs.clear();
+  res.rt_rows.clear();
+  for (auto const& it : out) {
+    b2r_journey bj{};
+    bj.start_time = it.j.start_time;
+    bj.dest_time = it.j.dest_time;
+    bj.dest = it.j.dest;
+    bj.transfers = it.j.transfers;
+    bj.error = it.j.error;
+    bj.n_legs = static_cast<uint16_t>(it.legs.size());
+    bj.first_leg = static_cast<uint32_t>(res.legs.size());
+    res.legs.insert(res.legs.end(), it.legs.begin(), it.legs.end());
+    res.journeys.push_back(bj);
+  }
+  res.view.status = q.status;
+  res.view.interval_from = fwd ? plan.iv_from : r.start_time + 1;
+  res.view.interval_to = fwd ? r.start_time : plan.iv_to;
+  res.view.n_rounds = r.n_rounds;
+  res.view.n_start_times = r.n_phases;
+  q.finished = true;
+}
+
+// the sweep's loop condition, pong.cc:236-239
+bool pong_continues(pong_plan const& plan, pong_run const& r) {
+  auto const better = [&](int32_t a, int32_t b) { return plan.fwd ? a < b : a > b; };
+  auto const end_time = plan.fwd ? plan.iv_to : plan.iv_from - 1;
+  uint32_t n = 0;
+  for (auto const& j : r.results) {
+    if (!better(j.dest_time, r.start_time)) continue;
+    auto const tt = std::abs(j.dest_time - j.start_time);
+    n += 1U + ((tt < plan.fastest_direct && tt <= plan.max_travel_time) ? 1U : 0U);
+  }
+  return (better(r.start_time, end_time) || n < 2U * plan.min_connection_count) &&
+         plan.ext_from <= r.start_time && r.start_time < plan.ext_to;
+}
+
+void stage_ping(b2r_engine& e, query_run& q) {
+  auto& r = *q.pong;
+  q.phase = q.p.pong->ping;
+  phase_starts(e.tt->view, q.phase, r.start_time, q.phase.starts);
+  q.adm_flags = kAdmRephase;
+  q.upload.clear();
+  r.in_ping = true;
+  q.readmit = true;
+}
+
+// the pong of ping result r.next (pong.cc:297-341): bounded by the ping's
+// round times, starting at its arrival, no worse than its departure
+void stage_pong(b2r_engine& e, query_run& q, bool first_of_iteration) {
+  auto& r = *q.pong;
+  auto const& pj = r.ping[r.next];
+  q.phase = q.p.pong->pong;
+  phase_starts(e.tt->view, q.phase, pj.dest_time, q.phase.starts);
+  q.phase.end_k = static_cast<uint8_t>(std::min<int>(pj.transfers, B2R_MAX_TRANSFERS) + 2);
+  q.phase.blast = static_cast<uint8_t>(pj.transfers + 1U);
+  q.phase.span = static_cast<int16_t>(std::abs(pj.dest_time - pj.start_time));
+  q.phase.recon_transfers = pj.transfers;
+  q.phase.recon_start = pj.dest_time;
+  q.phase.need_sweep = !first_of_iteration;
+  q.adm_flags = first_of_iteration ? (kAdmRephase | (r.ping.front().transfers + 1U)) : kAdmKeepRt;
+  q.upload = r.results;
+  r.in_ping = false;
+  q.readmit = true;
+}
+
+// a phase of a pong query finished on the device: the next phase is staged
+// (q.readmit) or the sweep ends (q.finished)
+void pong_phase_done(b2r_engine& e, query_run& q, exported& x) {
+  auto const& plan = *q.p.pong;
+  if (!q.pong) {
+    q.pong = std::make_unique<pong_run>();
+    q.pong->start_time = plan.fwd ? plan.iv_from : plan.iv_to - 1;
+  }
+  auto& r = *q.pong;
+  r.n_rounds += x.sl.n_rounds;
+  ++r.n_phases;
+  q.readmit = false;
+  if (x.sl.state == dev::S_ERROR) {
+    q.status = x.sl.error != 0 ? x.sl.error : B2R_ERR_INTERNAL;
+    finish_pong(e, q);
+    return;
+  }
+  auto const better = [&](int32_t a, int32_t b) { return plan.fwd ? a < b : a > b; };
+  auto const dominated = [&](dev::journey_rec const& j) {
+    for (auto const& o : r.results) {
+      if (dev::dominates(o, j)) return true;
+    }
+    return false;
+  };
+  if (r.in_ping) {
+    r.ping = x.js;
+    std::erase_if(r.ping, dominated);
+    if (r.ping.empty()) {  // no ping results, or all dominated (pong.cc:268-285)
+      finish_pong(e, q);
+      return;
+    }
+    std::sort(r.ping.begin(), r.ping.end(),
+              [](dev::journey_rec const& a, dev::journey_rec const& b) { return a.transfers > b.transfers; });
+    r.next = 0;
+    stage_pong(e, q, true);
+  } else {
+    r.results = x.js;
+    r.legs = std::move(x.legs);
+    auto& pj = r.ping[r.next];
+    auto const m = std::find_if(r.results.begin(), r.results.end(), [&](dev::journey_rec const& j) {
+      return j.transfers == pj.transfers && j.start_time == pj.dest_time;
+    });
+    if (m == r.results.end()) {  // "no pong" (pong.cc:328-333)
+      q.status = B2R_ERR_INTERNAL;
+      finish_pong(e, q);
+      return;
+    }
+    pj.start_time = m->dest_time;
+    if (++r.next < r.ping.size()) {
+      stage_pong(e, q, false);
+    } else {
+      auto const first = std::min_element(r.ping.begin(), r.ping.end(),
+                                          [&](dev::journey_rec const& a, dev::journey_rec const& b) {
+                                            return better(a.start_time, b.start_time);
+                                          });
+      auto const next = first->start_time + (plan.fwd ? 1 : -1);
+      if (!better(r.start_time, next)) {  // "no pong progress" (pong.cc:348-351)
+        q.status = B2R_ERR_INTERNAL;
+        finish_pong(e, q);
+        return;
+      }
+      r.start_time = next;
+      if (!pong_continues(plan, r)) {
+        finish_pong(e, q);
+        return;
+      }
+      stage_ping(e, q);
+    }
+  }
+  if (q.readmit && check_capacity(e, q.phase) != B2R_OK) {
+    q.readmit = false;
+    q.status = B2R_ERR_CAPACITY;
+    finish_pong(e, q);
+  }
+}
+
+// after an exported phase: pong queries go on to their next phase, search
+// queries to their next interval-extension phase or their result
+void phase_done(b2r_engine& e, query_run& q, exported& x) {
+  if (q.p.pong) {
+    pong_phase_done(e, q, x);
+  } else {
+    on_phase_done(e, q, x);
+  }
+}
+
 }  // namespace
 
 // ------------------------------------------------------------- the loop
@@ -943,8 +1254,19 @@ struct batch_runner {
     size_t next = 0;
     std::vector<int64_t>& slot_q = e.slot_query;
     std::fill(slot_q.begin(), slot_q.end(), -1);
+    // slots whose query's next pong phase is staged: their summaries are
+    // stale until the re-admission at the next admission point
+    std::vector<uint8_t> waiting(S, 0);
+    std::vector<uint32_t> pending;
     auto const admit_free = [&]() {
-      std::vector<std::pair<uint32_t, prepped_query const*>> adm;
+      std::vector<adm_req> adm;
+      for (auto const s : pending) {
+        auto& q = runs[static_cast<size_t>(slot_q[s])];
+        adm.push_back({s, &q.phase, q.adm_flags, &q.upload});
+        q.readmit = false;
+        waiting[s] = 0;
+      }
+      pending.clear();
       slot_picker pick{S, [&](uint32_t s) { return slot_q[s] == -1; }};
       while (next < runs.size()) {
         while (next < runs.size()) {
@@ -972,7 +1294,7 @@ struct batch_runner {
         auto const s = pick.take(sweeps(runs[next].p));
         if (s < 0) break;
         slot_q[s] = static_cast<int64_t>(next);
-        adm.emplace_back(static_cast<uint32_t>(s), &runs[next].p);
+        adm.push_back({static_cast<uint32_t>(s), &runs[next].p});
         ++next;
       }
       auto const t0 = std::chrono::steady_clock::now();
@@ -1017,7 +1339,10 @@ struct batch_runner {
     // every start-time group ends within end_k super-steps; the cap turns a
     // logic error into a reported failure instead of an endless loop
     uint64_t max_steps = 10000;
-    for (auto const& q : runs) max_steps += 40ull * (q.p.starts.size() + 2) * (q.p.end_k + 2);
+    for (auto const& q : runs) {
+      max_steps += 40ull * (q.p.starts.size() + 2) * (q.p.end_k + 2);
+      if (q.p.pong) max_steps += 40ull * 4096 * (q.p.end_k + 2);  // a sweep of many phases
+    }
     admit_free();
     while (busy()) {
       if (steps > max_steps) throw std::runtime_error("super-step cap exceeded");
@@ -1045,7 +1370,7 @@ struct batch_runner {
         if (x == kRetiring) x = -1;  // their retirement ran before this summary's chunk ended
       std::vector<uint32_t> done_slots, n_js, n_rows;
       for (uint32_t s = 0; s != S; ++s) {
-        if (slot_q[s] < 0) continue;
+        if (slot_q[s] < 0 || waiting[s]) continue;
         if (stale[s]) {
           stale[s] = 0;
           continue;
@@ -1060,10 +1385,9 @@ struct batch_runner {
       }
       admit_free();  // into free slots, queued before the next chunk
       // next chunk in flight unless every resident query has just finished
-      if (running() && (done_slots.size() < static_cast<size_t>(std::count_if(
-                                                 slot_q.begin(), slot_q.end(), [](int64_t x) { return x >= 0; })))) {
-        launch_chunk();
-      }
+      size_t n_active = 0;
+      for (uint32_t s = 0; s != S; ++s) n_active += (slot_q[s] >= 0 && !waiting[s]) ? 1U : 0U;
+      if (running() && done_slots.size() < n_active) launch_chunk();
       if (done_slots.empty()) continue;
       auto const t_exp = std::chrono::steady_clock::now();
       std::vector<exported> ex;
@@ -1075,9 +1399,12 @@ struct batch_runner {
       for (auto i = 0U; i != done_slots.size(); ++i) {
         auto const s = done_slots[i];
         auto& q = runs[static_cast<size_t>(slot_q[s])];
-        on_phase_done(e, q, ex[i]);
+        phase_done(e, q, ex[i]);
         q.res.view.latency_ms = now_ms;
-        if (q.rearm) {
+        if (q.readmit) {
+          pending.push_back(s);
+          waiting[s] = 1;
+        } else if (q.rearm) {
           rearm(e, s, q, st);
           stale[s] = in_flight ? 1 : 0;
         } else {
@@ -1170,6 +1497,7 @@ struct serve_state {
   std::deque<serve_item*> to_prepare, ready;
   std::unordered_map<uint64_t, std::unique_ptr<serve_item>> items;
   std::vector<serve_item*> slot_item;
+  std::vector<uint32_t> pending;  // slots whose pong query's next phase is staged
   uint64_t next_ticket{1};
   uint64_t unfinished{0};  // submitted, not finished
   bool stop{false};
@@ -1230,8 +1558,14 @@ struct serve_state {
     try {
       B2R_CUDA(cudaSetDevice(e.tt->device));
       while (true) {
-        std::vector<std::pair<uint32_t, prepped_query const*>> adm;
+        std::vector<adm_req> adm;
         bool any_busy = false;
+        for (auto const s : pending) {  // pong phases staged by the last export
+          auto& run = slot_item[s]->run;
+          adm.push_back({s, &run.phase, run.adm_flags, &run.upload});
+          run.readmit = false;
+        }
+        pending.clear();
         {
           std::unique_lock<std::mutex> lock{mu};
           auto const has_busy = [&] {
@@ -1270,7 +1604,7 @@ struct serve_state {
             if (s < 0) break;
             ready.pop_front();
             slot_item[s] = it;
-            adm.emplace_back(static_cast<uint32_t>(s), &it->run.p);
+            adm.push_back({static_cast<uint32_t>(s), &it->run.p});
           }
           any_busy = has_busy();
         }
@@ -1304,7 +1638,11 @@ struct serve_state {
         for (auto i = 0U; i != done_slots.size(); ++i) {
           auto const s = done_slots[i];
           auto& it = *slot_item[s];
-          on_phase_done(e, it.run, ex[i]);
+          phase_done(e, it.run, ex[i]);
+          if (it.run.readmit) {
+            pending.push_back(s);
+            continue;
+          }
           if (it.run.rearm) {
             rearm(e, s, it.run, st);
             continue;
@@ -1411,9 +1749,18 @@ int b2r_timetable_upload(const b2r_timetable_desc* d, int device, b2r_timetable*
       v.lb_bwd_index = t->lb_bwd_index.data();
       v.lb_bwd = t->lb_bwd.data();
       v.importance = nullptr;
-      v.route_clasz = nullptr;  // the host preparation does not filter routes
-      v.route_flags = nullptr;
-      v.route_section_flags = nullptr;
+      // route filters on the host: pong's direct alternatives
+      t->route_clasz.assign(nr, 10U);
+      if (d->route_clasz != nullptr) t->route_clasz.assign(d->route_clasz, d->route_clasz + nr);
+      t->route_flags.assign(nr, 0U);
+      if (d->route_flags != nullptr) t->route_flags.assign(d->route_flags, d->route_flags + nr);
+      t->route_section_flags.assign(d->route_stop_index[nr], 0U);
+      if (d->route_section_flags != nullptr) {
+        t->route_section_flags.assign(d->route_section_flags, d->route_section_flags + d->route_stop_index[nr]);
+      }
+      v.route_clasz = t->route_clasz.data();
+      v.route_flags = t->route_flags.data();
+      v.route_section_flags = t->route_section_flags.data();
 
       // route filter words: class | all-sections flags << 4 | some << 8
       std::vector<uint16_t> rfilter(nr, 10U);  // no classes given: bus
@@ -1559,7 +1906,7 @@ int b2r_engine_create(b2r_timetable* tt, const b2r_engine_config* cfg_in, b2r_en
         }
       }
       auto const nl = tt->d.n_loc;
-      e->bytes_per_slot = static_cast<uint64_t>(nl) * (b2r::dev::kK * 4 + 4 + 4 + 2 + 4) +
+      e->bytes_per_slot = static_cast<uint64_t>(nl) * (b2r::dev::kK * (4 + 2) + 4 + 4 + 2 + 4) +
                           static_cast<uint64_t>(e->max_j) *
                               (sizeof(b2r::dev::journey_rec) + b2r::dev::kMaxLegs * sizeof(b2r_leg)) +
                           e->max_starts * sizeof(b2r::dev::start_rec) +
@@ -1589,6 +1936,7 @@ int b2r_engine_create(b2r_timetable* tt, const b2r_engine_config* cfg_in, b2r_en
       al(st.slots, S);
       al(st.lanes, S);
       al(st.rt, static_cast<size_t>(b2r::dev::kK) * nl * S);
+      al(st.bounds, static_cast<size_t>(b2r::dev::kK) * nl * S);
       al(st.best, static_cast<size_t>(nl) * S);
       al(st.tmp, static_cast<size_t>(nl) * S);
       al(st.lb, static_cast<size_t>(nl) * S);

@@ -124,7 +124,12 @@ struct slot_t {
   uint8_t extend_earlier, extend_later, need_sweep, early_term;
   uint16_t allowed_claszes;  // bit c: transport class c allowed
   uint8_t req_flags;         // bit f: route flag f required
-  uint8_t pad_f;
+  uint8_t blast;             // bounds_last_k_ of a pong phase (raptor.h:172); 0: unbounded
+  uint8_t recon_mode;        // 0: new journeys of the interval, 1: only the journey
+                             // (recon_transfers, recon_start), 2: none
+  uint8_t recon_transfers;
+  int16_t span;              // worst time at destination = group start + dir(span)
+  int32_t recon_start;
   tts_t tts;
   uint32_t starts_off, n_starts;  // start pool
   uint32_t dest_off, n_dest;      // dest pool (loc, dist)
@@ -155,7 +160,7 @@ struct __align__(16) lane_t {
   uint8_t mode;  // bit0 intermodal dest, bit1 has dests, bit2 tts default
   uint16_t claszes;  // allowed transport classes
   uint8_t req;       // required route flags
-  uint8_t pad;
+  uint8_t blast;     // pong bounds: last round (0: none)
 };
 
 struct start_rec {
@@ -219,6 +224,9 @@ struct state {
   // all-pairs lower-bound tables (forward / backward search), or null
   uint16_t const* lb_table_fwd;
   uint16_t const* lb_table_bwd;
+  // pong bounds (raptor_state::bounds_storage_): rows of the ping's round
+  // times folded over the rounds, as keys of the bounded (pong) search
+  int16_t* bounds;  // [K][n_loc][S]
 };
 
 // ------------------------------------------------------------- helpers
@@ -277,6 +285,16 @@ __device__ __forceinline__ T adjusted(tts_t const& s, T d) {
   auto const prod = static_cast<T>(__float2int_rz(__fmul_rn(static_cast<float>(d), s.factor)));
   auto const mn = static_cast<T>(s.min_transfer_time);
   return static_cast<T>(static_cast<T>(s.additional_time) + (prod > mn ? prod : mn));
+}
+
+// within_bounds, raptor.h:458-489 (no vias): a label `key` at l in round k
+// of a bounded search may not be better than the bounding search's row
+// (blast - k) at l plus l's transfer time.
+__device__ __forceinline__ bool within_bounds(state const& st, uint32_t s, uint32_t blast, uint32_t k,
+                                              uint32_t l, int key) {
+  if (blast == 0u) return true;
+  auto const row = static_cast<int>(st.bounds[(static_cast<size_t>(blast - k) * st.tt.n_loc + l) * st.S + s]);
+  return key <= row + adjusted<int>(st.slots[s].tts, static_cast<int>(st.tt.transfer_time[l]));
 }
 
 // to_delta(day, mam) of raptor.h:1467-1469, as a key

@@ -120,6 +120,7 @@ __global__ void k_ctl_begin(state st) {
     ln.tad_k = sl.tad[sl.k];
     ln.claszes = sl.allowed_claszes;
     ln.req = sl.req_flags;
+    ln.blast = sl.blast;
     atomicOr(&st.run_mask[s >> 5], 1u << (s & 31));
     if (sl.need_sweep) atomicOr(&st.sweep_mask[s >> 5], 1u << (s & 31));
     ++sl.n_rounds;
@@ -306,7 +307,8 @@ __global__ void __launch_bounds__(256, 3) k_route_scan(state st) {
         if (et_valid && can_finish) {
           arrival_ran = true;
           auto const by = to_delta_key(fwd, et_day, ln.base, delta_count(ev));
-          if (by <= ln.tad_k && lbv != 0xFFFFu && by + static_cast<int>(lbv) <= ln.tad_k) {
+          if (by <= ln.tad_k && lbv != 0xFFFFu && by + static_cast<int>(lbv) <= ln.tad_k &&
+              (ln.blast == 0u || within_bounds(st, s, ln.blast, k, l, by))) {
             auto const word = enc(ln.gtag, by);
             auto* tp = &st.tmp[li(st, l, s)];
             if (st.profile) {
@@ -423,11 +425,12 @@ __global__ void k_transfers_pre(state st) {
     auto const fp = key_add(tk, 0);
     auto const bk = dec(st.best[li(st, d, s)], ln.gtag);
     auto& rtw = st.rt[rti(st, k, d, s)];
-    if (fp < bk && fp < dec(rtw, ln.qtag)) rtw = enc(ln.qtag, fp);
+    if (ln.blast == 0u && fp < bk && fp < dec(rtw, ln.qtag)) rtw = enc(ln.qtag, fp);
     auto const tad = static_cast<int>(sl.tad[k]);
     if (fp < bk && fp <= tad) {
       auto const lbv = st.lb[li(st, d, s)];
       if (lbv == 0xFFFFu || fp + static_cast<int>(lbv) > tad) continue;
+      if (!within_bounds(st, s, ln.blast, k, d, fp)) continue;
       rtw = enc(ln.qtag, fp);
       st.best[li(st, d, s)] = enc(ln.gtag, fp);
       atomicOr(&st.X[d * st.G + g], bit);  // listed by k_list_marked
@@ -470,11 +473,12 @@ __global__ void k_transfers(state st) {
         auto const fp = key_add(tk, tt);
         auto const bk = dec(st.best[li(st, l, s)], ln.gtag);
         auto& rtw = st.rt[rti(st, ln.k, l, s)];
-        if (fp < bk && fp < dec(rtw, ln.qtag)) rtw = enc(ln.qtag, fp);
+        if (ln.blast == 0u && fp < bk && fp < dec(rtw, ln.qtag)) rtw = enc(ln.qtag, fp);
         auto const tad = (ln.mode & 2u) ? tad_at(st, s, l, 0u) : static_cast<int>(st.tad_phase[s]);
         if (fp < bk && fp <= tad) {
           auto const lbv = st.lb[li(st, l, s)];
-          if (lbv != 0xFFFFu && fp + static_cast<int>(lbv) <= tad) {
+          if (lbv != 0xFFFFu && fp + static_cast<int>(lbv) <= tad &&
+              within_bounds(st, s, ln.blast, ln.k, l, fp)) {
             rtw = enc(ln.qtag, fp);
             st.best[li(st, l, s)] = enc(ln.gtag, fp);
             atomicOr(&st.X[e], 1u << b);  // listed by k_list_marked
@@ -570,11 +574,12 @@ __global__ void k_footpaths_pre(state st) {
     auto const fp = c[a].key;
     auto const bk = dec(st.best[li(st, d, s)], ln.gtag);
     auto& rtw = st.rt[rti(st, k, d, s)];
-    if (fp < bk && fp < dec(rtw, ln.qtag)) rtw = enc(ln.qtag, fp);
+    if (ln.blast == 0u && fp < bk && fp < dec(rtw, ln.qtag)) rtw = enc(ln.qtag, fp);
     auto const tad = static_cast<int>(sl.tad[k]);
     if (fp < bk && fp <= tad) {
       auto const lbv = st.lb[li(st, d, s)];
       if (lbv == 0xFFFFu || fp + static_cast<int>(lbv) > tad) continue;
+      if (!within_bounds(st, s, ln.blast, k, d, fp)) continue;
       rtw = enc(ln.qtag, fp);
       st.best[li(st, d, s)] = enc(ln.gtag, fp);
       atomicOr(&st.X[d * st.G + g], bit);  // listed by k_list_marked
@@ -617,11 +622,17 @@ __global__ void k_footpaths(state st) {
           auto const key = key_add(tk, adjusted<int>(slp->tts, static_cast<int>(B2R_FP_DURATION(fp))));
           auto const bk = dec(st.best[li(st, tgt, s)], ln.gtag);
           if (key >= bk) continue;
-          atomicMin(&st.rt[rti(st, ln.k, tgt, s)], enc(ln.qtag, key));
+          // the reference writes round_times ahead of its pruning only when
+          // unbounded (raptor.h:790-794)
+          if (ln.blast == 0u) atomicMin(&st.rt[rti(st, ln.k, tgt, s)], enc(ln.qtag, key));
           auto const tad = (ln.mode & 2u) ? tad_at(st, s, src, j) : tad_flat;
           if (key > tad) continue;
           auto const lbv = st.lb[li(st, tgt, s)];
           if (lbv != 0xFFFFu && key + static_cast<int>(lbv) <= tad) {
+            if (ln.blast != 0u) {
+              if (!within_bounds(st, s, ln.blast, ln.k, tgt, key)) continue;
+              atomicMin(&st.rt[rti(st, ln.k, tgt, s)], enc(ln.qtag, key));
+            }
             atomicMin(&st.best[li(st, tgt, s)], enc(ln.gtag, key));
             atomicOr(&st.X[tgt * st.G + g], 1u << b);  // listed by k_list_marked
           }
@@ -639,7 +650,7 @@ __global__ void k_ctl_end(state st) {
   if (sl.k >= sl.end_k) sl.state = S_COLLECT;
 }
 
-__device__ bool dominates(journey_rec const& a, journey_rec const& b) {  // journey.h:84-92
+__host__ __device__ inline bool dominates(journey_rec const& a, journey_rec const& b) {  // journey.h:84-92
   if (a.start_time <= a.dest_time) {
     return a.transfers <= b.transfers && a.start_time >= b.start_time && a.dest_time <= b.dest_time;
   }
@@ -718,9 +729,12 @@ __global__ void k_collect(state st) {
   for (auto i = 0u; i != sl.n_journeys; ++i) {
     auto const& j = els[i];
     auto const tt = j.dest_time > j.start_time ? j.dest_time - j.start_time : j.start_time - j.dest_time;
-    if (!j.reconstructed && !j.error &&
-        (sl.ontrip || (sl.iv_from <= j.start_time && j.start_time < sl.iv_to)) &&
-        tt < sl.fastest_direct) {
+    auto const want =
+        sl.recon_mode == 0 ? ((sl.ontrip || (sl.iv_from <= j.start_time && j.start_time < sl.iv_to)) &&
+                              tt < sl.fastest_direct)
+        : sl.recon_mode == 1 ? (j.transfers == sl.recon_transfers && j.start_time == sl.recon_start)  // pong.cc:322-339
+                             : false;
+    if (!j.reconstructed && !j.error && want) {
       st.recon_list[atomicAdd(&st.counters[C_RECON], 1u)] = (s << 16) | i;
     }
   }
@@ -823,9 +837,7 @@ __global__ void k_next(state st) {
     if (key < dec(rw, qtag)) rw = enc(qtag, key);
     atomicOr(&st.X[l * st.G + g], bit);  // listed by k_list_marked
   }
-  auto const span = sl.one_to_all ? static_cast<int>(sl.max_travel_time)
-                                  : (min(static_cast<int>(sl.fastest_direct), static_cast<int>(sl.max_travel_time)) + 1);
-  auto const worst = tas + (fwd ? span : -span);
+  auto const worst = tas + (fwd ? static_cast<int>(sl.span) : -static_cast<int>(sl.span));
   auto const d_worst = to_key(fwd, clamp16(worst - sl.base_days * 1440));
   for (auto i = 0; i != kK; ++i) {
     if (d_worst < sl.tad[i]) sl.tad[i] = static_cast<int16_t>(d_worst);

@@ -365,7 +365,150 @@ void sort_starts(bool fwd, std::vector<start_label>& s) {  // search.h:408-410
 
 }  // namespace
 
+// destination sets of a search: distances of intermodal offsets, or the
+// matching locations of station offsets (collect_destinations,
+// start_times.cc:321-353)
+void collect_dests(view const& v, prepped_query& p) {
+  p.intermodal_dest = p.dest_mode == B2R_MATCH_INTERMODAL;
+  if (p.intermodal_dest) {
+    std::map<uint32_t, uint16_t> dd;
+    for (auto const& o : p.dest_offsets) {
+      v.metas(B2R_MATCH_INTERMODAL, o.target, [&](uint32_t l) {
+        auto it = dd.find(l);
+        auto const val = static_cast<uint16_t>(o.duration);
+        if (it == dd.end()) dd.emplace(l, val);
+        else it->second = std::min(it->second, val);
+      });
+    }
+    for (auto const& [l, x] : dd) {
+      if (x != kUnreach) p.dest_dist.emplace_back(l, x);
+    }
+  } else {
+    for (auto const& o : p.dest_offsets) {
+      v.metas(p.dest_mode, o.target, [&](uint32_t l) { p.dest_locs.push_back(l); });
+    }
+    std::sort(p.dest_locs.begin(), p.dest_locs.end());
+    p.dest_locs.erase(std::unique(p.dest_locs.begin(), p.dest_locs.end()), p.dest_locs.end());
+  }
+}
+
+// pong_search, pong.cc:63-230: the sanitised query, its fastest direct
+// connection and base day, and the templates of the ping (the query's
+// direction, with the Dijkstra lower bounds) and of the pong (flipped,
+// without lower bounds: kPruneWithPingBounds).  Transfer time settings stay
+// as given: pong hands q.transfer_time_settings_ to both searches without
+// search::init's normalisation.
+void prepare_pong(host_view const& hv, b2r_query const& q, int lb_mode, prepped_query& out) {
+  view const v{hv.d};
+  out = prepped_query{};
+  if (q.kind != B2R_ONE_TO_ONE || (q.start_match_mode == B2R_MATCH_INTERMODAL && q.use_start_footpaths != 0)) {
+    out.status = B2R_ERR_INVALID_ARGUMENT;  // query::sanitize's verify (query.cc:59-62)
+    return;
+  }
+  auto plan = std::make_shared<pong_plan>();
+  auto const fwd = q.direction == B2R_FORWARD;
+  std::vector<b2r_offset> so(q.start, q.start + q.n_start), de(q.destination, q.destination + q.n_destination);
+  for (auto const* offs : {&so, &de}) {
+    for (auto const& o : *offs) {
+      if (o.target >= hv.d.n_locations) {
+        out.status = B2R_ERR_INVALID_ARGUMENT;
+        return;
+      }
+    }
+  }
+  auto const by_dur = [](b2r_offset const& a, b2r_offset const& b) { return a.duration < b.duration; };
+  std::sort(so.begin(), so.end(), by_dur);
+  std::sort(de.begin(), de.end(), by_dur);
+  tts_norm const raw{q.tts_default, q.tts_min_transfer_time, q.tts_additional_time, q.tts_factor};
+  auto const mtt = (q.max_travel_time < 0 || q.max_travel_time > B2R_MAX_TRAVEL_TIME_MIN)
+                       ? static_cast<int16_t>(B2R_MAX_TRAVEL_TIME_MIN)
+                       : q.max_travel_time;
+  auto const iv_from = q.is_interval != 0 ? q.interval_from : q.start_time;
+  auto const iv_to = q.is_interval != 0 ? q.interval_to : q.start_time;
+  auto const mid = static_cast<int64_t>(iv_from) + (iv_to - iv_from) / 2;
+  auto const base = static_cast<uint16_t>(round_to_days(mid) - hv.internal_from_days());
+  auto const fdirect = fastest_direct(v, q, so, de, raw, fwd);
+
+  auto const tmpl = [&](bool dir, uint8_t smode, uint8_t dmode, std::vector<b2r_offset> const& st,
+                        std::vector<b2r_offset> const& dt, prepped_query& t) {
+    t.fwd = dir;
+    t.one_to_all = false;
+    t.ontrip = q.is_interval == 0;
+    t.start_mode = smode;
+    t.dest_mode = dmode;
+    t.max_transfers = q.max_transfers;
+    t.max_start_offset_ = q.max_start_offset;
+    t.end_k = static_cast<uint8_t>(std::min<int>(q.max_transfers, B2R_MAX_TRANSFERS) + 2);
+    t.allowed_claszes = static_cast<uint16_t>(q.allowed_claszes & 0xFFFFU);
+    t.req_flags = static_cast<uint8_t>(
+        (q.require_bike_transport != 0 ? 1U << B2R_FLAG_BIKES : 0U) |
+        (q.require_car_transport != 0 ? 1U << B2R_FLAG_CARS : 0U) |
+        (q.no_compulsory_reservation != 0 ? 1U << B2R_FLAG_RESERVATION_NOT_REQUIRED : 0U));
+    t.start_offsets = st;
+    t.dest_offsets = dt;
+    t.tts_raw = raw;
+    t.tts = raw;
+    t.max_travel_time = mtt;
+    t.fastest_direct = fdirect;
+    t.base = base;
+    t.base_days = hv.internal_from_days() + base;
+    t.iv_from = iv_from;
+    t.iv_to = iv_to;
+    collect_dests(v, t);
+  };
+  auto& ping = plan->ping;
+  tmpl(fwd, q.start_match_mode, q.dest_match_mode, so, de, ping);
+  if (lb_mode == 1) lower_bounds(v, ping, ping.lb);
+  if (lb_mode == 2 || lb_mode == 3) lb_seeds(v, ping, ping.lb_seeds);
+  ping.use_start_footpaths = q.use_start_footpaths != 0;
+  ping.span = static_cast<int16_t>(std::min<int>(mtt + 1440, B2R_MAX_TRAVEL_TIME_MIN));  // kMinLookAhead
+  ping.recon_mode = 2;
+  auto& pong = plan->pong;
+  tmpl(!fwd, q.dest_match_mode, q.start_match_mode, de, so, pong);
+  pong.no_lb = true;
+  pong.use_start_footpaths = q.dest_match_mode != B2R_MATCH_INTERMODAL;  // pong.cc:291-295
+  pong.recon_mode = 1;
+  plan->iv_from = iv_from;
+  plan->iv_to = iv_to;
+  plan->ext_from = hv.d.date_range_from * 1440;
+  plan->ext_to = hv.d.date_range_to * 1440;
+  plan->fastest_direct = fdirect;
+  plan->max_travel_time = mtt;
+  plan->max_transfers = q.max_transfers;
+  plan->min_connection_count = q.min_connection_count;
+  plan->fwd = fwd;
+  plan->extend_earlier = q.extend_interval_earlier != 0;
+  plan->extend_later = q.extend_interval_later != 0;
+
+  // the first ping, at the first start time of the sweep
+  out = ping;
+  auto const t0 = fwd ? iv_from : iv_to - 1;
+  if (!(plan->ext_from <= t0 && t0 < plan->ext_to)) {  // pong.cc:243: no iteration at all
+    out.empty_result = true;
+    out.iv_from = fwd ? iv_from : t0 + 1;
+    out.iv_to = fwd ? t0 : iv_to;
+  } else {
+    collect_starts(v, out, false, t0, 0, 0, out.use_start_footpaths, false, out.starts);
+  }
+  out.pong = std::move(plan);
+}
+
+void phase_starts(host_view const& hv, prepped_query const& tmpl, int32_t t, std::vector<start_label>& out) {
+  view const v{hv.d};
+  out.clear();
+  collect_starts(v, tmpl, false, t, 0, 0, tmpl.use_start_footpaths, false, out);
+}
+
 void prepare(host_view const& hv, b2r_query const& q, int lb_mode, prepped_query& p) {
+  if (q.algorithm == B2R_ALGO_PONG) {
+    prepare_pong(hv, q, lb_mode, p);
+    return;
+  }
+  if (q.algorithm != B2R_ALGO_RAPTOR) {
+    p = prepped_query{};
+    p.status = B2R_ERR_INVALID_ARGUMENT;
+    return;
+  }
   view const v{hv.d};
   p = prepped_query{};
   p.fwd = q.direction == B2R_FORWARD;
@@ -414,6 +557,7 @@ void prepare(host_view const& hv, b2r_query const& q, int lb_mode, prepped_query
       });
     }
     p.lb.clear();  // one_to_all runs without lower bounds (lb = 0)
+    p.span = p.max_travel_time;  // one_to_all.cc:44-46
     return;
   }
 
@@ -434,27 +578,8 @@ void prepare(host_view const& hv, b2r_query const& q, int lb_mode, prepped_query
   p.tts.min_transfer_time = std::max<int16_t>(p.tts_raw.min_transfer_time, 0);
   p.tts.additional_time = std::max<int16_t>(p.tts_raw.additional_time, 0);
   p.tts.is_default = p.tts.factor == 1.0F && p.tts.min_transfer_time == 0 && p.tts.additional_time == 0;
-  p.intermodal_dest = p.dest_mode == B2R_MATCH_INTERMODAL;
-  if (p.intermodal_dest) {
-    std::map<uint32_t, uint16_t> dd;
-    for (auto const& o : p.dest_offsets) {
-      v.metas(B2R_MATCH_INTERMODAL, o.target, [&](uint32_t l) {
-        auto it = dd.find(l);
-        auto const val = static_cast<uint16_t>(o.duration);
-        if (it == dd.end()) dd.emplace(l, val);
-        else it->second = std::min(it->second, val);
-      });
-    }
-    for (auto const& [l, x] : dd) {
-      if (x != kUnreach) p.dest_dist.emplace_back(l, x);
-    }
-  } else {
-    for (auto const& o : p.dest_offsets) {
-      v.metas(p.dest_mode, o.target, [&](uint32_t l) { p.dest_locs.push_back(l); });
-    }
-    std::sort(p.dest_locs.begin(), p.dest_locs.end());
-    p.dest_locs.erase(std::unique(p.dest_locs.begin(), p.dest_locs.end()), p.dest_locs.end());
-  }
+  collect_dests(v, p);
+  p.span = static_cast<int16_t>(std::min<int>(p.fastest_direct, p.max_travel_time) + 1);  // search.h:426-429
   if (lb_mode == 1) lower_bounds(v, p, p.lb);
   if (lb_mode == 2 || lb_mode == 3) lb_seeds(v, p, p.lb_seeds);
   auto const mid = static_cast<int64_t>(p.iv_from) + (p.iv_to - p.iv_from) / 2;

@@ -6,6 +6,7 @@
 #pragma once
 
 #include <cstdint>
+#include <memory>
 #include <vector>
 
 #include "b2r.h"
@@ -26,6 +27,8 @@ struct tts_norm {  // transfer_time_settings after search::init()
   int16_t additional_time{0};
   float factor{1.0F};
 };
+
+struct pong_plan;
 
 struct prepped_query {
   int status{B2R_OK};
@@ -58,6 +61,34 @@ struct prepped_query {
   // Dijkstra seeds (location, distance) for lower bounds computed on the
   // device (dijkstra.cc:26-48)
   std::vector<std::pair<uint32_t, uint16_t>> lb_seeds;
+  // worst time at destination of a start-time group = its start + dir(span)
+  // (search.h:426-429; pong.cc:262-265 for a ping, the ping's departure
+  // for a pong)
+  int16_t span{0};
+  bool no_lb{false};      // run without lower bounds (a pong phase)
+  bool need_sweep{false}; // round times of an earlier phase stay in effect
+  uint8_t blast{0};       // pong bounds (raptor.h:172)
+  uint8_t recon_mode{0};  // 0: journeys of the interval, 1: one journey, 2: none
+  uint8_t recon_transfers{0};
+  int32_t recon_start{0};
+  bool use_start_footpaths{false};
+  // B2R_ALGO_PONG: the whole sweep (this query is then its first ping)
+  std::shared_ptr<pong_plan const> pong;
+};
+
+// pong_search (pong.cc:63-475): everything the host needs between the
+// phases.  `ping` and `pong` are phase templates (the query in its own and
+// in the flipped direction); a phase is a template plus its start labels and
+// bounds.
+struct pong_plan {
+  prepped_query ping, pong;
+  int32_t iv_from{0}, iv_to{0};  // search interval
+  int32_t ext_from{0}, ext_to{0};  // timetable::external_interval, minutes
+  int16_t fastest_direct{0};
+  int16_t max_travel_time{0};
+  uint8_t max_transfers{0};
+  uint32_t min_connection_count{0};
+  bool fwd{true}, extend_earlier{false}, extend_later{false};
 };
 
 // Row `src` of the all-pairs lower-bound table: shortest distances from
@@ -73,6 +104,12 @@ int32_t round_to_days(int64_t minutes);
 // all-pairs table on the device (lb_seeds filled).
 void prepare(host_view const& tt, b2r_query const& q, int lb_mode,
              prepped_query& out);
+
+// The start labels of one phase of a pong search at time t: get_starts
+// with a single start time (start_times.cc:241-319) over the phase
+// template's offsets.
+void phase_starts(host_view const& tt, prepped_query const& tmpl, int32_t t,
+                  std::vector<start_label>& out);
 
 // Start labels of [from, to) for an interval extension (search.h:294-312).
 void add_interval_starts(host_view const& tt, prepped_query const& p,

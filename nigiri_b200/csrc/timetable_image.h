@@ -24,7 +24,7 @@ struct b2r_timetable {
       fp_in, route_stop_index, route_stops, route_transport_from, route_transport_to,
       route_stop_time_from, transport_traffic_days, route_traffic_days, location_routes_index,
       location_routes, lb_fwd_index, lb_fwd, lb_bwd_index, lb_bwd, transport_route;
-  std::vector<uint8_t> location_type;
+  std::vector<uint8_t> location_type, route_clasz, route_flags, route_section_flags;
   std::vector<uint16_t> route_stop_times;
   std::vector<uint64_t> bitfields;
   b2r::host_view view{};

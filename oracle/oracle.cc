@@ -17,6 +17,7 @@
 #include <array>
 #include <iterator>
 #include <stdexcept>
+#include <string>
 #include <thread>
 #include <unordered_map>
 #include <vector>
@@ -2159,6 +2160,10 @@ struct or_result {
   std::vector<b2r_leg> legs;
 };
 
+namespace {
+thread_local std::string g_error;  // what the last failed or_search threw
+}  // namespace
+
 extern "C" {
 
 int or_search(const b2r_timetable_desc* tt, const b2r_query* q, or_result** out) {
@@ -2212,10 +2217,13 @@ int or_search(const b2r_timetable_desc* tt, const b2r_query* q, or_result** out)
     res->r.stats.algorithmic_bytes = oracle::byte_model(res->r.stats);
     *out = res.release();
     return B2R_OK;
-  } catch (std::exception const&) {
+  } catch (std::exception const& ex) {
+    g_error = ex.what();
     return B2R_ERR_INTERNAL;
   }
 }
+
+const char* or_last_error(void) { return g_error.c_str(); }
 
 int or_result_view(const or_result* r, b2r_result* view, or_stats* stats) {
   if (r == nullptr) return B2R_ERR_INVALID_ARGUMENT;

@@ -47,6 +47,7 @@ def lib():
         L.or_earliest_alternative.argtypes = [C.POINTER(A.TimetableDesc), C.POINTER(A.Query),
                                               C.c_uint32, C.c_uint32, C.c_int32, C.c_int32,
                                               C.POINTER(A.Leg)]
+        L.or_last_error.restype = C.c_char_p
         _lib = L
     return _lib
 
@@ -56,7 +57,7 @@ class OracleResult:
         self.h = C.c_void_p()
         rc = lib().or_search(C.byref(desc), C.byref(q), C.byref(self.h))
         if rc != 0:
-            raise RuntimeError(f"oracle failed: {rc}")
+            raise RuntimeError(f"oracle failed: {rc} {lib().or_last_error().decode()}")
         self.view = A.Result()
         self.stats = OrStats()
         lib().or_result_view(self.h, C.byref(self.view), C.byref(self.stats))
