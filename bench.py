@@ -271,6 +271,7 @@ def gpu_arm(args, rank, world, local):
     if rank == 0 and not args.no_extras:
         extras = extras_legs(args, h, dtt, qs, B, local)
         extras["served"] = served_leg(eng, qs, [5000.0, 15000.0, 25000.0, None], 4096)
+        extras["range"] = range_leg(eng, h, 1024, seed=1003)
         del eng
         if not args.no_national:
             extras["national"] = national_leg(local)
@@ -359,6 +360,56 @@ def result_key(r, n_loc):
     return ("journeys", r.status, records(r))
 
 
+def range_leg(eng, h, n, seed, reps=2):
+    """Range queries (generated range mix: 30..240 min windows, both
+    directions, station to station, walking allowed at both ends) run as
+    range RAPTOR and as pong on the same engine; queries/s on the device and
+    end to end, and the agreement nigiri's benchmark checks between the two
+    (the Pareto sets on the intersection of their final search intervals)."""
+    from nigiri_b200 import _abi as A
+    from nigiri_b200.timetable import QuerySet
+    lib = A.lib()
+    qs = QuerySet(h, 3, n, seed=seed)
+    arrs = {}
+    for algo, code in (("range_raptor", A.B2R_ALGO_RAPTOR), ("pong", A.B2R_ALGO_PONG)):
+        arr = (A.Query * qs.n)()
+        for i in range(qs.n):
+            arr[i] = qs.arr[i]
+            arr[i].use_start_footpaths = 1
+            arr[i].algorithm = code
+        arrs[algo] = arr
+    out = {"queries": qs.n, "unit": "queries/s"}
+    keys, ivs = {}, {}
+    for algo, arr in arrs.items():
+        res = (A.Result * qs.n)()
+        devs, walls = [], []
+        for rep in range(reps + 1):
+            t0 = time.perf_counter()
+            if lib.b2r_search_batch(eng.handle, arr, qs.n, res) != 0:
+                raise RuntimeError(lib.b2r_last_error().decode())
+            if rep > 0:  # the first run warms up
+                walls.append(time.perf_counter() - t0)
+                devs.append(eng.stats().device_ms / 1e3)
+        st = eng.stats()
+        out[algo] = {"value": qs.n * reps / sum(devs), "e2e": qs.n * reps / sum(walls),
+                     "super_steps": st.super_steps,
+                     "failed": sum(1 for i in range(qs.n) if res[i].status != 0)}
+        keys[algo] = [[(r.journeys[j].start_time, r.journeys[j].dest_time, r.journeys[j].transfers)
+                       for j in range(r.n_journeys)] for r in res[:qs.n]]
+        ivs[algo] = [(r.interval_from, r.interval_to) for r in res[:qs.n]]
+    agree = 0
+    for i in range(qs.n):
+        lo = max(ivs["range_raptor"][i][0], ivs["pong"][i][0])
+        hi = min(ivs["range_raptor"][i][1], ivs["pong"][i][1])
+        fwd = arrs["pong"][i].direction == A.B2R_FORWARD
+        inside = [sorted(t for t in keys[a][i] if lo <= (min(t[0], t[1]) if fwd else max(t[0], t[1])) < hi)
+                  for a in ("range_raptor", "pong")]
+        agree += 1 if inside[0] == inside[1] else 0
+    out["pareto_sets_agree"] = agree
+    out["pong_speedup"] = out["pong"]["value"] / out["range_raptor"]["value"]
+    return out
+
+
 def national_leg(local):
     """National-scale timetable (300k stops, 25k base routes, 2.7M transports,
     stay-seated chain routes).  Batched: batches of 256 mixing one-to-one, 1 h
@@ -408,6 +459,7 @@ def national_leg(local):
     out["served"] = served_leg(eng, sq, [200.0, 1000.0, 5000.0, 20000.0, None],
                                lambda r: 4096 if r is None else max(256, min(4096, int(r))),
                                keep_every=100, kept=kept)
+    out["range"] = range_leg(eng, h, 256, seed=1006, reps=1)
     del eng
     # CPU baseline on the kept queries, which also checks their answers
     sys.path.insert(0, os.path.join(ROOT, "tests"))

@@ -181,7 +181,7 @@ namespace {
 // bounds (raptor.h:117-170), round times and time_at_dest kept (a pong
 // after the first of its iteration), destination bits of the previous
 // phase cleared (the slot changes phase without retiring)
-constexpr uint32_t kAdmFillRows = 0xFFu;
+constexpr uint32_t kAdmFillRows = 0xFFu;  // rows folded by k_fill_bounds
 constexpr uint32_t kAdmKeepRt = 1u << 8;
 constexpr uint32_t kAdmRephase = 1u << 9;
 
@@ -189,7 +189,8 @@ struct adm_hdr {
   uint32_t slot;
   uint32_t n_starts, n_dest, n_off;
   uint32_t clear_rt;
-  uint32_t lb_mode;  // 0 zeros, 1 column in payload, 2 solved on the device, 3 from the table
+  uint32_t lb_mode;  // 0 zeros, 1 column in payload, 2 solved on the device, 3 from the table,
+                     // 4 kept (the column of the query's previous phase)
   uint32_t n_seeds;
   uint32_t flags;
   uint32_t n_keep, pad;
@@ -203,29 +204,13 @@ __global__ void k_admit(dev::state st, adm_hdr const* hdr, uint8_t const* payloa
   auto const h = hdr[a];
   auto const s = h.slot;
   auto const n_loc = st.tt.n_loc;
-  auto const fill_rows = h.flags & kAdmFillRows;
   __shared__ int16_t old_tad[dev::kK];
-  if (h.flags != 0u) {  // the slot's previous phase, read before it is overwritten
+  if ((h.flags & (kAdmKeepRt | kAdmRephase)) != 0u) {  // the slot's previous phase, read before it is overwritten
     auto const& old = st.slots[s];
     if ((h.flags & kAdmKeepRt) != 0u && threadIdx.x < dev::kK) old_tad[threadIdx.x] = old.tad[threadIdx.x];
     if ((h.flags & kAdmRephase) != 0u && !old.intermodal_dest && !old.one_to_all) {
       for (auto i = threadIdx.x; i < old.n_dest; i += blockDim.x) {
         atomicAnd(&st.D[st.dest_pool[old.dest_off + i].loc * st.G + (s >> 5)], ~(1u << (s & 31)));
-      }
-    }
-    if (fill_rows != 0u) {
-      // fill_bounds: row k = best of rounds 0..k of the previous (ping)
-      // search, stored as a key of the flipped (pong) search
-      auto const oq = dev::tagcode(old.gen_query);
-      auto const ofwd = old.fwd != 0;
-      for (auto l = threadIdx.x; l < n_loc; l += blockDim.x) {
-        int best = dev::kKeyInv;
-        for (auto k = 0u; k != fill_rows; ++k) {
-          auto const at = (static_cast<size_t>(k) * n_loc + l) * st.S + s;
-          auto const key = dev::dec(st.rt[at], oq);
-          if (key < best) best = key;
-          st.bounds[at] = static_cast<int16_t>(dev::to_key(!ofwd, dev::from_key(ofwd, best)));
-        }
       }
     }
     __syncthreads();
@@ -317,6 +302,32 @@ __global__ void k_admit(dev::state st, adm_hdr const* hdr, uint8_t const* payloa
   if (!sl.intermodal_dest && !sl.one_to_all) {
     for (auto i = threadIdx.x; i < h.n_dest; i += blockDim.x) {
       atomicOr(&st.D[dests[i].loc * st.G + (s >> 5)], 1u << (s & 31));
+    }
+  }
+}
+
+// fill_bounds (raptor.h:117-170) for the slots re-admitted to the first
+// pong of an iteration, before k_admit overwrites them: row k = the best of
+// rounds 0..k of the slot's ping, stored as a key of the flipped (pong)
+// search.  blockIdx.y = item, threads over locations.
+struct fill_item {
+  uint32_t slot, rows;
+};
+
+__global__ void k_fill_bounds(dev::state st, fill_item const* items) {
+  auto const it = items[blockIdx.y];
+  auto const s = it.slot;
+  auto const& sl = st.slots[s];
+  auto const oq = dev::tagcode(sl.gen_query);
+  auto const ofwd = sl.fwd != 0;
+  auto const n_loc = st.tt.n_loc;
+  for (auto l = blockIdx.x * blockDim.x + threadIdx.x; l < n_loc; l += gridDim.x * blockDim.x) {
+    int best = dev::kKeyInv;
+    for (auto k = 0u; k != it.rows; ++k) {
+      auto const at = (static_cast<size_t>(k) * n_loc + l) * st.S + s;
+      auto const key = dev::dec(st.rt[at], oq);
+      if (key < best) best = key;
+      st.bounds[at] = static_cast<int16_t>(dev::to_key(!ofwd, dev::from_key(ofwd, best)));
     }
   }
 }
@@ -541,6 +552,7 @@ slot_t make_slot(b2r_engine& e, uint32_t s, prepped_query const& p, bool& clear_
   sl.blast = p.blast;
   sl.recon_mode = p.recon_mode;
   sl.recon_transfers = p.recon_transfers;
+  sl.no_lb = p.no_lb ? 1 : 0;
   sl.recon_start = p.recon_start;
   sl.span = p.span;
   sl.n_starts = static_cast<uint32_t>(p.starts.size());
@@ -639,7 +651,7 @@ struct adm_req {
 void admit(b2r_engine& e, std::vector<adm_req> const& adm, cudaStream_t s) {
   if (adm.empty()) return;
   bool any_device_lb = false;
-  size_t need = adm.size() * sizeof(adm_hdr) + 256;
+  size_t need = adm.size() * (sizeof(adm_hdr) + sizeof(fill_item)) + 256 + 16;
   for (auto const& r : adm) {
     need += admission_bytes(e, *r.p) + 64 + (r.keep ? r.keep->size() * sizeof(dev::journey_rec) + 16 : 0);
   }
@@ -697,7 +709,7 @@ void admit(b2r_engine& e, std::vector<adm_req> const& adm, cudaStream_t s) {
     offs.insert(offs.end(), p.dest_offsets.begin(), p.dest_offsets.end());
     h.n_off = static_cast<uint32_t>(offs.size());
     h.off_off = put(offs.data(), offs.size() * sizeof(b2r_offset));
-    h.lb_mode = p.no_lb            ? 0
+    h.lb_mode = p.keep_lb          ? 4
                 : !p.lb.empty()      ? 1
                 : p.one_to_all       ? 0
                 : e.cfg.use_lower_bounds == 2 ? 2
@@ -713,8 +725,19 @@ void admit(b2r_engine& e, std::vector<adm_req> const& adm, cudaStream_t s) {
     h.off_seeds = put(seeds.data(), seeds.size() * sizeof(uint32_t));
     any_device_lb = any_device_lb || h.lb_mode == 2;
   }
+  std::vector<fill_item> fills;
+  for (auto const& r : adm) {
+    if ((r.flags & kAdmFillRows) != 0u) fills.push_back({r.slot, r.flags & kAdmFillRows});
+  }
+  auto const off_fills = put(fills.data(), fills.size() * sizeof(fill_item));
   e.h2d_bytes += off;
   B2R_CUDA(cudaMemcpyAsync(e.d_adm, e.h_adm, off, cudaMemcpyHostToDevice, s));
+  if (!fills.empty()) {
+    auto const bx = std::min<uint32_t>((e.tt->d.n_loc + 255u) / 256u, static_cast<uint32_t>(e.sms) * 2u);
+    k_fill_bounds<<<dim3(bx, static_cast<unsigned>(fills.size())), 256, 0, s>>>(
+        e.st, reinterpret_cast<fill_item const*>(e.d_adm + off_fills));
+    B2R_CUDA(cudaGetLastError());
+  }
   k_admit<<<static_cast<unsigned>(adm.size()), 256, 0, s>>>(
       e.st, reinterpret_cast<adm_hdr const*>(e.d_adm), e.d_adm, static_cast<uint32_t>(adm.size()),
       e.max_starts, e.max_dest, e.max_off);
@@ -1063,6 +1086,7 @@ bool pong_continues(pong_plan const& plan, pong_run const& r) {
 void stage_ping(b2r_engine& e, query_run& q) {
   auto& r = *q.pong;
   q.phase = q.p.pong->ping;
+  q.phase.keep_lb = true;  // the lower bounds of the first ping stay in the slot
   phase_starts(e.tt->view, q.phase, r.start_time, q.phase.starts);
   q.adm_flags = kAdmRephase;
   q.upload.clear();

@@ -128,6 +128,8 @@ struct slot_t {
   uint8_t recon_mode;        // 0: new journeys of the interval, 1: only the journey
                              // (recon_transfers, recon_start), 2: none
   uint8_t recon_transfers;
+  uint8_t no_lb;             // lower bounds read as 0 (a pong phase)
+  uint8_t pad_l;
   int16_t span;              // worst time at destination = group start + dir(span)
   int32_t recon_start;
   tts_t tts;
@@ -157,7 +159,7 @@ struct __align__(16) lane_t {
   uint8_t fwd;
   uint8_t k;
   uint8_t run;
-  uint8_t mode;  // bit0 intermodal dest, bit1 has dests, bit2 tts default
+  uint8_t mode;  // bit0 intermodal dest, bit1 has dests, bit2 tts default, bit3 no lower bounds
   uint16_t claszes;  // allowed transport classes
   uint8_t req;       // required route flags
   uint8_t blast;     // pong bounds: last round (0: none)

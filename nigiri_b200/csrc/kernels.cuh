@@ -116,7 +116,7 @@ __global__ void k_ctl_begin(state st) {
     ln.qtag = tagcode(sl.gen_query);
     ln.mode = (sl.intermodal_dest ? 1u : 0u) |
               ((!sl.intermodal_dest && !sl.one_to_all && sl.n_dest != 0) ? 2u : 0u) |
-              (sl.tts.is_default ? 4u : 0u);
+              (sl.tts.is_default ? 4u : 0u) | (sl.no_lb ? 8u : 0u);
     ln.tad_k = sl.tad[sl.k];
     ln.claszes = sl.allowed_claszes;
     ln.req = sl.req_flags;
@@ -284,7 +284,8 @@ __global__ void __launch_bounds__(256, 3) k_route_scan(state st) {
       // trip's arrival event one ahead
       auto stp = stop_word(0);
       auto xw = st.X[B2R_STOP_LOC(stp) * st.G + g];
-      auto lbv = st.lb[li(st, B2R_STOP_LOC(stp), s)];
+      auto const lb_off = (ln.mode & 8u) != 0u;
+      auto lbv = lb_off ? uint16_t{0} : st.lb[li(st, B2R_STOP_LOC(stp), s)];
       auto stp_next = n > 1u ? stop_word(1) : 0u;
       for (auto i = 0u; i != n; ++i) {
         ++p_stops;
@@ -294,7 +295,7 @@ __global__ void __launch_bounds__(256, 3) k_route_scan(state st) {
         if (i + 1u < n) {
           auto const ln_next = B2R_STOP_LOC(stp_next);
           xw_next = st.X[ln_next * st.G + g];
-          lb_next = st.lb[li(st, ln_next, s)];
+          lb_next = lb_off ? uint16_t{0} : st.lb[li(st, ln_next, s)];
         }
         auto const si = fwd ? i : n - 1u - i;
         auto const l = B2R_STOP_LOC(stp);
@@ -428,7 +429,7 @@ __global__ void k_transfers_pre(state st) {
     if (ln.blast == 0u && fp < bk && fp < dec(rtw, ln.qtag)) rtw = enc(ln.qtag, fp);
     auto const tad = static_cast<int>(sl.tad[k]);
     if (fp < bk && fp <= tad) {
-      auto const lbv = st.lb[li(st, d, s)];
+      auto const lbv = (ln.mode & 8u) ? uint16_t{0} : st.lb[li(st, d, s)];
       if (lbv == 0xFFFFu || fp + static_cast<int>(lbv) > tad) continue;
       if (!within_bounds(st, s, ln.blast, k, d, fp)) continue;
       rtw = enc(ln.qtag, fp);
@@ -476,7 +477,7 @@ __global__ void k_transfers(state st) {
         if (ln.blast == 0u && fp < bk && fp < dec(rtw, ln.qtag)) rtw = enc(ln.qtag, fp);
         auto const tad = (ln.mode & 2u) ? tad_at(st, s, l, 0u) : static_cast<int>(st.tad_phase[s]);
         if (fp < bk && fp <= tad) {
-          auto const lbv = st.lb[li(st, l, s)];
+          auto const lbv = (ln.mode & 8u) ? uint16_t{0} : st.lb[li(st, l, s)];
           if (lbv != 0xFFFFu && fp + static_cast<int>(lbv) <= tad &&
               within_bounds(st, s, ln.blast, ln.k, l, fp)) {
             rtw = enc(ln.qtag, fp);
@@ -577,7 +578,7 @@ __global__ void k_footpaths_pre(state st) {
     if (ln.blast == 0u && fp < bk && fp < dec(rtw, ln.qtag)) rtw = enc(ln.qtag, fp);
     auto const tad = static_cast<int>(sl.tad[k]);
     if (fp < bk && fp <= tad) {
-      auto const lbv = st.lb[li(st, d, s)];
+      auto const lbv = (ln.mode & 8u) ? uint16_t{0} : st.lb[li(st, d, s)];
       if (lbv == 0xFFFFu || fp + static_cast<int>(lbv) > tad) continue;
       if (!within_bounds(st, s, ln.blast, k, d, fp)) continue;
       rtw = enc(ln.qtag, fp);
@@ -627,7 +628,7 @@ __global__ void k_footpaths(state st) {
           if (ln.blast == 0u) atomicMin(&st.rt[rti(st, ln.k, tgt, s)], enc(ln.qtag, key));
           auto const tad = (ln.mode & 2u) ? tad_at(st, s, src, j) : tad_flat;
           if (key > tad) continue;
-          auto const lbv = st.lb[li(st, tgt, s)];
+          auto const lbv = (ln.mode & 8u) ? uint16_t{0} : st.lb[li(st, tgt, s)];
           if (lbv != 0xFFFFu && key + static_cast<int>(lbv) <= tad) {
             if (ln.blast != 0u) {
               if (!within_bounds(st, s, ln.blast, ln.k, tgt, key)) continue;

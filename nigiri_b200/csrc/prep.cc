@@ -466,6 +466,7 @@ void prepare_pong(host_view const& hv, b2r_query const& q, int lb_mode, prepped_
   auto& pong = plan->pong;
   tmpl(!fwd, q.dest_match_mode, q.start_match_mode, de, so, pong);
   pong.no_lb = true;
+  pong.keep_lb = true;
   pong.use_start_footpaths = q.dest_match_mode != B2R_MATCH_INTERMODAL;  // pong.cc:291-295
   pong.recon_mode = 1;
   plan->iv_from = iv_from;

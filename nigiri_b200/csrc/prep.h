@@ -66,6 +66,7 @@ struct prepped_query {
   // for a pong)
   int16_t span{0};
   bool no_lb{false};      // run without lower bounds (a pong phase)
+  bool keep_lb{false};    // leave the slot's lower-bound column as it is
   bool need_sweep{false}; // round times of an earlier phase stay in effect
   uint8_t blast{0};       // pong bounds (raptor.h:172)
   uint8_t recon_mode{0};  // 0: journeys of the interval, 1: one journey, 2: none
