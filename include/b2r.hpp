@@ -9,6 +9,7 @@
  *  - routing::journey / leg     include/nigiri/routing/journey.h:20-118
  *  - routing::routing_result    include/nigiri/routing/search.h:71-76
  *  - routing::raptor_search     include/nigiri/routing/raptor_search.h:9-17
+ *  - routing::pong_search       include/nigiri/routing/raptor/pong.h:21-29
  *  - routing::one_to_all        include/nigiri/routing/one_to_all.h:22-25
  *  - routing::raptor_state      round_times_ of raptor_state.h:22-111
  * restricted to what the engine runs: the static timetable (no real-time
@@ -190,9 +191,11 @@ namespace detail {
 
 // A query in the C ABI's layout; owns the offset arrays it points to.
 struct c_query {
-  c_query(query const& q, direction dir, uint8_t kind) : start{to_c(q.start_)}, dest{to_c(q.destination_)} {
+  c_query(query const& q, direction dir, uint8_t kind, uint8_t algorithm = B2R_ALGO_RAPTOR)
+      : start{to_c(q.start_)}, dest{to_c(q.destination_)} {
     b2r_query_init(&c);
     c.kind = kind;
+    c.algorithm = algorithm;
     c.direction = static_cast<uint8_t>(dir);
     if (auto const* t = std::get_if<unixtime_t>(&q.start_time_)) {
       c.start_time = *t;
@@ -267,12 +270,12 @@ inline std::vector<journey> journeys_of(b2r_result const& r) {
   return out;
 }
 
-// routing::raptor_search for many queries in one engine call (continuous
-// batching over the engine's resident slots).
-inline std::vector<routing_result> raptor_search(engine& e, std::span<query const> qs, direction dir) {
+namespace detail {
+inline std::vector<routing_result> search(engine& e, std::span<query const> qs, direction dir,
+                                          uint8_t algorithm) {
   std::vector<detail::c_query> cq;
   cq.reserve(qs.size());
-  for (auto const& q : qs) cq.emplace_back(q, dir, static_cast<uint8_t>(B2R_ONE_TO_ONE));
+  for (auto const& q : qs) cq.emplace_back(q, dir, static_cast<uint8_t>(B2R_ONE_TO_ONE), algorithm);
   std::vector<b2r_query> arr;
   arr.reserve(cq.size());
   for (auto const& x : cq) arr.push_back(x.c);
@@ -289,9 +292,27 @@ inline std::vector<routing_result> raptor_search(engine& e, std::span<query cons
   }
   return out;
 }
+}  // namespace detail
+
+// routing::raptor_search for many queries in one engine call (continuous
+// batching over the engine's resident slots).
+inline std::vector<routing_result> raptor_search(engine& e, std::span<query const> qs, direction dir) {
+  return detail::search(e, qs, dir, B2R_ALGO_RAPTOR);
+}
 
 inline routing_result raptor_search(engine& e, query const& q, direction dir) {
   return raptor_search(e, std::span<query const>{&q, 1U}, dir).front();
+}
+
+// routing::pong_search: the same range search by alternating forward and
+// backward searches.  A sweep that fails as the reference's would ("no
+// pong") returns status_ == B2R_ERR_INTERNAL instead of throwing.
+inline std::vector<routing_result> pong_search(engine& e, std::span<query const> qs, direction dir) {
+  return detail::search(e, qs, dir, B2R_ALGO_PONG);
+}
+
+inline routing_result pong_search(engine& e, query const& q, direction dir) {
+  return pong_search(e, std::span<query const>{&q, 1U}, dir).front();
 }
 
 // routing::one_to_all: the round times of every location.

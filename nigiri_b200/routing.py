@@ -123,7 +123,7 @@ class OneToAllResult:  # raptor_state rows of one_to_all
 class _QueryBuffer:
     """Owns the b2r_query structs and offset arrays of a batch."""
 
-    def __init__(self, queries: Sequence[Tuple[Query, str, int]]):
+    def __init__(self, queries: Sequence[Tuple[Query, str, int]], algorithm: int = A.B2R_ALGO_RAPTOR):
         n = len(queries)
         self.arr = (A.Query * max(1, n))()
         self.keep = []
@@ -131,6 +131,7 @@ class _QueryBuffer:
         for i, (q, direction, kind) in enumerate(queries):
             x = self.arr[i]
             lib.b2r_query_init(C.byref(x))
+            x.algorithm = algorithm
             st = (A.Offset * max(1, len(q.start)))()
             for j, o in enumerate(q.start):
                 st[j].target, st[j].duration, st[j].transport_mode_id = o.target, o.duration, o.transport_mode_id
@@ -315,6 +316,22 @@ def raptor_search(engine: Engine, queries: Sequence[Query], direction=FORWARD,
     list of per-query directions)."""
     dirs = direction if isinstance(direction, (list, tuple)) else [direction] * len(queries)
     qb = _QueryBuffer([(q, d, A.B2R_ONE_TO_ONE) for q, d in zip(queries, dirs)])
+
+    def conv(_, r):
+        return RoutingResult(_journeys(r), (r.interval_from, r.interval_to), r.status,
+                             r.n_rounds, r.n_start_times)
+    return engine.run(qb, len(queries), conv, plain=plain)
+
+
+def pong_search(engine: Engine, queries: Sequence[Query], direction=FORWARD,
+                plain: bool = False) -> List[RoutingResult]:
+    """routing::pong_search (src/routing/raptor/pong.cc): the range search
+    by alternating forward and backward searches; same results as
+    raptor_search on the intersection of their search intervals.  A query
+    whose sweep fails as the reference's would ("no pong", "no pong
+    progress") comes back with status B2R_ERR_INTERNAL."""
+    dirs = direction if isinstance(direction, (list, tuple)) else [direction] * len(queries)
+    qb = _QueryBuffer([(q, d, A.B2R_ONE_TO_ONE) for q, d in zip(queries, dirs)], A.B2R_ALGO_PONG)
 
     def conv(_, r):
         return RoutingResult(_journeys(r), (r.interval_from, r.interval_to), r.status,

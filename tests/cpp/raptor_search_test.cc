@@ -2,7 +2,9 @@
 // queries run through the C++ mirror of nigiri's routing interface
 // (b2r.hpp -> the B200 engine) and through the CPU oracle (test
 // infrastructure), and the complete journeys (every leg) must be equal.
-// One-to-all searches compare the round times of every location.
+// Range queries also run through pong_search (walking allowed at the
+// start, as at the destination).  One-to-all searches compare the round
+// times of every location.
 //
 //   raptor_search_test            exit 0 when every query matches
 #include <cstdio>
@@ -40,6 +42,10 @@ r::query from_c(b2r_query const& c) {  // the generator's queries in nigiri's te
   q.fastest_direct_factor_ = c.fastest_direct_factor;
   q.transfer_time_settings_ = {c.tts_default != 0, c.tts_min_transfer_time, c.tts_additional_time,
                                c.tts_factor};
+  q.allowed_claszes_ = static_cast<uint16_t>(c.allowed_claszes);
+  q.require_bike_transport_ = c.require_bike_transport != 0;
+  q.require_car_transport_ = c.require_car_transport != 0;
+  q.no_compulsory_reservation_ = c.no_compulsory_reservation != 0;
   return q;
 }
 
@@ -103,6 +109,30 @@ int run_workload(uint32_t workload, uint32_t timetable_seed, uint32_t n, uint64_
         std::printf("workload %u query %u (%s) differs\n", workload, i,
                     dir == r::direction::kForward ? "forward" : "backward");
         print("engine", got[i].journeys_);
+        print("oracle", want);
+      }
+    }
+    // pong_search on the range queries
+    std::vector<r::query> ranges;
+    std::vector<b2r_query> cr;
+    for (auto i = 0U; i != batch.size(); ++i) {
+      if (cq[i]->is_interval == 0) continue;
+      auto c = *cq[i];
+      c.use_start_footpaths = 1;
+      c.algorithm = B2R_ALGO_PONG;
+      cr.push_back(c);
+      ranges.push_back(from_c(c));
+    }
+    if (ranges.empty()) continue;
+    auto const pongs = r::pong_search(eng, ranges, dir);
+    for (auto i = 0U; i != ranges.size(); ++i) {
+      auto const want = oracle_journeys(d, cr[i]);
+      n_journeys += want.size();
+      if (pongs[i].status_ != B2R_OK || pongs[i].journeys_ != want) {
+        ++bad;
+        std::printf("workload %u pong query %u (%s) differs\n", workload, i,
+                    dir == r::direction::kForward ? "forward" : "backward");
+        print("engine", pongs[i].journeys_);
         print("oracle", want);
       }
     }
