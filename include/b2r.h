@@ -495,6 +495,37 @@ int b2r_tt_load(const char* path, b2r_host_timetable** out);
 int b2r_tt_desc(const b2r_host_timetable* t, b2r_timetable_desc* out);
 int b2r_tt_destroy(b2r_host_timetable* t);
 
+/* GTFS feeds (nigiri's loader::gtfs::load_timetable, the parts its routing
+ * tests exercise): agency (the first agency's time zone for every trip,
+ * noon_offsets.cc), stops with parent stations, routes (route_type ->
+ * transport class), trips with blocks and bike / car / reservation flags,
+ * stop times with pickup and drop-off restrictions, calendar,
+ * calendar_dates, transfers.txt type 2.  Not read: frequencies, flex,
+ * shapes, fares, stay-seated transfers, footpaths from stop proximity.
+ * Time zones come from TZif files (tzdata_dir, default /usr/share/zoneinfo).
+ * Mirrors loader_config (loader_interface.h:17-24). */
+typedef struct b2r_gtfs_config {
+  int32_t date_range_from, date_range_to; /* timetable::date_range_, days since the epoch */
+  uint32_t default_transfer_time;         /* minutes (2) */
+  uint16_t bikes_allowed_default;         /* bit c: trips of class c carry bikes unless trips.txt says */
+  uint16_t cars_allowed_default;
+  uint16_t reservation_not_required_default;
+  uint16_t pad_;
+  const char* default_tz;                 /* used when agency.txt names none */
+  const char* tzdata_dir;                 /* NULL: /usr/share/zoneinfo */
+} b2r_gtfs_config;
+void b2r_gtfs_config_init(b2r_gtfs_config* c);
+/* path: a directory with the feed's .txt files, or (is_text != 0) the feed
+ * as one text of "# <file>.txt" sections (the mem_dir format of nigiri's
+ * tests). */
+int b2r_tt_load_gtfs(const char* path, int is_text, const b2r_gtfs_config* cfg,
+                     b2r_host_timetable** out);
+/* Feed identifiers of a loaded timetable: the stop_id of location l (special
+ * stations: START, END, VIA0..VIA6), the route short name of transport x.
+ * The strings live as long as the timetable. */
+int b2r_tt_location_id(const b2r_host_timetable* t, uint32_t l, const char** id);
+int b2r_tt_transport_name(const b2r_host_timetable* t, uint32_t x, const char** name);
+
 /* Seeded synthetic query stream of a workload (configs 1..5). */
 typedef struct b2r_query_set b2r_query_set;
 int b2r_queries_generate(const b2r_host_timetable* t, uint32_t config,

@@ -57,6 +57,16 @@ class TimetableDesc(C.Structure):
     ]
 
 
+class GtfsConfig(C.Structure):
+    _fields_ = [
+        ("date_range_from", C.c_int32), ("date_range_to", C.c_int32),
+        ("default_transfer_time", C.c_uint32),
+        ("bikes_allowed_default", C.c_uint16), ("cars_allowed_default", C.c_uint16),
+        ("reservation_not_required_default", C.c_uint16), ("pad_", C.c_uint16),
+        ("default_tz", C.c_char_p), ("tzdata_dir", C.c_char_p),
+    ]
+
+
 class Offset(C.Structure):
     _fields_ = [("target", C.c_uint32), ("duration", C.c_int16),
                 ("pad_", C.c_int16), ("transport_mode_id", C.c_int32)]
@@ -171,7 +181,8 @@ EXPORTS = [
     "b2r_search_plain", "b2r_serve_start", "b2r_serve_stop", "b2r_submit",
     "b2r_poll", "b2r_wait", "b2r_release", "b2r_last_batch_stats",
     "b2r_tt_generate", "b2r_tt_build", "b2r_tt_save", "b2r_tt_load",
-    "b2r_tt_desc", "b2r_tt_destroy", "b2r_queries_generate",
+    "b2r_tt_desc", "b2r_tt_destroy", "b2r_gtfs_config_init", "b2r_tt_load_gtfs",
+    "b2r_tt_location_id", "b2r_tt_transport_name", "b2r_queries_generate",
     "b2r_queries_count", "b2r_queries_get", "b2r_queries_destroy",
     "b2r_one_to_all_noalloc", "b2r_last_batch_scan_profile",
     "b2r_engine_get_shape", "b2r_engine_set_shape", "b2r_engine_autotune",
@@ -206,6 +217,10 @@ def _declare(lib):
         "b2r_tt_load": (C.c_int, [C.c_char_p, C.POINTER(vp)]),
         "b2r_tt_desc": (C.c_int, [vp, C.POINTER(TimetableDesc)]),
         "b2r_tt_destroy": (C.c_int, [vp]),
+        "b2r_gtfs_config_init": (None, [C.POINTER(GtfsConfig)]),
+        "b2r_tt_load_gtfs": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(GtfsConfig), C.POINTER(vp)]),
+        "b2r_tt_location_id": (C.c_int, [vp, C.c_uint32, C.POINTER(C.c_char_p)]),
+        "b2r_tt_transport_name": (C.c_int, [vp, C.c_uint32, C.POINTER(C.c_char_p)]),
         "b2r_queries_generate": (C.c_int, [vp, C.c_uint32, C.c_uint64, C.c_uint32, C.POINTER(vp)]),
         "b2r_queries_count": (C.c_uint32, [vp]),
         "b2r_queries_get": (C.POINTER(Query), [vp, C.c_uint32]),

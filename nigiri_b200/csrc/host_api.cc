@@ -9,9 +9,6 @@
 #include "host_tt.h"
 #include "queries.h"
 
-struct b2r_host_timetable {
-  b2r::host_timetable t;
-};
 
 struct b2r_query_set {
   b2r::query_set s;

@@ -43,6 +43,9 @@ struct host_timetable {
 
   // generator metadata (coordinates in metres, for query generation)
   std::vector<float> x, y;
+  // feed identifiers of a loaded feed (GTFS stop_id per location, the
+  // display name of each transport), empty for generated timetables
+  std::vector<std::string> location_ids, transport_names;
 
   uint32_t n_bitfields() const {
     return static_cast<uint32_t>(bitfields.size() / 8U);
@@ -61,3 +64,8 @@ bool save(host_timetable const& t, std::string const& path);
 bool load(std::string const& path, host_timetable& t);
 
 }  // namespace b2r
+
+// the C ABI's host timetable handle
+struct b2r_host_timetable {
+  b2r::host_timetable t;
+};

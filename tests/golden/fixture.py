@@ -149,6 +149,44 @@ class FixtureTimetable:
             pass
 
 
+class GtfsFixture:
+    """A timetable read by the engine's GTFS reader (b2r_tt_load_gtfs) from
+    the feed text of one of nigiri's tests, with the same lookups as
+    FixtureTimetable (stop ids, transport names)."""
+
+    def __init__(self, name, lib):
+        cases = load_cases()
+        feed = cases["gtfs_feeds"][name]
+        self.spec = cases["timetables"][name]
+        self.lib = lib
+        cfg = A.GtfsConfig()
+        lib.b2r_gtfs_config_init(C.byref(cfg))
+        cfg.date_range_from, cfg.date_range_to = (_day(x) for x in self.spec["date_range"])
+        for k, v in feed["config"].items():
+            setattr(cfg, k, v)
+        self.handle = C.c_void_p()
+        rc = lib.b2r_tt_load_gtfs(feed["text"].encode(), 1, C.byref(cfg), C.byref(self.handle))
+        assert rc == 0, lib.b2r_last_error()
+        self.desc = A.TimetableDesc()
+        lib.b2r_tt_desc(self.handle, C.byref(self.desc))
+        s = C.c_char_p()
+        self.loc_name = {}
+        for l in range(self.desc.n_locations):
+            assert lib.b2r_tt_location_id(self.handle, l, C.byref(s)) == 0
+            self.loc_name[l] = s.value.decode()
+        self.loc_idx = {v: k for k, v in self.loc_name.items()}
+        self.transport_names = []
+        for t in range(self.desc.n_transports):
+            assert lib.b2r_tt_transport_name(self.handle, t, C.byref(s)) == 0
+            self.transport_names.append(s.value.decode())
+
+    def __del__(self):
+        try:
+            self.lib.b2r_tt_destroy(self.handle)
+        except Exception:
+            pass
+
+
 MODES = {"exact": A.B2R_MATCH_EXACT, "intermodal": A.B2R_MATCH_INTERMODAL,
          "equivalent": A.B2R_MATCH_EQUIVALENT, "only_children": A.B2R_MATCH_ONLY_CHILDREN}
 

@@ -183,13 +183,14 @@ def gtfs_dijkstra():
       AB_TRP A 09:00 -> B 09:30     UTC 07:00 -> 07:30
       BC_TRP B 10:00 -> C2 11:00    UTC 08:00 -> 09:00
       DB_TRP D1 09:30 -> B 09:45    UTC 07:30 -> 07:45
-      DC_TRP D2 10:30 -> C1 11:30   UTC 08:30 -> 09:30"""
+      DC_TRP D2 10:30 -> C1 11:30   UTC 08:30 -> 09:30
+    Route type 0: kTram (9)."""
     d = "2024-06-08"
     services = [
-        dict(utc_service("AB", ["A", "B"], d, [hm("07:00"), hm("07:30")]), id="AB_TRP"),
-        dict(utc_service("BC", ["B", "C2"], d, [hm("08:00"), hm("09:00")]), id="BC_TRP"),
-        dict(utc_service("DB", ["D1", "B"], d, [hm("07:30"), hm("07:45")]), id="DB_TRP"),
-        dict(utc_service("DC", ["D2", "C1"], d, [hm("08:30"), hm("09:30")]), id="DC_TRP"),
+        dict(utc_service("AB", ["A", "B"], d, [hm("07:00"), hm("07:30")]), id="AB_TRP", clasz=9),
+        dict(utc_service("BC", ["B", "C2"], d, [hm("08:00"), hm("09:00")]), id="BC_TRP", clasz=9),
+        dict(utc_service("DB", ["D1", "B"], d, [hm("07:30"), hm("07:45")]), id="DB_TRP", clasz=9),
+        dict(utc_service("DC", ["D2", "C1"], d, [hm("08:30"), hm("09:30")]), id="DC_TRP", clasz=9),
     ]
     parents = {"C1": "C", "C2": "C", "D1": "D", "D2": "D"}
     return {
@@ -658,6 +659,55 @@ def known_answers(ref_root: str):
     return ka
 
 
+# ----------------------------------------------------------------------------
+# The GTFS feeds of the tests behind the gtfs_* timetables, verbatim (the
+# text of their mem_dir::read raw strings), with the loader_config the test
+# passes: the GTFS reader must rebuild those timetables from them.
+# ----------------------------------------------------------------------------
+
+def raw_after(src: str, marker: str, nth: int = 0) -> str:
+    """The raw string literal (R"delim(...)delim") after the nth `marker`."""
+    pos = -1
+    for _ in range(nth + 1):
+        pos = src.index(marker, pos + 1)
+    m = re.compile(r'R"(\w*)\(').search(src, pos)
+    start = m.end()
+    return src[start:src.index(")" + m.group(1) + '"', start)]
+
+
+ALL_CLASSES = 0xFFFF
+GTFS_FEEDS = {
+    "gtfs_transfer_time": ("test/routing/transfer_time_settings_test.cc", "test_files =", 0, {}),
+    "gtfs_dijkstra": ("test/routing/dijkstra_test.cc", "dijkstra_files()", 0, {}),
+    "gtfs_clasz": ("test/routing/clasz_filter_test.cc", "test_files =", 0, {}),
+    "gtfs_bikes_1": ("test/routing/bike_transport_test.cc", "test_files_1 =", 0, {}),
+    "gtfs_bikes_2": ("test/routing/bike_transport_test.cc", "test_files2 =", 0, {}),
+    "gtfs_bikes_3": ("test/routing/bike_transport_test.cc", "test_files3 =", 0, {}),
+    "gtfs_reservation_1": ("test/routing/no_compulsory_reservation_test.cc", "test_files_1 =", 0,
+                           {"reservation_not_required_default": ALL_CLASSES}),
+    "gtfs_reservation_2": ("test/routing/no_compulsory_reservation_test.cc", "test_files2 =", 0,
+                           {"reservation_not_required_default": ALL_CLASSES}),
+    "gtfs_reservation_3": ("test/routing/no_compulsory_reservation_test.cc", "test_files3 =", 0,
+                           {"reservation_not_required_default": ALL_CLASSES}),
+    "gtfs_pong_lookahead": ("test/routing/pong_minlookahead_test.cc", "kTimetable =", 0, {}),
+    "gtfs_pong_gap": ("test/routing/pong_gap_truncation_test.cc", "test_files()", 0, {}),
+    "gtfs_alternative_bikes": ("test/routing/pong_get_earliest_alternative_test.cc", "kGTFS =", 0, {}),
+    "gtfs_alternative_cars": ("test/routing/pong_get_earliest_alternative_test.cc", "kGTFS =", 1, {}),
+}
+
+
+def gtfs_feeds(ref_root: str):
+    out = {}
+    for name, (path, marker, nth, config) in GTFS_FEEDS.items():
+        src = open(os.path.join(ref_root, path)).read()
+        if config.get("reservation_not_required_default") == ALL_CLASSES:
+            # the test's default_reservation_not_required: all 16 classes true
+            m = re.search(r"default_reservation_not_required\s*=\s*std::array<bool, kNumClasses>\{([^}]*)\}", src)
+            assert m and [x.strip() for x in m.group(1).split(",")] == ["true"] * 16
+        out[name] = {"ref": path, "text": raw_after(src, marker, nth), "config": config}
+    return out
+
+
 def main(ref_root: str):
     out_cases = []
     for case in cases():
@@ -676,7 +726,7 @@ def main(ref_root: str):
         case["expected"] = expected
         out_cases.append(case)
     doc = {"timetables": TIMETABLES, "cases": out_cases,
-           "known_answers": known_answers(ref_root),
+           "known_answers": known_answers(ref_root), "gtfs_feeds": gtfs_feeds(ref_root),
            "generated_by": "tests/golden/make_fixtures.py"}
     with open(os.path.join(HERE, "cases.json"), "w") as f:
         json.dump(doc, f, indent=1, sort_keys=True)

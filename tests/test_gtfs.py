@@ -1,0 +1,115 @@
+"""The GTFS reader (b2r_tt_load_gtfs) on the feeds of nigiri's routing tests:
+the timetables it builds give the golden journeys and known answers of
+those tests (through the oracle on the CPU, through the engine on the
+GPU), and match the timetables restated by hand for them."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import fixture as F
+import oracle_lib
+from nigiri_b200 import _abi as A
+
+CASES = F.load_cases()
+FEEDS = sorted(CASES["gtfs_feeds"])
+
+
+@pytest.fixture(scope="module")
+def loaded():
+    return {name: F.GtfsFixture(name, A.lib()) for name in FEEDS}
+
+
+def routes_of(tt):
+    """(stop ids, class, section flags, [(transport name, UTC days, times)])
+    per route, independent of route and bitfield numbering."""
+    d = tt.desc
+    nr, nt = d.n_routes, d.n_transports
+    arr = lambda p, n, dt: np.ctypeslib.as_array(p, shape=(n,)).astype(dt).copy() if n else np.zeros(0, dt)
+    rsi = arr(d.route_stop_index, nr + 1, np.int64)
+    stops = arr(d.route_stops, int(rsi[-1]), np.int64)
+    tf = arr(d.route_transport_from, nr, np.int64)
+    tto = arr(d.route_transport_to, nr, np.int64)
+    sf = arr(d.route_stop_time_from, nr, np.int64)
+    st = arr(d.route_stop_times, d.n_route_stop_times, np.int64)
+    tbf = arr(d.transport_traffic_days, nt, np.int64)
+    bfs = arr(d.bitfields, 8 * d.n_bitfields, np.uint64).reshape(-1, 8) if d.n_bitfields else None
+    clasz = arr(d.route_clasz, nr, np.int64)
+    sec = arr(d.route_section_flags, int(rsi[-1]), np.int64) if d.route_section_flags else np.zeros(int(rsi[-1]), np.int64)
+    out = []
+    for r in range(nr):
+        n = rsi[r + 1] - rsi[r]
+        n_t = tto[r] - tf[r]
+        names = tuple(tt.loc_name[int(w) & 0x0FFFFFFF] for w in stops[rsi[r]:rsi[r + 1]])
+        flags = tuple(int(w) >> 28 for w in stops[rsi[r]:rsi[r + 1]])
+        trs = []
+        for x in range(n_t):
+            t = tf[r] + x
+            days = tuple(int(i) for i in range(512)
+                         if (int(bfs[tbf[t]][i // 64]) >> (i % 64)) & 1)
+            times = tuple(int(st[sf[r] + slot * n_t + x]) for slot in range(2 * (n - 1)))
+            trs.append((tt.transport_names[t], days, times))
+        out.append((names, flags, int(clasz[r]), tuple(int(x) for x in sec[rsi[r]:rsi[r + 1] - 1]), tuple(trs)))
+    return sorted(out)
+
+
+@pytest.mark.parametrize("name", FEEDS)
+def test_reader_rebuilds_the_restated_timetable(name, loaded):
+    """Same routes (stops, pickup / drop-off flags, class, section flags),
+    same transports (names, UTC traffic days, UTC times) and the same
+    footpaths, transfer times and parents as the hand-restated fixture."""
+    got = loaded[name]
+    want = F.FixtureTimetable(CASES["timetables"][name], A.lib())
+    # traffic days are bits of the same internal interval in both
+    assert routes_of(got) == routes_of(want)
+
+    def locs(tt):
+        d = tt.desc
+        n = d.n_locations
+        tr = np.ctypeslib.as_array(d.transfer_time, shape=(n,))
+        par = np.ctypeslib.as_array(d.parent, shape=(n,)) if d.parent else np.full(n, 0xFFFFFFFF)
+        fi = np.ctypeslib.as_array(d.footpaths_out_index, shape=(n + 1,))
+        fo = np.ctypeslib.as_array(d.footpaths_out, shape=(int(fi[-1]),)) if fi[-1] else []
+        out = {}
+        for l in range(9, n):
+            fps = sorted((tt.loc_name[int(w) & 0x7FFFFF], int(w) >> 23) for w in fo[fi[l]:fi[l + 1]])
+            p = int(par[l])
+            out[tt.loc_name[l]] = (int(tr[l]), None if p == 0xFFFFFFFF else tt.loc_name[p], tuple(fps))
+        return out
+    assert locs(got) == locs(want)
+
+
+@pytest.mark.parametrize("case", [c for c in CASES["cases"] if c["timetable"] in CASES["gtfs_feeds"]],
+                         ids=lambda c: c["name"])
+def test_golden_cases_on_read_feeds(case, loaded):
+    tt = loaded[case["timetable"]]
+    q = F.FixtureQuery(A.lib(), tt, case["query"])
+    r = oracle_lib.OracleResult(tt.desc, q.q)
+    assert F.journeys_to_records(tt, r.view) == F.strip_expected(case["expected"])
+
+
+def test_reader_rejects_missing_time_zone():
+    cfg = A.GtfsConfig()
+    A.lib().b2r_gtfs_config_init(C.byref(cfg))
+    cfg.date_range_from, cfg.date_range_to = 19000, 19002
+    h = C.c_void_p()
+    text = b"# stops.txt\nstop_id,stop_name\nA,A\n"
+    assert A.lib().b2r_tt_load_gtfs(text, 1, C.byref(cfg), C.byref(h)) == A.B2R_ERR_INVALID_ARGUMENT
+    assert b"time zone" in A.lib().b2r_last_error()
+
+
+@pytest.mark.gpu
+def test_golden_cases_on_read_feeds_gpu(loaded):
+    """Feed text -> reader -> device image -> engine: the golden journeys."""
+    from nigiri_b200 import routing as R
+    for name in FEEDS:
+        tt = loaded[name]
+        dtt = R.Timetable(tt.desc, owner=tt)
+        eng = R.Engine(dtt, max_slots=32)
+        for c in CASES["cases"]:
+            if c["timetable"] != name:
+                continue
+            q = F.FixtureQuery(A.lib(), tt, c["query"])
+            res = A.Result()
+            assert A.lib().b2r_search_batch(eng.handle, C.byref(q.q), 1, C.byref(res)) == 0
+            assert F.journeys_to_records(tt, res) == F.strip_expected(c["expected"]), c["name"]
