@@ -38,6 +38,38 @@ class HostTimetable:
             lib.b2r_tt_save(h, os.path.join(cache_dir, f"tt_config{cfg}_seed{seed}.b2r").encode())
         return t
 
+    @classmethod
+    def load_gtfs(cls, feed: str, date_range: tuple[int, int], text: bool = False,
+                  default_transfer_time: int = 2, bikes_allowed_default: int = 0,
+                  cars_allowed_default: int = 0, reservation_not_required_default: int = 0,
+                  default_tz: str | None = None, tzdata_dir: str | None = None):
+        """A GTFS feed (a directory, or with text=True nigiri's "# file.txt"
+        text) read for timetable::date_range_ = date_range (days since the
+        epoch, [from, to)); the defaults mirror loader_config (bit c of a
+        *_default mask = transport class c)."""
+        cfg = A.GtfsConfig()
+        A.lib().b2r_gtfs_config_init(C.byref(cfg))
+        cfg.date_range_from, cfg.date_range_to = date_range
+        cfg.default_transfer_time = default_transfer_time
+        cfg.bikes_allowed_default = bikes_allowed_default
+        cfg.cars_allowed_default = cars_allowed_default
+        cfg.reservation_not_required_default = reservation_not_required_default
+        cfg.default_tz = default_tz.encode() if default_tz else None
+        cfg.tzdata_dir = tzdata_dir.encode() if tzdata_dir else None
+        h = C.c_void_p()
+        _check(A.lib().b2r_tt_load_gtfs(feed.encode(), 1 if text else 0, C.byref(cfg), C.byref(h)))
+        return cls(h)
+
+    def location_id(self, l: int) -> str:
+        s = C.c_char_p()
+        _check(A.lib().b2r_tt_location_id(self.handle, l, C.byref(s)))
+        return s.value.decode()
+
+    def transport_name(self, t: int) -> str:
+        s = C.c_char_p()
+        _check(A.lib().b2r_tt_transport_name(self.handle, t, C.byref(s)))
+        return s.value.decode()
+
     def close(self):
         if self.handle:
             A.lib().b2r_tt_destroy(self.handle)

@@ -88,6 +88,26 @@ def test_golden_cases_on_read_feeds(case, loaded):
     assert F.journeys_to_records(tt, r.view) == F.strip_expected(case["expected"])
 
 
+def test_python_reader_reads_a_feed_directory(tmp_path):
+    """HostTimetable.load_gtfs on a directory of files (the clasz test's
+    feed written out), with the stop ids and names it keeps."""
+    from nigiri_b200.timetable import HostTimetable
+    text = CASES["gtfs_feeds"]["gtfs_clasz"]["text"]
+    name = None
+    for line in text.splitlines():
+        if line.startswith("# "):
+            name = line[2:].strip()
+            (tmp_path / name).write_text("")
+        elif name:
+            with open(tmp_path / name, "a") as f:
+                f.write(line + "\n")
+    spec = CASES["timetables"]["gtfs_clasz"]
+    h = HostTimetable.load_gtfs(str(tmp_path), tuple(F._day(x) for x in spec["date_range"]))
+    ids = [h.location_id(l) for l in range(h.desc.n_locations)]
+    assert ids[9:] == ["A", "B", "C"]
+    assert sorted(h.transport_name(t) for t in range(h.desc.n_transports)) == ["1", "2", "X"]
+
+
 def test_reader_rejects_missing_time_zone():
     cfg = A.GtfsConfig()
     A.lib().b2r_gtfs_config_init(C.byref(cfg))
