@@ -157,7 +157,7 @@ class GtfsFixture:
     def __init__(self, name, lib):
         cases = load_cases()
         feed = cases["gtfs_feeds"][name]
-        self.spec = cases["timetables"][name]
+        self.spec = cases["timetables"].get(name, {"date_range": feed.get("date_range"), "locations": []})
         self.lib = lib
         cfg = A.GtfsConfig()
         lib.b2r_gtfs_config_init(C.byref(cfg))

@@ -696,8 +696,35 @@ GTFS_FEEDS = {
 }
 
 
+# feeds whose timetable only the reader builds (no hand restatement)
+GTFS_ONLY_FEEDS = {
+    "gtfs_shortest_fp": ("test/routing/shortest_fp_test.cc", "shortest_fp_files()", 0, {},
+                         ["2024-06-07", "2024-06-09"]),
+}
+
+
+def gtfs_only_cases():
+    """test/routing/shortest_fp_test.cc: intermodal searches over transfers.txt
+    footpaths, forward over 2024-06-07 and backward over 06-07 .. 06-09."""
+    a = [["A0", 3, 23], ["A1", 5, 23], ["A2", 10, 23]]
+    c = [["C3", 30, 42], ["C4", 20, 42], ["C5", 10, 42]]
+    ref = "test/routing/shortest_fp_test.cc"
+    return [
+        dict(name="shortest_fp_forward", timetable="gtfs_shortest_fp", ref=ref, golden="exp_fwd_journey",
+             query=dict(start=a, dest=c, interval=[t("2024-06-07 00:00"), t("2024-06-08 00:00")],
+                        direction="fwd", start_mode="intermodal", dest_mode="intermodal")),
+        dict(name="shortest_fp_backward", timetable="gtfs_shortest_fp", ref=ref, golden="exp_bwd_journey",
+             query=dict(start=c, dest=a, interval=[t("2024-06-07 00:00"), t("2024-06-09 00:00")],
+                        direction="bwd", start_mode="intermodal", dest_mode="intermodal")),
+    ]
+
+
 def gtfs_feeds(ref_root: str):
     out = {}
+    for name, (path, marker, nth, config, date_range) in GTFS_ONLY_FEEDS.items():
+        src = open(os.path.join(ref_root, path)).read()
+        out[name] = {"ref": path, "text": raw_after(src, marker, nth), "config": config,
+                     "date_range": date_range}
     for name, (path, marker, nth, config) in GTFS_FEEDS.items():
         src = open(os.path.join(ref_root, path)).read()
         if config.get("reservation_not_required_default") == ALL_CLASSES:
@@ -725,7 +752,11 @@ def main(ref_root: str):
         case["golden"] = list(g) if isinstance(g, tuple) else g
         case["expected"] = expected
         out_cases.append(case)
-    doc = {"timetables": TIMETABLES, "cases": out_cases,
+    gtfs_cases = []
+    for case in gtfs_only_cases():
+        src = open(os.path.join(ref_root, case["ref"])).read()
+        gtfs_cases.append(dict(case, expected=parse_journeys(raw_string(src, case["golden"]))))
+    doc = {"timetables": TIMETABLES, "cases": out_cases, "gtfs_cases": gtfs_cases,
            "known_answers": known_answers(ref_root), "gtfs_feeds": gtfs_feeds(ref_root),
            "generated_by": "tests/golden/make_fixtures.py"}
     with open(os.path.join(HERE, "cases.json"), "w") as f:

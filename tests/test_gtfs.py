@@ -13,6 +13,8 @@ from nigiri_b200 import _abi as A
 
 CASES = F.load_cases()
 FEEDS = sorted(CASES["gtfs_feeds"])
+RESTATED = [f for f in FEEDS if f in CASES["timetables"]]
+ALL_CASES = [c for c in CASES["cases"] if c["timetable"] in CASES["gtfs_feeds"]] + CASES["gtfs_cases"]
 
 
 @pytest.fixture(scope="module")
@@ -53,7 +55,7 @@ def routes_of(tt):
     return sorted(out)
 
 
-@pytest.mark.parametrize("name", FEEDS)
+@pytest.mark.parametrize("name", RESTATED)
 def test_reader_rebuilds_the_restated_timetable(name, loaded):
     """Same routes (stops, pickup / drop-off flags, class, section flags),
     same transports (names, UTC traffic days, UTC times) and the same
@@ -79,13 +81,22 @@ def test_reader_rebuilds_the_restated_timetable(name, loaded):
     assert locs(got) == locs(want)
 
 
-@pytest.mark.parametrize("case", [c for c in CASES["cases"] if c["timetable"] in CASES["gtfs_feeds"]],
-                         ids=lambda c: c["name"])
+@pytest.mark.parametrize("case", ALL_CASES, ids=lambda c: c["name"])
 def test_golden_cases_on_read_feeds(case, loaded):
     tt = loaded[case["timetable"]]
     q = F.FixtureQuery(A.lib(), tt, case["query"])
     r = oracle_lib.OracleResult(tt.desc, q.q)
     assert F.journeys_to_records(tt, r.view) == F.strip_expected(case["expected"])
+
+
+@pytest.mark.parametrize("case", CASES["gtfs_cases"], ids=lambda c: c["name"])
+def test_pong_on_read_feeds_in_window(case, loaded):
+    """The harness check of test/raptor_search.cc for the feed-only cases."""
+    tt = loaded[case["timetable"]]
+    qd = dict(case["query"], algorithm="pong")
+    r = oracle_lib.OracleResult(tt.desc, F.FixtureQuery(A.lib(), tt, qd).q)
+    got = F.journeys_to_records(tt, r.view)
+    assert F.in_window(qd, got) == F.in_window(qd, F.strip_expected(case["expected"]))
 
 
 def test_python_reader_reads_a_feed_directory(tmp_path):
@@ -126,7 +137,7 @@ def test_golden_cases_on_read_feeds_gpu(loaded):
         tt = loaded[name]
         dtt = R.Timetable(tt.desc, owner=tt)
         eng = R.Engine(dtt, max_slots=32)
-        for c in CASES["cases"]:
+        for c in ALL_CASES:
             if c["timetable"] != name:
                 continue
             q = F.FixtureQuery(A.lib(), tt, c["query"])
