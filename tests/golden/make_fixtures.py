@@ -700,6 +700,8 @@ GTFS_FEEDS = {
 GTFS_ONLY_FEEDS = {
     "gtfs_shortest_fp": ("test/routing/shortest_fp_test.cc", "shortest_fp_files()", 0, {},
                          ["2024-06-07", "2024-06-09"]),
+    "gtfs_egress_bound": ("test/routing/gpu_intermodal_egress_test.cc", "test_files()", 0, {},
+                          ["2024-06-16", "2024-06-19"]),
 }
 
 
@@ -717,6 +719,20 @@ def gtfs_only_cases():
              query=dict(start=c, dest=a, interval=[t("2024-06-07 00:00"), t("2024-06-09 00:00")],
                         direction="bwd", start_mode="intermodal", dest_mode="intermodal")),
     ]
+
+
+def gtfs_only_known_answers():
+    """test/routing/gpu_intermodal_egress_test.cc: the results contain the
+    1-transfer journey leaving the coordinate at 09:55 and arriving 11:00
+    (its EXPECT_TRUE(found)); nigiri's harness runs the query through range
+    RAPTOR and pong."""
+    return [dict(name="intermodal_egress_at_bound", timetable="gtfs_egress_bound",
+                 ref="test/routing/gpu_intermodal_egress_test.cc",
+                 query=dict(start=[["A", 5, 0], ["A2", 5, 0]], dest=[["C", 0, 0]],
+                            interval=[t("2024-06-17 09:45"), t("2024-06-17 10:45")],
+                            direction="fwd", start_mode="intermodal", dest_mode="intermodal",
+                            min_connection_count=1),
+                 contains=[t("2024-06-17 09:55"), t("2024-06-17 11:00"), 1])]
 
 
 def gtfs_feeds(ref_root: str):
@@ -757,6 +773,7 @@ def main(ref_root: str):
         src = open(os.path.join(ref_root, case["ref"])).read()
         gtfs_cases.append(dict(case, expected=parse_journeys(raw_string(src, case["golden"]))))
     doc = {"timetables": TIMETABLES, "cases": out_cases, "gtfs_cases": gtfs_cases,
+           "gtfs_known_answers": gtfs_only_known_answers(),
            "known_answers": known_answers(ref_root), "gtfs_feeds": gtfs_feeds(ref_root),
            "generated_by": "tests/golden/make_fixtures.py"}
     with open(os.path.join(HERE, "cases.json"), "w") as f:

@@ -89,6 +89,16 @@ def test_golden_cases_on_read_feeds(case, loaded):
     assert F.journeys_to_records(tt, r.view) == F.strip_expected(case["expected"])
 
 
+@pytest.mark.parametrize("algo", ["raptor", "pong"])
+@pytest.mark.parametrize("ka", CASES["gtfs_known_answers"], ids=lambda k: k["name"])
+def test_known_answers_on_read_feeds(ka, algo, loaded):
+    tt = loaded[ka["timetable"]]
+    q = F.FixtureQuery(A.lib(), tt, dict(ka["query"], algorithm=algo))
+    r = oracle_lib.OracleResult(tt.desc, q.q)
+    got = [[j["dep"], j["arr"], j["transfers"]] for j in F.journeys_to_records(tt, r.view)]
+    assert ka["contains"] in got, got
+
+
 @pytest.mark.parametrize("case", CASES["gtfs_cases"], ids=lambda c: c["name"])
 def test_pong_on_read_feeds_in_window(case, loaded):
     """The harness check of test/raptor_search.cc for the feed-only cases."""
@@ -144,3 +154,13 @@ def test_golden_cases_on_read_feeds_gpu(loaded):
             res = A.Result()
             assert A.lib().b2r_search_batch(eng.handle, C.byref(q.q), 1, C.byref(res)) == 0
             assert F.journeys_to_records(tt, res) == F.strip_expected(c["expected"]), c["name"]
+        for ka in CASES["gtfs_known_answers"]:
+            if ka["timetable"] != name:
+                continue
+            for algo in ("raptor", "pong"):
+                q = F.FixtureQuery(A.lib(), tt, dict(ka["query"], algorithm=algo))
+                res = A.Result()
+                assert A.lib().b2r_search_batch(eng.handle, C.byref(q.q), 1, C.byref(res)) == 0
+                assert res.status == 0, (ka["name"], algo)
+                got = [[j["dep"], j["arr"], j["transfers"]] for j in F.journeys_to_records(tt, res)]
+                assert ka["contains"] in got, (ka["name"], algo, got)
