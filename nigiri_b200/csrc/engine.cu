@@ -119,10 +119,7 @@ struct b2r_engine {
   // host bookkeeping
   std::vector<uint16_t> gen_query;  // per slot
   std::vector<int64_t> slot_query;  // query index in the current batch, -1 free
-  struct summary_t {
-    uint8_t state, pad[3];
-    uint32_t n_journeys;
-  };
+  using summary_t = b2r::dev::slot_summary;
   summary_t* d_summary{nullptr};
   summary_t* h_summary{nullptr};  // pinned
   uint32_t* h_lbcount{nullptr};   // pinned
@@ -266,25 +263,7 @@ __global__ void k_admit(dev::state st, adm_hdr const* hdr, uint8_t const* payloa
     }
     if (threadIdx.x == 0) atomicOr(&st.lb_mask[s >> 5], 1u << (s & 31));
   }
-  if (h.lb_mode == 3) {
-    // Dijkstra from the seeds (dijkstra.cc:18-67) as a minimum over table
-    // rows: every path of length <= kMaxTravelTime only passes locations
-    // closer than that, so min(seed distance + row) is the capped multi-
-    // source distance.
-    auto const* seeds = reinterpret_cast<uint32_t const*>(payload + h.off_seeds);
-    auto const* tab = st.slots[s].fwd ? st.lb_table_fwd : st.lb_table_bwd;
-    for (auto x = threadIdx.x; x < n_loc; x += blockDim.x) {
-      uint32_t best = 0xFFFFu;
-      for (auto i = 0u; i != h.n_seeds; ++i) {
-        auto const m = seeds[2 * i];
-        auto const d = tab[static_cast<size_t>(m) * n_loc + x];
-        if (d == 0xFFFFu) continue;
-        auto const c = seeds[2 * i + 1] + d;
-        if ((c <= B2R_MAX_TRAVEL_TIME_MIN || x == m) && c < best) best = c;
-      }
-      st.lb[static_cast<size_t>(x) * st.S + s] = static_cast<uint16_t>(best);
-    }
-    __syncthreads();
+  if (h.lb_mode == 3) {  // k_lb_fill has written the column
     if (threadIdx.x == 0) {  // children inherit the parent's bound, in location order
       auto const& T = st.tt;
       for (auto w = 0u; w != T.n_with_children; ++w) {
@@ -302,6 +281,58 @@ __global__ void k_admit(dev::state st, adm_hdr const* hdr, uint8_t const* payloa
   if (!sl.intermodal_dest && !sl.one_to_all) {
     for (auto i = threadIdx.x; i < h.n_dest; i += blockDim.x) {
       atomicOr(&st.D[dests[i].loc * st.G + (s >> 5)], 1u << (s & 31));
+    }
+  }
+}
+
+// Lower bounds from the all-pairs tables for the admissions in lower-bound
+// mode 3: Dijkstra from the seeds (dijkstra.cc:18-67) as a minimum over
+// table rows -- every path of length <= kMaxTravelTime only passes
+// locations closer than that, so min(seed distance + row) is the capped
+// multi-source distance.  blockIdx.y = slot group, blockIdx.x = a tile of
+// 128 locations: the tile's values are computed with the threads over
+// locations (table rows read in order) and written with a warp over the
+// group's slots per location, 64 contiguous bytes of lb.
+struct lb_group {
+  uint32_t g, first, count, pad;
+};
+struct lb_entry {
+  uint32_t lane, n_seeds, fwd, pad;
+  uint64_t off_seeds;
+};
+constexpr uint32_t kLbTile = 128;
+
+__global__ void k_lb_fill(dev::state st, lb_group const* groups, lb_entry const* entries,
+                          uint8_t const* payload) {
+  __shared__ uint16_t tile[32][kLbTile + 2];
+  auto const grp = groups[blockIdx.y];
+  auto const n_loc = st.tt.n_loc;
+  auto const x0 = blockIdx.x * kLbTile;
+  for (auto e = 0u; e != grp.count; ++e) {
+    auto const en = entries[grp.first + e];
+    auto const* seeds = reinterpret_cast<uint32_t const*>(payload + en.off_seeds);
+    auto const* tab = en.fwd ? st.lb_table_fwd : st.lb_table_bwd;
+    for (auto xi = threadIdx.x; xi < kLbTile; xi += blockDim.x) {
+      auto const x = x0 + xi;
+      uint32_t best = 0xFFFFu;
+      if (x < n_loc) {
+        for (auto i = 0u; i != en.n_seeds; ++i) {
+          auto const m = seeds[2 * i];
+          auto const d = tab[static_cast<size_t>(m) * n_loc + x];
+          if (d == 0xFFFFu) continue;
+          auto const c = seeds[2 * i + 1] + d;
+          if ((c <= B2R_MAX_TRAVEL_TIME_MIN || x == m) && c < best) best = c;
+        }
+      }
+      tile[e][xi] = static_cast<uint16_t>(best);
+    }
+  }
+  __syncthreads();
+  for (auto i = threadIdx.x; i < kLbTile * 32u; i += blockDim.x) {
+    auto const xi = i / 32u, e = i % 32u;
+    auto const x = x0 + xi;
+    if (e < grp.count && x < n_loc) {
+      st.lb[static_cast<size_t>(x) * st.S + grp.g * 32u + entries[grp.first + e].lane] = tile[e][xi];
     }
   }
 }
@@ -346,12 +377,6 @@ __global__ void k_retire(dev::state st, uint32_t const* slots, uint32_t n) {
   if (threadIdx.x == 0) st.slots[s].state = dev::S_IDLE;
 }
 
-__global__ void k_summary(dev::state st, b2r_engine::summary_t* out) {
-  auto const s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= st.S) return;
-  out[s].state = st.slots[s].state;
-  out[s].n_journeys = st.slots[s].n_journeys;
-}
 
 // profiling engines: the marked-entry count and cumulative stop visits after
 // route-scan launch `idx`
@@ -445,8 +470,7 @@ void enqueue_superstep(b2r_engine& e, cudaStream_t s) {
   auto const& st = e.st;
   auto const slot_blocks = (e.S + 127) / 128;
   auto const list_blocks = e.sms * 8;
-  dev::k_step_begin<<<list_blocks, 256, 0, s>>>(st);
-  dev::k_ctl_begin<<<slot_blocks, 128, 0, s>>>(st);
+  dev::k_ctl_begin<<<list_blocks, 256, 0, s>>>(st);
   dev::k_sweep<<<e.sms * 16, 256, 0, s>>>(st);
   dev::k_ctl_dest<<<slot_blocks, 128, 0, s>>>(st);
   auto const pair_blocks = e.sms * e.shape.pair_blocks_per_sm;
@@ -472,14 +496,11 @@ void enqueue_superstep(b2r_engine& e, cudaStream_t s) {
   }
   dev::k_list_reached<<<e.sms * 8, 256, 0, s>>>(st);
   dev::k_clear_x<<<list_blocks, 256, 0, s>>>(st);
-  dev::k_reset_x<<<1, 32, 0, s>>>(st);
   dev::k_transfers_pre<<<slot_blocks, 128, 0, s>>>(st);
   dev::k_transfers<<<pair_blocks, 256, 0, s>>>(st);
-  dev::k_intermodal<<<slot_blocks, 128, 0, s>>>(st);
-  dev::k_footpaths_pre<<<slot_blocks, 128, 0, s>>>(st);
+  dev::k_intermodal_fp_pre<<<slot_blocks, 128, 0, s>>>(st);
   dev::k_footpaths<<<pair_blocks, 256, 0, s>>>(st);
-  dev::k_ctl_end<<<slot_blocks, 128, 0, s>>>(st);
-  dev::k_collect<<<slot_blocks, 128, 0, s>>>(st);
+  dev::k_end_collect<<<slot_blocks, 128, 0, s>>>(st);
   cudaEvent_t rc_a = nullptr, rc_b = nullptr;
   if (e.cfg.profile) {
     while (e.prof_rc_used + 2 > e.prof_rc_ev.size()) {
@@ -493,11 +514,10 @@ void enqueue_superstep(b2r_engine& e, cudaStream_t s) {
   }
   dev::k_reconstruct<<<e.sms * e.shape.recon_blocks_per_sm, 128, 0, s>>>(st);
   if (e.cfg.profile) B2R_CUDA(cudaEventRecord(rc_b, s));
-  dev::k_next<<<slot_blocks, 128, 0, s>>>(st);
+  dev::k_next_summary<<<slot_blocks, 128, 0, s>>>(st);
   dev::k_list_marked<<<e.sms * 8, 256, 0, s>>>(st);
-  k_summary<<<slot_blocks, 128, 0, s>>>(st, e.d_summary);
 }
-constexpr uint64_t kLaunchesPerStep = 22;
+constexpr uint64_t kLaunchesPerStep = 17;
 
 // --------------------------------------------------------- admission
 size_t admission_bytes(b2r_engine const& e, prepped_query const& p) {
@@ -651,7 +671,7 @@ struct adm_req {
 void admit(b2r_engine& e, std::vector<adm_req> const& adm, cudaStream_t s) {
   if (adm.empty()) return;
   bool any_device_lb = false;
-  size_t need = adm.size() * (sizeof(adm_hdr) + sizeof(fill_item)) + 256 + 16;
+  size_t need = adm.size() * (sizeof(adm_hdr) + sizeof(fill_item) + sizeof(lb_group) + sizeof(lb_entry)) + 256 + 64;
   for (auto const& r : adm) {
     need += admission_bytes(e, *r.p) + 64 + (r.keep ? r.keep->size() * sizeof(dev::journey_rec) + 16 : 0);
   }
@@ -730,12 +750,38 @@ void admit(b2r_engine& e, std::vector<adm_req> const& adm, cudaStream_t s) {
     if ((r.flags & kAdmFillRows) != 0u) fills.push_back({r.slot, r.flags & kAdmFillRows});
   }
   auto const off_fills = put(fills.data(), fills.size() * sizeof(fill_item));
+  // lower-bound mode 3 admissions by slot group
+  std::vector<lb_entry> lb_entries;
+  std::vector<lb_group> lb_groups;
+  {
+    std::vector<std::pair<uint32_t, uint32_t>> by_slot;  // (slot, admission)
+    for (auto i = 0U; i != adm.size(); ++i) {
+      if (hdr[i].lb_mode == 3) by_slot.emplace_back(adm[i].slot, i);
+    }
+    std::sort(by_slot.begin(), by_slot.end());
+    for (auto const& [slot, i] : by_slot) {
+      auto const g = slot / 32U;
+      if (lb_groups.empty() || lb_groups.back().g != g) {
+        lb_groups.push_back({g, static_cast<uint32_t>(lb_entries.size()), 0U, 0U});
+      }
+      ++lb_groups.back().count;
+      lb_entries.push_back({slot % 32U, hdr[i].n_seeds, adm[i].p->fwd ? 1U : 0U, 0U, hdr[i].off_seeds});
+    }
+  }
+  auto const off_lb_groups = put(lb_groups.data(), lb_groups.size() * sizeof(lb_group));
+  auto const off_lb_entries = put(lb_entries.data(), lb_entries.size() * sizeof(lb_entry));
   e.h2d_bytes += off;
   B2R_CUDA(cudaMemcpyAsync(e.d_adm, e.h_adm, off, cudaMemcpyHostToDevice, s));
   if (!fills.empty()) {
     auto const bx = std::min<uint32_t>((e.tt->d.n_loc + 255u) / 256u, static_cast<uint32_t>(e.sms) * 2u);
     k_fill_bounds<<<dim3(bx, static_cast<unsigned>(fills.size())), 256, 0, s>>>(
         e.st, reinterpret_cast<fill_item const*>(e.d_adm + off_fills));
+    B2R_CUDA(cudaGetLastError());
+  }
+  if (!lb_groups.empty()) {
+    k_lb_fill<<<dim3((e.tt->d.n_loc + kLbTile - 1) / kLbTile, static_cast<unsigned>(lb_groups.size())), 256, 0,
+                s>>>(e.st, reinterpret_cast<lb_group const*>(e.d_adm + off_lb_groups),
+                     reinterpret_cast<lb_entry const*>(e.d_adm + off_lb_entries), e.d_adm);
     B2R_CUDA(cudaGetLastError());
   }
   k_admit<<<static_cast<unsigned>(adm.size()), 256, 0, s>>>(
@@ -1987,6 +2033,7 @@ int b2r_engine_create(b2r_timetable* tt, const b2r_engine_config* cfg_in, b2r_en
       al(st.tad_phase, S);
       al(st.status_word, 4);
       al(e->d_summary, S);
+      st.summary = e->d_summary;
       al(st.prof, 8);
       al(st.dist, static_cast<size_t>(nl) * S);
       al(st.F[0], static_cast<size_t>(nl) * G);

@@ -181,6 +181,12 @@ struct tl_entry {  // time_at_dest timeline of one phase
   int32_t tad;
 };
 
+// what the host reads of every slot after a super-step chunk
+struct slot_summary {
+  uint8_t state, pad[3];
+  uint32_t n_journeys;
+};
+
 // engine state: every device array in one POD passed by value
 struct state {
   dtt tt;
@@ -229,6 +235,7 @@ struct state {
   // pong bounds (raptor_state::bounds_storage_): rows of the ping's round
   // times folded over the rounds, as keys of the bounded (pong) search
   int16_t* bounds;  // [K][n_loc][S]
+  slot_summary* summary;  // [S]
 };
 
 // ------------------------------------------------------------- helpers

@@ -86,28 +86,32 @@ __device__ __forceinline__ void update_tad(slot_t& sl, uint32_t k, int key) {  /
 }
 
 // ----------------------------------------------------------- control
-__global__ void k_step_begin(state st) {
+// Start of a super-step: the route-reached marks of the last one cleared
+// (all threads), and per slot (threads < S, a warp per slot group) the lane
+// view and the group's run / sweep masks, written whole from ballots.  The
+// reached-list counter is reset by k_ctl_dest, after every thread here has
+// read it.
+__global__ void k_ctl_begin(state st) {
   auto const tid = blockIdx.x * blockDim.x + threadIdx.x;
   auto const ny = st.counters[C_Y];
   for (auto i = tid; i < ny; i += gridDim.x * blockDim.x) st.Y[st.ylist[i]] = 0u;
-  if (tid < st.G) {
-    st.run_mask[tid] = 0u;
-    st.sweep_mask[tid] = 0u;
-    st.any_mask[tid] = 0u;
-  }
-}
-
-__global__ void k_ctl_begin(state st) {
-  auto const s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s == 0) {
-    st.counters[C_Y] = 0u;
+  if (tid == 0) {
     st.counters[C_R] = 0u;
     st.counters[C_RECON] = 0u;
   }
-  if (s >= st.S) return;
+  if ((tid & ~31u) >= st.S) return;  // whole warps: S is a multiple of 32
+  auto const s = tid;
   auto& sl = st.slots[s];
   lane_t ln{};
-  if (sl.state == S_RUN) {
+  auto const run = sl.state == S_RUN;
+  auto const run_bits = __ballot_sync(kFull, run);
+  auto const sweep_bits = __ballot_sync(kFull, run && sl.need_sweep);
+  if ((s & 31u) == 0u) {
+    st.run_mask[s >> 5] = run_bits;
+    st.sweep_mask[s >> 5] = sweep_bits;
+    st.any_mask[s >> 5] = 0u;
+  }
+  if (run) {
     ln.run = 1;
     ln.fwd = sl.fwd;
     ln.k = sl.k;
@@ -121,8 +125,6 @@ __global__ void k_ctl_begin(state st) {
     ln.claszes = sl.allowed_claszes;
     ln.req = sl.req_flags;
     ln.blast = sl.blast;
-    atomicOr(&st.run_mask[s >> 5], 1u << (s & 31));
-    if (sl.need_sweep) atomicOr(&st.sweep_mask[s >> 5], 1u << (s & 31));
     ++sl.n_rounds;
   }
   st.lanes[s] = ln;
@@ -154,6 +156,7 @@ __global__ void k_sweep(state st) {
 // destination times into time_at_dest (raptor.h:224-226)
 __global__ void k_ctl_dest(state st) {
   auto const s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s == 0) st.counters[C_Y] = 0u;  // k_ctl_begin has cleared the listed words
   if (s >= st.S) return;
   auto& sl = st.slots[s];
   if (sl.state != S_RUN || sl.one_to_all) return;
@@ -396,9 +399,6 @@ __global__ void k_clear_x(state st) {
   for (auto i = tid; i < nx; i += gridDim.x * blockDim.x) st.X[st.xlist[i]] = 0u;
 }
 
-__global__ void k_reset_x(state st) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) st.counters[C_X] = 0u;
-}
 
 // ---------------------------------------------------- transfer phase
 // Destination stations of station-to-station queries first, in location
@@ -407,6 +407,7 @@ __global__ void k_reset_x(state st) {
 // those updates is kept per query.
 __global__ void k_transfers_pre(state st) {
   auto const s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s == 0) st.counters[C_X] = 0u;  // k_clear_x has cleared the listed marks
   if (s >= st.S) return;
   auto& sl = st.slots[s];
   auto const ln = st.lanes[s];
@@ -490,9 +491,7 @@ __global__ void k_transfers(state st) {
 
 // update_intermodal_footpaths, raptor.h:954-1026: per query, its egress
 // stations in location order
-__global__ void k_intermodal(state st) {
-  auto const s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= st.S) return;
+__device__ void intermodal_slot(state const& st, uint32_t s) {
   auto const ln = st.lanes[s];
   if (!ln.run || !(ln.mode & 1u)) return;
   auto& sl = st.slots[s];
@@ -520,9 +519,7 @@ struct fp_cand {
 
 // footpaths into destination stations, in the reference's processing order
 // (source location, then position in the source's footpath list)
-__global__ void k_footpaths_pre(state st) {
-  auto const s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= st.S) return;
+__device__ void footpaths_pre_slot(state const& st, uint32_t s) {
   auto& sl = st.slots[s];
   auto const ln = st.lanes[s];
   st.timeline_n[s] = 0u;
@@ -595,6 +592,15 @@ __global__ void k_footpaths_pre(state st) {
   st.timeline_n[s] = tl_n;
 }
 
+// update_intermodal_footpaths, then the footpaths into destination
+// stations, per slot (the order of raptor.h:376-378)
+__global__ void k_intermodal_fp_pre(state st) {
+  auto const s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= st.S) return;
+  intermodal_slot(st, s);
+  footpaths_pre_slot(st, s);
+}
+
 // update_footpaths, raptor.h:745-845: lane per reached (station, query),
 // walking the station's footpaths; labels of footpath targets are combined
 // with atomicMin (the phase's final labels and marks do not depend on the
@@ -642,9 +648,7 @@ __global__ void k_footpaths(state st) {
 }
 
 // ------------------------------------------------- round end / results
-__global__ void k_ctl_end(state st) {
-  auto const s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= st.S) return;
+__device__ void ctl_end_slot(state const& st, uint32_t s) {
   auto& sl = st.slots[s];
   if (sl.state != S_RUN) return;
   sl.k = static_cast<uint8_t>(sl.k + 1);
@@ -701,9 +705,7 @@ __device__ bool pareto_add(state const& st, uint32_t s, slot_t& sl, journey_rec 
 
 // result collection (raptor.h:393-413) and the reconstruction worklist
 // (search.h:457-475)
-__global__ void k_collect(state st) {
-  auto const s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= st.S) return;
+__device__ void collect_slot(state const& st, uint32_t s) {
   auto& sl = st.slots[s];
   if (sl.state != S_COLLECT || sl.one_to_all) return;
   auto const qtag = tagcode(sl.gen_query);
@@ -739,6 +741,14 @@ __global__ void k_collect(state st) {
       st.recon_list[atomicAdd(&st.counters[C_RECON], 1u)] = (s << 16) | i;
     }
   }
+}
+
+// end of the round, then result collection when the group's rounds are done
+__global__ void k_end_collect(state st) {
+  auto const s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= st.S) return;
+  ctl_end_slot(st, s);
+  collect_slot(st, s);
 }
 
 __global__ void k_reconstruct(state st) {
@@ -788,9 +798,7 @@ __global__ void k_reconstruct(state st) {
 // early termination (search.h:477-492) and seeding of the next start-time
 // group: next_start_time + add_start (raptor.h:179-203) + the
 // time_at_dest bound of execute (raptor.h:211-214)
-__global__ void k_next(state st) {
-  auto const s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= st.S) return;
+__device__ void next_slot(state const& st, uint32_t s) {
   auto& sl = st.slots[s];
   if (sl.state != S_COLLECT && sl.state != S_START) return;
   auto const fwd = sl.fwd != 0;
@@ -848,6 +856,15 @@ __global__ void k_next(state st) {
   sl.k = 1;
   sl.state = S_RUN;
   ++sl.n_groups_run;
+}
+
+// the next start-time group, then the slot's state for the host
+__global__ void k_next_summary(state st) {
+  auto const s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= st.S) return;
+  next_slot(st, s);
+  auto const& sl = st.slots[s];
+  st.summary[s] = {sl.state, {0, 0, 0}, sl.n_journeys};
 }
 
 // ------------------------------------------------------- lower bounds
