@@ -174,7 +174,7 @@ typedef struct b2r_offset {
 } b2r_offset;
 
 /* routing::query, query.h:70-100, restricted to the static (no rtt, no
- * vias, no td offsets, no filters, profile 0) instantiation. */
+ * vias, no td offsets, profile 0) instantiation. */
 typedef struct b2r_query {
   uint8_t kind;      /* b2r_query_kind */
   uint8_t direction; /* b2r_direction */
@@ -213,6 +213,13 @@ typedef struct b2r_query {
   /* B2R_ALGO_RAPTOR: routing::raptor_search (search<raptor>, raptor_search.cc);
    * B2R_ALGO_PONG: routing::pong_search (pong.cc:63-475), one-to-one only */
   uint8_t algorithm;
+  /* query::max_interval_ (query.h:89): when set, every search interval the
+   * interval estimator produces (interval_estimate.h:138-146) is clamped
+   * into [max_interval_from, max_interval_to] (unixtime minutes) */
+  uint8_t has_max_interval;
+  uint8_t pad2_[3];
+  int32_t max_interval_from;
+  int32_t max_interval_to;
 } b2r_query;
 
 /* Fill a query with nigiri's defaults (query.h:84-99). */
@@ -510,7 +517,7 @@ typedef struct b2r_gtfs_config {
   uint16_t bikes_allowed_default;         /* bit c: trips of class c carry bikes unless trips.txt says */
   uint16_t cars_allowed_default;
   uint16_t reservation_not_required_default;
-  uint16_t pad_;
+  uint16_t link_stop_distance;            /* metres: stops this close are linked by footpaths (100) */
   const char* default_tz;                 /* used when agency.txt names none */
   const char* tzdata_dir;                 /* NULL: /usr/share/zoneinfo */
 } b2r_gtfs_config;

@@ -90,6 +90,7 @@ struct query {
   unsigned min_connection_count_{0U};
   bool extend_interval_earlier_{false};
   bool extend_interval_later_{false};
+  std::optional<interval> max_interval_{};  // clamp of every interval extension
   std::optional<duration_t> fastest_direct_{};
   double fastest_direct_factor_{1.0};
   transfer_time_settings transfer_time_settings_{};
@@ -210,6 +211,11 @@ struct c_query {
     c.use_start_footpaths = q.use_start_footpaths_ ? 1 : 0;
     c.extend_interval_earlier = q.extend_interval_earlier_ ? 1 : 0;
     c.extend_interval_later = q.extend_interval_later_ ? 1 : 0;
+    if (q.max_interval_) {
+      c.has_max_interval = 1;
+      c.max_interval_from = q.max_interval_->from_;
+      c.max_interval_to = q.max_interval_->to_;
+    }
     c.start = start.data();
     c.n_start = static_cast<uint32_t>(start.size());
     c.destination = dest.data();

@@ -62,7 +62,7 @@ class GtfsConfig(C.Structure):
         ("date_range_from", C.c_int32), ("date_range_to", C.c_int32),
         ("default_transfer_time", C.c_uint32),
         ("bikes_allowed_default", C.c_uint16), ("cars_allowed_default", C.c_uint16),
-        ("reservation_not_required_default", C.c_uint16), ("pad_", C.c_uint16),
+        ("reservation_not_required_default", C.c_uint16), ("link_stop_distance", C.c_uint16),
         ("default_tz", C.c_char_p), ("tzdata_dir", C.c_char_p),
     ]
 
@@ -91,6 +91,8 @@ class Query(C.Structure):
         ("allowed_claszes", C.c_uint32), ("require_bike_transport", C.c_uint8),
         ("require_car_transport", C.c_uint8), ("no_compulsory_reservation", C.c_uint8),
         ("algorithm", C.c_uint8),
+        ("has_max_interval", C.c_uint8), ("pad2_", C.c_uint8 * 3),
+        ("max_interval_from", C.c_int32), ("max_interval_to", C.c_int32),
     ]
 
 

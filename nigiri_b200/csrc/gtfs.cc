@@ -4,10 +4,11 @@
 // stops with parents, routes (route_type -> transport class), trips with
 // blocks and bike / car / reservation flags, stop times with pickup and
 // drop-off restrictions, calendar and calendar_dates, and transfers.txt
-// (minimum transfer times, footpaths).  Not restated: frequencies, flex,
-// shapes, fares, translations, stay-seated transfers (transfer_type 4),
-// footpaths and equivalences from stop proximity or equal names, and the
-// footpath closure of build_footpaths.
+// (minimum transfer times, footpaths, stay-seated transfers joining trips
+// into one transport), footpaths between nearby and same-named stops, and
+// the footpath closure that finalize() builds.  Not restated: frequencies,
+// flex, shapes, fares, translations, location equivalences and the merging
+// of duplicate trips.
 #include <algorithm>
 #include <array>
 #include <cmath>
@@ -15,7 +16,10 @@
 #include <cstring>
 #include <fstream>
 #include <map>
+#include <limits>
 #include <optional>
+#include <queue>
+#include <set>
 #include <sstream>
 #include <string>
 #include <unordered_map>
@@ -30,6 +34,19 @@ namespace {
 
 constexpr uint32_t kNoParent = 0xFFFFFFFFu;
 constexpr uint32_t kSpecial = 9;  // special stations (special_stations.h:7-19)
+
+// geo::approx_squared_distance with approx_distance_lng_degrees (the geo
+// library, motis-project/geo at commit 7c78f91a, which the reference tree
+// does not carry): an equirectangular approximation, squared metres, the
+// longitude difference scaled at the first point's latitude.  Restated on a
+// sphere of radius 6,371 km.
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kMetersPerDegree = kPi * 6371000.0 / 180.0;
+double approx_squared_distance(std::pair<double, double> const& a, std::pair<double, double> const& b) {
+  auto const y = (a.first - b.first) * kMetersPerDegree;
+  auto const x = (a.second - b.second) * kMetersPerDegree * std::cos(a.first * kPi / 180.0);
+  return x * x + y * y;
+}
 
 // ------------------------------------------------------------------ CSV
 struct csv {
@@ -291,6 +308,14 @@ struct bits512 {
     return r;
   }
   bool operator<(bits512 const& o) const { return w < o.w; }
+  // std::bitset shift: bit i moves to bit i + n (to i - |n| for n < 0)
+  bits512 shifted(int n) const {
+    bits512 r;
+    for (auto i = 0; i != 512; ++i) {
+      if (test(static_cast<uint32_t>(i)) && i + n >= 0 && i + n < 512) r.set(static_cast<uint32_t>(i + n));
+    }
+    return r;
+  }
 };
 
 struct event {
@@ -373,7 +398,11 @@ bool load_gtfs(std::map<std::string, std::string> const& files, b2r_gtfs_config 
   // order (the reference registers in its hash map's order)
   auto const st = file("stops.txt");
   std::unordered_map<std::string, uint32_t> loc_of;
-  std::vector<std::string> ids, parent_ids;
+  std::vector<std::string> ids, parent_ids, names;
+  std::vector<std::pair<double, double>> coords;  // (lat, lng), clamped
+  auto const coordinate = [](std::string const& x, double lim) {
+    return std::clamp(x.empty() ? 0.0 : std::strtod(x.c_str(), nullptr), -lim, lim);
+  };
   for (auto r = size_t{0}; r != st.rows.size(); ++r) {
     auto const lt = st.get(r, st.col("location_type"));
     if (lt == "2" || lt == "3") continue;
@@ -382,12 +411,17 @@ bool load_gtfs(std::map<std::string, std::string> const& files, b2r_gtfs_config 
     loc_of[id] = kSpecial + static_cast<uint32_t>(ids.size());
     ids.push_back(id);
     parent_ids.push_back(st.get(r, st.col("parent_station")));
+    names.push_back(st.get(r, st.col("stop_name")));
+    coords.emplace_back(coordinate(st.get(r, st.col("stop_lat")), 90.0),
+                        coordinate(st.get(r, st.col("stop_lon")), 180.0));
   }
   for (auto const& p : parent_ids) {  // parents named only as parent_station
     if (!p.empty() && !loc_of.contains(p)) {
       loc_of[p] = kSpecial + static_cast<uint32_t>(ids.size());
       ids.push_back(p);
       parent_ids.emplace_back();
+      names.emplace_back();
+      coords.emplace_back(0.0, 0.0);
     }
   }
   auto const n_loc = kSpecial + static_cast<uint32_t>(ids.size());
@@ -399,20 +433,22 @@ bool load_gtfs(std::map<std::string, std::string> const& files, b2r_gtfs_config 
       loc_type[kSpecial + i] = B2R_LOC_TRACK;
     }
   }
-  // transfers.txt, type 2 (stop.cc:140-205): the minimum transfer time of a
-  // stop with itself, footpaths between stops, both in whole minutes
+  // transfers.txt (read_transfers, stop.cc:124-205): every row but types 3
+  // (not possible) and 4 (stay seated, read with the trips) gives the
+  // minimum transfer time of a stop with itself or a footpath between two
+  // stops, in whole minutes; empty fields read as 0
   std::vector<std::optional<int>> transfer(n_loc);
   std::vector<std::vector<std::pair<uint32_t, int>>> fps(n_loc);
+  auto const int_field = [](std::string const& x) { return x.empty() ? 0 : std::stoi(x); };
   {
     auto const tr = file("transfers.txt");
     for (auto r = size_t{0}; r != tr.rows.size(); ++r) {
-      if (tr.get(r, tr.col("transfer_type")) != "2") continue;
-      auto const mt = tr.get(r, tr.col("min_transfer_time"));
-      if (mt.empty()) continue;
+      auto const type = int_field(tr.get(r, tr.col("transfer_type")));
+      if (type == 3 || type == 4) continue;
       auto const a = loc_of.find(tr.get(r, tr.col("from_stop_id")));
       auto const b = loc_of.find(tr.get(r, tr.col("to_stop_id")));
       if (a == loc_of.end() || b == loc_of.end()) continue;
-      auto const minutes = std::stoi(mt) / 60;
+      auto const minutes = int_field(tr.get(r, tr.col("min_transfer_time"))) / 60;
       if (a->second == b->second) {
         auto& t = transfer[a->second];
         t = t.has_value() ? std::min(*t, minutes) : minutes;
@@ -430,6 +466,89 @@ bool load_gtfs(std::map<std::string, std::string> const& files, b2r_gtfs_config 
         if (std::none_of(back.begin(), back.end(), [&](auto const& x) { return x.first == l; })) {
           back.emplace_back(l, d);
         }
+      }
+    }
+  }
+
+  // Footpaths between a stop and its "metas" (stop::get_metas and
+  // read_stops, stop.cc:30-95, 380-402): itself, the stops of the same name,
+  // and -- unless it lies within 2 degrees of (0, 0) -- the stops within
+  // link_stop_distance; closed under parents and children; members farther
+  // than 500 m (2000 m for its own parent or child) dropped; the children of
+  // the rest added.  Each gets a walk of max(2, ceil(distance / 1.5 m/s))
+  // minutes both ways, unless a footpath to that stop exists.
+  {
+    auto const n_stops = static_cast<uint32_t>(ids.size());
+    auto const sq_dist = [&](uint32_t a, uint32_t b) { return approx_squared_distance(coords[a], coords[b]); };
+    std::vector<std::vector<uint32_t>> children(n_stops);
+    for (auto i = 0U; i != n_stops; ++i) {
+      if (parent[kSpecial + i] != kNoParent) children[parent[kSpecial + i] - kSpecial].push_back(i);
+    }
+    auto const parent_of = [&](uint32_t i) {
+      return parent[kSpecial + i] == kNoParent ? kNoParent : parent[kSpecial + i] - kSpecial;
+    };
+    std::unordered_map<std::string, std::vector<uint32_t>> same_name;
+    for (auto i = 0U; i != n_stops; ++i) {
+      if (!names[i].empty()) same_name[names[i]].push_back(i);
+    }
+    // stops by 0.002-degree cell, for the link_stop_distance radius search
+    constexpr double kCell = 0.002;
+    auto const cell = [&](double x) { return static_cast<int64_t>(std::floor(x / kCell)); };
+    std::map<std::pair<int64_t, int64_t>, std::vector<uint32_t>> grid;
+    for (auto i = 0U; i != n_stops; ++i) grid[{cell(coords[i].first), cell(coords[i].second)}].push_back(i);
+    auto const link = static_cast<double>(cfg.link_stop_distance);
+    auto const close = [&](uint32_t s, std::vector<uint32_t>& out) {
+      auto const [lat, lng] = coords[s];
+      if (cfg.link_stop_distance == 0U || (std::abs(lat) < 2.0 && std::abs(lng) < 2.0)) return;
+      auto const dlat = static_cast<int64_t>(std::ceil(link / kMetersPerDegree / kCell)) + 1;
+      auto const cosl = std::max(std::cos(lat * kPi / 180.0), 1e-3);
+      auto const dlng = std::min<int64_t>(static_cast<int64_t>(std::ceil(link / (kMetersPerDegree * cosl) / kCell)) + 1,
+                                          static_cast<int64_t>(360.0 / kCell));
+      for (auto y = cell(lat) - dlat; y <= cell(lat) + dlat; ++y) {
+        for (auto x = cell(lng) - dlng; x <= cell(lng) + dlng; ++x) {
+          auto const it = grid.find({y, x});
+          if (it == grid.end()) continue;
+          for (auto const j : it->second) {
+            if (sq_dist(s, j) <= link * link) out.push_back(j);
+          }
+        }
+      }
+    };
+    auto const add_if_not_exists = [&](uint32_t from, uint32_t to, int d) {
+      auto& v = fps[from];
+      if (std::none_of(v.begin(), v.end(), [&](auto const& x) { return x.first == to; })) v.emplace_back(to, d);
+    };
+    for (auto s = 0U; s != n_stops; ++s) {
+      std::vector<uint32_t> start{s};
+      if (!names[s].empty()) {
+        auto const& eq = same_name[names[s]];
+        start.insert(start.end(), eq.begin(), eq.end());
+      }
+      close(s, start);
+      std::set<uint32_t> todo(start.begin(), start.end()), done;
+      while (!todo.empty()) {
+        auto const next = *todo.begin();
+        todo.erase(todo.begin());
+        done.insert(next);
+        if (auto const p = parent_of(next); p != kNoParent && !done.contains(p)) todo.insert(p);
+        for (auto const c : children[next]) {
+          if (!done.contains(c)) todo.insert(c);
+        }
+      }
+      std::set<uint32_t> metas;
+      for (auto const m : done) {
+        auto const family = parent_of(s) == m || parent_of(m) == s;
+        auto const d2 = sq_dist(s, m);
+        if ((d2 > 500.0 * 500.0 && !family) || d2 > 2000.0 * 2000.0) continue;
+        metas.insert(m);
+      }
+      for (auto const m : std::set<uint32_t>(metas)) metas.insert(children[m].begin(), children[m].end());
+      for (auto const m : metas) {
+        auto const dist = std::sqrt(sq_dist(s, m));
+        auto const minutes = std::max(2, static_cast<int>(std::ceil((dist / 1.5) / 60.0)));
+        if (minutes > 511) continue;  // footpath::kMaxDuration
+        add_if_not_exists(kSpecial + s, kSpecial + m, minutes);
+        add_if_not_exists(kSpecial + m, kSpecial + s, minutes);
       }
     }
   }
@@ -531,8 +650,29 @@ bool load_gtfs(std::map<std::string, std::string> const& files, b2r_gtfs_config 
     }
   }
 
+  // transfers.txt, type 4 (stop.cc:156-165, load_timetable.cc:212-242):
+  // stay-seated transfers from trip to trip, each pair once, in file order
+  std::vector<std::vector<uint32_t>> seated_in(trips.size()), seated_out(trips.size());
+  {
+    auto const tr = file("transfers.txt");
+    auto const push_unique = [](std::vector<uint32_t>& v, uint32_t x) {
+      if (std::find(v.begin(), v.end(), x) == v.end()) v.push_back(x);
+    };
+    for (auto r = size_t{0}; r != tr.rows.size(); ++r) {
+      if (int_field(tr.get(r, tr.col("transfer_type"))) != 4) continue;
+      auto const a = trip_of.find(tr.get(r, tr.col("from_trip_id")));
+      auto const b = trip_of.find(tr.get(r, tr.col("to_trip_id")));
+      if (a == trip_of.end() || b == trip_of.end() || trips[a->second].bad || trips[b->second].bad) continue;
+      push_unique(seated_in[b->second], a->second);
+      push_unique(seated_out[a->second], b->second);
+    }
+  }
+  auto const has_seated = [&](uint32_t i) { return !seated_in[i].empty() || !seated_out[i].empty(); };
+
   // block::rule_services, trip.cc:31-106: chains of a block's trips whose
-  // first stop is the previous one's last stop, on the days all run
+  // first stop is the previous one's last stop, on the days all run.  Trips
+  // with stay-seated transfers are joined by the seated pass below; a block
+  // holding one builds its other trips alone (load_timetable.cc:335-360).
   struct combination {
     std::vector<uint32_t> trips;
     bits512 days;
@@ -543,7 +683,8 @@ bool load_gtfs(std::map<std::string, std::string> const& files, b2r_gtfs_config 
   for (auto i = 0U; i != trips.size(); ++i) {
     if (trips[i].bad) continue;
     if (trips[i].block.empty()) {
-      combos.push_back({{i}, trips[i].service});  // non-block trips first (load_timetable.cc:321-333)
+      // non-block trips first (load_timetable.cc:321-333)
+      if (!has_seated(i)) combos.push_back({{i}, trips[i].service});
     } else {
       if (!blocks.contains(trips[i].block)) block_order.push_back(trips[i].block);
       blocks[trips[i].block].push_back(i);
@@ -552,6 +693,12 @@ bool load_gtfs(std::map<std::string, std::string> const& files, b2r_gtfs_config 
   auto const loc_of_word = [](uint32_t w) { return w & 0x0FFFFFFFu; };
   for (auto const& b : block_order) {
     auto rule = blocks[b];
+    if (std::any_of(rule.begin(), rule.end(), has_seated)) {
+      for (auto const t : rule) {
+        if (!has_seated(t)) combos.push_back({{t}, trips[t].service});
+      }
+      continue;
+    }
     if (rule.size() == 1U) {
       combos.push_back({{rule.front()}, trips[rule.front()].service});
       continue;
@@ -593,7 +740,7 @@ bool load_gtfs(std::map<std::string, std::string> const& files, b2r_gtfs_config 
 
   // expand_local_to_utc, local_to_utc.h:130-240, and get_stop_seq (:245-270)
   std::vector<utc_trip> utc;
-  for (auto const& c : combos) {
+  auto const expand = [&](combination const& c, std::vector<utc_trip>& out) {
     auto const& first = trips[c.trips.front()];
     auto const first_dep = first.events.front().dep;
     auto const last_arr = trips[c.trips.back()].events.back().arr;
@@ -643,7 +790,143 @@ bool load_gtfs(std::map<std::string, std::string> const& files, b2r_gtfs_config 
           u.stop_seq.insert(u.stop_seq.end(), t.stops.begin() + 1, t.stops.end());
         }
       }
-      utc.push_back(std::move(u));
+      out.push_back(std::move(u));
+    }
+  };
+  for (auto const& c : combos) expand(c, utc);
+
+  // stay-seated transfers: expand_seated_trips (seated.h:29-66) and
+  // build_seated_trips (seated.cc:14-290).  Every trip with a seated
+  // transfer is expanded alone; then, repeatedly from the first expansion
+  // that has traffic days left:
+  //  1. the component: expansions linked by seated transfers (with a dwell
+  //     under two hours), each with its day offset against the first, while
+  //     the offset-aligned traffic days of all members still intersect;
+  //  2. its entries: members with no incoming transfer inside it;
+  //  3. depth-first from each entry along the outgoing transfers, appending
+  //     the next trip's times (shifted by the day offsets) and its stops after
+  //     the first -- the joint stop stays the arriving trip's last stop -- and
+  //     emitting a transport wherever no transfer continues;
+  //  4. the component's days are taken off its members.
+  // The reference takes queued expansions in hash-map order; this reader
+  // takes the lowest index first.
+  {
+    std::vector<int> rule_of(trips.size(), -1);
+    std::vector<uint32_t> rule_trip;  // rule index -> trip
+    for (auto i = 0U; i != trips.size(); ++i) {
+      if (!trips[i].bad && has_seated(i)) {
+        rule_of[i] = static_cast<int>(rule_trip.size());
+        rule_trip.push_back(i);
+      }
+    }
+    std::vector<utc_trip> rem;           // expansions
+    std::vector<uint32_t> rem_rule;      // expansion -> rule index
+    std::vector<std::vector<uint32_t>> rule_rems(rule_trip.size());
+    for (auto r = 0U; r != rule_trip.size(); ++r) {
+      std::vector<utc_trip> x;
+      expand({{rule_trip[r]}, trips[rule_trip[r]].service}, x);
+      for (auto& u : x) {
+        rule_rems[r].push_back(static_cast<uint32_t>(rem.size()));
+        rem_rule.push_back(r);
+        rem.push_back(std::move(u));
+      }
+    }
+    auto const rules = [&](std::vector<uint32_t> const& ts) {
+      std::vector<uint32_t> out;
+      for (auto const t : ts) out.push_back(static_cast<uint32_t>(rule_of[t]));
+      return out;
+    };
+    std::vector<std::vector<uint32_t>> in_r(rule_trip.size()), out_r(rule_trip.size());
+    for (auto r = 0U; r != rule_trip.size(); ++r) {
+      in_r[r] = rules(seated_in[rule_trip[r]]);
+      out_r[r] = rules(seated_out[rule_trip[r]]);
+    }
+    auto const first_dep = [&](uint32_t x) { return rem[x].times.front(); };
+    auto const last_arr = [&](uint32_t x) { return rem[x].times.back(); };
+    auto const day_change_offset = [&](uint32_t a, uint32_t b) {
+      return (last_arr(a) / 1440 - first_dep(a) / 1440) + (last_arr(a) % 1440 > first_dep(b) ? 1 : 0);
+    };
+    auto const valid_dwell = [&](uint32_t a, uint32_t b) {
+      auto diff = first_dep(b) - last_arr(a) % 1440;
+      if (diff < 0) diff += 1440;
+      return diff < 120;
+    };
+    std::vector<bool> has_bits(rem.size(), true);
+    for (auto next = 0U; next < rem.size();) {
+      if (!has_bits[next]) {
+        ++next;
+        continue;
+      }
+      // 1. the component (expansion -> day offset)
+      std::map<uint32_t, int> component;
+      auto comp_days = rem[next].days;
+      std::map<uint32_t, int> q{{next, 0}};
+      while (!q.empty()) {
+        auto const [cur, offset] = *q.begin();
+        q.erase(q.begin());
+        auto const both = rem[cur].days.shifted(-offset) & comp_days;
+        if (!both.any()) continue;
+        comp_days = both;
+        component.emplace(cur, offset);
+        for (auto const o : out_r[rem_rule[cur]]) {
+          for (auto const x : rule_rems[o]) {
+            if (component.contains(x) || !valid_dwell(cur, x)) continue;
+            q.emplace(x, offset + day_change_offset(cur, x));
+          }
+        }
+        for (auto const i : in_r[rem_rule[cur]]) {
+          for (auto const x : rule_rems[i]) {
+            if (component.contains(x) || !valid_dwell(x, cur)) continue;
+            q.emplace(x, offset - day_change_offset(x, cur));
+          }
+        }
+      }
+      auto const representative = [&](uint32_t rule) -> std::optional<std::pair<uint32_t, int>> {
+        for (auto const& [x, off] : component) {
+          if (rem_rule[x] == rule) return std::pair{x, off};
+        }
+        return std::nullopt;
+      };
+      // 2. entries
+      struct item {
+        utc_trip u;
+        uint32_t rule;
+        int transport_offset;
+      };
+      std::vector<item> stack;
+      for (auto const& [x, off] : component) {
+        auto const& ins = in_r[rem_rule[x]];
+        if (std::any_of(ins.begin(), ins.end(), [&](uint32_t i) { return representative(i).has_value(); })) continue;
+        auto start = rem[x];
+        start.days = comp_days.shifted(off);
+        stack.push_back({std::move(start), rem_rule[x], -off});
+      }
+      // 3. depth-first concatenation (a trip already in the chain ends it, so
+      // that a cycle of transfers cannot loop)
+      while (!stack.empty()) {
+        auto cur = std::move(stack.back());
+        stack.pop_back();
+        auto has_next = false;
+        for (auto const nx : out_r[cur.rule]) {
+          auto const r = representative(nx);
+          if (!r.has_value()) continue;
+          auto const& nr = rem[r->first];
+          if (std::find(cur.u.trips.begin(), cur.u.trips.end(), nr.trips.front()) != cur.u.trips.end()) continue;
+          auto copy = cur.u;
+          copy.trips.push_back(nr.trips.front());
+          for (auto const t : nr.times) copy.times.push_back(t + (cur.transport_offset + r->second) * 1440);
+          copy.stop_seq.insert(copy.stop_seq.end(), nr.stop_seq.begin() + 1, nr.stop_seq.end());
+          copy.sections.insert(copy.sections.end(), nr.sections.begin(), nr.sections.end());
+          stack.push_back({std::move(copy), rem_rule[r->first], cur.transport_offset});
+          has_next = true;
+        }
+        if (!has_next) utc.push_back(std::move(cur.u));
+      }
+      // 4. the days used
+      for (auto const& [x, off] : component) {
+        rem[x].days = rem[x].days & ~comp_days.shifted(off);
+        if (!rem[x].days.any()) has_bits[x] = false;
+      }
     }
   }
 
@@ -694,6 +977,88 @@ bool load_gtfs(std::map<std::string, std::string> const& files, b2r_gtfs_config 
   std::vector<uint8_t> tt_(n_loc, 0);
   for (auto l = kSpecial; l != n_loc; ++l) {
     tt_[l] = static_cast<uint8_t>(transfer[l].value_or(static_cast<int>(cfg.default_transfer_time)));
+  }
+  // build_footpaths' connect_components (build_footpaths.cc:68-345) as
+  // finalize() runs it by default (no walk-speed adjustment, no length
+  // bound): self-walks dropped and one edge kept per target; then in every
+  // connected component of the walk graph each member gets a walk to every
+  // other member, the shortest over edges lengthened to both ends' transfer
+  // times, itself at least both ends' transfer times (a component of two
+  // keeps its edge so lengthened); sorted by duration (sort_footpaths).
+  {
+    constexpr uint32_t kNone = 0xFFFFFFFFu;
+    std::vector<std::vector<std::pair<uint32_t, int>>> g(n_loc);
+    for (auto l = 0U; l != n_loc; ++l) {
+      for (auto const& [to, d] : fps[l]) {
+        if (to == l || std::any_of(g[l].begin(), g[l].end(), [&](auto const& x) { return x.first == to; })) continue;
+        g[l].emplace_back(to, std::min(d, 511));
+      }
+      std::stable_sort(g[l].begin(), g[l].end(), [](auto const& a, auto const& b) { return a.first < b.first; });
+    }
+    std::vector<uint32_t> comp(n_loc, kNone);  // find_components: first visitor's index
+    for (auto i = 0U; i != n_loc; ++i) {
+      if (comp[i] != kNone || g[i].empty()) continue;
+      std::vector<uint32_t> stack{i};
+      while (!stack.empty()) {
+        auto const j = stack.back();
+        stack.pop_back();
+        if (comp[j] == i) continue;
+        comp[j] = i;
+        for (auto const& [to, d] : g[j]) {
+          if (comp[to] != i) stack.push_back(to);
+        }
+      }
+    }
+    std::map<uint32_t, std::vector<uint32_t>> members;
+    for (auto l = 0U; l != n_loc; ++l) {
+      if (comp[l] != kNone) members[comp[l]].push_back(l);
+    }
+    auto const u8 = [](int m) { return std::min(m, 255); };  // u8_minutes
+    std::vector<std::vector<std::pair<uint32_t, int>>> closed(n_loc);
+    for (auto const& [c, ls] : members) {
+      if (ls.size() == 2U) {  // process_2_node_component
+        auto const a = ls[0], b = ls[1];
+        if (!g[a].empty()) closed[a].emplace_back(b, std::max({u8(g[a].front().second), int{tt_[a]}, int{tt_[b]}}));
+        if (!g[b].empty()) closed[b].emplace_back(a, std::max({u8(g[b].front().second), int{tt_[a]}, int{tt_[b]}}));
+        continue;
+      }
+      auto const n = ls.size();
+      auto const local = [&](uint32_t l) {
+        return static_cast<size_t>(std::lower_bound(ls.begin(), ls.end(), l) - ls.begin());
+      };
+      std::vector<std::vector<std::pair<size_t, int>>> adj(n);  // build_component_graph
+      for (auto i = size_t{0}; i != n; ++i) {
+        for (auto const& [to, d] : g[ls[i]]) {
+          auto const j = local(to);
+          auto const w = std::max({int{tt_[ls[i]]}, int{tt_[to]}, u8(d)});
+          adj[i].emplace_back(j, w);
+          adj[j].emplace_back(i, w);
+        }
+      }
+      std::vector<int> dist(n);
+      for (auto i = size_t{0}; i != n; ++i) {  // dijkstra per member
+        std::fill(dist.begin(), dist.end(), std::numeric_limits<int>::max());
+        dist[i] = 0;
+        std::priority_queue<std::pair<int, size_t>, std::vector<std::pair<int, size_t>>, std::greater<>> pq;
+        pq.emplace(0, i);
+        while (!pq.empty()) {
+          auto const [d, u] = pq.top();
+          pq.pop();
+          if (d != dist[u]) continue;
+          for (auto const& [v, w] : adj[u]) {
+            if (d + w < dist[v]) {
+              dist[v] = d + w;
+              pq.emplace(dist[v], v);
+            }
+          }
+        }
+        for (auto j = size_t{0}; j != n; ++j) {
+          if (j == i || dist[j] == std::numeric_limits<int>::max()) continue;
+          closed[ls[i]].emplace_back(ls[j], std::max({u8(std::min(dist[j], 511)), int{tt_[ls[i]]}, int{tt_[ls[j]]}}));
+        }
+      }
+    }
+    fps = std::move(closed);
   }
   std::vector<uint32_t> fp_index(n_loc + 1, 0), fp_data;
   for (auto l = 0U; l != n_loc; ++l) {
@@ -782,6 +1147,7 @@ extern "C" {
 void b2r_gtfs_config_init(b2r_gtfs_config* c) {
   std::memset(c, 0, sizeof(*c));
   c->default_transfer_time = 2;  // loader_config::default_transfer_time_
+  c->link_stop_distance = 100;   // loader_config::link_stop_distance_ (loader_interface.h:18)
 }
 
 int b2r_tt_load_gtfs(const char* path, int is_text, const b2r_gtfs_config* cfg, b2r_host_timetable** out) {

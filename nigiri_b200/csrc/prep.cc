@@ -19,6 +19,16 @@ int32_t round_to_days(int64_t m) {
 
 namespace {
 
+// interval_estimator::clamp (interval_estimate.h:138-146): into the
+// timetable's external interval, the data type's window, then the query's
+// max_interval_, one after another (std::clamp, both ends inclusive)
+int32_t clamp_interval_end(prepped_query const& p, int32_t ext_from, int32_t ext_to, int32_t x) {
+  x = std::clamp(x, ext_from, ext_to);
+  x = std::clamp(x, p.data_max_from, p.data_max_to);
+  if (p.has_max_interval) x = std::clamp(x, p.max_iv_from, p.max_iv_to);
+  return x;
+}
+
 constexpr uint16_t kUnreach = 0xFFFFu;
 constexpr int kMaxDur = 511;  // footpath::kMaxDuration
 
@@ -615,10 +625,10 @@ void prepare(host_view const& hv, b2r_query const& q, int lb_mode, prepped_query
                              round_to_days(static_cast<int64_t>(p.iv_from) +
                                            (p.iv_to - p.iv_from + kMaxIv) / 2) * 1440);
   }
-  auto const clampi = [&](int32_t x) {
-    x = std::clamp(x, ext_from, ext_to);
-    return std::clamp(x, p.data_max_from, p.data_max_to);
-  };
+  p.has_max_interval = q.has_max_interval != 0;
+  p.max_iv_from = q.max_interval_from;
+  p.max_iv_to = q.max_interval_to;
+  auto const clampi = [&](int32_t x) { return clamp_interval_end(p, ext_from, ext_to, x); };
   if (!p.ontrip && p.min_connection_count != 0 && (p.extend_earlier || p.extend_later)) {
     auto nf = p.iv_from, nt = p.iv_to;
     auto const ext = 60 * static_cast<int>(p.min_connection_count);
@@ -673,10 +683,7 @@ bool extend_interval(prepped_query const& p, int32_t ext_from, int32_t ext_to,
     if (p.extend_earlier) nf -= ext;
     if (p.extend_later) nt += ext;
   }
-  auto const clampi = [&](int32_t x) {
-    x = std::clamp(x, ext_from, ext_to);
-    return std::clamp(x, p.data_max_from, p.data_max_to);
-  };
+  auto const clampi = [&](int32_t x) { return clamp_interval_end(p, ext_from, ext_to, x); };
   nf = clampi(nf);
   nt = clampi(nt);
   auto const changed = nf != from || nt != to;

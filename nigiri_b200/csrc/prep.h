@@ -51,6 +51,8 @@ struct prepped_query {
   uint16_t allowed_claszes{0xFFFFU};  // bit c: transport class c allowed
   uint8_t req_flags{0U};              // bit f: route flag f required
   int32_t data_max_from{0}, data_max_to{0};  // interval_estimator clamp
+  bool has_max_interval{false};               // query::max_interval_
+  int32_t max_iv_from{0}, max_iv_to{0};
   tts_norm tts;
   tts_norm tts_raw;  // as given (fastest-direct uses it)
   std::vector<b2r_offset> start_offsets, dest_offsets;  // sanitized order

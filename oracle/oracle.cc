@@ -227,6 +227,8 @@ struct query_t {
   int16_t max_travel_time{kMaxTravelTime};
   uint32_t min_connection_count{0};
   bool extend_earlier{false}, extend_later{false};
+  bool has_max_interval{false};  // query::max_interval_, query.h:89
+  int32_t max_interval_from{0}, max_interval_to{0};
   tts_t tts;
   bool has_fastest_direct{false};
   int16_t fastest_direct{0};
@@ -274,6 +276,9 @@ query_t to_query(b2r_query const& q) {
   r.min_connection_count = q.min_connection_count;
   r.extend_earlier = q.extend_interval_earlier != 0;
   r.extend_later = q.extend_interval_later != 0;
+  r.has_max_interval = q.has_max_interval != 0;
+  r.max_interval_from = q.max_interval_from;
+  r.max_interval_to = q.max_interval_to;
   r.tts = {q.tts_default != 0, q.tts_min_transfer_time, q.tts_additional_time,
            q.tts_factor};
   r.has_fastest_direct = q.has_fastest_direct != 0;
@@ -1626,6 +1631,10 @@ void run_search(tt_view const& tt, query_t q, bool fwd, search_result& res) {
     itv.to = std::clamp(itv.to, ext_from, ext_to);
     itv.from = std::clamp(itv.from, data_max.from, data_max.to);
     itv.to = std::clamp(itv.to, data_max.from, data_max.to);
+    if (q.has_max_interval) {  // interval_estimate.h:142-145
+      itv.from = std::clamp(itv.from, q.max_interval_from, q.max_interval_to);
+      itv.to = std::clamp(itv.to, q.max_interval_from, q.max_interval_to);
+    }
   };
   auto const can_extend_earlier = [&](interval_t const& itv) {
     return q.extend_earlier && itv.from != ext_from;

@@ -229,6 +229,9 @@ class FixtureQuery:
         qq.min_connection_count = q.get("min_connection_count", 0)
         qq.extend_interval_earlier = 1 if q.get("extend_earlier") else 0
         qq.extend_interval_later = 1 if q.get("extend_later") else 0
+        if "max_interval" in q:
+            qq.has_max_interval = 1
+            qq.max_interval_from, qq.max_interval_to = q["max_interval"]
         if q.get("kind") == "one_to_all":
             qq.kind = A.B2R_ONE_TO_ALL
         if q.get("algorithm") == "pong":

@@ -178,8 +178,12 @@ def gtfs_dijkstra():
     """test/routing/dijkstra_test.cc dijkstra_files(): agency Europe/Berlin
     (UTC+2 on 2024-06-08), service S on 2024-06-08 only.  C1, C2 are children
     of C and D1, D2 children of station D; transfers.txt (type 2) gives
-    footpaths D1 <-> D2 of 600 s and C1 <-> C2 of 900 s (no coordinates, so
-    no other footpaths).
+    footpaths D1 <-> D2 of 600 s and C1 <-> C2 of 900 s.  The stop reader
+    links each stop with its parent and the parent's children (stop.cc
+    get_metas; no coordinates, so distance 0 and 2-minute walks, the existing
+    10 and 15 minutes kept), and finalize()'s footpath closure
+    (build_footpaths.cc:229-345) shortens the sibling walks to 4 minutes over
+    the parent.
       AB_TRP A 09:00 -> B 09:30     UTC 07:00 -> 07:30
       BC_TRP B 10:00 -> C2 11:00    UTC 08:00 -> 09:00
       DB_TRP D1 09:30 -> B 09:45    UTC 07:30 -> 07:45
@@ -197,7 +201,8 @@ def gtfs_dijkstra():
         "date_range": ["2024-06-07", "2024-06-09"],
         "locations": [{"id": x, "name": x, "transfer_time": 2, "parent": parents.get(x)}
                       for x in ["A", "B", "C", "C1", "C2", "D", "D1", "D2"]],
-        "footpaths": [["D1", "D2", 10], ["D2", "D1", 10], ["C1", "C2", 15], ["C2", "C1", 15]],
+        "footpaths": [[a, b, w] for p, (x, y) in (("C", ("C1", "C2")), ("D", ("D1", "D2")))
+                      for a, b, w in ((p, x, 2), (p, y, 2), (x, p, 2), (y, p, 2), (x, y, 4), (y, x, 4))],
         "routes": group_routes(services),
     }
 
@@ -702,12 +707,16 @@ GTFS_ONLY_FEEDS = {
                          ["2024-06-07", "2024-06-09"]),
     "gtfs_egress_bound": ("test/routing/gpu_intermodal_egress_test.cc", "test_files()", 0, {},
                           ["2024-06-16", "2024-06-19"]),
+    "gtfs_max_interval": ("test/routing/max_interval_test.cc", "test_files()", 0, {},
+                          ["2019-03-25", "2019-11-01"]),
 }
 
 
 def gtfs_only_cases():
     """test/routing/shortest_fp_test.cc: intermodal searches over transfers.txt
-    footpaths, forward over 2024-06-07 and backward over 06-07 .. 06-09."""
+    footpaths, forward over 2024-06-07 and backward over 06-07 .. 06-09;
+    test/routing/max_interval_test.cc: interval extension clamped by the
+    query's max_interval_."""
     a = [["A0", 3, 23], ["A1", 5, 23], ["A2", 10, 23]]
     c = [["C3", 30, 42], ["C4", 20, 42], ["C5", 10, 42]]
     ref = "test/routing/shortest_fp_test.cc"
@@ -718,6 +727,15 @@ def gtfs_only_cases():
         dict(name="shortest_fp_backward", timetable="gtfs_shortest_fp", ref=ref, golden="exp_bwd_journey",
              query=dict(start=c, dest=a, interval=[t("2024-06-07 00:00"), t("2024-06-09 00:00")],
                         direction="bwd", start_mode="intermodal", dest_mode="intermodal")),
+        # test/routing/max_interval_test.cc: three connections wanted, the
+        # interval may grow later, but only up to max_interval_ (12:00), so
+        # the 12:00 departure stays out
+        dict(name="max_interval", timetable="gtfs_max_interval", ref="test/routing/max_interval_test.cc",
+             golden="expected_journeys",
+             query=dict(start=[["A", 0, 0]], dest=[["B", 0, 0]],
+                        interval=[t("2019-05-01 10:00"), t("2019-05-01 11:00")], direction="fwd",
+                        min_connection_count=3, extend_later=True,
+                        max_interval=[t("2019-05-01 10:00"), t("2019-05-01 12:00")])),
     ]
 
 
@@ -735,8 +753,46 @@ def gtfs_only_known_answers():
                  contains=[t("2024-06-17 09:55"), t("2024-06-17 11:00"), 1])]
 
 
-def gtfs_feeds(ref_root: str):
+JOIN_SPLIT = "test/routing/join_split_test.cc"
+MONTHS = {m: i + 1 for i, m in enumerate(["January", "February", "March", "April", "May", "June", "July",
+                                          "August", "September", "October", "November", "December"])}
+
+
+def join_split_feeds(ref_root: str):
+    """test/routing/join_split_test.cc (join_split.complex): the feed with its
+    six trips.txt rows in the two orders the test loads (0..5 and 5..0)."""
+    src = open(os.path.join(ref_root, JOIN_SPLIT)).read()
+    body = raw_after(src, "mem_dir::read(fmt::format(")
+    assert "{{" not in body and body.count("{}") == 6
+    rows = re.findall(r'"([^"]*)"', re.search(r"kTrips\s*=\s*std::array\{([^}]*)\}", src).group(1))
     out = {}
+    for name, order in (("gtfs_join_split", range(6)), ("gtfs_join_split_rev", range(5, -1, -1))):
+        text = body
+        for i in order:
+            text = text.replace("{}", rows[i], 1)
+        out[name] = {"ref": JOIN_SPLIT, "text": text, "config": {}, "date_range": ["2025-06-12", "2025-06-22"]}
+    return out
+
+
+def join_split_cases(ref_root: str):
+    """join_split.complex's kTests before its real-time update: an ontrip
+    search at 00:00 UTC of the date finds journeys, all without a transfer
+    (the trips joined by stay-seated transfers are one transport)."""
+    src = open(os.path.join(ref_root, JOIN_SPLIT)).read()
+    tests = re.findall(r'\{"(\w+)", "(\w+)", (\d+)_y / (\w+) / (\d+), (true|false)\}', src)
+    assert len(tests) == 14
+    out = []
+    for feed in ("gtfs_join_split", "gtfs_join_split_rev"):
+        for a, b, y, mon, d, exp in tests:
+            out.append(dict(name=f"{feed}_{a}_{b}_{mon[:3].lower()}{d}", timetable=feed, ref=JOIN_SPLIT,
+                            query=dict(start=[[a, 0, 0]], dest=[[b, 0, 0]],
+                                       start_time=t(f"{y}-{MONTHS[mon]:02d}-{int(d):02d} 00:00")),
+                            nonempty=exp == "true", max_transfers_seen=0))
+    return out
+
+
+def gtfs_feeds(ref_root: str):
+    out = join_split_feeds(ref_root)
     for name, (path, marker, nth, config, date_range) in GTFS_ONLY_FEEDS.items():
         src = open(os.path.join(ref_root, path)).read()
         out[name] = {"ref": path, "text": raw_after(src, marker, nth), "config": config,
@@ -774,6 +830,7 @@ def main(ref_root: str):
         gtfs_cases.append(dict(case, expected=parse_journeys(raw_string(src, case["golden"]))))
     doc = {"timetables": TIMETABLES, "cases": out_cases, "gtfs_cases": gtfs_cases,
            "gtfs_known_answers": gtfs_only_known_answers(),
+           "gtfs_seated_cases": join_split_cases(ref_root),
            "known_answers": known_answers(ref_root), "gtfs_feeds": gtfs_feeds(ref_root),
            "generated_by": "tests/golden/make_fixtures.py"}
     with open(os.path.join(HERE, "cases.json"), "w") as f:

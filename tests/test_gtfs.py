@@ -109,6 +109,56 @@ def test_pong_on_read_feeds_in_window(case, loaded):
     assert F.in_window(qd, got) == F.in_window(qd, F.strip_expected(case["expected"]))
 
 
+@pytest.mark.parametrize("case", CASES["gtfs_seated_cases"], ids=lambda c: c["name"])
+def test_stay_seated_known_answers(case, loaded):
+    """join_split.complex (test/routing/join_split_test.cc): between stops
+    reached only over stay-seated transfers there are journeys, and none
+    has a transfer, in both trip orders of the feed."""
+    tt = loaded[case["timetable"]]
+    r = oracle_lib.OracleResult(tt.desc, F.FixtureQuery(A.lib(), tt, case["query"]).q)
+    got = F.journeys_to_records(tt, r.view)
+    assert (len(got) > 0) == case["nonempty"]
+    assert all(j["transfers"] <= case["max_transfers_seen"] for j in got)
+
+
+def transports_by_days(tt):
+    """(stop names, first trip's route, UTC traffic dates) per transport."""
+    import datetime
+    d = tt.desc
+    rsi = np.ctypeslib.as_array(d.route_stop_index, shape=(d.n_routes + 1,))
+    rs = np.ctypeslib.as_array(d.route_stops, shape=(int(rsi[-1]),))
+    tf = np.ctypeslib.as_array(d.route_transport_from, shape=(d.n_routes,))
+    tto = np.ctypeslib.as_array(d.route_transport_to, shape=(d.n_routes,))
+    tbf = np.ctypeslib.as_array(d.transport_traffic_days, shape=(d.n_transports,))
+    bfs = np.ctypeslib.as_array(d.bitfields, shape=(8 * d.n_bitfields,)).reshape(-1, 8)
+    base = datetime.date(1970, 1, 1) + datetime.timedelta(days=d.date_range_from - 5)
+    out = []
+    for r in range(d.n_routes):
+        names = "-".join(tt.loc_name[int(w) & 0x0FFFFFFF] for w in rs[rsi[r]:rsi[r + 1]])
+        for t in range(int(tf[r]), int(tto[r])):
+            days = tuple((base + datetime.timedelta(days=i)).day for i in range(512)
+                         if (int(bfs[tbf[t]][i // 64]) >> (i % 64)) & 1)
+            out.append((names, tt.transport_names[t], days))
+    return sorted(out)
+
+
+@pytest.mark.parametrize("name", ["gtfs_join_split", "gtfs_join_split_rev"])
+def test_stay_seated_transports(name, loaded):
+    """The transports of join_split.complex's day table (UTC first-departure
+    days in June 2025): i and k (01:00 local, days 11, 12, 16-19) continue
+    seated into x (12-14, 19, 21; x1 replaces it on 20) and on into j and l
+    (13-15, 17, 20, 21) where those run; the rest runs alone.  Per trip the
+    days of the transports holding it add up to the test's transportsXDays
+    (i 6, k 6, x 5, x1 1, j 6, l 6 = 30)."""
+    want = []
+    for first, a, c in (("i", "A", "C1"), ("k", "B", "C2")):
+        want += [(f"{a}-{c}", first, (16, 17)), (f"{a}-{c}-D", first, (11, 18)),
+                 (f"{a}-{c}-D-E", first, (12,)), (f"{a}-{c}-D-E", first, (19,)),
+                 (f"{a}-{c}-D-F", first, (12,)), (f"{a}-{c}-D-F", first, (19,))]
+    want += [("C-D-E", "x", (14, 21)), ("C-D-F", "x", (14, 21)), ("D1-E", "j", (15, 17)), ("D2-F", "l", (15, 17))]
+    assert transports_by_days(loaded[name]) == sorted(want)
+
+
 def test_python_reader_reads_a_feed_directory(tmp_path):
     """HostTimetable.load_gtfs on a directory of files (the clasz test's
     feed written out), with the stop ids and names it keeps."""
@@ -154,6 +204,15 @@ def test_golden_cases_on_read_feeds_gpu(loaded):
             res = A.Result()
             assert A.lib().b2r_search_batch(eng.handle, C.byref(q.q), 1, C.byref(res)) == 0
             assert F.journeys_to_records(tt, res) == F.strip_expected(c["expected"]), c["name"]
+        for c in CASES["gtfs_seated_cases"]:
+            if c["timetable"] != name:
+                continue
+            q = F.FixtureQuery(A.lib(), tt, c["query"])
+            res = A.Result()
+            assert A.lib().b2r_search_batch(eng.handle, C.byref(q.q), 1, C.byref(res)) == 0
+            exp = oracle_lib.OracleResult(tt.desc, q.q)
+            assert F.journeys_to_records(tt, res) == F.journeys_to_records(tt, exp.view), c["name"]
+            assert (res.n_journeys > 0) == c["nonempty"], c["name"]
         for ka in CASES["gtfs_known_answers"]:
             if ka["timetable"] != name:
                 continue
