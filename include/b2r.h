@@ -69,6 +69,16 @@ const char* b2r_last_error(void);
 #define B2R_FLAG_RESERVATION_NOT_REQUIRED 3u
 #define B2R_ALL_CLASZ 0xFFFFFFFFu
 
+/* Footpath profiles (types.h:204-210 profile_idx_t): profile 0 is the
+ * timetable's own footpaths; profile 2 (wheelchair) also boards and alights
+ * by the stops' wheelchair bits and needs wheelchair-accessible routes. */
+#define B2R_N_PROFILES 5u
+#define B2R_PROFILE_DEFAULT 0u
+#define B2R_PROFILE_FOOT 1u
+#define B2R_PROFILE_WHEELCHAIR 2u
+#define B2R_PROFILE_CAR 3u
+#define B2R_PROFILE_BIKE 4u
+
 /* Search algorithms (b2r_query::algorithm). */
 #define B2R_ALGO_RAPTOR 0u
 #define B2R_ALGO_PONG 1u
@@ -150,6 +160,19 @@ typedef struct b2r_timetable_desc {
   const uint8_t* route_clasz;
   const uint8_t* route_flags;
   const uint8_t* route_section_flags;
+
+  /* profiles 1..4 at index p - 1 (timetable.h:97-98 footpaths_out_[p] /
+   * footpaths_in_[p], :421-422 fwd / bwd_search_lb_graph_[p]), in the
+   * layout of profile 0's arrays above.  NULL: the profile has no footpaths
+   * (and, for the lower-bound graphs, no graph). */
+  const uint32_t* profile_footpaths_out_index[B2R_N_PROFILES - 1];
+  const uint32_t* profile_footpaths_out[B2R_N_PROFILES - 1];
+  const uint32_t* profile_footpaths_in_index[B2R_N_PROFILES - 1];
+  const uint32_t* profile_footpaths_in[B2R_N_PROFILES - 1];
+  const uint32_t* profile_lb_fwd_index[B2R_N_PROFILES - 1];
+  const uint32_t* profile_lb_fwd[B2R_N_PROFILES - 1];
+  const uint32_t* profile_lb_bwd_index[B2R_N_PROFILES - 1];
+  const uint32_t* profile_lb_bwd[B2R_N_PROFILES - 1];
 } b2r_timetable_desc;
 
 /* ------------------------------------------------------------- queries */
@@ -217,7 +240,10 @@ typedef struct b2r_query {
    * interval estimator produces (interval_estimate.h:138-146) is clamped
    * into [max_interval_from, max_interval_to] (unixtime minutes) */
   uint8_t has_max_interval;
-  uint8_t pad2_[3];
+  /* query::prf_idx_ (query.h:90): footpaths, lower bounds and -- for
+   * B2R_PROFILE_WHEELCHAIR -- stop and route accessibility of the profile */
+  uint8_t prf_idx;
+  uint8_t pad2_[2];
   int32_t max_interval_from;
   int32_t max_interval_to;
 } b2r_query;
@@ -495,6 +521,11 @@ typedef struct b2r_tt_base {
   const uint64_t* bitfields;
   const uint8_t* route_flags;         /* [n_routes] or NULL (no flags) */
   const uint8_t* route_section_flags; /* [route_stop_index[n_routes]] or NULL */
+  /* footpaths of profiles 1..4 at index p - 1, CSR like footpaths_out, or
+   * NULL (none); the builder derives their inbound lists and lower-bound
+   * graphs as build_lb_graph (build_lb_graph.h:11-99) does per profile */
+  const uint32_t* profile_footpaths_out_index[B2R_N_PROFILES - 1];
+  const uint32_t* profile_footpaths_out[B2R_N_PROFILES - 1];
 } b2r_tt_base;
 int b2r_tt_build(const b2r_tt_base* base, b2r_host_timetable** out);
 int b2r_tt_save(const b2r_host_timetable* t, const char* path);

@@ -91,6 +91,7 @@ struct query {
   bool extend_interval_earlier_{false};
   bool extend_interval_later_{false};
   std::optional<interval> max_interval_{};  // clamp of every interval extension
+  uint8_t prf_idx_{0U};                      // footpath profile (B2R_PROFILE_*)
   std::optional<duration_t> fastest_direct_{};
   double fastest_direct_factor_{1.0};
   transfer_time_settings transfer_time_settings_{};
@@ -211,6 +212,7 @@ struct c_query {
     c.use_start_footpaths = q.use_start_footpaths_ ? 1 : 0;
     c.extend_interval_earlier = q.extend_interval_earlier_ ? 1 : 0;
     c.extend_interval_later = q.extend_interval_later_ ? 1 : 0;
+    c.prf_idx = q.prf_idx_;
     if (q.max_interval_) {
       c.has_max_interval = 1;
       c.max_interval_from = q.max_interval_->from_;

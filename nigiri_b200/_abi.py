@@ -28,6 +28,7 @@ B2R_ONE_TO_ONE, B2R_ONE_TO_ALL = 0, 1
 B2R_FLAG_BIKES, B2R_FLAG_CARS, B2R_FLAG_WHEELCHAIR, B2R_FLAG_RESERVATION_NOT_REQUIRED = 0, 1, 2, 3
 B2R_ALL_CLASZ = 0xFFFFFFFF
 B2R_ALGO_RAPTOR, B2R_ALGO_PONG = 0, 1
+B2R_N_PROFILES, B2R_PROFILE_WHEELCHAIR = 5, 2
 B2R_LEG_TRANSPORT, B2R_LEG_FOOTPATH, B2R_LEG_OFFSET = 0, 1, 2
 
 _u8p, _u16p, _u32p, _u64p = (C.POINTER(C.c_uint8), C.POINTER(C.c_uint16),
@@ -54,6 +55,10 @@ class TimetableDesc(C.Structure):
         ("lb_fwd_index", _u32p), ("lb_fwd", _u32p),
         ("lb_bwd_index", _u32p), ("lb_bwd", _u32p),
         ("route_clasz", _u8p), ("route_flags", _u8p), ("route_section_flags", _u8p),
+        ("profile_footpaths_out_index", _u32p * 4), ("profile_footpaths_out", _u32p * 4),
+        ("profile_footpaths_in_index", _u32p * 4), ("profile_footpaths_in", _u32p * 4),
+        ("profile_lb_fwd_index", _u32p * 4), ("profile_lb_fwd", _u32p * 4),
+        ("profile_lb_bwd_index", _u32p * 4), ("profile_lb_bwd", _u32p * 4),
     ]
 
 
@@ -91,7 +96,7 @@ class Query(C.Structure):
         ("allowed_claszes", C.c_uint32), ("require_bike_transport", C.c_uint8),
         ("require_car_transport", C.c_uint8), ("no_compulsory_reservation", C.c_uint8),
         ("algorithm", C.c_uint8),
-        ("has_max_interval", C.c_uint8), ("pad2_", C.c_uint8 * 3),
+        ("has_max_interval", C.c_uint8), ("prf_idx", C.c_uint8), ("pad2_", C.c_uint8 * 2),
         ("max_interval_from", C.c_int32), ("max_interval_to", C.c_int32),
     ]
 
@@ -171,6 +176,7 @@ class TtBase(C.Structure):
         ("route_stop_times", _u16p), ("transport_bitfield", _u32p),
         ("n_bitfields", C.c_uint32), ("bitfields", _u64p),
         ("route_flags", _u8p), ("route_section_flags", _u8p),
+        ("profile_footpaths_out_index", _u32p * 4), ("profile_footpaths_out", _u32p * 4),
     ]
 
 

@@ -47,16 +47,15 @@ struct tt_access {
 // lookup_footpath (direct.cc:65-160) for one exact-match offset of
 // duration 0 at `anchor`: the reflexive transfer time if loc is the anchor,
 // or the shortest footpath between them.
-std::optional<b2r_leg> access_walk(tt_access const& t, tts_norm const& tts, uint32_t anchor, uint32_t loc,
-                                   int32_t time, bool boarding) {
+std::optional<b2r_leg> access_walk(tt_access const& t, tts_norm const& tts, uint32_t prf, uint32_t anchor,
+                                   uint32_t loc, int32_t time, bool boarding) {
   int best = kMaxFootpath;
   if (anchor == loc) best = adjusted_tt<uint8_t>(tts, t.d.transfer_time[anchor]);
   auto eff = kMaxFootpath;
-  auto const* idx = boarding ? t.d.footpaths_out_index : t.d.footpaths_in_index;
-  auto const* fps = boarding ? t.d.footpaths_out : t.d.footpaths_in;
-  for (auto i = idx[anchor]; i != idx[anchor + 1]; ++i) {
-    if (B2R_FP_TARGET(fps[i]) != loc) continue;
-    auto const a = adjusted_tt<int16_t>(tts, static_cast<int16_t>(B2R_FP_DURATION(fps[i])));
+  auto const [fb, fe] = footpaths_at(t.d, prf, boarding, anchor);
+  for (auto const* f = fb; f != fe; ++f) {
+    if (B2R_FP_TARGET(*f) != loc) continue;
+    auto const a = adjusted_tt<int16_t>(tts, static_cast<int16_t>(B2R_FP_DURATION(*f)));
     if (a < eff) eff = a;
   }
   if (eff < kMaxFootpath && eff < best) best = eff;
@@ -74,20 +73,16 @@ std::optional<b2r_leg> access_walk(tt_access const& t, tts_norm const& tts, uint
 
 }  // namespace
 
-bool earliest_alternative(host_view const& hv, tts_norm const& tts, uint32_t allowed_claszes,
+bool earliest_alternative(host_view const& hv, tts_norm const& tts, uint32_t prf, uint32_t allowed_claszes,
                           uint8_t required_flags, uint32_t from, uint32_t to, int32_t from_arr,
                           int32_t to_dep, std::array<b2r_leg, 3>& out) {
   tt_access const t{hv.d};
   auto const& d = hv.d;
   // collect_locations (direct.cc:183-240): the anchors and their footpath
-  // neighbours (out of `from`, into `to`)
+  // neighbours in the query's profile (out of `from`, into `to`)
   std::vector<uint32_t> boarding{from}, alighting{to};
-  for (auto i = d.footpaths_out_index[from]; i != d.footpaths_out_index[from + 1]; ++i) {
-    boarding.push_back(B2R_FP_TARGET(d.footpaths_out[i]));
-  }
-  for (auto i = d.footpaths_in_index[to]; i != d.footpaths_in_index[to + 1]; ++i) {
-    alighting.push_back(B2R_FP_TARGET(d.footpaths_in[i]));
-  }
+  for (auto [f, e] = footpaths_at(d, prf, true, from); f != e; ++f) boarding.push_back(B2R_FP_TARGET(*f));
+  for (auto [f, e] = footpaths_at(d, prf, false, to); f != e; ++f) alighting.push_back(B2R_FP_TARGET(*f));
   auto const contains = [](std::vector<uint32_t> const& v, uint32_t x) {
     return std::find(v.begin(), v.end(), x) != v.end();
   };
@@ -127,10 +122,10 @@ bool earliest_alternative(host_view const& hv, tts_norm const& tts, uint32_t all
       auto const stp = t.stop(r, i);
       auto const loc = B2R_STOP_LOC(stp);
       if (!board.has_value()) {
-        if (contains(boarding, loc) && B2R_STOP_IN(stp)) board = i;
+        if (contains(boarding, loc) && stop_in(stp, prf)) board = i;  // stop::in_allowed(prf_idx)
         continue;
       }
-      if (!contains(alighting, loc) || !B2R_STOP_OUT(stp)) continue;
+      if (!contains(alighting, loc) || !stop_out(stp, prf)) continue;
       auto const s_from = *board, s_to = i;
       board.reset();
       auto violates = false;  // sections_violate_constraints, direct.cc:242-260
@@ -151,8 +146,8 @@ bool earliest_alternative(host_view const& hv, tts_norm const& tts, uint32_t all
           if (!t.bit(d.transport_traffic_days[tr], static_cast<uint32_t>(start_day))) continue;
           auto const sd = static_cast<uint16_t>(start_day);
           auto const dep = t.event_time(r, x, sd, s_from, false), arr = t.event_time(r, x, sd, s_to, true);
-          auto const bw = access_walk(t, tts, from, board_loc, dep, true);
-          auto const aw = access_walk(t, tts, to, alight_loc, arr, false);
+          auto const bw = access_walk(t, tts, prf, from, board_loc, dep, true);
+          auto const aw = access_walk(t, tts, prf, to, alight_loc, arr, false);
           if (!bw.has_value() || !aw.has_value() || bw->dep_time < from_arr) continue;
           b2r_leg ride{};
           ride.kind = B2R_LEG_TRANSPORT;

@@ -573,6 +573,7 @@ slot_t make_slot(b2r_engine& e, uint32_t s, prepped_query const& p, bool& clear_
   sl.recon_mode = p.recon_mode;
   sl.recon_transfers = p.recon_transfers;
   sl.no_lb = p.no_lb ? 1 : 0;
+  sl.prf = p.prf;
   sl.recon_start = p.recon_start;
   sl.span = p.span;
   sl.n_starts = static_cast<uint32_t>(p.starts.size());
@@ -1081,7 +1082,7 @@ void finish_pong(b2r_engine& e, query_run& q) {
           continue;
         }
         std::array<b2r_leg, 3> alt;
-        if (earliest_alternative(v, plan.ping.tts, plan.ping.allowed_claszes, plan.ping.req_flags,
+        if (earliest_alternative(v, plan.ping.tts, plan.ping.prf, plan.ping.allowed_claszes, plan.ping.req_flags,
                                  loc(l[w], l[w].stop_to - 1U), loc(l[w + 4], l[w + 4].stop_from),
                                  l[w].arr_time, l[w + 4].dep_time, alt)) {
           l[w + 1] = alt[0];
@@ -1750,6 +1751,20 @@ extern "C" {
 int b2r_timetable_upload(const b2r_timetable_desc* d, int device, b2r_timetable** out) {
   B2R_API_GUARD({
     if (d == nullptr || out == nullptr) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
+    for (auto p = 0U; p != B2R_N_PROFILES - 1U; ++p) {  // a profile's lists come in (index, words) pairs
+      uint32_t const* const lists[8] = {d->profile_footpaths_out_index[p], d->profile_footpaths_out[p],
+                                        d->profile_footpaths_in_index[p],  d->profile_footpaths_in[p],
+                                        d->profile_lb_fwd_index[p],        d->profile_lb_fwd[p],
+                                        d->profile_lb_bwd_index[p],        d->profile_lb_bwd[p]};
+      auto ok = (lists[0] == nullptr) == (lists[2] == nullptr);  // footpaths out and in together
+      for (auto x = 0U; ok && x != 8U; x += 2U) {
+        if (lists[x] == nullptr) continue;
+        auto const n = lists[x][d->n_locations];
+        ok = n == 0U || lists[x + 1U] != nullptr;
+        for (auto i = 0U; ok && i != n; ++i) ok = B2R_FP_TARGET(lists[x + 1U][i]) < d->n_locations;
+      }
+      if (!ok) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "b2r_timetable_upload: malformed profile footpaths");
+    }
     try {
       B2R_CUDA(cudaSetDevice(device));
       auto t = std::make_unique<b2r_timetable>();
@@ -1819,6 +1834,27 @@ int b2r_timetable_upload(const b2r_timetable_desc* d, int device, b2r_timetable*
       v.lb_bwd_index = t->lb_bwd_index.data();
       v.lb_bwd = t->lb_bwd.data();
       v.importance = nullptr;
+      // footpath profiles 1..4: (index, words) of out, in, lb fwd, lb bwd
+      for (auto p = 0U; p != B2R_N_PROFILES - 1U; ++p) {
+        uint32_t const* const src[8] = {d->profile_footpaths_out_index[p], d->profile_footpaths_out[p],
+                                        d->profile_footpaths_in_index[p],  d->profile_footpaths_in[p],
+                                        d->profile_lb_fwd_index[p],        d->profile_lb_fwd[p],
+                                        d->profile_lb_bwd_index[p],        d->profile_lb_bwd[p]};
+        uint32_t const** const dst[8] = {&v.profile_footpaths_out_index[p], &v.profile_footpaths_out[p],
+                                         &v.profile_footpaths_in_index[p],  &v.profile_footpaths_in[p],
+                                         &v.profile_lb_fwd_index[p],        &v.profile_lb_fwd[p],
+                                         &v.profile_lb_bwd_index[p],        &v.profile_lb_bwd[p]};
+        auto& pc = t->profiles[p];
+        for (auto x = 0U; x != 8U; x += 2U) {
+          *dst[x] = nullptr;
+          *dst[x + 1U] = nullptr;
+          if (src[x] == nullptr) continue;
+          b2r::host_copy(pc.lists[x], src[x], nl + 1);
+          b2r::host_copy(pc.lists[x + 1U], src[x + 1U], src[x][nl]);
+          *dst[x] = pc.lists[x].data();
+          *dst[x + 1U] = pc.lists[x + 1U].data();
+        }
+      }
       // route filters on the host: pong's direct alternatives
       t->route_clasz.assign(nr, 10U);
       if (d->route_clasz != nullptr) t->route_clasz.assign(d->route_clasz, d->route_clasz + nr);
@@ -1885,6 +1921,20 @@ int b2r_timetable_upload(const b2r_timetable_desc* d, int device, b2r_timetable*
       dd.fp_out = up(d->footpaths_out, d->footpaths_out_index[nl]);
       dd.fp_in_idx = up(d->footpaths_in_index, nl + 1);
       dd.fp_in = up(d->footpaths_in, d->footpaths_in_index[nl]);
+      {  // footpath profiles 1..4 (a profile without footpaths: a zero index)
+        std::vector<uint32_t> zero(nl + 1, 0U);
+        auto* dz = up(zero.data(), zero.size());
+        std::vector<uint32_t const*> tab(4U * (B2R_N_PROFILES - 1U), dz);
+        for (auto p = 0U; p != B2R_N_PROFILES - 1U; ++p) {
+          auto const& pc = t->profiles[p];
+          for (auto x = 0U; x != 4U; x += 2U) {
+            if (pc.lists[x].empty()) continue;
+            tab[4U * p + x] = up(pc.lists[x].data(), nl + 1);
+            if (!pc.lists[x + 1U].empty()) tab[4U * p + x + 1U] = up(pc.lists[x + 1U].data(), pc.lists[x + 1U].size());
+          }
+        }
+        dd.fp_tab = up(tab.data(), tab.size());
+      }
       dd.route_stop_idx = up(d->route_stop_index, nr + 1);
       dd.route_stops = up(d->route_stops, d->route_stop_index[nr]);
       dd.route_tr_from = up(d->route_transport_from, nr);

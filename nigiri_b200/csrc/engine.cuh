@@ -51,6 +51,10 @@ struct dtt {
   uint32_t const* fp_out;
   uint32_t const* fp_in_idx;
   uint32_t const* fp_in;
+  // footpaths of profiles 1..4 (footpaths_out_[p] / footpaths_in_[p]):
+  // fp_tab[4 (p - 1) + 0..3] = out index, out, in index, in; a profile
+  // without footpaths points at an all-zero index
+  uint32_t const* const* fp_tab;
   uint32_t const* route_stop_idx;
   uint32_t const* route_stops;
   uint32_t const* route_tr_from;
@@ -129,7 +133,7 @@ struct slot_t {
                              // (recon_transfers, recon_start), 2: none
   uint8_t recon_transfers;
   uint8_t no_lb;             // lower bounds read as 0 (a pong phase)
-  uint8_t pad_l;
+  uint8_t prf;               // footpath profile (query::prf_idx_)
   int16_t span;              // worst time at destination = group start + dir(span)
   int32_t recon_start;
   tts_t tts;
@@ -159,7 +163,8 @@ struct __align__(16) lane_t {
   uint8_t fwd;
   uint8_t k;
   uint8_t run;
-  uint8_t mode;  // bit0 intermodal dest, bit1 has dests, bit2 tts default, bit3 no lower bounds
+  uint8_t mode;  // bit0 intermodal dest, bit1 has dests, bit2 tts default, bit3 no lower
+                 // bounds, bits 4-6 footpath profile
   uint16_t claszes;  // allowed transport classes
   uint8_t req;       // required route flags
   uint8_t blast;     // pong bounds: last round (0: none)
@@ -282,6 +287,22 @@ __device__ __forceinline__ bool route_allowed(dtt const& T, uint32_t r, uint32_t
 __device__ __forceinline__ bool section_ok(dtt const& T, uint32_t r_stop_base, uint32_t s, uint32_t sec) {
   return (static_cast<uint32_t>(T.route_sec[r_stop_base + s]) & sec) == sec;
 }
+
+// footpaths_out_[prf] (out) or footpaths_in_[prf] (timetable.h:97-98):
+// the CSR index and the footpath words
+__device__ __forceinline__ uint32_t const* fp_index(dtt const& T, uint32_t prf, bool out) {
+  if (prf == 0u) return out ? T.fp_out_idx : T.fp_in_idx;
+  return T.fp_tab[4u * (prf - 1u) + (out ? 0u : 2u)];
+}
+__device__ __forceinline__ uint32_t const* fp_words(dtt const& T, uint32_t prf, bool out) {
+  if (prf == 0u) return out ? T.fp_out : T.fp_in;
+  return T.fp_tab[4u * (prf - 1u) + (out ? 1u : 3u)];
+}
+
+// stop::in_allowed / out_allowed of the stop word, the wheelchair bits when
+// wc (stop.h:51-67 can_start / can_finish with is_wheelchair)
+__device__ __forceinline__ uint32_t stop_in_bit(uint32_t w, uint32_t wc) { return (w >> (28u + 2u * wc)) & 1u; }
+__device__ __forceinline__ uint32_t stop_out_bit(uint32_t w, uint32_t wc) { return (w >> (29u + 2u * wc)) & 1u; }
 
 __device__ __forceinline__ int delta_count(uint16_t d) {  // delta::count()
   return static_cast<int16_t>(static_cast<uint32_t>(d & 0x1Fu) * 1440u + (d >> 5));

@@ -183,6 +183,30 @@ host_timetable generate(uint32_t config, uint64_t seed) {
     t.fp_out_index.push_back(static_cast<uint32_t>(t.fp_out.size()));
   }
 
+  // ---- wheelchair profile: about one location in five is not accessible
+  //      (from the location index; no draws from the random stream, so the
+  //      rest of the timetable does not change); its footpaths are the walks
+  //      into accessible locations, half as long again
+  auto const accessible = [](uint32_t l) { return ((l * 2654435761u) >> 28) % 5u != 0u; };
+  {
+    auto& wp = t.profiles[B2R_PROFILE_WHEELCHAIR - 1U];
+    wp.fp_out_index.assign(1, 0U);
+    for (auto i = 0U; i != t.n_locations; ++i) {
+      std::vector<uint32_t> fps;
+      for (auto x = t.fp_out_index[i]; x != t.fp_out_index[i + 1]; ++x) {
+        auto const tgt = B2R_FP_TARGET(t.fp_out[x]);
+        if (!accessible(tgt)) continue;
+        auto const dur = std::min(511U, (B2R_FP_DURATION(t.fp_out[x]) * 3U + 1U) / 2U);
+        fps.push_back((tgt & 0x7FFFFFu) | (dur << 23));
+      }
+      std::stable_sort(fps.begin(), fps.end(), [](uint32_t a, uint32_t b) {
+        return B2R_FP_DURATION(a) < B2R_FP_DURATION(b);
+      });
+      wp.fp_out.insert(wp.fp_out.end(), fps.begin(), fps.end());
+      wp.fp_out_index.push_back(static_cast<uint32_t>(wp.fp_out.size()));
+    }
+  }
+
   // ---- service day bitfields (bit 0 = date_range_from - 5 days)
   std::vector<uint8_t> holiday(w.n_days, 0U);
   if (w.holiday_frac > 0.0) {
@@ -363,7 +387,7 @@ host_timetable generate(uint32_t config, uint64_t seed) {
     for (auto const& sub : subs) {
       for (auto x : seq) {
         t.route_stops.push_back((x & 0x0FFFFFFFu) | (1u << 28) | (1u << 29) |
-                                (1u << 30) | (1u << 31));
+                                (accessible(x) ? (1u << 30) | (1u << 31) : 0u));
       }
       t.route_stop_index.push_back(static_cast<uint32_t>(t.route_stops.size()));
       t.route_transport_from.push_back(static_cast<uint32_t>(t.transport_traffic_days.size()));

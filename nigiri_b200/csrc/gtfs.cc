@@ -334,9 +334,9 @@ struct trip {
   bool bad{false};
 };
 
-uint32_t stop_word(uint32_t loc, bool in, bool out) {
-  return (loc & 0x0FFFFFFFu) | (in ? 1u << 28 : 0u) | (out ? 1u << 29 : 0u) | (in ? 1u << 30 : 0u) |
-         (out ? 1u << 31 : 0u);
+uint32_t stop_word(uint32_t loc, bool in, bool out, bool in_wc, bool out_wc) {
+  return (loc & 0x0FFFFFFFu) | (in ? 1u << 28 : 0u) | (out ? 1u << 29 : 0u) | (in_wc ? 1u << 30 : 0u) |
+         (out_wc ? 1u << 31 : 0u);
 }
 
 // one transport of the timetable: a trip or a block chain on the UTC
@@ -399,6 +399,7 @@ bool load_gtfs(std::map<std::string, std::string> const& files, b2r_gtfs_config 
   auto const st = file("stops.txt");
   std::unordered_map<std::string, uint32_t> loc_of;
   std::vector<std::string> ids, parent_ids, names;
+  std::vector<bool> accessible;
   std::vector<std::pair<double, double>> coords;  // (lat, lng), clamped
   auto const coordinate = [](std::string const& x, double lim) {
     return std::clamp(x.empty() ? 0.0 : std::strtod(x.c_str(), nullptr), -lim, lim);
@@ -412,6 +413,8 @@ bool load_gtfs(std::map<std::string, std::string> const& files, b2r_gtfs_config 
     ids.push_back(id);
     parent_ids.push_back(st.get(r, st.col("parent_station")));
     names.push_back(st.get(r, st.col("stop_name")));
+    // wheelchair_boarding: unknown counts as accessible (stop.cc:266-268)
+    accessible.push_back(st.get(r, st.col("wheelchair_boarding")) != "2");
     coords.emplace_back(coordinate(st.get(r, st.col("stop_lat")), 90.0),
                         coordinate(st.get(r, st.col("stop_lon")), 180.0));
   }
@@ -421,6 +424,7 @@ bool load_gtfs(std::map<std::string, std::string> const& files, b2r_gtfs_config 
       ids.push_back(p);
       parent_ids.emplace_back();
       names.emplace_back();
+      accessible.push_back(true);
       coords.emplace_back(0.0, 0.0);
     }
   }
@@ -642,7 +646,9 @@ bool load_gtfs(std::map<std::string, std::string> const& files, b2r_gtfs_config 
       auto& v = rows[i];
       std::stable_sort(v.begin(), v.end(), [](auto const& a, auto const& b) { return std::get<0>(a) < std::get<0>(b); });
       for (auto const& [seq, l, ev, in, out] : v) {
-        trips[i].stops.push_back(stop_word(l, in, out));
+        // the wheelchair bits: in / out at an accessible stop (stop_time.cc:119-124)
+        auto const acc = accessible[l - kSpecial];
+        trips[i].stops.push_back(stop_word(l, in, out, acc && in, acc && out));
         trips[i].events.push_back(ev);
         trips[i].bad = trips[i].bad || ev.arr < 0 || ev.dep < 0;  // needs interpolation: skipped
       }
@@ -786,7 +792,8 @@ bool load_gtfs(std::map<std::string, std::string> const& files, b2r_gtfs_config 
           u.stop_seq = t.stops;
         } else {  // the joint stop: boarding of the next trip, alighting of the previous
           auto const prev = u.stop_seq.back(), cur = t.stops.front();
-          u.stop_seq.back() = stop_word(loc_of_word(prev), ((cur >> 28) & 1U) != 0U, ((prev >> 29) & 1U) != 0U);
+          u.stop_seq.back() = stop_word(loc_of_word(prev), ((cur >> 28) & 1U) != 0U, ((prev >> 29) & 1U) != 0U,
+                                        ((cur >> 30) & 1U) != 0U, ((prev >> 31) & 1U) != 0U);
           u.stop_seq.insert(u.stop_seq.end(), t.stops.begin() + 1, t.stops.end());
         }
       }

@@ -80,6 +80,22 @@ int b2r_tt_build(const b2r_tt_base* b, b2r_host_timetable** out) {
                           b->footpaths_out_index + b->n_locations + 1);
     t.fp_out.assign(b->footpaths_out,
                     b->footpaths_out + b->footpaths_out_index[b->n_locations]);
+    for (auto p = 0U; p != B2R_N_PROFILES - 1U; ++p) {
+      if (b->profile_footpaths_out_index[p] == nullptr) continue;
+      auto const* idx = b->profile_footpaths_out_index[p];
+      auto& x = t.profiles[p];
+      x.fp_out_index.assign(idx, idx + b->n_locations + 1);
+      auto ok = b->profile_footpaths_out[p] != nullptr || idx[b->n_locations] == 0U;
+      for (auto l = 0U; ok && l != b->n_locations; ++l) ok = idx[l] <= idx[l + 1];
+      if (ok && idx[b->n_locations] != 0U) {
+        x.fp_out.assign(b->profile_footpaths_out[p], b->profile_footpaths_out[p] + idx[b->n_locations]);
+        for (auto const fp : x.fp_out) ok = ok && B2R_FP_TARGET(fp) < b->n_locations;
+      }
+      if (!ok) {
+        delete h;
+        return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "b2r_tt_build: malformed profile footpaths");
+      }
+    }
     t.n_routes = b->n_routes;
     t.route_stop_index.assign(b->route_stop_index, b->route_stop_index + b->n_routes + 1);
     t.route_stops.assign(b->route_stops, b->route_stops + b->route_stop_index[b->n_routes]);

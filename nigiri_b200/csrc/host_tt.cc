@@ -69,16 +69,20 @@ struct ordered_min_map {
   }
 };
 
-void build_lb_graph(host_timetable& t, bool fwd, std::vector<uint32_t>& index,
+// loader/build_lb_graph.h:11-99 for one profile: its footpaths (in-lists
+// forward, out-lists backward) and the routes, without those that do not
+// carry cars (car profile) or bikes (bike profile) on any section
+void build_lb_graph(host_timetable& t, bool fwd, uint32_t prf, std::vector<uint32_t> const& fi,
+                    std::vector<uint32_t> const& fd, std::vector<uint32_t>& index,
                     std::vector<uint32_t>& data) {
-  // loader/build_lb_graph.h:11-99
   index.assign(1, 0U);
   data.clear();
   ordered_min_map weights;
+  auto const flag_set = [&](uint32_t f, uint32_t r) {  // timetable::is_flag_set
+    return !t.route_flags.empty() && ((t.route_flags[r] >> (2U * f)) & 3U) != 0U;
+  };
   auto const add_edges = [&](uint32_t l) {
     auto const parent_l = root_idx(t, l);
-    auto const& fi = fwd ? t.fp_in_index : t.fp_out_index;
-    auto const& fd = fwd ? t.fp_in : t.fp_out;
     for (auto i = fi[l]; i != fi[l + 1]; ++i) {
       auto const target = root_idx(t, B2R_FP_TARGET(fd[i]));
       if (target != parent_l) weights.update(target, B2R_FP_DURATION(fd[i]));
@@ -86,6 +90,10 @@ void build_lb_graph(host_timetable& t, bool fwd, std::vector<uint32_t>& index,
     for (auto ri = t.location_routes_index[l];
          ri != t.location_routes_index[l + 1]; ++ri) {
       auto const r = t.location_routes[ri];
+      if ((prf == B2R_PROFILE_CAR && !flag_set(B2R_FLAG_CARS, r)) ||
+          (prf == B2R_PROFILE_BIKE && !flag_set(B2R_FLAG_BIKES, r))) {
+        continue;
+      }
       auto const s0 = t.route_stop_index[r];
       auto const n = t.route_stop_index[r + 1] - s0;
       for (auto from = 0U; from + 1U < n; ++from) {
@@ -178,6 +186,19 @@ b2r_timetable_desc host_timetable::desc() const {
   d.route_flags = route_flags.empty() ? nullptr : route_flags.data();
   d.route_section_flags =
       route_section_flags.empty() ? nullptr : route_section_flags.data();
+  auto const ptr = [](std::vector<uint32_t> const& v) { return v.empty() ? nullptr : v.data(); };
+  for (auto p = 0U; p != B2R_N_PROFILES - 1U; ++p) {
+    auto const& x = profiles[p];
+    if (x.fp_out_index.empty()) continue;
+    d.profile_footpaths_out_index[p] = x.fp_out_index.data();
+    d.profile_footpaths_out[p] = x.fp_out.data();
+    d.profile_footpaths_in_index[p] = x.fp_in_index.data();
+    d.profile_footpaths_in[p] = x.fp_in.data();
+    d.profile_lb_fwd_index[p] = ptr(x.lb_fwd_index);
+    d.profile_lb_fwd[p] = x.lb_fwd.data();
+    d.profile_lb_bwd_index[p] = ptr(x.lb_bwd_index);
+    d.profile_lb_bwd[p] = x.lb_bwd.data();
+  }
   return d;
 }
 
@@ -212,24 +233,29 @@ void finalize(host_timetable& t) {
   }
 
   // footpaths_in from footpaths_out, then sorted by duration
-  // (build_footpaths.cc:404-415 sorts both lists by duration).
-  {
+  // (build_footpaths.cc:404-415 sorts both lists by duration); the same for
+  // every profile that has footpaths
+  auto const derive_in = [&](std::vector<uint32_t> const& oi, std::vector<uint32_t> const& od,
+                             std::vector<uint32_t>& ii, std::vector<uint32_t>& id) {
     std::vector<std::vector<uint32_t>> in(t.n_locations);
     for (auto l = 0U; l != t.n_locations; ++l) {
-      for (auto i = t.fp_out_index[l]; i != t.fp_out_index[l + 1]; ++i) {
-        in[B2R_FP_TARGET(t.fp_out[i])].push_back(
-            pack_fp(l, B2R_FP_DURATION(t.fp_out[i])));
+      for (auto i = oi[l]; i != oi[l + 1]; ++i) {
+        in[B2R_FP_TARGET(od[i])].push_back(pack_fp(l, B2R_FP_DURATION(od[i])));
       }
     }
-    t.fp_in_index.assign(1, 0U);
-    t.fp_in.clear();
+    ii.assign(1, 0U);
+    id.clear();
     for (auto& v : in) {
       std::stable_sort(v.begin(), v.end(), [](uint32_t a, uint32_t b) {
         return B2R_FP_DURATION(a) < B2R_FP_DURATION(b);
       });
-      t.fp_in.insert(t.fp_in.end(), v.begin(), v.end());
-      t.fp_in_index.push_back(static_cast<uint32_t>(t.fp_in.size()));
+      id.insert(id.end(), v.begin(), v.end());
+      ii.push_back(static_cast<uint32_t>(id.size()));
     }
+  };
+  derive_in(t.fp_out_index, t.fp_out, t.fp_in_index, t.fp_in);
+  for (auto& x : t.profiles) {
+    if (!x.fp_out_index.empty()) derive_in(x.fp_out_index, x.fp_out, x.fp_in_index, x.fp_in);
   }
 
   // location_routes: routes in registration order, no duplicates
@@ -287,8 +313,8 @@ void finalize(host_timetable& t) {
     t.bitfields.insert(t.bitfields.end(), combined, combined + 8);
   }
 
-  build_lb_graph(t, true, t.lb_fwd_index, t.lb_fwd);
-  build_lb_graph(t, false, t.lb_bwd_index, t.lb_bwd);
+  build_lb_graph(t, true, B2R_PROFILE_DEFAULT, t.fp_in_index, t.fp_in, t.lb_fwd_index, t.lb_fwd);
+  build_lb_graph(t, false, B2R_PROFILE_DEFAULT, t.fp_out_index, t.fp_out, t.lb_bwd_index, t.lb_bwd);
 
   // route flags: absent means no route carries any flag.  From per-section
   // flags, a route's flag f is "on all sections" when every section of the
@@ -318,6 +344,15 @@ void finalize(host_timetable& t) {
         t.route_section_flags[i] = all;
       }
     }
+  }
+
+  // lower-bound graphs of the profiles that have footpaths (with the route
+  // flags, which the car and bike profiles filter on)
+  for (auto p = 0U; p != B2R_N_PROFILES - 1U; ++p) {
+    auto& x = t.profiles[p];
+    if (x.fp_out_index.empty()) continue;
+    build_lb_graph(t, true, p + 1U, x.fp_in_index, x.fp_in, x.lb_fwd_index, x.lb_fwd);
+    build_lb_graph(t, false, p + 1U, x.fp_out_index, x.fp_out, x.lb_bwd_index, x.lb_bwd);
   }
 
   // importance, loader/init_finish.cc:64-102 (float accumulation into a
@@ -354,7 +389,7 @@ void finalize(host_timetable& t) {
 
 // ------------------------------------------------------------ persistence
 namespace {
-constexpr uint64_t kMagic = 0x3232424d49544232ull;  // "2BTIMB22"
+constexpr uint64_t kMagic = 0x3332424d49544232ull;  // "2BTIMB23"
 
 template <typename T>
 void put_vec(std::FILE* f, std::vector<T> const& v) {
@@ -380,6 +415,9 @@ bool get_vec(std::FILE* f, std::vector<T>& v) {
   X(bitfields) X(location_routes_index) X(location_routes) X(lb_fwd_index)     \
   X(lb_fwd) X(lb_bwd_index) X(lb_bwd) X(x) X(y) X(route_flags)                \
   X(route_section_flags)
+#define B2R_TT_PROFILE_FIELDS(X)                                               \
+  X(fp_out_index) X(fp_out) X(fp_in_index) X(fp_in) X(lb_fwd_index) X(lb_fwd)  \
+  X(lb_bwd_index) X(lb_bwd)
 
 bool save(host_timetable const& t, std::string const& path) {
   auto* f = std::fopen(path.c_str(), "wb");
@@ -392,6 +430,11 @@ bool save(host_timetable const& t, std::string const& path) {
 #define X(name) put_vec(f, t.name);
   B2R_TT_FIELDS(X)
 #undef X
+  for (auto const& x : t.profiles) {
+#define X(name) put_vec(f, x.name);
+    B2R_TT_PROFILE_FIELDS(X)
+#undef X
+  }
   return std::fclose(f) == 0;
 }
 
@@ -412,6 +455,11 @@ bool load(std::string const& path, host_timetable& t) {
 #define X(name) ok = ok && get_vec(f, t.name);
     B2R_TT_FIELDS(X)
 #undef X
+    for (auto& x : t.profiles) {
+#define X(name) ok = ok && get_vec(f, x.name);
+      B2R_TT_PROFILE_FIELDS(X)
+#undef X
+    }
   }
   std::fclose(f);
   return ok;

@@ -7,6 +7,7 @@
 // This is timetable construction, not the routing hot path.
 #pragma once
 
+#include <array>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -40,6 +41,13 @@ struct host_timetable {
   std::vector<uint64_t> bitfields;  // n_bitfields * 8
   std::vector<uint32_t> location_routes_index, location_routes;
   std::vector<uint32_t> lb_fwd_index, lb_fwd, lb_bwd_index, lb_bwd;
+  // footpath profiles 1..4 at index p - 1: footpaths (out as given, in
+  // derived) and their lower-bound graphs; empty vectors: no footpaths
+  struct profile {
+    std::vector<uint32_t> fp_out_index, fp_out, fp_in_index, fp_in;
+    std::vector<uint32_t> lb_fwd_index, lb_fwd, lb_bwd_index, lb_bwd;
+  };
+  std::array<profile, B2R_N_PROFILES - 1> profiles;
 
   // generator metadata (coordinates in metres, for query generation)
   std::vector<float> x, y;

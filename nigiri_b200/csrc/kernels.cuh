@@ -120,7 +120,7 @@ __global__ void k_ctl_begin(state st) {
     ln.qtag = tagcode(sl.gen_query);
     ln.mode = (sl.intermodal_dest ? 1u : 0u) |
               ((!sl.intermodal_dest && !sl.one_to_all && sl.n_dest != 0) ? 2u : 0u) |
-              (sl.tts.is_default ? 4u : 0u) | (sl.no_lb ? 8u : 0u);
+              (sl.tts.is_default ? 4u : 0u) | (sl.no_lb ? 8u : 0u) | (static_cast<uint32_t>(sl.prf) << 4);
     ln.tad_k = sl.tad[sl.k];
     ln.claszes = sl.allowed_claszes;
     ln.req = sl.req_flags;
@@ -269,8 +269,9 @@ __global__ void __launch_bounds__(256, 3) k_route_scan(state st) {
       auto const s = g * 32u + b;
       auto const ln = st.lanes[s];
       if (!ln.run) continue;
-      uint32_t sec = 0u;  // required flags checked per section
+      uint32_t sec = 0u;  // required flags checked per section (bits 0-3); bit 8: wheelchair profile
       if ((ln.claszes != 0xFFFFu || ln.req != 0u) && !route_allowed(T, r, ln.claszes, ln.req, sec)) continue;
+      if ((ln.mode & 0x70u) == (B2R_PROFILE_WHEELCHAIR << 4)) sec |= 0x100u;
       auto const bit = 1u << b;
       auto const fwd = ln.fwd != 0;
       auto const k = static_cast<uint32_t>(ln.k);
@@ -278,7 +279,12 @@ __global__ void __launch_bounds__(256, 3) k_route_scan(state st) {
       auto const n = T.route_stop_idx[r + 1] - sb;
       auto const n_t = T.route_tr_to[r] - T.route_tr_from[r];
       auto const* colbase = T.st + T.route_st_from[r];
-      auto const stop_word = [&](uint32_t i) { return T.route_stops[sb + (fwd ? i : n - 1u - i)]; };
+      // the stop word; for the wheelchair profile with its wheelchair bits in
+      // place of the in / out bits (can_start / can_finish, raptor.h:1252, 1304)
+      auto const stop_word = [&](uint32_t i) {
+        auto const w = T.route_stops[sb + (fwd ? i : n - 1u - i)];
+        return (sec & 0x100u) != 0u ? (w & 0xCFFFFFFFu) | ((w >> 2) & 0x30000000u) : w;
+      };
       bool et_valid = false;
       uint32_t et_off = 0;
       uint16_t et_day = 0;
@@ -304,7 +310,7 @@ __global__ void __launch_bounds__(256, 3) k_route_scan(state st) {
         auto const l = B2R_STOP_LOC(stp);
         auto const can_finish = fwd ? B2R_STOP_OUT(stp) : B2R_STOP_IN(stp);
         auto const can_start = fwd ? B2R_STOP_IN(stp) : B2R_STOP_OUT(stp);
-        if (sec != 0u && i != 0u && !section_ok(T, sb, fwd ? i - 1u : si, sec)) {
+        if (sec != 0u && i != 0u && !section_ok(T, sb, fwd ? i - 1u : si, sec & 15u)) {
           et_valid = false;  // raptor.h:1194-1217: the section ridden lacks a flag
         }
         bool arrival_ran = false;
@@ -536,15 +542,16 @@ __device__ void footpaths_pre_slot(state const& st, uint32_t s) {
   int nc = 0;
   for (auto i = 0u; i != sl.n_dest; ++i) {
     auto const d = st.dest_pool[sl.dest_off + i].loc;
-    auto const* iidx = fwd ? T.fp_in_idx : T.fp_out_idx;
-    auto const* idat = fwd ? T.fp_in : T.fp_out;
+    auto const prf = static_cast<uint32_t>(ln.mode >> 4);
+    auto const* iidx = fp_index(T, prf, !fwd);
+    auto const* idat = fp_words(T, prf, !fwd);
     for (auto x = iidx[d]; x != iidx[d + 1]; ++x) {
       auto const src = B2R_FP_TARGET(idat[x]);
       if (!(st.Y[src * st.G + g] & bit)) continue;
       auto const tk = dec(st.tmp[li(st, src, s)], ln.gtag);
       if (tk == kKeyInv) continue;
-      auto const* oidx = fwd ? T.fp_out_idx : T.fp_in_idx;
-      auto const* odat = fwd ? T.fp_out : T.fp_in;
+      auto const* oidx = fp_index(T, prf, fwd);
+      auto const* odat = fp_words(T, prf, fwd);
       for (auto y = oidx[src]; y != oidx[src + 1]; ++y) {
         if (B2R_FP_TARGET(odat[y]) != d) continue;
         if (nc == kMaxC) {
@@ -617,8 +624,9 @@ __global__ void k_footpaths(state st) {
         auto const tk = dec(st.tmp[li(st, src, s)], ln.gtag);
         if (tk == kKeyInv) return;
         auto const fwd = ln.fwd != 0;
-        auto const* idx = fwd ? T.fp_out_idx : T.fp_in_idx;
-        auto const* dat = fwd ? T.fp_out : T.fp_in;
+        auto const prf = static_cast<uint32_t>(ln.mode >> 4);
+        auto const* idx = fp_index(T, prf, fwd);
+        auto const* dat = fp_words(T, prf, fwd);
         auto const fb = idx[src], n = idx[src + 1] - fb;
         slot_t const* slp = &st.slots[s];
         auto const tad_flat = (ln.mode & 2u) ? 0 : static_cast<int>(slp->tad[ln.k]);

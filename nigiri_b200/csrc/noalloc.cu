@@ -71,6 +71,7 @@ struct params {
   dev::tts_t tts;
   uint16_t claszes;  // allowed transport classes
   uint8_t req;       // required route flags
+  uint8_t prf;       // footpath profile (query::prf_idx_)
   b2r_offset off[B2R_NOALLOC_MAX_OFFSETS];
 };
 
@@ -243,8 +244,9 @@ __global__ void __cluster_dims__(kCtas, 1, 1) __launch_bounds__(kThreads, 1)
         auto const si = fwd ? i : n - 1u - i;
         auto const stp = T.route_stops[sb + si];
         auto const l = B2R_STOP_LOC(stp);
-        auto const can_finish = fwd ? B2R_STOP_OUT(stp) : B2R_STOP_IN(stp);
-        auto const can_start = fwd ? B2R_STOP_IN(stp) : B2R_STOP_OUT(stp);
+        auto const wc = P.prf == B2R_PROFILE_WHEELCHAIR ? 1u : 0u;  // one_to_all.cc:69
+        auto const can_finish = fwd ? dev::stop_out_bit(stp, wc) : dev::stop_in_bit(stp, wc);
+        auto const can_start = fwd ? dev::stop_in_bit(stp, wc) : dev::stop_out_bit(stp, wc);
         if (sec != 0u && i != 0u && !dev::section_ok(T, sb, fwd ? i - 1u : si, sec)) {
           et_valid = false;  // raptor.h:1194-1217
         }
@@ -321,8 +323,8 @@ __global__ void __cluster_dims__(kCtas, 1, 1) __launch_bounds__(kThreads, 1)
     // targets combined with atomicMin
     {
       auto const ny = ldu(&cnt[CY0 + cx]);
-      auto const* idx = fwd ? T.fp_out_idx : T.fp_in_idx;
-      auto const* dat = fwd ? T.fp_out : T.fp_in;
+      auto const* idx = dev::fp_index(T, P.prf, fwd);
+      auto const* dat = dev::fp_words(T, P.prf, fwd);
       for (auto i = tid; i < ny; i += kAll) {
         auto const src = ldu(&ylist[i]);
         auto const tk = ldk(&tmp[src]);
@@ -427,8 +429,11 @@ int run(b2r_timetable const* tt, b2r_query const* q, int16_t* round_times, uint6
   P.base_days = tt->d.internal_from_days + P.base;
   P.tts = {q->tts_default, q->tts_min_transfer_time, q->tts_additional_time, q->tts_factor};
   P.claszes = static_cast<uint16_t>(q->allowed_claszes & 0xFFFFu);
+  if (q->prf_idx >= B2R_N_PROFILES) return fail(B2R_ERR_INVALID_ARGUMENT, "b2r_one_to_all_noalloc: prf_idx out of range");
+  P.prf = q->prf_idx;
   P.req = static_cast<uint8_t>((q->require_bike_transport != 0 ? 1u << B2R_FLAG_BIKES : 0u) |
                                (q->require_car_transport != 0 ? 1u << B2R_FLAG_CARS : 0u) |
+                               (q->prf_idx == B2R_PROFILE_WHEELCHAIR ? 1u << B2R_FLAG_WHEELCHAIR : 0u) |
                                (q->no_compulsory_reservation != 0 ? 1u << B2R_FLAG_RESERVATION_NOT_REQUIRED : 0u));
   auto const span = static_cast<int>(q->max_travel_time);
   auto const worst = std::clamp(q->start_time + (fwd ? span : -span) - P.base_days * 1440, -32768, 32767);

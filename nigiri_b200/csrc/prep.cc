@@ -32,6 +32,16 @@ int32_t clamp_interval_end(prepped_query const& p, int32_t ext_from, int32_t ext
 constexpr uint16_t kUnreach = 0xFFFFu;
 constexpr int kMaxDur = 511;  // footpath::kMaxDuration
 
+// the route flags a query requires (raptor.h:251-257, direct.cc:503-513):
+// bikes, cars, no compulsory reservation, and wheelchair accessibility for
+// the wheelchair profile
+uint8_t required_flags(b2r_query const& q) {
+  return static_cast<uint8_t>((q.require_bike_transport != 0 ? 1U << B2R_FLAG_BIKES : 0U) |
+                              (q.require_car_transport != 0 ? 1U << B2R_FLAG_CARS : 0U) |
+                              (q.prf_idx == B2R_PROFILE_WHEELCHAIR ? 1U << B2R_FLAG_WHEELCHAIR : 0U) |
+                              (q.no_compulsory_reservation != 0 ? 1U << B2R_FLAG_RESERVATION_NOT_REQUIRED : 0U));
+}
+
 template <typename T>
 T adjust(tts_norm const& s, T d) {  // transfer_time_settings.h:20-31
   if (s.is_default) return d;
@@ -133,12 +143,11 @@ int16_t fastest_direct(view const& v, b2r_query const& q, std::vector<b2r_offset
     if (it->second.empty()) buckets.erase(it);
     if (l == B2R_SPECIAL_END) break;
     if (get(l) < dcur) continue;
-    auto const* idx = fwd ? v.d.footpaths_out_index : v.d.footpaths_in_index;
-    auto const* fps = fwd ? v.d.footpaths_out : v.d.footpaths_in;
-    for (auto i = idx[l]; i != idx[l + 1]; ++i) {
-      auto const nd = dcur + adjust<uint16_t>(raw, static_cast<uint16_t>(B2R_FP_DURATION(fps[i])));
+    auto const [fb, fe] = footpaths_at(v.d, q.prf_idx, fwd, l);
+    for (auto const* f = fb; f != fe; ++f) {
+      auto const nd = dcur + adjust<uint16_t>(raw, static_cast<uint16_t>(B2R_FP_DURATION(*f)));
       if (nd > 65535u) continue;
-      auto const tgt = B2R_FP_TARGET(fps[i]);
+      auto const tgt = B2R_FP_TARGET(*f);
       if (!dest_off.contains(tgt)) continue;
       auto& td = get(tgt);
       if (nd < td && nd < 65535u) {
@@ -205,17 +214,16 @@ void lower_bounds(view const& v, prepped_query const& p, std::vector<uint16_t>& 
       dist[m] = std::min(dd, dist[m]);
     });
   }
-  auto const* gi = p.fwd ? v.d.lb_fwd_index : v.d.lb_bwd_index;
-  auto const* gd = p.fwd ? v.d.lb_fwd : v.d.lb_bwd;
   while (size != 0) {
     while (bucket[cur].empty()) ++cur;
     auto const l = bucket[cur].back();
     bucket[cur].pop_back();
     --size;
     if (dist[l] < cur) continue;
-    for (auto e = gi[l]; e != gi[l + 1]; ++e) {
-      auto const tgt = B2R_FP_TARGET(gd[e]);
-      auto const nd = static_cast<uint32_t>(cur) + B2R_FP_DURATION(gd[e]);
+    auto const [eb, ee] = lb_edges_at(v.d, p.prf, p.fwd, l);  // the profile's graph
+    for (auto const* e = eb; e != ee; ++e) {
+      auto const tgt = B2R_FP_TARGET(*e);
+      auto const nd = static_cast<uint32_t>(cur) + B2R_FP_DURATION(*e);
       if (nd < dist[tgt] && nd < kBuckets) {
         dist[tgt] = static_cast<uint16_t>(nd);
         push(tgt, nd);
@@ -288,7 +296,7 @@ void interval_starts(view const& v, prepped_query const& p, int32_t iv_from, int
     for (auto i = 0U; i != n; ++i) {
       auto const stp = d.route_stops[s0 + i];
       if (B2R_STOP_LOC(stp) != l) continue;
-      if ((!fwd && (i == 0U || !B2R_STOP_OUT(stp))) || (fwd && (i + 1U == n || !B2R_STOP_IN(stp)))) {
+      if ((!fwd && (i == 0U || !stop_out(stp, p.prf))) || (fwd && (i + 1U == n || !stop_in(stp, p.prf)))) {
         continue;
       }
       auto const st_from = fwd ? iv_from : iv_from - p.max_start_offset_;
@@ -343,12 +351,10 @@ void collect_starts(view const& v, prepped_query const& p, bool interval, int32_
     v.metas(p.start_mode, o.target, [&](uint32_t l) {
       upd(l, o.duration);
       if (use_fp) {
-        auto const* idx = p.fwd ? v.d.footpaths_out_index : v.d.footpaths_in_index;
-        auto const* fps = p.fwd ? v.d.footpaths_out : v.d.footpaths_in;
-        for (auto i = idx[l]; i != idx[l + 1]; ++i) {
-          upd(B2R_FP_TARGET(fps[i]),
-              static_cast<int16_t>(o.duration +
-                                   adjust<int16_t>(p.tts, static_cast<int16_t>(B2R_FP_DURATION(fps[i])))));
+        auto const [fb, fe] = footpaths_at(v.d, p.prf, p.fwd, l);
+        for (auto const* f = fb; f != fe; ++f) {
+          upd(B2R_FP_TARGET(*f),
+              static_cast<int16_t>(o.duration + adjust<int16_t>(p.tts, static_cast<int16_t>(B2R_FP_DURATION(*f)))));
         }
       }
     });
@@ -450,10 +456,8 @@ void prepare_pong(host_view const& hv, b2r_query const& q, int lb_mode, prepped_
     t.max_start_offset_ = q.max_start_offset;
     t.end_k = static_cast<uint8_t>(std::min<int>(q.max_transfers, B2R_MAX_TRANSFERS) + 2);
     t.allowed_claszes = static_cast<uint16_t>(q.allowed_claszes & 0xFFFFU);
-    t.req_flags = static_cast<uint8_t>(
-        (q.require_bike_transport != 0 ? 1U << B2R_FLAG_BIKES : 0U) |
-        (q.require_car_transport != 0 ? 1U << B2R_FLAG_CARS : 0U) |
-        (q.no_compulsory_reservation != 0 ? 1U << B2R_FLAG_RESERVATION_NOT_REQUIRED : 0U));
+    t.req_flags = required_flags(q);
+    t.prf = q.prf_idx;
     t.start_offsets = st;
     t.dest_offsets = dt;
     t.tts_raw = raw;
@@ -468,8 +472,11 @@ void prepare_pong(host_view const& hv, b2r_query const& q, int lb_mode, prepped_
   };
   auto& ping = plan->ping;
   tmpl(fwd, q.start_match_mode, q.dest_match_mode, so, de, ping);
-  if (lb_mode == 1) lower_bounds(v, ping, ping.lb);
-  if (lb_mode == 2 || lb_mode == 3) lb_seeds(v, ping, ping.lb_seeds);
+  // the device lower-bound tables and solver cover profile 0; other
+  // profiles take the host Dijkstra over their own graph
+  auto const host_lb = lb_mode == 1 || (lb_mode >= 2 && ping.prf != 0U);
+  if (host_lb) lower_bounds(v, ping, ping.lb);
+  if (!host_lb && (lb_mode == 2 || lb_mode == 3)) lb_seeds(v, ping, ping.lb_seeds);
   ping.use_start_footpaths = q.use_start_footpaths != 0;
   ping.span = static_cast<int16_t>(std::min<int>(mtt + 1440, B2R_MAX_TRAVEL_TIME_MIN));  // kMinLookAhead
   ping.recon_mode = 2;
@@ -511,6 +518,11 @@ void phase_starts(host_view const& hv, prepped_query const& tmpl, int32_t t, std
 }
 
 void prepare(host_view const& hv, b2r_query const& q, int lb_mode, prepped_query& p) {
+  if (q.prf_idx >= B2R_N_PROFILES) {  // profile_idx_t below kNProfiles (types.h:204-210)
+    p = prepped_query{};
+    p.status = B2R_ERR_INVALID_ARGUMENT;
+    return;
+  }
   if (q.algorithm == B2R_ALGO_PONG) {
     prepare_pong(hv, q, lb_mode, p);
     return;
@@ -534,10 +546,8 @@ void prepare(host_view const& hv, b2r_query const& q, int lb_mode, prepped_query
   p.extend_earlier = q.extend_interval_earlier != 0;
   p.extend_later = q.extend_interval_later != 0;
   p.allowed_claszes = static_cast<uint16_t>(q.allowed_claszes & 0xFFFFU);  // 16 classes
-  p.req_flags = static_cast<uint8_t>(
-      (q.require_bike_transport != 0 ? 1U << B2R_FLAG_BIKES : 0U) |
-      (q.require_car_transport != 0 ? 1U << B2R_FLAG_CARS : 0U) |
-      (q.no_compulsory_reservation != 0 ? 1U << B2R_FLAG_RESERVATION_NOT_REQUIRED : 0U));
+  p.req_flags = required_flags(q);
+  p.prf = q.prf_idx;
   p.start_offsets.assign(q.start, q.start + q.n_start);
   p.dest_offsets.assign(q.destination, q.destination + q.n_destination);
   p.tts_raw = {q.tts_default, q.tts_min_transfer_time, q.tts_additional_time, q.tts_factor};
@@ -591,8 +601,9 @@ void prepare(host_view const& hv, b2r_query const& q, int lb_mode, prepped_query
   p.tts.is_default = p.tts.factor == 1.0F && p.tts.min_transfer_time == 0 && p.tts.additional_time == 0;
   collect_dests(v, p);
   p.span = static_cast<int16_t>(std::min<int>(p.fastest_direct, p.max_travel_time) + 1);  // search.h:426-429
-  if (lb_mode == 1) lower_bounds(v, p, p.lb);
-  if (lb_mode == 2 || lb_mode == 3) lb_seeds(v, p, p.lb_seeds);
+  auto const host_lb = lb_mode == 1 || (lb_mode >= 2 && p.prf != 0U);  // as for pong's ping
+  if (host_lb) lower_bounds(v, p, p.lb);
+  if (!host_lb && (lb_mode == 2 || lb_mode == 3)) lb_seeds(v, p, p.lb_seeds);
   auto const mid = static_cast<int64_t>(p.iv_from) + (p.iv_to - p.iv_from) / 2;
   p.base = static_cast<uint16_t>(round_to_days(mid) - hv.internal_from_days());
   p.base_days = hv.internal_from_days() + p.base;

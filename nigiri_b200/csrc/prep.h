@@ -7,6 +7,7 @@
 
 #include <cstdint>
 #include <memory>
+#include <utility>
 #include <vector>
 
 #include "b2r.h"
@@ -50,6 +51,7 @@ struct prepped_query {
   bool extend_earlier{false}, extend_later{false};
   uint16_t allowed_claszes{0xFFFFU};  // bit c: transport class c allowed
   uint8_t req_flags{0U};              // bit f: route flag f required
+  uint8_t prf{0U};                    // query::prf_idx_
   int32_t data_max_from{0}, data_max_to{0};  // interval_estimator clamp
   bool has_max_interval{false};               // query::max_interval_
   int32_t max_iv_from{0}, max_iv_to{0};
@@ -127,5 +129,37 @@ struct host_view {
   b2r_timetable_desc d;
   int32_t internal_from_days() const { return d.date_range_from - 5; }
 };
+
+// footpaths_out_[prf][l] (out) or footpaths_in_[prf][l] as [begin, end);
+// empty for a profile without footpaths
+inline std::pair<uint32_t const*, uint32_t const*> footpaths_at(b2r_timetable_desc const& d, uint32_t prf,
+                                                                bool out, uint32_t l) {
+  auto const* idx = prf == 0U ? (out ? d.footpaths_out_index : d.footpaths_in_index)
+                              : (out ? d.profile_footpaths_out_index[prf - 1U] : d.profile_footpaths_in_index[prf - 1U]);
+  auto const* dat = prf == 0U ? (out ? d.footpaths_out : d.footpaths_in)
+                              : (out ? d.profile_footpaths_out[prf - 1U] : d.profile_footpaths_in[prf - 1U]);
+  if (idx == nullptr) return {nullptr, nullptr};
+  return {dat + idx[l], dat + idx[l + 1]};
+}
+
+// fwd / bwd_search_lb_graph_[prf][l]; empty for a profile without a graph
+inline std::pair<uint32_t const*, uint32_t const*> lb_edges_at(b2r_timetable_desc const& d, uint32_t prf, bool fwd,
+                                                               uint32_t l) {
+  auto const* idx = prf == 0U ? (fwd ? d.lb_fwd_index : d.lb_bwd_index)
+                              : (fwd ? d.profile_lb_fwd_index[prf - 1U] : d.profile_lb_bwd_index[prf - 1U]);
+  auto const* dat = prf == 0U ? (fwd ? d.lb_fwd : d.lb_bwd)
+                              : (fwd ? d.profile_lb_fwd[prf - 1U] : d.profile_lb_bwd[prf - 1U]);
+  if (idx == nullptr) return {nullptr, nullptr};
+  return {dat + idx[l], dat + idx[l + 1]};
+}
+
+// stop::in_allowed(p) / out_allowed(p), stop.h:44-49: the wheelchair bits
+// for the wheelchair profile
+inline bool stop_in(uint32_t w, uint32_t prf) {
+  return prf == B2R_PROFILE_WHEELCHAIR ? B2R_STOP_IN_WC(w) != 0U : B2R_STOP_IN(w) != 0U;
+}
+inline bool stop_out(uint32_t w, uint32_t prf) {
+  return prf == B2R_PROFILE_WHEELCHAIR ? B2R_STOP_OUT_WC(w) != 0U : B2R_STOP_OUT(w) != 0U;
+}
 
 }  // namespace b2r

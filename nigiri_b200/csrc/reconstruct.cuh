@@ -171,6 +171,8 @@ struct recon_ctx {
         l = B2R_STOP_LOC(w);
         // departure section forward, arrival section backward
         cut = sec != 0u && !section_ok(*T, T->route_stop_idx[r], fwd ? si : si - 1u, sec);
+        // plain in / out bits for every profile: reconstruct.cc:252-253
+        // passes the bool is_wheelchair as a profile index (0 or 1)
         if (!cut && !((fwd && !B2R_STOP_IN(w)) || (!fwd && !B2R_STOP_OUT(w)))) {
           event_time = unix_to_delta(ev_time(t, day, si, !fwd));
           auto const round_time = rt_t(k - 1, l);
@@ -363,8 +365,8 @@ struct recon_ctx {
     auto const same = (k == j->transfers + 1u)
                           ? 0
                           : static_cast<int>(adjusted<uint8_t>(sl->tts, T->transfer_time[l]));
-    auto const* idx = fwd ? T->fp_in_idx : T->fp_out_idx;
-    auto const* fps = fwd ? T->fp_in : T->fp_out;
+    auto const* idx = fp_index(*T, sl->prf, !fwd);  // the query's profile (reconstruct.cc:81, 761)
+    auto const* fps = fp_words(*T, sl->prf, !fwd);
     auto const fb = idx[l];
     auto const raw = [&](uint32_t f, uint32_t& tg, int& dur) {
       if (f == 0u) {
@@ -420,8 +422,8 @@ struct recon_ctx {
     }
     auto const jst = unix_to_delta(j->start_time);
     auto const fp_target_time = rt_t(0, lsl);
-    auto const* idx = fwd ? T->fp_in_idx : T->fp_out_idx;
-    auto const* fps = fwd ? T->fp_in : T->fp_out;
+    auto const* idx = fp_index(*T, sl->prf, !fwd);  // the query's profile (reconstruct.cc:81, 761)
+    auto const* fps = fp_words(*T, sl->prf, !fwd);
     for (auto i = idx[lsl]; i != idx[lsl + 1]; ++i) {
       auto const tgt = B2R_FP_TARGET(fps[i]);
       auto const d = static_cast<int>(adjusted<int16_t>(sl->tts, static_cast<int16_t>(B2R_FP_DURATION(fps[i]))));
@@ -482,8 +484,10 @@ struct recon_ctx {
     auto const end = static_cast<uint32_t>(tl.stop_to - 1u);
     for (auto si = 0u; si < end; ++si) {
       if (!B2R_STOP_IN(word_at(tl, si))) continue;
-      for (auto i = T->fp_out_idx[start_loc]; i != T->fp_out_idx[start_loc + 1]; ++i) {
-        auto const fp = T->fp_out[i];
+      auto const* oidx = fp_index(*T, sl->prf, true);  // optimize_footpaths.cc:91
+      auto const* ofp = fp_words(*T, sl->prf, true);
+      for (auto i = oidx[start_loc]; i != oidx[start_loc + 1]; ++i) {
+        auto const fp = ofp[i];
         if (B2R_FP_TARGET(fp) != loc_at(tl, si)) continue;
         auto const d = static_cast<int>(adjusted<int16_t>(sl->tts, static_cast<int16_t>(B2R_FP_DURATION(fp))));
         if (d < best) {
@@ -547,8 +551,10 @@ struct recon_ctx {
     auto const size = n_stops(r_of(tl));
     for (auto si = from; si < size; ++si) {
       if (!B2R_STOP_OUT(word_at(tl, si))) continue;
-      for (auto i = T->fp_in_idx[dest_loc]; i != T->fp_in_idx[dest_loc + 1]; ++i) {
-        auto const fp = T->fp_in[i];
+      auto const* iidx = fp_index(*T, sl->prf, false);  // optimize_footpaths.cc:215
+      auto const* ifp = fp_words(*T, sl->prf, false);
+      for (auto i = iidx[dest_loc]; i != iidx[dest_loc + 1]; ++i) {
+        auto const fp = ifp[i];
         if (B2R_FP_TARGET(fp) != loc_at(tl, si)) continue;
         auto const d = static_cast<int>(adjusted<int16_t>(sl->tts, static_cast<int16_t>(B2R_FP_DURATION(fp))));
         if (d < best) {
@@ -611,8 +617,10 @@ struct recon_ctx {
         auto const sf = from_start + x / to_end, s2 = x % to_end;
         if (!B2R_STOP_OUT(word_at(lf, sf)) || !B2R_STOP_IN(word_at(lt, s2))) continue;
         auto const a = loc_at(lf, sf), b = loc_at(lt, s2);
-        for (auto y = T->fp_out_idx[a]; y != T->fp_out_idx[a + 1]; ++y) {
-          auto const fp = T->fp_out[y];
+        auto const* oidx = fp_index(*T, sl->prf, true);  // optimize_footpaths.cc:405
+        auto const* ofp = fp_words(*T, sl->prf, true);
+        for (auto y = oidx[a]; y != oidx[a + 1]; ++y) {
+          auto const fp = ofp[y];
           if (B2R_FP_TARGET(fp) != b) continue;
           auto const d = static_cast<int>(adjusted<int16_t>(sl->tts, static_cast<int16_t>(B2R_FP_DURATION(fp))));
           auto const arr = time_at(lf, sf, true);

@@ -27,6 +27,12 @@ struct b2r_timetable {
   std::vector<uint8_t> location_type, route_clasz, route_flags, route_section_flags;
   std::vector<uint16_t> route_stop_times;
   std::vector<uint64_t> bitfields;
+  // footpath profiles 1..4: footpaths (out, in) and lower-bound graphs
+  // (fwd, bwd), CSR index then words, empty when the profile has none
+  struct profile_copy {
+    std::vector<uint32_t> lists[8];
+  };
+  profile_copy profiles[B2R_N_PROFILES - 1];
   b2r::host_view view{};
   // all-pairs lower-bound tables [source][location] (u16 minutes, 0xFFFF
   // unreachable) for forward and backward searches, built by the first

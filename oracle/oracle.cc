@@ -64,6 +64,39 @@ inline int32_t round_days(int64_t minutes) {
 // ------------------------------------------------- timetable accessors
 struct tt_view {
   b2r_timetable_desc const& d;
+  uint32_t prf{0};  // the query's footpath profile (query::prf_idx_)
+  mutable std::vector<uint32_t> zero_{};
+
+  // footpaths_out_[prf] (out) or footpaths_in_[prf] (timetable.h:97-98) and
+  // fwd / bwd_search_lb_graph_[prf] (:421-422): CSR index and words; a
+  // profile without them reads as an all-zero index
+  uint32_t const* zero_index() const {
+    if (zero_.empty()) zero_.assign(d.n_locations + 1U, 0U);
+    return zero_.data();
+  }
+  uint32_t const* fp_index(bool out) const {
+    auto const* x = prf == 0U ? (out ? d.footpaths_out_index : d.footpaths_in_index)
+                              : (out ? d.profile_footpaths_out_index[prf - 1U] : d.profile_footpaths_in_index[prf - 1U]);
+    return x != nullptr ? x : zero_index();
+  }
+  uint32_t const* fp_words(bool out) const {
+    auto const* x = prf == 0U ? (out ? d.footpaths_out : d.footpaths_in)
+                              : (out ? d.profile_footpaths_out[prf - 1U] : d.profile_footpaths_in[prf - 1U]);
+    return x != nullptr ? x : zero_index();
+  }
+  uint32_t const* lb_index(bool fwd) const {
+    auto const* x = prf == 0U ? (fwd ? d.lb_fwd_index : d.lb_bwd_index)
+                              : (fwd ? d.profile_lb_fwd_index[prf - 1U] : d.profile_lb_bwd_index[prf - 1U]);
+    return x != nullptr ? x : zero_index();
+  }
+  uint32_t const* lb_words(bool fwd) const {
+    auto const* x = prf == 0U ? (fwd ? d.lb_fwd : d.lb_bwd)
+                              : (fwd ? d.profile_lb_fwd[prf - 1U] : d.profile_lb_bwd[prf - 1U]);
+    return x != nullptr ? x : zero_index();
+  }
+  // stop::in_allowed(p) / out_allowed(p) (stop.h:44-49)
+  bool stop_in(uint32_t w) const { return (prf == B2R_PROFILE_WHEELCHAIR ? B2R_STOP_IN_WC(w) : B2R_STOP_IN(w)) != 0U; }
+  bool stop_out(uint32_t w) const { return (prf == B2R_PROFILE_WHEELCHAIR ? B2R_STOP_OUT_WC(w) : B2R_STOP_OUT(w)) != 0U; }
 
   int32_t internal_from_days() const {
     return d.date_range_from - B2R_TIMETABLE_OFFSET_DAYS;
@@ -288,6 +321,8 @@ query_t to_query(b2r_query const& q) {
   r.required_flags = static_cast<uint8_t>(
       (q.require_bike_transport != 0 ? 1U << B2R_FLAG_BIKES : 0U) |
       (q.require_car_transport != 0 ? 1U << B2R_FLAG_CARS : 0U) |
+      // is_wheelchair: the wheelchair-accessible route filter (raptor.h:256)
+      (q.prf_idx == B2R_PROFILE_WHEELCHAIR ? 1U << B2R_FLAG_WHEELCHAIR : 0U) |
       (q.no_compulsory_reservation != 0
            ? 1U << B2R_FLAG_RESERVATION_NOT_REQUIRED
            : 0U));
@@ -651,8 +686,8 @@ struct raptor_t {
 
   void update_footpaths(unsigned k) {  // raptor.h:745-845
     prev_station_mark.for_each([&](uint32_t i) {
-      auto const& idx = fwd ? tt.d.footpaths_out_index : tt.d.footpaths_in_index;
-      auto const* fps = fwd ? tt.d.footpaths_out : tt.d.footpaths_in;
+      auto const* idx = tt.fp_index(fwd);
+      auto const* fps = tt.fp_words(fwd);
       for (auto fi = idx[i]; fi != idx[i + 1]; ++fi) {
         ++st.n_footpaths_visited;
         auto const fp = fps[fi];
@@ -714,8 +749,9 @@ struct raptor_t {
       auto const stp = tt.stop(r, stop_idx);
       auto const l = B2R_STOP_LOC(stp);
       auto const is_last = i == n_stops - 1U;
-      auto const can_finish = fwd ? B2R_STOP_OUT(stp) : B2R_STOP_IN(stp);
-      auto const can_start = fwd ? B2R_STOP_IN(stp) : B2R_STOP_OUT(stp);
+      // stop::can_finish / can_start (stop.h:51-67) with is_wheelchair
+      auto const can_finish = fwd ? tt.stop_out(stp) : tt.stop_in(stp);
+      auto const can_start = fwd ? tt.stop_in(stp) : tt.stop_out(stp);
 
       // section filters, raptor.h:1194-1217: the trip carried into this
       // stop is dropped if the section it rode lacks a required flag
@@ -872,8 +908,8 @@ void add_starts_in_interval(tt_view const& tt, bool fwd, interval_t const& iv,
     for (auto i = 0U; i != n; ++i) {
       auto const stp = tt.stop(r, i);
       if (B2R_STOP_LOC(stp) != l) continue;
-      if ((!fwd && (i == 0U || !B2R_STOP_OUT(stp))) ||
-          (fwd && (i == n - 1U || !B2R_STOP_IN(stp)))) {
+      if ((!fwd && (i == 0U || !tt.stop_out(stp))) ||  // out_allowed(prf_idx)
+          (fwd && (i == n - 1U || !tt.stop_in(stp)))) {
         continue;
       }
       add_start_times_at_stop(
@@ -917,8 +953,8 @@ void get_starts(tt_view const& tt, bool fwd, start_time_v const& st,
     for_each_meta(tt, q.start_mode, o.target, [&](uint32_t l) {
       update(l, o.duration);
       if (q.use_start_footpaths) {
-        auto const& idx = fwd ? tt.d.footpaths_out_index : tt.d.footpaths_in_index;
-        auto const* fps = fwd ? tt.d.footpaths_out : tt.d.footpaths_in;
+        auto const* idx = tt.fp_index(fwd);
+        auto const* fps = tt.fp_words(fwd);
         for (auto fi = idx[l]; fi != idx[l + 1]; ++fi) {
           update(B2R_FP_TARGET(fps[fi]),
                  static_cast<int16_t>(
@@ -1011,8 +1047,8 @@ void dijkstra_lb(tt_view const& tt, query_t const& q, bool fwd,
       dists[meta] = std::min(d, dists[meta]);
     });
   }
-  auto const* gi = fwd ? tt.d.lb_fwd_index : tt.d.lb_bwd_index;
-  auto const* gd = fwd ? tt.d.lb_fwd : tt.d.lb_bwd;
+  auto const* gi = tt.lb_index(fwd);
+  auto const* gd = tt.lb_words(fwd);
   while (!pq.empty()) {
     auto const l = pq.top();
     pq.pop();
@@ -1072,8 +1108,8 @@ int16_t get_fastest_direct(tt_view const& tt, query_t const& q, bool fwd) {
     pq.pop();
     if (l.l == kEnd) break;
     if (get_dist(l.l) < l.d) continue;
-    auto const& idx = fwd ? tt.d.footpaths_out_index : tt.d.footpaths_in_index;
-    auto const* fps = fwd ? tt.d.footpaths_out : tt.d.footpaths_in;
+    auto const* idx = tt.fp_index(fwd);
+    auto const* fps = tt.fp_words(fwd);
     for (auto fi = idx[l.l]; fi != idx[l.l + 1]; ++fi) {
       auto const new_dist =
           static_cast<uint32_t>(l.d) +
@@ -1142,6 +1178,9 @@ struct reconstructor {
           !section_ok(tt, r, fwd ? stop_idx : stop_idx - 1U, sections)) {
         break;
       }
+      // reconstruct.cc:252-253 passes the bool is_wheelchair where
+      // stop::in_allowed takes a profile index: profile 0 or 1, never the
+      // wheelchair profile, so reconstruction reads the plain bits
       if ((fwd && !B2R_STOP_IN(stp)) || (!fwd && !B2R_STOP_OUT(stp))) continue;
       auto const event_time = unix_to_delta(base, stop_time(t, day, stop_idx, !fwd));
       auto const round_time = rt(k - 1, l);
@@ -1186,6 +1225,7 @@ struct reconstructor {
       auto const n = tt.n_stops(r);
       for (auto i = 0U; i != n; ++i) {
         auto const stp = tt.stop(r, i);
+        // plain bits as above (reconstruct.cc:505-509)
         if (B2R_STOP_LOC(stp) != l || (fwd && (i == 0U || !B2R_STOP_OUT(stp))) ||
             (!fwd && (i == n - 1U || !B2R_STOP_IN(stp)))) {
           continue;
@@ -1248,8 +1288,8 @@ struct reconstructor {
             : static_cast<int>(adjusted<uint8_t>(q.tts, tt.d.transfer_time[l]));
     auto transfer = check_fp(k, l, curr_time, l, same_stop_dur, false);
     if (transfer.has_value()) return *transfer;
-    auto const& idx = fwd ? tt.d.footpaths_in_index : tt.d.footpaths_out_index;
-    auto const* fps = fwd ? tt.d.footpaths_in : tt.d.footpaths_out;
+    auto const* idx = tt.fp_index(!fwd);
+    auto const* fps = tt.fp_words(!fwd);
     for (auto fi = idx[l]; fi != idx[l + 1]; ++fi) {
       auto res = check_fp(k, l, curr_time, B2R_FP_TARGET(fps[fi]),
                           static_cast<int>(B2R_FP_DURATION(fps[fi])), true);
@@ -1267,8 +1307,8 @@ struct reconstructor {
         better_eq(j.start_time, leg_start_time)) {
       return std::nullopt;
     }
-    auto const& idx = fwd ? tt.d.footpaths_in_index : tt.d.footpaths_out_index;
-    auto const* fps = fwd ? tt.d.footpaths_in : tt.d.footpaths_out;
+    auto const* idx = tt.fp_index(!fwd);
+    auto const* fps = tt.fp_words(!fwd);
     auto const j_start_time = unix_to_delta(base, j.start_time);
     auto const fp_target_time = rt(0, leg_start_location);
     if (q.start_mode == B2R_MATCH_INTERMODAL) {
@@ -1381,9 +1421,9 @@ struct reconstructor {
     auto const end = static_cast<uint32_t>(transport_leg.stop_to - 1U);
     for (auto s = 0U; s < end; ++s) {
       if (!B2R_STOP_IN(sword(transport_leg, s))) continue;
-      for (auto fi = tt.d.footpaths_out_index[start_loc];
-           fi != tt.d.footpaths_out_index[start_loc + 1]; ++fi) {
-        auto const fp = tt.d.footpaths_out[fi];
+      for (auto fi = tt.fp_index(true)[start_loc];
+           fi != tt.fp_index(true)[start_loc + 1]; ++fi) {
+        auto const fp = tt.fp_words(true)[fi];
         if (B2R_FP_TARGET(fp) != sloc(transport_leg, s)) continue;
         auto const fp_dur =
             adjusted<int16_t>(jq.tts, static_cast<int16_t>(B2R_FP_DURATION(fp)));
@@ -1451,9 +1491,9 @@ struct reconstructor {
     auto const size = run_size(transport_leg);
     for (auto s = range_from; s < size; ++s) {
       if (!B2R_STOP_OUT(sword(transport_leg, s))) continue;
-      for (auto fi = tt.d.footpaths_in_index[dest_loc];
-           fi != tt.d.footpaths_in_index[dest_loc + 1]; ++fi) {
-        auto const fp = tt.d.footpaths_in[fi];
+      for (auto fi = tt.fp_index(false)[dest_loc];
+           fi != tt.fp_index(false)[dest_loc + 1]; ++fi) {
+        auto const fp = tt.fp_words(false)[fi];
         if (B2R_FP_TARGET(fp) != sloc(transport_leg, s)) continue;
         auto const fp_dur =
             adjusted<int16_t>(jq.tts, static_cast<int16_t>(B2R_FP_DURATION(fp)));
@@ -1510,9 +1550,9 @@ struct reconstructor {
           if (!B2R_STOP_IN(sword(leg_to, stt))) continue;
           auto const lf = sloc(leg_from, sf);
           auto const lt = sloc(leg_to, stt);
-          for (auto fi = tt.d.footpaths_out_index[lf];
-               fi != tt.d.footpaths_out_index[lf + 1]; ++fi) {
-            auto const fp = tt.d.footpaths_out[fi];
+          for (auto fi = tt.fp_index(true)[lf];
+               fi != tt.fp_index(true)[lf + 1]; ++fi) {
+            auto const fp = tt.fp_words(true)[fi];
             if (B2R_FP_TARGET(fp) != lt) continue;
             auto const fp_dur =
                 adjusted<int16_t>(jq.tts, static_cast<int16_t>(B2R_FP_DURATION(fp)));
@@ -1839,8 +1879,8 @@ std::optional<leg_t> lookup_footpath(tt_view const& tt, query_t const& q, uint32
     }
     if (!use_footpaths) continue;
     auto eff = kFpMaxDuration;
-    auto const& idx = boarding ? tt.d.footpaths_out_index : tt.d.footpaths_in_index;
-    auto const* fps = boarding ? tt.d.footpaths_out : tt.d.footpaths_in;
+    auto const* idx = tt.fp_index(boarding);
+    auto const* fps = tt.fp_words(boarding);
     for (auto fi = idx[l]; fi != idx[l + 1]; ++fi) {
       if (B2R_FP_TARGET(fps[fi]) != loc) continue;
       auto const adj =
@@ -1873,11 +1913,11 @@ std::optional<std::array<leg_t, 3>> first_direct_journey(tt_view const& tt, quer
                                                          unixtime time) {
   auto const from = q.start.front().target, to = q.dest.front().target;
   std::vector<uint32_t> boarding{from}, alighting{to};
-  for (auto fi = tt.d.footpaths_out_index[from]; fi != tt.d.footpaths_out_index[from + 1]; ++fi) {
-    boarding.push_back(B2R_FP_TARGET(tt.d.footpaths_out[fi]));
+  for (auto fi = tt.fp_index(true)[from]; fi != tt.fp_index(true)[from + 1]; ++fi) {
+    boarding.push_back(B2R_FP_TARGET(tt.fp_words(true)[fi]));
   }
-  for (auto fi = tt.d.footpaths_in_index[to]; fi != tt.d.footpaths_in_index[to + 1]; ++fi) {
-    alighting.push_back(B2R_FP_TARGET(tt.d.footpaths_in[fi]));
+  for (auto fi = tt.fp_index(false)[to]; fi != tt.fp_index(false)[to + 1]; ++fi) {
+    alighting.push_back(B2R_FP_TARGET(tt.fp_words(false)[fi]));
   }
   auto const has = [](std::vector<uint32_t> const& v, uint32_t x) {
     return std::find(v.begin(), v.end(), x) != v.end();
@@ -1922,7 +1962,7 @@ std::optional<std::array<leg_t, 3>> first_direct_journey(tt_view const& tt, quer
       auto const stp = tt.stop(r, i);
       auto const loc = B2R_STOP_LOC(stp);
       if (board.has_value()) {
-        if (!has(alighting, loc) || !B2R_STOP_OUT(stp)) continue;
+        if (!has(alighting, loc) || !tt.stop_out(stp)) continue;  // out_allowed(prf_idx)
         auto const a = *board, b = i;
         board.reset();
         // sections_violate_constraints, direct.cc:242-260
@@ -1958,7 +1998,7 @@ std::optional<std::array<leg_t, 3>> first_direct_journey(tt_view const& tt, quer
             break;
           }
         }
-      } else if (has(boarding, loc) && B2R_STOP_IN(stp)) {
+      } else if (has(boarding, loc) && tt.stop_in(stp)) {
         board = i;
       }
     }
@@ -2177,9 +2217,10 @@ extern "C" {
 
 int or_search(const b2r_timetable_desc* tt, const b2r_query* q, or_result** out) {
   if (tt == nullptr || q == nullptr || out == nullptr) return B2R_ERR_INVALID_ARGUMENT;
+  if (q->prf_idx >= B2R_N_PROFILES) return B2R_ERR_INVALID_ARGUMENT;  // profile_idx_t < kNProfiles
   try {
     auto res = std::make_unique<or_result>();
-    oracle::tt_view const v{*tt};
+    oracle::tt_view const v{*tt, q->prf_idx};
     auto const qq = oracle::to_query(*q);
     auto const fwd = q->direction == B2R_FORWARD;
     if (q->kind == B2R_ONE_TO_ALL) {
@@ -2271,7 +2312,7 @@ int or_earliest_alternative(const b2r_timetable_desc* tt, const b2r_query* q, ui
                             uint32_t to, int32_t from_arr, int32_t to_dep, b2r_leg* legs) {
   if (tt == nullptr || q == nullptr || legs == nullptr) return B2R_ERR_INVALID_ARGUMENT;
   try {
-    oracle::tt_view const v{*tt};
+    oracle::tt_view const v{*tt, q->prf_idx};
     auto const qq = oracle::to_query(*q);
     auto const r = oracle::get_earliest_alternative(v, qq, from, to, from_arr, to_dep);
     if (!r.has_value()) return 0;
@@ -2303,7 +2344,7 @@ int or_earliest_alternative(const b2r_timetable_desc* tt, const b2r_query* q, ui
 int or_get_starts(const b2r_timetable_desc* tt, const b2r_query* q, int32_t* tas,
                   int32_t* tst, uint32_t* stop, uint32_t capacity, uint32_t* n) {
   try {
-    oracle::tt_view const v{*tt};
+    oracle::tt_view const v{*tt, q->prf_idx};
     auto qq = oracle::to_query(*q);
     qq.sanitize();
     auto const fwd = q->direction == B2R_FORWARD;
@@ -2328,7 +2369,7 @@ int or_get_starts(const b2r_timetable_desc* tt, const b2r_query* q, int32_t* tas
 
 int or_lower_bounds(const b2r_timetable_desc* tt, const b2r_query* q, uint16_t* dists) {
   try {
-    oracle::tt_view const v{*tt};
+    oracle::tt_view const v{*tt, q->prf_idx};
     auto qq = oracle::to_query(*q);
     qq.sanitize();
     std::vector<uint16_t> lb;
