@@ -197,7 +197,7 @@ typedef struct b2r_offset {
 } b2r_offset;
 
 /* routing::query, query.h:70-100, restricted to the static (no rtt, no
- * vias, no td offsets, profile 0) instantiation. */
+ * vias, no td offsets) instantiation. */
 typedef struct b2r_query {
   uint8_t kind;      /* b2r_query_kind */
   uint8_t direction; /* b2r_direction */

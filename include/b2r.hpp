@@ -13,8 +13,9 @@
  *  - routing::one_to_all        include/nigiri/routing/one_to_all.h:22-25
  *  - routing::raptor_state      round_times_ of raptor_state.h:22-111
  * restricted to what the engine runs: the static timetable (no real-time
- * overlay), no vias, no time-dependent offsets, no wheelchair profile
- * (profile 0); class, bike, car and reservation filters included.  Times are minutes since the epoch
+ * overlay), no vias, no time-dependent offsets; footpath profiles (the
+ * wheelchair profile among them) and the class, bike, car and reservation
+ * filters included.  Times are minutes since the epoch
  * (unixtime_t), durations minutes.
  *
  * Errors: every call that fails throws b2r::error with the C ABI's status

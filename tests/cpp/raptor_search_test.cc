@@ -3,7 +3,8 @@
 // (b2r.hpp -> the B200 engine) and through the CPU oracle (test
 // infrastructure), and the complete journeys (every leg) must be equal.
 // Range queries also run through pong_search (walking allowed at the
-// start, as at the destination).  One-to-all searches compare the round
+// start, as at the destination), and the first queries again in the
+// wheelchair profile.  One-to-all searches compare the round
 // times of every location.
 //
 //   raptor_search_test            exit 0 when every query matches
@@ -46,6 +47,8 @@ r::query from_c(b2r_query const& c) {  // the generator's queries in nigiri's te
   q.require_bike_transport_ = c.require_bike_transport != 0;
   q.require_car_transport_ = c.require_car_transport != 0;
   q.no_compulsory_reservation_ = c.no_compulsory_reservation != 0;
+  q.prf_idx_ = c.prf_idx;
+  if (c.has_max_interval != 0) q.max_interval_ = r::interval{c.max_interval_from, c.max_interval_to};
   return q;
 }
 
@@ -133,6 +136,30 @@ int run_workload(uint32_t workload, uint32_t timetable_seed, uint32_t n, uint64_
         std::printf("workload %u pong query %u (%s) differs\n", workload, i,
                     dir == r::direction::kForward ? "forward" : "backward");
         print("engine", pongs[i].journeys_);
+        print("oracle", want);
+      }
+    }
+  }
+  // the wheelchair profile on the first one-to-one queries, both directions
+  for (auto dir : {r::direction::kForward, r::direction::kBackward}) {
+    std::vector<r::query> batch;
+    std::vector<b2r_query> cw;
+    for (auto i = 0U; i != n_q && cw.size() != 20U; ++i) {
+      auto c = *b2r_queries_get(qs, i);
+      if (c.kind != B2R_ONE_TO_ONE || c.direction != static_cast<uint8_t>(dir)) continue;
+      c.prf_idx = B2R_PROFILE_WHEELCHAIR;
+      cw.push_back(c);
+      batch.push_back(from_c(c));
+    }
+    if (batch.empty()) continue;
+    auto const got = r::raptor_search(eng, batch, dir);
+    for (auto i = 0U; i != batch.size(); ++i) {
+      auto const want = oracle_journeys(d, cw[i]);
+      n_journeys += want.size();
+      if (got[i].status_ != B2R_OK || got[i].journeys_ != want) {
+        ++bad;
+        std::printf("workload %u wheelchair query %u differs\n", workload, i);
+        print("engine", got[i].journeys_);
         print("oracle", want);
       }
     }
