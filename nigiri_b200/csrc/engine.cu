@@ -306,28 +306,37 @@ __global__ void k_lb_fill(dev::state st, lb_group const* groups, lb_entry const*
                           uint8_t const* payload) {
   __shared__ uint16_t tile[32][kLbTile + 2];
   auto const grp = groups[blockIdx.y];
-  auto const n_loc = st.tt.n_loc;
+  auto const stride = st.lb_stride;  // table row length, a multiple of 8
   auto const x0 = blockIdx.x * kLbTile;
-  for (auto e = 0u; e != grp.count; ++e) {
-    auto const en = entries[grp.first + e];
-    auto const* seeds = reinterpret_cast<uint32_t const*>(payload + en.off_seeds);
-    auto const* tab = en.fwd ? st.lb_table_fwd : st.lb_table_bwd;
-    for (auto xi = threadIdx.x; xi < kLbTile; xi += blockDim.x) {
-      auto const x = x0 + xi;
-      uint32_t best = 0xFFFFu;
-      if (x < n_loc) {
-        for (auto i = 0u; i != en.n_seeds; ++i) {
-          auto const m = seeds[2 * i];
-          auto const d = tab[static_cast<size_t>(m) * n_loc + x];
+  // work items (entry, chunk of 8 locations): one 16-byte table load per
+  // seed and chunk, eight running minima
+  constexpr uint32_t kChunks = kLbTile / 8u;
+  for (auto item = threadIdx.x; item < grp.count * kChunks; item += blockDim.x) {
+    auto const e = item / kChunks, ch = item % kChunks;
+    auto const xc = x0 + ch * 8u;
+    uint32_t best[8];
+    for (auto j = 0u; j != 8u; ++j) best[j] = 0xFFFFu;
+    if (xc < stride) {  // the chunk lies inside the row (stride % 8 == 0)
+      auto const en = entries[grp.first + e];
+      auto const* seeds = reinterpret_cast<uint32_t const*>(payload + en.off_seeds);
+      auto const* tab = en.fwd ? st.lb_table_fwd : st.lb_table_bwd;
+      for (auto i = 0u; i != en.n_seeds; ++i) {
+        auto const m = seeds[2 * i];
+        auto const sd = seeds[2 * i + 1];
+        auto const v = *reinterpret_cast<uint4 const*>(tab + static_cast<size_t>(m) * stride + xc);
+        uint32_t const w[4] = {v.x, v.y, v.z, v.w};
+        for (auto j = 0u; j != 8u; ++j) {
+          auto const d = (w[j >> 1] >> (16u * (j & 1u))) & 0xFFFFu;
           if (d == 0xFFFFu) continue;
-          auto const c = seeds[2 * i + 1] + d;
-          if ((c <= B2R_MAX_TRAVEL_TIME_MIN || x == m) && c < best) best = c;
+          auto const c = sd + d;
+          if ((c <= B2R_MAX_TRAVEL_TIME_MIN || xc + j == m) && c < best[j]) best[j] = c;
         }
       }
-      tile[e][xi] = static_cast<uint16_t>(best);
     }
+    for (auto j = 0u; j != 8u; ++j) tile[e][ch * 8u + j] = static_cast<uint16_t>(best[j]);
   }
   __syncthreads();
+  auto const n_loc = st.tt.n_loc;
   for (auto i = threadIdx.x; i < kLbTile * 32u; i += blockDim.x) {
     auto const xi = i / 32u, e = i % 32u;
     auto const x = x0 + xi;
@@ -638,27 +647,29 @@ void ensure_lb_table(b2r_timetable& t, unsigned threads) {
   std::lock_guard<std::mutex> lock{t.lb_table_mutex};
   if (t.lb_table[0] != nullptr) return;
   auto const n = static_cast<size_t>(t.d.n_loc);
+  auto const stride = (n + 7U) / 8U * 8U;  // rows 16-byte aligned for vector loads, padding unreachable
   constexpr size_t kBlock = 1024;
-  std::vector<uint16_t> buf(kBlock * n);
+  std::vector<uint16_t> buf(kBlock * stride, uint16_t{0xFFFFu});
   for (auto dir = 0; dir != 2; ++dir) {
-    auto* dst = dmalloc<uint16_t>(n * n, t.bytes);
+    auto* dst = dmalloc<uint16_t>(n * stride, t.bytes);
     t.allocs.push_back(dst);
     for (size_t b = 0; b < n; b += kBlock) {
       auto const rows = std::min(kBlock, n - b);
       std::atomic<size_t> next{0};
       auto work = [&]() {
         for (auto r = next++; r < rows; r = next++) {
-          lb_table_row(t.view, dir == 0, static_cast<uint32_t>(b + r), buf.data() + r * n);
+          lb_table_row(t.view, dir == 0, static_cast<uint32_t>(b + r), buf.data() + r * stride);
         }
       };
       std::vector<std::thread> pool;
       for (auto i = 1U; i < threads; ++i) pool.emplace_back(work);
       work();
       for (auto& th : pool) th.join();
-      B2R_CUDA(cudaMemcpy(dst + b * n, buf.data(), rows * n * sizeof(uint16_t), cudaMemcpyHostToDevice));
+      B2R_CUDA(cudaMemcpy(dst + b * stride, buf.data(), rows * stride * sizeof(uint16_t), cudaMemcpyHostToDevice));
     }
     t.lb_table[dir] = dst;
   }
+  t.lb_stride = static_cast<uint32_t>(stride);
 }
 
 // one admission: a query (or the next phase of one) into slot `slot`
@@ -2093,6 +2104,7 @@ int b2r_engine_create(b2r_timetable* tt, const b2r_engine_config* cfg_in, b2r_en
       al(st.lb_mask, G);
       st.lb_table_fwd = tt->lb_table[0];
       st.lb_table_bwd = tt->lb_table[1];
+      st.lb_stride = tt->lb_stride;
       B2R_CUDA(cudaMemset(st.dist, 0xFF, static_cast<size_t>(nl) * S * 4));
       B2R_CUDA(cudaMemset(st.F[0], 0, static_cast<size_t>(nl) * G * 4));
       B2R_CUDA(cudaMemset(st.F[1], 0, static_cast<size_t>(nl) * G * 4));

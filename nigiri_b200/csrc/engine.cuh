@@ -237,6 +237,7 @@ struct state {
   // all-pairs lower-bound tables (forward / backward search), or null
   uint16_t const* lb_table_fwd;
   uint16_t const* lb_table_bwd;
+  uint32_t lb_stride;  // table row length (n_loc rounded up to 8)
   // pong bounds (raptor_state::bounds_storage_): rows of the ping's round
   // times folded over the rounds, as keys of the bounded (pong) search
   int16_t* bounds;  // [K][n_loc][S]

@@ -38,6 +38,7 @@ struct b2r_timetable {
   // unreachable) for forward and backward searches, built by the first
   // engine that uses them
   uint16_t* lb_table[2]{nullptr, nullptr};
+  uint32_t lb_stride{0};  // row length: n_locations rounded up to a multiple of 8
   std::mutex lb_table_mutex;
 
   ~b2r_timetable() {
