@@ -189,19 +189,53 @@ __global__ void k_mark_routes(state st) {
 }
 
 // list of the words of W[0, n) that are nonzero, one counter add per warp
+// The indices of the non-zero words of W[0, n) appended to `list` (in no
+// particular order).  Each thread reads 4 words with one 16-byte load
+// (W comes from cudaMalloc and i is a multiple of 4), the block scans the
+// counts and reserves its range with one atomicAdd per 4 * blockDim words.
 __device__ __forceinline__ void list_nonzero(state const& st, uint32_t const* W, uint32_t n,
                                              uint32_t* list, uint32_t counter) {
-  auto const lane = threadIdx.x & 31u;
-  auto const stride = gridDim.x * blockDim.x;
-  for (auto i0 = blockIdx.x * blockDim.x; i0 < n; i0 += stride) {
-    auto const i = i0 + threadIdx.x;
-    auto const on = i < n && W[i] != 0u;
-    auto const m = __ballot_sync(kFull, on);
-    if (m == 0u) continue;
-    uint32_t at = 0;
-    if (lane == 0) at = atomicAdd(&st.counters[counter], static_cast<uint32_t>(__popc(m)));
-    at = __shfl_sync(kFull, at, 0);
-    if (on) list[at + static_cast<uint32_t>(__popc(m & ((1u << lane) - 1u)))] = i;
+  __shared__ uint32_t warp_off[32];
+  __shared__ uint32_t base;
+  auto const lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, n_warps = blockDim.x >> 5;
+  auto const per_block = blockDim.x * 4u;
+  for (auto b0 = blockIdx.x * per_block; b0 < n; b0 += gridDim.x * per_block) {
+    auto const i = b0 + threadIdx.x * 4u;
+    uint32_t w[4] = {0u, 0u, 0u, 0u};
+    if (i + 3u < n) {
+      auto const v = *reinterpret_cast<uint4 const*>(W + i);
+      w[0] = v.x;
+      w[1] = v.y;
+      w[2] = v.z;
+      w[3] = v.w;
+    } else {
+      for (auto j = 0u; j != 4u; ++j) w[j] = i + j < n ? W[i + j] : 0u;
+    }
+    auto const cnt = static_cast<uint32_t>(w[0] != 0u) + static_cast<uint32_t>(w[1] != 0u) +
+                     static_cast<uint32_t>(w[2] != 0u) + static_cast<uint32_t>(w[3] != 0u);
+    auto incl = cnt;  // inclusive scan over the warp
+    for (auto d = 1u; d < 32u; d <<= 1) {
+      auto const y = __shfl_up_sync(kFull, incl, d);
+      if (lane >= d) incl += y;
+    }
+    if (lane == 31u) warp_off[warp] = incl;
+    __syncthreads();
+    if (warp == 0u) {  // scan of the warp totals, then the block's reservation
+      auto const ws = lane < n_warps ? warp_off[lane] : 0u;
+      auto x = ws;
+      for (auto d = 1u; d < 32u; d <<= 1) {
+        auto const y = __shfl_up_sync(kFull, x, d);
+        if (lane >= d) x += y;
+      }
+      if (lane < n_warps) warp_off[lane] = x - ws;
+      if (lane == 31u) base = x != 0u ? atomicAdd(&st.counters[counter], x) : 0u;
+    }
+    __syncthreads();
+    auto at = base + warp_off[warp] + (incl - cnt);
+    for (auto j = 0u; j != 4u; ++j) {
+      if (w[j] != 0u) list[at++] = i + j;
+    }
+    __syncthreads();  // warp_off and base are reused by the next pass
   }
 }
 
