@@ -172,23 +172,56 @@ __global__ void k_ctl_dest(state st) {
 }
 
 // station marks -> route marks (raptor.h:228-241)
+// A warp takes 32 marked (location, group) words and spreads their
+// (word, route) pairs over its lanes, so that hub stations with many routes
+// do not hold one lane.  The per-group "any route marked" word is read
+// before its atomicOr: it only gains bits during the kernel, so a read that
+// shows the bits set makes the atomic redundant, and same-address atomics
+// would queue in L2.
 __global__ void k_mark_routes(state st) {
   auto const nx = st.counters[C_X];
-  for (auto i = blockIdx.x * blockDim.x + threadIdx.x; i < nx; i += gridDim.x * blockDim.x) {
-    auto const e = st.xlist[i];
-    auto const g = e % st.G, l = e / st.G;
-    auto const w = st.X[e] & st.run_mask[g];
-    if (w == 0u) continue;
-    auto const rb = st.tt.loc_routes_idx[l], re = st.tt.loc_routes_idx[l + 1];
-    if (rb == re) continue;
-    atomicOr(&st.any_mask[g], w);
-    for (auto ri = rb; ri != re; ++ri) {
-      atomicOr(&st.R[st.tt.loc_routes[ri] * st.G + g], w);  // listed by k_list_routes
+  auto const lane = threadIdx.x & 31u;
+  auto const warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  auto const n_warps = (gridDim.x * blockDim.x) >> 5;
+  for (auto w0 = warp * 32u; w0 < nx; w0 += n_warps * 32u) {
+    auto const i = w0 + lane;
+    uint32_t g = 0, w = 0, rb = 0, cnt = 0;
+    if (i < nx) {
+      auto const e = st.xlist[i];
+      g = e % st.G;
+      auto const l = e / st.G;
+      w = st.X[e] & st.run_mask[g];
+      if (w != 0u) {
+        rb = st.tt.loc_routes_idx[l];
+        cnt = st.tt.loc_routes_idx[l + 1] - rb;
+        if (cnt != 0u && (st.any_mask[g] & w) != w) atomicOr(&st.any_mask[g], w);
+      }
+    }
+    auto end = cnt;  // inclusive prefix sum of the route counts
+    for (auto o = 1u; o < 32u; o <<= 1) {
+      auto const v = __shfl_up_sync(kFull, end, o);
+      if (lane >= o) end += v;
+    }
+    auto const total = __shfl_sync(kFull, end, 31);
+    for (auto p0 = 0u; p0 < total; p0 += 32u) {
+      auto const p = p0 + lane;
+      uint32_t owner = 0;  // first lane whose prefix end exceeds p
+      for (auto b = 16u; b > 0u; b >>= 1) {
+        if (__shfl_sync(kFull, end, static_cast<int>(owner + b - 1u)) <= p) owner += b;
+      }
+      auto const o_first = __shfl_sync(kFull, end, static_cast<int>(owner)) -
+                           __shfl_sync(kFull, cnt, static_cast<int>(owner));
+      auto const o_rb = __shfl_sync(kFull, rb, static_cast<int>(owner));
+      auto const o_g = __shfl_sync(kFull, g, static_cast<int>(owner));
+      auto const o_w = __shfl_sync(kFull, w, static_cast<int>(owner));
+      if (p < total) {
+        auto const r = st.tt.loc_routes[o_rb + (p - o_first)];
+        atomicOr(&st.R[r * st.G + o_g], o_w);  // listed by k_list_routes
+      }
     }
   }
 }
 
-// list of the words of W[0, n) that are nonzero, one counter add per warp
 // The indices of the non-zero words of W[0, n) appended to `list` (in no
 // particular order).  Each thread reads 4 words with one 16-byte load
 // (W comes from cudaMalloc and i is a multiple of 4), the block scans the
