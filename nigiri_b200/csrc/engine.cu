@@ -643,16 +643,28 @@ void solve_lower_bounds(b2r_engine& e, cudaStream_t s) {
 // Dijkstra distances from location s over the forward- / backward-search
 // lower-bound graph.  Built on the host threads in row blocks and uploaded
 // block by block; kept with the timetable for every later engine.
+// Both tables and the stride are published together once both are built:
+// an exception half way leaves the timetable without tables (lb_stride 0),
+// never with one of them.
 void ensure_lb_table(b2r_timetable& t, unsigned threads) {
   std::lock_guard<std::mutex> lock{t.lb_table_mutex};
-  if (t.lb_table[0] != nullptr) return;
+  if (t.lb_stride != 0U) return;
   auto const n = static_cast<size_t>(t.d.n_loc);
   auto const stride = (n + 7U) / 8U * 8U;  // rows 16-byte aligned for vector loads, padding unreachable
   constexpr size_t kBlock = 1024;
   std::vector<uint16_t> buf(kBlock * stride, uint16_t{0xFFFFu});
+  uint16_t* built[2] = {nullptr, nullptr};
+  struct guard {  // frees what was built unless published
+    uint16_t** p;
+    ~guard() {
+      for (auto i = 0; i != 2; ++i)
+        if (p[i] != nullptr) cudaFree(p[i]);
+    }
+  } g{built};
+  uint64_t bytes = 0;
   for (auto dir = 0; dir != 2; ++dir) {
-    auto* dst = dmalloc<uint16_t>(n * stride, t.bytes);
-    t.allocs.push_back(dst);
+    auto* dst = dmalloc<uint16_t>(n * stride, bytes);
+    built[dir] = dst;
     for (size_t b = 0; b < n; b += kBlock) {
       auto const rows = std::min(kBlock, n - b);
       std::atomic<size_t> next{0};
@@ -667,8 +679,13 @@ void ensure_lb_table(b2r_timetable& t, unsigned threads) {
       for (auto& th : pool) th.join();
       B2R_CUDA(cudaMemcpy(dst + b * stride, buf.data(), rows * stride * sizeof(uint16_t), cudaMemcpyHostToDevice));
     }
-    t.lb_table[dir] = dst;
   }
+  for (auto dir = 0; dir != 2; ++dir) {
+    t.lb_table[dir] = built[dir];
+    t.allocs.push_back(built[dir]);
+    built[dir] = nullptr;
+  }
+  t.bytes += bytes;
   t.lb_stride = static_cast<uint32_t>(stride);
 }
 
@@ -1914,6 +1931,53 @@ int b2r_timetable_upload(const b2r_timetable_desc* d, int device, b2r_timetable*
         }
       }
 
+      // trip order check for the route scan's parallel boarding: the trips
+      // (transport, service day) of a route must compare the same way at
+      // every event of the route, equal at all or strictly ordered at all.
+      // A trip on day d is its transport's times shifted by d days, so with
+      // the transports sorted by their first departure within its day, the
+      // neighbours (and the last against the first one day later) cover
+      // every pair: consistent neighbours order all trips consistently.
+      std::vector<uint8_t> fifo(nr, 1U);
+      {
+        std::vector<uint32_t> ord;
+        std::vector<int32_t> shift;
+        for (auto r = 0U; r != nr; ++r) {
+          auto const n_t = d->route_transport_to[r] - d->route_transport_from[r];
+          auto const n_s = d->route_stop_index[r + 1] - d->route_stop_index[r];
+          if (n_s < 2U || n_t == 0U) continue;
+          auto const n_slots = 2U * (n_s - 1U);
+          auto const* c = d->route_stop_times + d->route_stop_time_from[r];
+          auto const count = [&](uint32_t slot, uint32_t x) {
+            auto const w = c[slot * n_t + x];
+            return static_cast<int32_t>(w & 31U) * 1440 + static_cast<int32_t>(w >> 5);
+          };
+          ord.resize(n_t);
+          shift.resize(n_t);
+          for (auto x = 0U; x != n_t; ++x) {
+            ord[x] = x;
+            auto const c0 = count(0U, x);
+            shift[x] = (c0 >= 0 ? c0 / 1440 : -((-c0 + 1439) / 1440)) * 1440;
+          }
+          std::stable_sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) {
+            return count(0U, a) - shift[a] < count(0U, b) - shift[b];
+          });
+          for (auto q = 0U; q != n_t && fifo[r] != 0U; ++q) {
+            auto const a = ord[q];
+            auto const wrap = q + 1U == n_t;
+            auto const b = wrap ? ord[0] : ord[q + 1U];
+            auto const off = (wrap ? 1440 : 0) - shift[b] + shift[a];
+            bool all_zero = true, all_pos = true;
+            for (auto slot = 0U; slot != n_slots; ++slot) {
+              auto const diff = count(slot, b) + off - count(slot, a);
+              all_zero = all_zero && diff == 0;
+              all_pos = all_pos && diff > 0;
+            }
+            if (!all_zero && !all_pos) fifo[r] = 0U;
+          }
+        }
+      }
+
       auto& dd = t->d;
       dd.n_loc = nl;
       dd.n_routes = nr;
@@ -1959,6 +2023,7 @@ int b2r_timetable_upload(const b2r_timetable_desc* d, int device, b2r_timetable*
       dd.loc_routes_idx = up(d->location_routes_index, nl + 1);
       dd.loc_routes = up(d->location_routes, d->location_routes_index[nl]);
       dd.route_sorted = up(sorted.data(), nr);
+      dd.route_fifo = up(fifo.data(), nr);
       dd.route_filter = up(rfilter.data(), nr);
       dd.route_sec = up(rsec.data(), rsec.size());
       dd.lbg_fwd_idx = up(d->lb_fwd_index, nl + 1);

@@ -68,6 +68,9 @@ struct dtt {
   uint32_t const* loc_routes_idx;
   uint32_t const* loc_routes;
   uint8_t const* route_sorted;  // 1: every event column is ordered by mam
+  // 1: the route's trips (transport, service day) compare the same way at
+  // every event of the route, equal at all or strictly ordered at all
+  uint8_t const* route_fifo;
   // lower-bound graphs (build_lb_graph.h), packed footpath words
   uint32_t const* lbg_fwd_idx;
   uint32_t const* lbg_fwd;

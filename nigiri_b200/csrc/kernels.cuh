@@ -287,177 +287,272 @@ __global__ void k_ctl_marked(state st) {
 }
 
 // ------------------------------------------------------------ route scan
-// update_route, raptor.h:1177-1349 (no vias) for every
-// (route, query) pair marked this round.  A warp takes 32 marked (route,
-// group of 32 queries) entries, lists their (route, query) pairs and gives
-// one pair to each lane per pass: resident queries are unrelated, so an
-// entry holds few queries, and a lane per query of one entry would leave
-// most lanes idle.  Each lane walks its route in search direction carrying
-// its query's current trip, with the next stops' words, station marks and
-// lower bounds loaded ahead.  Labels are combined with atomicMin and marks
-// with atomicOr, so the order of the pairs does not matter.
-__global__ void __launch_bounds__(256, 3) k_route_scan(state st) {
-  auto const lane = threadIdx.x & 31u;
-  auto const warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  auto const n_warps = (gridDim.x * blockDim.x) >> 5;
-  auto const nr = st.counters[C_R];
-  auto const& T = st.tt;
-  uint32_t p_ev = 0, p_days = 0, p_writes = 0, p_stops = 0;
-  for (auto w0 = warp * 32u; w0 < nr; w0 += n_warps * 32u) {
-    // lane: entry w0 + lane, its query mask and the inclusive prefix sum
-    auto const w = w0 + lane;
-    uint32_t e = 0, mask = 0;
-    if (w < nr) {
-      e = st.rlist[w];
-      mask = st.R[e];
-      st.R[e] = 0u;
+// update_route, raptor.h:1177-1349 (no vias), for every (route, query) pair
+// marked this round.
+//
+// The reference walks a route's stops in order, carrying the trip it rides
+// (et).  At a stop marked last round it looks up the earliest trip
+// boardable there (get_earliest_transport) and switches to it when that
+// trip is at least as good at this stop as the current one; at every stop
+// it improves the arrival label with the current trip.  Walked like that,
+// one (route, query) pair is a chain of dependent loads as long as the
+// route.
+//
+// Here a warp takes one pair and its lanes take the stops, 32 at a time:
+// * every boardable stop looks up its own earliest trip at once (the
+//   lookup depends only on that stop's labels);
+// * on a route whose trips keep one order at every event
+//   (b2r_timetable: route_fifo), "switch when at least as good at this
+//   stop" is "keep the best trip so far, the later stop on ties", whatever
+//   stop compares them, so a warp prefix-minimum over the lanes gives the
+//   trip each stop is reached by;
+// * every stop then reads its arrival event of that trip.
+// The result equals the sequential walk's; routes without that order,
+// queries with per-section filters and a boarding without a current best
+// label (which the round structure rules out) take the sequential walk.
+// Labels are combined with atomicMin and marks with atomicOr, so the order
+// of the pairs does not matter.
+
+struct scan_ctr {
+  uint32_t stops, ev, days, writes, warp_steps;
+};
+
+// the stop word at position i of route (sb, n) in search direction; for the
+// wheelchair profile with its wheelchair bits in place of the in / out bits
+// (can_start / can_finish, raptor.h:1252, 1304)
+__device__ __forceinline__ uint32_t scan_stop_word(dtt const& T, uint32_t sb, uint32_t n, bool fwd, uint32_t i,
+                                                   uint32_t sec) {
+  auto const w = T.route_stops[sb + (fwd ? i : n - 1u - i)];
+  return (sec & 0x100u) != 0u ? (w & 0xCFFFFFFFu) | ((w >> 2) & 0x30000000u) : w;
+}
+
+// the arrival-side label update of one stop (raptor.h:1242-1302)
+__device__ __forceinline__ void scan_arrive(state const& st, lane_t const& ln, uint32_t s, uint32_t g, uint32_t bit,
+                                            uint32_t l, uint16_t lbv, int by, scan_ctr& pc) {
+  if (by <= ln.tad_k && lbv != 0xFFFFu && by + static_cast<int>(lbv) <= ln.tad_k &&
+      (ln.blast == 0u || within_bounds(st, s, ln.blast, ln.k, l, by))) {
+    auto const word = enc(ln.gtag, by);
+    auto* tp = &st.tmp[li(st, l, s)];
+    if (st.profile) {
+      if (word < atomicMin(tp, word)) ++pc.writes;
+    } else {
+      atomicMin(tp, word);  // result unused: no round trip
     }
-    auto const cnt = static_cast<uint32_t>(__popc(mask));
-    auto end = cnt;
-    for (auto o = 1u; o < 32u; o <<= 1) {
-      auto const v = __shfl_up_sync(kFull, end, o);
-      if (lane >= o) end += v;
-    }
-    auto const total = __shfl_sync(kFull, end, 31);
-    for (auto p0 = 0u; p0 < total; p0 += 32u) {
-      auto const p = p0 + lane;
-      uint32_t owner = 0;  // first lane whose prefix end exceeds p
-      for (auto b = 16u; b > 0u; b >>= 1) {
-        if (__shfl_sync(kFull, end, static_cast<int>(owner + b - 1u)) <= p) owner += b;
-      }
-      auto const o_e = __shfl_sync(kFull, e, static_cast<int>(owner));
-      auto o_mask = __shfl_sync(kFull, mask, static_cast<int>(owner));
-      auto const o_first = __shfl_sync(kFull, end, static_cast<int>(owner)) -
-                           __shfl_sync(kFull, cnt, static_cast<int>(owner));
-      if (p >= total) continue;
-      for (auto x = p - o_first; x != 0u; --x) o_mask &= o_mask - 1u;
-      auto const b = static_cast<uint32_t>(__ffs(o_mask) - 1);
-      auto const g = o_e % st.G, r = o_e / st.G;
-      auto const s = g * 32u + b;
-      auto const ln = st.lanes[s];
-      if (!ln.run) continue;
-      uint32_t sec = 0u;  // required flags checked per section (bits 0-3); bit 8: wheelchair profile
-      if ((ln.claszes != 0xFFFFu || ln.req != 0u) && !route_allowed(T, r, ln.claszes, ln.req, sec)) continue;
-      if ((ln.mode & 0x70u) == (B2R_PROFILE_WHEELCHAIR << 4)) sec |= 0x100u;
-      auto const bit = 1u << b;
-      auto const fwd = ln.fwd != 0;
-      auto const k = static_cast<uint32_t>(ln.k);
-      auto const sb = T.route_stop_idx[r];
-      auto const n = T.route_stop_idx[r + 1] - sb;
-      auto const n_t = T.route_tr_to[r] - T.route_tr_from[r];
-      auto const* colbase = T.st + T.route_st_from[r];
-      // the stop word; for the wheelchair profile with its wheelchair bits in
-      // place of the in / out bits (can_start / can_finish, raptor.h:1252, 1304)
-      auto const stop_word = [&](uint32_t i) {
-        auto const w = T.route_stops[sb + (fwd ? i : n - 1u - i)];
-        return (sec & 0x100u) != 0u ? (w & 0xCFFFFFFFu) | ((w >> 2) & 0x30000000u) : w;
-      };
-      bool et_valid = false;
-      uint32_t et_off = 0;
-      uint16_t et_day = 0;
-      uint16_t ev = 0;  // arrival event of the current trip at this stop
-      // loads ahead: stop word two stops ahead, mark, bound and the current
-      // trip's arrival event one ahead
-      auto stp = stop_word(0);
-      auto xw = st.X[B2R_STOP_LOC(stp) * st.G + g];
-      auto const lb_off = (ln.mode & 8u) != 0u;
-      auto lbv = lb_off ? uint16_t{0} : st.lb[li(st, B2R_STOP_LOC(stp), s)];
-      auto stp_next = n > 1u ? stop_word(1) : 0u;
-      for (auto i = 0u; i != n; ++i) {
-        ++p_stops;
-        auto const stp_after = i + 2u < n ? stop_word(i + 2u) : 0u;
-        uint32_t xw_next = 0;
-        uint16_t lb_next = 0;
-        if (i + 1u < n) {
-          auto const ln_next = B2R_STOP_LOC(stp_next);
-          xw_next = st.X[ln_next * st.G + g];
-          lb_next = lb_off ? uint16_t{0} : st.lb[li(st, ln_next, s)];
-        }
-        auto const si = fwd ? i : n - 1u - i;
-        auto const l = B2R_STOP_LOC(stp);
-        auto const can_finish = fwd ? B2R_STOP_OUT(stp) : B2R_STOP_IN(stp);
-        auto const can_start = fwd ? B2R_STOP_IN(stp) : B2R_STOP_OUT(stp);
-        if (sec != 0u && i != 0u && !section_ok(T, sb, fwd ? i - 1u : si, sec & 15u)) {
-          et_valid = false;  // raptor.h:1194-1217: the section ridden lacks a flag
-        }
-        bool arrival_ran = false;
-        if (et_valid && can_finish) {
-          arrival_ran = true;
-          auto const by = to_delta_key(fwd, et_day, ln.base, delta_count(ev));
-          if (by <= ln.tad_k && lbv != 0xFFFFu && by + static_cast<int>(lbv) <= ln.tad_k &&
-              (ln.blast == 0u || within_bounds(st, s, ln.blast, k, l, by))) {
-            auto const word = enc(ln.gtag, by);
-            auto* tp = &st.tmp[li(st, l, s)];
-            if (st.profile) {
-              if (word < atomicMin(tp, word)) ++p_writes;
-            } else {
-              atomicMin(tp, word);  // result unused: no round trip
-            }
-            atomicOr(&st.Y[l * st.G + g], bit);  // listed by k_list_reached
-          }
-        }
-        if (i + 1u != n && can_start && (xw & bit)) {
-          if (lbv == 0xFFFFu) break;  // raptor.h:1309-1311: no later stop of this query
-          auto const board_col = n_t * (si * 2u - (fwd ? 0u : 1u));
-          auto const et_time =
-              et_valid ? to_delta_key(fwd, et_day, ln.base, delta_count(colbase[board_col + et_off]))
-                       : kKeyInv;
-          auto const prt = dec(st.rt[rti(st, k - 1u, l, s)], ln.qtag);
-          if (prt != kKeyInv && prt <= et_time) {
-            auto const t_prt = from_key(fwd, prt);
-            auto const minutes = static_cast<int>(ln.base) * 1440 + t_prt;
-            auto const day = static_cast<uint16_t>(minutes / 1440);
-            auto const mam = minutes % 1440;
-            uint32_t nt = 0;
-            uint16_t nd = 0;
-            auto const found = et_search(T, fwd, r, si, day, mam, static_cast<int>(lbv), ln.tad_k,
-                                         ln.base, nt, nd, p_ev, p_days);
-            if (found) {
-              // current_best (raptor.h:1328-1329) is valid whenever the arrival
-              // part ran or the station carries a label of this start time
-              auto const cb_valid = arrival_ran || dec(st.best[li(st, l, s)], ln.gtag) != kKeyInv ||
-                                    dec(st.tmp[li(st, l, s)], ln.gtag) != kKeyInv;
-              auto const nt_time =
-                  to_delta_key(fwd, nd, ln.base, delta_count(colbase[board_col + nt]));
-              if (!cb_valid || nt_time <= et_time) {
-                et_valid = true;
-                et_off = nt;
-                et_day = nd;
-              }
-            }
-          }
-        }
-        if (et_valid && i + 1u < n) {  // the next stop's arrival event of the (new) current trip
-          auto const si_next = fwd ? i + 1u : n - 2u - i;
-          ev = colbase[n_t * (si_next * 2u - (fwd ? 1u : 0u)) + et_off];
-        }
-        stp = stp_next;
-        stp_next = stp_after;
-        xw = xw_next;
-        lbv = lb_next;
-      }
-    }
+    atomicOr(&st.Y[l * st.G + g], bit);  // listed by k_list_reached
   }
-  if (st.profile) {  // work counters for the roofline (warp-reduced)
-    __syncwarp();
-    auto steps_max = p_stops;
-    for (auto o = 16; o > 0; o >>= 1) {
-      p_stops += __shfl_xor_sync(kFull, p_stops, o);
-      p_ev += __shfl_xor_sync(kFull, p_ev, o);
-      p_days += __shfl_xor_sync(kFull, p_days, o);
-      p_writes += __shfl_xor_sync(kFull, p_writes, o);
-      steps_max = max(steps_max, __shfl_xor_sync(kFull, steps_max, o));
+}
+
+// The reference's sequential walk of one (route, query) pair from position
+// i0 on, entering with the current trip (et_valid, et_off, et_day).
+__device__ __noinline__ void scan_walk_seq(state const& st, lane_t const ln, uint32_t r, uint32_t g, uint32_t b,
+                                           uint32_t sec, uint32_t i0, bool et_valid, uint32_t et_off,
+                                           uint16_t et_day, scan_ctr& pc) {
+  auto const& T = st.tt;
+  auto const s = g * 32u + b;
+  auto const bit = 1u << b;
+  auto const fwd = ln.fwd != 0;
+  auto const k = static_cast<uint32_t>(ln.k);
+  auto const sb = T.route_stop_idx[r];
+  auto const n = T.route_stop_idx[r + 1] - sb;
+  auto const n_t = T.route_tr_to[r] - T.route_tr_from[r];
+  auto const* colbase = T.st + T.route_st_from[r];
+  auto const lb_off = (ln.mode & 8u) != 0u;
+  for (auto i = i0; i < n; ++i) {
+    ++pc.stops;
+    ++pc.warp_steps;
+    auto const stp = scan_stop_word(T, sb, n, fwd, i, sec);
+    auto const si = fwd ? i : n - 1u - i;
+    auto const l = B2R_STOP_LOC(stp);
+    auto const lbv = lb_off ? uint16_t{0} : st.lb[li(st, l, s)];
+    auto const can_finish = fwd ? B2R_STOP_OUT(stp) : B2R_STOP_IN(stp);
+    auto const can_start = fwd ? B2R_STOP_IN(stp) : B2R_STOP_OUT(stp);
+    if ((sec & 15u) != 0u && i != 0u && !section_ok(T, sb, fwd ? i - 1u : si, sec & 15u)) {
+      et_valid = false;  // raptor.h:1194-1217: the section ridden lacks a flag
     }
-    if (lane == 0) {
-      atomicAdd(&st.prof[0], static_cast<unsigned long long>(p_stops));
-      atomicAdd(&st.prof[1], static_cast<unsigned long long>(p_ev));
-      atomicAdd(&st.prof[2], static_cast<unsigned long long>(p_days));
-      atomicAdd(&st.prof[3], static_cast<unsigned long long>(p_writes));
-      atomicAdd(&st.prof[5], static_cast<unsigned long long>(steps_max));  // warp stop steps
+    bool arrival_ran = false;
+    if (et_valid && can_finish) {
+      arrival_ran = true;
+      auto const ev = colbase[n_t * (si * 2u - (fwd ? 1u : 0u)) + et_off];
+      scan_arrive(st, ln, s, g, bit, l, lbv, to_delta_key(fwd, et_day, ln.base, delta_count(ev)), pc);
+    }
+    if (i + 1u == n || !can_start || !(st.X[l * st.G + g] & bit)) continue;
+    if (lbv == 0xFFFFu) break;  // raptor.h:1309-1311: no later stop of this query
+    auto const board_col = n_t * (si * 2u - (fwd ? 0u : 1u));
+    auto const et_time =
+        et_valid ? to_delta_key(fwd, et_day, ln.base, delta_count(colbase[board_col + et_off])) : kKeyInv;
+    auto const prt = dec(st.rt[rti(st, k - 1u, l, s)], ln.qtag);
+    if (prt == kKeyInv || prt > et_time) continue;
+    auto const minutes = static_cast<int>(ln.base) * 1440 + from_key(fwd, prt);
+    uint32_t nt = 0;
+    uint16_t nd = 0;
+    if (!et_search(T, fwd, r, si, static_cast<uint16_t>(minutes / 1440), minutes % 1440, static_cast<int>(lbv),
+                   ln.tad_k, ln.base, nt, nd, pc.ev, pc.days)) {
+      continue;
+    }
+    // current_best (raptor.h:1328-1329) is valid whenever the arrival part
+    // ran or the station carries a label of this start time
+    auto const cb_valid = arrival_ran || dec(st.best[li(st, l, s)], ln.gtag) != kKeyInv ||
+                          dec(st.tmp[li(st, l, s)], ln.gtag) != kKeyInv;
+    if (!cb_valid || to_delta_key(fwd, nd, ln.base, delta_count(colbase[board_col + nt])) <= et_time) {
+      et_valid = true;
+      et_off = nt;
+      et_day = nd;
     }
   }
 }
 
+// One (route, query) pair, the warp's lanes over its stops.
+__device__ __forceinline__ void scan_pair(state const& st, lane_t const& ln, uint32_t r, uint32_t g, uint32_t b,
+                                          uint32_t lane, scan_ctr& pc) {
+  auto const& T = st.tt;
+  auto const s = g * 32u + b;
+  uint32_t sec = 0u;  // required flags checked per section (bits 0-3); bit 8: wheelchair profile
+  if ((ln.claszes != 0xFFFFu || ln.req != 0u) && !route_allowed(T, r, ln.claszes, ln.req, sec)) return;
+  if ((ln.mode & 0x70u) == (B2R_PROFILE_WHEELCHAIR << 4)) sec |= 0x100u;
+  if ((sec & 15u) != 0u || T.route_fifo[r] == 0u) {
+    if (lane == 0u) scan_walk_seq(st, ln, r, g, b, sec, 0u, false, 0u, 0u, pc);
+    return;
+  }
+  auto const bit = 1u << b;
+  auto const fwd = ln.fwd != 0;
+  auto const k = static_cast<uint32_t>(ln.k);
+  auto const sb = T.route_stop_idx[r];
+  auto const n = T.route_stop_idx[r + 1] - sb;
+  auto const n_t = T.route_tr_to[r] - T.route_tr_from[r];
+  auto const* colbase = T.st + T.route_st_from[r];
+  auto const lb_off = (ln.mode & 8u) != 0u;
+  // the trip carried over from the earlier chunks: its order key (the time
+  // at the route's first departure event, negated backward: smaller is
+  // better), transport offset and service day
+  bool c_valid = false;
+  int c_key = 0;
+  uint32_t c_off = 0;
+  uint16_t c_day = 0;
+  for (auto i0 = 0u; i0 < n; i0 += 32u) {
+    auto const i = i0 + lane;
+    auto const act = i < n;
+    auto const si = fwd ? i : n - 1u - i;
+    uint32_t stp = 0, l = 0;
+    bool marked = false;
+    uint16_t lbv = 0;
+    if (act) {
+      stp = scan_stop_word(T, sb, n, fwd, i, sec);
+      l = B2R_STOP_LOC(stp);
+      marked = (st.X[l * st.G + g] & bit) != 0u;
+      if (!lb_off) lbv = st.lb[li(st, l, s)];
+    }
+    auto const can_finish = act && (fwd ? B2R_STOP_OUT(stp) : B2R_STOP_IN(stp)) != 0u;
+    auto const boardable = act && i + 1u != n && (fwd ? B2R_STOP_IN(stp) : B2R_STOP_OUT(stp)) != 0u && marked;
+    // raptor.h:1309-1311: the walk ends at the first boardable stop the
+    // query cannot reach, after that stop's arrival
+    auto const brk = __ballot_sync(kFull, boardable && lbv == 0xFFFFu);
+    auto const fb = brk != 0u ? static_cast<uint32_t>(__ffs(brk) - 1) : 32u;
+    // this stop's earliest boardable trip (raptor.h:1313-1327)
+    bool cand = false, cb_bad = false;
+    uint32_t nt = 0;
+    uint16_t nd = 0;
+    int key = 0;
+    if (boardable && lane < fb) {
+      auto const prt = dec(st.rt[rti(st, k - 1u, l, s)], ln.qtag);
+      if (prt != kKeyInv) {
+        auto const minutes = static_cast<int>(ln.base) * 1440 + from_key(fwd, prt);
+        if (et_search(T, fwd, r, si, static_cast<uint16_t>(minutes / 1440), minutes % 1440, static_cast<int>(lbv),
+                      ln.tad_k, ln.base, nt, nd, pc.ev, pc.days)) {
+          cand = true;
+          cb_bad = dec(st.best[li(st, l, s)], ln.gtag) == kKeyInv && dec(st.tmp[li(st, l, s)], ln.gtag) == kKeyInv;
+          auto const t = (static_cast<int>(nd) - static_cast<int>(ln.base)) * 1440 + delta_count(colbase[nt]);
+          key = fwd ? t : -t;
+        }
+      }
+    }
+    if (__ballot_sync(kFull, cb_bad) != 0u) {  // the boarding rule then depends on the walk's order
+      if (lane == 0u) scan_walk_seq(st, ln, r, g, b, sec, i0, c_valid, c_off, c_day, pc);
+      return;
+    }
+    if (lane == 0u) {
+      pc.stops += min(n - i0, min(fb + 1u, 32u));
+      ++pc.warp_steps;
+    }
+    // prefix minimum of (key, later stop first) over the lanes; |key| is
+    // below 2^20 (days < 512), so key + 2^20 takes 21 bits above 5 for the
+    // lane
+    auto v = cand ? (static_cast<uint32_t>(key + (1 << 20)) << 5) | (31u - lane) : 0xFFFFFFFFu;
+    for (auto o = 1u; o < 32u; o <<= 1) {
+      auto const y = __shfl_up_sync(kFull, v, o);
+      if (lane >= o) v = min(v, y);
+    }
+    auto ex = __shfl_up_sync(kFull, v, 1);  // best candidate before this stop
+    if (lane == 0u) ex = 0xFFFFFFFFu;
+    auto const tot = __shfl_sync(kFull, v, 31);
+    auto const src = static_cast<int>(31u - (ex & 31u));
+    auto const x_off = __shfl_sync(kFull, nt, src);
+    auto const x_day = static_cast<uint16_t>(__shfl_sync(kFull, static_cast<uint32_t>(nd), src));
+    // the carried trip loses ties to the later stops of this chunk
+    auto const use_x = ex != 0xFFFFFFFFu && (!c_valid || static_cast<int>(ex >> 5) - (1 << 20) <= c_key);
+    auto const et_valid = use_x || c_valid;
+    if (act && lane <= fb && et_valid && can_finish) {
+      auto const et_off = use_x ? x_off : c_off;
+      auto const et_day = use_x ? x_day : c_day;
+      auto const ev = colbase[n_t * (si * 2u - (fwd ? 1u : 0u)) + et_off];
+      scan_arrive(st, ln, s, g, bit, l, lbv, to_delta_key(fwd, et_day, ln.base, delta_count(ev)), pc);
+    }
+    if (fb != 32u) return;
+    if (tot != 0xFFFFFFFFu) {
+      auto const t_src = static_cast<int>(31u - (tot & 31u));
+      auto const t_off = __shfl_sync(kFull, nt, t_src);
+      auto const t_day = static_cast<uint16_t>(__shfl_sync(kFull, static_cast<uint32_t>(nd), t_src));
+      auto const t_key = static_cast<int>(tot >> 5) - (1 << 20);
+      if (!c_valid || t_key <= c_key) {
+        c_valid = true;
+        c_key = t_key;
+        c_off = t_off;
+        c_day = t_day;
+      }
+    }
+  }
+}
+
+// A warp per marked (route, group of 32 queries) entry, one pair of the
+// entry after the other.
+__global__ void __launch_bounds__(256) k_route_scan(const __grid_constant__ state st) {
+  auto const lane = threadIdx.x & 31u;
+  auto const warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  auto const n_warps = (gridDim.x * blockDim.x) >> 5;
+  auto const nr = st.counters[C_R];
+  scan_ctr pc{0u, 0u, 0u, 0u, 0u};
+  for (auto w = warp; w < nr; w += n_warps) {
+    auto const e = st.rlist[w];
+    auto mask = st.R[e];
+    __syncwarp();
+    if (lane == 0u) st.R[e] = 0u;
+    auto const g = e % st.G, r = e / st.G;
+    while (mask != 0u) {
+      auto const b = static_cast<uint32_t>(__ffs(mask) - 1);
+      mask &= mask - 1u;
+      auto const ln = st.lanes[g * 32u + b];
+      if (!ln.run) continue;
+      scan_pair(st, ln, r, g, b, lane, pc);
+      __syncwarp();
+    }
+  }
+  if (st.profile) {  // work counters for the roofline (warp-reduced)
+    __syncwarp();
+    for (auto o = 16; o > 0; o >>= 1) {
+      pc.stops += __shfl_xor_sync(kFull, pc.stops, o);
+      pc.ev += __shfl_xor_sync(kFull, pc.ev, o);
+      pc.days += __shfl_xor_sync(kFull, pc.days, o);
+      pc.writes += __shfl_xor_sync(kFull, pc.writes, o);
+      pc.warp_steps += __shfl_xor_sync(kFull, pc.warp_steps, o);
+    }
+    if (lane == 0) {
+      atomicAdd(&st.prof[0], static_cast<unsigned long long>(pc.stops));
+      atomicAdd(&st.prof[1], static_cast<unsigned long long>(pc.ev));
+      atomicAdd(&st.prof[2], static_cast<unsigned long long>(pc.days));
+      atomicAdd(&st.prof[3], static_cast<unsigned long long>(pc.writes));
+      atomicAdd(&st.prof[5], static_cast<unsigned long long>(pc.warp_steps));  // warp stop steps
+    }
+  }
+}
 // frontier list of the stations marked this round (transfers, footpaths,
 // start labels): every nonzero station-mark word (location, group)
 __global__ void k_list_marked(state st) { list_nonzero(st, st.X, st.tt.n_loc * st.G, st.xlist, C_X); }
