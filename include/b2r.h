@@ -368,9 +368,8 @@ int b2r_search_batch(b2r_engine* e, const b2r_query* qs, uint32_t n,
  * src/routing/gpu/raptor.cu:894-990).  Same results as b2r_search_batch. */
 int b2r_search_plain(b2r_engine* e, const b2r_query* q, b2r_result* out);
 
-/* One-to-all search of ONE query that allocates nothing.  It has no
- * counterpart in the reference: nigiri's one_to_all (one_to_all.cc:52-92)
- * allocates its raptor_state per call.
+/* One-to-all search of ONE query that allocates nothing.  This entry point
+ * has no counterpart in the reference.
  *
  * For callers that cannot allocate device memory on the query path:
  * request handlers of a serving process whose device memory is owned by
@@ -388,14 +387,16 @@ int b2r_search_plain(b2r_engine* e, const b2r_query* q, b2r_result* out);
  *   are rejected with B2R_ERR_CAPACITY and a message (b2r_last_error).
  * - round_times (host memory, capacity elements) receives n_rows rows of
  *   n_locations int16 deltas relative to *base_day, exactly the rows
- *   b2r_search_batch returns for the same query (raptor_state::
- *   round_times_).  n_rows = min(max_transfers, B2R_MAX_TRANSFERS) + 2.
+ *   b2r_search_batch returns for the same query.
+ *   n_rows = min(max_transfers, B2R_MAX_TRANSFERS) + 2.
  * - stream: a cudaStream_t on tt's device, or NULL for the default stream.
  *   The call returns when the rows are in round_times.
  * - Set-up: the first call on a device, with that device current, loads the
  *   library's device module (the driver reserves the scratch array then)
  *   and looks up the array's address; later calls reuse it.  Make the first
- *   call on each device before any stream capture.
+ *   call on each device before any stream capture.  The address is kept per
+ *   device for the life of the process: a caller that resets a device
+ *   (cudaDeviceReset) must not call this entry point on it again.
  * - Every call on a device shares the one scratch array: calls that overlap
  *   on the GPU (from two streams or two host threads) race and corrupt each
  *   other's results.  Issue them one at a time per device.
