@@ -84,3 +84,24 @@ class OracleResult:
             lib().or_result_free(self.h)
         except Exception:
             pass
+
+
+def answers(desc, qarr, idx, threads=None):
+    """The oracle's complete answers for queries qarr[i], i in idx, computed
+    on host threads (the oracle's calls release the interpreter lock):
+    i -> ("journeys", records) or, for one-to-all queries, ("rows", base day,
+    round-time rows)."""
+    from concurrent.futures import ThreadPoolExecutor
+    lib()
+    threads = threads or max(1, min(32, len(os.sched_getaffinity(0))))
+
+    def one(i):
+        q = qarr[i]
+        o = OracleResult(desc, q)
+        if q.kind == A.B2R_ONE_TO_ALL:
+            rows, _, base_day = o.state()
+            return i, ("rows", base_day, rows)
+        return i, ("journeys", o.records())
+
+    with ThreadPoolExecutor(threads) as ex:
+        return dict(ex.map(one, list(idx)))
