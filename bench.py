@@ -49,6 +49,12 @@ def parse():
                    help="with --ncu-case: count route-scan work (stop visits, events)")
     p.add_argument("--ncu-workload", type=int, default=2, choices=[1, 2, 3, 4, 5],
                    help="with --ncu-case: the workload's timetable and queries")
+    p.add_argument("--shape", metavar="B,T,P,R,S",
+                   help="with --ncu-case: launch shape (route-scan blocks per SM, threads, pair "
+                        "blocks per SM, reconstruction blocks per SM, super-steps per sync)")
+    p.add_argument("--ncu-summary", metavar="CSV",
+                   help="summarise an ncu --csv log (launches, time, share and any other metric "
+                        "per kernel) and exit; runs on a machine without a GPU")
     return p.parse_args()
 
 
@@ -244,6 +250,7 @@ def gpu_arm(args, rank, world, local):
     clocks = ClockSampler(local)
     clocks.start()
     walls, devs, lats, launches, h2d, d2h = [], [], [], 0, 0, 0
+    kept = {}  # query index -> engine records, checked against the oracle after timing
     for k in range(args.steps):
         flush.fill_(k & 0xFF)
         torch.cuda.synchronize()
@@ -258,6 +265,9 @@ def gpu_arm(args, rank, world, local):
         d2h += st.d2h_bytes
         for i in range(B):
             lats.append(out[i].latency_ms)
+        if rank == 0:  # outside the batch's own timing: step 0 whole, 1% of the others
+            for i in (range(B) if k == 0 else range(0, B, 100)):
+                kept[(args.warmup + k) * B + i] = journey_records(out[i])
     ck = clocks.stop()
     tot_wall, tot_dev = sum(walls), sum(devs)
     tot_wall, tot_dev = replicas.max_over_ranks([tot_wall, tot_dev], pg, f"cuda:{local}")
@@ -268,11 +278,19 @@ def gpu_arm(args, rank, world, local):
     h2d_step = h2d // max(1, args.steps)
 
     extras = {}
+    if rank == 0:
+        extras["checked_against_cpu"] = oracle_check(h.desc, qs.arr, kept, host_threads())
+        extras["checked_against_cpu"]["sample"] = (
+            f"every query of timed step 0 ({B}) and every 100th of the other {args.steps - 1} steps")
     if rank == 0 and not args.no_extras:
         extras = extras_legs(args, h, dtt, qs, B, local)
         extras["served"] = served_leg(eng, qs, [5000.0, 15000.0, 25000.0, None], 4096)
         extras["range"] = range_leg(eng, h, 1024, seed=1003)
         del eng
+        extras["batch_sweep"] = batch_sweep_leg(dtt, h, shape, (64, 256), local)
+        extras["batch_sweep"]["1024"] = {"value": value, "e2e": e2e, "p99_ms": percentile(lats, 0.99),
+                                         "unit": "queries/s", "note": "the headline steps"}
+        extras["small_city"] = small_city_leg(local)
         if not args.no_national:
             extras["national"] = national_leg(local)
     if rank == 0:
@@ -349,6 +367,35 @@ def served_leg(eng, qs, rates, n_per_rate, seed=17, keep_every=0, kept=None):
     return out
 
 
+def journey_records(r):
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from journeys import records
+    return (r.status, records(r))
+
+
+def oracle_check(desc, qarr, kept, threads):
+    """The engine's answers (query index -> (status, journey records)) against
+    the CPU oracle's on the same queries: departure, arrival, transfers and
+    every leg must be identical.  The oracle runs on host threads (its calls
+    release the interpreter lock)."""
+    from concurrent.futures import ThreadPoolExecutor
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib
+    oracle_lib.lib()
+
+    def one(i):
+        return i, (0, oracle_lib.OracleResult(desc, qarr[i]).records())
+
+    mismatches, first = 0, []
+    with ThreadPoolExecutor(max(1, threads)) as ex:
+        for i, want in ex.map(one, sorted(kept)):
+            if kept[i] != want:
+                mismatches += 1
+                if len(first) < 5:
+                    first.append(i)
+    return {"queries": len(kept), "mismatches": mismatches, "first_mismatches": first}
+
+
 def result_key(r, n_loc):
     """A query's complete answer: journeys with every leg, or one-to-all rows."""
     import numpy as np
@@ -410,6 +457,88 @@ def range_leg(eng, h, n, seed, reps=2):
     return out
 
 
+def batch_sweep_leg(dtt, h, shape, sizes, local, reps=3):
+    """The regional workload in batches of 64 and 256 resident queries (the
+    batch sizes the configuration names beside 1,024), each on an engine of
+    that many slots with the launch shape tuned at 1,024: device and
+    end-to-end queries/s and the per-query latency percentiles."""
+    from nigiri_b200 import _abi as A
+    from nigiri_b200 import routing as R
+    from nigiri_b200.timetable import QuerySet
+    lib = A.lib()
+    out = {}
+    for B in sizes:
+        eng = R.Engine(dtt, max_slots=B)
+        sh = A.LaunchShape()
+        for f, v in shape.items():
+            setattr(sh, f, v)
+        eng.shape = sh
+        qs = QuerySet(h, WORKLOAD, B * (reps + 1), seed=5000 + B)
+        res = (A.Result * B)()
+        devs, walls, lat = [], [], []
+        for k in range(reps + 1):
+            arr = qs.subset(range(k * B, (k + 1) * B))
+            t0 = time.perf_counter()
+            if lib.b2r_search_batch(eng.handle, arr, B, res) != 0:
+                raise RuntimeError(lib.b2r_last_error().decode())
+            if k > 0:  # the first batch warms up
+                walls.append(time.perf_counter() - t0)
+                devs.append(eng.stats().device_ms / 1e3)
+                lat += [res[i].latency_ms for i in range(B)]
+        out[str(B)] = {"value": B * reps / sum(devs), "e2e": B * reps / sum(walls), "unit": "queries/s",
+                       "p50_ms": percentile(lat, 0.5), "p99_ms": percentile(lat, 0.99),
+                       "queries": B * reps}
+        del eng
+    return out
+
+
+def small_city_leg(local):
+    """The 1,000-stop city: its 1,000 one-to-one queries batched (one batch),
+    one query per launch sequence (plain), and on the CPU oracle (all host
+    threads), with every batched answer compared with the oracle's."""
+    from nigiri_b200 import _abi as A
+    from nigiri_b200 import routing as R
+    from nigiri_b200.timetable import HostTimetable, QuerySet
+    lib = A.lib()
+    h = HostTimetable.generate(1)
+    dtt = R.Timetable(h.desc, device=local, owner=h)
+    n = 1000
+    qs = QuerySet(h, 1, n, seed=1001)
+    eng = R.Engine(dtt, max_slots=1024)
+    res = (A.Result * n)()
+    walls, devs = [], []
+    for rep in range(3):
+        t0 = time.perf_counter()
+        if lib.b2r_search_batch(eng.handle, qs.arr, n, res) != 0:
+            raise RuntimeError(lib.b2r_last_error().decode())
+        if rep > 0:
+            walls.append(time.perf_counter() - t0)
+            devs.append(eng.stats().device_ms / 1e3)
+    kept = {i: journey_records(res[i]) for i in range(n)}
+    out = {"timetable": f"{h.desc.n_locations:,} locations, {h.desc.n_routes:,} routes",
+           "queries": n,
+           "batched": {"value": 2 * n / sum(devs), "e2e": 2 * n / sum(walls), "unit": "queries/s"}}
+    del eng
+    plain = R.Engine(dtt, max_slots=32, use_graphs=False)
+    one = A.Result()
+    lat = []
+    t0 = time.perf_counter()
+    for i in range(n):
+        a = time.perf_counter()
+        if lib.b2r_search_plain(plain.handle, C.byref(qs.arr[i]), C.byref(one)) != 0:
+            raise RuntimeError(lib.b2r_last_error().decode())
+        lat.append((time.perf_counter() - a) * 1e3)
+    out["plain_gpu"] = {"value": n / (time.perf_counter() - t0), "unit": "queries/s",
+                        "p50_ms": percentile(lat, 0.5), "p99_ms": percentile(lat, 0.99)}
+    del plain
+    threads = host_threads()
+    wall, lat, _ = cpu_run(h.desc, qs.arr, n, threads)
+    out["cpu_baseline"] = {"value": n / wall, "unit": "queries/s", "cores": threads, "kind": "port",
+                           "p99_ms": percentile(lat, 0.99)}
+    out["checked_against_cpu"] = oracle_check(h.desc, qs.arr, kept, threads)
+    return out
+
+
 def national_leg(local):
     """National-scale timetable (300k stops, 25k base routes, 2.7M transports,
     stay-seated chain routes).  Batched: batches of 256 mixing one-to-one, 1 h
@@ -456,7 +585,7 @@ def national_leg(local):
     # served (continuous batching), 1% of the answers kept for the check
     sq = QuerySet(h, 5, 4096, seed=1005)
     kept = {}
-    out["served"] = served_leg(eng, sq, [200.0, 1000.0, 5000.0, 20000.0, None],
+    out["served"] = served_leg(eng, sq, [100.0, 1000.0, 5000.0, 20000.0, None],
                                lambda r: 4096 if r is None else max(256, min(4096, int(r))),
                                keep_every=100, kept=kept)
     out["range"] = range_leg(eng, h, 256, seed=1006, reps=1)
@@ -557,13 +686,18 @@ def ncu_case(args, local):
     h = HostTimetable.generate(args.ncu_workload)
     dtt = R.Timetable(h.desc, device=local, owner=h)
     eng = R.Engine(dtt, max_slots=args.batch, use_graphs=False, profile=args.ncu_counters)
+    if args.shape:
+        eng.shape = A.LaunchShape(*[int(x) for x in args.shape.split(",")])
     qs = QuerySet(h, args.ncu_workload, args.batch, seed=1000 + args.ncu_workload)
     out = (A.Result * args.batch)()
     rc = A.lib().b2r_search_batch(eng.handle, qs.arr, args.batch, out)
     if rc != 0:
         raise RuntimeError(A.lib().b2r_last_error().decode())
     st = eng.stats()
+    sh = eng.shape
     print(json.dumps({"ncu_case": True, "batch": args.batch, "super_steps": st.super_steps,
+                      "shape": [sh.scan_blocks_per_sm, sh.scan_threads, sh.pair_blocks_per_sm,
+                                sh.recon_blocks_per_sm, sh.steps_per_sync],
                       "kernel_launches": st.kernel_launches, "device_ms": st.device_ms,
                       "route_scan_launches": st.route_scan_launches,
                       "route_stop_visits": st.route_stop_visits,
@@ -574,8 +708,46 @@ def ncu_case(args, local):
                       "route_scan_bytes": st.route_scan_bytes}))
 
 
+def ncu_summary(path):
+    """Per-kernel table of an ncu --csv log: launches, total and mean
+    gpu__time_duration, share of the total, and the per-launch mean of every
+    other metric captured (DRAM bytes and the like)."""
+    import csv
+    scale = {"ns": 1e-6, "nsecond": 1e-6, "us": 1e-3, "usecond": 1e-3, "ms": 1.0, "msecond": 1.0,
+             "s": 1e3, "second": 1e3}
+    bytes_scale = {"byte": 1, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9, "KB": 1e3, "MB": 1e6, "GB": 1e9}
+    with open(path, newline="") as f:
+        lines = [ln for ln in f if ln.startswith('"')]  # ncu's own log lines are not quoted
+    per = {}
+    for row in csv.DictReader(lines):
+        name = row["Kernel Name"].split("(")[0]
+        k = per.setdefault(name, {"launches": set(), "ms": 0.0, "other": {}})
+        k["launches"].add(row["ID"])
+        metric, unit = row["Metric Name"], row["Metric Unit"]
+        val = float(row["Metric Value"].replace(",", ""))
+        if metric == "gpu__time_duration.sum":
+            k["ms"] += val * scale.get(unit, 1e-6)
+        else:
+            k["other"].setdefault(metric, 0.0)
+            k["other"][metric] += val * bytes_scale.get(unit, 1)
+    total = sum(k["ms"] for k in per.values())
+    n_launch = sum(len(k["launches"]) for k in per.values())
+    print(f"total {total:.3f} ms over {n_launch} launches")
+    metrics = sorted({m for k in per.values() for m in k["other"]})
+    head = f"{'kernel':<24} {'launches':>8} {'total ms':>9} {'share':>7} {'mean us':>9}"
+    print(head + "".join(f" {m + ' / launch':>34}" for m in metrics))
+    for name, k in sorted(per.items(), key=lambda x: -x[1]["ms"]):
+        n = len(k["launches"])
+        line = (f"{name:<24} {n:>8} {k['ms']:>9.3f} {100 * k['ms'] / max(total, 1e-12):>6.2f}% "
+                f"{1e3 * k['ms'] / max(n, 1):>9.1f}")
+        print(line + "".join(f" {k['other'].get(m, 0.0) / max(n, 1):>34,.0f}" for m in metrics))
+
+
 def main():
     args = parse()
+    if args.ncu_summary:
+        ncu_summary(args.ncu_summary)
+        return
     rank, world, local = dist_env()
     if args.ncu_case:
         ncu_case(args, local)
