@@ -421,10 +421,11 @@ int b2r_poll(b2r_engine* e, uint64_t ticket, b2r_result* out);
 int b2r_wait(b2r_engine* e, uint64_t ticket, b2r_result* out);
 int b2r_release(b2r_engine* e, uint64_t ticket);
 
-/* Timing of the last b2r_search_batch: device milliseconds of the
- * super-step chunks (CUDA events, admission/export gaps excluded), wall time
- * of the call, and the number of kernel launches issued (graph nodes
- * included). */
+/* Timing of the last b2r_search_batch: device milliseconds (CUDA events:
+ * the union of the intervals in which super-step chunks and the
+ * finished-slot kernels, deferred reconstruction and result export, ran;
+ * host-only gaps between them are excluded), wall time of the call, and the
+ * number of kernel launches issued (graph nodes included). */
 typedef struct b2r_batch_stats {
   double device_ms;
   double host_prep_ms; /* wall time of the whole call */

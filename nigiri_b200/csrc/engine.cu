@@ -128,6 +128,7 @@ struct b2r_engine {
   b2r::dev::journey_rec* d_keep{};  // journeys kept across interval-extension phases
   // host<->device bytes copied by the current batch call
   uint64_t h2d_bytes{0}, d2h_bytes{0};
+  uint64_t aux_launches{0};  // kernels launched outside the super-steps (admission, export, ...)
   // host time of the current batch call: preparation (summed over the
   // workers), admission, export + finalisation, waiting for preparation
   std::atomic<uint64_t> prep_ns{0};
@@ -144,6 +145,13 @@ struct b2r_engine {
 
   b2r_batch_stats last{};
   cudaEvent_t ev0{nullptr}, ev1{nullptr};
+  // device busy time of a batch: the intervals (ms after ev_base) in which
+  // super-step chunks (main stream) and finished-slot work (reconstruction
+  // and export kernels, second stream) ran; their union is the batch's
+  // device time
+  cudaEvent_t ev_base{nullptr}, ev2a{nullptr}, ev2b{nullptr};
+  bool base_recorded{false};
+  std::vector<std::pair<double, double>> busy;
   // profiling: event pairs bracketing each route-scan launch
   std::vector<cudaEvent_t> prof_ev;
   size_t prof_used{0};
@@ -462,6 +470,9 @@ b2r_engine::~b2r_engine() {
   if (stream2 != nullptr) cudaStreamDestroy(stream2);
   if (ev0 != nullptr) cudaEventDestroy(ev0);
   if (ev1 != nullptr) cudaEventDestroy(ev1);
+  if (ev_base != nullptr) cudaEventDestroy(ev_base);
+  if (ev2a != nullptr) cudaEventDestroy(ev2a);
+  if (ev2b != nullptr) cudaEventDestroy(ev2b);
   if (h_summary != nullptr) cudaFreeHost(h_summary);
   if (h_lbcount != nullptr) cudaFreeHost(h_lbcount);
   if (h_adm != nullptr) cudaFreeHost(h_adm);
@@ -580,6 +591,9 @@ slot_t make_slot(b2r_engine& e, uint32_t s, prepped_query const& p, bool& clear_
   sl.req_flags = p.req_flags;
   sl.blast = p.blast;
   sl.recon_mode = p.recon_mode;
+  // one start-time group and nothing after it: the journeys can wait until
+  // the slot is done and be rebuilt while the next super-steps run
+  sl.recon_defer = (p.ontrip && !p.one_to_all && p.recon_mode == 0) ? 1 : 0;
   sl.recon_transfers = p.recon_transfers;
   sl.no_lb = p.no_lb ? 1 : 0;
   sl.prf = p.prf;
@@ -615,6 +629,7 @@ void solve_lower_bounds(b2r_engine& e, cudaStream_t s) {
   uint32_t pending = 1;
   uint64_t chunks = 0;
   while (pending != 0) {
+    e.aux_launches += 24;  // 4 x 2 iterations of 3 kernels
     if (e.lb_graph != nullptr) {
       B2R_CUDA(cudaGraphLaunch(e.lb_graph, s));
     } else {
@@ -629,6 +644,7 @@ void solve_lower_bounds(b2r_engine& e, cudaStream_t s) {
     if (chunks > 100000) throw std::runtime_error("lower-bound solver did not converge");
   }
   e.lb_chunks += chunks;
+  e.aux_launches += e.tt->d.n_with_children != 0 ? 2 : 1;
   if (e.tt->d.n_with_children != 0) {
     dev::k_lb_children<<<(e.S + 127) / 128, 128, 0, s>>>(e.st);
   }
@@ -803,16 +819,19 @@ void admit(b2r_engine& e, std::vector<adm_req> const& adm, cudaStream_t s) {
   B2R_CUDA(cudaMemcpyAsync(e.d_adm, e.h_adm, off, cudaMemcpyHostToDevice, s));
   if (!fills.empty()) {
     auto const bx = std::min<uint32_t>((e.tt->d.n_loc + 255u) / 256u, static_cast<uint32_t>(e.sms) * 2u);
+    ++e.aux_launches;
     k_fill_bounds<<<dim3(bx, static_cast<unsigned>(fills.size())), 256, 0, s>>>(
         e.st, reinterpret_cast<fill_item const*>(e.d_adm + off_fills));
     B2R_CUDA(cudaGetLastError());
   }
   if (!lb_groups.empty()) {
+    ++e.aux_launches;
     k_lb_fill<<<dim3((e.tt->d.n_loc + kLbTile - 1) / kLbTile, static_cast<unsigned>(lb_groups.size())), 256, 0,
                 s>>>(e.st, reinterpret_cast<lb_group const*>(e.d_adm + off_lb_groups),
                      reinterpret_cast<lb_entry const*>(e.d_adm + off_lb_entries), e.d_adm);
     B2R_CUDA(cudaGetLastError());
   }
+  ++e.aux_launches;
   k_admit<<<static_cast<unsigned>(adm.size()), 256, 0, s>>>(
       e.st, reinterpret_cast<adm_hdr const*>(e.d_adm), e.d_adm, static_cast<uint32_t>(adm.size()),
       e.max_starts, e.max_dest, e.max_off);
@@ -827,6 +846,7 @@ void retire(b2r_engine& e, std::vector<uint32_t> const& slots, cudaStream_t s) {
   d = e.d_exp_list;
   e.h2d_bytes += slots.size() * sizeof(uint32_t);
   B2R_CUDA(cudaMemcpyAsync(d, slots.data(), slots.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+  ++e.aux_launches;
   k_retire<<<static_cast<unsigned>(slots.size()), 128, 0, s>>>(e.st, d, static_cast<uint32_t>(slots.size()));
   B2R_CUDA(cudaGetLastError());
 }
@@ -844,7 +864,15 @@ void export_slots(b2r_engine& e, std::vector<uint32_t> const& slots,
   out.assign(slots.size(), {});
   if (slots.empty()) return;
   std::vector<exp_item> items(slots.size());
-  size_t off = (slots.size() * sizeof(exp_item) + 255) & ~size_t{255};
+  // the journeys of slots whose reconstruction waits for the slot to finish
+  // (k_reconstruct_done skips the others), uploaded after the items
+  std::vector<uint32_t> recon;
+  for (auto i = 0U; i != slots.size(); ++i) {
+    for (auto ji = 0U; ji != n_js[i]; ++ji) recon.push_back((slots[i] << 16) | ji);
+  }
+  auto const recon_off = (slots.size() * sizeof(exp_item) + 15) & ~size_t{15};
+  auto const header = recon_off + recon.size() * sizeof(uint32_t);
+  size_t off = (header + 255) & ~size_t{255};
   for (auto i = 0U; i != slots.size(); ++i) {
     auto& it = items[i];
     it.slot = slots[i];
@@ -872,19 +900,37 @@ void export_slots(b2r_engine& e, std::vector<uint32_t> const& slots,
     B2R_CUDA(cudaMalloc(&e.d_exp, e.exp_cap));
   }
   std::memcpy(e.h_exp, items.data(), items.size() * sizeof(exp_item));
-  e.h2d_bytes += items.size() * sizeof(exp_item);
-  B2R_CUDA(cudaMemcpyAsync(e.d_exp, e.h_exp, items.size() * sizeof(exp_item), cudaMemcpyHostToDevice, s));
+  if (!recon.empty()) std::memcpy(e.h_exp + recon_off, recon.data(), recon.size() * sizeof(uint32_t));
+  e.h2d_bytes += header;
+  B2R_CUDA(cudaMemcpyAsync(e.d_exp, e.h_exp, header, cudaMemcpyHostToDevice, s));
+  if (e.base_recorded) B2R_CUDA(cudaEventRecord(e.ev2a, s));
+  if (!recon.empty()) {
+    ++e.aux_launches;
+    dev::k_reconstruct_done<<<static_cast<unsigned>(std::min<size_t>(
+                                  (recon.size() + 3) / 4, static_cast<size_t>(e.sms) * e.shape.recon_blocks_per_sm)),
+                              128, 0, s>>>(e.st, reinterpret_cast<uint32_t const*>(e.d_exp + recon_off),
+                                           static_cast<uint32_t>(recon.size()));
+    B2R_CUDA(cudaGetLastError());
+  }
   uint32_t row_blocks = 1;  // spread one-to-all rows over the SMs
   for (auto const r : n_rows) {
     if (r != 0) row_blocks = std::max<uint32_t>(row_blocks, static_cast<uint32_t>(e.sms) * 4u /
                                                                 static_cast<uint32_t>(slots.size()) + 1u);
   }
+  ++e.aux_launches;
   k_export<<<dim3(static_cast<unsigned>(slots.size()), row_blocks), 256, 0, s>>>(
       e.st, reinterpret_cast<exp_item const*>(e.d_exp), static_cast<uint32_t>(slots.size()), e.d_exp);
   B2R_CUDA(cudaGetLastError());
+  if (e.base_recorded) B2R_CUDA(cudaEventRecord(e.ev2b, s));
   e.d2h_bytes += off;
   B2R_CUDA(cudaMemcpyAsync(e.h_exp, e.d_exp, off, cudaMemcpyDeviceToHost, s));
   B2R_CUDA(cudaStreamSynchronize(s));
+  if (e.base_recorded) {
+    float a = 0, b = 0;
+    B2R_CUDA(cudaEventElapsedTime(&a, e.ev_base, e.ev2a));
+    B2R_CUDA(cudaEventElapsedTime(&b, e.ev_base, e.ev2b));
+    e.busy.emplace_back(a, b);
+  }
   for (auto i = 0U; i != slots.size(); ++i) {
     auto const& it = items[i];
     auto& o = out[i];
@@ -1332,6 +1378,7 @@ void rearm(b2r_engine& e, uint32_t s, query_run& q, cudaStream_t st) {
   auto* dj = e.d_keep;  // engine-owned, reused (this function synchronises)
   B2R_CUDA(cudaMemcpyAsync(dj, q.keep.data(), q.keep.size() * sizeof(dev::journey_rec),
                            cudaMemcpyHostToDevice, st));
+  ++e.aux_launches;
   k_set_journeys<<<1, 32, 0, st>>>(e.st, s, dj, static_cast<uint32_t>(q.keep.size()));
   B2R_CUDA(cudaMemcpyAsync(e.st.slots + s, &cur, sizeof(slot_t), cudaMemcpyHostToDevice, st));
   B2R_CUDA(cudaStreamSynchronize(st));
@@ -1340,16 +1387,40 @@ void rearm(b2r_engine& e, uint32_t s, query_run& q, cudaStream_t st) {
   q.rearm = false;
 }
 
+// length of the union of [start, end) intervals
+double busy_union_ms(std::vector<std::pair<double, double>> v) {
+  std::sort(v.begin(), v.end());
+  double total = 0, lo = 0, hi = -1;
+  for (auto const& [a, b] : v) {
+    if (a > hi) {
+      if (hi > lo) total += hi - lo;
+      lo = a;
+      hi = b;
+    } else {
+      hi = std::max(hi, b);
+    }
+  }
+  if (hi > lo) total += hi - lo;
+  return total;
+}
+
 struct batch_runner {
   b2r_engine& e;
   std::vector<query_run>& runs;
   bool use_graph;
   uint64_t launches{0}, steps{0};
-  double busy_ms{0};  // device time of the super-step chunks
+  double busy_ms{0};  // device time: union of the chunks' and the finished-slot work's intervals
 
   void run(uint32_t chunk) {
     auto const S = e.S;
     auto* st = e.stream;
+    e.busy.clear();
+    B2R_CUDA(cudaEventRecord(e.ev_base, st));
+    e.base_recorded = true;
+    struct unrecord {  // the serving loop exports without a base event
+      b2r_engine& e;
+      ~unrecord() { e.base_recorded = false; }
+    } unrec{e};
     size_t next = 0;
     std::vector<int64_t>& slot_q = e.slot_query;
     std::fill(slot_q.begin(), slot_q.end(), -1);
@@ -1460,9 +1531,10 @@ struct batch_runner {
       B2R_CUDA(cudaStreamSynchronize(st));
       in_flight = false;
       {
-        float ms = 0;
-        B2R_CUDA(cudaEventElapsedTime(&ms, e.ev0, e.ev1));
-        busy_ms += ms;
+        float a = 0, b = 0;
+        B2R_CUDA(cudaEventElapsedTime(&a, e.ev_base, e.ev0));
+        B2R_CUDA(cudaEventElapsedTime(&b, e.ev_base, e.ev1));
+        e.busy.emplace_back(a, b);
       }
       std::copy(e.h_summary, e.h_summary + S, sum.begin());
       for (auto& x : slot_q)
@@ -1516,6 +1588,7 @@ struct batch_runner {
       if (!in_flight) admit_free();
     }
     B2R_CUDA(cudaStreamSynchronize(st));
+    busy_ms = busy_union_ms(e.busy);
   }
 };
 
@@ -2196,6 +2269,9 @@ int b2r_engine_create(b2r_timetable* tt, const b2r_engine_config* cfg_in, b2r_en
       B2R_CUDA(cudaStreamCreateWithFlags(&e->stream2, cudaStreamNonBlocking));
       B2R_CUDA(cudaEventCreate(&e->ev0));
       B2R_CUDA(cudaEventCreate(&e->ev1));
+      B2R_CUDA(cudaEventCreate(&e->ev_base));
+      B2R_CUDA(cudaEventCreate(&e->ev2a));
+      B2R_CUDA(cudaEventCreate(&e->ev2b));
       if (e->cfg.use_graphs) {
         b2r::capture_graph(*e);
         cudaGraph_t g = nullptr;
@@ -2240,6 +2316,7 @@ int b2r_search_batch(b2r_engine* e, const b2r_query* qs, uint32_t n, b2r_result*
       e->lb_chunks = 0;
       e->h2d_bytes = 0;
       e->d2h_bytes = 0;
+      e->aux_launches = 0;
       e->prep_ns = 0;
       e->admit_ms = e->export_ms = e->idle_ms = 0;
       b2r::preparer prep;
@@ -2253,7 +2330,7 @@ int b2r_search_batch(b2r_engine* e, const b2r_query* qs, uint32_t n, b2r_result*
       e->last = {};
       e->last.device_ms = br.busy_ms;
       e->last.host_prep_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();  // wall of the call
-      e->last.kernel_launches = br.launches;
+      e->last.kernel_launches = br.launches + e->aux_launches;
       e->last.super_steps = br.steps;
       e->last.lb_ms = e->lb_ms;
       e->last.lb_iterations = e->lb_chunks * 8;
@@ -2320,12 +2397,13 @@ int b2r_search_plain(b2r_engine* e, const b2r_query* q, b2r_result* out) {
     try {
       B2R_CUDA(cudaSetDevice(e->tt->device));
       std::vector<b2r::query_run> runs(1);
+      e->aux_launches = 0;
       b2r::preparer prep;
       prep.start(*e, q, 1, runs, true);
       b2r::batch_runner br{*e, runs, false};
       br.run(1);
       e->last = {};
-      e->last.kernel_launches = br.launches;
+      e->last.kernel_launches = br.launches + e->aux_launches;
       e->last.super_steps = br.steps;
       b2r::fill_out(*e, runs, out);
       return B2R_OK;

@@ -146,7 +146,8 @@ struct slot_t {
   uint32_t doff_off, n_doff;      // destination offsets
   // dynamic
   uint8_t k;
-  uint8_t pad0;
+  uint8_t recon_defer;  // set at admission: journeys are rebuilt when the slot is done, off the
+                        // rounds' path (a single start-time group: no later round changes them)
   uint16_t gen_group;
   uint32_t next_start;   // index of the next start label (group cursor)
   int32_t cur_start_time;

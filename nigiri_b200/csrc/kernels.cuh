@@ -873,6 +873,17 @@ __device__ bool pareto_add(state const& st, uint32_t s, slot_t& sl, journey_rec 
   return true;
 }
 
+// whether journey j of the slot is to be reconstructed now (search.h:457-475;
+// a pong phase rebuilds only the journey of its ping result, pong.cc:322-339)
+__device__ __forceinline__ bool recon_wanted(slot_t const& sl, journey_rec const& j) {
+  if (j.reconstructed || j.error) return false;
+  auto const tt = j.dest_time > j.start_time ? j.dest_time - j.start_time : j.start_time - j.dest_time;
+  return sl.recon_mode == 0 ? ((sl.ontrip || (sl.iv_from <= j.start_time && j.start_time < sl.iv_to)) &&
+                               tt < sl.fastest_direct)
+         : sl.recon_mode == 1 ? (j.transfers == sl.recon_transfers && j.start_time == sl.recon_start)
+                              : false;
+}
+
 // result collection (raptor.h:393-413) and the reconstruction worklist
 // (search.h:457-475)
 __device__ void collect_slot(state const& st, uint32_t s) {
@@ -898,18 +909,10 @@ __device__ void collect_slot(state const& st, uint32_t s) {
       }
     }
   }
+  if (sl.recon_defer) return;  // rebuilt when the slot is done (k_reconstruct_done)
   auto* els = st.journeys + static_cast<size_t>(s) * st.max_j;
   for (auto i = 0u; i != sl.n_journeys; ++i) {
-    auto const& j = els[i];
-    auto const tt = j.dest_time > j.start_time ? j.dest_time - j.start_time : j.start_time - j.dest_time;
-    auto const want =
-        sl.recon_mode == 0 ? ((sl.ontrip || (sl.iv_from <= j.start_time && j.start_time < sl.iv_to)) &&
-                              tt < sl.fastest_direct)
-        : sl.recon_mode == 1 ? (j.transfers == sl.recon_transfers && j.start_time == sl.recon_start)  // pong.cc:322-339
-                             : false;
-    if (!j.reconstructed && !j.error && want) {
-      st.recon_list[atomicAdd(&st.counters[C_RECON], 1u)] = (s << 16) | i;
-    }
+    if (recon_wanted(sl, els[i])) st.recon_list[atomicAdd(&st.counters[C_RECON], 1u)] = (s << 16) | i;
   }
 }
 
@@ -921,16 +924,11 @@ __global__ void k_end_collect(state st) {
   collect_slot(st, s);
 }
 
-__global__ void k_reconstruct(state st) {
-  auto const lane = threadIdx.x & 31u;
-  auto const warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  auto const n_warps = (gridDim.x * blockDim.x) >> 5;
-  auto const n = st.counters[C_RECON];
-  for (auto i = warp; i < n; i += n_warps) {
+// One journey (slot s, index ji) rebuilt by the calling warp.
+__device__ __forceinline__ void reconstruct_one(state const& st, uint32_t s, uint32_t ji, uint32_t lane) {
+  {
     uint64_t t_begin = 0;
     if (st.profile) asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t_begin));
-    auto const e = st.recon_list[i];
-    auto const s = e >> 16, ji = e & 0xFFFFu;
     auto& sl = st.slots[s];
     auto& j = st.journeys[static_cast<size_t>(s) * st.max_j + ji];
     recon_ctx c;
@@ -962,6 +960,37 @@ __global__ void k_reconstruct(state st) {
         atomicAdd(&st.prof[7], 1ull);
       }
     }
+  }
+}
+
+// the journeys collected in this super-step (queries with several
+// start-time groups: their next group changes the round times)
+__global__ void k_reconstruct(state st) {
+  auto const lane = threadIdx.x & 31u;
+  auto const warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  auto const n_warps = (gridDim.x * blockDim.x) >> 5;
+  auto const n = st.counters[C_RECON];
+  for (auto i = warp; i < n; i += n_warps) {
+    auto const e = st.recon_list[i];
+    reconstruct_one(st, e >> 16, e & 0xFFFFu, lane);
+  }
+}
+
+// The journeys of finished slots whose reconstruction was deferred, listed
+// by the host as (slot << 16 | journey index): launched on the export stream
+// while the next super-steps run.  A finished slot is left alone by the
+// super-step kernels, so its round times are stable.
+__global__ void k_reconstruct_done(state st, uint32_t const* list, uint32_t n) {
+  auto const lane = threadIdx.x & 31u;
+  auto const warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  auto const n_warps = (gridDim.x * blockDim.x) >> 5;
+  for (auto i = warp; i < n; i += n_warps) {
+    auto const e = list[i];
+    auto const s = e >> 16, ji = e & 0xFFFFu;
+    auto const& sl = st.slots[s];
+    if (!sl.recon_defer || ji >= sl.n_journeys) continue;
+    if (!recon_wanted(sl, st.journeys[static_cast<size_t>(s) * st.max_j + ji])) continue;
+    reconstruct_one(st, s, ji, lane);
   }
 }
 
