@@ -49,9 +49,10 @@ def parse():
                    help="with --ncu-case: count route-scan work (stop visits, events)")
     p.add_argument("--ncu-workload", type=int, default=2, choices=[1, 2, 3, 4, 5],
                    help="with --ncu-case: the workload's timetable and queries")
-    p.add_argument("--shape", metavar="B,T,P,R,S",
+    p.add_argument("--shape", metavar="B,T,P,R,S,O",
                    help="with --ncu-case: launch shape (route-scan blocks per SM, threads, pair "
-                        "blocks per SM, reconstruction blocks per SM, super-steps per sync)")
+                        "blocks per SM, reconstruction blocks per SM, super-steps per sync, "
+                        "route-scan occupancy build)")
     p.add_argument("--ncu-summary", metavar="CSV",
                    help="summarise an ncu --csv log (launches, time, share and any other metric "
                         "per kernel) and exit; runs on a machine without a GPU")
@@ -697,7 +698,7 @@ def ncu_case(args, local):
     sh = eng.shape
     print(json.dumps({"ncu_case": True, "batch": args.batch, "super_steps": st.super_steps,
                       "shape": [sh.scan_blocks_per_sm, sh.scan_threads, sh.pair_blocks_per_sm,
-                                sh.recon_blocks_per_sm, sh.steps_per_sync],
+                                sh.recon_blocks_per_sm, sh.steps_per_sync, sh.scan_occupancy],
                       "kernel_launches": st.kernel_launches, "device_ms": st.device_ms,
                       "route_scan_launches": st.route_scan_launches,
                       "route_stop_visits": st.route_stop_visits,

@@ -467,6 +467,10 @@ typedef struct b2r_launch_shape {
   uint32_t pair_blocks_per_sm;  /* route marking, transfers, footpaths (8) */
   uint32_t recon_blocks_per_sm; /* reconstruction, 128-thread blocks (4) */
   uint32_t steps_per_sync;      /* super-steps between host checks (4) */
+  uint32_t scan_occupancy;      /* route scan build: 0 = 64 registers per
+                                   thread (up to 32 resident warps per SM),
+                                   1 = 40 (up to 48 warps, some values kept
+                                   in local memory) (0) */
 } b2r_launch_shape;
 int b2r_engine_get_shape(const b2r_engine* e, b2r_launch_shape* out);
 /* Rejects values out of range; re-captures the super-step graph. */

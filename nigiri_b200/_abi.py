@@ -157,7 +157,7 @@ class BatchStats(C.Structure):
 class LaunchShape(C.Structure):
     _fields_ = [("scan_blocks_per_sm", C.c_uint32), ("scan_threads", C.c_uint32),
                 ("pair_blocks_per_sm", C.c_uint32), ("recon_blocks_per_sm", C.c_uint32),
-                ("steps_per_sync", C.c_uint32)]
+                ("steps_per_sync", C.c_uint32), ("scan_occupancy", C.c_uint32)]
 
 
 class TuneReport(C.Structure):

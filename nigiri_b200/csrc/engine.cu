@@ -111,7 +111,7 @@ struct b2r_engine {
   cudaStream_t stream{nullptr};
   cudaGraphExec_t graph{nullptr};
   cudaStream_t stream2{nullptr};  // exports overlapping the super-steps
-  b2r_launch_shape shape{8, 256, 8, 4, 4};  // launch shape of the super-step
+  b2r_launch_shape shape{8, 256, 8, 4, 4, 0};  // launch shape of the super-step
   cudaGraphExec_t lb_graph{nullptr};  // 4 x 2 Bellman-Ford iterations
   int sms{132};
   std::vector<void*> allocs;
@@ -508,7 +508,11 @@ void enqueue_superstep(b2r_engine& e, cudaStream_t s) {
     ev_b = e.prof_ev[e.prof_used++];
     B2R_CUDA(cudaEventRecord(ev_a, s));
   }
-  dev::k_route_scan<<<e.sms * e.shape.scan_blocks_per_sm, e.shape.scan_threads, 0, s>>>(st);
+  if (e.shape.scan_occupancy != 0U) {
+    dev::k_route_scan<6><<<e.sms * e.shape.scan_blocks_per_sm, e.shape.scan_threads, 0, s>>>(st);
+  } else {
+    dev::k_route_scan<4><<<e.sms * e.shape.scan_blocks_per_sm, e.shape.scan_threads, 0, s>>>(st);
+  }
   if (e.cfg.profile) {
     B2R_CUDA(cudaEventRecord(ev_b, s));
     auto const idx = static_cast<uint32_t>(e.prof_used / 2 - 1);
@@ -2048,6 +2052,13 @@ int b2r_timetable_upload(const b2r_timetable_desc* d, int device, b2r_timetable*
             }
             if (!all_zero && !all_pos) fifo[r] = 0U;
           }
+          // bit 1: on such a route whose columns are ordered by minute and
+          // whose transports all leave the first stop on their service day,
+          // (service day, transport offset) orders the trips as their times
+          // do (the route scan's order key needs no event read then)
+          bool first_day = true;
+          for (auto x = 0U; x != n_t && first_day; ++x) first_day = (c[x] & 31U) == 0U;
+          if (fifo[r] != 0U && sorted[r] != 0U && first_day && n_t < 16384U) fifo[r] |= 2U;
         }
       }
 
@@ -2427,11 +2438,11 @@ int b2r_engine_set_shape(b2r_engine* e, const b2r_launch_shape* sh) {
                     sh->scan_threads >= 32 && sh->scan_threads <= 256 && sh->scan_threads % 32 == 0 &&
                     sh->pair_blocks_per_sm >= 1 && sh->pair_blocks_per_sm <= 64 &&
                     sh->recon_blocks_per_sm >= 1 && sh->recon_blocks_per_sm <= 64 &&
-                    sh->steps_per_sync >= 1 && sh->steps_per_sync <= 64;
+                    sh->steps_per_sync >= 1 && sh->steps_per_sync <= 64 && sh->scan_occupancy <= 1;
     if (!ok) {
       return b2r::fail(B2R_ERR_INVALID_ARGUMENT,
                        "launch shape out of range (blocks per SM 1..64, scan threads 32..256 in steps "
-                       "of 32, steps per sync 1..64)");
+                       "of 32, steps per sync 1..64, scan occupancy 0..1)");
     }
     try {
       B2R_CUDA(cudaSetDevice(e->tt->device));
@@ -2482,7 +2493,8 @@ int b2r_engine_autotune(b2r_engine* e, const b2r_query* sample, uint32_t n, b2r_
                                        {&b2r_launch_shape::scan_threads, {128, 256}},
                                        {&b2r_launch_shape::pair_blocks_per_sm, {2, 4, 8, 16}},
                                        {&b2r_launch_shape::recon_blocks_per_sm, {1, 2, 4, 8}},
-                                       {&b2r_launch_shape::steps_per_sync, {1, 2, 4, 8}}};
+                                       {&b2r_launch_shape::steps_per_sync, {1, 2, 4, 8}},
+                                       {&b2r_launch_shape::scan_occupancy, {0, 1}}};
       for (auto pass = 0; pass != 3; ++pass) {
         auto changed = false;
         for (auto const& k : knobs) {

@@ -68,8 +68,11 @@ struct dtt {
   uint32_t const* loc_routes_idx;
   uint32_t const* loc_routes;
   uint8_t const* route_sorted;  // 1: every event column is ordered by mam
-  // 1: the route's trips (transport, service day) compare the same way at
-  // every event of the route, equal at all or strictly ordered at all
+  // bit 0: the route's trips (transport, service day) compare the same way
+  // at every event of the route, equal at all or strictly ordered at all;
+  // bit 1: and (service day, transport offset) orders them as their times
+  // do (columns ordered by minute, every first departure on its service day,
+  // fewer than 16384 transports)
   uint8_t const* route_fifo;
   // lower-bound graphs (build_lb_graph.h), packed footpath words
   uint32_t const* lbg_fwd_idx;
@@ -271,7 +274,7 @@ __device__ __forceinline__ int from_key(bool fwd, int k) { return fwd ? k : ~k; 
 __device__ __forceinline__ int key_add(int key, int x) { return clamp16(key + x); }
 
 __device__ __forceinline__ bool bf_test(dtt const& T, uint32_t bf, uint32_t i) {
-  return i < B2R_MAX_DAYS && ((T.bf[8ull * bf + (i >> 6)] >> (i & 63u)) & 1ull);
+  return i < B2R_MAX_DAYS && ((__ldg(T.bf + 8ull * bf + (i >> 6)) >> (i & 63u)) & 1ull);
 }
 
 // The route filters of loop_routes (raptor.h:499-545) and of get_transport

@@ -322,7 +322,7 @@ struct scan_ctr {
 // (can_start / can_finish, raptor.h:1252, 1304)
 __device__ __forceinline__ uint32_t scan_stop_word(dtt const& T, uint32_t sb, uint32_t n, bool fwd, uint32_t i,
                                                    uint32_t sec) {
-  auto const w = T.route_stops[sb + (fwd ? i : n - 1u - i)];
+  auto const w = __ldg(T.route_stops + sb + (fwd ? i : n - 1u - i));
   return (sec & 0x100u) != 0u ? (w & 0xCFFFFFFFu) | ((w >> 2) & 0x30000000u) : w;
 }
 
@@ -409,23 +409,27 @@ __device__ __forceinline__ void scan_pair(state const& st, lane_t const& ln, uin
   uint32_t sec = 0u;  // required flags checked per section (bits 0-3); bit 8: wheelchair profile
   if ((ln.claszes != 0xFFFFu || ln.req != 0u) && !route_allowed(T, r, ln.claszes, ln.req, sec)) return;
   if ((ln.mode & 0x70u) == (B2R_PROFILE_WHEELCHAIR << 4)) sec |= 0x100u;
-  if ((sec & 15u) != 0u || T.route_fifo[r] == 0u) {
+  auto const order = static_cast<uint32_t>(__ldg(T.route_fifo + r));
+  if ((sec & 15u) != 0u || order == 0u) {
     if (lane == 0u) scan_walk_seq(st, ln, r, g, b, sec, 0u, false, 0u, 0u, pc);
     return;
   }
   auto const bit = 1u << b;
   auto const fwd = ln.fwd != 0;
   auto const k = static_cast<uint32_t>(ln.k);
-  auto const sb = T.route_stop_idx[r];
-  auto const n = T.route_stop_idx[r + 1] - sb;
-  auto const n_t = T.route_tr_to[r] - T.route_tr_from[r];
-  auto const* colbase = T.st + T.route_st_from[r];
+  auto const sb = __ldg(T.route_stop_idx + r);
+  auto const n = __ldg(T.route_stop_idx + r + 1) - sb;
+  auto const n_t = __ldg(T.route_tr_to + r) - __ldg(T.route_tr_from + r);
+  auto const* colbase = T.st + __ldg(T.route_st_from + r);
   auto const lb_off = (ln.mode & 8u) != 0u;
-  // the trip carried over from the earlier chunks: its order key (the time
-  // at the route's first departure event, negated backward: smaller is
-  // better), transport offset and service day
+  // The trips' order key, below 2^21, smaller is better: with route_fifo
+  // bit 1 (service day - base + 64) * n_t + transport offset (the service
+  // day lies within 64 days of the base day, n_t < 2^14), else the time at
+  // the route's first departure event (|t| < 2^20 minutes) + 2^20; both
+  // mirrored backward, where later is better.
+  // The trip carried over from the earlier chunks: key, offset, day.
   bool c_valid = false;
-  int c_key = 0;
+  uint32_t c_key = 0;
   uint32_t c_off = 0;
   uint16_t c_day = 0;
   for (auto i0 = 0u; i0 < n; i0 += 32u) {
@@ -435,11 +439,13 @@ __device__ __forceinline__ void scan_pair(state const& st, lane_t const& ln, uin
     uint32_t stp = 0, l = 0;
     bool marked = false;
     uint16_t lbv = 0;
+    uint32_t prw = 0xFFFFFFFFu;  // previous round's label, loaded beside the mark
     if (act) {
       stp = scan_stop_word(T, sb, n, fwd, i, sec);
       l = B2R_STOP_LOC(stp);
       marked = (st.X[l * st.G + g] & bit) != 0u;
       if (!lb_off) lbv = st.lb[li(st, l, s)];
+      if (i + 1u != n && (fwd ? B2R_STOP_IN(stp) : B2R_STOP_OUT(stp)) != 0u) prw = st.rt[rti(st, k - 1u, l, s)];
     }
     auto const can_finish = act && (fwd ? B2R_STOP_OUT(stp) : B2R_STOP_IN(stp)) != 0u;
     auto const boardable = act && i + 1u != n && (fwd ? B2R_STOP_IN(stp) : B2R_STOP_OUT(stp)) != 0u && marked;
@@ -451,17 +457,22 @@ __device__ __forceinline__ void scan_pair(state const& st, lane_t const& ln, uin
     bool cand = false, cb_bad = false;
     uint32_t nt = 0;
     uint16_t nd = 0;
-    int key = 0;
+    uint32_t key = 0;
     if (boardable && lane < fb) {
-      auto const prt = dec(st.rt[rti(st, k - 1u, l, s)], ln.qtag);
+      auto const prt = dec(prw, ln.qtag);
       if (prt != kKeyInv) {
         auto const minutes = static_cast<int>(ln.base) * 1440 + from_key(fwd, prt);
         if (et_search(T, fwd, r, si, static_cast<uint16_t>(minutes / 1440), minutes % 1440, static_cast<int>(lbv),
                       ln.tad_k, ln.base, nt, nd, pc.ev, pc.days)) {
           cand = true;
           cb_bad = dec(st.best[li(st, l, s)], ln.gtag) == kKeyInv && dec(st.tmp[li(st, l, s)], ln.gtag) == kKeyInv;
-          auto const t = (static_cast<int>(nd) - static_cast<int>(ln.base)) * 1440 + delta_count(colbase[nt]);
-          key = fwd ? t : -t;
+          if ((order & 2u) != 0u) {
+            auto const x = static_cast<uint32_t>(static_cast<int>(nd) - static_cast<int>(ln.base) + 64) * n_t + nt;
+            key = fwd ? x : (1u << 21) - 1u - x;
+          } else {
+            auto const t = (static_cast<int>(nd) - static_cast<int>(ln.base)) * 1440 + delta_count(__ldg(colbase + nt));
+            key = static_cast<uint32_t>((fwd ? t : -t) + (1 << 20));
+          }
         }
       }
     }
@@ -473,10 +484,9 @@ __device__ __forceinline__ void scan_pair(state const& st, lane_t const& ln, uin
       pc.stops += min(n - i0, min(fb + 1u, 32u));
       ++pc.warp_steps;
     }
-    // prefix minimum of (key, later stop first) over the lanes; |key| is
-    // below 2^20 (days < 512), so key + 2^20 takes 21 bits above 5 for the
-    // lane
-    auto v = cand ? (static_cast<uint32_t>(key + (1 << 20)) << 5) | (31u - lane) : 0xFFFFFFFFu;
+    // prefix minimum of (key, later stop first) over the lanes: the key's
+    // 21 bits above 5 for the lane
+    auto v = cand ? (key << 5) | (31u - lane) : 0xFFFFFFFFu;
     for (auto o = 1u; o < 32u; o <<= 1) {
       auto const y = __shfl_up_sync(kFull, v, o);
       if (lane >= o) v = min(v, y);
@@ -488,12 +498,12 @@ __device__ __forceinline__ void scan_pair(state const& st, lane_t const& ln, uin
     auto const x_off = __shfl_sync(kFull, nt, src);
     auto const x_day = static_cast<uint16_t>(__shfl_sync(kFull, static_cast<uint32_t>(nd), src));
     // the carried trip loses ties to the later stops of this chunk
-    auto const use_x = ex != 0xFFFFFFFFu && (!c_valid || static_cast<int>(ex >> 5) - (1 << 20) <= c_key);
+    auto const use_x = ex != 0xFFFFFFFFu && (!c_valid || (ex >> 5) <= c_key);
     auto const et_valid = use_x || c_valid;
     if (act && lane <= fb && et_valid && can_finish) {
       auto const et_off = use_x ? x_off : c_off;
       auto const et_day = use_x ? x_day : c_day;
-      auto const ev = colbase[n_t * (si * 2u - (fwd ? 1u : 0u)) + et_off];
+      auto const ev = __ldg(colbase + n_t * (si * 2u - (fwd ? 1u : 0u)) + et_off);
       scan_arrive(st, ln, s, g, bit, l, lbv, to_delta_key(fwd, et_day, ln.base, delta_count(ev)), pc);
     }
     if (fb != 32u) return;
@@ -501,7 +511,7 @@ __device__ __forceinline__ void scan_pair(state const& st, lane_t const& ln, uin
       auto const t_src = static_cast<int>(31u - (tot & 31u));
       auto const t_off = __shfl_sync(kFull, nt, t_src);
       auto const t_day = static_cast<uint16_t>(__shfl_sync(kFull, static_cast<uint32_t>(nd), t_src));
-      auto const t_key = static_cast<int>(tot >> 5) - (1 << 20);
+      auto const t_key = tot >> 5;
       if (!c_valid || t_key <= c_key) {
         c_valid = true;
         c_key = t_key;
@@ -513,8 +523,10 @@ __device__ __forceinline__ void scan_pair(state const& st, lane_t const& ln, uin
 }
 
 // A warp per marked (route, group of 32 queries) entry, one pair of the
-// entry after the other.
-__global__ void __launch_bounds__(256) k_route_scan(const __grid_constant__ state st) {
+// entry after the other.  Two builds, with four or six blocks of 256
+// threads resident per SM (64 or 40 registers; the launch shape picks one).
+template <int MinBlocks>
+__global__ void __launch_bounds__(256, MinBlocks) k_route_scan(const __grid_constant__ state st) {
   auto const lane = threadIdx.x & 31u;
   auto const warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   auto const n_warps = (gridDim.x * blockDim.x) >> 5;
