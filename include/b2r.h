@@ -410,6 +410,116 @@ int b2r_one_to_all_noalloc(const b2r_timetable* tt, const b2r_query* q,
                            int16_t* round_times, uint64_t capacity,
                            uint32_t* n_rows, int32_t* base_day, void* stream);
 
+/* ------------------------------------------------------------------------
+ * The Algo concept of routing::search<Dir, Algo>.
+ *
+ * nigiri's search<Dir, Algo> (search.h:78-505) prepares a query
+ * (search::init, search.h:84-172: transfer-time normalisation, destination
+ * set, lower bounds, base day; add_start_labels, search.h:401-411) and then
+ * drives an Algo through reset_arrivals / next_start_time / add_start /
+ * execute / reconstruct (raptor.h:56-73, 174-203, 205-414, 416-452).
+ * b2r_search_prepare is that preparation on the host; b2r_raptor is the
+ * Algo: one query's raptor_state resident on the device, each execute the
+ * rounds of one start time.  Static timetable, no vias, no time-dependent
+ * offsets. */
+typedef struct b2r_start {     /* routing::start, start_times.h:21-26 */
+  int32_t time_at_start;       /* minutes since the epoch */
+  int32_t time_at_stop;
+  uint32_t location;
+} b2r_start;
+
+typedef struct b2r_search_plan {
+  int32_t status;              /* B2R_OK, or why the query cannot be searched */
+  uint8_t direction;
+  uint8_t ontrip;              /* start_time_ is a point in time */
+  uint8_t start_dest_overlap;  /* search.h:354-378: the result is empty */
+  uint8_t max_transfers;
+  int32_t base_day;            /* days since the epoch (search.h:148-160) */
+  int32_t interval_from, interval_to; /* search_interval_ after
+                                         interval_estimator::initial */
+  int16_t fastest_direct;      /* fastest_direct_ (minutes) */
+  int16_t max_travel_time;     /* query::max_travel_time_ after sanitize */
+  uint8_t tts_default;         /* transfer_time_settings after search::init */
+  uint8_t pad2;
+  int16_t tts_min_transfer_time, tts_additional_time;
+  float tts_factor;
+  uint32_t n_starts;           /* state_.starts_ in search order */
+  const b2r_start* starts;
+  uint32_t n_destinations;     /* is_destination_: set bits, ascending */
+  const uint32_t* destinations;
+  const uint16_t* dist_to_dest;/* n_locations entries (0xFFFF: none), or NULL
+                                  for a station-to-station query */
+  const uint16_t* lower_bounds;/* n_locations: travel_time_lower_bound_
+                                  (0xFFFF: unreachable) */
+} b2r_search_plan;
+
+/* The host part of search::init for query q (raptor queries; q->kind
+ * B2R_ONE_TO_ONE).  The plan owns its arrays; free it with
+ * b2r_search_plan_free. */
+int b2r_search_prepare(const b2r_timetable* tt, const b2r_query* q, b2r_search_plan** out);
+void b2r_search_plan_free(b2r_search_plan* p);
+/* One interval extension of search::execute (search.h:275-316): the search
+ * interval grown for n_missing more results (interval_estimator::
+ * extension), and plan->starts replaced by the start labels of the new
+ * parts in search order.  *changed = 0: the interval cannot grow, the
+ * search ends.  *reset_arrivals = 1: the Algo's arrivals are to be reset
+ * and the results outside the old interval removed first
+ * (remove_ontrip_results). */
+int b2r_search_extend(const b2r_timetable* tt, b2r_search_plan* plan, uint32_t n_missing,
+                      uint8_t* changed, uint8_t* reset_arrivals);
+
+/* The Algo's constructor arguments (raptor.h:56-73), static instantiation:
+ * no real-time overlay, no vias, no time-dependent offsets. */
+typedef struct b2r_raptor_args {
+  uint8_t direction;
+  uint8_t prf_idx;             /* footpath profile; B2R_PROFILE_WHEELCHAIR
+                                  is the reference's is_wheelchair */
+  uint8_t require_bike_transport, require_car_transport;
+  uint8_t no_compulsory_reservation;
+  uint8_t tts_default;
+  uint16_t allowed_claszes;    /* clasz_mask_t */
+  int16_t tts_min_transfer_time, tts_additional_time;
+  float tts_factor;
+  int32_t base_day;            /* the base day, days since the epoch */
+  uint32_t n_destinations;     /* is_dest: set bits */
+  const uint32_t* destinations;
+  const uint16_t* dist_to_dest;/* n_locations entries, or NULL */
+  const uint16_t* lower_bounds;/* n_locations entries, or NULL: lb = 0 */
+} b2r_raptor_args;
+
+typedef struct b2r_raptor b2r_raptor;
+/* A raptor state on tt's device with the constructor's arguments (copied).
+ * One host thread at a time, like the reference's per-thread search
+ * state. */
+int b2r_raptor_create(b2r_timetable* tt, const b2r_raptor_args* args, b2r_raptor** out);
+int b2r_raptor_destroy(b2r_raptor* r);
+/* raptor::reset_arrivals (raptor.h:174-177): round times and
+ * time_at_dest invalid before the next execute. */
+int b2r_raptor_reset_arrivals(b2r_raptor* r);
+/* raptor::next_start_time (raptor.h:179-188): best / tmp and the marks
+ * reset, the start labels of the next execute start empty. */
+int b2r_raptor_next_start_time(b2r_raptor* r);
+/* raptor::add_start (raptor.h:190-203): a start label at location l at
+ * time t (minutes since the epoch). */
+int b2r_raptor_add_start(b2r_raptor* r, uint32_t location, int32_t time);
+/* raptor::execute (raptor.h:205-414): the rounds from the start labels
+ * added since next_start_time, then the journeys of every round that
+ * reaches a destination, as the reference adds them to its pareto set
+ * (start_time, dest_time, dest, transfers; no legs).  At most `capacity`
+ * are written; *n receives their number (B2R_ERR_CAPACITY if more). */
+int b2r_raptor_execute(b2r_raptor* r, int32_t start_time, uint8_t max_transfers,
+                       int32_t worst_time_at_dest, b2r_journey* results,
+                       uint32_t capacity, uint32_t* n);
+/* raptor::reconstruct (raptor.h:416-452, reconstruct.cc:162-902): the legs
+ * of journey j (its start_time, dest_time, dest and transfers) from the
+ * round times of the last execute, for query q (offsets, match modes).
+ * On success j->n_legs legs go to legs[0..] (capacity at least 40); a
+ * journey the reference could not rebuild comes back with j->error = 1. */
+int b2r_raptor_reconstruct(b2r_raptor* r, const b2r_query* q, b2r_journey* j,
+                           b2r_leg* legs, uint32_t capacity);
+/* Rounds run so far (raptor_stats::n_rounds_). */
+uint64_t b2r_raptor_rounds(const b2r_raptor* r);
+
 /* Serving: asynchronous submission.  Queries are admitted into free slots at
  * super-step boundaries by a driver thread; results are fetched by ticket. */
 int b2r_serve_start(b2r_engine* e);

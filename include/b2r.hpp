@@ -24,11 +24,14 @@
  */
 #pragma once
 
+#include <algorithm>
 #include <cstdint>
+#include <iterator>
 #include <optional>
 #include <span>
 #include <stdexcept>
 #include <string>
+#include <tuple>
 #include <utility>
 #include <variant>
 #include <vector>
@@ -129,7 +132,47 @@ struct journey {
   uint32_t dest_{0};
   uint8_t transfers_{0};
   bool error_{false};
+  bool is_reconstructed_{false};
   friend bool operator==(journey const&, journey const&) = default;
+
+  // journey::dominates, journey.h:84-92
+  bool dominates(journey const& o) const {
+    if (start_time_ <= dest_time_) {
+      return transfers_ <= o.transfers_ && start_time_ >= o.start_time_ && dest_time_ <= o.dest_time_;
+    }
+    return transfers_ <= o.transfers_ && start_time_ <= o.start_time_ && dest_time_ >= o.dest_time_;
+  }
+};
+
+// routing::pareto_set, pareto_set.h:13-60: add() keeps only undominated
+// elements, in insertion order.
+template <typename T>
+struct pareto_set {
+  using iterator = typename std::vector<T>::iterator;
+  std::tuple<bool, iterator, iterator> add(T&& el) {
+    auto n_removed = std::size_t{0};
+    for (auto i = std::size_t{0}; i < els_.size(); ++i) {
+      if (els_[i].dominates(el)) return {false, end(), begin() + static_cast<std::ptrdiff_t>(i)};
+      if (el.dominates(els_[i])) {
+        ++n_removed;
+        continue;
+      }
+      els_[i - n_removed] = els_[i];
+    }
+    els_.resize(els_.size() - n_removed);
+    els_.emplace_back(std::move(el));
+    return {true, std::prev(end()), end()};
+  }
+  iterator begin() { return els_.begin(); }
+  iterator end() { return els_.end(); }
+  std::size_t size() const { return els_.size(); }
+  bool empty() const { return els_.empty(); }
+  void clear() { els_.clear(); }
+  template <typename Fn>
+  void erase_if(Fn&& fn) {
+    els_.erase(std::remove_if(els_.begin(), els_.end(), fn), els_.end());
+  }
+  std::vector<T> els_;
 };
 
 struct routing_result {
@@ -154,18 +197,31 @@ struct raptor_state {
 // arrays are copied, so they may be freed after construction.
 class timetable {
 public:
-  explicit timetable(b2r_timetable_desc const& d, int device = 0) : n_locations_{d.n_locations} {
+  explicit timetable(b2r_timetable_desc const& d, int device = 0)
+      : n_locations_{d.n_locations}, internal_from_days_{d.date_range_from - B2R_TIMETABLE_OFFSET_DAYS} {
     check(b2r_timetable_upload(&d, device, &h_), "b2r_timetable_upload");
   }
+  // an image uploaded elsewhere (from description d), not destroyed here
+  timetable(b2r_timetable* uploaded, b2r_timetable_desc const& d)
+      : h_{uploaded},
+        n_locations_{d.n_locations},
+        internal_from_days_{d.date_range_from - B2R_TIMETABLE_OFFSET_DAYS},
+        owned_{false} {}
   timetable(timetable const&) = delete;
   timetable& operator=(timetable const&) = delete;
-  ~timetable() { b2r_timetable_destroy(h_); }
+  ~timetable() {
+    if (owned_) b2r_timetable_destroy(h_);
+  }
   b2r_timetable* handle() const { return h_; }
   uint32_t n_locations() const { return n_locations_; }
+  // first day of timetable::internal_interval(), days since the epoch
+  int32_t internal_from_days() const { return internal_from_days_; }
 
 private:
   b2r_timetable* h_{nullptr};
   uint32_t n_locations_;
+  int32_t internal_from_days_;
+  bool owned_{true};
 };
 
 // Resident query slots on one GPU (b2r_engine_create).  Like nigiri's
@@ -252,6 +308,50 @@ struct c_query {
 
 }  // namespace detail
 
+// A C ABI query in nigiri's terms (the inverse of detail::c_query).
+inline query query_of(b2r_query const& c) {
+  query q;
+  if (c.is_interval != 0) q.start_time_ = interval{c.interval_from, c.interval_to};
+  else q.start_time_ = c.start_time;
+  q.start_match_mode_ = static_cast<location_match_mode>(c.start_match_mode);
+  q.dest_match_mode_ = static_cast<location_match_mode>(c.dest_match_mode);
+  q.use_start_footpaths_ = c.use_start_footpaths != 0;
+  for (auto i = 0U; i != c.n_start; ++i) {
+    q.start_.push_back({c.start[i].target, c.start[i].duration, c.start[i].transport_mode_id});
+  }
+  for (auto i = 0U; i != c.n_destination; ++i) {
+    q.destination_.push_back({c.destination[i].target, c.destination[i].duration,
+                              c.destination[i].transport_mode_id});
+  }
+  q.max_start_offset_ = c.max_start_offset;
+  q.max_transfers_ = c.max_transfers;
+  q.max_travel_time_ = c.max_travel_time;
+  q.min_connection_count_ = c.min_connection_count;
+  q.extend_interval_earlier_ = c.extend_interval_earlier != 0;
+  q.extend_interval_later_ = c.extend_interval_later != 0;
+  if (c.has_fastest_direct != 0) q.fastest_direct_ = c.fastest_direct;
+  q.fastest_direct_factor_ = c.fastest_direct_factor;
+  q.transfer_time_settings_ = {c.tts_default != 0, c.tts_min_transfer_time, c.tts_additional_time, c.tts_factor};
+  q.allowed_claszes_ = static_cast<uint16_t>(c.allowed_claszes);
+  q.require_bike_transport_ = c.require_bike_transport != 0;
+  q.require_car_transport_ = c.require_car_transport != 0;
+  q.no_compulsory_reservation_ = c.no_compulsory_reservation != 0;
+  q.prf_idx_ = c.prf_idx;
+  if (c.has_max_interval != 0) q.max_interval_ = interval{c.max_interval_from, c.max_interval_to};
+  return q;
+}
+
+// One C ABI leg as a routing::journey::leg.
+inline leg leg_of(b2r_leg const& l) {
+  leg y{l.from, l.to, l.dep_time, l.arr_time, {}};
+  switch (l.kind) {
+    case B2R_LEG_TRANSPORT: y.uses_ = run_enter_exit{l.transport, l.day, l.stop_from, l.stop_to}; break;
+    case B2R_LEG_FOOTPATH: y.uses_ = footpath{l.transport, l.duration}; break;
+    default: y.uses_ = offset{l.transport, l.duration, l.transport_mode_id};
+  }
+  return y;
+}
+
 // The journeys of one C ABI result, as routing::journey values.
 inline std::vector<journey> journeys_of(b2r_result const& r) {
   std::vector<journey> out;
@@ -264,16 +364,8 @@ inline std::vector<journey> journeys_of(b2r_result const& r) {
     x.dest_ = j.dest;
     x.transfers_ = j.transfers;
     x.error_ = j.error != 0;
-    for (auto k = 0U; k != j.n_legs; ++k) {
-      auto const& l = r.legs[j.first_leg + k];
-      leg y{l.from, l.to, l.dep_time, l.arr_time, {}};
-      switch (l.kind) {
-        case B2R_LEG_TRANSPORT: y.uses_ = run_enter_exit{l.transport, l.day, l.stop_from, l.stop_to}; break;
-        case B2R_LEG_FOOTPATH: y.uses_ = footpath{l.transport, l.duration}; break;
-        default: y.uses_ = offset{l.transport, l.duration, l.transport_mode_id};
-      }
-      x.legs_.push_back(std::move(y));
-    }
+    x.is_reconstructed_ = true;  // the engine returns rebuilt journeys only
+    for (auto k = 0U; k != j.n_legs; ++k) x.legs_.push_back(leg_of(r.legs[j.first_leg + k]));
     out.push_back(std::move(x));
   }
   return out;
@@ -337,6 +429,240 @@ inline raptor_state one_to_all(engine& e, query const& q, direction dir) {
   s.round_times_.assign(r.round_times, r.round_times + static_cast<size_t>(r.n_rows) * s.n_locations_);
   return s;
 }
+
+// ---------------------------------------------------------------------------
+// The Algo concept of routing::search<Dir, Algo> over the engine.
+//
+// search<Dir, Algo> constructs its Algo with the query's prepared state
+// (search.h:148-171) and drives it through reset_arrivals, next_start_time,
+// add_start, execute and reconstruct.  b2r_algo is that Algo for the
+// B200 engine: one query's raptor_state resident on the device (the C ABI's
+// b2r_raptor), each execute the rounds of one start time; the search
+// direction is a template parameter as in raptor<SearchDir, ...>.  Its constructor
+// takes raptor's arguments (raptor.h:56-73) for the static timetable: the
+// real-time overlay, vias and time-dependent offsets must be absent
+// (b2r::error B2R_ERR_UNSUPPORTED otherwise).
+
+struct b2r_algo_state {};  // raptor_state's place: the device state is the algo's own
+
+struct b2r_algo_stats {
+  uint64_t n_rounds_{0};
+};
+
+struct via_stop {};   // vias are not supported: the list must be empty
+struct td_offset {};  // time-dependent offsets are not supported
+
+template <direction SearchDir>
+class b2r_algo {
+public:
+  using algo_state_t = b2r_algo_state;
+  using algo_stats_t = b2r_algo_stats;
+  static constexpr bool kUseLowerBounds = true;
+
+  b2r_algo(b2r::timetable& tt, void const* rtt, algo_state_t&, std::vector<bool> const& is_dest,
+           std::vector<std::vector<bool>> const& is_via, std::vector<uint16_t> const& dist_to_dest,
+           std::vector<std::pair<uint32_t, std::vector<td_offset>>> const& td_dist_to_dest,
+           std::vector<uint16_t> const& lb, std::vector<via_stop> const& via_stops, uint16_t base,
+           uint16_t allowed_claszes, bool require_bike_transport, bool require_car_transport, bool is_wheelchair,
+           bool no_compulsory_reservation, transfer_time_settings const& tts, uint8_t prf_idx) {
+    if (rtt != nullptr || !via_stops.empty() || !td_dist_to_dest.empty()) {
+      throw error{B2R_ERR_UNSUPPORTED, "b2r_algo: real-time overlay, vias and time-dependent offsets"};
+    }
+    for (auto const& v : is_via) {
+      if (std::find(v.begin(), v.end(), true) != v.end()) throw error{B2R_ERR_UNSUPPORTED, "b2r_algo: vias"};
+    }
+    (void)is_wheelchair;  // the wheelchair profile (prf_idx) carries it
+    std::vector<uint32_t> dests;
+    for (auto l = std::size_t{0}; l < is_dest.size(); ++l) {
+      if (is_dest[l]) dests.push_back(static_cast<uint32_t>(l));
+    }
+    b2r_raptor_args a{};
+    a.direction = static_cast<uint8_t>(SearchDir);
+    a.prf_idx = prf_idx;
+    a.require_bike_transport = require_bike_transport ? 1 : 0;
+    a.require_car_transport = require_car_transport ? 1 : 0;
+    a.no_compulsory_reservation = no_compulsory_reservation ? 1 : 0;
+    a.tts_default = tts.default_ ? 1 : 0;
+    a.allowed_claszes = allowed_claszes;
+    a.tts_min_transfer_time = tts.min_transfer_time_;
+    a.tts_additional_time = tts.additional_time_;
+    a.tts_factor = tts.factor_;
+    a.base_day = tt.internal_from_days() + base;
+    a.n_destinations = static_cast<uint32_t>(dests.size());
+    a.destinations = dests.data();
+    a.dist_to_dest = dist_to_dest.empty() ? nullptr : dist_to_dest.data();
+    a.lower_bounds = lb.empty() ? nullptr : lb.data();
+    check(b2r_raptor_create(tt.handle(), &a, &h_), "b2r_raptor_create");
+  }
+  b2r_algo(b2r_algo const&) = delete;
+  b2r_algo& operator=(b2r_algo const&) = delete;
+  ~b2r_algo() { b2r_raptor_destroy(h_); }
+
+  void reset_arrivals() { check(b2r_raptor_reset_arrivals(h_), "reset_arrivals"); }
+  void next_start_time() { check(b2r_raptor_next_start_time(h_), "next_start_time"); }
+  void add_start(uint32_t l, unixtime_t t) { check(b2r_raptor_add_start(h_, l, t), "add_start"); }
+
+  void execute(unixtime_t start_time, uint8_t max_transfers, unixtime_t worst_time_at_dest,
+               pareto_set<journey>& results) {
+    std::vector<b2r_journey> js(B2R_K * 64U);
+    uint32_t n = 0;
+    check(b2r_raptor_execute(h_, start_time, max_transfers, worst_time_at_dest, js.data(),
+                             static_cast<uint32_t>(js.size()), &n),
+          "execute");
+    for (auto i = 0U; i != n; ++i) {  // raptor.h:393-413
+      journey j;
+      j.start_time_ = js[i].start_time;
+      j.dest_time_ = js[i].dest_time;
+      j.dest_ = js[i].dest;
+      j.transfers_ = js[i].transfers;
+      results.add(std::move(j));
+    }
+  }
+
+  void reconstruct(query const& q, journey& j) {
+    detail::c_query cq{q, SearchDir, static_cast<uint8_t>(B2R_ONE_TO_ONE)};
+    b2r_journey bj{j.start_time_, j.dest_time_, j.dest_, j.transfers_, 0, 0, 0};
+    std::vector<b2r_leg> legs(64);
+    check(b2r_raptor_reconstruct(h_, &cq.c, &bj, legs.data(), static_cast<uint32_t>(legs.size())),
+          "reconstruct");
+    if (bj.error != 0) throw error{B2R_ERR_INTERNAL, "reconstruct failed"};
+    j.legs_.clear();
+    for (auto i = 0U; i != bj.n_legs; ++i) j.legs_.push_back(leg_of(legs[i]));
+    j.is_reconstructed_ = true;
+  }
+
+  algo_stats_t get_stats() const { return {b2r_raptor_rounds(h_)}; }
+
+private:
+  b2r_raptor* h_{nullptr};
+};
+
+// routing::search<SearchDir, Algo> (search.h:78-505) for the static
+// timetable: search::init's preparation (b2r_search_prepare), the start
+// times in groups with early termination, reconstruction of the new
+// journeys, interval extension, and the final filtering and ordering.
+template <direction SearchDir, typename Algo>
+class search {
+  static constexpr bool kFwd = SearchDir == direction::kForward;
+
+public:
+  search(b2r::timetable& tt, typename Algo::algo_state_t& state, query q)
+      : tt_{tt}, state_{state}, q_{std::move(q)} {}
+
+  routing_result execute() {
+    detail::c_query cq{q_, SearchDir, static_cast<uint8_t>(B2R_ONE_TO_ONE)};
+    b2r_search_plan* plan = nullptr;
+    check(b2r_search_prepare(tt_.handle(), &cq.c, &plan), "b2r_search_prepare");
+    struct free_plan {
+      b2r_search_plan* p;
+      ~free_plan() { b2r_search_plan_free(p); }
+    } guard{plan};
+    routing_result res;
+    res.status_ = plan->status;
+    res.interval_ = {plan->interval_from, plan->interval_to};
+    if (plan->status != B2R_OK || plan->start_dest_overlap != 0) return res;
+
+    std::vector<bool> is_dest(tt_.n_locations(), false);
+    for (auto i = 0U; i != plan->n_destinations; ++i) is_dest[plan->destinations[i]] = true;
+    std::vector<uint16_t> dist, lb;
+    if (plan->dist_to_dest != nullptr) dist.assign(plan->dist_to_dest, plan->dist_to_dest + tt_.n_locations());
+    if (plan->lower_bounds != nullptr) lb.assign(plan->lower_bounds, plan->lower_bounds + tt_.n_locations());
+    transfer_time_settings const tts{plan->tts_default != 0, plan->tts_min_transfer_time,
+                                     plan->tts_additional_time, plan->tts_factor};
+    Algo algo{tt_, nullptr, state_, is_dest, {}, dist, {}, lb, {},
+              static_cast<uint16_t>(plan->base_day - tt_.internal_from_days()), q_.allowed_claszes_,
+              q_.require_bike_transport_, q_.require_car_transport_, q_.prf_idx_ == B2R_PROFILE_WHEELCHAIR,
+              q_.no_compulsory_reservation_, tts, q_.prf_idx_};
+
+    ontrip_ = plan->ontrip != 0;
+    interval_ = {plan->interval_from, plan->interval_to};
+    fastest_direct_ = plan->fastest_direct;
+    max_travel_time_ = plan->max_travel_time;
+    while (true) {  // search.h:227-317
+      search_interval(algo, *plan);
+      if (results_.empty() || ontrip_ || n_results_in_interval() >= q_.min_connection_count_) break;
+      uint8_t changed = 0, reset = 0;
+      check(b2r_search_extend(tt_.handle(), plan, q_.min_connection_count_ - n_results_in_interval(), &changed,
+                              &reset),
+            "b2r_search_extend");
+      if (changed == 0) break;
+      if (reset != 0) {
+        algo.reset_arrivals();
+        results_.erase_if([&](journey const& j) { return !contains(j.start_time_); });  // remove_ontrip_results
+      }
+      interval_ = {plan->interval_from, plan->interval_to};
+    }
+    if (!ontrip_) {  // search.h:319-336
+      results_.erase_if([&](journey const& j) {
+        return !contains(j.start_time_) || j.travel_time() >= fastest_direct_ || j.travel_time() > max_travel_time_;
+      });
+      std::sort(results_.begin(), results_.end(), [](journey const& a, journey const& b) {
+        return std::tie(a.start_time_, a.transfers_) < std::tie(b.start_time_, b.transfers_);
+      });
+    }
+    results_.erase_if([](journey const& j) { return !j.is_reconstructed_; });
+    res.journeys_ = results_.els_;
+    res.interval_ = interval_;
+    res.n_rounds_ = algo.get_stats().n_rounds_;
+    res.n_start_times_ = n_start_times_;
+    return res;
+  }
+
+private:
+  bool contains(unixtime_t t) const { return interval_.from_ <= t && t < interval_.to_; }
+
+  unsigned n_results_in_interval() {  // search.h:380-389
+    if (ontrip_) return static_cast<unsigned>(results_.size());
+    return static_cast<unsigned>(
+        std::count_if(results_.begin(), results_.end(), [&](journey const& j) { return contains(j.start_time_); }));
+  }
+
+  // search.h:419-494: one execute per group of start labels with the same
+  // time at start
+  void search_interval(Algo& algo, b2r_search_plan const& plan) {
+    auto early_termination = false;
+    for (auto i = 0U; i < plan.n_starts;) {
+      auto j = i;
+      while (j != plan.n_starts && plan.starts[j].time_at_start == plan.starts[i].time_at_start) ++j;
+      if (!early_termination) {
+        algo.next_start_time();
+        auto const start_time = plan.starts[i].time_at_start;
+        for (auto x = i; x != j; ++x) algo.add_start(plan.starts[x].location, plan.starts[x].time_at_stop);
+        auto const worst_time_at_dest =
+            start_time + (kFwd ? 1 : -1) * (std::min(fastest_direct_, max_travel_time_) + 1);
+        algo.execute(start_time, q_.max_transfers_, worst_time_at_dest, results_);
+        ++n_start_times_;
+        for (auto& jr : results_) {
+          if (!jr.is_reconstructed_ && !jr.error_ && (ontrip_ || contains(jr.start_time_)) &&
+              jr.travel_time() < fastest_direct_) {
+            try {
+              algo.reconstruct(q_, jr);
+            } catch (error const&) {
+              jr.error_ = true;
+            }
+          }
+        }
+        if (q_.min_connection_count_ > 0 && n_results_in_interval() >= q_.min_connection_count_ &&
+            ((kFwd && q_.extend_interval_earlier_ && !q_.extend_interval_later_) ||
+             (!kFwd && !q_.extend_interval_earlier_ && q_.extend_interval_later_))) {
+          early_termination = true;
+          if (kFwd) interval_.from_ = start_time;
+          else interval_.to_ = start_time + 1;
+        }
+      }
+      i = j;
+    }
+  }
+
+  b2r::timetable& tt_;
+  typename Algo::algo_state_t& state_;
+  query q_;
+  pareto_set<journey> results_;
+  bool ontrip_{true};
+  interval interval_{};
+  int fastest_direct_{0}, max_travel_time_{0};
+  uint64_t n_start_times_{0};
+};
 
 }  // namespace routing
 }  // namespace b2r

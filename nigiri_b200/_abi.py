@@ -194,6 +194,9 @@ EXPORTS = [
     "b2r_queries_count", "b2r_queries_get", "b2r_queries_destroy",
     "b2r_one_to_all_noalloc", "b2r_last_batch_scan_profile",
     "b2r_engine_get_shape", "b2r_engine_set_shape", "b2r_engine_autotune",
+    "b2r_search_prepare", "b2r_search_extend", "b2r_search_plan_free", "b2r_raptor_create",
+    "b2r_raptor_destroy", "b2r_raptor_reset_arrivals", "b2r_raptor_next_start_time",
+    "b2r_raptor_add_start", "b2r_raptor_execute", "b2r_raptor_reconstruct", "b2r_raptor_rounds",
 ]
 
 
@@ -241,6 +244,20 @@ def _declare(lib):
                                                   C.POINTER(C.c_uint32)]),
         "b2r_one_to_all_noalloc": (C.c_int, [vp, C.POINTER(Query), C.POINTER(C.c_int16), C.c_uint64,
                                              C.POINTER(C.c_uint32), C.POINTER(C.c_int32), vp]),
+        # the Algo concept (search::init's preparation and one raptor state)
+        "b2r_search_prepare": (C.c_int, [vp, C.POINTER(Query), C.POINTER(vp)]),
+        "b2r_search_extend": (C.c_int, [vp, vp, C.c_uint32, C.POINTER(C.c_uint8), C.POINTER(C.c_uint8)]),
+        "b2r_search_plan_free": (None, [vp]),
+        "b2r_raptor_create": (C.c_int, [vp, vp, C.POINTER(vp)]),
+        "b2r_raptor_destroy": (C.c_int, [vp]),
+        "b2r_raptor_reset_arrivals": (C.c_int, [vp]),
+        "b2r_raptor_next_start_time": (C.c_int, [vp]),
+        "b2r_raptor_add_start": (C.c_int, [vp, C.c_uint32, C.c_int32]),
+        "b2r_raptor_execute": (C.c_int, [vp, C.c_int32, C.c_uint8, C.c_int32, C.POINTER(Journey), C.c_uint32,
+                                         C.POINTER(C.c_uint32)]),
+        "b2r_raptor_reconstruct": (C.c_int, [vp, C.POINTER(Query), C.POINTER(Journey), C.POINTER(Leg),
+                                             C.c_uint32]),
+        "b2r_raptor_rounds": (C.c_uint64, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -2667,3 +2667,326 @@ int b2r_release(b2r_engine* e, uint64_t ticket) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------ the Algo concept
+// routing::search<Dir, Algo>'s Algo over the engine: one query's raptor
+// state in slot 0 of a 32-slot engine.  Each execute is one admission of a
+// single start-time group (the start labels added since next_start_time);
+// round times and time_at_dest carry over from the previous execute unless
+// reset_arrivals came in between, as raptor_state's do.  Results come back
+// as the slot's collected journeys; legs are rebuilt on request from the
+// round times the last execute left.
+struct b2r_search_plan_impl {
+  b2r_search_plan view{};
+  b2r::prepped_query p;  // the whole preparation (interval extension reads it)
+  std::vector<b2r_start> starts;
+  std::vector<uint32_t> dests;
+  std::vector<uint16_t> dist, lb;
+  void set_starts(std::vector<b2r::start_label> const& v) {
+    starts.clear();
+    for (auto const& s : v) starts.push_back({s.time_at_start, s.time_at_stop, s.stop});
+    view.n_starts = static_cast<uint32_t>(starts.size());
+    view.starts = starts.data();
+  }
+};
+
+struct b2r_raptor {
+  b2r_engine* e{nullptr};
+  b2r::prepped_query tmpl;              // the constructor's arguments
+  std::vector<b2r::start_label> starts;  // added since next_start_time
+  bool fresh{true};                      // reset_arrivals since the last execute
+  bool lb_sent{false};                   // the lower-bound column is on the device
+  bool executed{false};
+  b2r::dev::slot_t sl{};                 // slot 0 as the last execute left it
+  uint64_t n_rounds{0};
+  ~b2r_raptor() {
+    if (e != nullptr) b2r_engine_destroy(e);
+  }
+};
+
+namespace b2r {
+namespace {
+
+// super-steps until slot 0's phase is over; its summary
+dev::slot_summary run_slot0(b2r_engine& e) {
+  auto* st = e.stream;
+  for (uint64_t step = 0;; ++step) {
+    if (step > 100000) throw std::runtime_error("super-step cap exceeded");
+    if (e.cfg.use_graphs != 0 && e.graph != nullptr) {
+      B2R_CUDA(cudaGraphLaunch(e.graph, st));
+    } else {
+      enqueue_superstep(e, st);
+      B2R_CUDA(cudaGetLastError());
+    }
+    B2R_CUDA(cudaMemcpyAsync(e.h_summary, e.d_summary, sizeof(b2r_engine::summary_t), cudaMemcpyDeviceToHost, st));
+    B2R_CUDA(cudaStreamSynchronize(st));
+    auto const state = e.h_summary[0].state;
+    if (state == dev::S_DONE || state == dev::S_ERROR) return e.h_summary[0];
+  }
+}
+
+}  // namespace
+}  // namespace b2r
+
+extern "C" {
+
+int b2r_search_prepare(const b2r_timetable* tt, const b2r_query* q, b2r_search_plan** out) {
+  B2R_API_GUARD({
+    if (tt == nullptr || q == nullptr || out == nullptr) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
+    if (q->kind != B2R_ONE_TO_ONE || q->algorithm != B2R_ALGO_RAPTOR) {
+      return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "b2r_search_prepare: one-to-one raptor queries only");
+    }
+    b2r::prepped_query p;
+    b2r::prepare(tt->view, *q, 1, p);  // lower bounds by the reference's Dijkstra on the host
+    auto x = std::make_unique<b2r_search_plan_impl>();
+    auto& v = x->view;
+    v.status = p.status;
+    v.direction = q->direction;
+    v.ontrip = p.ontrip ? 1 : 0;
+    v.start_dest_overlap = p.empty_result ? 1 : 0;
+    v.max_transfers = q->max_transfers;
+    v.base_day = p.base_days;
+    v.interval_from = p.iv_from;
+    v.interval_to = p.iv_to;
+    v.fastest_direct = p.fastest_direct;
+    v.max_travel_time = p.max_travel_time;
+    v.tts_default = p.tts.is_default;
+    v.tts_min_transfer_time = p.tts.min_transfer_time;
+    v.tts_additional_time = p.tts.additional_time;
+    v.tts_factor = p.tts.factor;
+    x->set_starts(p.starts);
+    if (p.intermodal_dest) {
+      x->dist.assign(tt->d.n_loc, uint16_t{0xFFFFu});
+      for (auto const& [l, dd] : p.dest_dist) x->dist[l] = dd;
+      x->dests.push_back(B2R_SPECIAL_END);
+    } else {
+      x->dests = p.dest_locs;
+    }
+    x->lb = p.lb;
+    x->p = std::move(p);
+    v.n_destinations = static_cast<uint32_t>(x->dests.size());
+    v.destinations = x->dests.data();
+    v.dist_to_dest = x->dist.empty() ? nullptr : x->dist.data();
+    v.lower_bounds = x->lb.empty() ? nullptr : x->lb.data();
+    *out = &x.release()->view;
+    return B2R_OK;
+  });
+}
+
+int b2r_search_extend(const b2r_timetable* tt, b2r_search_plan* plan, uint32_t n_missing, uint8_t* changed,
+                      uint8_t* reset_arrivals) {
+  B2R_API_GUARD({
+    if (tt == nullptr || plan == nullptr || changed == nullptr || reset_arrivals == nullptr) {
+      return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
+    }
+    auto* x = reinterpret_cast<b2r_search_plan_impl*>(plan);
+    auto& p = x->p;
+    *changed = 0;
+    *reset_arrivals = 0;
+    auto nf = p.iv_from, nt = p.iv_to;
+    auto const& d = tt->host;
+    if (!b2r::extend_interval(p, d.date_range_from * 1440, d.date_range_to * 1440, n_missing, nf, nt)) {
+      return B2R_OK;
+    }
+    std::vector<b2r::start_label> starts;  // search.h:290-312
+    if (nf != p.iv_from) {
+      b2r::add_interval_starts(tt->view, p, nf, p.iv_from, !p.fwd, starts);
+      if (!p.fwd) *reset_arrivals = 1;
+    }
+    if (nt != p.iv_to) {
+      b2r::add_interval_starts(tt->view, p, p.iv_to, nt, p.fwd, starts);
+      if (p.fwd) *reset_arrivals = 1;
+    }
+    p.iv_from = nf;
+    p.iv_to = nt;
+    x->view.interval_from = nf;
+    x->view.interval_to = nt;
+    x->set_starts(starts);
+    *changed = 1;
+    return B2R_OK;
+  });
+}
+
+void b2r_search_plan_free(b2r_search_plan* p) {
+  // the view is the first member of its owner
+  delete reinterpret_cast<b2r_search_plan_impl*>(p);
+}
+
+int b2r_raptor_create(b2r_timetable* tt, const b2r_raptor_args* a, b2r_raptor** out) {
+  B2R_API_GUARD({
+    if (tt == nullptr || a == nullptr || out == nullptr) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
+    if (a->prf_idx >= B2R_N_PROFILES) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "profile index out of range");
+    if (a->n_destinations != 0 && a->destinations == nullptr) {
+      return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null destination array");
+    }
+    auto const nl = tt->d.n_loc;
+    auto r = std::make_unique<b2r_raptor>();
+    auto& p = r->tmpl;
+    p.fwd = a->direction == B2R_FORWARD;
+    p.ontrip = true;  // one start-time group per execute
+    p.allowed_claszes = a->allowed_claszes;
+    p.req_flags = static_cast<uint8_t>((a->require_bike_transport != 0 ? 1U << B2R_FLAG_BIKES : 0U) |
+                                       (a->require_car_transport != 0 ? 1U << B2R_FLAG_CARS : 0U) |
+                                       (a->prf_idx == B2R_PROFILE_WHEELCHAIR ? 1U << B2R_FLAG_WHEELCHAIR : 0U) |
+                                       (a->no_compulsory_reservation != 0 ? 1U << B2R_FLAG_RESERVATION_NOT_REQUIRED : 0U));
+    p.prf = a->prf_idx;
+    p.tts = {a->tts_default, a->tts_min_transfer_time, a->tts_additional_time, a->tts_factor};
+    p.tts_raw = p.tts;
+    p.base_days = a->base_day;
+    auto const base = a->base_day - tt->view.internal_from_days();
+    if (base < 0 || base >= B2R_MAX_DAYS) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "base day outside the timetable");
+    p.base = static_cast<uint16_t>(base);
+    p.intermodal_dest = a->dist_to_dest != nullptr;
+    if (p.intermodal_dest) {
+      for (auto l = 0U; l != nl; ++l) {
+        if (a->dist_to_dest[l] != 0xFFFFu) p.dest_dist.emplace_back(l, a->dist_to_dest[l]);
+      }
+    } else {
+      for (auto i = 0U; i != a->n_destinations; ++i) {
+        if (a->destinations[i] >= nl) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "destination out of range");
+        p.dest_locs.push_back(a->destinations[i]);
+      }
+      std::sort(p.dest_locs.begin(), p.dest_locs.end());
+      p.dest_locs.erase(std::unique(p.dest_locs.begin(), p.dest_locs.end()), p.dest_locs.end());
+    }
+    if (a->lower_bounds != nullptr) p.lb.assign(a->lower_bounds, a->lower_bounds + nl);
+    p.recon_mode = 2;  // legs on request (b2r_raptor_reconstruct)
+    p.fastest_direct = 32767;
+    p.max_travel_time = B2R_MAX_TRAVEL_TIME_MIN;
+    b2r_engine_config cfg;
+    b2r_engine_config_init(&cfg);
+    cfg.max_slots = 32;
+    cfg.use_lower_bounds = 0;  // the column comes with the arguments
+    if (auto const rc = b2r_engine_create(tt, &cfg, &r->e); rc != B2R_OK) return rc;
+    if (b2r::check_capacity(*r->e, p) != B2R_OK) {
+      return b2r::fail(B2R_ERR_CAPACITY, "b2r_raptor_create: more destinations than a slot holds");
+    }
+    *out = r.release();
+    return B2R_OK;
+  });
+}
+
+int b2r_raptor_destroy(b2r_raptor* r) {
+  delete r;
+  return B2R_OK;
+}
+
+int b2r_raptor_reset_arrivals(b2r_raptor* r) {
+  if (r == nullptr) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
+  r->fresh = true;
+  return B2R_OK;
+}
+
+int b2r_raptor_next_start_time(b2r_raptor* r) {
+  if (r == nullptr) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
+  r->starts.clear();  // best, tmp and marks: the next group's generation
+  return B2R_OK;
+}
+
+int b2r_raptor_add_start(b2r_raptor* r, uint32_t location, int32_t time) {
+  if (r == nullptr) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
+  if (location >= r->e->tt->d.n_loc) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "start location out of range");
+  if (r->starts.size() >= r->e->max_starts) return b2r::fail(B2R_ERR_CAPACITY, "too many start labels");
+  r->starts.push_back({0, time, location});
+  return B2R_OK;
+}
+
+int b2r_raptor_execute(b2r_raptor* r, int32_t start_time, uint8_t max_transfers, int32_t worst_time_at_dest,
+                       b2r_journey* results, uint32_t capacity, uint32_t* n) {
+  B2R_API_GUARD({
+    if (r == nullptr || n == nullptr || (capacity != 0 && results == nullptr)) {
+      return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
+    }
+    *n = 0;
+    auto& e = *r->e;
+    try {
+      B2R_CUDA(cudaSetDevice(e.tt->device));
+      auto p = r->tmpl;
+      for (auto const& s : r->starts) p.starts.push_back({start_time, s.time_at_stop, s.stop});
+      p.max_transfers = max_transfers;
+      p.end_k = static_cast<uint8_t>(std::min<int>(max_transfers, B2R_MAX_TRANSFERS) + 2);
+      auto const span = p.fwd ? static_cast<int64_t>(worst_time_at_dest) - start_time
+                              : static_cast<int64_t>(start_time) - worst_time_at_dest;
+      p.span = static_cast<int16_t>(std::clamp<int64_t>(span, -32768, 32767));
+      p.iv_from = p.iv_to = start_time;
+      p.need_sweep = !r->fresh;  // round times of earlier executes stay in effect
+      p.keep_lb = r->lb_sent;
+      uint32_t const flags = r->fresh ? 0U : b2r::kAdmKeepRt;
+      b2r::admit(e, {{0U, &p, flags}}, e.stream);
+      auto const sum = b2r::run_slot0(e);
+      std::vector<b2r::exported> ex;
+      b2r::export_slots(e, {0U}, {sum.n_journeys}, {0U}, ex, e.stream2);
+      r->sl = ex[0].sl;
+      r->fresh = false;
+      r->lb_sent = r->lb_sent || !p.lb.empty();
+      r->executed = true;
+      r->n_rounds = r->sl.n_rounds;
+      if (r->sl.state == b2r::dev::S_ERROR) {
+        return b2r::fail(r->sl.error != 0 ? r->sl.error : B2R_ERR_INTERNAL, "execute failed on the device");
+      }
+      *n = static_cast<uint32_t>(ex[0].js.size());
+      if (ex[0].js.size() > capacity) return b2r::fail(B2R_ERR_CAPACITY, "result capacity exceeded");
+      for (auto i = 0U; i != ex[0].js.size(); ++i) {
+        auto const& j = ex[0].js[i];
+        results[i] = b2r_journey{j.start_time, j.dest_time, j.dest, j.transfers, 0, 0, 0};
+      }
+      return B2R_OK;
+    } catch (b2r::cuda_error const& ex) {
+      return b2r::fail(B2R_ERR_CUDA, ex.what());
+    }
+  });
+}
+
+int b2r_raptor_reconstruct(b2r_raptor* r, const b2r_query* q, b2r_journey* j, b2r_leg* legs, uint32_t capacity) {
+  B2R_API_GUARD({
+    if (r == nullptr || q == nullptr || j == nullptr || legs == nullptr) {
+      return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
+    }
+    if (!r->executed) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "b2r_raptor_reconstruct before execute");
+    if (capacity < static_cast<uint32_t>(b2r::dev::kMaxLegs)) {
+      return b2r::fail(B2R_ERR_CAPACITY, "leg capacity below the longest journey (40 legs)");
+    }
+    auto& e = *r->e;
+    // the query's offsets in query::sanitize's order (query.cc:59-67)
+    std::vector<b2r_offset> so(q->start, q->start + (q->start != nullptr ? q->n_start : 0U));
+    std::vector<b2r_offset> dz(q->destination, q->destination + (q->destination != nullptr ? q->n_destination : 0U));
+    auto const by_dur = [](b2r_offset const& a, b2r_offset const& b) { return a.duration < b.duration; };
+    std::sort(so.begin(), so.end(), by_dur);
+    std::sort(dz.begin(), dz.end(), by_dur);
+    if (so.size() + dz.size() > e.max_off) return b2r::fail(B2R_ERR_CAPACITY, "too many offsets");
+    try {
+      B2R_CUDA(cudaSetDevice(e.tt->device));
+      auto sl = r->sl;
+      sl.start_mode = q->start_match_mode;
+      sl.dest_mode = q->dest_match_mode;
+      sl.ontrip = q->is_interval == 0 ? 1 : 0;
+      sl.soff_off = 0;
+      sl.n_soff = static_cast<uint32_t>(so.size());
+      sl.doff_off = sl.n_soff;
+      sl.n_doff = static_cast<uint32_t>(dz.size());
+      so.insert(so.end(), dz.begin(), dz.end());
+      b2r::dev::journey_rec jr{j->start_time, j->dest_time, j->dest, j->transfers, 0, 0, 0, 0, 0};
+      auto* s = e.stream;
+      if (!so.empty()) {
+        B2R_CUDA(cudaMemcpyAsync(e.st.off_pool, so.data(), so.size() * sizeof(b2r_offset), cudaMemcpyHostToDevice, s));
+      }
+      B2R_CUDA(cudaMemcpyAsync(e.st.slots, &sl, sizeof(sl), cudaMemcpyHostToDevice, s));
+      B2R_CUDA(cudaMemcpyAsync(e.st.journeys, &jr, sizeof(jr), cudaMemcpyHostToDevice, s));
+      b2r::dev::k_reconstruct_one<<<1, 32, 0, s>>>(e.st, 0U, 0U);
+      B2R_CUDA(cudaGetLastError());
+      B2R_CUDA(cudaMemcpyAsync(&jr, e.st.journeys, sizeof(jr), cudaMemcpyDeviceToHost, s));
+      B2R_CUDA(cudaMemcpyAsync(legs, e.st.legs, b2r::dev::kMaxLegs * sizeof(b2r_leg), cudaMemcpyDeviceToHost, s));
+      B2R_CUDA(cudaStreamSynchronize(s));
+      j->error = jr.error;
+      j->n_legs = jr.error != 0 ? 0 : jr.n_legs;
+      j->first_leg = 0;
+      return B2R_OK;
+    } catch (b2r::cuda_error const& ex) {
+      return b2r::fail(B2R_ERR_CUDA, ex.what());
+    }
+  });
+}
+
+uint64_t b2r_raptor_rounds(const b2r_raptor* r) { return r == nullptr ? 0 : r->n_rounds; }
+
+}  // extern "C"

@@ -988,6 +988,12 @@ __global__ void k_reconstruct(state st) {
   }
 }
 
+// One given journey of slot s (index ji), one warp: the Algo interface's
+// reconstruct.
+__global__ void k_reconstruct_one(state st, uint32_t s, uint32_t ji) {
+  reconstruct_one(st, s, ji, threadIdx.x & 31u);
+}
+
 // The journeys of finished slots whose reconstruction was deferred, listed
 // by the host as (slot << 16 | journey index): launched on the export stream
 // while the next super-steps run.  A finished slot is left alone by the

@@ -4,7 +4,9 @@
 // infrastructure), and the complete journeys (every leg) must be equal.
 // Range queries also run through pong_search (walking allowed at the
 // start, as at the destination), and the first queries again in the
-// wheelchair profile.  One-to-all searches compare the round
+// wheelchair profile.  The first one-to-one and range queries of each
+// direction also run through search<Dir, Algo> (nigiri's driver restated
+// in b2r.hpp) with the engine's Algo, b2r_algo.  One-to-all searches compare the round
 // times of every location.
 //
 //   raptor_search_test            exit 0 when every query matches
@@ -19,38 +21,7 @@ namespace r = b2r::routing;
 
 namespace {
 
-r::query from_c(b2r_query const& c) {  // the generator's queries in nigiri's terms
-  r::query q;
-  if (c.is_interval) q.start_time_ = r::interval{c.interval_from, c.interval_to};
-  else q.start_time_ = c.start_time;
-  q.start_match_mode_ = static_cast<r::location_match_mode>(c.start_match_mode);
-  q.dest_match_mode_ = static_cast<r::location_match_mode>(c.dest_match_mode);
-  q.use_start_footpaths_ = c.use_start_footpaths != 0;
-  for (auto i = 0U; i != c.n_start; ++i) {
-    q.start_.push_back({c.start[i].target, c.start[i].duration, c.start[i].transport_mode_id});
-  }
-  for (auto i = 0U; i != c.n_destination; ++i) {
-    q.destination_.push_back({c.destination[i].target, c.destination[i].duration,
-                              c.destination[i].transport_mode_id});
-  }
-  q.max_start_offset_ = c.max_start_offset;
-  q.max_transfers_ = c.max_transfers;
-  q.max_travel_time_ = c.max_travel_time;
-  q.min_connection_count_ = c.min_connection_count;
-  q.extend_interval_earlier_ = c.extend_interval_earlier != 0;
-  q.extend_interval_later_ = c.extend_interval_later != 0;
-  if (c.has_fastest_direct) q.fastest_direct_ = c.fastest_direct;
-  q.fastest_direct_factor_ = c.fastest_direct_factor;
-  q.transfer_time_settings_ = {c.tts_default != 0, c.tts_min_transfer_time, c.tts_additional_time,
-                               c.tts_factor};
-  q.allowed_claszes_ = static_cast<uint16_t>(c.allowed_claszes);
-  q.require_bike_transport_ = c.require_bike_transport != 0;
-  q.require_car_transport_ = c.require_car_transport != 0;
-  q.no_compulsory_reservation_ = c.no_compulsory_reservation != 0;
-  q.prf_idx_ = c.prf_idx;
-  if (c.has_max_interval != 0) q.max_interval_ = r::interval{c.max_interval_from, c.max_interval_to};
-  return q;
-}
+r::query from_c(b2r_query const& c) { return r::query_of(c); }
 
 void print(char const* who, std::vector<r::journey> const& js) {
   std::printf("  %s: %zu journeys\n", who, js.size());
@@ -80,7 +51,8 @@ std::vector<r::journey> oracle_journeys(b2r_timetable_desc const& d, b2r_query c
   return out;
 }
 
-int run_workload(uint32_t workload, uint32_t timetable_seed, uint32_t n, uint64_t query_seed) {
+int run_workload(uint32_t workload, uint32_t timetable_seed, uint32_t n, uint64_t query_seed,
+                 uint32_t algo_queries) {
   b2r_host_timetable* h = nullptr;
   b2r::check(b2r_tt_generate(workload, timetable_seed, &h), "b2r_tt_generate");
   b2r_timetable_desc d{};
@@ -92,7 +64,7 @@ int run_workload(uint32_t workload, uint32_t timetable_seed, uint32_t n, uint64_
   b2r::timetable tt{d};
   b2r::engine eng{tt};
   int bad = 0;
-  size_t n_journeys = 0;
+  size_t n_journeys = 0, n_algo = 0;
   for (auto dir : {r::direction::kForward, r::direction::kBackward}) {
     std::vector<r::query> batch;
     std::vector<b2r_query const*> cq;
@@ -113,6 +85,24 @@ int run_workload(uint32_t workload, uint32_t timetable_seed, uint32_t n, uint64_
                     dir == r::direction::kForward ? "forward" : "backward");
         print("engine", got[i].journeys_);
         print("oracle", want);
+      }
+      // the same query through search<Dir, Algo> with the engine's Algo
+      // (nigiri's own driver loop over reset_arrivals .. reconstruct)
+      if (i < algo_queries) {
+        r::b2r_algo_state state;
+        auto const via_algo =
+            dir == r::direction::kForward
+                ? r::search<r::direction::kForward, r::b2r_algo<r::direction::kForward>>{tt, state, batch[i]}.execute()
+                : r::search<r::direction::kBackward, r::b2r_algo<r::direction::kBackward>>{tt, state, batch[i]}
+                      .execute();
+        ++n_algo;
+        if (via_algo.status_ != B2R_OK || via_algo.journeys_ != want) {
+          ++bad;
+          std::printf("workload %u query %u (%s) differs through search<Dir, b2r_algo>\n", workload, i,
+                      dir == r::direction::kForward ? "forward" : "backward");
+          print("search<Dir, b2r_algo>", via_algo.journeys_);
+          print("oracle", want);
+        }
       }
     }
     // pong_search on the range queries
@@ -186,7 +176,8 @@ int run_workload(uint32_t workload, uint32_t timetable_seed, uint32_t n, uint64_
       std::printf("workload %u one_to_all %u differs\n", workload, i);
     }
   }
-  std::printf("workload %u: %u queries, %zu journeys, %d differ\n", workload, n_q, n_journeys, bad);
+  std::printf("workload %u: %u queries (%zu also through search<Dir, b2r_algo>), %zu journeys, %d differ\n",
+              workload, n_q, n_algo, n_journeys, bad);
   b2r_queries_destroy(qs);
   b2r_tt_destroy(h);
   return bad;
@@ -196,8 +187,8 @@ int run_workload(uint32_t workload, uint32_t timetable_seed, uint32_t n, uint64_
 
 int main() {
   try {
-    auto bad = run_workload(1, 1, 200, 4711);  // city, forward one-to-one
-    bad += run_workload(3, 2, 48, 4712);        // regional, range, both directions
+    auto bad = run_workload(1, 1, 200, 4711, 60);  // city, forward one-to-one
+    bad += run_workload(3, 2, 48, 4712, 12);        // regional, range, both directions
     std::printf(bad == 0 ? "ok\n" : "FAILED\n");
     return bad == 0 ? 0 : 1;
   } catch (b2r::error const& e) {
