@@ -284,7 +284,7 @@ def gpu_arm(args, rank, world, local):
         extras["checked_against_cpu"]["sample"] = (
             f"every query of timed step 0 ({B}) and every 100th of the other {args.steps - 1} steps")
     if rank == 0 and not args.no_extras:
-        extras = extras_legs(args, h, dtt, qs, B, local)
+        extras.update(extras_legs(args, h, dtt, qs, B, local))
         extras["served"] = served_leg(eng, qs, [5000.0, 15000.0, 25000.0, None], 4096)
         extras["range"] = range_leg(eng, h, 1024, seed=1003)
         del eng
