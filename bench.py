@@ -137,8 +137,9 @@ def measured_peak():
 
 
 def ncu_traffic_per_unit():
-    """DRAM bytes per scanned (route, query) stop step of the route scan
-    from the committed ncu capture (profiles/route_scan_traffic.json)."""
+    """The route scan's DRAM bytes per launch from the committed ncu capture
+    of the bench's batch and launch shape (profiles/route_scan_traffic.json),
+    with a few counters of the same kernel's detailed capture."""
     try:
         with open(os.path.join(ROOT, "profiles", "route_scan_traffic.json")) as f:
             return json.load(f)
@@ -284,7 +285,7 @@ def gpu_arm(args, rank, world, local):
         extras["checked_against_cpu"]["sample"] = (
             f"every query of timed step 0 ({B}) and every 100th of the other {args.steps - 1} steps")
     if rank == 0 and not args.no_extras:
-        extras.update(extras_legs(args, h, dtt, qs, B, local))
+        extras.update(extras_legs(args, h, dtt, qs, B, local, shape))
         extras["served"] = served_leg(eng, qs, [5000.0, 15000.0, 25000.0, None], 4096)
         extras["range"] = range_leg(eng, h, 1024, seed=1003)
         del eng
@@ -614,7 +615,7 @@ def national_leg(local):
     return out
 
 
-def extras_legs(args, h, dtt, qs, B, local):
+def extras_legs(args, h, dtt, qs, B, local, shape):
     """Plain one-query-per-launch baseline, route-scan roofline and the CPU
     baseline (rank 0, outside the timed region)."""
     import torch
@@ -639,30 +640,42 @@ def extras_legs(args, h, dtt, qs, B, local):
                         "p50_ms": percentile(lat, 0.5), "p99_ms": percentile(lat, 0.99),
                         "queries": n_plain}
     del plain
-    # roofline of the route scan: CUDA events around every launch
-    prof = R.Engine(dtt, max_slots=B, profile=True)
+    # roofline of the route scan: the algorithmic bytes come from a counting
+    # build (profile = 1), the launch times from CUDA events around every
+    # launch of the build the bench runs (profile = 2, the tuned shape); both
+    # run the step-0 batch without graphs
+    sh = A.LaunchShape()
+    for f, v in shape.items():
+        setattr(sh, f, v)
     arr = qs.subset(range(B))
     o = (A.Result * B)()
-    if lib.b2r_search_batch(prof.handle, arr, B, o) != 0:
-        raise RuntimeError(lib.b2r_last_error().decode())
-    st = prof.stats()
+    runs = {}
+    for mode in (1, 2):
+        prof = R.Engine(dtt, max_slots=B, profile=mode)
+        prof.shape = sh
+        if lib.b2r_search_batch(prof.handle, arr, B, o) != 0:
+            raise RuntimeError(lib.b2r_last_error().decode())
+        runs[mode] = prof.stats()
+        del prof
+    st, tm = runs[1], runs[2]
     per_launch_bytes = st.route_scan_bytes / max(1, st.route_scan_launches)
-    per_launch_s = st.route_scan_ms / 1e3 / max(1, st.route_scan_launches)
-    traffic = None
-    t = ncu_traffic_per_unit()
-    if t is not None and st.route_stop_visits:
-        traffic = t["dram_bytes_per_stop_visit"] * st.route_stop_visits / max(1, st.route_scan_launches)
+    per_launch_s = tm.route_scan_ms / 1e3 / max(1, tm.route_scan_launches)
+    traffic, cap = None, ncu_traffic_per_unit()
+    if cap is not None and cap.get("batch") == B and cap.get("shape") == [getattr(sh, f) for f, _ in
+                                                                          A.LaunchShape._fields_]:
+        traffic = cap["dram_bytes_per_launch"]
     out["roofline"] = {
         "bound": "hbm", "achieved": per_launch_bytes / per_launch_s / 1e9, "peak": None,
         "unit": "GB/s", "frac": None, "traffic": traffic,
-        "kernel": "k_route_scan", "launches": st.route_scan_launches,
+        "traffic_source": None if traffic is None else cap.get("command"),
+        "limiter": "latency of dependent L2/DRAM loads (ncu: issue active, long-scoreboard stalls)",
+        "kernel": "k_route_scan", "launches": tm.route_scan_launches,
         "avg_launch_ms": per_launch_s * 1e3, "algorithmic_bytes_per_launch": per_launch_bytes,
         "route_stop_visits": st.route_stop_visits,
         "lane_utilisation": st.route_stop_visits / max(1, 32 * st.route_warp_steps),
-        "route_scan_share_of_device_time":
-            st.route_scan_ms / max(1e-9, st.device_ms),
+        "route_scan_share_of_device_time": tm.route_scan_ms / max(1e-9, tm.device_ms),
+        "ncu": None if cap is None else cap.get("ncu"),
     }
-    del prof
     # CPU baseline: the oracle on a bounded sample, all host threads
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     threads = host_threads()

@@ -342,7 +342,9 @@ typedef struct b2r_engine_config {
   uint32_t max_starts;      /* start labels per query (default 4096) */
   uint32_t steps_per_sync;  /* super-steps between host checks (default 4) */
   uint32_t profile;         /* 1 = time route scans with CUDA events and
-                               count their work (disables graphs) */
+                               count their work (a counting build of the
+                               scan), 2 = time them only (the build the
+                               launch shape selects); both disable graphs */
   uint32_t reserved[4];
 } b2r_engine_config;
 
@@ -577,10 +579,10 @@ typedef struct b2r_launch_shape {
   uint32_t pair_blocks_per_sm;  /* route marking, transfers, footpaths (8) */
   uint32_t recon_blocks_per_sm; /* reconstruction, 128-thread blocks (4) */
   uint32_t steps_per_sync;      /* super-steps between host checks (4) */
-  uint32_t scan_occupancy;      /* route scan build: 0 = 64 registers per
-                                   thread (up to 32 resident warps per SM),
-                                   1 = 40 (up to 48 warps, some values kept
-                                   in local memory) (0) */
+  uint32_t scan_occupancy;      /* route scan build: 4, 5 or 6 resident
+                                   blocks of 256 threads per SM (0, 1, 2;
+                                   fewer registers per thread, the last two
+                                   keep a few values in local memory) (0) */
 } b2r_launch_shape;
 int b2r_engine_get_shape(const b2r_engine* e, b2r_launch_shape* out);
 /* Rejects values out of range; re-captures the super-step graph. */

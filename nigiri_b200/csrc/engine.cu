@@ -508,10 +508,18 @@ void enqueue_superstep(b2r_engine& e, cudaStream_t s) {
     ev_b = e.prof_ev[e.prof_used++];
     B2R_CUDA(cudaEventRecord(ev_a, s));
   }
-  if (e.shape.scan_occupancy != 0U) {
-    dev::k_route_scan<6><<<e.sms * e.shape.scan_blocks_per_sm, e.shape.scan_threads, 0, s>>>(st);
-  } else {
-    dev::k_route_scan<4><<<e.sms * e.shape.scan_blocks_per_sm, e.shape.scan_threads, 0, s>>>(st);
+  dev::k_route_scan_seq<<<list_blocks, 256, 0, s>>>(st);
+  {
+    auto const grid = e.sms * e.shape.scan_blocks_per_sm, block = e.shape.scan_threads;
+    if (e.cfg.profile == 1U) {
+      dev::k_route_scan<4, true><<<grid, block, 0, s>>>(st);
+    } else if (e.shape.scan_occupancy == 2U) {
+      dev::k_route_scan<6, false><<<grid, block, 0, s>>>(st);
+    } else if (e.shape.scan_occupancy == 1U) {
+      dev::k_route_scan<5, false><<<grid, block, 0, s>>>(st);
+    } else {
+      dev::k_route_scan<4, false><<<grid, block, 0, s>>>(st);
+    }
   }
   if (e.cfg.profile) {
     B2R_CUDA(cudaEventRecord(ev_b, s));
@@ -541,7 +549,7 @@ void enqueue_superstep(b2r_engine& e, cudaStream_t s) {
   dev::k_next_summary<<<slot_blocks, 128, 0, s>>>(st);
   dev::k_list_marked<<<e.sms * 8, 256, 0, s>>>(st);
 }
-constexpr uint64_t kLaunchesPerStep = 17;
+constexpr uint64_t kLaunchesPerStep = 18;
 
 // --------------------------------------------------------- admission
 size_t admission_bytes(b2r_engine const& e, prepped_query const& p) {
@@ -2258,7 +2266,7 @@ int b2r_engine_create(b2r_timetable* tt, const b2r_engine_config* cfg_in, b2r_en
       B2R_CUDA(cudaMemset(st.F[0], 0, static_cast<size_t>(nl) * G * 4));
       B2R_CUDA(cudaMemset(st.F[1], 0, static_cast<size_t>(nl) * G * 4));
       B2R_CUDA(cudaMemset(st.lb_mask, 0, G * 4));
-      st.profile = cfg.profile ? 1u : 0u;
+      st.profile = cfg.profile == 1U ? 1u : 0u;  // device work counters
       B2R_CUDA(cudaMemset(st.prof, 0, 8 * sizeof(unsigned long long)));
       al(e->d_exp_list, S);
       al(e->d_keep, e->max_j);
@@ -2438,11 +2446,11 @@ int b2r_engine_set_shape(b2r_engine* e, const b2r_launch_shape* sh) {
                     sh->scan_threads >= 32 && sh->scan_threads <= 256 && sh->scan_threads % 32 == 0 &&
                     sh->pair_blocks_per_sm >= 1 && sh->pair_blocks_per_sm <= 64 &&
                     sh->recon_blocks_per_sm >= 1 && sh->recon_blocks_per_sm <= 64 &&
-                    sh->steps_per_sync >= 1 && sh->steps_per_sync <= 64 && sh->scan_occupancy <= 1;
+                    sh->steps_per_sync >= 1 && sh->steps_per_sync <= 64 && sh->scan_occupancy <= 2;
     if (!ok) {
       return b2r::fail(B2R_ERR_INVALID_ARGUMENT,
                        "launch shape out of range (blocks per SM 1..64, scan threads 32..256 in steps "
-                       "of 32, steps per sync 1..64, scan occupancy 0..1)");
+                       "of 32, steps per sync 1..64, scan occupancy 0..2)");
     }
     try {
       B2R_CUDA(cudaSetDevice(e->tt->device));
@@ -2494,7 +2502,7 @@ int b2r_engine_autotune(b2r_engine* e, const b2r_query* sample, uint32_t n, b2r_
                                        {&b2r_launch_shape::pair_blocks_per_sm, {2, 4, 8, 16}},
                                        {&b2r_launch_shape::recon_blocks_per_sm, {1, 2, 4, 8}},
                                        {&b2r_launch_shape::steps_per_sync, {1, 2, 4, 8}},
-                                       {&b2r_launch_shape::scan_occupancy, {0, 1}}};
+                                       {&b2r_launch_shape::scan_occupancy, {0, 1, 2}}};
       for (auto pass = 0; pass != 3; ++pass) {
         auto changed = false;
         for (auto const& k : knobs) {
@@ -2530,7 +2538,7 @@ int b2r_last_batch_scan_profile(const b2r_engine* e, double* scan_ms, uint64_t* 
                                 uint64_t* stop_visits, uint32_t cap, uint32_t* n) {
   B2R_API_GUARD({
     if (e == nullptr || n == nullptr) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
-    if (!e->cfg.profile) return b2r::fail(B2R_ERR_UNSUPPORTED, "engine was not created with profile = 1");
+    if (!e->cfg.profile) return b2r::fail(B2R_ERR_UNSUPPORTED, "engine was not created with profile = 1 or 2");
     auto const launches = static_cast<uint32_t>(std::min<size_t>(e->prof_used / 2, b2r_engine::kProfRows));
     *n = launches;
     auto const m = std::min(cap, launches);

@@ -307,9 +307,9 @@ __global__ void k_ctl_marked(state st) {
 //   stop compares them, so a warp prefix-minimum over the lanes gives the
 //   trip each stop is reached by;
 // * every stop then reads its arrival event of that trip.
-// The result equals the sequential walk's; routes without that order,
-// queries with per-section filters and a boarding without a current best
-// label (which the round structure rules out) take the sequential walk.
+// The result equals the sequential walk's; routes without that order and
+// queries with per-section filters take the sequential walk
+// (k_route_scan_seq).
 // Labels are combined with atomicMin and marks with atomicOr, so the order
 // of the pairs does not matter.
 
@@ -327,13 +327,14 @@ __device__ __forceinline__ uint32_t scan_stop_word(dtt const& T, uint32_t sb, ui
 }
 
 // the arrival-side label update of one stop (raptor.h:1242-1302)
+template <bool Prof>
 __device__ __forceinline__ void scan_arrive(state const& st, lane_t const& ln, uint32_t s, uint32_t g, uint32_t bit,
                                             uint32_t l, uint16_t lbv, int by, scan_ctr& pc) {
   if (by <= ln.tad_k && lbv != 0xFFFFu && by + static_cast<int>(lbv) <= ln.tad_k &&
       (ln.blast == 0u || within_bounds(st, s, ln.blast, ln.k, l, by))) {
     auto const word = enc(ln.gtag, by);
     auto* tp = &st.tmp[li(st, l, s)];
-    if (st.profile) {
+    if constexpr (Prof) {
       if (word < atomicMin(tp, word)) ++pc.writes;
     } else {
       atomicMin(tp, word);  // result unused: no round trip
@@ -342,11 +343,9 @@ __device__ __forceinline__ void scan_arrive(state const& st, lane_t const& ln, u
   }
 }
 
-// The reference's sequential walk of one (route, query) pair from position
-// i0 on, entering with the current trip (et_valid, et_off, et_day).
-__device__ __noinline__ void scan_walk_seq(state const& st, lane_t const ln, uint32_t r, uint32_t g, uint32_t b,
-                                           uint32_t sec, uint32_t i0, bool et_valid, uint32_t et_off,
-                                           uint16_t et_day, scan_ctr& pc) {
+// The reference's sequential walk of one (route, query) pair.
+__device__ __forceinline__ void scan_walk_seq(state const& st, lane_t const& ln, uint32_t r, uint32_t g,
+                                              uint32_t b, uint32_t sec, scan_ctr& pc) {
   auto const& T = st.tt;
   auto const s = g * 32u + b;
   auto const bit = 1u << b;
@@ -357,7 +356,10 @@ __device__ __noinline__ void scan_walk_seq(state const& st, lane_t const ln, uin
   auto const n_t = T.route_tr_to[r] - T.route_tr_from[r];
   auto const* colbase = T.st + T.route_st_from[r];
   auto const lb_off = (ln.mode & 8u) != 0u;
-  for (auto i = i0; i < n; ++i) {
+  bool et_valid = false;
+  uint32_t et_off = 0;
+  uint16_t et_day = 0;
+  for (auto i = 0u; i < n; ++i) {
     ++pc.stops;
     ++pc.warp_steps;
     auto const stp = scan_stop_word(T, sb, n, fwd, i, sec);
@@ -373,7 +375,7 @@ __device__ __noinline__ void scan_walk_seq(state const& st, lane_t const ln, uin
     if (et_valid && can_finish) {
       arrival_ran = true;
       auto const ev = colbase[n_t * (si * 2u - (fwd ? 1u : 0u)) + et_off];
-      scan_arrive(st, ln, s, g, bit, l, lbv, to_delta_key(fwd, et_day, ln.base, delta_count(ev)), pc);
+      scan_arrive<true>(st, ln, s, g, bit, l, lbv, to_delta_key(fwd, et_day, ln.base, delta_count(ev)), pc);
     }
     if (i + 1u == n || !can_start || !(st.X[l * st.G + g] & bit)) continue;
     if (lbv == 0xFFFFu) break;  // raptor.h:1309-1311: no later stop of this query
@@ -401,19 +403,57 @@ __device__ __noinline__ void scan_walk_seq(state const& st, lane_t const ln, uin
   }
 }
 
-// One (route, query) pair, the warp's lanes over its stops.
+// The filters of a (route, query) pair: false if the route is filtered
+// out; sec receives the flags checked per section (bits 0-3) and bit 8 for
+// the wheelchair profile's stop bits.
+__device__ __forceinline__ bool scan_filters(dtt const& T, lane_t const& ln, uint32_t r, uint32_t& sec) {
+  sec = 0u;
+  if ((ln.claszes != 0xFFFFu || ln.req != 0u) && !route_allowed(T, r, ln.claszes, ln.req, sec)) return false;
+  if ((ln.mode & 0x70u) == (B2R_PROFILE_WHEELCHAIR << 4)) sec |= 0x100u;
+  return true;
+}
+
+// The pairs the parallel scan leaves to the sequential walk: routes without
+// one trip order at every event, queries with per-section filters.  A
+// thread per marked (route, group) entry, before k_route_scan (which clears
+// the route marks).
+__global__ void __launch_bounds__(256) k_route_scan_seq(const __grid_constant__ state st) {
+  auto const& T = st.tt;
+  auto const nr = st.counters[C_R];
+  scan_ctr pc{0u, 0u, 0u, 0u, 0u};
+  for (auto w = blockIdx.x * blockDim.x + threadIdx.x; w < nr; w += gridDim.x * blockDim.x) {
+    auto const e = st.rlist[w];
+    auto const g = e % st.G, r = e / st.G;
+    auto const fifo = __ldg(T.route_fifo + r) != 0u;
+    for (auto mask = st.R[e]; mask != 0u; mask &= mask - 1u) {
+      auto const b = static_cast<uint32_t>(__ffs(mask) - 1);
+      auto const ln = st.lanes[g * 32u + b];
+      uint32_t sec = 0u;
+      if (!ln.run || !scan_filters(T, ln, r, sec)) continue;
+      if ((sec & 15u) == 0u && fifo) continue;  // k_route_scan's
+      scan_walk_seq(st, ln, r, g, b, sec, pc);
+    }
+  }
+  if (st.profile && (pc.stops | pc.ev | pc.days | pc.writes) != 0u) {
+    atomicAdd(&st.prof[0], static_cast<unsigned long long>(pc.stops));
+    atomicAdd(&st.prof[1], static_cast<unsigned long long>(pc.ev));
+    atomicAdd(&st.prof[2], static_cast<unsigned long long>(pc.days));
+    atomicAdd(&st.prof[3], static_cast<unsigned long long>(pc.writes));
+    atomicAdd(&st.prof[5], static_cast<unsigned long long>(pc.warp_steps));
+  }
+}
+
+// One (route, query) pair, the warp's lanes over its stops.  Prof: count
+// the work for the roofline (profiling engines only).
+template <bool Prof>
 __device__ __forceinline__ void scan_pair(state const& st, lane_t const& ln, uint32_t r, uint32_t g, uint32_t b,
                                           uint32_t lane, scan_ctr& pc) {
   auto const& T = st.tt;
   auto const s = g * 32u + b;
-  uint32_t sec = 0u;  // required flags checked per section (bits 0-3); bit 8: wheelchair profile
-  if ((ln.claszes != 0xFFFFu || ln.req != 0u) && !route_allowed(T, r, ln.claszes, ln.req, sec)) return;
-  if ((ln.mode & 0x70u) == (B2R_PROFILE_WHEELCHAIR << 4)) sec |= 0x100u;
+  uint32_t sec = 0u;
+  if (!scan_filters(T, ln, r, sec)) return;
   auto const order = static_cast<uint32_t>(__ldg(T.route_fifo + r));
-  if ((sec & 15u) != 0u || order == 0u) {
-    if (lane == 0u) scan_walk_seq(st, ln, r, g, b, sec, 0u, false, 0u, 0u, pc);
-    return;
-  }
+  if ((sec & 15u) != 0u || order == 0u) return;  // k_route_scan_seq's
   auto const bit = 1u << b;
   auto const fwd = ln.fwd != 0;
   auto const k = static_cast<uint32_t>(ln.k);
@@ -439,13 +479,11 @@ __device__ __forceinline__ void scan_pair(state const& st, lane_t const& ln, uin
     uint32_t stp = 0, l = 0;
     bool marked = false;
     uint16_t lbv = 0;
-    uint32_t prw = 0xFFFFFFFFu;  // previous round's label, loaded beside the mark
     if (act) {
       stp = scan_stop_word(T, sb, n, fwd, i, sec);
       l = B2R_STOP_LOC(stp);
       marked = (st.X[l * st.G + g] & bit) != 0u;
       if (!lb_off) lbv = st.lb[li(st, l, s)];
-      if (i + 1u != n && (fwd ? B2R_STOP_IN(stp) : B2R_STOP_OUT(stp)) != 0u) prw = st.rt[rti(st, k - 1u, l, s)];
     }
     auto const can_finish = act && (fwd ? B2R_STOP_OUT(stp) : B2R_STOP_IN(stp)) != 0u;
     auto const boardable = act && i + 1u != n && (fwd ? B2R_STOP_IN(stp) : B2R_STOP_OUT(stp)) != 0u && marked;
@@ -459,11 +497,17 @@ __device__ __forceinline__ void scan_pair(state const& st, lane_t const& ln, uin
     uint16_t nd = 0;
     uint32_t key = 0;
     if (boardable && lane < fb) {
-      auto const prt = dec(prw, ln.qtag);
+      auto const prt = dec(st.rt[rti(st, k - 1u, l, s)], ln.qtag);
       if (prt != kKeyInv) {
         auto const minutes = static_cast<int>(ln.base) * 1440 + from_key(fwd, prt);
-        if (et_search(T, fwd, r, si, static_cast<uint16_t>(minutes / 1440), minutes % 1440, static_cast<int>(lbv),
-                      ln.tad_k, ln.base, nt, nd, pc.ev, pc.days)) {
+        uint32_t n_ev = 0, n_days = 0;
+        auto const found = et_search(T, fwd, r, si, static_cast<uint16_t>(minutes / 1440), minutes % 1440,
+                                     static_cast<int>(lbv), ln.tad_k, ln.base, nt, nd, n_ev, n_days);
+        if constexpr (Prof) {
+          pc.ev += n_ev;
+          pc.days += n_days;
+        }
+        if (found) {
           cand = true;
           cb_bad = dec(st.best[li(st, l, s)], ln.gtag) == kKeyInv && dec(st.tmp[li(st, l, s)], ln.gtag) == kKeyInv;
           if ((order & 2u) != 0u) {
@@ -476,13 +520,15 @@ __device__ __forceinline__ void scan_pair(state const& st, lane_t const& ln, uin
         }
       }
     }
-    if (__ballot_sync(kFull, cb_bad) != 0u) {  // the boarding rule then depends on the walk's order
-      if (lane == 0u) scan_walk_seq(st, ln, r, g, b, sec, i0, c_valid, c_off, c_day, pc);
-      return;
-    }
-    if (lane == 0u) {
-      pc.stops += min(n - i0, min(fb + 1u, 32u));
-      ++pc.warp_steps;
+    // a marked station always carries a best label of its start time
+    // (marks come with best updates), so the boarding rule never meets an
+    // invalid current_best; were it to, the query is failed loudly
+    if (cb_bad) atomicOr(&st.counters[C_ERR], 4u);
+    if constexpr (Prof) {
+      if (lane == 0u) {
+        pc.stops += min(n - i0, min(fb + 1u, 32u));
+        ++pc.warp_steps;
+      }
     }
     // prefix minimum of (key, later stop first) over the lanes: the key's
     // 21 bits above 5 for the lane
@@ -504,7 +550,7 @@ __device__ __forceinline__ void scan_pair(state const& st, lane_t const& ln, uin
       auto const et_off = use_x ? x_off : c_off;
       auto const et_day = use_x ? x_day : c_day;
       auto const ev = __ldg(colbase + n_t * (si * 2u - (fwd ? 1u : 0u)) + et_off);
-      scan_arrive(st, ln, s, g, bit, l, lbv, to_delta_key(fwd, et_day, ln.base, delta_count(ev)), pc);
+      scan_arrive<Prof>(st, ln, s, g, bit, l, lbv, to_delta_key(fwd, et_day, ln.base, delta_count(ev)), pc);
     }
     if (fb != 32u) return;
     if (tot != 0xFFFFFFFFu) {
@@ -523,9 +569,10 @@ __device__ __forceinline__ void scan_pair(state const& st, lane_t const& ln, uin
 }
 
 // A warp per marked (route, group of 32 queries) entry, one pair of the
-// entry after the other.  Two builds, with four or six blocks of 256
-// threads resident per SM (64 or 40 registers; the launch shape picks one).
-template <int MinBlocks>
+// entry after the other.  Builds with four, five or six blocks of 256
+// threads resident per SM (the launch shape picks one), and with work
+// counters for profiling engines.
+template <int MinBlocks, bool Prof>
 __global__ void __launch_bounds__(256, MinBlocks) k_route_scan(const __grid_constant__ state st) {
   auto const lane = threadIdx.x & 31u;
   auto const warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -543,11 +590,11 @@ __global__ void __launch_bounds__(256, MinBlocks) k_route_scan(const __grid_cons
       mask &= mask - 1u;
       auto const ln = st.lanes[g * 32u + b];
       if (!ln.run) continue;
-      scan_pair(st, ln, r, g, b, lane, pc);
+      scan_pair<Prof>(st, ln, r, g, b, lane, pc);
       __syncwarp();
     }
   }
-  if (st.profile) {  // work counters for the roofline (warp-reduced)
+  if constexpr (Prof) {  // work counters for the roofline (warp-reduced)
     __syncwarp();
     for (auto o = 16; o > 0; o >>= 1) {
       pc.stops += __shfl_xor_sync(kFull, pc.stops, o);
