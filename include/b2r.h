@@ -341,10 +341,12 @@ typedef struct b2r_engine_config {
   uint32_t route_block;     /* launch shape: warps per CTA in the route scan */
   uint32_t max_starts;      /* start labels per query (default 4096) */
   uint32_t steps_per_sync;  /* super-steps between host checks (default 4) */
-  uint32_t profile;         /* 1 = time route scans with CUDA events and
-                               count their work (a counting build of the
-                               scan), 2 = time them only (the build the
-                               launch shape selects); both disable graphs */
+  uint32_t profile;         /* 1 = time route scans with CUDA events around
+                               every launch and count their work (a
+                               counting build of the scan; no graphs);
+                               2 = time them only: the build the launch
+                               shape selects, events inside the super-step
+                               graph, one super-step per host check */
   uint32_t reserved[4];
 } b2r_engine_config;
 

@@ -150,6 +150,11 @@ struct b2r_engine {
   // and export kernels, second stream) ran; their union is the batch's
   // device time
   cudaEvent_t ev_base{nullptr}, ev2a{nullptr}, ev2b{nullptr};
+  // timing engines (profile = 2): the route phase of every super-step,
+  // bracketed inside the graph and read after each super-step
+  cudaEvent_t ev_scan_a{nullptr}, ev_scan_b{nullptr};
+  double scan_ms{0};
+  uint64_t scan_launches{0};
   bool base_recorded{false};
   std::vector<std::pair<double, double>> busy;
   // profiling: event pairs bracketing each route-scan launch
@@ -471,6 +476,8 @@ b2r_engine::~b2r_engine() {
   if (ev0 != nullptr) cudaEventDestroy(ev0);
   if (ev1 != nullptr) cudaEventDestroy(ev1);
   if (ev_base != nullptr) cudaEventDestroy(ev_base);
+  if (ev_scan_a != nullptr) cudaEventDestroy(ev_scan_a);
+  if (ev_scan_b != nullptr) cudaEventDestroy(ev_scan_b);
   if (ev2a != nullptr) cudaEventDestroy(ev2a);
   if (ev2b != nullptr) cudaEventDestroy(ev2b);
   if (h_summary != nullptr) cudaFreeHost(h_summary);
@@ -498,7 +505,9 @@ void enqueue_superstep(b2r_engine& e, cudaStream_t s) {
   dev::k_list_routes<<<e.sms * 8, 256, 0, s>>>(st);
   dev::k_ctl_marked<<<slot_blocks, 128, 0, s>>>(st);
   cudaEvent_t ev_a = nullptr, ev_b = nullptr;
-  if (e.cfg.profile) {  // CUDA events on the launching stream around the scan
+  if (e.cfg.profile == 2U) {  // timing build: one event pair, captured in the super-step graph
+    B2R_CUDA(cudaEventRecord(e.ev_scan_a, s));
+  } else if (e.cfg.profile) {  // CUDA events on the launching stream around the scan
     while (e.prof_used + 2 > e.prof_ev.size()) {
       cudaEvent_t x;
       B2R_CUDA(cudaEventCreate(&x));
@@ -521,7 +530,9 @@ void enqueue_superstep(b2r_engine& e, cudaStream_t s) {
       dev::k_route_scan<4, false><<<grid, block, 0, s>>>(st);
     }
   }
-  if (e.cfg.profile) {
+  if (e.cfg.profile == 2U) {
+    B2R_CUDA(cudaEventRecord(e.ev_scan_b, s));
+  } else if (e.cfg.profile) {
     B2R_CUDA(cudaEventRecord(ev_b, s));
     auto const idx = static_cast<uint32_t>(e.prof_used / 2 - 1);
     if (idx < b2r_engine::kProfRows) k_prof_row<<<1, 1, 0, s>>>(st, e.d_prof_rows, idx);
@@ -534,7 +545,7 @@ void enqueue_superstep(b2r_engine& e, cudaStream_t s) {
   dev::k_footpaths<<<pair_blocks, 256, 0, s>>>(st);
   dev::k_end_collect<<<slot_blocks, 128, 0, s>>>(st);
   cudaEvent_t rc_a = nullptr, rc_b = nullptr;
-  if (e.cfg.profile) {
+  if (e.cfg.profile == 1U) {
     while (e.prof_rc_used + 2 > e.prof_rc_ev.size()) {
       cudaEvent_t x;
       B2R_CUDA(cudaEventCreate(&x));
@@ -545,7 +556,7 @@ void enqueue_superstep(b2r_engine& e, cudaStream_t s) {
     B2R_CUDA(cudaEventRecord(rc_a, s));
   }
   dev::k_reconstruct<<<e.sms * e.shape.recon_blocks_per_sm, 128, 0, s>>>(st);
-  if (e.cfg.profile) B2R_CUDA(cudaEventRecord(rc_b, s));
+  if (e.cfg.profile == 1U) B2R_CUDA(cudaEventRecord(rc_b, s));
   dev::k_next_summary<<<slot_blocks, 128, 0, s>>>(st);
   dev::k_list_marked<<<e.sms * 8, 256, 0, s>>>(st);
 }
@@ -1547,6 +1558,11 @@ struct batch_runner {
         B2R_CUDA(cudaEventElapsedTime(&a, e.ev_base, e.ev0));
         B2R_CUDA(cudaEventElapsedTime(&b, e.ev_base, e.ev1));
         e.busy.emplace_back(a, b);
+        if (e.cfg.profile == 2U) {  // one super-step per chunk: its route phase
+          B2R_CUDA(cudaEventElapsedTime(&a, e.ev_scan_a, e.ev_scan_b));
+          e.scan_ms += a;
+          ++e.scan_launches;
+        }
       }
       std::copy(e.h_summary, e.h_summary + S, sum.begin());
       for (auto& x : slot_q)
@@ -2180,7 +2196,7 @@ int b2r_engine_create(b2r_timetable* tt, const b2r_engine_config* cfg_in, b2r_en
       e->sms = b2r::n_sms(tt->device);
       e->max_j = std::max(32U, std::min(4096U, (cfg.max_journeys + 31U) & ~31U));
       e->max_starts = cfg.max_starts != 0 ? cfg.max_starts : 4096U;
-      if (cfg.profile) e->cfg.use_graphs = 0;
+      if (cfg.profile == 1U) e->cfg.use_graphs = 0;
       if (cfg.steps_per_sync != 0) e->shape.steps_per_sync = cfg.steps_per_sync;
       e->max_dest = 512U;
       e->max_off = 128U;
@@ -2289,6 +2305,8 @@ int b2r_engine_create(b2r_timetable* tt, const b2r_engine_config* cfg_in, b2r_en
       B2R_CUDA(cudaEventCreate(&e->ev0));
       B2R_CUDA(cudaEventCreate(&e->ev1));
       B2R_CUDA(cudaEventCreate(&e->ev_base));
+      B2R_CUDA(cudaEventCreate(&e->ev_scan_a));
+      B2R_CUDA(cudaEventCreate(&e->ev_scan_b));
       B2R_CUDA(cudaEventCreate(&e->ev2a));
       B2R_CUDA(cudaEventCreate(&e->ev2b));
       if (e->cfg.use_graphs) {
@@ -2342,7 +2360,9 @@ int b2r_search_batch(b2r_engine* e, const b2r_query* qs, uint32_t n, b2r_result*
       prep.start(*e, qs, n, runs, false);
       b2r::batch_runner br{*e, runs, e->cfg.use_graphs != 0 && e->graph != nullptr};
       if (e->cfg.profile) B2R_CUDA(cudaMemsetAsync(e->st.prof, 0, 8 * sizeof(unsigned long long), e->stream));
-      br.run(e->shape.steps_per_sync);
+      e->scan_ms = 0;
+      e->scan_launches = 0;
+      br.run(e->cfg.profile == 2U ? 1U : e->shape.steps_per_sync);
       prep.join();
       auto const t1 = std::chrono::steady_clock::now();
       B2R_CUDA(cudaStreamSynchronize(e->stream));
@@ -2359,7 +2379,10 @@ int b2r_search_batch(b2r_engine* e, const b2r_query* qs, uint32_t n, b2r_result*
       e->last.host_admit_ms = e->admit_ms;
       e->last.host_export_ms = e->export_ms;
       e->last.host_idle_ms = e->idle_ms;
-      if (e->cfg.profile) {
+      if (e->cfg.profile == 2U) {
+        e->last.route_scan_launches = e->scan_launches;
+        e->last.route_scan_ms = e->scan_ms;
+      } else if (e->cfg.profile) {
         double scan_ms = 0;
         for (size_t i = 0; i + 1 < e->prof_used; i += 2) {
           float x = 0;
@@ -2538,7 +2561,7 @@ int b2r_last_batch_scan_profile(const b2r_engine* e, double* scan_ms, uint64_t* 
                                 uint64_t* stop_visits, uint32_t cap, uint32_t* n) {
   B2R_API_GUARD({
     if (e == nullptr || n == nullptr) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
-    if (!e->cfg.profile) return b2r::fail(B2R_ERR_UNSUPPORTED, "engine was not created with profile = 1 or 2");
+    if (e->cfg.profile != 1U) return b2r::fail(B2R_ERR_UNSUPPORTED, "engine was not created with profile = 1");
     auto const launches = static_cast<uint32_t>(std::min<size_t>(e->prof_used / 2, b2r_engine::kProfRows));
     *n = launches;
     auto const m = std::min(cap, launches);
