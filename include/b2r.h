@@ -273,6 +273,11 @@ typedef struct b2r_leg {
   int16_t duration;    /* footpath / offset duration */
   int16_t pad2_;
   int32_t transport_mode_id; /* offset */
+  uint32_t rt_transport;     /* transport: the real-time run ridden
+                                (rt::run::rt_), B2R_INVALID_IDX for a static
+                                one; `transport` and `day` then name the
+                                static trip it runs for, B2R_INVALID_IDX for
+                                an added trip */
 } b2r_leg;
 
 /* journey, journey.h:84-118 */
@@ -413,6 +418,55 @@ int b2r_search_plain(b2r_engine* e, const b2r_query* q, b2r_result* out);
 int b2r_one_to_all_noalloc(const b2r_timetable* tt, const b2r_query* q,
                            int16_t* round_times, uint64_t capacity,
                            uint32_t* n_rows, int32_t* base_day, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Real-time overlay: what rt_timetable (include/nigiri/rt/rt_timetable.h:
+ * 48-311) holds for routing, after the real-time updates are applied.
+ * - Static transports whose service changed on some days get new traffic
+ *   days (transport_traffic_days_ with kRtBitfieldFlag, bitfields_).
+ * - Every delayed, rerouted or added run is an rt transport with its own
+ *   stop sequence and event times (rt_transport_location_seq_,
+ *   rt_transport_stop_times_), class and route flags
+ *   (rt_transport_section_clasz_, rt_transport_flags_,
+ *   rt_flags_per_section_).
+ * An engine bound to an overlay (b2r_engine_set_rt) searches with it as
+ * raptor<Dir, Rt = true> does: rt transports are marked from their stations
+ * (raptor.h:228-241), scanned by update_rt_transport (raptor.h:1068-1175),
+ * taken first by reconstruction (reconstruct.cc:381-452) and boarded by
+ * interval start times (start_times.cc:177-215). */
+typedef struct b2r_rt_desc {
+  uint32_t n_changed;                /* static transports with new traffic days */
+  const uint32_t* changed_transport; /* their indices */
+  const uint64_t* changed_days;      /* n_changed x 8 words: their 512-bit days */
+  uint32_t n_rt_transports;
+  const uint32_t* rt_stop_index;     /* n_rt_transports + 1 */
+  const uint32_t* rt_stops;          /* stop words (B2R_STOP_*) */
+  const int32_t* rt_event_times;     /* per rt transport 2 (n_stops - 1) times,
+                                        minutes since the epoch, in the order of
+                                        rt_transport_stop_times_: departure at
+                                        stop 0, arrival at stop 1, departure at
+                                        stop 1, ..., arrival at the last stop;
+                                        rt transport i starts at
+                                        2 (rt_stop_index[i] - i) */
+  const uint32_t* rt_static_transport; /* the static trip it runs for, or
+                                          B2R_INVALID_IDX (added) */
+  const uint16_t* rt_static_day;     /* that trip's traffic day index */
+  const uint8_t* rt_clasz;           /* class of its first section; NULL: 10 */
+  const uint8_t* rt_flags;           /* route flags as route_flags; NULL: none */
+  const uint8_t* rt_section_flags;   /* per rt stop like route_section_flags;
+                                        NULL: none */
+} b2r_rt_desc;
+
+typedef struct b2r_rt b2r_rt;
+/* Uploads an overlay for timetable tt (the arrays are copied). */
+int b2r_rt_upload(b2r_timetable* tt, const b2r_rt_desc* d, b2r_rt** out);
+int b2r_rt_destroy(b2r_rt* rt);
+/* Searches of this engine use the overlay from the next call on (NULL: the
+ * static timetable).  The overlay must outlive the binding.  While one is
+ * bound the engine prunes without lower bounds (lb = 0): the timetable's
+ * bounds do not cover added runs, and bounds only prune, so the journeys
+ * are the same. */
+int b2r_engine_set_rt(b2r_engine* e, const b2r_rt* rt);
 
 /* ------------------------------------------------------------------------
  * The Algo concept of routing::search<Dir, Algo>.
@@ -593,8 +647,9 @@ int b2r_engine_set_shape(b2r_engine* e, const b2r_launch_shape* shape);
 /* Autotuner: runs `sample` (n queries, results discarded) three times per
  * candidate launch shape, one knob at a time over a small grid of values
  * (coordinate descent, repeated until a pass changes nothing, at most three
- * passes), keeps the shape with the shortest batch wall time and reports
- * what it tried.  The last-batch results and statistics are overwritten. */
+ * passes), then measures the starting shape and the pick once more side by
+ * side and keeps the faster (so best_ms <= start_ms), and reports what it
+ * tried.  The last-batch results and statistics are overwritten. */
 typedef struct b2r_tune_report {
   uint32_t n_tried;
   b2r_launch_shape start, best;

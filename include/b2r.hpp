@@ -105,10 +105,11 @@ struct query {
   bool no_compulsory_reservation_{false};
 };
 
-struct run_enter_exit {  // journey::run_enter_exit (transport, day, stops)
+struct run_enter_exit {  // journey::run_enter_exit (transport, day, stops, real-time run)
   uint32_t transport_{0};
   uint16_t day_{0};
   uint16_t stop_from_{0}, stop_to_{0};  // stop_range_ [from, to)
+  uint32_t rt_transport_{B2R_INVALID_IDX};  // rt::run::rt_
   friend bool operator==(run_enter_exit const&, run_enter_exit const&) = default;
 };
 
@@ -345,7 +346,9 @@ inline query query_of(b2r_query const& c) {
 inline leg leg_of(b2r_leg const& l) {
   leg y{l.from, l.to, l.dep_time, l.arr_time, {}};
   switch (l.kind) {
-    case B2R_LEG_TRANSPORT: y.uses_ = run_enter_exit{l.transport, l.day, l.stop_from, l.stop_to}; break;
+    case B2R_LEG_TRANSPORT:
+      y.uses_ = run_enter_exit{l.transport, l.day, l.stop_from, l.stop_to, l.rt_transport};
+      break;
     case B2R_LEG_FOOTPATH: y.uses_ = footpath{l.transport, l.duration}; break;
     default: y.uses_ = offset{l.transport, l.duration, l.transport_mode_id};
   }

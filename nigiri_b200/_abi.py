@@ -107,7 +107,18 @@ class Leg(C.Structure):
         ("arr_time", C.c_int32), ("kind", C.c_uint8), ("pad_", C.c_uint8),
         ("day", C.c_uint16), ("transport", C.c_uint32), ("stop_from", C.c_uint16),
         ("stop_to", C.c_uint16), ("duration", C.c_int16), ("pad2_", C.c_int16),
-        ("transport_mode_id", C.c_int32),
+        ("transport_mode_id", C.c_int32), ("rt_transport", C.c_uint32),
+    ]
+
+
+class RtDesc(C.Structure):  # b2r_rt_desc
+    _fields_ = [
+        ("n_changed", C.c_uint32), ("changed_transport", C.POINTER(C.c_uint32)),
+        ("changed_days", C.POINTER(C.c_uint64)), ("n_rt_transports", C.c_uint32),
+        ("rt_stop_index", C.POINTER(C.c_uint32)), ("rt_stops", C.POINTER(C.c_uint32)),
+        ("rt_event_times", C.POINTER(C.c_int32)), ("rt_static_transport", C.POINTER(C.c_uint32)),
+        ("rt_static_day", C.POINTER(C.c_uint16)), ("rt_clasz", C.POINTER(C.c_uint8)),
+        ("rt_flags", C.POINTER(C.c_uint8)), ("rt_section_flags", C.POINTER(C.c_uint8)),
     ]
 
 
@@ -197,6 +208,7 @@ EXPORTS = [
     "b2r_search_prepare", "b2r_search_extend", "b2r_search_plan_free", "b2r_raptor_create",
     "b2r_raptor_destroy", "b2r_raptor_reset_arrivals", "b2r_raptor_next_start_time",
     "b2r_raptor_add_start", "b2r_raptor_execute", "b2r_raptor_reconstruct", "b2r_raptor_rounds",
+    "b2r_rt_upload", "b2r_rt_destroy", "b2r_engine_set_rt",
 ]
 
 
@@ -258,6 +270,10 @@ def _declare(lib):
         "b2r_raptor_reconstruct": (C.c_int, [vp, C.POINTER(Query), C.POINTER(Journey), C.POINTER(Leg),
                                              C.c_uint32]),
         "b2r_raptor_rounds": (C.c_uint64, [vp]),
+        # the real-time overlay
+        "b2r_rt_upload": (C.c_int, [vp, C.POINTER(RtDesc), C.POINTER(vp)]),
+        "b2r_rt_destroy": (C.c_int, [vp]),
+        "b2r_engine_set_rt": (C.c_int, [vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -61,6 +61,7 @@ std::optional<b2r_leg> access_walk(tt_access const& t, tts_norm const& tts, uint
   if (eff < kMaxFootpath && eff < best) best = eff;
   if (best >= kMaxFootpath) return std::nullopt;
   b2r_leg l{};
+  l.rt_transport = B2R_INVALID_IDX;
   l.kind = B2R_LEG_FOOTPATH;
   l.from = boarding ? anchor : loc;
   l.to = boarding ? loc : anchor;
@@ -150,6 +151,7 @@ bool earliest_alternative(host_view const& hv, tts_norm const& tts, uint32_t prf
           auto const aw = access_walk(t, tts, prf, to, alight_loc, arr, false);
           if (!bw.has_value() || !aw.has_value() || bw->dep_time < from_arr) continue;
           b2r_leg ride{};
+          ride.rt_transport = B2R_INVALID_IDX;
           ride.kind = B2R_LEG_TRANSPORT;
           ride.from = board_loc;
           ride.to = alight_loc;

@@ -105,6 +105,9 @@ using row_vector = std::vector<int16_t, uninit_allocator<int16_t>>;
 struct b2r_engine {
   b2r_timetable* tt{nullptr};
   b2r_engine_config cfg{};
+  b2r::host_view view{};      // the timetable's host view, with the bound overlay
+  b2r_rt const* rt{nullptr};  // the bound real-time overlay, if any
+  int lb_mode() const { return rt != nullptr ? 0 : static_cast<int>(cfg.use_lower_bounds); }
   uint32_t S{0}, G{0}, max_j{0}, max_starts{0}, max_dest{0}, max_off{0};
   uint64_t bytes_per_slot{0}, bytes{0};
   b2r::dev::state st{};
@@ -485,6 +488,8 @@ b2r_engine::~b2r_engine() {
   if (h_adm != nullptr) cudaFreeHost(h_adm);
   if (h_exp != nullptr) cudaFreeHost(h_exp);
   for (auto* p : allocs) cudaFree(p);
+  if (st.RT_R != nullptr) cudaFree(st.RT_R);
+  if (st.rtlist != nullptr) cudaFree(st.rtlist);
 }
 
 namespace b2r {
@@ -503,6 +508,10 @@ void enqueue_superstep(b2r_engine& e, cudaStream_t s) {
   auto const pair_blocks = e.sms * e.shape.pair_blocks_per_sm;
   dev::k_mark_routes<<<pair_blocks, 256, 0, s>>>(st);
   dev::k_list_routes<<<e.sms * 8, 256, 0, s>>>(st);
+  if (st.tt.n_rt != 0U) {  // a real-time overlay is bound: its runs are marked too
+    dev::k_mark_rt<<<list_blocks, 256, 0, s>>>(st);
+    dev::k_list_rt<<<e.sms * 8, 256, 0, s>>>(st);
+  }
   dev::k_ctl_marked<<<slot_blocks, 128, 0, s>>>(st);
   cudaEvent_t ev_a = nullptr, ev_b = nullptr;
   if (e.cfg.profile == 2U) {  // timing build: one event pair, captured in the super-step graph
@@ -537,6 +546,7 @@ void enqueue_superstep(b2r_engine& e, cudaStream_t s) {
     auto const idx = static_cast<uint32_t>(e.prof_used / 2 - 1);
     if (idx < b2r_engine::kProfRows) k_prof_row<<<1, 1, 0, s>>>(st, e.d_prof_rows, idx);
   }
+  if (st.tt.n_rt != 0U) dev::k_rt_scan<<<pair_blocks, 256, 0, s>>>(st);
   dev::k_list_reached<<<e.sms * 8, 256, 0, s>>>(st);
   dev::k_clear_x<<<list_blocks, 256, 0, s>>>(st);
   dev::k_transfers_pre<<<slot_blocks, 128, 0, s>>>(st);
@@ -560,7 +570,7 @@ void enqueue_superstep(b2r_engine& e, cudaStream_t s) {
   dev::k_next_summary<<<slot_blocks, 128, 0, s>>>(st);
   dev::k_list_marked<<<e.sms * 8, 256, 0, s>>>(st);
 }
-constexpr uint64_t kLaunchesPerStep = 18;
+uint64_t launches_per_step(b2r_engine const& e) { return e.st.tt.n_rt != 0U ? 21U : 18U; }
 
 // --------------------------------------------------------- admission
 size_t admission_bytes(b2r_engine const& e, prepped_query const& p) {
@@ -800,8 +810,8 @@ void admit(b2r_engine& e, std::vector<adm_req> const& adm, cudaStream_t s) {
     h.lb_mode = p.keep_lb          ? 4
                 : !p.lb.empty()      ? 1
                 : p.one_to_all       ? 0
-                : e.cfg.use_lower_bounds == 2 ? 2
-                : e.cfg.use_lower_bounds == 3 ? 3
+                : e.lb_mode() == 2 ? 2
+                : e.lb_mode() == 3 ? 3
                                               : 0;
     h.off_lb = put(p.lb.data(), p.lb.size() * sizeof(uint16_t));
     std::vector<uint32_t> seeds;
@@ -1103,14 +1113,14 @@ void on_phase_done(b2r_engine& e, query_run& q, exported& x) {
     keep = std::move(k2);
   };
   if (nf != x.sl.iv_from) {
-    add_interval_starts(e.tt->view, p, nf, x.sl.iv_from, !p.fwd, starts);
+    add_interval_starts(e.view, p, nf, x.sl.iv_from, !p.fwd, starts);
     if (!p.fwd) {
       q.reset_arrivals = true;
       remove_outside();
     }
   }
   if (nt != x.sl.iv_to) {
-    add_interval_starts(e.tt->view, p, x.sl.iv_to, nt, p.fwd, starts);
+    add_interval_starts(e.view, p, x.sl.iv_to, nt, p.fwd, starts);
     if (p.fwd) {
       q.reset_arrivals = true;
       remove_outside();
@@ -1231,7 +1241,7 @@ void stage_ping(b2r_engine& e, query_run& q) {
   auto& r = *q.pong;
   q.phase = q.p.pong->ping;
   q.phase.keep_lb = true;  // the lower bounds of the first ping stay in the slot
-  phase_starts(e.tt->view, q.phase, r.start_time, q.phase.starts);
+  phase_starts(e.view, q.phase, r.start_time, q.phase.starts);
   q.adm_flags = kAdmRephase;
   q.upload.clear();
   r.in_ping = true;
@@ -1244,7 +1254,7 @@ void stage_pong(b2r_engine& e, query_run& q, bool first_of_iteration) {
   auto& r = *q.pong;
   auto const& pj = r.ping[r.next];
   q.phase = q.p.pong->pong;
-  phase_starts(e.tt->view, q.phase, pj.dest_time, q.phase.starts);
+  phase_starts(e.view, q.phase, pj.dest_time, q.phase.starts);
   q.phase.end_k = static_cast<uint8_t>(std::min<int>(pj.transfers, B2R_MAX_TRANSFERS) + 2);
   q.phase.blast = static_cast<uint8_t>(pj.transfers + 1U);
   q.phase.span = static_cast<int16_t>(std::abs(pj.dest_time - pj.start_time));
@@ -1520,7 +1530,7 @@ struct batch_runner {
           enqueue_superstep(e, st);
           B2R_CUDA(cudaGetLastError());
         }
-        launches += kLaunchesPerStep;
+        launches += launches_per_step(e);
         ++steps;
       }
       B2R_CUDA(cudaEventRecord(e.ev1, st));
@@ -1639,11 +1649,11 @@ struct preparer {
     auto const hw = std::max(1U, std::thread::hardware_concurrency());
     auto const n_threads = std::max(1U, std::min<uint32_t>(
         e.cfg.host_threads != 0 ? e.cfg.host_threads : (hw > 1 ? hw - 1 : 1), n));
-    auto const lb_mode = static_cast<int>(e.cfg.use_lower_bounds);
+    auto const lb_mode = e.lb_mode();
     auto work = [&e, qs, n, &runs, lb_mode, this]() {
       for (auto i = next++; i < n; i = next++) {
         auto const t0 = std::chrono::steady_clock::now();
-        prepare(e.tt->view, qs[i], lb_mode, runs[i].p);
+        prepare(e.view, qs[i], lb_mode, runs[i].p);
         e.prep_ns += static_cast<uint64_t>(
             std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0).count());
         runs[i].ready.store(true, std::memory_order_release);
@@ -1725,7 +1735,7 @@ struct serve_state {
   }
 
   void prep_loop() {
-    auto const lb_mode = static_cast<int>(e.cfg.use_lower_bounds);
+    auto const lb_mode = e.lb_mode();
     std::unique_lock<std::mutex> lock{mu};
     while (true) {
       cv_prep.wait(lock, [&] { return stop || !to_prepare.empty(); });
@@ -1735,7 +1745,7 @@ struct serve_state {
       lock.unlock();
       auto status = B2R_OK;
       try {
-        prepare(e.tt->view, it->q, lb_mode, it->run.p);
+        prepare(e.view, it->q, lb_mode, it->run.p);
       } catch (...) {
         status = B2R_ERR_INTERNAL;
       }
@@ -2107,6 +2117,9 @@ int b2r_timetable_upload(const b2r_timetable_desc* d, int device, b2r_timetable*
       {  // footpath profiles 1..4 (a profile without footpaths: a zero index)
         std::vector<uint32_t> zero(nl + 1, 0U);
         auto* dz = up(zero.data(), zero.size());
+        dd.n_rt = 0;  // no real-time runs until an engine binds an overlay
+        dd.loc_rt_idx = dz;
+        dd.lrs_rt_idx = dz;
         std::vector<uint32_t const*> tab(4U * (B2R_N_PROFILES - 1U), dz);
         for (auto p = 0U; p != B2R_N_PROFILES - 1U; ++p) {
           auto const& pc = t->profiles[p];
@@ -2192,6 +2205,7 @@ int b2r_engine_create(b2r_timetable* tt, const b2r_engine_config* cfg_in, b2r_en
       b2r_engine_config_init(&cfg);
       if (cfg_in != nullptr) cfg = *cfg_in;
       e->tt = tt;
+      e->view = tt->view;
       e->cfg = cfg;
       e->sms = b2r::n_sms(tt->device);
       e->max_j = std::max(32U, std::min(4096U, (cfg.max_journeys + 31U) & ~31U));
@@ -2545,6 +2559,18 @@ int b2r_engine_autotune(b2r_engine* e, const b2r_query* sample, uint32_t n, b2r_
         }
         if (!changed) break;
         cur_ms = measure(cur);  // re-measured: the first figure may have been a lucky one
+      }
+      // the start and the pick measured once more side by side, so that a
+      // lucky early figure cannot leave a slower shape in place
+      auto const start_again = measure(rep.start);
+      auto const best_again = measure(cur);
+      rep.n_tried += 2;
+      rep.start_ms = start_again;
+      if (start_again < best_again) {
+        cur = rep.start;
+        cur_ms = start_again;
+      } else {
+        cur_ms = best_again;
       }
       if (b2r_engine_set_shape(e, &cur) != B2R_OK) return B2R_ERR_CUDA;
       rep.best = cur;
@@ -3019,5 +3045,139 @@ int b2r_raptor_reconstruct(b2r_raptor* r, const b2r_query* q, b2r_journey* j, b2
 }
 
 uint64_t b2r_raptor_rounds(const b2r_raptor* r) { return r == nullptr ? 0 : r->n_rounds; }
+
+}  // extern "C"
+
+// ------------------------------------------------------- real-time overlay
+// The device arrays of an overlay: the timetable image with the overlay's
+// traffic days (transport_bf repointed at appended bitfields) and its runs.
+struct b2r_rt {
+  b2r_timetable* tt{nullptr};
+  b2r::rt_host host;
+  b2r::dev::dtt d{};
+  std::vector<void*> allocs;
+  uint64_t bytes{0};
+  ~b2r_rt() {
+    for (auto* p : allocs) cudaFree(p);
+  }
+};
+
+extern "C" {
+
+int b2r_rt_upload(b2r_timetable* tt, const b2r_rt_desc* desc, b2r_rt** out) {
+  B2R_API_GUARD({
+    if (tt == nullptr || desc == nullptr || out == nullptr) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
+    auto r = std::make_unique<b2r_rt>();
+    r->tt = tt;
+    auto const nl = tt->d.n_loc, ntr = tt->d.n_transports;
+    if (!r->host.init(*desc, nl, ntr)) {
+      return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "b2r_rt_upload: malformed overlay");
+    }
+    auto const& h = r->host;
+    try {
+      B2R_CUDA(cudaSetDevice(tt->device));
+      auto up = [&](auto const* p, size_t n) {
+        auto* x = b2r::dupload(p, n, r->bytes);
+        r->allocs.push_back(x);
+        return x;
+      };
+      auto& d = r->d;
+      d = tt->d;
+      // traffic days: the changed transports point at bitfields appended to
+      // the timetable's (rt_timetable::transport_traffic_days_ with
+      // kRtBitfieldFlag)
+      auto const n_bf = static_cast<uint32_t>(tt->host.n_bitfields);
+      std::vector<uint32_t> tbf(tt->transport_traffic_days.begin(), tt->transport_traffic_days.end());
+      std::vector<uint64_t> bf(tt->bitfields.begin(), tt->bitfields.end());
+      bf.insert(bf.end(), h.changed_days.begin(), h.changed_days.end());
+      for (auto i = 0U; i != h.changed_transport.size(); ++i) tbf[h.changed_transport[i]] = n_bf + i;
+      d.transport_bf = up(tbf.data(), tbf.size());
+      d.bf = up(bf.data(), bf.size());
+      auto const n_rt = h.d.n_rt_transports;
+      d.n_rt = n_rt;
+      d.rt_stop_idx = up(h.stop_index.data(), h.stop_index.size());
+      d.rt_stops = up(h.stops.data(), h.stops.size());
+      d.rt_times = up(h.times.data(), h.times.size());
+      std::vector<uint16_t> filt(n_rt);
+      for (auto x = 0U; x != n_rt; ++x) {  // class | all-sections flags << 4 | some << 8, as route_filter
+        uint32_t all = 0U, some = 0U;
+        for (auto f = 0U; f != 4U; ++f) {
+          all |= ((h.flags[x] >> (2U * f)) & 1U) << f;
+          some |= ((h.flags[x] >> (2U * f + 1U)) & 1U) << f;
+        }
+        filt[x] = static_cast<uint16_t>(h.clasz[x] | (all << 4) | (some << 8));
+      }
+      d.rt_filter = up(filt.data(), filt.size());
+      d.rt_sec = up(h.section_flags.data(), h.section_flags.size());
+      d.rt_static = up(h.static_transport.data(), h.static_transport.size());
+      d.rt_static_day = up(h.static_day.data(), h.static_day.size());
+      d.loc_rt_idx = up(h.loc_idx.data(), h.loc_idx.size());
+      d.loc_rt = up(h.loc_rt.data(), h.loc_rt.size());
+      // location -> (run, stop position) in reconstruction's order: the
+      // runs of location_rt_transports_, then stop positions ascending
+      std::vector<uint32_t> idx(nl + 1U, 0U), xs;
+      std::vector<uint16_t> ss;
+      for (auto l = 0U; l != nl; ++l) {
+        for (auto k = h.loc_idx[l]; k != h.loc_idx[l + 1]; ++k) {
+          auto const x = h.loc_rt[k];
+          for (auto i = 0U; i != h.n_stops(x); ++i) {
+            if (B2R_STOP_LOC(h.stop(x, i)) == l) {
+              xs.push_back(x);
+              ss.push_back(static_cast<uint16_t>(i));
+            }
+          }
+        }
+        idx[l + 1U] = static_cast<uint32_t>(xs.size());
+      }
+      d.lrs_rt_idx = up(idx.data(), idx.size());
+      d.lrs_rt = up(xs.data(), xs.size());
+      d.lrs_rt_stop = up(ss.data(), ss.size());
+      *out = r.release();
+      return B2R_OK;
+    } catch (b2r::cuda_error const& ex) {
+      return b2r::fail(B2R_ERR_CUDA, ex.what());
+    }
+  });
+}
+
+int b2r_rt_destroy(b2r_rt* rt) {
+  delete rt;
+  return B2R_OK;
+}
+
+int b2r_engine_set_rt(b2r_engine* e, const b2r_rt* rt) {
+  B2R_API_GUARD({
+    if (e == nullptr) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
+    if (e->serving) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "engine is serving");
+    if (rt != nullptr && rt->tt != e->tt) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "overlay of another timetable");
+    try {
+      B2R_CUDA(cudaSetDevice(e->tt->device));
+      B2R_CUDA(cudaStreamSynchronize(e->stream));
+      auto const n_rt = rt != nullptr ? rt->d.n_rt : 0U;
+      if (e->st.RT_R != nullptr) cudaFree(e->st.RT_R);
+      if (e->st.rtlist != nullptr) cudaFree(e->st.rtlist);
+      e->st.RT_R = nullptr;
+      e->st.rtlist = nullptr;
+      if (n_rt != 0U) {
+        auto const words = static_cast<size_t>(n_rt) * e->G;
+        B2R_CUDA(cudaMalloc(&e->st.RT_R, words * sizeof(uint32_t)));
+        B2R_CUDA(cudaMalloc(&e->st.rtlist, words * sizeof(uint32_t)));
+        B2R_CUDA(cudaMemset(e->st.RT_R, 0, words * sizeof(uint32_t)));
+      }
+      e->rt = rt;
+      e->st.tt = rt != nullptr ? rt->d : e->tt->d;
+      e->view = e->tt->view;
+      e->view.rt = rt != nullptr ? &rt->host : nullptr;
+      if (e->graph != nullptr) {  // the graph holds the old image and kernels
+        cudaGraphExecDestroy(e->graph);
+        e->graph = nullptr;
+        b2r::capture_graph(*e);
+      }
+      return B2R_OK;
+    } catch (b2r::cuda_error const& ex) {
+      return b2r::fail(B2R_ERR_CUDA, ex.what());
+    }
+  });
+}
 
 }  // extern "C"

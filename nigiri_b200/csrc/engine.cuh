@@ -92,6 +92,25 @@ struct dtt {
   // the flags of the section s -> s + 1 (route_flags_per_section_)
   uint16_t const* route_filter;
   uint8_t const* route_sec;
+  // real-time overlay (an engine bound to one; n_rt = 0 otherwise): rt
+  // transports with their stop words, unix event times (transport x's
+  // event at stop i: rt_times[2 (rt_stop_idx[x] - x) + 2 i - is_arr]),
+  // filter words like route_filter and per-stop section flags; the static
+  // trip each runs for; location -> rt transports (route marking) and
+  // location -> (rt transport, stop position) pairs (reconstruction)
+  uint32_t n_rt;
+  uint32_t const* rt_stop_idx;
+  uint32_t const* rt_stops;
+  int32_t const* rt_times;
+  uint16_t const* rt_filter;
+  uint8_t const* rt_sec;
+  uint32_t const* rt_static;
+  uint16_t const* rt_static_day;
+  uint32_t const* loc_rt_idx;
+  uint32_t const* loc_rt;
+  uint32_t const* lrs_rt_idx;
+  uint32_t const* lrs_rt;
+  uint16_t const* lrs_rt_stop;
 };
 
 // --------------------------------------------------------- per-slot data
@@ -214,6 +233,8 @@ struct state {
   uint32_t* X;      // station marks  [n_loc][G]
   uint32_t* Y;      // route-reached marks [n_loc][G]
   uint32_t* R;      // route marks [n_routes][G]
+  uint32_t* RT_R;   // rt transport marks [n_rt][G] (an overlay is bound)
+  uint32_t* rtlist; // frontier list of (rt transport * G + g)
   uint32_t* D;      // is-destination bits [n_loc][G]
   uint32_t* xlist;  // frontier lists of (loc * G + g)
   uint32_t* ylist;
@@ -286,6 +307,15 @@ __device__ __forceinline__ bool route_allowed(dtt const& T, uint32_t r, uint32_t
                                               uint32_t& sec) {
   auto const f = static_cast<uint32_t>(T.route_filter[r]);
   auto const need = req & ~(f >> 4);  // required, not on all sections
+  sec = need;
+  return ((claszes >> (f & 15u)) & 1u) != 0u && (need & ~(f >> 8) & 15u) == 0u;
+}
+
+// the same for a filter word of that layout (rt transports: the class of
+// the first section, raptor.h:583-588)
+__device__ __forceinline__ bool filter_allowed(uint16_t fw, uint32_t claszes, uint32_t req, uint32_t& sec) {
+  auto const f = static_cast<uint32_t>(fw);
+  auto const need = req & ~(f >> 4);
   sec = need;
   return ((claszes >> (f & 15u)) & 1u) != 0u && (need & ~(f >> 8) & 15u) == 0u;
 }

@@ -11,7 +11,7 @@
 
 namespace b2r::dev {
 
-enum : uint32_t { C_X = 0, C_Y = 1, C_R = 2, C_RECON = 3, C_ERR = 4, C_F0 = 5, C_F1 = 6 };
+enum : uint32_t { C_X = 0, C_Y = 1, C_R = 2, C_RECON = 3, C_ERR = 4, C_F0 = 5, C_F1 = 6, C_RT = 7 };
 
 __device__ __forceinline__ size_t li(state const& st, uint32_t l, uint32_t s) {
   return static_cast<size_t>(l) * st.S + s;
@@ -98,6 +98,7 @@ __global__ void k_ctl_begin(state st) {
   if (tid == 0) {
     st.counters[C_R] = 0u;
     st.counters[C_RECON] = 0u;
+    st.counters[C_RT] = 0u;
   }
   if ((tid & ~31u) >= st.S) return;  // whole warps: S is a multiple of 32
   auto const s = tid;
@@ -274,6 +275,28 @@ __device__ __forceinline__ void list_nonzero(state const& st, uint32_t const* W,
 
 // marked (route, group) entries of this round
 __global__ void k_list_routes(state st) { list_nonzero(st, st.R, st.tt.n_routes * st.G, st.rlist, C_R); }
+
+// ------------------------------------------------ real-time transports
+// station marks -> rt transport marks (raptor.h:234-240), a thread per
+// marked (location, group) word; a marked rt transport also keeps its
+// queries in the round (any_marked)
+__global__ void k_mark_rt(state st) {
+  auto const nx = st.counters[C_X];
+  auto const& T = st.tt;
+  for (auto i = blockIdx.x * blockDim.x + threadIdx.x; i < nx; i += gridDim.x * blockDim.x) {
+    auto const e = st.xlist[i];
+    auto const g = e % st.G, l = e / st.G;
+    auto const w = st.X[e] & st.run_mask[g];
+    if (w == 0u) continue;
+    auto const b = T.loc_rt_idx[l], n = T.loc_rt_idx[l + 1] - b;
+    if (n == 0u) continue;
+    if ((st.any_mask[g] & w) != w) atomicOr(&st.any_mask[g], w);
+    for (auto j = 0u; j != n; ++j) atomicOr(&st.RT_R[T.loc_rt[b + j] * st.G + g], w);  // listed by k_list_rt
+  }
+}
+
+// marked (rt transport, group) entries of this round
+__global__ void k_list_rt(state st) { list_nonzero(st, st.RT_R, st.tt.n_rt * st.G, st.rtlist, C_RT); }
 
 __global__ void k_ctl_marked(state st) {
   auto const s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -612,6 +635,62 @@ __global__ void __launch_bounds__(256, MinBlocks) k_route_scan(const __grid_cons
     }
   }
 }
+// update_rt_transport, raptor.h:1068-1175 (no vias), a lane per marked
+// (rt transport, query) pair walking the run in search direction: et is
+// whether the query rides the run when it passes the stop.  The filters are
+// loop_rt_routes' (raptor.h:583-626): the class of the first section and
+// the route flags, section by section where set on some sections only.
+__global__ void k_rt_scan(state st) {
+  auto const& T = st.tt;
+  for_each_pair(
+      st.rtlist, st.counters[C_RT],
+      [&](uint32_t e) {
+        auto const m = st.RT_R[e];
+        st.RT_R[e] = 0u;
+        return m;
+      },
+      [&](uint32_t e, uint32_t b) {
+        auto const g = e % st.G, x = e / st.G;
+        auto const s = g * 32u + b;
+        auto const ln = st.lanes[s];
+        if (!ln.run) return;
+        uint32_t sec = 0u;
+        if ((ln.claszes != 0xFFFFu || ln.req != 0u) && !filter_allowed(T.rt_filter[x], ln.claszes, ln.req, sec)) {
+          return;
+        }
+        if ((ln.mode & 0x70u) == (B2R_PROFILE_WHEELCHAIR << 4)) sec |= 0x100u;
+        auto const bit = 1u << b;
+        auto const fwd = ln.fwd != 0;
+        auto const k = static_cast<uint32_t>(ln.k);
+        auto const sb = T.rt_stop_idx[x];
+        auto const n = T.rt_stop_idx[x + 1] - sb;
+        auto const* tm = T.rt_times + 2ull * (sb - x);
+        auto const base_min = (T.internal_from_days + static_cast<int32_t>(ln.base)) * 1440;
+        auto const lb_off = (ln.mode & 8u) != 0u;
+        scan_ctr pc{};
+        bool et = false;
+        for (auto i = 0u; i != n; ++i) {
+          auto const si = fwd ? i : n - 1u - i;
+          auto w = T.rt_stops[sb + si];
+          if ((sec & 0x100u) != 0u) w = (w & 0xCFFFFFFFu) | ((w >> 2) & 0x30000000u);
+          auto const l = B2R_STOP_LOC(w);
+          if ((sec & 15u) != 0u && i != 0u &&
+              (static_cast<uint32_t>(T.rt_sec[sb + (fwd ? si - 1u : si)]) & (sec & 15u)) != (sec & 15u)) {
+            et = false;
+          }
+          auto const lbv = lb_off ? uint16_t{0} : st.lb[li(st, l, s)];
+          if (et && (fwd ? si != 0u : si + 1u != n) && (fwd ? B2R_STOP_OUT(w) : B2R_STOP_IN(w))) {
+            auto const by = to_key(fwd, clamp16(tm[2u * si - (fwd ? 1u : 0u)] - base_min));
+            scan_arrive<false>(st, ln, s, g, bit, l, lbv, by, pc);
+          }
+          if (lbv == 0xFFFFu) break;  // raptor.h:1156-1158: before the boarding test
+          if (i + 1u == n || !(fwd ? B2R_STOP_IN(w) : B2R_STOP_OUT(w)) || !(st.X[l * st.G + g] & bit)) continue;
+          auto const by = to_key(fwd, clamp16(tm[2u * si - (fwd ? 0u : 1u)] - base_min));
+          if (dec(st.rt[rti(st, k - 1u, l, s)], ln.qtag) <= by) et = true;
+        }
+      });
+}
+
 // frontier list of the stations marked this round (transfers, footpaths,
 // start labels): every nonzero station-mark word (location, group)
 __global__ void k_list_marked(state st) { list_nonzero(st, st.X, st.tt.n_loc * st.G, st.xlist, C_X); }

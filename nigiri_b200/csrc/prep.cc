@@ -52,6 +52,10 @@ T adjust(tts_norm const& s, T d) {  // transfer_time_settings.h:20-31
 
 struct view {
   b2r_timetable_desc const& d;
+  rt_host const* rt{nullptr};
+  // timetable / rt_timetable::is_transport_active: the overlay's days for
+  // a transport it changed
+  bool transport_active(uint32_t t, uint32_t day) const;
   template <typename Fn>
   void kids(uint32_t l, Fn&& fn) const {
     if (d.children_index == nullptr) return;
@@ -281,6 +285,16 @@ bool bf_test(b2r_timetable_desc const& d, uint32_t bf, uint32_t i) {
   return i < B2R_MAX_DAYS && ((d.bitfields[8ull * bf + i / 64] >> (i % 64)) & 1ULL);
 }
 
+bool view::transport_active(uint32_t t, uint32_t day) const {
+  if (rt != nullptr) {
+    auto const it = rt->changed.find(t);
+    if (it != rt->changed.end()) {
+      return day < B2R_MAX_DAYS && ((rt->changed_days[8ull * it->second + day / 64] >> (day % 64)) & 1ULL);
+    }
+  }
+  return bf_test(d, d.transport_traffic_days[t], day);
+}
+
 // add_starts_in_interval + add_start_times_at_stop, start_times.cc:40-239
 void interval_starts(view const& v, prepped_query const& p, int32_t iv_from, int32_t iv_to,
                      uint32_t l, int16_t off, bool add_ontrip, std::vector<start_label>& out) {
@@ -309,8 +323,8 @@ void interval_starts(view const& v, prepped_query const& p, int32_t iv_from, int
         auto const mam = cnt % 1440;
         for (uint32_t day = first; day <= last; ++day) {
           auto const ev_time = v.internal_from_min() + static_cast<int32_t>(day) * 1440 + mam;
-          if (!bf_test(d, d.transport_traffic_days[t], static_cast<uint16_t>(day - day_off)) ||
-              ev_time < st_from || ev_time >= st_to) {
+          if (!v.transport_active(t, static_cast<uint16_t>(day - day_off)) || ev_time < st_from ||
+              ev_time >= st_to) {
             continue;
           }
           if (off == kMaxDur) continue;
@@ -325,11 +339,28 @@ void interval_starts(view const& v, prepped_query const& p, int32_t iv_from, int
       }
     }
   }
+  if (v.rt != nullptr) {  // real-time starts, start_times.cc:177-215
+    auto const& rt = *v.rt;
+    for (auto xi = rt.loc_idx[l]; xi != rt.loc_idx[l + 1]; ++xi) {
+      auto const x = rt.loc_rt[xi];
+      auto const n = rt.n_stops(x);
+      for (auto i = 0U; i != n; ++i) {
+        auto const stp = rt.stop(x, i);
+        if (B2R_STOP_LOC(stp) != l) continue;
+        if ((!fwd && (i == 0U || !stop_out(stp, p.prf))) || (fwd && (i + 1U == n || !stop_in(stp, p.prf)))) continue;
+        auto const ev_time = rt.event(x, i, !fwd);
+        auto const tas = fwd ? ev_time - off : ev_time + off;
+        if (tas < iv_from || tas >= iv_to) continue;
+        out.push_back({tas, ev_time, l});
+      }
+    }
+  }
   if (add_ontrip) {
     auto const tas = fwd ? iv_to : iv_from - 1;
     if (off != kMaxDur) out.push_back({tas, fwd ? iv_to + off : iv_from - 1 - off, l});
   }
 }
+
 
 // get_starts, start_times.cc:241-319: shortest offset per start location
 // (insertion ordered), then ontrip labels or interval departures.
@@ -415,7 +446,7 @@ void collect_dests(view const& v, prepped_query& p) {
 // as given: pong hands q.transfer_time_settings_ to both searches without
 // search::init's normalisation.
 void prepare_pong(host_view const& hv, b2r_query const& q, int lb_mode, prepped_query& out) {
-  view const v{hv.d};
+  view const v{hv.d, hv.rt};
   out = prepped_query{};
   if (q.kind != B2R_ONE_TO_ONE || (q.start_match_mode == B2R_MATCH_INTERMODAL && q.use_start_footpaths != 0)) {
     out.status = B2R_ERR_INVALID_ARGUMENT;  // query::sanitize's verify (query.cc:59-62)
@@ -512,7 +543,7 @@ void prepare_pong(host_view const& hv, b2r_query const& q, int lb_mode, prepped_
 }
 
 void phase_starts(host_view const& hv, prepped_query const& tmpl, int32_t t, std::vector<start_label>& out) {
-  view const v{hv.d};
+  view const v{hv.d, hv.rt};
   out.clear();
   collect_starts(v, tmpl, false, t, 0, 0, tmpl.use_start_footpaths, false, out);
 }
@@ -524,6 +555,11 @@ void prepare(host_view const& hv, b2r_query const& q, int lb_mode, prepped_query
     return;
   }
   if (q.algorithm == B2R_ALGO_PONG) {
+    if (hv.rt != nullptr) {  // pong over a real-time overlay is not implemented
+      p = prepped_query{};
+      p.status = B2R_ERR_UNSUPPORTED;
+      return;
+    }
     prepare_pong(hv, q, lb_mode, p);
     return;
   }
@@ -532,7 +568,7 @@ void prepare(host_view const& hv, b2r_query const& q, int lb_mode, prepped_query
     p.status = B2R_ERR_INVALID_ARGUMENT;
     return;
   }
-  view const v{hv.d};
+  view const v{hv.d, hv.rt};
   p = prepped_query{};
   p.fwd = q.direction == B2R_FORWARD;
   p.one_to_all = q.kind == B2R_ONE_TO_ALL;
@@ -675,7 +711,7 @@ void prepare(host_view const& hv, b2r_query const& q, int lb_mode, prepped_query
 
 void add_interval_starts(host_view const& hv, prepped_query const& p, int32_t from, int32_t to,
                          bool add_ontrip, std::vector<start_label>& starts) {
-  view const v{hv.d};
+  view const v{hv.d, hv.rt};
   collect_starts(v, p, true, 0, from, to, false, add_ontrip, starts);
   sort_starts(p.fwd, starts);
 }
@@ -701,6 +737,74 @@ bool extend_interval(prepped_query const& p, int32_t ext_from, int32_t ext_to,
   from = nf;
   to = nt;
   return changed;
+}
+
+bool rt_host::init(b2r_rt_desc const& src, uint32_t n_loc, uint32_t n_transports) {
+  auto const n_rt = src.n_rt_transports;
+  if ((src.n_changed != 0 && (src.changed_transport == nullptr || src.changed_days == nullptr)) ||
+      (n_rt != 0 && (src.rt_stop_index == nullptr || src.rt_stops == nullptr || src.rt_event_times == nullptr))) {
+    return false;
+  }
+  changed_transport.assign(src.changed_transport, src.changed_transport + src.n_changed);
+  changed_days.assign(src.changed_days, src.changed_days + 8ull * src.n_changed);
+  for (auto i = 0U; i != src.n_changed; ++i) {
+    if (changed_transport[i] >= n_transports) return false;
+    changed[changed_transport[i]] = i;
+  }
+  if (n_rt != 0) {
+    stop_index.assign(src.rt_stop_index, src.rt_stop_index + n_rt + 1);
+  } else {
+    stop_index.assign(1, 0U);
+  }
+  if (stop_index[0] != 0U) return false;
+  for (auto x = 0U; x != n_rt; ++x) {
+    if (stop_index[x + 1] < stop_index[x] + 2U) return false;  // a run has two stops at least
+  }
+  auto const n_stops_all = stop_index.back();
+  stops.assign(src.rt_stops, src.rt_stops + n_stops_all);
+  for (auto w : stops) {
+    if (B2R_STOP_LOC(w) >= n_loc) return false;
+  }
+  times.assign(src.rt_event_times, src.rt_event_times + 2ull * (n_stops_all - n_rt));
+  static_transport.assign(n_rt, B2R_INVALID_IDX);
+  if (src.rt_static_transport != nullptr) static_transport.assign(src.rt_static_transport, src.rt_static_transport + n_rt);
+  static_day.assign(n_rt, 0U);
+  if (src.rt_static_day != nullptr) static_day.assign(src.rt_static_day, src.rt_static_day + n_rt);
+  clasz.assign(n_rt, 10U);
+  if (src.rt_clasz != nullptr) clasz.assign(src.rt_clasz, src.rt_clasz + n_rt);
+  for (auto c : clasz) {
+    if (c >= 16U) return false;
+  }
+  flags.assign(n_rt, 0U);
+  if (src.rt_flags != nullptr) flags.assign(src.rt_flags, src.rt_flags + n_rt);
+  section_flags.assign(n_stops_all, 0U);
+  if (src.rt_section_flags != nullptr) section_flags.assign(src.rt_section_flags, src.rt_section_flags + n_stops_all);
+  // location_rt_transports_: each run once per location, in run order
+  std::vector<std::vector<uint32_t>> by_loc(n_loc);
+  for (auto x = 0U; x != n_rt; ++x) {
+    for (auto i = stop_index[x]; i != stop_index[x + 1]; ++i) {
+      auto& v = by_loc[B2R_STOP_LOC(stops[i])];
+      if (v.empty() || v.back() != x) v.push_back(x);
+    }
+  }
+  loc_idx.assign(n_loc + 1U, 0U);
+  loc_rt.clear();
+  for (auto l = 0U; l != n_loc; ++l) {
+    loc_idx[l + 1U] = loc_idx[l] + static_cast<uint32_t>(by_loc[l].size());
+    loc_rt.insert(loc_rt.end(), by_loc[l].begin(), by_loc[l].end());
+  }
+  d = src;
+  d.changed_transport = changed_transport.data();
+  d.changed_days = changed_days.data();
+  d.rt_stop_index = stop_index.data();
+  d.rt_stops = stops.data();
+  d.rt_event_times = times.data();
+  d.rt_static_transport = static_transport.data();
+  d.rt_static_day = static_day.data();
+  d.rt_clasz = clasz.data();
+  d.rt_flags = flags.data();
+  d.rt_section_flags = section_flags.data();
+  return true;
 }
 
 }  // namespace b2r

@@ -7,6 +7,7 @@
 
 #include <cstdint>
 #include <memory>
+#include <unordered_map>
 #include <utility>
 #include <vector>
 
@@ -124,9 +125,34 @@ void add_interval_starts(host_view const& tt, prepped_query const& p,
 bool extend_interval(prepped_query const& p, int32_t ext_from, int32_t ext_to,
                      uint32_t num_con_req, int32_t& from, int32_t& to);
 
-// The flattened timetable as seen by host code (plain pointers).
+// A real-time overlay on the host: a copy of its description and the
+// lookups rt_timetable keeps (the changed traffic days by transport,
+// location_rt_transports_ in rt transport order, rt_timetable.cc:54-59).
+struct rt_host {
+  b2r_rt_desc d{};
+  std::vector<uint32_t> changed_transport, stop_index, stops, static_transport;
+  std::vector<uint64_t> changed_days;
+  std::vector<int32_t> times;
+  std::vector<uint16_t> static_day;
+  std::vector<uint8_t> clasz, flags, section_flags;
+  std::unordered_map<uint32_t, uint32_t> changed;  // transport -> row of changed_days
+  std::vector<uint32_t> loc_idx, loc_rt;
+
+  // copies d's arrays; false if d is malformed for a timetable of n_loc
+  // locations and n_transports transports
+  bool init(b2r_rt_desc const& src, uint32_t n_loc, uint32_t n_transports);
+  uint32_t n_stops(uint32_t x) const { return stop_index[x + 1] - stop_index[x]; }
+  uint32_t stop(uint32_t x, uint32_t i) const { return stops[stop_index[x] + i]; }
+  int32_t event(uint32_t x, uint32_t i, bool arr) const {  // rt_timetable::unix_event_time
+    return times[2ull * (stop_index[x] - x) + 2ull * i - (arr ? 1U : 0U)];
+  }
+};
+
+// The flattened timetable as seen by host code (plain pointers), with the
+// real-time overlay the searching engine is bound to, if any.
 struct host_view {
   b2r_timetable_desc d;
+  rt_host const* rt{nullptr};
   int32_t internal_from_days() const { return d.date_range_from - 5; }
 };
 

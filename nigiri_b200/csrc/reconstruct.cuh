@@ -103,6 +103,7 @@ struct recon_ctx {
   // -------------------------------------------------------------- legs
   __device__ b2r_leg make_leg(uint32_t a, uint32_t b, int32_t ta, int32_t tb) const {
     b2r_leg l{};
+    l.rt_transport = B2R_INVALID_IDX;
     l.from = fwd ? a : b;
     l.to = fwd ? b : a;
     l.dep_time = fwd ? ta : tb;
@@ -199,6 +200,51 @@ struct recon_ctx {
     return false;
   }
 
+  // find_start_in_prev_round on a real-time run (rt::frun::from_rt): the
+  // run's own stops and event times, as above.
+  __device__ bool find_start_in_prev_round_rt(unsigned k, uint32_t x, uint32_t finish, uint32_t sec,
+                                              b2r_leg& out) const {
+    auto const sb = T->rt_stop_idx[x];
+    auto const size = T->rt_stop_idx[x + 1] - sb;
+    auto const* tm = T->rt_times + 2ull * (sb - x);
+    auto const n = fwd ? finish + 1u : size - finish;
+    for (auto i0 = 1u; i0 < n; i0 += 32u) {
+      auto const i = i0 + lane;
+      bool ok = false, cut = false;
+      uint32_t si = 0, l = 0;
+      int event_time = 0;
+      if (i < n) {
+        si = fwd ? finish - i : finish + i;
+        auto const w = T->rt_stops[sb + si];
+        l = B2R_STOP_LOC(w);
+        cut = sec != 0u && (static_cast<uint32_t>(T->rt_sec[sb + (fwd ? si : si - 1u)]) & sec) != sec;
+        if (!cut && !((fwd && !B2R_STOP_IN(w)) || (!fwd && !B2R_STOP_OUT(w)))) {
+          event_time = unix_to_delta(tm[2u * si - (fwd ? 0u : 1u)]);
+          auto const round_time = rt_t(k - 1, l);
+          ok = beq(round_time, event_time) ||
+               (k == 1 && sl->start_mode == B2R_MATCH_EQUIVALENT && is_journey_start(l) &&
+                (ontrip ? beq(round_time, event_time) : round_time == event_time));
+        }
+      }
+      auto m = __ballot_sync(kFull, ok);
+      auto const cuts = __ballot_sync(kFull, cut);
+      if (cuts != 0u) m &= (1u << (__ffs(cuts) - 1)) - 1u;
+      if (m != 0u) {
+        auto const src = __ffs(m) - 1;
+        si = __shfl_sync(kFull, si, src);
+        l = __shfl_sync(kFull, l, src);
+        event_time = __shfl_sync(kFull, event_time, src);
+        out = make_leg(l, B2R_STOP_LOC(T->rt_stops[sb + finish]), delta_to_unix(event_time),
+                       tm[2u * finish - (fwd ? 1u : 0u)]);
+        set_run(out, T->rt_static[x], T->rt_static_day[x], si, finish);
+        out.rt_transport = x;
+        return true;
+      }
+      if (cuts != 0u) return false;
+    }
+    return false;
+  }
+
   // The transports of route r whose event at stop si has the minutes after
   // midnight of `time` (reconstruct.cc:292-373), one at a time from
   // `cursor`: columns are ordered by minutes after midnight, so they form
@@ -243,9 +289,11 @@ struct recon_ctx {
 
   // get_transport (reconstruct.cc:375-545) for a list of footpath
   // candidates, tried in order: candidate f reaches location `target(f)` at
-  // `time(f)`; its (route, stop position) pairs are visited in the
-  // reference's order.  All pairs of all candidates form one sequence that
-  // the lanes take 32 at a time; the first success in sequence order wins.
+  // `time(f)`; its real-time (run, stop position) pairs and then its (route,
+  // stop position) pairs are visited in the reference's order
+  // (reconstruct.cc:381-452 first).  All pairs of all candidates form one
+  // sequence that the lanes take 32 at a time; the first success in
+  // sequence order wins.
   // get(f, target, time) describes candidate f (lane-local); returns the
   // winning candidate or -1.
   template <typename Get>
@@ -253,12 +301,14 @@ struct recon_ctx {
     for (auto f0 = 0u; f0 < n_cand; f0 += 32u) {
       // lane f: candidate f0 + f, its pair range and the inclusive prefix sum
       auto const f = f0 + lane;
-      uint32_t tg = 0, pb = 0, cnt = 0;
+      uint32_t tg = 0, pb = 0, cnt = 0, rb = 0, rcnt = 0;
       int tm = 0;
       if (f < n_cand) {
         get(f, tg, tm);
         pb = T->lrs_idx[tg];
-        cnt = T->lrs_idx[tg + 1] - pb;
+        rb = T->lrs_rt_idx[tg];
+        rcnt = T->lrs_rt_idx[tg + 1] - rb;
+        cnt = rcnt + (T->lrs_idx[tg + 1] - pb);
       }
       auto end = cnt;
       for (auto o = 1u; o < 32u; o <<= 1) {
@@ -279,11 +329,27 @@ struct recon_ctx {
         auto const o_pb = __shfl_sync(kFull, pb, static_cast<int>(owner));
         auto const o_end = __shfl_sync(kFull, end, static_cast<int>(owner));
         auto const o_cnt = __shfl_sync(kFull, cnt, static_cast<int>(owner));
-        bool has = false;
+        auto const o_rb = __shfl_sync(kFull, rb, static_cast<int>(owner));
+        auto const o_rcnt = __shfl_sync(kFull, rcnt, static_cast<int>(owner));
+        bool has = false, is_rt = false;
         uint32_t r = 0, i = 0, cursor = 0, t = 0, sec = 0;
         uint16_t tday = 0;
-        if (p < total) {
-          auto const x = o_pb + (p - (o_end - o_cnt));
+        if (p < total && p - (o_end - o_cnt) < o_rcnt) {  // a real-time run at the stop
+          auto const x = o_rb + (p - (o_end - o_cnt));
+          is_rt = true;
+          r = T->lrs_rt[x];
+          i = static_cast<uint32_t>(T->lrs_rt_stop[x]);
+          auto const sb = T->rt_stop_idx[r];
+          auto const n = T->rt_stop_idx[r + 1] - sb;
+          auto const w = T->rt_stops[sb + i];
+          auto const allowed = (sl->allowed_claszes == 0xFFFFu && sl->req_flags == 0u) ||
+                               filter_allowed(T->rt_filter[r], sl->allowed_claszes, sl->req_flags, sec);
+          // an earlier arrival than the label is accepted (reconstruct.cc:437-440)
+          has = allowed &&
+                !((fwd && (i == 0u || !B2R_STOP_OUT(w))) || (!fwd && (i + 1u == n || !B2R_STOP_IN(w)))) &&
+                beq(T->rt_times[2ull * (sb - r) + 2u * i - (fwd ? 1u : 0u)], delta_to_unix(o_tm));
+        } else if (p < total) {
+          auto const x = o_pb + (p - (o_end - o_cnt) - o_rcnt);
           r = T->lrs_route[x];
           i = static_cast<uint32_t>(T->lrs_stop[x]);
           auto const w = stopw(r, i);
@@ -302,10 +368,13 @@ struct recon_ctx {
           auto const bday = static_cast<uint16_t>(__shfl_sync(kFull, static_cast<uint32_t>(tday), src));
           auto const bi = __shfl_sync(kFull, i, src);
           auto const bsec = __shfl_sync(kFull, sec, src);
-          if (find_start_in_prev_round(k, bt, bday, bi, bsec, out)) {
+          auto const brt = __shfl_sync(kFull, is_rt ? 1u : 0u, src) != 0u;
+          auto const bx = __shfl_sync(kFull, r, src);
+          if (brt ? find_start_in_prev_round_rt(k, bx, bi, bsec, out)
+                  : find_start_in_prev_round(k, bt, bday, bi, bsec, out)) {
             return static_cast<int>(f0 + __shfl_sync(kFull, owner, src));
           }
-          if (static_cast<int>(lane) == src) has = next_transport(o_tm, r, i, cursor, t, tday);
+          if (static_cast<int>(lane) == src) has = !is_rt && next_transport(o_tm, r, i, cursor, t, tday);
         }
       }
     }

@@ -62,9 +62,36 @@ inline int32_t round_days(int64_t minutes) {
 }
 
 // ------------------------------------------------- timetable accessors
+// the real-time overlay (rt_timetable, rt/rt_timetable.h:48-311): the
+// description and the lookups rt_timetable keeps (changed traffic days by
+// transport, location_rt_transports_)
+struct rt_overlay {
+  b2r_rt_desc const* d{nullptr};
+  std::unordered_map<uint32_t, uint32_t> changed;  // transport -> its row of changed_days
+  std::vector<uint32_t> loc_idx, loc_rt;            // location_rt_transports_ (CSR)
+
+  rt_overlay(b2r_rt_desc const* desc, uint32_t n_loc) : d{desc} {
+    if (d == nullptr) return;
+    for (auto i = 0U; i != d->n_changed; ++i) changed[d->changed_transport[i]] = i;
+    std::vector<std::vector<uint32_t>> by_loc(n_loc);
+    for (auto x = 0U; x != d->n_rt_transports; ++x) {
+      for (auto i = d->rt_stop_index[x]; i != d->rt_stop_index[x + 1]; ++i) {
+        auto const l = B2R_STOP_LOC(d->rt_stops[i]);
+        if (by_loc[l].empty() || by_loc[l].back() != x) by_loc[l].push_back(x);
+      }
+    }
+    loc_idx.assign(n_loc + 1U, 0U);
+    for (auto l = 0U; l != n_loc; ++l) {
+      loc_idx[l + 1U] = loc_idx[l] + static_cast<uint32_t>(by_loc[l].size());
+      loc_rt.insert(loc_rt.end(), by_loc[l].begin(), by_loc[l].end());
+    }
+  }
+};
+
 struct tt_view {
   b2r_timetable_desc const& d;
   uint32_t prf{0};  // the query's footpath profile (query::prf_idx_)
+  rt_overlay const* rt{nullptr};
   mutable std::vector<uint32_t> zero_{};
 
   // footpaths_out_[prf] (out) or footpaths_in_[prf] (timetable.h:97-98) and
@@ -109,8 +136,35 @@ struct tt_view {
     if (i >= B2R_MAX_DAYS) return false;
     return ((d.bitfields[8ull * bf + i / 64] >> (i % 64)) & 1ULL) != 0ULL;
   }
+  // timetable / rt_timetable::is_transport_active (rt_timetable.h:210-213):
+  // the overlay's days for a transport it changed
   bool transport_active(uint32_t t, uint16_t day) const {
+    if (has_rt()) {
+      auto const it = rt->changed.find(t);
+      if (it != rt->changed.end()) {
+        return day < B2R_MAX_DAYS && ((rt->d->changed_days[8ull * it->second + day / 64] >> (day % 64)) & 1ULL);
+      }
+    }
     return bf_test(d.transport_traffic_days[t], day);
+  }
+  // rt transports: stop sequence, unix event times (rt_timetable::
+  // unix_event_time), class, flags and section flags
+  bool has_rt() const { return rt != nullptr && rt->d != nullptr; }
+  uint32_t n_rt() const { return has_rt() ? rt->d->n_rt_transports : 0U; }
+  uint32_t rt_n_stops(uint32_t x) const { return rt->d->rt_stop_index[x + 1] - rt->d->rt_stop_index[x]; }
+  uint32_t rt_stop(uint32_t x, uint32_t i) const { return rt->d->rt_stops[rt->d->rt_stop_index[x] + i]; }
+  unixtime rt_event(uint32_t x, uint32_t i, bool arr) const {
+    return rt->d->rt_event_times[2ull * (rt->d->rt_stop_index[x] - x) + 2ull * i - (arr ? 1U : 0U)];
+  }
+  uint8_t rt_clasz(uint32_t x) const { return rt->d->rt_clasz == nullptr ? 10U : rt->d->rt_clasz[x]; }
+  uint8_t rt_flags(uint32_t x) const { return rt->d->rt_flags == nullptr ? 0U : rt->d->rt_flags[x]; }
+  uint8_t rt_section_flags(uint32_t x, uint32_t section) const {
+    return rt->d->rt_section_flags == nullptr ? 0U : rt->d->rt_section_flags[rt->d->rt_stop_index[x] + section];
+  }
+  template <typename Fn>
+  void location_rt(uint32_t l, Fn&& fn) const {
+    if (!has_rt()) return;
+    for (auto i = rt->loc_idx[l]; i != rt->loc_idx[l + 1]; ++i) fn(rt->loc_rt[i]);
   }
   bool route_active(uint32_t r, uint16_t day) const {
     return bf_test(d.route_traffic_days[r], day);
@@ -341,6 +395,7 @@ struct leg_t {
   uint32_t target{0};
   int16_t duration{0};
   int32_t mode_id{0};
+  uint32_t rt_transport{kInvalidIdx};  // rt::run::rt_ of a real-time run
 };
 
 // journey::leg ctor, journey.h:45-60
@@ -354,6 +409,7 @@ leg_t make_leg(bool fwd, uint32_t a, uint32_t b, unixtime ta, unixtime tb) {
 }
 void set_run(leg_t& l, uint32_t t, uint16_t day, uint16_t a, uint16_t b) {
   l.kind = B2R_LEG_TRANSPORT;
+  l.rt_transport = kInvalidIdx;
   l.transport = t;
   l.day = day;
   l.stop_from = std::min(a, b);
@@ -459,6 +515,23 @@ bool route_allowed(tt_view const& tt, uint32_t allowed_claszes, uint8_t required
   return true;
 }
 
+// the same filters for rt transport x: the class of its first section and
+// its route flags (raptor.h:583-626, reconstruct.cc:382-429)
+bool rt_allowed(tt_view const& tt, uint32_t allowed_claszes, uint8_t required_flags,
+                uint32_t x, uint8_t& sections) {
+  sections = 0U;
+  auto const c = tt.rt_clasz(x);
+  if (c >= 32U || ((allowed_claszes >> c) & 1U) == 0U) return false;
+  auto const fl = tt.rt_flags(x);
+  for (auto f = 0U; f != 4U; ++f) {
+    if (((required_flags >> f) & 1U) == 0U) continue;
+    if ((fl >> (2U * f)) & 1U) continue;
+    if (((fl >> (2U * f + 1U)) & 1U) == 0U) return false;
+    sections = static_cast<uint8_t>(sections | (1U << f));
+  }
+  return true;
+}
+
 // whether the section from stop s to stop s + 1 of route r carries every
 // flag in `sections`
 bool section_ok(tt_view const& tt, uint32_t r, uint32_t s, uint8_t sections) {
@@ -473,7 +546,7 @@ struct raptor_t {
   bool one_to_all;
   uint32_t n_loc, n_routes;
   std::vector<delta_t> tmp, best, rt;  // rt[k * n_loc + l]
-  bitvec station_mark, prev_station_mark, route_mark;
+  bitvec station_mark, prev_station_mark, route_mark, rt_transport_mark;
   bitvec const& is_dest;
   std::vector<uint16_t> const& dist_to_end;
   std::vector<uint16_t> const& lb;
@@ -516,6 +589,7 @@ struct raptor_t {
     station_mark.resize(n_loc);
     prev_station_mark.resize(n_loc);
     route_mark.resize(n_routes);
+    rt_transport_mark.resize(std::max(1U, t.n_rt()));
     reset_arrivals();
     if (!dist_to_end.empty()) {  // raptor.h:101-112
       end_reachable.resize(n_loc);
@@ -538,6 +612,7 @@ struct raptor_t {
     prev_station_mark.clear();
     station_mark.clear();
     route_mark.clear();
+    rt_transport_mark.clear();
   }
 
   void add_start(uint32_t l, unixtime t) {  // raptor.h:190-203
@@ -613,6 +688,10 @@ struct raptor_t {
           any_marked = true;
           route_mark.set(tt.d.location_routes[ri]);
         }
+        tt.location_rt(i, [&](uint32_t x) {  // raptor.h:234-240
+          any_marked = true;
+          rt_transport_mark.set(x);
+        });
       });
       if (!any_marked) break;
 
@@ -625,9 +704,16 @@ struct raptor_t {
         ++st.n_routes_visited;
         any_marked |= update_route(k, r, sections);
       });
+      rt_transport_mark.for_each([&](uint32_t x) {  // loop_rt_routes, raptor.h:577-678
+        uint8_t sections = 0U;
+        if (!rt_allowed(tt, allowed_claszes, required_flags, x, sections)) return;
+        ++st.n_routes_visited;
+        any_marked |= update_rt_transport(k, x, sections);
+      });
       if (!any_marked) break;
 
       route_mark.clear();
+      rt_transport_mark.clear();
       std::swap(prev_station_mark, station_mark);
       station_mark.clear();
 
@@ -802,6 +888,43 @@ struct raptor_t {
     return any_marked;
   }
 
+  // update_rt_transport, raptor.h:1068-1175 (no vias): et is whether the
+  // query rides the run when it passes the stop
+  bool update_rt_transport(unsigned k, uint32_t x, uint8_t sections) {
+    auto const n_stops = tt.rt_n_stops(x);
+    auto any_marked = false;
+    auto et = false;
+    st.n_route_stops_visited += n_stops;
+    for (auto i = 0U; i != n_stops; ++i) {
+      auto const stop_idx = fwd ? i : n_stops - i - 1U;
+      auto const stp = tt.rt_stop(x, stop_idx);
+      auto const l = B2R_STOP_LOC(stp);
+      auto const is_last = i == n_stops - 1U;
+      if (sections != 0U && i != 0U &&
+          (tt.rt_section_flags(x, fwd ? stop_idx - 1U : stop_idx) & sections) != sections) {
+        et = false;
+      }
+      if ((fwd && stop_idx != 0U) || (!fwd && stop_idx != n_stops - 1U)) {
+        auto const by_transport = unix_to_delta(base_days(), tt.rt_event(x, stop_idx, fwd));
+        if (et && (fwd ? tt.stop_out(stp) : tt.stop_in(stp))) {
+          if (is_better_or_eq(by_transport, time_at_dest[k]) && lb_reachable(l) &&
+              is_better_or_eq(by_transport + dir(get_lb(l)), time_at_dest[k]) &&
+              within_bounds(k, l, by_transport)) {
+            tmp[l] = static_cast<delta_t>(get_best(by_transport, tmp[l]));
+            ++st.n_label_writes;
+            station_mark.set(l);
+            any_marked = true;
+          }
+        }
+      }
+      if (!lb_reachable(l)) break;
+      if (is_last || !(fwd ? tt.stop_in(stp) : tt.stop_out(stp)) || !prev_station_mark.test(l)) continue;
+      auto const by_transport = unix_to_delta(base_days(), tt.rt_event(x, stop_idx, !fwd));
+      if (is_better_or_eq(RT(k - 1, l), by_transport)) et = true;
+    }
+    return any_marked;
+  }
+
   // raptor.h:1351-1442
   bool get_earliest_transport(unsigned k, uint32_t r, uint32_t stop_idx,
                               uint16_t day_at_stop, int16_t mam_at_stop,
@@ -873,13 +996,13 @@ void add_start_times_at_stop(tt_view const& tt, bool fwd, uint32_t r,
   auto const first_day = tt.day_idx_mam(iv_at_stop.from).first;
   auto const last_day = tt.day_idx_mam(iv_at_stop.to).first;
   for (auto t = tt.d.route_transport_from[r]; t != tt.d.route_transport_to[r]; ++t) {
-    auto const bf = tt.d.transport_traffic_days[t];
     auto const ev = tt.event_mam(t, stop_idx, !fwd);
     auto const cnt = static_cast<int16_t>(B2R_DELTA_DAYS(ev) * 1440 + B2R_DELTA_MAM(ev));
     auto const day_offset = static_cast<uint16_t>(cnt / 1440);
     auto const stop_time_mam = cnt % 1440;
     for (auto day = first_day; day <= last_day; ++day) {
-      if (tt.bf_test(bf, static_cast<uint16_t>(day - day_offset)) &&
+      // the overlay's traffic days where it changed them (start_times.cc:64-65)
+      if (tt.transport_active(t, static_cast<uint16_t>(day - day_offset)) &&
           iv_at_stop.contains(tt.to_unixtime(day, stop_time_mam))) {
         auto const ev_time = tt.to_unixtime(day, stop_time_mam);
         auto const d = offset;
@@ -919,6 +1042,19 @@ void add_starts_in_interval(tt_view const& tt, bool fwd, interval_t const& iv,
           offset, starts);
     }
   }
+  // real-time starts, start_times.cc:177-215
+  tt.location_rt(l, [&](uint32_t x) {
+    auto const n = tt.rt_n_stops(x);
+    for (auto i = 0U; i != n; ++i) {
+      auto const stp = tt.rt_stop(x, i);
+      if (B2R_STOP_LOC(stp) != l) continue;
+      if ((!fwd && (i == 0U || !tt.stop_out(stp))) || (fwd && (i == n - 1U || !tt.stop_in(stp)))) continue;
+      auto const ev_time = tt.rt_event(x, i, !fwd);
+      auto const time_at_start = fwd ? ev_time - offset : ev_time + offset;
+      if (!iv.contains(time_at_start)) continue;
+      starts.push_back({time_at_start, ev_time, l});
+    }
+  });
   if (add_ontrip) {
     auto const time_at_start = fwd ? iv.to : iv.from - 1;
     auto const d = offset;
@@ -1198,6 +1334,38 @@ struct reconstructor {
     return std::nullopt;
   }
 
+  // find_start_in_prev_round (reconstruct.cc:186-280) on a real-time run:
+  // its own stops and event times (rt::frun::from_rt)
+  std::optional<leg_t> find_start_in_prev_round_rt(unsigned k, uint32_t x, uint32_t finish, uint8_t sections) {
+    auto const size = tt.rt_n_stops(x);
+    auto const n_stops = fwd ? finish + 1U : size - finish;
+    for (auto i = 1U; i < n_stops; ++i) {
+      auto const stop_idx = fwd ? finish - i : finish + i;
+      auto const stp = tt.rt_stop(x, stop_idx);
+      auto const l = B2R_STOP_LOC(stp);
+      if (sections != 0U &&
+          (tt.rt_section_flags(x, fwd ? stop_idx : stop_idx - 1U) & sections) != sections) {
+        break;
+      }
+      if ((fwd && !B2R_STOP_IN(stp)) || (!fwd && !B2R_STOP_OUT(stp))) continue;
+      auto const event_time = unix_to_delta(base, tt.rt_event(x, stop_idx, !fwd));
+      auto const round_time = rt(k - 1, l);
+      if (better_eq(round_time, event_time) ||
+          (k == 1 && q.start_mode == B2R_MATCH_EQUIVALENT && is_journey_start(l) &&
+           start_matches(round_time, event_time))) {
+        auto leg = make_leg(fwd, l, B2R_STOP_LOC(tt.rt_stop(x, finish)), delta_to_unix(base, event_time),
+                            tt.rt_event(x, finish, fwd));
+        auto const st = tt.rt->d->rt_static_transport;
+        set_run(leg, st != nullptr ? st[x] : kInvalidIdx,
+                tt.rt->d->rt_static_day != nullptr ? tt.rt->d->rt_static_day[x] : uint16_t{0},
+                static_cast<uint16_t>(stop_idx), static_cast<uint16_t>(finish));
+        leg.rt_transport = x;
+        return leg;
+      }
+    }
+    return std::nullopt;
+  }
+
   // reconstruct.cc:292-373
   std::optional<leg_t> get_route_transport(unsigned k, delta_t time, uint32_t r,
                                            uint32_t stop_idx, uint8_t sections) {
@@ -1215,8 +1383,26 @@ struct reconstructor {
     return std::nullopt;
   }
 
-  // reconstruct.cc:375-545 (no rtt)
+  // reconstruct.cc:375-545: real-time runs first (381-452; an earlier
+  // arrival than the label is accepted), then the routes
   std::optional<leg_t> get_transport(unsigned k, uint32_t l, delta_t time) {
+    std::optional<leg_t> found;
+    tt.location_rt(l, [&](uint32_t x) {
+      if (found.has_value()) return;
+      uint8_t sections = 0U;
+      if (!rt_allowed(tt, q.allowed_claszes, q.required_flags, x, sections)) return;
+      auto const n = tt.rt_n_stops(x);
+      for (auto i = 0U; i != n && !found.has_value(); ++i) {
+        auto const stp = tt.rt_stop(x, i);
+        if (B2R_STOP_LOC(stp) != l || (fwd && (i == 0U || !B2R_STOP_OUT(stp))) ||
+            (!fwd && (i == n - 1U || !B2R_STOP_IN(stp))) ||
+            !better_eq(tt.rt_event(x, i, fwd), delta_to_unix(base, time))) {
+          continue;
+        }
+        found = find_start_in_prev_round_rt(k, x, i, sections);
+      }
+    });
+    if (found.has_value()) return found;
     for (auto ri = tt.d.location_routes_index[l]; ri != tt.d.location_routes_index[l + 1];
          ++ri) {
       auto const r = tt.d.location_routes[ri];
@@ -2216,11 +2402,16 @@ thread_local std::string g_error;  // what the last failed or_search threw
 extern "C" {
 
 int or_search(const b2r_timetable_desc* tt, const b2r_query* q, or_result** out) {
+  return or_search_rt(tt, nullptr, q, out);
+}
+
+int or_search_rt(const b2r_timetable_desc* tt, const b2r_rt_desc* rtd, const b2r_query* q, or_result** out) {
   if (tt == nullptr || q == nullptr || out == nullptr) return B2R_ERR_INVALID_ARGUMENT;
   if (q->prf_idx >= B2R_N_PROFILES) return B2R_ERR_INVALID_ARGUMENT;  // profile_idx_t < kNProfiles
   try {
     auto res = std::make_unique<or_result>();
-    oracle::tt_view const v{*tt, q->prf_idx};
+    oracle::rt_overlay const ov{rtd, tt->n_locations};
+    oracle::tt_view const v{*tt, q->prf_idx, rtd != nullptr ? &ov : nullptr};
     auto const qq = oracle::to_query(*q);
     auto const fwd = q->direction == B2R_FORWARD;
     if (q->kind == B2R_ONE_TO_ALL) {
@@ -2250,11 +2441,13 @@ int or_search(const b2r_timetable_desc* tt, const b2r_query* q, or_result** out)
         bl.dep_time = l.dep;
         bl.arr_time = l.arr;
         bl.kind = l.kind;
+        bl.rt_transport = B2R_INVALID_IDX;
         if (l.kind == B2R_LEG_TRANSPORT) {
           bl.transport = l.transport;
           bl.day = l.day;
           bl.stop_from = l.stop_from;
           bl.stop_to = l.stop_to;
+          bl.rt_transport = l.rt_transport;
         } else {
           bl.transport = l.target;
           bl.duration = l.duration;
@@ -2324,6 +2517,7 @@ int or_earliest_alternative(const b2r_timetable_desc* tt, const b2r_query* q, ui
       bl.dep_time = l.dep;
       bl.arr_time = l.arr;
       bl.kind = l.kind;
+      bl.rt_transport = B2R_INVALID_IDX;
       if (l.kind == B2R_LEG_TRANSPORT) {
         bl.transport = l.transport;
         bl.day = l.day;

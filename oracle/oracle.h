@@ -14,7 +14,9 @@
  *   src/routing/dijkstra.cc:18-67, dijkstra.h:31-70 (lower bounds)
  *   src/routing/get_fastest_direct.cc:12-100
  *   include/nigiri/routing/interval_estimate.h:12-151
- *   src/routing/raptor/reconstruct.cc:22-160, 162-877 (Vias = 0, no rtt)
+ *   src/routing/raptor/reconstruct.cc:22-160, 162-877 (Vias = 0)
+ *   raptor.h:1068-1175 (update_rt_transport), rt branches of raptor.h,
+ *     start_times.cc:40-215 and reconstruct.cc:297-452 (Rt = true)
  *   src/routing/raptor/optimize_footpaths.cc:15-457
  *   src/routing/one_to_all.cc:26-104
  *   include/nigiri/routing/pareto_set.h:21-37, journey.h:84-118
@@ -53,6 +55,10 @@ typedef struct or_stats {
 /* Run one query exactly as raptor_search / one_to_all would. */
 int or_search(const b2r_timetable_desc* tt, const b2r_query* q,
               or_result** out);
+/* The same with a real-time overlay (raptor<Dir, Rt = true>, the rt
+ * branches of start_times.cc and reconstruct.cc); rt may be NULL. */
+int or_search_rt(const b2r_timetable_desc* tt, const b2r_rt_desc* rt,
+                 const b2r_query* q, or_result** out);
 int or_result_view(const or_result* r, b2r_result* view, or_stats* stats);
 /* Final raptor_state: round_times [B2R_K][n_locations] and best
  * [n_locations] as int16 deltas (for state-level parity). */

@@ -24,16 +24,19 @@ b2r_leg c_leg(r::leg const& l) {
     x.day = t->day_;
     x.stop_from = t->stop_from_;
     x.stop_to = t->stop_to_;
+    x.rt_transport = t->rt_transport_;
   } else if (auto const* f = std::get_if<r::footpath>(&l.uses_)) {
     x.kind = B2R_LEG_FOOTPATH;
     x.transport = f->target_;
     x.duration = f->duration_;
+    x.rt_transport = B2R_INVALID_IDX;
   } else {
     auto const& o = std::get<r::offset>(l.uses_);
     x.kind = B2R_LEG_OFFSET;
     x.transport = o.target_;
     x.duration = o.duration_;
     x.transport_mode_id = o.transport_mode_id_;
+    x.rt_transport = B2R_INVALID_IDX;
   }
   return x;
 }

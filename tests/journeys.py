@@ -14,7 +14,7 @@ def records(res: A.Result, name_of=None, transport_name=None):
             L = res.legs[li]
             leg = (L.kind, nm(L.from_), nm(L.to), L.dep_time, L.arr_time)
             if L.kind == A.B2R_LEG_TRANSPORT:
-                leg += (L.transport, L.day, L.stop_from, L.stop_to)
+                leg += (L.transport, L.day, L.stop_from, L.stop_to, L.rt_transport)
             else:
                 leg += (L.transport, L.duration, L.transport_mode_id)
             rec["legs"].append(leg)

@@ -35,6 +35,7 @@ int main() {
          sizeof(b2r_query), sizeof(b2r_leg), sizeof(b2r_journey), sizeof(b2r_result),
          sizeof(b2r_engine_config), sizeof(b2r_batch_stats), sizeof(b2r_tt_base),
          sizeof(b2r_launch_shape), sizeof(b2r_tune_report), sizeof(b2r_gtfs_config));
+  printf("%zu %zu\n", sizeof(b2r_rt_desc), offsetof(b2r_leg, rt_transport));
   printf("%zu %zu %zu\n", offsetof(b2r_query, tts_factor), offsetof(b2r_leg, transport_mode_id),
          offsetof(b2r_result, n_start_times));
   return 0;
@@ -51,7 +52,9 @@ int main() {
                      C.sizeof(A.Leg), C.sizeof(A.Journey), C.sizeof(A.Result),
                      C.sizeof(A.EngineConfig), C.sizeof(A.BatchStats), C.sizeof(A.TtBase),
                      C.sizeof(A.LaunchShape), C.sizeof(A.TuneReport), C.sizeof(A.GtfsConfig)]
-    offs = [int(x) for x in out[1].split()]
+    rt = [int(x) for x in out[1].split()]
+    assert rt == [C.sizeof(A.RtDesc), A.Leg.rt_transport.offset]
+    offs = [int(x) for x in out[2].split()]
     assert offs == [A.Query.tts_factor.offset, A.Leg.transport_mode_id.offset,
                     A.Result.n_start_times.offset]
 
