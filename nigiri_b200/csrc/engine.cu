@@ -497,6 +497,16 @@ namespace {
 
 using dev::slot_t;
 
+// An event record that becomes an event node of the graph when the stream
+// is being captured (a plain record inside a capture only orders streams),
+// so that its time can be read after every launch of the graph.
+cudaError_t record_in_graph(cudaEvent_t ev, cudaStream_t s) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (auto const rc = cudaStreamIsCapturing(s, &cs); rc != cudaSuccess) return rc;
+  return cs == cudaStreamCaptureStatusActive ? cudaEventRecordWithFlags(ev, s, cudaEventRecordExternal)
+                                             : cudaEventRecord(ev, s);
+}
+
 // ------------------------------------------------------------- super-step
 void enqueue_superstep(b2r_engine& e, cudaStream_t s) {
   auto const& st = e.st;
@@ -515,7 +525,7 @@ void enqueue_superstep(b2r_engine& e, cudaStream_t s) {
   dev::k_ctl_marked<<<slot_blocks, 128, 0, s>>>(st);
   cudaEvent_t ev_a = nullptr, ev_b = nullptr;
   if (e.cfg.profile == 2U) {  // timing build: one event pair, captured in the super-step graph
-    B2R_CUDA(cudaEventRecord(e.ev_scan_a, s));
+    B2R_CUDA(record_in_graph(e.ev_scan_a, s));
   } else if (e.cfg.profile) {  // CUDA events on the launching stream around the scan
     while (e.prof_used + 2 > e.prof_ev.size()) {
       cudaEvent_t x;
@@ -540,7 +550,7 @@ void enqueue_superstep(b2r_engine& e, cudaStream_t s) {
     }
   }
   if (e.cfg.profile == 2U) {
-    B2R_CUDA(cudaEventRecord(e.ev_scan_b, s));
+    B2R_CUDA(record_in_graph(e.ev_scan_b, s));
   } else if (e.cfg.profile) {
     B2R_CUDA(cudaEventRecord(ev_b, s));
     auto const idx = static_cast<uint32_t>(e.prof_used / 2 - 1);

@@ -509,11 +509,24 @@ struct recon_ctx {
   }
 
   // ---------------------------------------------- optimize_footpaths.cc
+  // the stops and event times of a leg's run (rt::frun): a real-time run's
+  // own, else the static trip's
   __device__ uint32_t r_of(b2r_leg const& l) const { return T->transport_route[l.transport]; }
-  __device__ uint32_t loc_at(b2r_leg const& l, uint32_t si) const { return B2R_STOP_LOC(stopw(r_of(l), si)); }
-  __device__ uint32_t word_at(b2r_leg const& l, uint32_t si) const { return stopw(r_of(l), si); }
+  __device__ uint32_t word_at(b2r_leg const& l, uint32_t si) const {
+    if (l.rt_transport != B2R_INVALID_IDX) return T->rt_stops[T->rt_stop_idx[l.rt_transport] + si];
+    return stopw(r_of(l), si);
+  }
+  __device__ uint32_t loc_at(b2r_leg const& l, uint32_t si) const { return B2R_STOP_LOC(word_at(l, si)); }
   __device__ int32_t time_at(b2r_leg const& l, uint32_t si, bool arr) const {
+    if (l.rt_transport != B2R_INVALID_IDX) {
+      auto const x = l.rt_transport;
+      return T->rt_times[2ull * (T->rt_stop_idx[x] - x) + 2u * si - (arr ? 1u : 0u)];
+    }
     return ev_time(l.transport, l.day, si, arr);
+  }
+  __device__ uint32_t run_size(b2r_leg const& l) const {
+    if (l.rt_transport != B2R_INVALID_IDX) return T->rt_stop_idx[l.rt_transport + 1] - T->rt_stop_idx[l.rt_transport];
+    return n_stops(r_of(l));
   }
 
   // optimize_footpaths.cc:15-60; `offs` = start offsets of the journey query
@@ -586,7 +599,7 @@ struct recon_ctx {
     auto& tl = legs[n_legs - 2];
     auto best = static_cast<int>(ol.duration);
     auto const from = static_cast<uint32_t>(tl.stop_from + 1u);
-    auto const size = n_stops(r_of(tl));
+    auto const size = run_size(tl);
     for (auto si = from; si < size; ++si) {
       if (!B2R_STOP_OUT(word_at(tl, si))) continue;
       for (auto i = 0u; i != n_offs; ++i) {
@@ -617,7 +630,7 @@ struct recon_ctx {
     auto const dest_loc = fl.to;
     auto best = static_cast<int>(adjusted<int16_t>(sl->tts, fl.duration));
     auto const from = static_cast<uint32_t>(tl.stop_from + 1u);
-    auto const size = n_stops(r_of(tl));
+    auto const size = run_size(tl);
     for (auto si = from; si < size; ++si) {
       if (!B2R_STOP_OUT(word_at(tl, si))) continue;
       auto const* iidx = fp_index(*T, sl->prf, false);  // optimize_footpaths.cc:215
@@ -674,7 +687,7 @@ struct recon_ctx {
       auto const lt = legs[i + 2];
       if (lf.kind != B2R_LEG_TRANSPORT || lp.kind != B2R_LEG_FOOTPATH || lt.kind != B2R_LEG_TRANSPORT) continue;
       auto const from_start = static_cast<uint32_t>(lf.stop_from + 1u);
-      auto const from_size = n_stops(r_of(lf));
+      auto const from_size = run_size(lf);
       auto const to_end = static_cast<uint32_t>(lt.stop_to - 1u);
       auto const pbest0 = penalty(lp.duration, lt.dep_time - lp.arr_time, lf.from, lt.to);
       auto const n_sf = from_size > from_start ? from_size - from_start : 0u;

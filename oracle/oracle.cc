@@ -1555,16 +1555,19 @@ struct reconstructor {
   }
 
   // ---------------------------------------------- optimize_footpaths.cc
+  // the stops and event times of a leg's run (rt::frun: a real-time run's
+  // own, else the static trip's)
   unixtime stime(leg_t const& transport_leg, uint32_t s, bool arr) const {
+    if (transport_leg.rt_transport != kInvalidIdx) return tt.rt_event(transport_leg.rt_transport, s, arr);
     return tt.event_time(transport_leg.transport, transport_leg.day, s, arr);
   }
-  uint32_t sloc(leg_t const& transport_leg, uint32_t s) const {
-    return B2R_STOP_LOC(tt.stop(tt.d.transport_route[transport_leg.transport], s));
-  }
   uint32_t sword(leg_t const& transport_leg, uint32_t s) const {
+    if (transport_leg.rt_transport != kInvalidIdx) return tt.rt_stop(transport_leg.rt_transport, s);
     return tt.stop(tt.d.transport_route[transport_leg.transport], s);
   }
+  uint32_t sloc(leg_t const& transport_leg, uint32_t s) const { return B2R_STOP_LOC(sword(transport_leg, s)); }
   uint32_t run_size(leg_t const& transport_leg) const {
+    if (transport_leg.rt_transport != kInvalidIdx) return tt.rt_n_stops(transport_leg.rt_transport);
     return tt.n_stops(tt.d.transport_route[transport_leg.transport]);
   }
 

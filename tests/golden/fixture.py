@@ -263,7 +263,8 @@ def journeys_to_records(tt: FixtureTimetable, res: A.Result):
             if L.kind == A.B2R_LEG_TRANSPORT:
                 leg["kind"] = "transport"
                 leg["n_stops"] = L.stop_to - L.stop_from
-                leg["trip_name"] = tt.transport_names[L.transport]
+                # an added real-time trip runs for no static trip
+                leg["trip_name"] = None if L.transport == 0xFFFFFFFF else tt.transport_names[L.transport]
             elif L.kind == A.B2R_LEG_FOOTPATH:
                 leg["kind"] = "footpath"
                 leg["duration"] = L.duration
@@ -296,7 +297,7 @@ def strip_expected(expected, names_by_trip=None):
             x = {k: leg[k] for k in ("from", "to", "dep", "arr", "kind")}
             if leg["kind"] == "transport":
                 x["n_stops"] = leg["n_stops"]
-                x["trip_name"] = leg["trip_name"]
+                x["trip_name"] = leg.get("trip_name")
             elif leg["kind"] == "footpath":
                 x["duration"] = leg["duration"]
             else:
@@ -305,3 +306,88 @@ def strip_expected(expected, names_by_trip=None):
             r["legs"].append(x)
         out.append(r)
     return out
+
+
+class RtOverlay:
+    """A b2r_rt_desc and the arrays it points to.  changed: (transport,
+    8 uint64 day words) pairs; runs: dicts with stop words, times (minutes
+    since the epoch, rt_transport_stop_times_ order), static transport and
+    day, and optionally clasz, flags and section flags."""
+
+    def __init__(self, changed, runs):
+        import numpy as np
+        self.changed_t = np.array([c[0] for c in changed] or [0], np.uint32)
+        self.changed_d = np.array([w for c in changed for w in c[1]] or [0], np.uint64)
+        idx, stops, times, st, sd, cl, fl, sec = [0], [], [], [], [], [], [], []
+        for r in runs:
+            assert len(r["times"]) == 2 * (len(r["stops"]) - 1)
+            stops += r["stops"]
+            idx.append(len(stops))
+            times += r["times"]
+            st.append(r.get("static_transport", 0xFFFFFFFF))
+            sd.append(r.get("static_day", 0))
+            cl.append(r.get("clasz", 10))
+            fl.append(r.get("flags", 0))
+            sec += r.get("section_flags", [0] * len(r["stops"]))
+        self.arrays = [np.array(idx, np.uint32), np.array(stops or [0], np.uint32),
+                       np.array(times or [0], np.int32), np.array(st or [0], np.uint32),
+                       np.array(sd or [0], np.uint16), np.array(cl or [0], np.uint8),
+                       np.array(fl or [0], np.uint8), np.array(sec or [0], np.uint8)]
+        a = self.arrays
+        p = lambda arr, t: arr.ctypes.data_as(C.POINTER(t))
+        self.desc = A.RtDesc()
+        self.desc.n_changed = len(changed)
+        self.desc.changed_transport = p(self.changed_t, C.c_uint32)
+        self.desc.changed_days = p(self.changed_d, C.c_uint64)
+        self.desc.n_rt_transports = len(runs)
+        self.desc.rt_stop_index = p(a[0], C.c_uint32)
+        self.desc.rt_stops = p(a[1], C.c_uint32)
+        self.desc.rt_event_times = p(a[2], C.c_int32)
+        self.desc.rt_static_transport = p(a[3], C.c_uint32)
+        self.desc.rt_static_day = p(a[4], C.c_uint16)
+        self.desc.rt_clasz = p(a[5], C.c_uint8)
+        self.desc.rt_flags = p(a[6], C.c_uint8)
+        self.desc.rt_section_flags = p(a[7], C.c_uint8)
+
+
+def stop_word(loc):
+    """A stop word with every in / out bit set (an added run's stops)."""
+    return loc | (0xF << 28)
+
+
+def transport_days(desc, t):
+    """The 8 day words of transport t's static traffic days."""
+    bf = desc.transport_traffic_days[t]
+    return [desc.bitfields[8 * bf + i] for i in range(8)]
+
+
+def rt_overlay_of_case(tt, spec):
+    """The overlay a rt case restates, on the timetable the reader built:
+    trips named by route short name, days as UTC dates."""
+    d = tt.desc
+    first = d.date_range_from - 5
+
+    def day_idx(s):
+        return _day(s) - first
+
+    def transport(name):
+        xs = [i for i, n in enumerate(tt.transport_names) if n == name]
+        assert len(xs) == 1, (name, xs)
+        return xs[0]
+
+    changed = []
+    for c in spec["changed"]:
+        t = transport(c["trip_name"])
+        words = transport_days(d, t)
+        if not c["runs"]:
+            di = day_idx(c["day"])
+            words[di // 64] &= ~(1 << (di % 64))
+        changed.append((t, words))
+    runs = []
+    for r in spec["runs"]:
+        run = dict(stops=[stop_word(tt.loc_idx[x]) for x in r["stops"]], times=r["times"])
+        if r["trip_name"] is not None:
+            run["static_transport"] = transport(r["trip_name"])
+            run["static_day"] = day_idx(r["day"])
+        runs.append(run)
+    return RtOverlay(changed, runs)

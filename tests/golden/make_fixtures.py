@@ -709,7 +709,42 @@ GTFS_ONLY_FEEDS = {
                           ["2024-06-16", "2024-06-19"]),
     "gtfs_max_interval": ("test/routing/max_interval_test.cc", "test_files()", 0, {},
                           ["2019-03-25", "2019-11-01"]),
+    "gtfs_rt_routing": ("test/routing/rt_routing_test.cc", "test_files()", 0, {},
+                        ["2019-03-25", "2019-11-01"]),
 }
+
+
+RT_ROUTING = "test/routing/rt_routing_test.cc"
+
+
+def rt_cases():
+    """test/routing/rt_routing_test.cc: each test applies one GTFS-RT update
+    and runs an ontrip search.  The update is restated as the overlay it
+    leaves in rt_timetable (gtfsrt_update.cc), in UTC:
+    * rt_raptor_forward / _backward: RE 2 (T_RE2, 00:30 local on 2019-05-03
+      = 22:30 UTC on its service day 2019-05-02) is 2 h late from its first
+      stop on; the delay carries to the later stops, so the run leaves B
+      00:30, passes C 00:45 and reaches D 01:00 UTC on 2019-05-03, and the
+      static trip no longer runs on 2019-05-02;
+    * rt_raptor_unscheduled: an added trip (NEW) from B 00:30 to D 01:00 UTC
+      on 2019-05-03 (stop_time_update times 1556843400 and 1556845200 s)."""
+    delayed = {"changed": [{"trip_name": "RE 2", "day": "2019-05-02", "runs": False}],
+               "runs": [{"trip_name": "RE 2", "day": "2019-05-02", "stops": ["B", "C", "D"],
+                         "times": [t("2019-05-03 00:30"), t("2019-05-03 00:45"), t("2019-05-03 00:45"),
+                                   t("2019-05-03 01:00")]}]}
+    added = {"changed": [],
+             "runs": [{"trip_name": None, "day": None, "stops": ["B", "D"],
+                       "times": [t("2019-05-03 00:30"), t("2019-05-03 01:00")]}]}
+    return [
+        dict(name="rt_raptor_forward", timetable="gtfs_rt_routing", ref=RT_ROUTING, golden="kFwdJourneys",
+             rt=delayed, query=dict(start=[["A", 0, 0]], dest=[["D", 0, 0]], start_time=t("2019-05-02 23:00"))),
+        dict(name="rt_raptor_backward", timetable="gtfs_rt_routing", ref=RT_ROUTING, golden="kBwdJourneys",
+             rt=delayed, query=dict(start=[["D", 0, 0]], dest=[["A", 0, 0]], start_time=t("2019-05-03 02:00"),
+                                    direction="bwd")),
+        dict(name="rt_raptor_unscheduled", timetable="gtfs_rt_routing", ref=RT_ROUTING,
+             golden="unscheduled_journeys", rt=added,
+             query=dict(start=[["A", 0, 0]], dest=[["D", 0, 0]], start_time=t("2019-05-02 23:00"))),
+    ]
 
 
 def gtfs_only_cases():
@@ -828,7 +863,11 @@ def main(ref_root: str):
     for case in gtfs_only_cases():
         src = open(os.path.join(ref_root, case["ref"])).read()
         gtfs_cases.append(dict(case, expected=parse_journeys(raw_string(src, case["golden"]))))
-    doc = {"timetables": TIMETABLES, "cases": out_cases, "gtfs_cases": gtfs_cases,
+    rt = []
+    for case in rt_cases():
+        src = open(os.path.join(ref_root, case["ref"])).read()
+        rt.append(dict(case, expected=parse_journeys(raw_string(src, case["golden"]))))
+    doc = {"timetables": TIMETABLES, "cases": out_cases, "gtfs_cases": gtfs_cases, "rt_cases": rt,
            "gtfs_known_answers": gtfs_only_known_answers(),
            "gtfs_seated_cases": join_split_cases(ref_root),
            "known_answers": known_answers(ref_root), "gtfs_feeds": gtfs_feeds(ref_root),

@@ -31,6 +31,9 @@ def lib():
         vp = C.c_void_p
         L.or_search.argtypes = [C.POINTER(A.TimetableDesc), C.POINTER(A.Query), C.POINTER(vp)]
         L.or_search.restype = C.c_int
+        L.or_search_rt.argtypes = [C.POINTER(A.TimetableDesc), C.POINTER(A.RtDesc), C.POINTER(A.Query),
+                                   C.POINTER(vp)]
+        L.or_search_rt.restype = C.c_int
         L.or_result_view.argtypes = [vp, C.POINTER(A.Result), C.POINTER(OrStats)]
         L.or_result_state.argtypes = [vp, C.POINTER(C.POINTER(C.c_int16)),
                                       C.POINTER(C.POINTER(C.c_int16)), C.POINTER(C.c_int32)]
@@ -53,9 +56,13 @@ def lib():
 
 
 class OracleResult:
-    def __init__(self, desc, q):
+    def __init__(self, desc, q, rt=None):
+        """rt: a b2r_rt_desc (the real-time overlay) or None."""
         self.h = C.c_void_p()
-        rc = lib().or_search(C.byref(desc), C.byref(q), C.byref(self.h))
+        if rt is None:
+            rc = lib().or_search(C.byref(desc), C.byref(q), C.byref(self.h))
+        else:
+            rc = lib().or_search_rt(C.byref(desc), C.byref(rt), C.byref(q), C.byref(self.h))
         if rc != 0:
             raise RuntimeError(f"oracle failed: {rc} {lib().or_last_error().decode()}")
         self.view = A.Result()
@@ -86,7 +93,7 @@ class OracleResult:
             pass
 
 
-def answers(desc, qarr, idx, threads=None):
+def answers(desc, qarr, idx, threads=None, rt=None):
     """The oracle's complete answers for queries qarr[i], i in idx, computed
     on host threads (the oracle's calls release the interpreter lock):
     i -> ("journeys", records) or, for one-to-all queries, ("rows", base day,
@@ -97,7 +104,7 @@ def answers(desc, qarr, idx, threads=None):
 
     def one(i):
         q = qarr[i]
-        o = OracleResult(desc, q)
+        o = OracleResult(desc, q, rt)
         if q.kind == A.B2R_ONE_TO_ALL:
             rows, _, base_day = o.state()
             return i, ("rows", base_day, rows)
