@@ -661,8 +661,9 @@ def extras_legs(args, h, dtt, qs, B, local, shape):
     per_launch_bytes = st.route_scan_bytes / max(1, st.route_scan_launches)
     per_launch_s = tm.route_scan_ms / 1e3 / max(1, tm.route_scan_launches)
     traffic, cap = None, ncu_traffic_per_unit()
-    if cap is not None and cap.get("batch") == B and cap.get("shape") == [getattr(sh, f) for f, _ in
-                                                                          A.LaunchShape._fields_]:
+    # the capture's batch and route-scan build (the grid shape changes no
+    # DRAM traffic of the work, the build's spills could)
+    if cap is not None and cap.get("batch") == B and cap.get("shape", [None] * 6)[5] == sh.scan_occupancy:
         traffic = cap["dram_bytes_per_launch"]
     out["roofline"] = {
         "bound": "hbm", "achieved": per_launch_bytes / per_launch_s / 1e9, "peak": None,
