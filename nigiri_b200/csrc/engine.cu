@@ -1606,7 +1606,12 @@ struct batch_runner {
       // next chunk in flight unless every resident query has just finished
       size_t n_active = 0;
       for (uint32_t s = 0; s != S; ++s) n_active += (slot_q[s] >= 0 && !waiting[s]) ? 1U : 0U;
-      if (running() && done_slots.size() < n_active) launch_chunk();
+      // a finished pong phase is followed by the next phase of its sweep:
+      // that phase is staged from the export, so the next chunk waits for
+      // it instead of leaving the slot idle for a whole chunk
+      auto phase_follows = false;
+      for (auto const s : done_slots) phase_follows = phase_follows || runs[static_cast<size_t>(slot_q[s])].p.pong;
+      if (!phase_follows && running() && done_slots.size() < n_active) launch_chunk();
       if (done_slots.empty()) continue;
       auto const t_exp = std::chrono::steady_clock::now();
       std::vector<exported> ex;
