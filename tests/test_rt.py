@@ -48,12 +48,41 @@ def test_oracle_without_the_overlay_misses_the_delayed_connection(feed):
     assert F.journeys_to_records(feed, r.view) != F.strip_expected(case["expected"])
 
 
-def generated_overlay(h, seed, n_delayed=60, n_cancelled=30, n_added=30):
+def query_days(h, qs):
+    """The traffic day indices around the queries' start times."""
+    first = h.desc.date_range_from - 5
+    out = set()
+    for i in range(qs.n):
+        q = qs.arr[i]
+        t = q.interval_from if q.is_interval else q.start_time
+        d = t // 1440 - first
+        out.update((d - 1, d))
+    return sorted(x for x in out if 0 <= x < 512)
+
+
+def ridden_trips(answers):
+    """(transport, traffic day) of the static rides in oracle answers."""
+    out = []
+    for kind, recs in answers.values():
+        if kind != "journeys":
+            continue
+        for j in recs:
+            for leg in j["legs"]:
+                if leg[0] == A.B2R_LEG_TRANSPORT and leg[-1] == 0xFFFFFFFF:
+                    out.append((leg[5], leg[6]))
+    return sorted(set(out))
+
+
+def generated_overlay(h, seed, days_near, focus=(), n_delayed=600, n_cancelled=200, n_added=600):
     """A real-time state on a generated timetable: runs delayed from some
     stop on (later, never faster), runs cancelled, and added runs that copy
-    a trip's times shifted later.  The delayed and cancelled trips leave the
-    static schedule on their day."""
+    a trip's times shifted later, all on traffic days in `days_near`.  The
+    delayed and cancelled trips leave the static schedule on their day.
+    The trips in `focus` ((transport, day) pairs, e.g. the ones the static
+    answers ride) are changed first."""
     rnd = random.Random(seed)
+    near = set(days_near)
+    focus = list(focus)
     d = h.desc
     first = d.date_range_from - 5
     nr = d.n_routes
@@ -81,16 +110,26 @@ def generated_overlay(h, seed, n_delayed=60, n_cancelled=30, n_added=30):
                 out.append((first + day) * 1440 + (ev & 31) * 1440 + (ev >> 5))
         return out
 
-    while len(runs) + len(changed) < n_delayed + n_cancelled + n_added:
-        r = rnd.randrange(nr)
-        if tto[r] == tfrom[r]:
-            continue
-        t = rnd.randrange(int(tfrom[r]), int(tto[r]))
-        words, days = active_day(t)
-        days = [x for x in days if 20 <= x < 60]  # around the generated queries' dates
-        if not days or t in used:
-            continue
-        day = rnd.choice(days)
+    wanted = n_delayed + n_cancelled + n_added
+    for _ in range(200 * wanted):  # bounded: a timetable may have few such trips
+        if len(runs) + len(changed) >= wanted:
+            break
+        if focus:
+            t, day = focus.pop(0)
+            r = int(d.transport_route[t])
+            words, days = active_day(t)
+            if t in used or day not in days:
+                continue
+        else:
+            r = rnd.randrange(nr)
+            if tto[r] == tfrom[r]:
+                continue
+            t = rnd.randrange(int(tfrom[r]), int(tto[r]))
+            words, days = active_day(t)
+            days = [x for x in days if x in near]
+            if not days or t in used:
+                continue
+            day = rnd.choice(days)
         stops = [int(x) for x in rstops[int(rsi[r]):int(rsi[r + 1])]]
         times = trip_times(r, t, day)
         kind = rnd.randrange(3)
@@ -111,6 +150,21 @@ def generated_overlay(h, seed, n_delayed=60, n_cancelled=30, n_added=30):
                              times=[x + shift for x in times],
                              clasz=int(d.route_clasz[r]) if d.route_clasz else 10))
     return F.RtOverlay(sorted(changed.items()), runs)
+
+
+def test_oracle_rides_generated_real_time_runs():
+    """The generated overlay is ridden: on the city timetable some of the
+    oracle's journeys use real-time runs, and some answers change."""
+    h = HostTimetable.generate(1)
+    qs = QuerySet(h, 1, 60, seed=7001)
+    static = oracle_lib.answers(h.desc, qs.arr, range(qs.n))
+    ov = generated_overlay(h, 71, query_days(h, qs), focus=ridden_trips(static))
+    assert ov.desc.n_rt_transports >= 30 and ov.desc.n_changed >= 30
+    with_rt = oracle_lib.answers(h.desc, qs.arr, range(qs.n), rt=ov.desc)
+    rt_legs = sum(1 for i in range(qs.n) for j in with_rt[i][1] for leg in j["legs"]
+                  if leg[0] == A.B2R_LEG_TRANSPORT and leg[-1] != 0xFFFFFFFF)
+    assert rt_legs > 0
+    assert any(with_rt[i] != static[i] for i in range(qs.n))
 
 
 def bound_engine(desc, ov, max_slots=256):
@@ -151,9 +205,10 @@ def test_engine_rt_generated_matches_oracle(workload, n):
     one-to-all rows."""
     lib = A.lib()
     h = HostTimetable.generate(1 if workload == 1 else 2)
-    ov = generated_overlay(h, seed=70 + workload)
-    tt, eng, rt = bound_engine(h.desc, ov)
     qs = QuerySet(h, workload, n, seed=7000 + workload)
+    static = oracle_lib.answers(h.desc, qs.arr, range(qs.n))
+    ov = generated_overlay(h, 70 + workload, query_days(h, qs), focus=ridden_trips(static))
+    tt, eng, rt = bound_engine(h.desc, ov)
     arr = (A.Query * (qs.n + 8))()
     for i in range(qs.n):
         arr[i] = qs.arr[i]
