@@ -102,6 +102,69 @@ struct uninit_allocator : std::allocator<T> {
 };
 using row_vector = std::vector<int16_t, uninit_allocator<int16_t>>;
 
+// One-to-all rows of one result: page-locked host memory when the batch
+// path copies the rows straight into it from the device, else ordinary
+// heap memory (the serving loop, whose results live until b2r_release).
+class row_buf {
+ public:
+  row_buf() = default;
+  row_buf(row_buf const&) = delete;
+  row_buf& operator=(row_buf const&) = delete;
+  row_buf(row_buf&& o) noexcept { take(o); }
+  row_buf& operator=(row_buf&& o) noexcept {
+    if (this != &o) {
+      free_mem();
+      take(o);
+    }
+    return *this;
+  }
+  ~row_buf() { free_mem(); }
+  // n values; a new block only if the current one is too small
+  void resize(size_t n, bool pinned) {
+    if (n > cap_ || pinned != pinned_) {
+      free_mem();
+      if (pinned) {
+        void* q = nullptr;
+        if (cudaMallocHost(&q, n * sizeof(int16_t)) != cudaSuccess) throw std::bad_alloc{};
+        p_ = static_cast<int16_t*>(q);
+      } else {
+        p_ = static_cast<int16_t*>(::operator new(n * sizeof(int16_t)));
+      }
+      cap_ = n;
+      pinned_ = pinned;
+    }
+    n_ = n;
+  }
+  void clear() { n_ = 0; }
+  bool empty() const { return n_ == 0; }
+  size_t size() const { return n_; }
+  size_t capacity() const { return cap_; }
+  bool pinned() const { return pinned_; }
+  int16_t* data() { return p_; }
+  int16_t const* data() const { return p_; }
+
+ private:
+  void take(row_buf& o) {
+    p_ = o.p_;
+    n_ = o.n_;
+    cap_ = o.cap_;
+    pinned_ = o.pinned_;
+    o.p_ = nullptr;
+    o.n_ = o.cap_ = 0;
+  }
+  void free_mem() {
+    if (p_ != nullptr) {
+      if (pinned_) cudaFreeHost(p_);
+      else ::operator delete(p_);
+    }
+    p_ = nullptr;
+    n_ = cap_ = 0;
+  }
+  int16_t* p_{nullptr};
+  size_t n_{0}, cap_{0};
+  bool pinned_{false};
+};
+
 struct b2r_engine {
   b2r_timetable* tt{nullptr};
   b2r_engine_config cfg{};
@@ -153,6 +216,7 @@ struct b2r_engine {
   // and export kernels, second stream) ran; their union is the batch's
   // device time
   cudaEvent_t ev_base{nullptr}, ev2a{nullptr}, ev2b{nullptr};
+  cudaEvent_t ev_hdr{nullptr};  // an export's headers are on the host
   // timing engines (profile = 2): the route phase of every super-step,
   // bracketed inside the graph and read after each super-step
   cudaEvent_t ev_scan_a{nullptr}, ev_scan_b{nullptr};
@@ -174,10 +238,13 @@ struct b2r_engine {
   struct result_store {
     std::vector<b2r_journey> journeys;
     std::vector<b2r_leg> legs;
-    row_vector rt_rows;
+    row_buf rt_rows;
     b2r_result view{};
   };
   std::vector<result_store> results;
+  // page-locked one-to-all row buffers of results that the caller has given
+  // up (the previous call's): the next batch copies rows straight into them
+  std::vector<row_buf> row_pool;
 
   // serving (b2r_serve_start .. b2r_serve_stop): driver thread, preparation
   // pool and tickets; type-erased because the state is defined further down
@@ -411,11 +478,19 @@ __global__ void k_prof_row(dev::state st, unsigned long long* rows, uint32_t idx
 }
 
 // export: per listed slot, journey headers + leg blocks (+ one-to-all rows)
+// legs exported with a slot's journeys
+enum : uint32_t {
+  kLegsAll = 0,    // kMaxLegs per journey
+  kLegsMatch = 1,  // one journey: the first matching (recon_transfers, recon_start), the one a
+                   // pong phase rebuilds; its index precedes the legs (UINT32_MAX: none)
+  kLegsNone = 2,   // journey headers only (a ping phase rebuilds nothing)
+};
+
 struct exp_item {
   uint32_t slot;
   uint32_t n_j;
   uint32_t n_rows;  // one-to-all rows (0 otherwise)
-  uint32_t pad;
+  uint32_t legs_mode;
   uint64_t off_j, off_legs, off_rows, off_slot;
 };
 
@@ -433,10 +508,33 @@ __global__ void k_export(dev::state st, exp_item const* items, uint32_t n_items,
     for (auto i = threadIdx.x; i < it.n_j; i += blockDim.x) {
       js[i] = st.journeys[static_cast<size_t>(s) * st.max_j + i];
     }
-    for (auto x = threadIdx.x; x < it.n_j * dev::kMaxLegs; x += blockDim.x) {
-      auto const i = x / dev::kMaxLegs, k = x % dev::kMaxLegs;
-      auto const blk = st.journeys[static_cast<size_t>(s) * st.max_j + i].block;
-      legs[x] = st.legs[(static_cast<size_t>(s) * st.max_j + blk) * dev::kMaxLegs + k];
+    if (it.legs_mode == kLegsAll) {
+      for (auto x = threadIdx.x; x < it.n_j * dev::kMaxLegs; x += blockDim.x) {
+        auto const i = x / dev::kMaxLegs, k = x % dev::kMaxLegs;
+        auto const blk = st.journeys[static_cast<size_t>(s) * st.max_j + i].block;
+        legs[x] = st.legs[(static_cast<size_t>(s) * st.max_j + blk) * dev::kMaxLegs + k];
+      }
+    } else if (it.legs_mode == kLegsMatch) {
+      __shared__ uint32_t match;
+      if (threadIdx.x == 0) {
+        match = UINT32_MAX;
+        for (auto i = 0u; i != it.n_j; ++i) {
+          auto const& j = st.journeys[static_cast<size_t>(s) * st.max_j + i];
+          if (j.transfers == sl.recon_transfers && j.start_time == sl.recon_start) {
+            match = i;
+            break;
+          }
+        }
+        *reinterpret_cast<uint32_t*>(out + it.off_legs) = match;
+      }
+      __syncthreads();
+      if (match != UINT32_MAX) {
+        auto* one = reinterpret_cast<b2r_leg*>(out + it.off_legs + 16);
+        auto const blk = st.journeys[static_cast<size_t>(s) * st.max_j + match].block;
+        for (auto k = threadIdx.x; k < static_cast<uint32_t>(dev::kMaxLegs); k += blockDim.x) {
+          one[k] = st.legs[(static_cast<size_t>(s) * st.max_j + blk) * dev::kMaxLegs + k];
+        }
+      }
     }
   }
   if (it.n_rows != 0) {
@@ -483,6 +581,7 @@ b2r_engine::~b2r_engine() {
   if (ev_scan_b != nullptr) cudaEventDestroy(ev_scan_b);
   if (ev2a != nullptr) cudaEventDestroy(ev2a);
   if (ev2b != nullptr) cudaEventDestroy(ev2b);
+  if (ev_hdr != nullptr) cudaEventDestroy(ev_hdr);
   if (h_summary != nullptr) cudaFreeHost(h_summary);
   if (h_lbcount != nullptr) cudaFreeHost(h_lbcount);
   if (h_adm != nullptr) cudaFreeHost(h_adm);
@@ -894,23 +993,54 @@ void retire(b2r_engine& e, std::vector<uint32_t> const& slots, cudaStream_t s) {
   B2R_CUDA(cudaGetLastError());
 }
 
+// results of the previous call are no longer the caller's: their
+// page-locked row buffers go back to the pool (at most 512 of them)
+void recycle_rows(b2r_engine& e) {
+  for (auto& r : e.results) {
+    if (r.rt_rows.pinned() && e.row_pool.size() < 512) e.row_pool.push_back(std::move(r.rt_rows));
+  }
+  e.results.clear();
+}
+
+// a page-locked row buffer of n values: the smallest pooled one that holds
+// them, else a new one
+row_buf take_rows(b2r_engine& e, size_t n) {
+  auto best = e.row_pool.end();
+  for (auto it = e.row_pool.begin(); it != e.row_pool.end(); ++it) {
+    if (it->capacity() >= n && (best == e.row_pool.end() || it->capacity() < best->capacity())) best = it;
+  }
+  row_buf v;
+  if (best != e.row_pool.end()) {
+    v = std::move(*best);
+    e.row_pool.erase(best);
+  }
+  v.resize(n, true);
+  return v;
+}
+
 struct exported {
   slot_t sl;
   std::vector<dev::journey_rec> js;
-  std::vector<b2r_leg> legs;  // n_j * kMaxLegs
-  row_vector rows;
+  std::vector<b2r_leg> legs;  // kLegsAll: n_j * kMaxLegs; kLegsMatch: kMaxLegs of journey legs_of
+  uint32_t legs_of{UINT32_MAX};
+  row_buf rows;
 };
 
 void export_slots(b2r_engine& e, std::vector<uint32_t> const& slots,
                   std::vector<uint32_t> const& n_js, std::vector<uint32_t> const& n_rows,
-                  std::vector<exported>& out, cudaStream_t s) {
-  out.assign(slots.size(), {});
+                  std::vector<exported>& out, cudaStream_t s,
+                  std::vector<uint8_t> const* legs_modes = nullptr, bool pinned_rows = false) {
+  out.clear();
+  out.resize(slots.size());
   if (slots.empty()) return;
   std::vector<exp_item> items(slots.size());
   // the journeys of slots whose reconstruction waits for the slot to finish
   // (k_reconstruct_done skips the others), uploaded after the items
+  // (a deferred slot runs one start-time group of a one-to-one search, whose
+  // legs are exported in full)
   std::vector<uint32_t> recon;
   for (auto i = 0U; i != slots.size(); ++i) {
+    if (legs_modes != nullptr && (*legs_modes)[i] != kLegsAll) continue;
     for (auto ji = 0U; ji != n_js[i]; ++ji) recon.push_back((slots[i] << 16) | ji);
   }
   auto const recon_off = (slots.size() * sizeof(exp_item) + 15) & ~size_t{15};
@@ -921,6 +1051,7 @@ void export_slots(b2r_engine& e, std::vector<uint32_t> const& slots,
     it.slot = slots[i];
     it.n_j = n_js[i];
     it.n_rows = n_rows[i];
+    it.legs_mode = legs_modes != nullptr ? (*legs_modes)[i] : kLegsAll;
     off = (off + 15) & ~size_t{15};
     it.off_slot = off;
     off += sizeof(slot_t);
@@ -929,7 +1060,15 @@ void export_slots(b2r_engine& e, std::vector<uint32_t> const& slots,
     off += it.n_j * sizeof(dev::journey_rec);
     off = (off + 15) & ~size_t{15};
     it.off_legs = off;
-    off += static_cast<size_t>(it.n_j) * dev::kMaxLegs * sizeof(b2r_leg);
+    off += it.legs_mode == kLegsAll     ? static_cast<size_t>(it.n_j) * dev::kMaxLegs * sizeof(b2r_leg)
+           : it.legs_mode == kLegsMatch ? 16 + dev::kMaxLegs * sizeof(b2r_leg)
+                                        : 0;
+  }
+  // the one-to-all rows after everything else: with page-locked result
+  // buffers they go from here straight into them
+  auto const rows_begin = (off + 255) & ~size_t{255};
+  off = rows_begin;
+  for (auto& it : items) {
     off = (off + 15) & ~size_t{15};
     it.off_rows = off;
     off += static_cast<size_t>(it.n_rows) * e.tt->d.n_loc * sizeof(int16_t);
@@ -966,8 +1105,23 @@ void export_slots(b2r_engine& e, std::vector<uint32_t> const& slots,
   B2R_CUDA(cudaGetLastError());
   if (e.base_recorded) B2R_CUDA(cudaEventRecord(e.ev2b, s));
   e.d2h_bytes += off;
-  B2R_CUDA(cudaMemcpyAsync(e.h_exp, e.d_exp, off, cudaMemcpyDeviceToHost, s));
-  B2R_CUDA(cudaStreamSynchronize(s));
+  // headers, journeys and legs; the rows either into the page-locked
+  // result buffers (left in flight: later work on this stream, and the end
+  // of the batch, wait for them) or through the staging buffer
+  B2R_CUDA(cudaMemcpyAsync(e.h_exp, e.d_exp, pinned_rows ? rows_begin : off, cudaMemcpyDeviceToHost, s));
+  if (pinned_rows) {
+    B2R_CUDA(cudaEventRecord(e.ev_hdr, s));
+    for (auto i = 0U; i != slots.size(); ++i) {
+      auto const& it = items[i];
+      if (it.n_rows == 0) continue;
+      out[i].rows = take_rows(e, static_cast<size_t>(it.n_rows) * e.tt->d.n_loc);
+      B2R_CUDA(cudaMemcpyAsync(out[i].rows.data(), e.d_exp + it.off_rows, out[i].rows.size() * sizeof(int16_t),
+                               cudaMemcpyDeviceToHost, s));
+    }
+    B2R_CUDA(cudaEventSynchronize(e.ev_hdr));
+  } else {
+    B2R_CUDA(cudaStreamSynchronize(s));
+  }
   if (e.base_recorded) {
     float a = 0, b = 0;
     B2R_CUDA(cudaEventElapsedTime(&a, e.ev_base, e.ev2a));
@@ -980,27 +1134,21 @@ void export_slots(b2r_engine& e, std::vector<uint32_t> const& slots,
     std::memcpy(&o.sl, e.h_exp + it.off_slot, sizeof(slot_t));
     o.js.resize(it.n_j);
     std::memcpy(o.js.data(), e.h_exp + it.off_j, it.n_j * sizeof(dev::journey_rec));
-    o.legs.resize(static_cast<size_t>(it.n_j) * dev::kMaxLegs);
-    std::memcpy(o.legs.data(), e.h_exp + it.off_legs, o.legs.size() * sizeof(b2r_leg));
-    o.rows.resize(static_cast<size_t>(it.n_rows) * e.tt->d.n_loc);
-  }
-  // one-to-all rows (n_rows x n_locations each): large copies out of the
-  // pinned staging buffer, split over a few threads
-  size_t row_bytes = 0;
-  for (auto const& o : out) row_bytes += o.rows.size() * sizeof(int16_t);
-  auto const copy_rows = [&](size_t first, size_t step) {
-    for (auto i = first; i < slots.size(); i += step) {
-      std::memcpy(out[i].rows.data(), e.h_exp + items[i].off_rows, out[i].rows.size() * sizeof(int16_t));
+    if (it.legs_mode == kLegsAll) {
+      o.legs.resize(static_cast<size_t>(it.n_j) * dev::kMaxLegs);
+      std::memcpy(o.legs.data(), e.h_exp + it.off_legs, o.legs.size() * sizeof(b2r_leg));
+    } else if (it.legs_mode == kLegsMatch) {
+      std::memcpy(&o.legs_of, e.h_exp + it.off_legs, sizeof(uint32_t));
+      if (o.legs_of < it.n_j) {
+        auto const n = o.js[o.legs_of].n_legs;
+        o.legs.resize(n);
+        std::memcpy(o.legs.data(), e.h_exp + it.off_legs + 16, n * sizeof(b2r_leg));
+      }
     }
-  };
-  if (row_bytes < (size_t{32} << 20)) {
-    copy_rows(0, 1);
-  } else {
-    auto const n_threads = std::min<size_t>(8, std::max(1U, std::thread::hardware_concurrency() / 2));
-    std::vector<std::thread> pool;
-    for (size_t t = 1; t < n_threads; ++t) pool.emplace_back(copy_rows, t, n_threads);
-    copy_rows(0, n_threads);
-    for (auto& th : pool) th.join();
+    if (!pinned_rows && it.n_rows != 0) {
+      o.rows.resize(static_cast<size_t>(it.n_rows) * e.tt->d.n_loc, false);
+      std::memcpy(o.rows.data(), e.h_exp + it.off_rows, o.rows.size() * sizeof(int16_t));
+    }
   }
 }
 
@@ -1011,7 +1159,10 @@ void export_slots(b2r_engine& e, std::vector<uint32_t> const& slots,
 struct pong_run {
   int32_t start_time{0};
   std::vector<dev::journey_rec> results;  // the shared result set, pong frame
-  std::vector<b2r_leg> legs;              // kMaxLegs per result
+  // legs of the rebuilt results by their device leg block: a block keeps its
+  // journey while that journey stays in the result set, and a journey is
+  // rebuilt (and its legs exported) in the pong phase that matches it
+  std::unordered_map<uint32_t, std::vector<b2r_leg>> legs_of_block;
   std::vector<dev::journey_rec> ping;     // this iteration's ping results
   size_t next{0};                         // ping result of the next pong
   bool in_ping{true};
@@ -1170,8 +1321,12 @@ void finish_pong(b2r_engine& e, query_run& q) {
     }
     item it{j, {}};
     std::swap(it.j.start_time, it.j.dest_time);
-    it.legs.assign(r.legs.begin() + static_cast<std::ptrdiff_t>(i) * dev::kMaxLegs,
-                   r.legs.begin() + static_cast<std::ptrdiff_t>(i) * dev::kMaxLegs + j.n_legs);
+    auto const lf = r.legs_of_block.find(j.block);
+    if (lf == r.legs_of_block.end() || lf->second.size() != j.n_legs) {  // rebuilt, but its legs never came
+      q.status = B2R_ERR_INTERNAL;
+      continue;
+    }
+    it.legs = lf->second;
     auto const swap = [](uint32_t l) {
       return l == B2R_SPECIAL_START ? B2R_SPECIAL_END : l == B2R_SPECIAL_END ? B2R_SPECIAL_START : l;
     };
@@ -1314,7 +1469,7 @@ void pong_phase_done(b2r_engine& e, query_run& q, exported& x) {
     stage_pong(e, q, true);
   } else {
     r.results = x.js;
-    r.legs = std::move(x.legs);
+    if (x.legs_of < x.js.size()) r.legs_of_block[x.js[x.legs_of].block] = std::move(x.legs);
     auto& pj = r.ping[r.next];
     auto const m = std::find_if(r.results.begin(), r.results.end(), [&](dev::journey_rec const& j) {
       return j.transfers == pj.transfers && j.start_time == pj.dest_time;
@@ -1351,6 +1506,13 @@ void pong_phase_done(b2r_engine& e, query_run& q, exported& x) {
     q.status = B2R_ERR_CAPACITY;
     finish_pong(e, q);
   }
+}
+
+// the legs the host reads after the phase running in a query's slot: none
+// after a ping, the rebuilt journey's after a pong, all others' in full
+uint8_t legs_mode(query_run const& q) {
+  if (!q.p.pong) return kLegsAll;
+  return (!q.pong || q.pong->in_ping) ? kLegsNone : kLegsMatch;
 }
 
 // after an exported phase: pong queries go on to their next phase, search
@@ -1457,6 +1619,12 @@ struct batch_runner {
   void run(uint32_t chunk) {
     auto const S = e.S;
     auto* st = e.stream;
+    // row copies into result buffers may still be in flight when an error
+    // unwinds the batch: they end before those buffers can be freed
+    struct drain {
+      cudaStream_t s;
+      ~drain() { cudaStreamSynchronize(s); }
+    } drain2{e.stream2};
     e.busy.clear();
     B2R_CUDA(cudaEventRecord(e.ev_base, st));
     e.base_recorded = true;
@@ -1531,9 +1699,9 @@ struct batch_runner {
       return false;
     };
     auto const busy = [&]() { return next < runs.size() || running(); };
-    auto const launch_chunk = [&]() {
+    auto const launch_chunk = [&](uint32_t n_steps) {
       B2R_CUDA(cudaEventRecord(e.ev0, st));
-      for (uint32_t c = 0; c != chunk; ++c) {
+      for (uint32_t c = 0; c != n_steps; ++c) {
         if (use_graph) {
           B2R_CUDA(cudaGraphLaunch(e.graph, st));
         } else {
@@ -1569,7 +1737,7 @@ struct batch_runner {
           admit_free();
           continue;
         }
-        launch_chunk();
+        launch_chunk(chunk);
       }
       B2R_CUDA(cudaStreamSynchronize(st));
       in_flight = false;
@@ -1611,11 +1779,13 @@ struct batch_runner {
       // it instead of leaving the slot idle for a whole chunk
       auto phase_follows = false;
       for (auto const s : done_slots) phase_follows = phase_follows || runs[static_cast<size_t>(slot_q[s])].p.pong;
-      if (!phase_follows && running() && done_slots.size() < n_active) launch_chunk();
+      if (!phase_follows && running() && done_slots.size() < n_active) launch_chunk(chunk);
       if (done_slots.empty()) continue;
       auto const t_exp = std::chrono::steady_clock::now();
       std::vector<exported> ex;
-      export_slots(e, done_slots, n_js, n_rows, ex, e.stream2);
+      std::vector<uint8_t> modes;
+      for (auto const s : done_slots) modes.push_back(legs_mode(runs[static_cast<size_t>(slot_q[s])]));
+      export_slots(e, done_slots, n_js, n_rows, ex, e.stream2, &modes, true);
       std::vector<uint32_t> retired;
       auto const now_ms = std::chrono::duration<double, std::milli>(
                               std::chrono::steady_clock::now() - e.batch_t0)
@@ -1641,6 +1811,7 @@ struct batch_runner {
       if (!in_flight) admit_free();
     }
     B2R_CUDA(cudaStreamSynchronize(st));
+    B2R_CUDA(cudaStreamSynchronize(e.stream2));  // one-to-all rows still on their way
     busy_ms = busy_union_ms(e.busy);
   }
 };
@@ -1858,7 +2029,9 @@ struct serve_state {
         }
         if (done_slots.empty()) continue;
         std::vector<exported> ex;
-        export_slots(e, done_slots, n_js, n_rows, ex, st);
+        std::vector<uint8_t> modes;
+        for (auto const s : done_slots) modes.push_back(legs_mode(slot_item[s]->run));
+        export_slots(e, done_slots, n_js, n_rows, ex, st, &modes);
         std::vector<uint32_t> retired;
         for (auto i = 0U; i != done_slots.size(); ++i) {
           auto const s = done_slots[i];
@@ -2245,7 +2418,7 @@ int b2r_engine_create(b2r_timetable* tt, const b2r_engine_config* cfg_in, b2r_en
                           e->max_starts * sizeof(b2r::dev::start_rec) +
                           e->max_dest * sizeof(b2r::dev::dest_rec) + e->max_off * sizeof(b2r_offset) +
                           b2r::dev::kMaxTimeline * sizeof(b2r::dev::tl_entry) +
-                          (static_cast<uint64_t>(nl) * 4 + tt->d.n_routes) / 8 + 256;
+                          (static_cast<uint64_t>(nl) * (4 + b2r::dev::kK) + tt->d.n_routes) / 8 + 256;
       auto by_budget = cfg.hbm_budget / std::max<uint64_t>(1, e->bytes_per_slot);
       auto slots = std::min<uint64_t>(std::max(32U, cfg.max_slots), by_budget);
       slots &= ~uint64_t{31};
@@ -2269,6 +2442,7 @@ int b2r_engine_create(b2r_timetable* tt, const b2r_engine_config* cfg_in, b2r_en
       al(st.slots, S);
       al(st.lanes, S);
       al(st.rt, static_cast<size_t>(b2r::dev::kK) * nl * S);
+      al(st.touched, static_cast<size_t>(b2r::dev::kK) * G * nl);
       al(st.bounds, static_cast<size_t>(b2r::dev::kK) * nl * S);
       al(st.best, static_cast<size_t>(nl) * S);
       al(st.tmp, static_cast<size_t>(nl) * S);
@@ -2318,6 +2492,7 @@ int b2r_engine_create(b2r_timetable* tt, const b2r_engine_config* cfg_in, b2r_en
       if (cfg.profile) al(e->d_prof_rows, 2 * b2r_engine::kProfRows);
       B2R_CUDA(cudaMemset(st.slots, 0, S * sizeof(b2r::dev::slot_t)));
       B2R_CUDA(cudaMemset(st.rt, 0xFF, static_cast<size_t>(b2r::dev::kK) * nl * S * 4));
+      B2R_CUDA(cudaMemset(st.touched, 0, static_cast<size_t>(b2r::dev::kK) * G * nl * 4));
       B2R_CUDA(cudaMemset(st.best, 0xFF, static_cast<size_t>(nl) * S * 4));
       B2R_CUDA(cudaMemset(st.tmp, 0xFF, static_cast<size_t>(nl) * S * 4));
       B2R_CUDA(cudaMemset(st.X, 0, static_cast<size_t>(nl) * G * 4));
@@ -2338,6 +2513,7 @@ int b2r_engine_create(b2r_timetable* tt, const b2r_engine_config* cfg_in, b2r_en
       B2R_CUDA(cudaEventCreate(&e->ev_scan_b));
       B2R_CUDA(cudaEventCreate(&e->ev2a));
       B2R_CUDA(cudaEventCreate(&e->ev2b));
+      B2R_CUDA(cudaEventCreateWithFlags(&e->ev_hdr, cudaEventDisableTiming));
       if (e->cfg.use_graphs) {
         b2r::capture_graph(*e);
         cudaGraph_t g = nullptr;
@@ -2373,6 +2549,7 @@ int b2r_search_batch(b2r_engine* e, const b2r_query* qs, uint32_t n, b2r_result*
     if (e->serving) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "engine is serving");
     try {
       B2R_CUDA(cudaSetDevice(e->tt->device));
+      b2r::recycle_rows(*e);
       std::vector<b2r::query_run> runs(n);
       auto const t0 = std::chrono::steady_clock::now();
       e->batch_t0 = t0;
@@ -2467,6 +2644,7 @@ int b2r_search_plain(b2r_engine* e, const b2r_query* q, b2r_result* out) {
     }
     try {
       B2R_CUDA(cudaSetDevice(e->tt->device));
+      b2r::recycle_rows(*e);
       std::vector<b2r::query_run> runs(1);
       e->aux_launches = 0;
       b2r::preparer prep;
@@ -2987,7 +3165,8 @@ int b2r_raptor_execute(b2r_raptor* r, int32_t start_time, uint8_t max_transfers,
       b2r::admit(e, {{0U, &p, flags}}, e.stream);
       auto const sum = b2r::run_slot0(e);
       std::vector<b2r::exported> ex;
-      b2r::export_slots(e, {0U}, {sum.n_journeys}, {0U}, ex, e.stream2);
+      std::vector<uint8_t> const no_legs{b2r::kLegsNone};  // legs on request (b2r_raptor_reconstruct)
+      b2r::export_slots(e, {0U}, {sum.n_journeys}, {0U}, ex, e.stream2, &no_legs);
       r->sl = ex[0].sl;
       r->fresh = false;
       r->lb_sent = r->lb_sent || !p.lb.empty();

@@ -190,7 +190,8 @@ struct __align__(16) lane_t {
   uint8_t k;
   uint8_t run;
   uint8_t mode;  // bit0 intermodal dest, bit1 has dests, bit2 tts default, bit3 no lower
-                 // bounds, bits 4-6 footpath profile
+                 // bounds, bits 4-6 footpath profile, bit7 round times kept for a later
+                 // start-time group (the writes set their touched bits)
   uint16_t claszes;  // allowed transport classes
   uint8_t req;       // required route flags
   uint8_t blast;     // pong bounds: last round (0: none)
@@ -227,6 +228,9 @@ struct state {
   slot_t* slots;
   lane_t* lanes;
   uint32_t* rt;     // [K][n_loc][S]
+  uint32_t* touched;  // [K][G][n_loc]: bit b of (k, g, l) is set by every round-time write
+                      // at (k, l) of slot g * 32 + b while that slot may run a later
+                      // start-time group (lane mode bit 7); the sweep reads only the set bits
   uint32_t* best;   // [n_loc][S]
   uint32_t* tmp;    // [n_loc][S]
   uint16_t* lb;     // [n_loc][S]

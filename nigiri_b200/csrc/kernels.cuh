@@ -78,6 +78,24 @@ __device__ __forceinline__ void for_each_pair(uint32_t const* list, uint32_t n, 
   }
 }
 
+// A slot keeps its round times for a later start-time group unless it runs
+// one group and nothing after it: a one-to-one query at one start time whose
+// journeys are collected as usual, or a one-to-all query at one start time.
+// Range queries, interval extension, pong phases and step-driven searches
+// keep them (raptor.h:174-177: only reset_arrivals clears them).
+__device__ __forceinline__ bool keeps_round_times(slot_t const& sl) {
+  if (sl.ontrip && sl.one_to_all) return false;
+  return !(sl.ontrip && sl.recon_mode == 0);
+}
+
+// the touched bit of a round-time write (k, l) of slot s
+__device__ __forceinline__ void touch(state const& st, lane_t const& ln, uint32_t k, uint32_t l, uint32_t s) {
+  if (!(ln.mode & 128u)) return;
+  auto* w = st.touched + (static_cast<size_t>(k) * st.G + (s >> 5)) * st.tt.n_loc + l;
+  auto const bit = 1u << (s & 31u);
+  if ((*w & bit) == 0u) atomicOr(w, bit);
+}
+
 __device__ __forceinline__ void update_tad(slot_t& sl, uint32_t k, int key) {  // raptor.h:1479-1486
   if (sl.one_to_all) return;
   for (auto i = k; i < kK; ++i) {
@@ -121,7 +139,8 @@ __global__ void k_ctl_begin(state st) {
     ln.qtag = tagcode(sl.gen_query);
     ln.mode = (sl.intermodal_dest ? 1u : 0u) |
               ((!sl.intermodal_dest && !sl.one_to_all && sl.n_dest != 0) ? 2u : 0u) |
-              (sl.tts.is_default ? 4u : 0u) | (sl.no_lb ? 8u : 0u) | (static_cast<uint32_t>(sl.prf) << 4);
+              (sl.tts.is_default ? 4u : 0u) | (sl.no_lb ? 8u : 0u) | (static_cast<uint32_t>(sl.prf) << 4) |
+              (keeps_round_times(sl) ? 128u : 0u);
     ln.tad_k = sl.tad[sl.k];
     ln.claszes = sl.allowed_claszes;
     ln.req = sl.req_flags;
@@ -133,23 +152,55 @@ __global__ void k_ctl_begin(state st) {
 
 // best <- min(best, round_times[k]) over all locations (raptor.h:219-223)
 // for the slots whose earlier start-time groups left round times behind
-// (range queries).  Warp per (location, slot group) over the groups holding
-// such slots only, lane = slot: admission packs range queries into the same
-// groups, so the lanes read neighbouring words.
+// (range queries).  Only locations whose touched word of (round, slot group)
+// has the slot's bit can hold such a round time, so a warp reads the words
+// of 32 locations at once (one coalesced load per chunk) and, for every
+// location with bits, its lanes read the slot-minor round times and best
+// labels of the group's slots side by side.  Bits whose entry belongs to an
+// earlier query of the slot (its tag no longer matches) are cleared here;
+// any later write sets them again.  Slots of one group at different rounds
+// are taken one round at a time.
 __global__ void k_sweep(state st) {
   auto const lane = threadIdx.x & 31u;
   auto const warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   auto const n_warps = (gridDim.x * blockDim.x) >> 5;
+  auto const n_loc = st.tt.n_loc;
+  auto const n_chunks = (n_loc + 31u) / 32u;
   for (auto g = 0u; g != st.G; ++g) {
     auto const m = st.sweep_mask[g];
-    if (m == 0u || !((m >> lane) & 1u)) continue;
+    if (m == 0u) continue;
     auto const s = g * 32u + lane;
     auto const ln = st.lanes[s];
-    for (auto l = warp; l < st.tt.n_loc; l += n_warps) {
-      auto const r = dec(st.rt[rti(st, ln.k, l, s)], ln.qtag);
-      if (r == kKeyInv) continue;
-      auto& bw = st.best[li(st, l, s)];
-      if (r < dec(bw, ln.gtag)) bw = enc(ln.gtag, r);
+    auto const mine = ((m >> lane) & 1u) != 0u;
+    auto pending = m;
+    while (pending != 0u) {
+      auto const k = __shfl_sync(kFull, static_cast<uint32_t>(ln.k), __ffs(pending) - 1);
+      auto const same = __ballot_sync(kFull, mine && static_cast<uint32_t>(ln.k) == k);
+      pending &= ~same;
+      auto* tw = st.touched + (static_cast<size_t>(k) * st.G + g) * n_loc;
+      for (auto c = warp; c < n_chunks; c += n_warps) {
+        auto const l = c * 32u + lane;
+        auto const word = l < n_loc ? tw[l] : 0u;
+        auto todo = __ballot_sync(kFull, (word & same) != 0u);
+        while (todo != 0u) {
+          auto const src = static_cast<uint32_t>(__ffs(todo) - 1);
+          todo &= todo - 1u;
+          auto const bits = __shfl_sync(kFull, word, static_cast<int>(src)) & same;
+          auto const at = c * 32u + src;
+          auto stale = false;
+          if ((bits >> lane) & 1u) {
+            auto const r = dec(st.rt[rti(st, k, at, s)], ln.qtag);
+            if (r == kKeyInv) {
+              stale = true;
+            } else {
+              auto& bw = st.best[li(st, at, s)];
+              if (r < dec(bw, ln.gtag)) bw = enc(ln.gtag, r);
+            }
+          }
+          auto const gone = __ballot_sync(kFull, stale);
+          if (gone != 0u && lane == src) tw[l] = word & ~gone;
+        }
+      }
     }
   }
 }
@@ -733,13 +784,17 @@ __global__ void k_transfers_pre(state st) {
     auto const fp = key_add(tk, 0);
     auto const bk = dec(st.best[li(st, d, s)], ln.gtag);
     auto& rtw = st.rt[rti(st, k, d, s)];
-    if (ln.blast == 0u && fp < bk && fp < dec(rtw, ln.qtag)) rtw = enc(ln.qtag, fp);
+    if (ln.blast == 0u && fp < bk && fp < dec(rtw, ln.qtag)) {
+      rtw = enc(ln.qtag, fp);
+      touch(st, ln, k, d, s);
+    }
     auto const tad = static_cast<int>(sl.tad[k]);
     if (fp < bk && fp <= tad) {
       auto const lbv = (ln.mode & 8u) ? uint16_t{0} : st.lb[li(st, d, s)];
       if (lbv == 0xFFFFu || fp + static_cast<int>(lbv) > tad) continue;
       if (!within_bounds(st, s, ln.blast, k, d, fp)) continue;
       rtw = enc(ln.qtag, fp);
+      touch(st, ln, k, d, s);
       st.best[li(st, d, s)] = enc(ln.gtag, fp);
       atomicOr(&st.X[d * st.G + g], bit);  // listed by k_list_marked
       if (fp < tad && tl_n < kMaxTimeline) {
@@ -781,13 +836,17 @@ __global__ void k_transfers(state st) {
         auto const fp = key_add(tk, tt);
         auto const bk = dec(st.best[li(st, l, s)], ln.gtag);
         auto& rtw = st.rt[rti(st, ln.k, l, s)];
-        if (ln.blast == 0u && fp < bk && fp < dec(rtw, ln.qtag)) rtw = enc(ln.qtag, fp);
+        if (ln.blast == 0u && fp < bk && fp < dec(rtw, ln.qtag)) {
+          rtw = enc(ln.qtag, fp);
+          touch(st, ln, ln.k, l, s);
+        }
         auto const tad = (ln.mode & 2u) ? tad_at(st, s, l, 0u) : static_cast<int>(st.tad_phase[s]);
         if (fp < bk && fp <= tad) {
           auto const lbv = (ln.mode & 8u) ? uint16_t{0} : st.lb[li(st, l, s)];
           if (lbv != 0xFFFFu && fp + static_cast<int>(lbv) <= tad &&
               within_bounds(st, s, ln.blast, ln.k, l, fp)) {
             rtw = enc(ln.qtag, fp);
+            touch(st, ln, ln.k, l, s);
             st.best[li(st, l, s)] = enc(ln.gtag, fp);
             atomicOr(&st.X[e], 1u << b);  // listed by k_list_marked
           }
@@ -811,6 +870,7 @@ __device__ void intermodal_slot(state const& st, uint32_t s) {
     auto const end_time = key_add(tk, static_cast<int>(dr.dist));
     if (end_time <= sl.tad[ln.k]) {
       st.rt[rti(st, ln.k, B2R_SPECIAL_END, s)] = enc(ln.qtag, end_time);
+      touch(st, ln, ln.k, B2R_SPECIAL_END, s);
       st.best[li(st, B2R_SPECIAL_END, s)] = enc(ln.gtag, end_time);
       update_tad(sl, ln.k, end_time);
     }
@@ -842,7 +902,7 @@ __device__ void footpaths_pre_slot(state const& st, uint32_t s) {
   int nc = 0;
   for (auto i = 0u; i != sl.n_dest; ++i) {
     auto const d = st.dest_pool[sl.dest_off + i].loc;
-    auto const prf = static_cast<uint32_t>(ln.mode >> 4);
+    auto const prf = (static_cast<uint32_t>(ln.mode) >> 4) & 7u;
     auto const* iidx = fp_index(T, prf, !fwd);
     auto const* idat = fp_words(T, prf, !fwd);
     for (auto x = iidx[d]; x != iidx[d + 1]; ++x) {
@@ -879,13 +939,17 @@ __device__ void footpaths_pre_slot(state const& st, uint32_t s) {
     auto const fp = c[a].key;
     auto const bk = dec(st.best[li(st, d, s)], ln.gtag);
     auto& rtw = st.rt[rti(st, k, d, s)];
-    if (ln.blast == 0u && fp < bk && fp < dec(rtw, ln.qtag)) rtw = enc(ln.qtag, fp);
+    if (ln.blast == 0u && fp < bk && fp < dec(rtw, ln.qtag)) {
+      rtw = enc(ln.qtag, fp);
+      touch(st, ln, k, d, s);
+    }
     auto const tad = static_cast<int>(sl.tad[k]);
     if (fp < bk && fp <= tad) {
       auto const lbv = (ln.mode & 8u) ? uint16_t{0} : st.lb[li(st, d, s)];
       if (lbv == 0xFFFFu || fp + static_cast<int>(lbv) > tad) continue;
       if (!within_bounds(st, s, ln.blast, k, d, fp)) continue;
       rtw = enc(ln.qtag, fp);
+      touch(st, ln, k, d, s);
       st.best[li(st, d, s)] = enc(ln.gtag, fp);
       atomicOr(&st.X[d * st.G + g], bit);  // listed by k_list_marked
       if (fp < tad && tl_n < kMaxTimeline) {
@@ -924,7 +988,7 @@ __global__ void k_footpaths(state st) {
         auto const tk = dec(st.tmp[li(st, src, s)], ln.gtag);
         if (tk == kKeyInv) return;
         auto const fwd = ln.fwd != 0;
-        auto const prf = static_cast<uint32_t>(ln.mode >> 4);
+        auto const prf = (static_cast<uint32_t>(ln.mode) >> 4) & 7u;
         auto const* idx = fp_index(T, prf, fwd);
         auto const* dat = fp_words(T, prf, fwd);
         auto const fb = idx[src], n = idx[src + 1] - fb;
@@ -939,7 +1003,10 @@ __global__ void k_footpaths(state st) {
           if (key >= bk) continue;
           // the reference writes round_times ahead of its pruning only when
           // unbounded (raptor.h:790-794)
-          if (ln.blast == 0u) atomicMin(&st.rt[rti(st, ln.k, tgt, s)], enc(ln.qtag, key));
+          if (ln.blast == 0u) {
+            atomicMin(&st.rt[rti(st, ln.k, tgt, s)], enc(ln.qtag, key));
+            touch(st, ln, ln.k, tgt, s);
+          }
           auto const tad = (ln.mode & 2u) ? tad_at(st, s, src, j) : tad_flat;
           if (key > tad) continue;
           auto const lbv = (ln.mode & 8u) ? uint16_t{0} : st.lb[li(st, tgt, s)];
@@ -947,6 +1014,7 @@ __global__ void k_footpaths(state st) {
             if (ln.blast != 0u) {
               if (!within_bounds(st, s, ln.blast, ln.k, tgt, key)) continue;
               atomicMin(&st.rt[rti(st, ln.k, tgt, s)], enc(ln.qtag, key));
+              touch(st, ln, ln.k, tgt, s);
             }
             atomicMin(&st.best[li(st, tgt, s)], enc(ln.gtag, key));
             atomicOr(&st.X[tgt * st.G + g], 1u << b);  // listed by k_list_marked
