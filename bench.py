@@ -562,6 +562,10 @@ def national_leg(local):
     # then cover 8 slot groups, not 32)
     B = 256
     eng = R.Engine(dtt, max_slots=B)
+    # launch shape picked by the autotuner on a separate sample of the mix
+    tune_qs = QuerySet(h, 4, B, seed=9004)
+    tune = eng.autotune(tune_qs.arr, tune_qs.n)
+    out["launch_shape"] = {f: getattr(tune.best, f) for f, _ in A.LaunchShape._fields_}
     qs = QuerySet(h, 4, B * 4, seed=1004)
     res = (A.Result * B)()
     devs, walls = [], []
@@ -701,8 +705,10 @@ def extras_legs(args, h, dtt, qs, B, local, shape):
 
 
 def ncu_case(args, local):
-    """One batch of `--batch` workload-2 queries, kernels launched one by one
-    (no graph) so that a profiler sees every launch."""
+    """One batch of `--batch` queries of workload `--ncu-workload` (2: the
+    regional one-to-one batch, 4: the national mix) on an engine of that many
+    slots, kernels launched one by one (no graph) so that a profiler sees
+    every launch."""
     from nigiri_b200 import _abi as A
     from nigiri_b200 import routing as R
     from nigiri_b200.timetable import HostTimetable, QuerySet

@@ -245,6 +245,8 @@ struct b2r_engine {
   // page-locked one-to-all row buffers of results that the caller has given
   // up (the previous call's): the next batch copies rows straight into them
   std::vector<row_buf> row_pool;
+  size_t row_pool_bytes{0};
+  std::mutex row_mu;  // the pool: the serving loop takes, b2r_release gives back
 
   // serving (b2r_serve_start .. b2r_serve_stop): driver thread, preparation
   // pool and tickets; type-erased because the state is defined further down
@@ -993,26 +995,39 @@ void retire(b2r_engine& e, std::vector<uint32_t> const& slots, cudaStream_t s) {
   B2R_CUDA(cudaGetLastError());
 }
 
+// a page-locked row buffer back into the pool (at most 512 buffers and
+// 4 GiB; beyond that it is freed)
+void give_rows(b2r_engine& e, row_buf&& r) {
+  if (!r.pinned()) return;
+  std::lock_guard<std::mutex> lock{e.row_mu};
+  auto const bytes = r.capacity() * sizeof(int16_t);
+  if (e.row_pool.size() >= 512 || e.row_pool_bytes + bytes > (size_t{4} << 30)) return;
+  e.row_pool_bytes += bytes;
+  e.row_pool.push_back(std::move(r));
+}
+
 // results of the previous call are no longer the caller's: their
-// page-locked row buffers go back to the pool (at most 512 of them)
+// page-locked row buffers go back to the pool
 void recycle_rows(b2r_engine& e) {
-  for (auto& r : e.results) {
-    if (r.rt_rows.pinned() && e.row_pool.size() < 512) e.row_pool.push_back(std::move(r.rt_rows));
-  }
+  for (auto& r : e.results) give_rows(e, std::move(r.rt_rows));
   e.results.clear();
 }
 
 // a page-locked row buffer of n values: the smallest pooled one that holds
 // them, else a new one
 row_buf take_rows(b2r_engine& e, size_t n) {
-  auto best = e.row_pool.end();
-  for (auto it = e.row_pool.begin(); it != e.row_pool.end(); ++it) {
-    if (it->capacity() >= n && (best == e.row_pool.end() || it->capacity() < best->capacity())) best = it;
-  }
   row_buf v;
-  if (best != e.row_pool.end()) {
-    v = std::move(*best);
-    e.row_pool.erase(best);
+  {
+    std::lock_guard<std::mutex> lock{e.row_mu};
+    auto best = e.row_pool.end();
+    for (auto it = e.row_pool.begin(); it != e.row_pool.end(); ++it) {
+      if (it->capacity() >= n && (best == e.row_pool.end() || it->capacity() < best->capacity())) best = it;
+    }
+    if (best != e.row_pool.end()) {
+      e.row_pool_bytes -= best->capacity() * sizeof(int16_t);
+      v = std::move(*best);
+      e.row_pool.erase(best);
+    }
   }
   v.resize(n, true);
   return v;
@@ -2031,7 +2046,8 @@ struct serve_state {
         std::vector<exported> ex;
         std::vector<uint8_t> modes;
         for (auto const s : done_slots) modes.push_back(legs_mode(slot_item[s]->run));
-        export_slots(e, done_slots, n_js, n_rows, ex, st, &modes);
+        export_slots(e, done_slots, n_js, n_rows, ex, st, &modes, true);
+        B2R_CUDA(cudaStreamSynchronize(st));  // the rows, before any ticket shows finished
         std::vector<uint32_t> retired;
         for (auto i = 0U; i != done_slots.size(); ++i) {
           auto const s = done_slots[i];
@@ -2911,6 +2927,7 @@ int b2r_release(b2r_engine* e, uint64_t ticket) {
     auto const found = ss->items.find(ticket);
     if (found == ss->items.end()) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "unknown ticket");
     if (!found->second->finished) return b2r::fail(B2R_ERR_NOT_READY, "ticket still running");
+    b2r::give_rows(*e, std::move(found->second->run.res.rt_rows));
     ss->items.erase(found);
     return B2R_OK;
   });

@@ -154,12 +154,12 @@ __global__ void k_ctl_begin(state st) {
 // for the slots whose earlier start-time groups left round times behind
 // (range queries).  Only locations whose touched word of (round, slot group)
 // has the slot's bit can hold such a round time, so a warp reads the words
-// of 32 locations at once (one coalesced load per chunk) and, for every
-// location with bits, its lanes read the slot-minor round times and best
-// labels of the group's slots side by side.  Bits whose entry belongs to an
-// earlier query of the slot (its tag no longer matches) are cleared here;
-// any later write sets them again.  Slots of one group at different rounds
-// are taken one round at a time.
+// of 32 locations at once (one coalesced load) and spreads their set bits,
+// the (location, slot) pairs, over its lanes: every lane loads one round
+// time and best label, independent of the others.  Bits whose entry belongs
+// to an earlier query of the slot (its tag no longer matches) are cleared
+// here; any later write sets them again.  Slots of one group at different
+// rounds are taken one round at a time.
 __global__ void k_sweep(state st) {
   auto const lane = threadIdx.x & 31u;
   auto const warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -169,8 +169,7 @@ __global__ void k_sweep(state st) {
   for (auto g = 0u; g != st.G; ++g) {
     auto const m = st.sweep_mask[g];
     if (m == 0u) continue;
-    auto const s = g * 32u + lane;
-    auto const ln = st.lanes[s];
+    auto const ln = st.lanes[g * 32u + lane];
     auto const mine = ((m >> lane) & 1u) != 0u;
     auto pending = m;
     while (pending != 0u) {
@@ -180,25 +179,42 @@ __global__ void k_sweep(state st) {
       auto* tw = st.touched + (static_cast<size_t>(k) * st.G + g) * n_loc;
       for (auto c = warp; c < n_chunks; c += n_warps) {
         auto const l = c * 32u + lane;
-        auto const word = l < n_loc ? tw[l] : 0u;
-        auto todo = __ballot_sync(kFull, (word & same) != 0u);
-        while (todo != 0u) {
-          auto const src = static_cast<uint32_t>(__ffs(todo) - 1);
-          todo &= todo - 1u;
-          auto const bits = __shfl_sync(kFull, word, static_cast<int>(src)) & same;
-          auto const at = c * 32u + src;
-          auto stale = false;
-          if ((bits >> lane) & 1u) {
-            auto const r = dec(st.rt[rti(st, k, at, s)], ln.qtag);
+        auto const word = l < n_loc ? (tw[l] & same) : 0u;
+        if (__ballot_sync(kFull, word != 0u) == 0u) continue;
+        auto const cnt = static_cast<uint32_t>(__popc(word));
+        auto end = cnt;  // inclusive prefix sum of the pair counts
+        for (auto o = 1u; o < 32u; o <<= 1) {
+          auto const y = __shfl_up_sync(kFull, end, o);
+          if (lane >= o) end += y;
+        }
+        auto const total = __shfl_sync(kFull, end, 31);
+        for (auto p0 = 0u; p0 < total; p0 += 32u) {
+          auto const p = p0 + lane;
+          uint32_t owner = 0;  // first lane whose prefix end exceeds p
+          for (auto b = 16u; b > 0u; b >>= 1) {
+            if (__shfl_sync(kFull, end, static_cast<int>(owner + b - 1u)) <= p) owner += b;
+          }
+          auto o_word = __shfl_sync(kFull, word, static_cast<int>(owner));
+          auto const o_first = __shfl_sync(kFull, end, static_cast<int>(owner)) -
+                               __shfl_sync(kFull, cnt, static_cast<int>(owner));
+          uint32_t b = 0u;
+          if (p < total) {
+            for (auto x = p - o_first; x != 0u; --x) o_word &= o_word - 1u;
+            b = static_cast<uint32_t>(__ffs(o_word) - 1);
+          }
+          auto const qtag = __shfl_sync(kFull, static_cast<uint32_t>(ln.qtag), static_cast<int>(b));
+          auto const gtag = __shfl_sync(kFull, static_cast<uint32_t>(ln.gtag), static_cast<int>(b));
+          if (p < total) {
+            auto const at = c * 32u + owner;
+            auto const s = g * 32u + b;
+            auto const r = dec(st.rt[rti(st, k, at, s)], static_cast<uint16_t>(qtag));
             if (r == kKeyInv) {
-              stale = true;
+              atomicAnd(tw + at, ~(1u << b));
             } else {
               auto& bw = st.best[li(st, at, s)];
-              if (r < dec(bw, ln.gtag)) bw = enc(ln.gtag, r);
+              if (r < dec(bw, static_cast<uint16_t>(gtag))) bw = enc(static_cast<uint16_t>(gtag), r);
             }
           }
-          auto const gone = __ballot_sync(kFull, stale);
-          if (gone != 0u && lane == src) tw[l] = word & ~gone;
         }
       }
     }
@@ -244,8 +260,8 @@ __global__ void k_mark_routes(state st) {
       auto const l = e / st.G;
       w = st.X[e] & st.run_mask[g];
       if (w != 0u) {
-        rb = st.tt.loc_routes_idx[l];
-        cnt = st.tt.loc_routes_idx[l + 1] - rb;
+        rb = __ldg(st.tt.loc_routes_idx + l);
+        cnt = __ldg(st.tt.loc_routes_idx + l + 1) - rb;
         if (cnt != 0u && (st.any_mask[g] & w) != w) atomicOr(&st.any_mask[g], w);
       }
     }
@@ -267,7 +283,7 @@ __global__ void k_mark_routes(state st) {
       auto const o_g = __shfl_sync(kFull, g, static_cast<int>(owner));
       auto const o_w = __shfl_sync(kFull, w, static_cast<int>(owner));
       if (p < total) {
-        auto const r = st.tt.loc_routes[o_rb + (p - o_first)];
+        auto const r = __ldg(st.tt.loc_routes + o_rb + (p - o_first));
         atomicOr(&st.R[r * st.G + o_g], o_w);  // listed by k_list_routes
       }
     }
