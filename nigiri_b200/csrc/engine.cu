@@ -1013,9 +1013,16 @@ void recycle_rows(b2r_engine& e) {
   e.results.clear();
 }
 
-// a page-locked row buffer of n values: the smallest pooled one that holds
-// them, else a new one
-row_buf take_rows(b2r_engine& e, size_t n) {
+// rows of a result: where export_slots puts them
+enum class row_target {
+  staging,  // ordinary memory, through the page-locked staging buffer
+  pinned,   // a page-locked buffer: pooled, else newly allocated
+  pooled,   // a pooled page-locked buffer if one is free, else as staging
+};
+
+// a row buffer of n values: the smallest pooled page-locked one that holds
+// them; else a new page-locked one (may_pin) or ordinary memory
+row_buf take_rows(b2r_engine& e, size_t n, bool may_pin = true) {
   row_buf v;
   {
     std::lock_guard<std::mutex> lock{e.row_mu};
@@ -1029,8 +1036,24 @@ row_buf take_rows(b2r_engine& e, size_t n) {
       e.row_pool.erase(best);
     }
   }
-  v.resize(n, true);
+  v.resize(n, v.pinned() || may_pin);
   return v;
+}
+
+// page-locked row buffers for up to `count` one-to-all results, allocated
+// ahead (the serving loop takes from the pool and never allocates any)
+void prewarm_rows(b2r_engine& e, uint32_t count, size_t max_bytes) {
+  auto const n = static_cast<size_t>(dev::kK) * e.tt->d.n_loc;
+  size_t have = 0;
+  {
+    std::lock_guard<std::mutex> lock{e.row_mu};
+    for (auto const& r : e.row_pool) have += r.capacity() >= n ? 1U : 0U;
+  }
+  for (auto i = have; i < count && (i + 1) * n * sizeof(int16_t) <= max_bytes; ++i) {
+    row_buf r;
+    r.resize(n, true);
+    give_rows(e, std::move(r));
+  }
 }
 
 struct exported {
@@ -1044,7 +1067,7 @@ struct exported {
 void export_slots(b2r_engine& e, std::vector<uint32_t> const& slots,
                   std::vector<uint32_t> const& n_js, std::vector<uint32_t> const& n_rows,
                   std::vector<exported>& out, cudaStream_t s,
-                  std::vector<uint8_t> const* legs_modes = nullptr, bool pinned_rows = false) {
+                  std::vector<uint8_t> const* legs_modes = nullptr, row_target rows_to = row_target::staging) {
   out.clear();
   out.resize(slots.size());
   if (slots.empty()) return;
@@ -1123,20 +1146,34 @@ void export_slots(b2r_engine& e, std::vector<uint32_t> const& slots,
   // headers, journeys and legs; the rows either into the page-locked
   // result buffers (left in flight: later work on this stream, and the end
   // of the batch, wait for them) or through the staging buffer
-  B2R_CUDA(cudaMemcpyAsync(e.h_exp, e.d_exp, pinned_rows ? rows_begin : off, cudaMemcpyDeviceToHost, s));
-  if (pinned_rows) {
-    B2R_CUDA(cudaEventRecord(e.ev_hdr, s));
-    for (auto i = 0U; i != slots.size(); ++i) {
-      auto const& it = items[i];
-      if (it.n_rows == 0) continue;
-      out[i].rows = take_rows(e, static_cast<size_t>(it.n_rows) * e.tt->d.n_loc);
-      B2R_CUDA(cudaMemcpyAsync(out[i].rows.data(), e.d_exp + it.off_rows, out[i].rows.size() * sizeof(int16_t),
+  B2R_CUDA(cudaMemcpyAsync(e.h_exp, e.d_exp, rows_begin, cudaMemcpyDeviceToHost, s));
+  // rows for ordinary memory go through the staging buffer and are on the
+  // host with the headers; rows for page-locked buffers go straight there
+  // and are left in flight (later work on this stream, and the end of the
+  // batch, wait for them)
+  std::vector<uint8_t> direct(slots.size(), 0);
+  for (auto i = 0U; i != slots.size(); ++i) {
+    auto const& it = items[i];
+    if (it.n_rows == 0) continue;
+    auto const n = static_cast<size_t>(it.n_rows) * e.tt->d.n_loc;
+    if (rows_to == row_target::staging) {
+      out[i].rows.resize(n, false);
+    } else {
+      out[i].rows = take_rows(e, n, rows_to == row_target::pinned);
+    }
+    direct[i] = out[i].rows.pinned() ? 1 : 0;
+    if (!direct[i]) {
+      B2R_CUDA(cudaMemcpyAsync(e.h_exp + it.off_rows, e.d_exp + it.off_rows, n * sizeof(int16_t),
                                cudaMemcpyDeviceToHost, s));
     }
-    B2R_CUDA(cudaEventSynchronize(e.ev_hdr));
-  } else {
-    B2R_CUDA(cudaStreamSynchronize(s));
   }
+  B2R_CUDA(cudaEventRecord(e.ev_hdr, s));
+  for (auto i = 0U; i != slots.size(); ++i) {
+    if (!direct[i]) continue;
+    B2R_CUDA(cudaMemcpyAsync(out[i].rows.data(), e.d_exp + items[i].off_rows, out[i].rows.size() * sizeof(int16_t),
+                             cudaMemcpyDeviceToHost, s));
+  }
+  B2R_CUDA(cudaEventSynchronize(e.ev_hdr));
   if (e.base_recorded) {
     float a = 0, b = 0;
     B2R_CUDA(cudaEventElapsedTime(&a, e.ev_base, e.ev2a));
@@ -1160,8 +1197,7 @@ void export_slots(b2r_engine& e, std::vector<uint32_t> const& slots,
         std::memcpy(o.legs.data(), e.h_exp + it.off_legs + 16, n * sizeof(b2r_leg));
       }
     }
-    if (!pinned_rows && it.n_rows != 0) {
-      o.rows.resize(static_cast<size_t>(it.n_rows) * e.tt->d.n_loc, false);
+    if (it.n_rows != 0 && !direct[i]) {
       std::memcpy(o.rows.data(), e.h_exp + it.off_rows, o.rows.size() * sizeof(int16_t));
     }
   }
@@ -1800,7 +1836,7 @@ struct batch_runner {
       std::vector<exported> ex;
       std::vector<uint8_t> modes;
       for (auto const s : done_slots) modes.push_back(legs_mode(runs[static_cast<size_t>(slot_q[s])]));
-      export_slots(e, done_slots, n_js, n_rows, ex, e.stream2, &modes, true);
+      export_slots(e, done_slots, n_js, n_rows, ex, e.stream2, &modes, row_target::pinned);
       std::vector<uint32_t> retired;
       auto const now_ms = std::chrono::duration<double, std::milli>(
                               std::chrono::steady_clock::now() - e.batch_t0)
@@ -1962,65 +1998,81 @@ struct serve_state {
     }
   }
 
+  // Free slots and staged pong phases admitted (queued on the main stream);
+  // with nothing resident and nothing in flight it waits for prepared
+  // queries.  Returns false when the loop is to end, else whether any slot
+  // holds a query.
+  bool admit_ready(std::vector<uint8_t>& retiring, std::vector<uint8_t>& waiting, bool in_flight, bool& busy) {
+    std::vector<adm_req> adm;
+    for (auto const s : pending) {  // pong phases staged by the last export
+      auto& run = slot_item[s]->run;
+      adm.push_back({s, &run.phase, run.adm_flags, &run.upload});
+      run.readmit = false;
+      waiting[s] = 0;
+    }
+    pending.clear();
+    {
+      std::unique_lock<std::mutex> lock{mu};
+      auto const has_busy = [&] {
+        for (auto* x : slot_item)
+          if (x != nullptr) return true;
+        return false;
+      };
+      if (!has_busy() && !in_flight && adm.empty()) {
+        cv_driver.wait(lock, [&] { return !ready.empty() || (stop && unfinished == 0); });
+        if (ready.empty() && stop && unfinished == 0) return false;
+      }
+      slot_picker pick{e.S, [&](uint32_t s) { return slot_item[s] == nullptr && retiring[s] == 0; }};
+      while (!ready.empty()) {
+        while (!ready.empty()) {
+          auto* it = ready.front();
+          auto const& p = it->run.p;
+          if (p.status != B2R_OK || p.empty_result) {
+            ready.pop_front();
+            it->run.res.view.interval_from = p.iv_from;
+            it->run.res.view.interval_to = p.iv_to;
+            fail_item(*it, p.status);
+            cv_done.notify_all();
+            continue;
+          }
+          if (auto const c = check_capacity(e, p); c != B2R_OK) {
+            ready.pop_front();
+            fail_item(*it, c);
+            cv_done.notify_all();
+            continue;
+          }
+          break;
+        }
+        if (ready.empty()) break;
+        auto* it = ready.front();
+        auto const s = pick.take(sweeps(it->run.p));
+        if (s < 0) break;
+        ready.pop_front();
+        slot_item[s] = it;
+        adm.push_back({static_cast<uint32_t>(s), &it->run.p});
+      }
+      busy = has_busy();
+    }
+    admit(e, adm, e.stream);
+    return true;
+  }
+
+  // Pipelined like the batch loop: right after the sync of chunk c the
+  // next chunk is launched, and the slots that finished in c are exported
+  // on the second stream while it runs.  Retirements, re-arms and staged
+  // pong phases are then queued behind that chunk, whose summary predates
+  // them: such slots are skipped in it (retiring, stale, waiting) and only
+  // then reused.
   void driver_loop() {
     auto* st = e.stream;
     auto const chunk = e.cfg.steps_per_sync != 0 ? e.cfg.steps_per_sync : std::min(2U, e.shape.steps_per_sync);
     auto const use_graph = e.cfg.use_graphs != 0 && e.graph != nullptr;
     try {
       B2R_CUDA(cudaSetDevice(e.tt->device));
-      while (true) {
-        std::vector<adm_req> adm;
-        bool any_busy = false;
-        for (auto const s : pending) {  // pong phases staged by the last export
-          auto& run = slot_item[s]->run;
-          adm.push_back({s, &run.phase, run.adm_flags, &run.upload});
-          run.readmit = false;
-        }
-        pending.clear();
-        {
-          std::unique_lock<std::mutex> lock{mu};
-          auto const has_busy = [&] {
-            for (auto* x : slot_item)
-              if (x != nullptr) return true;
-            return false;
-          };
-          if (!has_busy()) {
-            cv_driver.wait(lock, [&] { return !ready.empty() || (stop && unfinished == 0); });
-            if (ready.empty() && stop && unfinished == 0) return;
-          }
-          slot_picker pick{e.S, [&](uint32_t s) { return slot_item[s] == nullptr; }};
-          while (!ready.empty()) {
-            while (!ready.empty()) {
-              auto* it = ready.front();
-              auto const& p = it->run.p;
-              if (p.status != B2R_OK || p.empty_result) {
-                ready.pop_front();
-                it->run.res.view.interval_from = p.iv_from;
-                it->run.res.view.interval_to = p.iv_to;
-                fail_item(*it, p.status);
-                cv_done.notify_all();
-                continue;
-              }
-              if (auto const c = check_capacity(e, p); c != B2R_OK) {
-                ready.pop_front();
-                fail_item(*it, c);
-                cv_done.notify_all();
-                continue;
-              }
-              break;
-            }
-            if (ready.empty()) break;
-            auto* it = ready.front();
-            auto const s = pick.take(sweeps(it->run.p));
-            if (s < 0) break;
-            ready.pop_front();
-            slot_item[s] = it;
-            adm.push_back({static_cast<uint32_t>(s), &it->run.p});
-          }
-          any_busy = has_busy();
-        }
-        admit(e, adm, st);
-        if (!any_busy) continue;
+      std::vector<uint8_t> retiring(e.S, 0), stale(e.S, 0), waiting(e.S, 0);
+      std::vector<b2r_engine::summary_t> sum(e.S);
+      bool in_flight = false;
+      auto const launch_chunk = [&]() {
         for (uint32_t c = 0; c != chunk; ++c) {
           if (use_graph) {
             B2R_CUDA(cudaGraphLaunch(e.graph, st));
@@ -2031,23 +2083,49 @@ struct serve_state {
         }
         B2R_CUDA(cudaMemcpyAsync(e.h_summary, e.d_summary, e.S * sizeof(b2r_engine::summary_t),
                                  cudaMemcpyDeviceToHost, st));
+        in_flight = true;
+      };
+      while (true) {
+        if (!in_flight) {
+          std::fill(retiring.begin(), retiring.end(), 0);  // nothing in flight predates a retirement
+          bool busy = false;
+          if (!admit_ready(retiring, waiting, false, busy)) return;
+          if (!busy) continue;
+          launch_chunk();
+        }
         B2R_CUDA(cudaStreamSynchronize(st));
+        in_flight = false;
+        std::copy(e.h_summary, e.h_summary + e.S, sum.begin());
         std::vector<uint32_t> done_slots, n_js, n_rows;
         for (uint32_t s = 0; s != e.S; ++s) {
-          if (slot_item[s] == nullptr) continue;
-          auto const state = e.h_summary[s].state;
+          if (slot_item[s] == nullptr || waiting[s]) continue;
+          if (stale[s]) {
+            stale[s] = 0;
+            continue;
+          }
+          auto const state = sum[s].state;
           if (state == dev::S_DONE || state == dev::S_ERROR) {
             done_slots.push_back(s);
-            n_js.push_back(e.h_summary[s].n_journeys);
+            n_js.push_back(sum[s].n_journeys);
             n_rows.push_back(slot_item[s]->run.p.one_to_all ? slot_item[s]->run.p.end_k : 0u);
           }
         }
+        std::fill(retiring.begin(), retiring.end(), 0);  // their retirement precedes what is queued next
+        bool busy = false;
+        if (!admit_ready(retiring, waiting, true, busy)) return;
+        // a finished pong phase is followed by its next phase, staged from
+        // the export: the next chunk waits for it
+        auto phase_follows = false;
+        for (auto const s : done_slots) phase_follows = phase_follows || slot_item[s]->run.p.pong;
+        size_t n_active = 0;  // resident queries the next chunk would run, the finished ones included
+        for (uint32_t s = 0; s != e.S; ++s) n_active += (slot_item[s] != nullptr && !waiting[s]) ? 1U : 0U;
+        if (!phase_follows && busy && done_slots.size() < n_active) launch_chunk();
         if (done_slots.empty()) continue;
         std::vector<exported> ex;
         std::vector<uint8_t> modes;
         for (auto const s : done_slots) modes.push_back(legs_mode(slot_item[s]->run));
-        export_slots(e, done_slots, n_js, n_rows, ex, st, &modes, true);
-        B2R_CUDA(cudaStreamSynchronize(st));  // the rows, before any ticket shows finished
+        export_slots(e, done_slots, n_js, n_rows, ex, e.stream2, &modes, row_target::pooled);
+        B2R_CUDA(cudaStreamSynchronize(e.stream2));  // the rows, before any ticket shows finished
         std::vector<uint32_t> retired;
         for (auto i = 0U; i != done_slots.size(); ++i) {
           auto const s = done_slots[i];
@@ -2055,13 +2133,16 @@ struct serve_state {
           phase_done(e, it.run, ex[i]);
           if (it.run.readmit) {
             pending.push_back(s);
+            waiting[s] = 1;
             continue;
           }
           if (it.run.rearm) {
             rearm(e, s, it.run, st);
+            stale[s] = in_flight ? 1 : 0;
             continue;
           }
           retired.push_back(s);
+          retiring[s] = in_flight ? 1 : 0;
           std::lock_guard<std::mutex> lock{mu};
           slot_item[s] = nullptr;
           finish(it);
@@ -2833,6 +2914,12 @@ int b2r_serve_start(b2r_engine* e) {
   B2R_API_GUARD({
     if (e == nullptr) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
     if (e->serving) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "engine is already serving");
+    try {  // page-locked rows for the one-to-all results the loop exports
+      B2R_CUDA(cudaSetDevice(e->tt->device));
+      b2r::prewarm_rows(*e, 32, size_t{512} << 20);
+    } catch (std::exception const& ex) {
+      return b2r::fail(B2R_ERR_CUDA, ex.what());
+    }
     auto ss = std::make_shared<b2r::serve_state>(*e);
     auto const hw = std::max(1U, std::thread::hardware_concurrency());
     auto const n_prep = e->cfg.host_threads != 0 ? e->cfg.host_threads : std::max(1U, std::min(8U, hw / 2));
