@@ -593,6 +593,7 @@ def national_leg(local):
     out["plain_gpu"] = {"value": n_plain / (time.perf_counter() - t0), "unit": "queries/s", "queries": n_plain}
     del plain
     eng = R.Engine(dtt, max_slots=1024)
+    eng.shape = tune.best  # the shape tuned on the mix above
     # served (continuous batching), 1% of the answers kept for the check
     sq = QuerySet(h, 5, 4096, seed=1005)
     kept = {}
