@@ -171,7 +171,7 @@ def reference_arm(args, rank, world):
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from nigiri_b200.timetable import HostTimetable, QuerySet
     h = HostTimetable.generate(WORKLOAD)
-    sample = args.cpu_sample or 512
+    sample = args.cpu_sample or args.batch  # the GPU arm's batch: the same queries, step by step
     threads = host_threads()
     qs = QuerySet(h, WORKLOAD, sample * (args.steps + args.warmup), seed=1000 + WORKLOAD)
     for w in range(args.warmup):
