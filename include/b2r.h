@@ -624,6 +624,14 @@ typedef struct b2r_batch_stats {
   double host_idle_ms;        /* driver waiting for preparation, no slot busy */
 } b2r_batch_stats;
 int b2r_last_batch_stats(const b2r_engine* e, b2r_batch_stats* s);
+/* Counters of the serving loop since b2r_serve_start (the engine's current
+ * or last serving run): super_steps and kernel_launches run, and host
+ * milliseconds spent admitting (host_admit_ms), exporting, finalising and
+ * retiring finished slots (host_export_ms), waiting for prepared queries
+ * with nothing resident (host_idle_ms), preparing queries summed over the
+ * preparation threads (host_prep_cpu_ms), and waiting for super-step
+ * chunks to end (device_ms).  Other fields are 0. */
+int b2r_serve_stats(const b2r_engine* e, b2r_batch_stats* out);
 
 /* Launch shape of the super-step's main kernels.  Results do not depend on
  * it; throughput does, with the timetable, the query mix and the slot

@@ -198,7 +198,7 @@ EXPORTS = [
     "b2r_engine_config_init", "b2r_engine_create", "b2r_engine_destroy",
     "b2r_engine_bytes_per_slot", "b2r_engine_slots", "b2r_search_batch",
     "b2r_search_plain", "b2r_serve_start", "b2r_serve_stop", "b2r_submit",
-    "b2r_poll", "b2r_wait", "b2r_release", "b2r_last_batch_stats",
+    "b2r_poll", "b2r_wait", "b2r_release", "b2r_serve_stats", "b2r_last_batch_stats",
     "b2r_tt_generate", "b2r_tt_build", "b2r_tt_save", "b2r_tt_load",
     "b2r_tt_desc", "b2r_tt_destroy", "b2r_gtfs_config_init", "b2r_tt_load_gtfs",
     "b2r_tt_location_id", "b2r_tt_transport_name", "b2r_queries_generate",
@@ -234,6 +234,7 @@ def _declare(lib):
         "b2r_wait": (C.c_int, [vp, C.c_uint64, C.POINTER(Result)]),
         "b2r_release": (C.c_int, [vp, C.c_uint64]),
         "b2r_last_batch_stats": (C.c_int, [vp, C.POINTER(BatchStats)]),
+        "b2r_serve_stats": (C.c_int, [vp, C.POINTER(BatchStats)]),
         "b2r_tt_generate": (C.c_int, [C.c_uint32, C.c_uint64, C.POINTER(vp)]),
         "b2r_tt_build": (C.c_int, [C.POINTER(TtBase), C.POINTER(vp)]),
         "b2r_tt_save": (C.c_int, [vp, C.c_char_p]),

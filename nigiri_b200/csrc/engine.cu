@@ -1017,12 +1017,11 @@ void recycle_rows(b2r_engine& e) {
 enum class row_target {
   staging,  // ordinary memory, through the page-locked staging buffer
   pinned,   // a page-locked buffer: pooled, else newly allocated
-  pooled,   // a pooled page-locked buffer if one is free, else as staging
 };
 
-// a row buffer of n values: the smallest pooled page-locked one that holds
-// them; else a new page-locked one (may_pin) or ordinary memory
-row_buf take_rows(b2r_engine& e, size_t n, bool may_pin = true) {
+// a page-locked row buffer of n values: the smallest pooled one that holds
+// them, else a new one
+row_buf take_rows(b2r_engine& e, size_t n) {
   row_buf v;
   {
     std::lock_guard<std::mutex> lock{e.row_mu};
@@ -1036,7 +1035,7 @@ row_buf take_rows(b2r_engine& e, size_t n, bool may_pin = true) {
       e.row_pool.erase(best);
     }
   }
-  v.resize(n, v.pinned() || may_pin);
+  v.resize(n, true);
   return v;
 }
 
@@ -1159,7 +1158,7 @@ void export_slots(b2r_engine& e, std::vector<uint32_t> const& slots,
     if (rows_to == row_target::staging) {
       out[i].rows.resize(n, false);
     } else {
-      out[i].rows = take_rows(e, n, rows_to == row_target::pinned);
+      out[i].rows = take_rows(e, n);
     }
     direct[i] = out[i].rows.pinned() ? 1 : 0;
     if (!direct[i]) {
@@ -1952,6 +1951,8 @@ struct serve_state {
   std::string failed_msg;
   std::vector<std::thread> prep_pool;
   std::thread driver;
+  // counters for b2r_serve_stats (nanoseconds of host time by step)
+  std::atomic<uint64_t> n_steps{0}, n_launches{0}, admit_ns{0}, export_ns{0}, idle_ns{0}, prep_ns{0}, sync_ns{0};
 
   void finish(serve_item& it) {  // with mu held
     auto& r = it.run.res;
@@ -1981,11 +1982,13 @@ struct serve_state {
       to_prepare.pop_front();
       lock.unlock();
       auto status = B2R_OK;
+      auto const t0 = std::chrono::steady_clock::now();
       try {
         prepare(e.view, it->q, lb_mode, it->run.p);
       } catch (...) {
         status = B2R_ERR_INTERNAL;
       }
+      prep_ns += ns_since(t0);
       lock.lock();
       if (status != B2R_OK) {
         fail_item(*it, status);
@@ -2019,7 +2022,9 @@ struct serve_state {
         return false;
       };
       if (!has_busy() && !in_flight && adm.empty()) {
+        auto const t0 = std::chrono::steady_clock::now();
         cv_driver.wait(lock, [&] { return !ready.empty() || (stop && unfinished == 0); });
+        idle_ns += ns_since(t0);
         if (ready.empty() && stop && unfinished == 0) return false;
       }
       slot_picker pick{e.S, [&](uint32_t s) { return slot_item[s] == nullptr && retiring[s] == 0; }};
@@ -2052,10 +2057,18 @@ struct serve_state {
         adm.push_back({static_cast<uint32_t>(s), &it->run.p});
       }
       busy = has_busy();
+      backlog = !ready.empty();  // prepared queries wait for slots
     }
+    auto const t0 = std::chrono::steady_clock::now();
     admit(e, adm, e.stream);
+    admit_ns += ns_since(t0);
     return true;
   }
+  static uint64_t ns_since(std::chrono::steady_clock::time_point t0) {
+    return static_cast<uint64_t>(
+        std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0).count());
+  }
+  bool backlog{false};
 
   // Pipelined like the batch loop: right after the sync of chunk c the
   // next chunk is launched, and the slots that finished in c are exported
@@ -2072,8 +2085,14 @@ struct serve_state {
       std::vector<uint8_t> retiring(e.S, 0), stale(e.S, 0), waiting(e.S, 0);
       std::vector<b2r_engine::summary_t> sum(e.S);
       bool in_flight = false;
+      // 2 super-steps per check for short latencies; while queries wait for
+      // slots, the batch loop's tuned chunk (as long as a batch, the loop
+      // is throughput-bound then)
       auto const launch_chunk = [&]() {
-        for (uint32_t c = 0; c != chunk; ++c) {
+        auto const n_steps = backlog ? std::max(chunk, e.shape.steps_per_sync) : chunk;
+        this->n_steps += n_steps;
+        n_launches += n_steps * launches_per_step(e);
+        for (uint32_t c = 0; c != n_steps; ++c) {
           if (use_graph) {
             B2R_CUDA(cudaGraphLaunch(e.graph, st));
           } else {
@@ -2093,7 +2112,9 @@ struct serve_state {
           if (!busy) continue;
           launch_chunk();
         }
+        auto const t_sync = std::chrono::steady_clock::now();
         B2R_CUDA(cudaStreamSynchronize(st));
+        sync_ns += ns_since(t_sync);
         in_flight = false;
         std::copy(e.h_summary, e.h_summary + e.S, sum.begin());
         std::vector<uint32_t> done_slots, n_js, n_rows;
@@ -2121,10 +2142,11 @@ struct serve_state {
         for (uint32_t s = 0; s != e.S; ++s) n_active += (slot_item[s] != nullptr && !waiting[s]) ? 1U : 0U;
         if (!phase_follows && busy && done_slots.size() < n_active) launch_chunk();
         if (done_slots.empty()) continue;
+        auto const t_exp = std::chrono::steady_clock::now();
         std::vector<exported> ex;
         std::vector<uint8_t> modes;
         for (auto const s : done_slots) modes.push_back(legs_mode(slot_item[s]->run));
-        export_slots(e, done_slots, n_js, n_rows, ex, e.stream2, &modes, row_target::pooled);
+        export_slots(e, done_slots, n_js, n_rows, ex, e.stream2, &modes, row_target::pinned);
         B2R_CUDA(cudaStreamSynchronize(e.stream2));  // the rows, before any ticket shows finished
         std::vector<uint32_t> retired;
         for (auto i = 0U; i != done_slots.size(); ++i) {
@@ -2148,6 +2170,7 @@ struct serve_state {
           finish(it);
         }
         retire(e, retired, st);
+        export_ns += ns_since(t_exp);
         cv_done.notify_all();
       }
     } catch (std::exception const& ex) {
@@ -2916,7 +2939,7 @@ int b2r_serve_start(b2r_engine* e) {
     if (e->serving) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "engine is already serving");
     try {  // page-locked rows for the one-to-all results the loop exports
       B2R_CUDA(cudaSetDevice(e->tt->device));
-      b2r::prewarm_rows(*e, 32, size_t{512} << 20);
+      b2r::prewarm_rows(*e, 64, size_t{1} << 30);
     } catch (std::exception const& ex) {
       return b2r::fail(B2R_ERR_CUDA, ex.what());
     }
@@ -3016,6 +3039,23 @@ int b2r_release(b2r_engine* e, uint64_t ticket) {
     if (!found->second->finished) return b2r::fail(B2R_ERR_NOT_READY, "ticket still running");
     b2r::give_rows(*e, std::move(found->second->run.res.rt_rows));
     ss->items.erase(found);
+    return B2R_OK;
+  });
+}
+
+int b2r_serve_stats(const b2r_engine* e, b2r_batch_stats* out) {
+  B2R_API_GUARD({
+    if (e == nullptr || out == nullptr) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "null argument");
+    auto* ss = static_cast<b2r::serve_state const*>(e->serve.get());
+    if (ss == nullptr) return b2r::fail(B2R_ERR_INVALID_ARGUMENT, "engine never served");
+    *out = b2r_batch_stats{};
+    out->super_steps = ss->n_steps.load();
+    out->kernel_launches = ss->n_launches.load();
+    out->host_admit_ms = static_cast<double>(ss->admit_ns.load()) / 1e6;
+    out->host_export_ms = static_cast<double>(ss->export_ns.load()) / 1e6;
+    out->host_idle_ms = static_cast<double>(ss->idle_ns.load()) / 1e6;
+    out->host_prep_cpu_ms = static_cast<double>(ss->prep_ns.load()) / 1e6;
+    out->device_ms = static_cast<double>(ss->sync_ns.load()) / 1e6;
     return B2R_OK;
   });
 }

@@ -384,6 +384,12 @@ class Server:
         _check(A.lib().b2r_wait(self.engine.handle, ticket, C.byref(r)))
         return r
 
+    def stats(self) -> A.BatchStats:
+        """Counters of the serving loop since start (b2r_serve_stats)."""
+        s = A.BatchStats()
+        _check(A.lib().b2r_serve_stats(self.engine.handle, C.byref(s)))
+        return s
+
     def release(self, ticket: int):
         _check(A.lib().b2r_release(self.engine.handle, ticket))
 

@@ -83,6 +83,9 @@ def test_served_results_equal_results_alone():
         assert r.latency_ms > 0
         srv.release(tickets[i])
     srv.stop()
+    st = srv.stats()  # the loop's counters stay readable after the stop
+    assert st.super_steps > 0 and st.kernel_launches >= st.super_steps
+    assert st.host_export_ms > 0 and st.host_prep_cpu_ms > 0
     for i in range(n):
         assert got[i] == want[i], i
     assert sum(1 for w in want if w[0] == "journeys" and w[2]) > 10
