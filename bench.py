@@ -697,6 +697,10 @@ def extras_legs(args, h, dtt, qs, B, local, shape):
         "lane_utilisation": st.route_stop_visits / max(1, 32 * st.route_warp_steps),
         "route_scan_share_of_device_time": tm.route_scan_ms / max(1e-9, tm.device_ms),
         "ncu": None if cap is None else cap.get("ncu"),
+        # L2 throughput of the same kernel as a fraction of its peak (ncu,
+        # detailed capture at batch 256): the level that serves its loads
+        "l2_frac": (None if cap is None or not cap.get("ncu")
+                    else cap["ncu"]["l2_throughput_pct"] / 100.0),
     }
     # CPU baseline: the oracle on a bounded sample, all host threads
     sys.path.insert(0, os.path.join(ROOT, "tests"))
