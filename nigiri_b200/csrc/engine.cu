@@ -1953,6 +1953,7 @@ struct serve_state {
   std::thread driver;
   // counters for b2r_serve_stats (nanoseconds of host time by step)
   std::atomic<uint64_t> n_steps{0}, n_launches{0}, admit_ns{0}, export_ns{0}, idle_ns{0}, prep_ns{0}, sync_ns{0};
+  bool backlog{false};  // the last admission left prepared queries waiting for slots (driver thread)
 
   void finish(serve_item& it) {  // with mu held
     auto& r = it.run.res;
@@ -2068,7 +2069,6 @@ struct serve_state {
     return static_cast<uint64_t>(
         std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0).count());
   }
-  bool backlog{false};
 
   // Pipelined like the batch loop: right after the sync of chunk c the
   // next chunk is launched, and the slots that finished in c are exported
