@@ -1600,6 +1600,10 @@ struct slot_picker {
 
 bool sweeps(prepped_query const& p) { return !p.ontrip && !p.one_to_all; }
 
+// one start-time group and nothing after it: the slot's journeys are final
+// when it is done (the queries whose reconstruction waits for that)
+bool single_group(prepped_query const& p) { return p.ontrip && !p.one_to_all && p.recon_mode == 0 && !p.pong; }
+
 // a new interval-extension phase for the query in slot s (search.h:283-316)
 void rearm(b2r_engine& e, uint32_t s, query_run& q, cudaStream_t st) {
   // new phase: upload the new starts (and journeys kept), keep the rt
@@ -1741,6 +1745,8 @@ struct batch_runner {
     // ignored) until that summary has been read.
     constexpr int64_t kRetiring = -2;
     std::vector<uint8_t> stale(S, 0);  // rearmed: the next summary predates it
+    std::vector<uint8_t> held(S, 0);   // finished, export held back (below)
+    std::vector<uint32_t> held_nj(S, 0), held_list;
     std::vector<b2r_engine::summary_t> sum(S);
     bool in_flight = false;
     auto const running = [&]() {
@@ -1807,7 +1813,7 @@ struct batch_runner {
         if (x == kRetiring) x = -1;  // their retirement ran before this summary's chunk ended
       std::vector<uint32_t> done_slots, n_js, n_rows;
       for (uint32_t s = 0; s != S; ++s) {
-        if (slot_q[s] < 0 || waiting[s]) continue;
+        if (slot_q[s] < 0 || waiting[s] || held[s]) continue;
         if (stale[s]) {
           stale[s] = 0;
           continue;
@@ -1823,13 +1829,47 @@ struct batch_runner {
       admit_free();  // into free slots, queued before the next chunk
       // next chunk in flight unless every resident query has just finished
       size_t n_active = 0;
-      for (uint32_t s = 0; s != S; ++s) n_active += (slot_q[s] >= 0 && !waiting[s]) ? 1U : 0U;
+      for (uint32_t s = 0; s != S; ++s) n_active += (slot_q[s] >= 0 && !waiting[s] && !held[s]) ? 1U : 0U;
+      auto const others_run = done_slots.size() < n_active;
+      // Finished queries of one start-time group and nothing after it wait
+      // in their slots (held) while other slots run and no query waits for
+      // a slot, and are exported together: half of the slots at once, or
+      // all of them when nothing else runs.  Each export's journey
+      // rebuilding lasts as long as its longest journey, so fewer exports
+      // rebuild the same journeys in less device time.
+      {
+        std::vector<uint32_t> d2, j2, r2;
+        for (auto i = 0U; i != done_slots.size(); ++i) {
+          auto const s = done_slots[i];
+          if (others_run && next >= runs.size() && single_group(runs[static_cast<size_t>(slot_q[s])].p)) {
+            held[s] = 1;
+            held_nj[s] = n_js[i];
+            held_list.push_back(s);
+          } else {
+            d2.push_back(s);
+            j2.push_back(n_js[i]);
+            r2.push_back(n_rows[i]);
+          }
+        }
+        if (!held_list.empty() && (!others_run || next < runs.size() || held_list.size() >= S / 2U)) {
+          for (auto const s : held_list) {
+            held[s] = 0;
+            d2.push_back(s);
+            j2.push_back(held_nj[s]);
+            r2.push_back(0u);
+          }
+          held_list.clear();
+        }
+        done_slots.swap(d2);
+        n_js.swap(j2);
+        n_rows.swap(r2);
+      }
       // a finished pong phase is followed by the next phase of its sweep:
       // that phase is staged from the export, so the next chunk waits for
       // it instead of leaving the slot idle for a whole chunk
       auto phase_follows = false;
       for (auto const s : done_slots) phase_follows = phase_follows || runs[static_cast<size_t>(slot_q[s])].p.pong;
-      if (!phase_follows && running() && done_slots.size() < n_active) launch_chunk(chunk);
+      if (!phase_follows && running() && others_run) launch_chunk(chunk);
       if (done_slots.empty()) continue;
       auto const t_exp = std::chrono::steady_clock::now();
       std::vector<exported> ex;
