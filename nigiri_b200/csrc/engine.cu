@@ -1833,8 +1833,8 @@ struct batch_runner {
       auto const others_run = done_slots.size() < n_active;
       // Finished queries of one start-time group and nothing after it wait
       // in their slots (held) while other slots run and no query waits for
-      // a slot, and are exported together: half of the slots at once, or
-      // all of them when nothing else runs.  Each export's journey
+      // a slot, and are exported together: a quarter of the slots at once,
+      // or all of them when nothing else runs.  Each export's journey
       // rebuilding lasts as long as its longest journey, so fewer exports
       // rebuild the same journeys in less device time.
       {
@@ -1851,7 +1851,7 @@ struct batch_runner {
             r2.push_back(n_rows[i]);
           }
         }
-        if (!held_list.empty() && (!others_run || next < runs.size() || held_list.size() >= S / 2U)) {
+        if (!held_list.empty() && (!others_run || next < runs.size() || held_list.size() >= S / 4U)) {
           for (auto const s : held_list) {
             held[s] = 0;
             d2.push_back(s);
