@@ -243,10 +243,18 @@ def gpu_arm(args, rank, world, local):
         st = engine.stats()
         return t1 - t0, st, out
 
-    # launch shape picked by the autotuner on a separate sample of the workload
-    tune_qs = QuerySet(h, WORKLOAD, B, seed=9000 + WORKLOAD)
-    tune = eng.autotune(tune_qs.arr, tune_qs.n)
-    shape = {f: getattr(tune.best, f) for f, _ in A.LaunchShape._fields_}
+    # launch shape picked by the autotuner on a separate sample of the
+    # workload, on rank 0; every rank then runs rank 0's shape
+    fields = [f for f, _ in A.LaunchShape._fields_]
+    tune = None
+    picked = [0] * len(fields)
+    if rank == 0:
+        tune_qs = QuerySet(h, WORKLOAD, B, seed=9000 + WORKLOAD)
+        tune = eng.autotune(tune_qs.arr, tune_qs.n)
+        picked = [getattr(tune.best, f) for f in fields]
+    picked = replicas.from_rank0(picked, pg, f"cuda:{local}")
+    eng.shape = A.LaunchShape(*picked)
+    shape = dict(zip(fields, picked))
     for w in range(args.warmup):
         one_batch(w * B)
     clocks = ClockSampler(local)
@@ -302,7 +310,7 @@ def gpu_arm(args, rank, world, local):
             "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot_dev / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int16",
-            "data": "synthetic (seeded generator: timetable seed 2, query seed 1002+rank)",
+            "data": "synthetic (seeded generator: timetable seed 2, query seed 1002 + 7919 x rank)",
             "config": config_block(args, B),
             "method": dict(METHOD, launch_shape=shape,
                            autotune={"tried": tune.n_tried, "start_ms": tune.start_ms,

@@ -35,6 +35,17 @@ def max_over_ranks(values: Sequence[float], group=None, device=None) -> List[flo
     return t.tolist()
 
 
+def from_rank0(values: Sequence[int], group=None, device=None) -> List[int]:
+    """Rank 0's integers on every rank (a launch shape tuned once, so that
+    every replica times the same kernels); identity without a group."""
+    if group is None:
+        return [int(v) for v in values]
+    import torch
+    t = torch.tensor([int(v) for v in values], dtype=torch.int64, device=device)
+    group.broadcast(t, src=0)
+    return [int(v) for v in t.tolist()]
+
+
 def whole_job_throughput(units_per_rank: int, world: int, slowest_seconds: float) -> float:
     """Units all ranks processed / the slowest rank's time."""
     return units_per_rank * world / slowest_seconds

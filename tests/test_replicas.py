@@ -41,8 +41,9 @@ def _rank(rank, world, port, out):
         # 2 (r + 1) seconds of wall time for its 1024 queries
         times = replicas.max_over_ranks([rank + 1.0, 2.0 * (rank + 1)], dist)
         qps = replicas.whole_job_throughput(1024, world, times[0])
+        shape = replicas.from_rank0([32 + rank, 256, 8 * (rank + 1), 2, 4, rank], dist)
         dist.barrier()
-        out[rank] = (times, qps, list(replicas.shard(4096, rank, world)))
+        out[rank] = (times, qps, list(replicas.shard(4096, rank, world)), shape)
     finally:
         dist.destroy_process_group()
 
@@ -56,7 +57,8 @@ def test_two_gloo_ranks_take_the_slowest_rank():
                        start_method="spawn")
     assert set(out.keys()) == {0, 1}
     for r in range(world):
-        times, qps, part = out[r]
+        times, qps, part, shape = out[r]
         assert times == [2.0, 4.0]          # max over ranks, on every rank
+        assert shape == [32, 256, 8, 2, 4, 0]  # rank 0's launch shape, on every rank
         assert qps == pytest.approx(1024 * 2 / 2.0)
     assert sorted(out[0][2] + out[1][2]) == list(range(4096))
