@@ -64,6 +64,18 @@ class FixtureTimetable:
             lst = sorted(fps[l], key=lambda w: w >> 23)  # stable by duration
             fp_data += lst
             fp_index[l + 1] = len(fp_data)
+        # footpaths of profiles 1..4 ("profile_footpaths": {"p": [[a, b, min]]})
+        self.profile_fp = {}
+        for prf, lst in spec.get("profile_footpaths", {}).items():
+            pf = [[] for _ in range(n_loc)]
+            for a_, b_, dur in lst:
+                pf[self.loc_idx[a_]].append((self.loc_idx[b_] & 0x7FFFFF) | (dur << 23))
+            idx = np.zeros(n_loc + 1, np.uint32)
+            dat = []
+            for l in range(n_loc):
+                dat += sorted(pf[l], key=lambda w: w >> 23)
+                idx[l + 1] = len(dat)
+            self.profile_fp[int(prf)] = (idx, np.array(dat or [0], np.uint32))
         # bitfields: one per distinct traffic day set
         bf_list = [np.zeros(8, np.uint64)]
         bf_of = {}
@@ -76,10 +88,11 @@ class FixtureTimetable:
         transport_bf = []
         self.transport_names = []
         for r in spec["routes"]:
-            for s in r["stops"]:
+            for k, s in enumerate(r["stops"]):
                 w = r.get("stop_flags", {}).get(s, (1, 1))
+                wc = r["stop_wc"][k] if "stop_wc" in r else (1, 1)  # wheelchair in / out
                 route_stops.append(self.loc_idx[s] | (w[0] << 28) | (w[1] << 29)
-                                   | (1 << 30) | (1 << 31))
+                                   | (wc[0] << 30) | (wc[1] << 31))
             route_stop_index.append(len(route_stops))
             route_clasz.append(r.get("clasz", 10))
             section_flags += list(r.get("sections", [0] * (len(r["stops"]) - 1))) + [0]
@@ -125,6 +138,9 @@ class FixtureTimetable:
             base.parent = p(a["parent"], C.c_uint32)
         base.footpaths_out_index = p(a["fp_index"], C.c_uint32)
         base.footpaths_out = p(a["fp_data"], C.c_uint32)
+        for prf, (idx, dat) in self.profile_fp.items():
+            base.profile_footpaths_out_index[prf - 1] = p(idx, C.c_uint32)
+            base.profile_footpaths_out[prf - 1] = p(dat, C.c_uint32)
         base.n_routes = len(spec["routes"])
         base.route_stop_index = p(a["route_stop_index"], C.c_uint32)
         base.route_stops = p(a["route_stops"], C.c_uint32)
@@ -238,6 +254,8 @@ class FixtureQuery:
             qq.algorithm = A.B2R_ALGO_PONG
         if "claszes" in q:
             qq.allowed_claszes = q["claszes"]
+        if "prf" in q:
+            qq.prf_idx = q["prf"]
         qq.require_bike_transport = 1 if q.get("bikes") else 0
         qq.require_car_transport = 1 if q.get("cars") else 0
         qq.no_compulsory_reservation = 1 if q.get("no_reservation") else 0

@@ -63,7 +63,8 @@ def group_routes(services):
     order = []
     for svc in services:
         k = (tuple(svc["stops"]), svc.get("clasz", 10),
-             tuple(svc.get("sections", [0] * (len(svc["stops"]) - 1))))
+             tuple(svc.get("sections", [0] * (len(svc["stops"]) - 1))),
+             tuple(tuple(x) for x in svc.get("wc", ())))
         if k not in keys:
             keys[k] = [[svc]]
             order.append(k)
@@ -78,10 +79,13 @@ def group_routes(services):
     routes = []
     for k in order:
         for sub in keys[k]:
-            routes.append({"stops": list(k[0]), "clasz": k[1], "sections": list(k[2]),
-                           "transports": [
-                               {kk: v for kk, v in x.items()
-                                if kk not in ("stops", "clasz", "sections")} for x in sub]})
+            route = {"stops": list(k[0]), "clasz": k[1], "sections": list(k[2]),
+                     "transports": [
+                         {kk: v for kk, v in x.items()
+                          if kk not in ("stops", "clasz", "sections", "wc")} for x in sub]}
+            if k[3]:
+                route["stop_wc"] = [list(x) for x in k[3]]
+            routes.append(route)
     return routes
 
 
@@ -358,6 +362,7 @@ def gtfs_pong_gap():
 
 
 FLAG_CARS = 1
+FLAG_WHEELCHAIR = 2
 
 
 def gtfs_alternative_block(flag, first_has):
@@ -401,6 +406,53 @@ FOOTPATH = re.compile(r"^\s+FOOTPATH \(duration=(\d+)\)$")
 MUMO = re.compile(r"^\s+MUMO \(id=(\d+), duration=(\d+)\)$")
 TRIP = re.compile(r"\{name=([^,]*), day=([^,]*), id=([^,]*), src=")
 STOPLINE = re.compile(r"^\s+\d+: ")
+
+
+def gtfs_wheelchair_assistance():
+    """test/routing/wheelchair_assistance_test.cc: agency Europe/Berlin
+    (UTC+2 on 2024-06-19), service S on 2024-06-19 only, route type 101
+    (high speed: clasz 1), every trip wheelchair accessible (the wheelchair
+    route flag on every section), no stop with wheelchair_boarding = 2:
+      T1 A 00:00 - B1 00:30 - C 01:10   every hour from 00:00 to 23:00
+      T2 B2 00:40 - C 00:50             every hour from 00:40 to 23:40
+    (frequencies.txt, local times).  For high-speed, long-distance and night
+    trips the loader keeps a stop time's wheelchair boarding (alighting) bit
+    only while assistance is available at the stop at its local departure
+    (arrival) minute (include/nigiri/loader/gtfs/local_to_utc.h:277-340);
+    the assistance of a stop is the first entry within 800 m
+    (include/nigiri/loader/assistance.h:17-28).  The test's entries A, B
+    (at B1 and B2) and C are open 08:00-22:00 local (C's "Th; 08:00-22:00":
+    its second rule covers every day).  Trips whose bits differ get routes of
+    their own (the route key is the stop sequence with these bits).  The test
+    adds the footpath B1 -> B2 (5 min) to profiles 0 and 2 (wheelchair)."""
+    def open_at(minute):  # local minutes after 2024-06-19 00:00
+        m = minute % 1440
+        return 8 * 60 <= m < 22 * 60
+
+    services = []
+    for j in range(24):
+        d = 60 * j  # local departure at A
+        ev = [d, d + 30, d + 30, d + 70]  # A dep, B1 arr, B1 dep, C arr
+        wc = [[1 if open_at(ev[0]) else 0, 1], [1 if open_at(ev[2]) else 0, 1 if open_at(ev[1]) else 0],
+              [1, 1 if open_at(ev[3]) else 0]]
+        services.append(dict(utc_service("RE 1", ["A", "B1", "C"], "2024-06-19", [x - 120 for x in ev]),
+                             clasz=1, sections=[1 << FLAG_WHEELCHAIR] * 2, wc=wc))
+    for j in range(24):
+        d = 40 + 60 * j  # local departure at B2
+        ev = [d, d + 10]
+        wc = [[1 if open_at(ev[0]) else 0, 1], [1, 1 if open_at(ev[1]) else 0]]
+        services.append(dict(utc_service("RE 2", ["B2", "C"], "2024-06-19", [x - 120 for x in ev]),
+                             clasz=1, sections=[1 << FLAG_WHEELCHAIR], wc=wc))
+    return {
+        "date_range": ["2024-06-18", "2024-06-20"],
+        "locations": [{"id": x, "name": x, "transfer_time": 2} for x in ("A", "B1", "B2", "C", "D")],
+        "footpaths": [["B1", "B2", 5]],
+        "profile_footpaths": {"2": [["B1", "B2", 5]]},
+        "routes": group_routes(services),
+    }
+
+
+TIMETABLES["gtfs_wheelchair_assistance"] = gtfs_wheelchair_assistance()
 
 
 def unix_min(s: str) -> int:
@@ -651,6 +703,18 @@ def known_answers(ref_root: str):
     ka.append(dict(name="pong_gap_truncation_pong", kind="departures", timetable="gtfs_pong_gap",
                    ref="test/routing/pong_gap_truncation_test.cc",
                    query=dict(gq, algorithm="pong"), not_before=t("2024-06-19 10:00")))
+    # wheelchair_assistance_test.cc: A -> C, 05:00-21:00 UTC on 2024-06-19,
+    # the first and last departures of the walking (0) and wheelchair (2)
+    # profiles' results
+    src = open(os.path.join(ref_root, "test/routing/wheelchair_assistance_test.cc")).read()
+    assert "sys_days{2024_y / June / 19} + 6_hours" in src and "sys_days{2024_y / June / 19} + 19_hours" in src
+    for prf, first, last in ((0, "05:00", "20:00"), (2, "06:00", "19:00")):
+        ka.append(dict(name=f"wheelchair_assistance_prf{prf}", kind="departure_range",
+                       timetable="gtfs_wheelchair_assistance",
+                       ref="test/routing/wheelchair_assistance_test.cc",
+                       query=dict(start=[["A", 0, 0]], dest=[["C", 0, 0]], direction="fwd",
+                                  interval=[t("2024-06-19 05:00"), t("2024-06-19 21:00")], prf=prf),
+                       expected=[t(f"2024-06-19 {first}"), t(f"2024-06-19 {last}")]))
     # pong_get_earliest_alternative_test.cc: A -> C between 06:00 and 12:00
     # UTC on the block transport, found without the flag, not with it
     for tt_name, key in (("gtfs_alternative_bikes", "bikes"), ("gtfs_alternative_cars", "cars")):

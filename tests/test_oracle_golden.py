@@ -86,6 +86,10 @@ def test_oracle_known_answers(ka, timetables):
             assert deps == ka["expected"]
         if "not_before" in ka:
             assert all(d >= ka["not_before"] for d in deps)
+    elif ka["kind"] == "departure_range":  # the first and last departure of the results
+        r = oracle_lib.OracleResult(tt.desc, q.q)
+        deps = sorted(j["dep"] for j in F.journeys_to_records(tt, r.view))
+        assert deps and [deps[0], deps[-1]] == ka["expected"]
     elif ka["kind"] == "earliest_alternative":
         legs = (A.Leg * 3)()
         qq = q.q

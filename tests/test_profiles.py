@@ -172,3 +172,27 @@ def test_profile_without_footpaths_and_bad_profile(engines):
     for i in range(qs.n - 1):
         assert records(out[i]) == oracle_lib.OracleResult(h.desc, arr[i]).records(), i
     assert out[qs.n - 1].status == A.B2R_ERR_INVALID_ARGUMENT
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prf", [0, WC])
+def test_wheelchair_assistance_golden_on_gpu(prf):
+    """nigiri's wheelchair_assistance_test.cc restated as a fixture (the
+    assistance hours turned into the stop times' wheelchair bits): the
+    engine's first and last departures are the test's, and every journey is
+    the oracle's."""
+    import fixture as F
+    from nigiri_b200 import routing as R
+    cases = F.load_cases()
+    ka = next(k for k in cases["known_answers"] if k["name"] == f"wheelchair_assistance_prf{prf}")
+    ftt = F.FixtureTimetable(cases["timetables"][ka["timetable"]], A.lib())
+    tt = R.Timetable(ftt.desc, owner=ftt)
+    eng = R.Engine(tt, max_slots=32)
+    q = F.FixtureQuery(A.lib(), ftt, ka["query"])
+    out = A.Result()
+    assert A.lib().b2r_search_batch(eng.handle, C.byref(q.q), 1, C.byref(out)) == 0
+    got = F.journeys_to_records(ftt, out)
+    deps = sorted(j["dep"] for j in got)
+    assert deps and [deps[0], deps[-1]] == ka["expected"]
+    ref = oracle_lib.OracleResult(ftt.desc, q.q)  # owns the records its view points to
+    assert got == F.journeys_to_records(ftt, ref.view)
