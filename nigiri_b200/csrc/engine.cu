@@ -614,7 +614,9 @@ void enqueue_superstep(b2r_engine& e, cudaStream_t s) {
   auto const slot_blocks = (e.S + 127) / 128;
   auto const list_blocks = e.sms * 8;
   dev::k_ctl_begin<<<list_blocks, 256, 0, s>>>(st);
-  dev::k_sweep<<<e.sms * 16, 256, 0, s>>>(st);
+  // a warp per 32-location chunk of the sweep: one pass over the locations
+  auto const sweep_chunks = (st.tt.n_loc + 31U) / 32U;
+  dev::k_sweep<<<std::min<uint32_t>(e.sms * 16U, std::max<uint32_t>(1U, (sweep_chunks + 7U) / 8U)), 256, 0, s>>>(st);
   dev::k_ctl_dest<<<slot_blocks, 128, 0, s>>>(st);
   auto const pair_blocks = e.sms * e.shape.pair_blocks_per_sm;
   dev::k_mark_routes<<<pair_blocks, 256, 0, s>>>(st);
