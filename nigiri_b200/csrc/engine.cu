@@ -82,26 +82,6 @@ void host_copy(std::vector<T>& v, T const* p, size_t n) {
 }  // namespace b2r
 
 // ==================================================================== engine
-// Allocator whose value-initialisation is default-initialisation: large
-// result arrays that are overwritten right away are not zero-filled first.
-template <typename T>
-struct uninit_allocator : std::allocator<T> {
-  template <typename U>
-  struct rebind {
-    using other = uninit_allocator<U>;
-  };
-  using std::allocator<T>::allocator;
-  template <typename U>
-  void construct(U* p) noexcept {
-    ::new (static_cast<void*>(p)) U;
-  }
-  template <typename U, typename... Args>
-  void construct(U* p, Args&&... args) {
-    ::new (static_cast<void*>(p)) U(std::forward<Args>(args)...);
-  }
-};
-using row_vector = std::vector<int16_t, uninit_allocator<int16_t>>;
-
 // One-to-all rows of one result: page-locked host memory when the batch
 // path copies the rows straight into it from the device, else ordinary
 // heap memory (the serving loop, whose results live until b2r_release).
